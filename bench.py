@@ -1,0 +1,344 @@
+"""Benchmark: FP32 PageRank on a scale-24 RMAT graph, one B200 per rank.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the configuration the headline metric is quoted on): RMAT scale 24
+(16.8M vertices), edge factor 16, a/b/c/d = .57/.19/.19/.05, symmetrised and
+deduplicated (~5.3e8 directed entries), uint32 CSR in NWGraph's adjacency<1>
+layout, damping 0.85, 20 fixed sweeps (threshold 0), FP32 scores. One step =
+one full solve. Inputs are seeded synthetic (the reference's GAP datasets are
+not available here); col[] alone (2.1 GB) is far larger than L2, so no L2
+flush is needed between steps.
+
+Our arm prints one JSON line with
+  value     GTEPS per sweep (nnz / sweep time) over K solves with the CSR and
+            degrees resident in HBM, CUDA events on the launching stream,
+            max over ranks;
+  e2e       the same metric through the public API with pinned HOST buffers:
+            graph upload + validation + tiling, the solve, ranks back to host;
+  roofline  the sweep kernel against the measured HBM copy bandwidth, with the
+            graded bytes per sweep 4 nnz + 4 (n+1) + 20 n;
+  cpu_baseline  NWGraph's page_rank (v11) compiled from its headers at its
+            release flags, timed on this host's cores on a 2-sweep sample.
+With --gpus N (torchrun) every rank solves its own resident replica
+(weak scaling, no data-path collective).
+
+--impl reference runs NWGraph's own page_rank on this host's CPU cores
+(rank 0 only), each step a 2-sweep sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "PR GTEPS/iter & %HBM roofline; batched PPR vs looped plain at 1e-6 L1; bwd/fwd"
+UNIT = "GTEPS"
+DAMPING = 0.85
+SWEEPS = 20
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=int, default=24)
+    ap.add_argument("--edge-factor", type=float, default=16)
+    ap.add_argument("--seed", type=int, default=42)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-sample-sweeps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def graded_bytes(n, nnz):
+    return 4.0 * nnz + 4.0 * (n + 1) + 20.0 * n
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def sweep_traffic_per_launch():
+    """DRAM bytes per sweep launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "pr_sweep_scale24.md")
+    try:
+        m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.out = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.out.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_graph(args):
+    from nwgraph_b200 import graphs as G
+    t0 = time.time()
+    g = G.rmat(args.scale, args.edge_factor, args.seed)
+    return g, g.out_degree(), time.time() - t0
+
+
+def cpu_reference_sample(g, deg, sweeps, nthreads):
+    """NWGraph page_rank v11 at its release flags on this host (oracle/_ref),
+    or the C restatement of page_rank_v10 when the reference build is absent."""
+    import oracle as O
+    if O.ref_available(fast=True):
+        rg = O.RefGraph(g.row_ptr, g.col, deg, fast=True)
+        _, it, _, secs = rg.page_rank(11, DAMPING, 0.0, sweeps, nthreads)
+        rg.close()
+        t = float(np.mean(secs))
+        return {"value": g.nnz / t / 1e9, "unit": UNIT, "cores": nthreads, "kind": "reference",
+                "sample": f"{it} sweeps of nw::graph::page_rank (v11, -Ofast, TBB-API shim) on the full graph; "
+                          f"mean sweep {t * 1e3:.1f} ms from the reference's own trace"}
+    t0 = time.perf_counter()
+    O.jacobi_f32(g.row_ptr, g.col, deg, DAMPING, 0.0, 1)
+    t = time.perf_counter() - t0
+    return {"value": g.nnz / t / 1e9, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "1 sweep of the C restatement of page_rank_v10 on the full graph (includes init)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    g, deg, _ = make_graph(args)
+    nthreads = os.cpu_count() or 1
+    import oracle as O
+    kind = "reference" if O.ref_available(fast=True) else "port"
+    if kind == "reference":
+        rg = O.RefGraph(g.row_ptr, g.col, deg, fast=True)
+        run = lambda: rg.page_rank(11, DAMPING, 0.0, args.cpu_sample_sweeps, nthreads)[3]  # noqa: E731
+    else:
+        run = lambda: np.array([_time_port(g, deg)])  # noqa: E731
+    for _ in range(args.warmup):
+        run()
+    secs = np.concatenate([run() for _ in range(args.steps)])
+    t = float(np.mean(secs))
+    value = g.nnz / t / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3 * args.cpu_sample_sweeps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"rmat{args.scale}_ef{int(args.edge_factor)}_pagerank_f32", "n": g.n, "nnz": g.nnz,
+                   "sweeps_per_step": args.cpu_sample_sweeps, "damping": DAMPING},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads if kind == "reference" else 1, "kind": kind,
+                         "sample": f"{args.steps} steps x {args.cpu_sample_sweeps} sweeps of nw::graph::page_rank "
+                                   f"(v11) on the full graph, sweep times from its own trace"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _time_port(g, deg):
+    import oracle as O
+    t0 = time.perf_counter()
+    O.jacobi_f32(g.row_ptr, g.col, deg, DAMPING, 0.0, 1)
+    return time.perf_counter() - t0
+
+
+def run_ours(args):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    from nwgraph_b200 import Graph
+    g, deg, gen_s = make_graph(args)
+    n, nnz = g.n, g.nnz
+    B = graded_bytes(n, nnz)
+    stream = torch.cuda.current_stream(dev)
+
+    # ---- resident: CSR + degrees in HBM ------------------------------------
+    rp_d = torch.from_numpy(g.row_ptr.view(np.int32)).to(dev)
+    cl_d = torch.from_numpy(g.col.view(np.int32)).to(dev)
+    deg_d = torch.from_numpy(deg.view(np.int32)).to(dev)
+    out_d = torch.empty(n, dtype=torch.float32, device=dev)
+    h = Graph(rp_d, cl_d)
+    del rp_d, cl_d
+    for _ in range(max(args.warmup, 3)):
+        h.page_rank(deg_d, out_d, DAMPING, 0.0, SWEEPS, stream=stream)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    sweep_ms, iters = 0.0, 0
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            st = h.page_rank(deg_d, out_d, DAMPING, 0.0, SWEEPS, stream=stream)
+            sweep_ms += st.device_ms
+            iters += st.iterations
+        e1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    total_ms = e0.elapsed_time(e1)
+    t = torch.tensor([total_ms, sweep_ms / max(iters, 1)], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms, t_sweep_ms = float(t[0]), float(t[1])
+    ms_per_step = total_ms / args.steps
+    value = world * nnz * SWEEPS / (ms_per_step * 1e-3) / 1e9
+    # threshold-1e-4 run (config: "20 fixed iterations plus a threshold-1e-4 run")
+    st_thr = h.page_rank(deg_d, out_d, DAMPING, 1e-4, 1000, stream=stream)
+
+    # ---- end to end through the public API with pinned host buffers ---------
+    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
+    rp_h, cl_h, deg_h = pin(g.row_ptr), pin(g.col), pin(deg)
+    out_h = torch.empty(n, dtype=torch.float32).pin_memory().numpy()
+    e2e_steps = max(1, args.e2e_steps)
+
+    def e2e_step():
+        with Graph(rp_h, cl_h) as hh:
+            hh.page_rank(deg_h, out_h, DAMPING, 0.0, SWEEPS)
+
+    e2e_step()  # warm-up (context, allocator)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    w0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    f1.record(stream)
+    torch.cuda.synchronize()
+    wall_e2e = (time.perf_counter() - w0) / e2e_steps
+    e2e_ms = f0.elapsed_time(f1) / e2e_steps
+    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_ms = float(te[0])
+    e2e_value = world * nnz * SWEEPS / (e2e_ms * 1e-3) / 1e9
+
+    info = h.info()
+    h.release()
+
+    peak, peak_kind = peaks()
+    achieved = B / (t_sweep_ms * 1e-3) / 1e9
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_reference_sample(g, deg, args.cpu_sample_sweeps, os.cpu_count() or 1)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"rmat{args.scale}_ef{int(args.edge_factor)}_pagerank_f32", "n": n, "nnz": nnz,
+                   "sweeps_per_step": SWEEPS, "threshold": 0.0, "damping": DAMPING,
+                   "l2": "inputs larger than L2 (col 4*nnz bytes), no flush", "parallelism": f"replicas{world}",
+                   "tile_items": info["tile_items"], "grid": info["grid"], "num_tiles": info["num_tiles"]},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": sweep_traffic_per_launch(), "peak_kind": peak_kind,
+                     "bytes_per_sweep": B, "sweep_ms": t_sweep_ms},
+        "gteps_per_sweep_kernel": nnz / (t_sweep_ms * 1e-3) / 1e9,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(4 * (n + 1) + 4 * nnz + 4 * n),
+                "d2h_bytes_per_step": int(4 * n), "ms_per_step": e2e_ms, "wall_ms_per_step": wall_e2e * 1e3,
+                "includes": "H2D of row_ptr+col+degrees, device validation + tiling, 20 sweeps, D2H of ranks"},
+        "threshold_run": {"threshold": 1e-4, "sweeps": st_thr.iterations, "converged": st_thr.converged,
+                          "device_ms": st_thr.device_ms},
+        "gpu_launches": args.steps * (SWEEPS + 2),
+        "clocks": clk.summary(),
+        "graph_gen_s": gen_s,
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

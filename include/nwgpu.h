@@ -1,0 +1,132 @@
+/*
+ * nwgpu.h -- C ABI of the B200 PageRank engine (libnwgpu.so).
+ *
+ * This is the drop-in boundary for NWGraph's PageRank hot path. It replaces
+ *
+ *   template <adjacency_list_graph Graph, typename Real>
+ *   void nw::graph::page_rank(const Graph& graph,
+ *                             const std::vector<vertex_id_type>& degrees,
+ *                             std::vector<Real>& page_rank,
+ *                             Real damping_factor, Real threshold,
+ *                             size_t max_iters, size_t num_threads);
+ *     include/nwgraph/algorithms/page_rank.hpp:89-91 (v11)
+ *     include/nwgraph/experimental/algorithms/page_rank.hpp:377-379 (v10, same signature)
+ *
+ * with a graph handle (the CSR uploaded once) and a solve call carrying the
+ * same parameters. The C++20 layer in include/nwgraph_gpu/page_rank.hpp keeps
+ * the reference's exact call surface on top of these functions.
+ *
+ * Conventions
+ *  - Every function returns an int status (NWGPU_OK == 0); none throws or
+ *    aborts. nwgpu_last_error() returns the calling thread's last message.
+ *  - The CSR is NWGraph's adjacency<1> (include/nwgraph/adjacency.hpp:86-195):
+ *    row_ptr = indices_ (n+1 uint32), col = std::get<0>(to_be_indexed_)
+ *    (nnz uint32); row i lists the in-neighbours j of i (edge j -> i).
+ *    uint32 indices as default_index_t (include/nwgraph/util/defaults.hpp:23-24).
+ *  - out_degree[j] is the out-degree of j, as the benchmark's build_degrees
+ *    computes it (bench/gapbs/common.hpp:110-121).
+ *  - A handle owns one CUDA stream; calls on one handle are serialised by the
+ *    caller, calls on distinct handles may run concurrently.
+ *  - There is no CPU fallback: without a usable sm_100 device every call that
+ *    needs one returns NWGPU_ERR_CUDA / NWGPU_ERR_NO_DEVICE.
+ */
+#ifndef NWGPU_H
+#define NWGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NWGPU_ABI_VERSION 1
+
+enum nwgpu_status {
+  NWGPU_OK = 0,
+  NWGPU_ERR_INVALID_ARG = 1,   /* null pointer, bad size, damping outside [0,1], ... */
+  NWGPU_ERR_INVALID_GRAPH = 2, /* row_ptr not monotone, row_ptr[n] != nnz, col[k] >= n */
+  NWGPU_ERR_CUDA = 3,          /* a CUDA runtime call failed (message has the CUDA error) */
+  NWGPU_ERR_OUT_OF_MEMORY = 4,
+  NWGPU_ERR_ABORTED = 5,       /* nwgpu_abort() was called while the solve ran */
+  NWGPU_ERR_NO_DEVICE = 6,     /* no CUDA device, or not compute capability 10.x */
+  NWGPU_ERR_UNSUPPORTED = 7
+};
+
+typedef struct nwgpu_graph nwgpu_graph;
+
+/* nwgpu_graph_create flags */
+#define NWGPU_GRAPH_DEVICE_PTRS 0x1u /* row_ptr / col / weights are device pointers (copied device-to-device) */
+#define NWGPU_GRAPH_TRANSPOSE 0x2u   /* also keep the out-row CSR (adjacency<0>) needed by nwgpu_pr_vjp */
+
+/* Upload a CSR once (replaces the per-call use of graph.indices_ /
+ * to_be_indexed_ at page_rank.hpp:129). Validates it on the device
+ * (monotone row_ptr, row_ptr[0] == 0, row_ptr[n] == nnz, every col < n) and
+ * partitions it into equal-work merge-path tiles. weights may be NULL
+ * (unweighted); with weights the graph can also run weighted PageRank and its
+ * adjoint. Uses the current CUDA device. */
+int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float* weights, uint64_t n, uint64_t nnz,
+                       uint32_t flags, nwgpu_graph** out);
+int nwgpu_graph_destroy(nwgpu_graph* g);
+
+typedef struct nwgpu_graph_info {
+  uint64_t n, nnz;
+  uint64_t num_tiles;    /* merge-path tiles of one sweep */
+  uint32_t tile_items;   /* rows + entries per tile */
+  uint32_t grid;         /* persistent CTAs per sweep */
+  uint64_t device_bytes; /* HBM held by the handle */
+  int32_t  device;
+  int32_t  has_weights, has_transpose;
+} nwgpu_graph_info;
+int nwgpu_graph_get_info(const nwgpu_graph* g, nwgpu_graph_info* info);
+
+/* Solve modes */
+#define NWGPU_MODE_PARITY 0u     /* page_rank_v10 semantics: Jacobi, leak (no dangling redistribution) */
+/* Launch strategies */
+#define NWGPU_LAUNCH_GRAPH 0u    /* CUDA graph; device-side while loop, convergence tested on the GPU */
+#define NWGPU_LAUNCH_STREAM 1u   /* one kernel per sweep on the stream; sweeps after convergence exit at once */
+
+typedef struct nwgpu_pr_options {
+  uint32_t size;        /* sizeof(nwgpu_pr_options); 0 fields mean defaults */
+  uint32_t mode;        /* NWGPU_MODE_* */
+  uint32_t launch;      /* NWGPU_LAUNCH_* */
+  uint32_t device_ptrs; /* 1: degrees / ranks / vectors are device pointers */
+  uint32_t reserved0;
+  void*    stream;      /* cudaStream_t to run the solve on; NULL = the handle's own stream */
+  uint32_t reserved[2];
+} nwgpu_pr_options;
+
+typedef struct nwgpu_pr_stats {
+  uint64_t iterations;     /* sweeps run, counting the one whose error fell below threshold */
+  double   final_error;    /* L1 change of the last sweep (FP64, as page_rank.hpp:125-134) */
+  int32_t  converged;      /* final_error < threshold */
+  double   device_ms;      /* CUDA-event time of the sweep loop */
+  double   ms_per_iter;
+  double   bytes_per_iter; /* algorithmic bytes of one sweep: 4 nnz + 4 (n+1) + 20 n */
+  double   gteps;          /* nnz * iterations / device time */
+  double*  errors;         /* optional, caller-owned: per-sweep L1 errors */
+  uint64_t errors_cap;     /* capacity of errors[] */
+} nwgpu_pr_stats;
+
+/* PageRank over the uploaded graph: the body of page_rank / page_rank_v10
+ * (page_rank.hpp:92-147). ranks[n] is fully overwritten; damping, threshold
+ * and max_iters mean what they mean there (stop after the first sweep whose
+ * FP64 L1 change is < threshold, at most max_iters sweeps). out_degree[n] and
+ * ranks[n] are host pointers unless options->device_ptrs. */
+int nwgpu_pr_run(nwgpu_graph* g, const uint32_t* out_degree, float* ranks, float damping, float threshold,
+                 uint64_t max_iters, const nwgpu_pr_options* options, nwgpu_pr_stats* stats);
+
+/* Ask a running solve on g to stop at its next sweep boundary; the solve
+ * returns NWGPU_ERR_ABORTED. Safe to call from another host thread. */
+int nwgpu_abort(nwgpu_graph* g);
+
+/* Thread-local message for the last failing call (empty if none). Returns
+ * the message length. */
+int nwgpu_last_error(char* buf, size_t len);
+
+int nwgpu_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NWGPU_H */

@@ -1,0 +1,431 @@
+// C ABI of the PageRank engine (declared in include/nwgpu.h).
+//
+// Host side of the drop-in: nwgpu_graph_create uploads and validates the CSR
+// once and tiles it on the device; nwgpu_pr_run replaces the body of
+// nw::graph::page_rank / page_rank_v10 (include/nwgraph/algorithms/page_rank.hpp:92-147,
+// include/nwgraph/experimental/algorithms/page_rank.hpp:383-431) with one
+// CUDA-graph launch whose while loop runs the fused sweep kernel until the
+// device-side test "error < threshold" or max_iters stops it.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+
+#include "../../include/nwgpu.h"
+#include "engine.h"
+
+using namespace nwgpu;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+  char    buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    return fail(NWGPU_ERR_OUT_OF_MEMORY, "%s: %s", what, cudaGetErrorString(e));
+  }
+  return fail(NWGPU_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(call, what)                       \
+  do {                                       \
+    cudaError_t _e = (call);                 \
+    if (_e != cudaSuccess) return cuda_fail(_e, what); \
+  } while (0)
+
+int default_ipt() { return 8; }
+
+}  // namespace
+
+struct nwgpu_graph {
+  int          device = 0;
+  int          sms = 148;
+  cudaStream_t stream = nullptr;
+  uint64_t     n = 0, nnz = 0;
+  uint32_t*    row_ptr = nullptr;
+  uint32_t*    col = nullptr;
+  float*       weights = nullptr;
+  uint32_t*    t_row_ptr = nullptr;  // out-row CSR (adjacency<0>) for the adjoint
+  uint32_t*    t_col = nullptr;
+  uint32_t*    t_perm = nullptr;     // t_col entry -> entry of the in-row CSR
+  Tiling       tiling{};
+  int          grid = 0;
+  uint64_t     device_bytes = 0;
+
+  // Plain-solve buffers, allocated on first use and kept.
+  bool         solve_ready = false;
+  float*       rank = nullptr;
+  float*       contrib[2] = {nullptr, nullptr};
+  uint32_t*    deg = nullptr;
+  float*       cpart = nullptr;
+  float*       epart = nullptr;
+  uint32_t*    cnt = nullptr;
+  double*      res_part = nullptr;
+  PrState*     st = nullptr;
+  double*      err_hist = nullptr;
+  uint32_t     err_cap = 4096;
+  PrState*     h_st = nullptr;               // pinned mirror of *st
+  unsigned int* h_abort = nullptr;           // mapped pinned abort word
+  unsigned int* d_abort = nullptr;
+  cudaEvent_t  ev0 = nullptr, ev1 = nullptr;
+
+  // CUDA graph of the sweep loop (arm node -> while node { sweep }).
+  cudaGraph_t     cg = nullptr;
+  cudaGraphExec_t cg_exec = nullptr;
+  float           cg_damping = 0.f, cg_base = 0.f;  // scalars baked into cg_exec
+
+  ~nwgpu_graph() {
+    if (cg_exec) cudaGraphExecDestroy(cg_exec);
+    if (cg) cudaGraphDestroy(cg);
+    void* dev_ptrs[] = {row_ptr, col, weights, t_row_ptr, t_col, t_perm, tiling.tile_row, tiling.tile_nnz, rank,
+                        contrib[0], contrib[1], deg, cpart, epart, cnt, res_part, st, err_hist};
+    for (void* p : dev_ptrs)
+      if (p) cudaFree(p);
+    if (h_st) cudaFreeHost(h_st);
+    if (h_abort) cudaFreeHost(h_abort);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+template <class T>
+cudaError_t dalloc(nwgpu_graph* g, T** p, uint64_t count) {
+  const uint64_t bytes = (count ? count : 1) * sizeof(T);
+  cudaError_t    e = cudaMalloc((void**)p, bytes);
+  if (e == cudaSuccess) g->device_bytes += bytes;
+  return e;
+}
+
+int check_device(int* dev_out, int* sms_out) {
+  int dev = 0, count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return fail(NWGPU_ERR_NO_DEVICE, "no CUDA device available (%s)", cudaGetErrorString(e));
+  }
+  CK(cudaGetDevice(&dev), "cudaGetDevice");
+  int major = 0, sms = 0;
+  CK(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev), "cudaDeviceGetAttribute");
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+  if (major != 10) return fail(NWGPU_ERR_NO_DEVICE, "device %d is sm_%d0, this build targets sm_100a only", dev, major);
+  *dev_out = dev;
+  *sms_out = sms;
+  return NWGPU_OK;
+}
+
+int ensure_solve_buffers(nwgpu_graph* g) {
+  if (g->solve_ready) return NWGPU_OK;
+  const uint64_t n = g->n, T = g->tiling.num_tiles;
+  CK(dalloc(g, &g->rank, n), "cudaMalloc(rank)");
+  CK(dalloc(g, &g->contrib[0], n), "cudaMalloc(contrib)");
+  CK(dalloc(g, &g->contrib[1], n), "cudaMalloc(contrib)");
+  CK(dalloc(g, &g->deg, n), "cudaMalloc(deg)");
+  CK(dalloc(g, &g->cpart, T + 1), "cudaMalloc(cpart)");
+  CK(dalloc(g, &g->epart, T + 1), "cudaMalloc(epart)");
+  CK(dalloc(g, &g->cnt, T + 1), "cudaMalloc(cnt)");
+  CK(dalloc(g, &g->res_part, (uint64_t)g->grid), "cudaMalloc(res_part)");
+  CK(dalloc(g, &g->st, 1), "cudaMalloc(state)");
+  CK(dalloc(g, &g->err_hist, g->err_cap), "cudaMalloc(err_hist)");
+  CK(cudaMemsetAsync(g->cnt, 0, (T + 1) * sizeof(uint32_t), g->stream), "cudaMemset(cnt)");
+  CK(cudaMemsetAsync(g->st, 0, sizeof(PrState), g->stream), "cudaMemset(state)");
+  CK(cudaHostAlloc((void**)&g->h_st, sizeof(PrState), cudaHostAllocDefault), "cudaHostAlloc(state)");
+  CK(cudaHostAlloc((void**)&g->h_abort, sizeof(unsigned int), cudaHostAllocMapped), "cudaHostAlloc(abort)");
+  *g->h_abort = 0;
+  CK(cudaHostGetDevicePointer((void**)&g->d_abort, g->h_abort, 0), "cudaHostGetDevicePointer(abort)");
+  CK(cudaEventCreate(&g->ev0), "cudaEventCreate");
+  CK(cudaEventCreate(&g->ev1), "cudaEventCreate");
+  g->solve_ready = true;
+  return NWGPU_OK;
+}
+
+SweepArgs make_sweep_args(nwgpu_graph* g, float damping, float base, int use_cond, cudaGraphConditionalHandle cond) {
+  SweepArgs a = {};
+  a.row_ptr = g->row_ptr;
+  a.col = g->col;
+  a.tile_row = g->tiling.tile_row;
+  a.tile_nnz = g->tiling.tile_nnz;
+  a.num_tiles = g->tiling.num_tiles;
+  a.contrib0 = g->contrib[0];
+  a.contrib1 = g->contrib[1];
+  a.rank = g->rank;
+  a.deg = g->deg;
+  a.cpart = g->cpart;
+  a.epart = g->epart;
+  a.cnt = g->cnt;
+  a.res_part = g->res_part;
+  a.st = g->st;
+  a.err_hist = g->err_hist;
+  a.err_cap = g->err_cap;
+  a.abort_word = g->d_abort;
+  a.cond = cond;
+  a.use_cond = use_cond;
+  a.damping = damping;
+  a.base = base;
+  return a;
+}
+
+int build_loop_graph(nwgpu_graph* g, float damping, float base) {
+  if (g->cg_exec) {
+    cudaGraphExecDestroy(g->cg_exec);
+    g->cg_exec = nullptr;
+  }
+  if (g->cg) {
+    cudaGraphDestroy(g->cg);
+    g->cg = nullptr;
+  }
+  CK(cudaGraphCreate(&g->cg, 0), "cudaGraphCreate");
+  cudaGraphNode_t arm;
+  CK(add_pr_arm_node(g->cg, g->st, &arm), "cudaGraphAddKernelNode(arm)");
+  cudaGraphConditionalHandle cond;
+  CK(cudaGraphConditionalHandleCreate(&cond, g->cg, 1u, cudaGraphCondAssignDefault), "cudaGraphConditionalHandleCreate");
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = cond;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t wnode;
+  CK(cudaGraphAddNode(&wnode, g->cg, &arm, 1, &cp), "cudaGraphAddNode(while)");
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  SweepArgs   a = make_sweep_args(g, damping, base, 1, cond);
+  CK(add_pr_sweep_node(body, a, g->tiling.items_per_thread, g->grid), "cudaGraphAddKernelNode(sweep)");
+  CK(cudaGraphInstantiate(&g->cg_exec, g->cg, 0), "cudaGraphInstantiate");
+  return NWGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int nwgpu_abi_version(void) { return NWGPU_ABI_VERSION; }
+
+int nwgpu_last_error(char* buf, size_t len) {
+  if (buf && len) {
+    size_t m = g_last_error.size() < len - 1 ? g_last_error.size() : len - 1;
+    memcpy(buf, g_last_error.data(), m);
+    buf[m] = '\0';
+  }
+  return (int)g_last_error.size();
+}
+
+int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float* weights, uint64_t n, uint64_t nnz,
+                       uint32_t flags, nwgpu_graph** out) {
+  g_last_error.clear();
+  if (!out) return fail(NWGPU_ERR_INVALID_ARG, "out is NULL");
+  *out = nullptr;
+  if (!row_ptr) return fail(NWGPU_ERR_INVALID_ARG, "row_ptr is NULL");
+  if (nnz && !col) return fail(NWGPU_ERR_INVALID_ARG, "col is NULL with nnz > 0");
+  if (n >= 0xFFFFFFFFull) return fail(NWGPU_ERR_INVALID_ARG, "n = %llu does not fit uint32 vertex ids", (unsigned long long)n);
+  if (nnz > 0xFFFFFFFFull) return fail(NWGPU_ERR_INVALID_ARG, "nnz = %llu does not fit uint32 row pointers", (unsigned long long)nnz);
+  if (flags & NWGPU_GRAPH_TRANSPOSE) return fail(NWGPU_ERR_UNSUPPORTED, "NWGPU_GRAPH_TRANSPOSE is not available in this build");
+  int dev, sms;
+  int rc = check_device(&dev, &sms);
+  if (rc) return rc;
+
+  nwgpu_graph* g = new (std::nothrow) nwgpu_graph();
+  if (!g) return fail(NWGPU_ERR_OUT_OF_MEMORY, "host allocation failed");
+  g->device = dev;
+  g->sms = sms;
+  g->n = n;
+  g->nnz = nnz;
+  auto bail = [&](int code) {
+    delete g;
+    return code;
+  };
+  cudaError_t e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return bail(cuda_fail(e, "cudaStreamCreate"));
+  const cudaMemcpyKind kind = (flags & NWGPU_GRAPH_DEVICE_PTRS) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  if ((e = dalloc(g, &g->row_ptr, n + 1)) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(row_ptr)"));
+  if ((e = dalloc(g, &g->col, nnz)) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(col)"));
+  if ((e = cudaMemcpyAsync(g->row_ptr, row_ptr, (n + 1) * sizeof(uint32_t), kind, g->stream)) != cudaSuccess)
+    return bail(cuda_fail(e, "copy row_ptr"));
+  if (nnz && (e = cudaMemcpyAsync(g->col, col, nnz * sizeof(uint32_t), kind, g->stream)) != cudaSuccess)
+    return bail(cuda_fail(e, "copy col"));
+  if (weights) {
+    if ((e = dalloc(g, &g->weights, nnz)) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(weights)"));
+    if (nnz && (e = cudaMemcpyAsync(g->weights, weights, nnz * sizeof(float), kind, g->stream)) != cudaSuccess)
+      return bail(cuda_fail(e, "copy weights"));
+  }
+  // Validate on the device before any kernel indexes with these arrays.
+  unsigned int* d_err = nullptr;
+  unsigned int  h_err = 0;
+  if ((e = cudaMalloc(&d_err, sizeof(unsigned int))) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(err)"));
+  cudaMemsetAsync(d_err, 0, sizeof(unsigned int), g->stream);
+  e = validate_csr(g->row_ptr, g->col, n, nnz, d_err, g->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h_err, d_err, sizeof(unsigned int), cudaMemcpyDeviceToHost, g->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  cudaFree(d_err);
+  if (e != cudaSuccess) return bail(cuda_fail(e, "validate"));
+  if (h_err) {
+    return bail(fail(NWGPU_ERR_INVALID_GRAPH, "invalid CSR:%s%s%s", (h_err & 1u) ? " row_ptr[0] != 0 or row_ptr[n] != nnz;" : "",
+                     (h_err & 2u) ? " row_ptr decreases;" : "", (h_err & 4u) ? " col index >= n;" : ""));
+  }
+  const int ipt = default_ipt();
+  if ((e = build_tiling(g->row_ptr, n, nnz, ipt, &g->tiling, g->stream)) != cudaSuccess)
+    return bail(cuda_fail(e, "build_tiling"));
+  g->device_bytes += 2ull * (g->tiling.num_tiles + 1) * sizeof(uint32_t);
+  const uint64_t want = (uint64_t)sms * sweep_blocks_per_sm(ipt);
+  g->grid = (int)(want < g->tiling.num_tiles ? want : (g->tiling.num_tiles ? g->tiling.num_tiles : 1));
+  if ((e = cudaStreamSynchronize(g->stream)) != cudaSuccess) return bail(cuda_fail(e, "graph create"));
+  *out = g;
+  return NWGPU_OK;
+}
+
+int nwgpu_graph_destroy(nwgpu_graph* g) {
+  g_last_error.clear();
+  if (!g) return NWGPU_OK;
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  delete g;
+  return NWGPU_OK;
+}
+
+int nwgpu_graph_get_info(const nwgpu_graph* g, nwgpu_graph_info* info) {
+  if (!g || !info) return fail(NWGPU_ERR_INVALID_ARG, "NULL argument");
+  memset(info, 0, sizeof(*info));
+  info->n = g->n;
+  info->nnz = g->nnz;
+  info->num_tiles = g->tiling.num_tiles;
+  info->tile_items = (uint32_t)(kSweepThreads * g->tiling.items_per_thread);
+  info->grid = (uint32_t)g->grid;
+  info->device_bytes = g->device_bytes;
+  info->device = g->device;
+  info->has_weights = g->weights != nullptr;
+  info->has_transpose = g->t_col != nullptr;
+  return NWGPU_OK;
+}
+
+int nwgpu_abort(nwgpu_graph* g) {
+  if (!g) return fail(NWGPU_ERR_INVALID_ARG, "NULL graph");
+  if (g->h_abort) *(volatile unsigned int*)g->h_abort = 1u;
+  return NWGPU_OK;
+}
+
+int nwgpu_pr_run(nwgpu_graph* g, const uint32_t* out_degree, float* ranks, float damping, float threshold,
+                 uint64_t max_iters, const nwgpu_pr_options* options, nwgpu_pr_stats* stats) {
+  g_last_error.clear();
+  if (!g) return fail(NWGPU_ERR_INVALID_ARG, "graph is NULL");
+  if (g->n && (!out_degree || !ranks)) return fail(NWGPU_ERR_INVALID_ARG, "out_degree / ranks is NULL");
+  if (!(damping >= 0.0f && damping <= 1.0f)) return fail(NWGPU_ERR_INVALID_ARG, "damping %g outside [0, 1]", (double)damping);
+  nwgpu_pr_options opt = {};
+  if (options) memcpy(&opt, options, options->size && options->size < sizeof(opt) ? options->size : sizeof(opt));
+  if (opt.mode != NWGPU_MODE_PARITY) return fail(NWGPU_ERR_UNSUPPORTED, "mode %u is not supported", opt.mode);
+  if (opt.launch > NWGPU_LAUNCH_STREAM) return fail(NWGPU_ERR_INVALID_ARG, "launch %u unknown", opt.launch);
+  const uint64_t n = g->n;
+  const double   bytes_iter = 4.0 * (double)g->nnz + 4.0 * (double)(n + 1) + 20.0 * (double)n;
+  if (stats) {
+    double*  eb = stats->errors;
+    uint64_t ec = stats->errors_cap;
+    memset(stats, 0, sizeof(*stats));
+    stats->errors = eb;
+    stats->errors_cap = ec;
+    stats->bytes_per_iter = bytes_iter;
+  }
+  // page_rank.hpp:92-94: N = graph.size(); constants in double, stored as Real.
+  const float init = (float)(1.0 / (double)n);
+  const float base = (float)((1.0 - (double)damping) / (double)n);
+  if (n == 0) {
+    // The reference's sweep reduces over an empty range: error 0.
+    const uint64_t its = (max_iters == 0) ? 0 : ((0.0 < (double)threshold) ? 1 : max_iters);
+    if (stats) {
+      stats->iterations = its;
+      stats->converged = its > 0 && 0.0 < (double)threshold;
+    }
+    return NWGPU_OK;
+  }
+  int rc = ensure_solve_buffers(g);
+  if (rc) return rc;
+  // A caller stream must first see the handle's set-up work.
+  cudaStream_t s = opt.stream ? (cudaStream_t)opt.stream : g->stream;
+  if (s != g->stream) CK(cudaStreamSynchronize(g->stream), "handle stream");
+  const cudaMemcpyKind in_kind = opt.device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  const cudaMemcpyKind out_kind = opt.device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  *(volatile unsigned int*)g->h_abort = 0u;
+
+  CK(cudaMemcpyAsync(g->deg, out_degree, n * sizeof(uint32_t), in_kind, s), "copy out_degree");
+  PrState h = {};
+  h.iter = 0;
+  h.max_iters = max_iters;
+  h.chunk_end = kGraphChunk;
+  h.threshold = (double)threshold;
+  h.last_error = 0.0;
+  h.done = (max_iters == 0) ? 1u : 0u;
+  *g->h_st = h;
+  CK(cudaMemcpyAsync(g->st, g->h_st, sizeof(PrState), cudaMemcpyHostToDevice, s), "copy state");
+  SweepArgs a = make_sweep_args(g, damping, base, 0, cudaGraphConditionalHandle{});
+  CK(launch_pr_init(a, n, init, s), "pr_init");
+
+  CK(cudaEventRecord(g->ev0, s), "cudaEventRecord");
+  if (opt.launch == NWGPU_LAUNCH_GRAPH) {
+    // The loop graph bakes in damping and base; rebuild it when they change.
+    if (!g->cg_exec || g->cg_damping != damping || g->cg_base != base) {
+      rc = build_loop_graph(g, damping, base);
+      if (rc) return rc;
+      g->cg_damping = damping;
+      g->cg_base = base;
+    }
+    // Each launch runs at most kGraphChunk sweeps; the host checks the state
+    // between launches (one launch for max_iters <= kGraphChunk).
+    const uint64_t max_launches = max_iters / kGraphChunk + 2;
+    for (uint64_t launches = 0;; ++launches) {
+      if (launches == max_launches)
+        return fail(NWGPU_ERR_CUDA, "sweep loop did not finish after %llu graph launches",
+                    (unsigned long long)launches);
+      CK(cudaGraphLaunch(g->cg_exec, s), "cudaGraphLaunch");
+      CK(cudaMemcpyAsync(g->h_st, g->st, sizeof(PrState), cudaMemcpyDeviceToHost, s), "copy state");
+      CK(cudaStreamSynchronize(s), "sweep loop");
+      if (g->h_st->done) break;
+    }
+  } else {
+    // One kernel per sweep; sweeps queued after convergence exit immediately.
+    uint64_t launched = 0;
+    for (;;) {
+      const uint64_t batch = (max_iters - launched) < kGraphChunk ? (max_iters - launched) : kGraphChunk;
+      for (uint64_t b = 0; b < batch; ++b) CK(launch_pr_sweep(a, g->tiling.items_per_thread, g->grid, s), "pr_sweep");
+      launched += batch;
+      CK(cudaMemcpyAsync(g->h_st, g->st, sizeof(PrState), cudaMemcpyDeviceToHost, s), "copy state");
+      CK(cudaStreamSynchronize(s), "sweep loop");
+      if (g->h_st->done || launched >= max_iters) break;
+    }
+  }
+  CK(cudaEventRecord(g->ev1, s), "cudaEventRecord");
+  CK(cudaMemcpyAsync(ranks, g->rank, n * sizeof(float), out_kind, s), "copy ranks");
+  CK(cudaStreamSynchronize(s), "copy ranks");
+  const PrState fin = *g->h_st;
+  if (stats) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+    stats->iterations = fin.iter;
+    stats->final_error = fin.last_error;
+    stats->converged = (int32_t)fin.converged;
+    stats->device_ms = ms;
+    stats->ms_per_iter = fin.iter ? ms / (double)fin.iter : 0.0;
+    stats->gteps = ms > 0 ? (double)g->nnz * (double)fin.iter / (ms * 1e6) : 0.0;
+    if (stats->errors && stats->errors_cap) {
+      uint64_t m = fin.iter < stats->errors_cap ? fin.iter : stats->errors_cap;
+      if (m > g->err_cap) m = g->err_cap;
+      if (m) {
+        CK(cudaMemcpyAsync(stats->errors, g->err_hist, m * sizeof(double), cudaMemcpyDeviceToHost, s), "copy errors");
+        CK(cudaStreamSynchronize(s), "copy errors");
+      }
+    }
+  }
+  if (fin.aborted) return fail(NWGPU_ERR_ABORTED, "solve aborted after %llu sweeps", (unsigned long long)fin.iter);
+  return NWGPU_OK;
+}
+
+}  // extern "C"

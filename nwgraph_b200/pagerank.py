@@ -1,0 +1,194 @@
+"""Python mirror of ``nw::graph::page_rank`` on the B200 engine.
+
+The reference call (include/nwgraph/algorithms/page_rank.hpp:89-91)::
+
+    page_rank(graph, degrees, page_rank, damping_factor, threshold, max_iters, num_threads)
+
+keeps its parameter list here: ``graph`` is a compressed adjacency<1>
+(``row_ptr``/``col`` arrays, or any object exposing NWGraph's public
+``indices_`` / ``to_be_indexed_`` members), ``degrees`` the out-degrees,
+``page_rank`` a pre-sized float32 buffer that is fully overwritten, and
+``num_threads`` is accepted and ignored exactly as in the reference (where it
+is unused; parallelism comes from the device). Semantics are those of
+``page_rank_v10`` (experimental/algorithms/page_rank.hpp:377-432): Jacobi
+sweeps, FP32 scores, FP64 L1 error, stop after the first sweep whose error is
+below ``threshold`` or after ``max_iters`` sweeps. Failures raise
+:class:`NwgpuError` (the C++ layer throws ``std::runtime_error``); there is
+no CPU fallback.
+
+Arrays may be host numpy arrays or CUDA tensors (``torch``), which are
+passed to the engine as device pointers without a host round trip.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+from ._native import NwgpuError
+
+
+def _is_cuda_tensor(x) -> bool:
+    return hasattr(x, "is_cuda") and bool(getattr(x, "is_cuda"))
+
+
+def _ptr(x, dtype):
+    """(address, on_device, keepalive) for a numpy array or a torch tensor."""
+    if x is None:
+        return None, False, None
+    if _is_cuda_tensor(x):
+        import torch
+        want = {np.uint32: (torch.int32, torch.uint32), np.float32: (torch.float32,), np.float64: (torch.float64,)}
+        if x.dtype not in want[dtype]:
+            raise TypeError(f"tensor dtype {x.dtype} does not match {np.dtype(dtype).name}")
+        if not x.is_contiguous():
+            raise ValueError("device tensors must be contiguous")
+        return x.data_ptr(), True, x
+    if hasattr(x, "is_cuda"):  # CPU torch tensor
+        x = x.numpy()
+    a = np.ascontiguousarray(x, dtype=dtype)
+    return a.ctypes.data, False, a
+
+
+def _csr_arrays(graph):
+    """row_ptr, col of an adjacency<1>-like object."""
+    if hasattr(graph, "indices_") and hasattr(graph, "to_be_indexed_"):
+        tbi = graph.to_be_indexed_
+        return graph.indices_, (tbi[0] if isinstance(tbi, (tuple, list)) else tbi)
+    return graph.row_ptr, graph.col
+
+
+@dataclass
+class PageRankStats:
+    iterations: int
+    final_error: float
+    converged: bool
+    device_ms: float
+    ms_per_iter: float
+    bytes_per_iter: float
+    gteps: float
+    errors: np.ndarray | None = None
+
+
+class Graph:
+    """A CSR resident in HBM (one ``nwgpu_graph`` handle).
+
+    Upload once, solve many times: the reference re-reads ``graph.indices_`` /
+    ``to_be_indexed_`` on every call (page_rank.hpp:129); here the arrays are
+    copied, validated and tiled on the device at construction.
+    """
+
+    def __init__(self, row_ptr, col, weights=None, n=None, nnz=None):
+        rp, rp_dev, self._k0 = _ptr(row_ptr, np.uint32)
+        cl, cl_dev, self._k1 = _ptr(col, np.uint32)
+        w, w_dev, self._k2 = _ptr(weights, np.float32)
+        if len({rp_dev, cl_dev} | ({w_dev} if weights is not None else set())) != 1:
+            raise ValueError("row_ptr, col and weights must all be on the host or all on the device")
+        self.n = int(n if n is not None else len(row_ptr) - 1)
+        self.nnz = int(nnz if nnz is not None else len(col))
+        flags = N.GRAPH_DEVICE_PTRS if rp_dev else 0
+        h = C.c_void_p()
+        N.check(N.lib().nwgpu_graph_create(rp, cl, w, self.n, self.nnz, flags, C.byref(h)))
+        self._h = h
+        self._k0 = self._k1 = self._k2 = None
+
+    @classmethod
+    def from_adjacency(cls, graph, weights=None):
+        rp, cl = _csr_arrays(graph)
+        return cls(rp, cl, weights)
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise ValueError("graph was released")
+        return self._h
+
+    def info(self) -> dict:
+        gi = N.GraphInfo()
+        N.check(N.lib().nwgpu_graph_get_info(self.handle, C.byref(gi)))
+        return {f: getattr(gi, f) for f, _ in gi._fields_}
+
+    def release(self):
+        if getattr(self, "_h", None) is not None:
+            N.lib().nwgpu_graph_destroy(self._h)
+            self._h = None
+
+    close = release
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.release()
+
+    def abort(self):
+        N.check(N.lib().nwgpu_abort(self.handle))
+
+    # ------------------------------------------------------------------
+    def page_rank(self, degrees, page_rank, damping_factor=0.85, threshold=1e-4, max_iters=20,
+                  launch: str = "graph", record_errors: bool = False, stream=None) -> PageRankStats:
+        """Solve into ``page_rank`` (fully overwritten). Returns the stats.
+
+        ``stream`` (a ``torch.cuda.Stream`` or raw ``cudaStream_t`` int) runs the
+        solve on the caller's stream instead of the handle's own.
+        """
+        if len(page_rank) != self.n or len(degrees) != self.n:
+            raise ValueError(f"degrees/page_rank must have {self.n} entries")
+        dp, d_dev, keep_d = _ptr(degrees, np.uint32)
+        out_dev = _is_cuda_tensor(page_rank)
+        if d_dev != out_dev:
+            raise ValueError("degrees and page_rank must both be host arrays or both device tensors")
+        if out_dev:
+            if page_rank.dtype.__str__() != "torch.float32" or not page_rank.is_contiguous():
+                raise TypeError("page_rank must be a contiguous float32 tensor")
+            rp = page_rank.data_ptr()
+            host_out = None
+        else:
+            if not (isinstance(page_rank, np.ndarray) and page_rank.dtype == np.float32
+                    and page_rank.flags.c_contiguous):
+                raise TypeError("page_rank must be a contiguous float32 numpy array (filled in place)")
+            host_out = page_rank
+            rp = host_out.ctypes.data
+        opt = N.PrOptions(size=C.sizeof(N.PrOptions), mode=N.MODE_PARITY,
+                          launch=N.LAUNCH_STREAM if launch == "stream" else N.LAUNCH_GRAPH,
+                          device_ptrs=1 if out_dev else 0)
+        if stream is not None:
+            opt.stream = int(getattr(stream, "cuda_stream", stream))
+        st = N.PrStats()
+        errs = None
+        if record_errors:
+            cap = int(min(max(int(max_iters), 1), 4096))
+            errs = np.zeros(cap, np.float64)
+            st.errors = errs.ctypes.data_as(C.POINTER(C.c_double))
+            st.errors_cap = cap
+        N.check(N.lib().nwgpu_pr_run(self.handle, dp, rp, C.c_float(damping_factor), C.c_float(threshold),
+                                     int(max_iters), C.byref(opt), C.byref(st)))
+        del keep_d
+        return PageRankStats(int(st.iterations), float(st.final_error), bool(st.converged), float(st.device_ms),
+                             float(st.ms_per_iter), float(st.bytes_per_iter), float(st.gteps),
+                             None if errs is None else errs[: min(int(st.iterations), len(errs))])
+
+
+def page_rank(graph, degrees, page_rank, damping_factor=0.85, threshold=1e-4, max_iters=20, num_threads=None):
+    """Drop-in for ``nw::graph::page_rank`` (page_rank.hpp:89-148).
+
+    ``graph`` may be a resident :class:`Graph` (warm call) or a CSR / adjacency
+    object (uploaded for this call and released after). ``num_threads`` is
+    unused, as in the reference. Returns None, like the reference; use
+    :meth:`Graph.page_rank` for statistics.
+    """
+    del num_threads
+    if isinstance(graph, Graph):
+        graph.page_rank(degrees, page_rank, damping_factor, threshold, max_iters)
+        return None
+    with Graph.from_adjacency(graph) as g:
+        g.page_rank(degrees, page_rank, damping_factor, threshold, max_iters)
+    return None

@@ -1,0 +1,250 @@
+/*
+ * CPU oracle for the PageRank hot path -- TEST INFRASTRUCTURE ONLY.
+ *
+ * Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg load
+ * this library, and only as the checker. The product (nwgraph_b200 +
+ * libnwgpu.so) never calls it and has no CPU fallback.
+ *
+ * Parity pin: orc_pr_jacobi_f32 and orc_pr_gauss_seidel_f32 are checked
+ * bit-for-bit against NWGraph's page_rank_v10 / page_rank (v11, 1 thread)
+ * compiled from the reference headers (oracle/_ref/libnwref.so), and
+ * orc_pr_v1_f64 against the karate golden vector of test/page_rank_test.cpp:72-75
+ * (fixtures in tests/golden/, generated by tests/golden/make_golden.py).
+ * The extensions (personalized teleport, edge weights, implicit adjoint) have
+ * no counterpart in the reference; they are pinned by FP64 central finite
+ * differences and by internal consistency (tests/test_oracle.py).
+ *
+ * CSR convention (adjacency<1> of the reference, adjacency.hpp:86-195):
+ * row i lists the in-neighbours j of i, i.e. entry k of row i is edge j->i;
+ * deg[j] is the out-degree of j (bench/gapbs/common.hpp:110-121).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* Constants exactly as page_rank.hpp:92-94: computed in double, stored as float. */
+static void pr_constants_f32(uint64_t n, float damping, float* init, float* base) {
+  *init = (float)(1.0 / (double)n);
+  *base = (float)((1.0 - (double)damping) / (double)n);
+}
+
+/*
+ * Restates nw::graph::page_rank_v10 (experimental/algorithms/page_rank.hpp:377-432):
+ * Jacobi. Per sweep: contrib[i] = rank[i] / deg[i] (:401-405), then per row in
+ * row order z = sum of contrib over the row in CSR order (:413-415),
+ * rank = base + d*z (:417, contracted to one FMA as GCC does for the
+ * reference's gnu++20 build), error += |new - old| in double (:418); stop
+ * after the sweep when error < threshold (:427). Returns sweeps run.
+ * errors[] (may be NULL) receives each sweep's L1 error.
+ */
+int64_t orc_pr_jacobi_f32(const uint32_t* row_ptr, const uint32_t* col, uint64_t n, const uint32_t* deg, float* rank,
+                          float damping, float threshold, uint64_t max_iters, double* errors) {
+  float init, base;
+  pr_constants_f32(n, damping, &init, &base);
+  float* contrib = (float*)malloc((n ? n : 1) * sizeof(float));
+  if (!contrib) return -1;
+  for (uint64_t i = 0; i < n; ++i) rank[i] = init;
+  uint64_t it = 0;
+  for (; it < max_iters; ++it) {
+    for (uint64_t i = 0; i < n; ++i) contrib[i] = rank[i] / (float)deg[i];
+    double err = 0.0;
+    for (uint64_t i = 0; i < n; ++i) {
+      float z = 0.0f;
+      for (uint32_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k) z += contrib[col[k]];
+      float old = rank[i];
+      rank[i] = fmaf(damping, z, base);
+      err += (double)fabsf(rank[i] - old);
+    }
+    if (errors) errors[it] = err;
+    if (err < (double)threshold) {
+      ++it;
+      break;
+    }
+  }
+  free(contrib);
+  return (int64_t)it;
+}
+
+/*
+ * Restates nw::graph::page_rank v11 (algorithms/page_rank.hpp:89-148) run on
+ * one thread: Gauss-Seidel, contrib initialised once (:114-118) and rewritten
+ * in place right after each row's update (:135), so later rows of the same
+ * sweep read the new value.
+ */
+int64_t orc_pr_gauss_seidel_f32(const uint32_t* row_ptr, const uint32_t* col, uint64_t n, const uint32_t* deg,
+                                float* rank, float damping, float threshold, uint64_t max_iters, double* errors) {
+  float init, base;
+  pr_constants_f32(n, damping, &init, &base);
+  float* contrib = (float*)malloc((n ? n : 1) * sizeof(float));
+  if (!contrib) return -1;
+  for (uint64_t i = 0; i < n; ++i) rank[i] = init;
+  for (uint64_t i = 0; i < n; ++i) contrib[i] = rank[i] / (float)deg[i];
+  uint64_t it = 0;
+  for (; it < max_iters; ++it) {
+    double err = 0.0;
+    for (uint64_t i = 0; i < n; ++i) {
+      float z = 0.0f;
+      for (uint32_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k) z += contrib[col[k]];
+      float old = rank[i];
+      rank[i] = fmaf(damping, z, base);
+      err += (double)fabsf(rank[i] - old);
+      contrib[i] = rank[i] / (float)deg[i];
+    }
+    if (errors) errors[it] = err;
+    if (err < (double)threshold) {
+      ++it;
+      break;
+    }
+  }
+  free(contrib);
+  return (int64_t)it;
+}
+
+/*
+ * Restates page_rank_v1 (experimental/algorithms/page_rank.hpp:82-119) with
+ * Real = double, the form test/page_rank_test.cpp:93 calls: serial Jacobi,
+ * init/base from page_rank.size() (:88-89), contrib = rank/deg (:99-102).
+ */
+int64_t orc_pr_v1_f64(const uint32_t* row_ptr, const uint32_t* col, uint64_t n, const uint32_t* deg, double* rank,
+                      double damping, double threshold, uint64_t max_iters) {
+  const double init = 1.0 / (double)n;
+  const double base = (1.0 - damping) / (double)n;
+  double*      contrib = (double*)malloc((n ? n : 1) * sizeof(double));
+  if (!contrib) return -1;
+  for (uint64_t i = 0; i < n; ++i) rank[i] = init;
+  uint64_t it = 0;
+  for (; it < max_iters; ++it) {
+    double err = 0.0;
+    for (uint64_t i = 0; i < n; ++i) contrib[i] = rank[i] / (double)deg[i];
+    for (uint64_t i = 0; i < n; ++i) {
+      double z = 0.0;
+      for (uint32_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k) z += contrib[col[k]];
+      double old = rank[i];
+      rank[i] = fma(damping, z, base);
+      err += fabs(rank[i] - old);
+    }
+    if (err < threshold) {
+      ++it;
+      break;
+    }
+  }
+  free(contrib);
+  return (int64_t)it;
+}
+
+/*
+ * Out-weight sums s[j] = sum of w over the out-edges of j, gathered from the
+ * in-row CSR (entry k of row i is edge col[k] -> i). With w == NULL this is the
+ * out-degree.
+ */
+void orc_out_weight(const uint32_t* row_ptr, const uint32_t* col, uint64_t n, const float* w, double* s) {
+  for (uint64_t j = 0; j < n; ++j) s[j] = 0.0;
+  uint64_t nnz = row_ptr[n];
+  for (uint64_t k = 0; k < nnz; ++k) s[col[k]] += w ? (double)w[k] : 1.0;
+}
+
+/*
+ * General FP64 Jacobi power iteration with the reference's leak semantics
+ * (no dangling redistribution, page_rank.hpp:94,133):
+ *   r_i <- (1-d) t_i + d * sum_{k in row i} wn_k r_{col[k]}
+ * where wn_k = w_k / s_{col[k]} (weighted, out-normalised) or 1/deg (w == NULL),
+ * and t = teleport (NULL means the uniform 1/n of plain PageRank).
+ * r starts at r0 (NULL: t, or 1/n for plain). Runs until the L1 change of a
+ * sweep is < tol or max_iters sweeps. Returns sweeps run; *final_err = last L1.
+ * This is the FP64 oracle O3 (plain) and O4 (PPR / weighted).
+ */
+int64_t orc_pr_f64(const uint32_t* row_ptr, const uint32_t* col, uint64_t n, const float* w, const double* teleport,
+                   const double* r0, double damping, double tol, uint64_t max_iters, double* r, double* final_err) {
+  double* s = (double*)malloc((n ? n : 1) * sizeof(double));
+  double* c = (double*)malloc((n ? n : 1) * sizeof(double));
+  double* nr = (double*)malloc((n ? n : 1) * sizeof(double));
+  if (!s || !c || !nr) return -1;
+  orc_out_weight(row_ptr, col, n, w, s);
+  for (uint64_t i = 0; i < n; ++i) r[i] = r0 ? r0[i] : (teleport ? teleport[i] : 1.0 / (double)n);
+  uint64_t it = 0;
+  double   err = INFINITY;
+  for (; it < max_iters; ++it) {
+    for (uint64_t j = 0; j < n; ++j) c[j] = r[j] / s[j];
+    err = 0.0;
+    for (uint64_t i = 0; i < n; ++i) {
+      double z = 0.0;
+      for (uint32_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k) z += (w ? (double)w[k] : 1.0) * c[col[k]];
+      double t = teleport ? teleport[i] : 1.0 / (double)n;
+      nr[i] = (1.0 - damping) * t + damping * z;
+      err += fabs(nr[i] - r[i]);
+    }
+    memcpy(r, nr, n * sizeof(double));
+    if (err < tol) {
+      ++it;
+      break;
+    }
+  }
+  if (final_err) *final_err = err;
+  free(s);
+  free(c);
+  free(nr);
+  return (int64_t)it;
+}
+
+/*
+ * Implicit adjoint of the converged fixed point r = (1-d) t + d P r,
+ * P_{i j} = wn(j->i). For L = sum_v cvec_v r_v:
+ *   lambda = cvec + d P^T lambda, i.e. lambda_j = c_j + d sum_{i: j->i} wn(j->i) lambda_i
+ *   dL/dt = (1-d) lambda
+ *   dL/dw(j->i) = d r_j / s_j * (lambda_i - sum_{i'} wn(j->i') lambda_{i'})
+ * (the last term is the derivative through the out-normalisation; w == NULL
+ * means unit weights). The transpose is applied as a scatter over the in-row
+ * CSR. Iterates lambda to L1 change < tol. Writes lambda, dL/dt (n) and
+ * dL/dw (nnz, may be NULL). Returns sweeps run.
+ */
+int64_t orc_pr_vjp_f64(const uint32_t* row_ptr, const uint32_t* col, uint64_t n, const float* w, const double* r,
+                       const double* cvec, double damping, double tol, uint64_t max_iters, double* lambda, double* d_t,
+                       double* d_w) {
+  uint64_t nnz = row_ptr[n];
+  double*  s = (double*)malloc((n ? n : 1) * sizeof(double));
+  double*  nl = (double*)malloc((n ? n : 1) * sizeof(double));
+  double*  q = (double*)malloc((n ? n : 1) * sizeof(double));
+  if (!s || !nl || !q) return -1;
+  orc_out_weight(row_ptr, col, n, w, s);
+  for (uint64_t j = 0; j < n; ++j) lambda[j] = cvec[j];
+  uint64_t it = 0;
+  for (; it < max_iters; ++it) {
+    for (uint64_t j = 0; j < n; ++j) nl[j] = 0.0;
+    for (uint64_t i = 0; i < n; ++i)
+      for (uint32_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k) {
+        uint32_t j = col[k];
+        nl[j] += (w ? (double)w[k] : 1.0) / s[j] * lambda[i];
+      }
+    double err = 0.0;
+    for (uint64_t j = 0; j < n; ++j) {
+      double v = cvec[j] + damping * nl[j];
+      err += fabs(v - lambda[j]);
+      lambda[j] = v;
+    }
+    if (err < tol) {
+      ++it;
+      break;
+    }
+  }
+  for (uint64_t j = 0; j < n; ++j) d_t[j] = (1.0 - damping) * lambda[j];
+  if (d_w) {
+    /* q_j = sum_{i: j->i} wn(j->i) lambda_i */
+    for (uint64_t j = 0; j < n; ++j) q[j] = 0.0;
+    for (uint64_t i = 0; i < n; ++i)
+      for (uint32_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k) {
+        uint32_t j = col[k];
+        q[j] += (w ? (double)w[k] : 1.0) / s[j] * lambda[i];
+      }
+    for (uint64_t i = 0; i < n; ++i)
+      for (uint32_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k) {
+        uint32_t j = col[k];
+        d_w[k] = damping * r[j] / s[j] * (lambda[i] - q[j]);
+      }
+  }
+  (void)nnz;
+  free(s);
+  free(nl);
+  free(q);
+  return (int64_t)it;
+}

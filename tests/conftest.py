@@ -1,0 +1,48 @@
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a B200 (sm_100a) and libnwgpu.so")
+    config.addinivalue_line("markers", "slow: larger inputs (seconds of CPU oracle time)")
+
+
+@pytest.fixture(scope="session")
+def karate():
+    return dict(np.load(os.path.join(GOLDEN, "karate.npz")))
+
+
+@pytest.fixture(scope="session")
+def small_graphs():
+    z = np.load(os.path.join(GOLDEN, "small_graphs.npz"))
+    out = {}
+    for key in z.files:
+        name, field = key.split("/", 1)
+        out.setdefault(name, {})[field] = z[key]
+    return out
+
+
+def has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.fixture(scope="session")
+def gpu():
+    """GPU tests fail (never skip) without a device: `-m gpu` runs on a B200."""
+    if not has_gpu():
+        pytest.fail("no CUDA device visible to a `gpu`-marked test")
+    import nwgraph_b200._native as N
+    N.lib()
+    return True

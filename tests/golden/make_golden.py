@@ -1,0 +1,125 @@
+"""Regenerate the golden fixtures in tests/golden/ (run in a container that has
+the reference tree; the GPU host only reads the committed .npz files).
+
+    python tests/golden/make_golden.py [--ref /root/reference]
+
+* ``karate.npz`` -- the karate edge list and the 34 expected values of
+  test/page_rank_test.cpp:41-75 (parsed from the test source as text), the
+  adjacency<1> CSR the reference's fill builds from it
+  (include/nwgraph/build.hpp:209-232), and NWGraph's own outputs on it:
+  page_rank_v1<double> at threshold 1e-7 (what the unit test checks) and
+  FP32 page_rank_v10 / page_rank at 20 sweeps.
+* ``small_graphs.npz`` -- a handful of small graphs (RMAT scale 8 and 10, a
+  grid, a star, a path, a directed graph with sinks and sources, isolated
+  vertices) with NWGraph's FP32 page_rank_v10 (20 sweeps, threshold 0, and
+  threshold 1e-4 with its sweep count and per-sweep errors) and page_rank v11
+  on one thread.
+
+All reference outputs come from oracle/_ref/libnwref.so, built from the
+reference headers by oracle/Makefile.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import re
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import oracle as O  # noqa: E402
+from nwgraph_b200 import graphs as G  # noqa: E402
+
+
+def parse_vector(src: str, name: str):
+    m = re.search(r"std::vector<\w+>\s*(?:const\s+)?%s\s*=\s*\{([^}]*)\}" % name, src)
+    if not m:
+        raise ValueError(f"vector {name} not found")
+    return [float(x) for x in m.group(1).replace("\n", " ").split(",") if x.strip()]
+
+
+def ref_runs(rp, cl, deg):
+    out = {}
+    r10, it10, _, _ = O.ref_page_rank(10, rp, cl, deg, 0.85, 0.0, 20, 1)
+    r11, it11, _, _ = O.ref_page_rank(11, rp, cl, deg, 0.85, 0.0, 20, 1)
+    r10t, it10t, e10t, _ = O.ref_page_rank(10, rp, cl, deg, 0.85, 1e-4, 100, 1)
+    out["v10_20"] = r10
+    out["v11_20_t1"] = r11
+    out["v10_thr"] = r10t
+    out["v10_thr_iters"] = np.array([it10t], np.int64)
+    out["v10_thr_errors"] = e10t
+    return out
+
+
+def directed_with_sinks(n=300, m=1500, seed=3):
+    rng = np.random.default_rng(seed)
+    src = rng.integers(0, n, size=m)
+    dst = rng.integers(0, n, size=m)
+    # vertices >= n - 20 are sinks (no out-edges); < 10 are sources (no in-edges)
+    keep = (src < n - 20) & (dst >= 10) & (src != dst)
+    return G.from_edges(src[keep], dst[keep], n, symmetrize=False)
+
+
+def star(n=1000):
+    s = np.zeros(n - 1, np.uint32)
+    d = np.arange(1, n, dtype=np.uint32)
+    return G.from_edges(s, d, n, symmetrize=True)
+
+
+def path(n=500):
+    s = np.arange(0, n - 1, dtype=np.uint32)
+    return G.from_edges(s, s + 1, n, symmetrize=True)
+
+
+def isolated_mix(n=700, seed=5):
+    rng = np.random.default_rng(seed)
+    s = rng.integers(0, n // 2, size=900)
+    d = rng.integers(0, n // 2, size=900)
+    return G.from_edges(s, d, n, symmetrize=True)  # upper half of the ids is isolated
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default=os.environ.get("NWGRAPH_REF", "/root/reference"))
+    args = ap.parse_args()
+    O.build(with_reference=True)
+
+    src = open(os.path.join(args.ref, "test", "page_rank_test.cpp")).read()
+    i = np.array(parse_vector(src, "i"), np.uint32)
+    j = np.array(parse_vector(src, "j"), np.uint32)
+    answer = np.array(parse_vector(src, "answer"), np.float64)
+    rp, cl = O.ref_fill_adj1(i, j, 34)
+    deg = O.ref_build_degrees(rp, cl)
+    v1 = O.ref_page_rank_v1_f64(rp, cl, deg, 0.85, 1e-7, 100)
+    k = {"edge_i": i, "edge_j": j, "answer": answer, "row_ptr": rp, "col": cl, "deg": deg, "v1_f64": v1}
+    k.update(ref_runs(rp, cl, deg))
+    np.savez_compressed(os.path.join(HERE, "karate.npz"), **k)
+    print("karate: max rel err of reference v1 vs golden", float(np.max(np.abs(v1 - answer) / answer)))
+
+    graphs = {
+        "rmat8": G.rmat(8, 16, 42),
+        "rmat10": G.rmat(10, 16, 42),
+        "grid": G.grid(1024),
+        "star": star(),
+        "path": path(),
+        "directed": directed_with_sinks(),
+        "isolated": isolated_mix(),
+    }
+    out = {}
+    for name, g in graphs.items():
+        deg = O.ref_build_degrees(g.row_ptr, g.col)
+        out[f"{name}/row_ptr"] = g.row_ptr
+        out[f"{name}/col"] = g.col
+        out[f"{name}/deg"] = deg
+        for key, val in ref_runs(g.row_ptr, g.col, deg).items():
+            out[f"{name}/{key}"] = val
+        print(name, "n", g.n, "nnz", g.nnz, "v10 thr iters", int(out[f"{name}/v10_thr_iters"][0]))
+    np.savez_compressed(os.path.join(HERE, "small_graphs.npz"), **out)
+
+
+if __name__ == "__main__":
+    main()
