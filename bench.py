@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-sample-sweeps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--launch", default="graph", choices=["graph", "stream"],
+                    help="sweep loop as a CUDA graph with a device-side while loop, or one launch per sweep")
     return ap.parse_args()
 
 
@@ -236,7 +238,7 @@ def run_ours(args):
     h = Graph(rp_d, cl_d)
     del rp_d, cl_d
     for _ in range(max(args.warmup, 3)):
-        h.page_rank(deg_d, out_d, DAMPING, 0.0, SWEEPS, stream=stream)
+        h.page_rank(deg_d, out_d, DAMPING, 0.0, SWEEPS, stream=stream, launch=args.launch)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -246,7 +248,7 @@ def run_ours(args):
     with ClockSampler(local) as clk:
         e0.record(stream)
         for _ in range(args.steps):
-            st = h.page_rank(deg_d, out_d, DAMPING, 0.0, SWEEPS, stream=stream)
+            st = h.page_rank(deg_d, out_d, DAMPING, 0.0, SWEEPS, stream=stream, launch=args.launch)
             sweep_ms += st.device_ms
             iters += st.iterations
         e1.record(stream)
@@ -261,7 +263,7 @@ def run_ours(args):
     ms_per_step = total_ms / args.steps
     value = world * nnz * SWEEPS / (ms_per_step * 1e-3) / 1e9
     # threshold-1e-4 run (config: "20 fixed iterations plus a threshold-1e-4 run")
-    st_thr = h.page_rank(deg_d, out_d, DAMPING, 1e-4, 1000, stream=stream)
+    st_thr = h.page_rank(deg_d, out_d, DAMPING, 1e-4, 1000, stream=stream, launch=args.launch)
 
     # ---- end to end through the public API with pinned host buffers ---------
     pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
@@ -271,7 +273,7 @@ def run_ours(args):
 
     def e2e_step():
         with Graph(rp_h, cl_h) as hh:
-            hh.page_rank(deg_h, out_h, DAMPING, 0.0, SWEEPS)
+            hh.page_rank(deg_h, out_h, DAMPING, 0.0, SWEEPS, launch=args.launch)
 
     e2e_step()  # warm-up (context, allocator)
     torch.cuda.synchronize()
@@ -313,7 +315,8 @@ def run_ours(args):
         "config": {"workload": f"rmat{args.scale}_ef{int(args.edge_factor)}_pagerank_f32", "n": n, "nnz": nnz,
                    "sweeps_per_step": SWEEPS, "threshold": 0.0, "damping": DAMPING,
                    "l2": "inputs larger than L2 (col 4*nnz bytes), no flush", "parallelism": f"replicas{world}",
-                   "tile_items": info["tile_items"], "grid": info["grid"], "num_tiles": info["num_tiles"]},
+                   "tile_items": info["tile_items"], "grid": info["grid"], "num_tiles": info["num_tiles"],
+                   "launch": args.launch},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": sweep_traffic_per_launch(), "peak_kind": peak_kind,
                      "bytes_per_sweep": B, "sweep_ms": t_sweep_ms},

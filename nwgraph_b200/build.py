@@ -4,8 +4,8 @@
 
 * ``libnwgpu.so``  -- CUDA kernels + the C ABI of include/nwgpu.h (nvcc, sm_100a)
 * ``libnwgen.so``  -- seeded synthetic graph builder, include/nwgraph_gen.h (g++)
-* ``nwgraph_b200/tests_bin/dropin_test`` -- C++20 drop-in test program for the
-  header layer include/nwgraph_gpu/page_rank.hpp (links libnwgpu.so)
+* ``tests/cpp/dropin_test`` -- C++20 drop-in test program for the header layer
+  include/nwgraph_gpu/page_rank.hpp (links libnwgpu.so)
 
 The libraries are written next to this file so they travel with the source
 tree; nothing is installed into site-packages.
@@ -68,9 +68,23 @@ def build_gen(force=False):
     return target
 
 
+def build_dropin_test(force=False):
+    """tests/cpp/dropin_test: the C++20 header layer over libnwgpu.so."""
+    src = os.path.join(ROOT, "tests", "cpp", "dropin_test.cpp")
+    target = os.path.join(ROOT, "tests", "cpp", "dropin_test")
+    lib = os.path.join(HERE, "libnwgpu.so")
+    deps = [src, lib, os.path.join(INCLUDE, "nwgraph_gpu", "page_rank.hpp"), os.path.join(INCLUDE, "nwgpu.h")]
+    if not os.path.exists(src) or (not force and not _stale(target, deps)):
+        return target
+    _run([CXX, "-std=c++20", "-O2", "-pthread", f"-I{INCLUDE}", "-o", target, src, f"-L{HERE}", "-l:libnwgpu.so",
+          "-Wl,-rpath,$ORIGIN/../../nwgraph_b200"])
+    return target
+
+
 def build_all(force=False):
     build_gen(force)
     build_cuda(force)
+    build_dropin_test(force)
 
 
 if __name__ == "__main__":

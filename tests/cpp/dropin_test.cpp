@@ -1,0 +1,76 @@
+// Drop-in test of include/nwgraph_gpu/page_rank.hpp: the same call a user of
+// nw::graph::page_rank makes (include/nwgraph/algorithms/page_rank.hpp:89-91),
+// with the namespace switched to nw::graph::gpu.
+//
+//   dropin_test <dir>  reads <dir>/row_ptr.u32, col.u32, deg.u32, runs
+//   gpu::page_rank(graph, degrees, ranks, 0.85f, 0.0f, 20, 1) twice (the second
+//   call reuses the resident CSR), writes <dir>/ranks.f32, and checks the error
+//   path. Exit status 0 on success.
+//
+// The graph type is a stand-in with NWGraph's public CSR members
+// (indices_, to_be_indexed_ as in include/nwgraph/containers/compressed.hpp:71-73),
+// so this test needs no reference headers on the GPU host.
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "nwgraph_gpu/page_rank.hpp"
+
+struct csr_graph {
+  using vertex_id_type = std::uint32_t;
+  std::vector<std::uint32_t>              indices_;
+  std::tuple<std::vector<std::uint32_t>> to_be_indexed_;
+  std::size_t                             size() const { return indices_.size() - 1; }
+};
+
+template <class T>
+std::vector<T> read_all(const std::string& path) {
+  std::ifstream in(path, std::ios::binary | std::ios::ate);
+  if (!in) throw std::runtime_error("cannot open " + path);
+  std::size_t bytes = (std::size_t)in.tellg();
+  std::vector<T> v(bytes / sizeof(T));
+  in.seekg(0);
+  in.read(reinterpret_cast<char*>(v.data()), (std::streamsize)bytes);
+  return v;
+}
+
+int main(int argc, char** argv) {
+  if (argc != 2) {
+    std::fprintf(stderr, "usage: %s <dir>\n", argv[0]);
+    return 2;
+  }
+  const std::string dir = argv[1];
+  csr_graph g;
+  g.indices_ = read_all<std::uint32_t>(dir + "/row_ptr.u32");
+  std::get<0>(g.to_be_indexed_) = read_all<std::uint32_t>(dir + "/col.u32");
+  std::vector<std::uint32_t> degrees = read_all<std::uint32_t>(dir + "/deg.u32");
+  std::vector<float>         ranks(g.size());
+
+  nw::graph::gpu::page_rank(g, degrees, ranks, 0.85f, 0.0f, 20, 1);
+  std::vector<float> again(g.size());
+  nw::graph::gpu::page_rank(g, degrees, again, 0.85f, 0.0f, 20, 1);  // resident CSR reused
+  if (std::memcmp(ranks.data(), again.data(), ranks.size() * sizeof(float)) != 0) {
+    std::fprintf(stderr, "second call differs\n");
+    return 1;
+  }
+  bool threw = false;
+  try {
+    std::vector<std::uint32_t> short_deg(degrees.begin(), degrees.end() - 1);
+    nw::graph::gpu::page_rank(g, short_deg, ranks, 0.85f, 0.0f, 20, 1);
+  } catch (const nw::graph::gpu::gpu_error& e) {
+    threw = e.status() == NWGPU_ERR_INVALID_ARG;
+  }
+  if (!threw) {
+    std::fprintf(stderr, "size mismatch did not throw\n");
+    return 1;
+  }
+  nw::graph::gpu::release(g);
+  std::ofstream out(dir + "/ranks.f32", std::ios::binary);
+  out.write(reinterpret_cast<const char*>(ranks.data()), (std::streamsize)(ranks.size() * sizeof(float)));
+  std::printf("dropin ok n=%zu\n", g.size());
+  return 0;
+}

@@ -1,0 +1,58 @@
+"""The C++20 drop-in layer (include/nwgraph_gpu/page_rank.hpp) on the GPU.
+
+* tests/cpp/dropin_test: a graph type with NWGraph's public CSR members, the
+  reference's exact call with the namespace switched to nw::graph::gpu;
+* oracle/_ref/dropin_ref: the same call on NWGraph's own adjacency<1> read
+  from MatrixMarket with read_mm, next to the reference's page_rank_v10 in the
+  same process (built where the reference tree exists; shipped as a binary).
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import ROOT
+from nwgraph_b200 import graphs as G
+
+pytestmark = pytest.mark.gpu
+
+DROPIN = os.path.join(ROOT, "tests", "cpp", "dropin_test")
+DROPIN_REF = os.path.join(ROOT, "oracle", "_ref", "dropin_ref")
+
+
+def write_mtx(path, g):
+    rows = np.repeat(np.arange(g.n, dtype=np.int64), np.diff(g.row_ptr))
+    with open(path, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate pattern general\n")
+        f.write(f"{g.n} {g.n} {g.nnz}\n")
+        # adjacency<1> groups by the second index: line "j+1 i+1" puts j in row i
+        np.savetxt(f, np.stack([g.col.astype(np.int64) + 1, rows + 1], axis=1), fmt="%d")
+
+
+def test_cpp_dropin_standin_graph(gpu, tmp_path):
+    assert os.path.exists(DROPIN), "build() must produce tests/cpp/dropin_test"
+    g = G.rmat(13, 16, 21)
+    deg = g.out_degree()
+    g.row_ptr.tofile(tmp_path / "row_ptr.u32")
+    g.col.tofile(tmp_path / "col.u32")
+    deg.tofile(tmp_path / "deg.u32")
+    res = subprocess.run([DROPIN, str(tmp_path)], capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0, res.stdout + res.stderr
+    ranks = np.fromfile(tmp_path / "ranks.f32", np.float32)
+    ref, _, _ = O.jacobi_f32(g.row_ptr, g.col, deg, 0.85, 0.0, 20)
+    d = np.abs(ranks.astype(np.float64) - ref)
+    assert d.max() <= 1e-6 and d.sum() <= 1e-5
+
+
+@pytest.mark.skipif(not os.path.exists(DROPIN_REF), reason="oracle/_ref/dropin_ref not built")
+@pytest.mark.parametrize("scale", [10, 16])
+def test_cpp_dropin_on_reference_adjacency(gpu, tmp_path, scale):
+    """Config 1's path: RMAT written as .mtx, read by read_mm into adjacency<1>."""
+    g = G.rmat(scale, 16, 42)
+    path = tmp_path / f"rmat{scale}.mtx"
+    write_mtx(path, g)
+    res = subprocess.run([DROPIN_REF, str(path), "20"], capture_output=True, text=True, timeout=600)
+    assert res.returncode == 0, res.stdout + res.stderr
+    assert "dropin_ref" in res.stdout
