@@ -58,11 +58,15 @@ typedef struct nwgpu_graph nwgpu_graph;
 /* nwgpu_graph_create flags */
 #define NWGPU_GRAPH_DEVICE_PTRS 0x1u /* row_ptr / col / weights are device pointers (copied device-to-device) */
 #define NWGPU_GRAPH_TRANSPOSE 0x2u   /* also keep the out-row CSR (adjacency<0>) needed by nwgpu_pr_vjp */
+#define NWGPU_GRAPH_NO_RELABEL 0x4u  /* keep the input vertex order on the device (default: hubs first) */
 
 /* Upload a CSR once (replaces the per-call use of graph.indices_ /
  * to_be_indexed_ at page_rank.hpp:129). Validates it on the device
- * (monotone row_ptr, row_ptr[0] == 0, row_ptr[n] == nnz, every col < n) and
- * partitions it into equal-work merge-path tiles. weights may be NULL
+ * (monotone row_ptr, row_ptr[0] == 0, row_ptr[n] == nnz, every col < n),
+ * renumbers vertices by descending out-degree unless NWGPU_GRAPH_NO_RELABEL
+ * (each row keeps its entries in input order, so its sum has the same terms in
+ * the same order; results are returned in input order) and partitions it into
+ * equal-work merge-path tiles. weights may be NULL
  * (unweighted); with weights the graph can also run weighted PageRank and its
  * adjoint. Uses the current CUDA device. */
 int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float* weights, uint64_t n, uint64_t nnz,

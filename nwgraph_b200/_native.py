@@ -23,6 +23,7 @@ ERR_UNSUPPORTED = 7
 
 GRAPH_DEVICE_PTRS = 0x1
 GRAPH_TRANSPOSE = 0x2
+GRAPH_NO_RELABEL = 0x4
 
 MODE_PARITY = 0
 LAUNCH_GRAPH = 0

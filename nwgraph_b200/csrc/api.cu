@@ -1,11 +1,12 @@
 // C ABI of the PageRank engine (declared in include/nwgpu.h).
 //
 // Host side of the drop-in: nwgpu_graph_create uploads and validates the CSR
-// once and tiles it on the device; nwgpu_pr_run replaces the body of
-// nw::graph::page_rank / page_rank_v10 (include/nwgraph/algorithms/page_rank.hpp:92-147,
+// once, relabels it (hubs first) and tiles it on the device; nwgpu_pr_run
+// replaces the body of nw::graph::page_rank / page_rank_v10
+// (include/nwgraph/algorithms/page_rank.hpp:92-147,
 // include/nwgraph/experimental/algorithms/page_rank.hpp:383-431) with one
-// CUDA-graph launch whose while loop runs the fused sweep kernel until the
-// device-side test "error < threshold" or max_iters stops it.
+// CUDA-graph launch whose while loop runs the sweep and finishing kernels
+// until the device-side test "error < threshold" or max_iters stops it.
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -33,20 +34,21 @@ int fail(int code, const char* fmt, ...) {
 }
 
 int cuda_fail(cudaError_t e, const char* what) {
-  if (e == cudaErrorMemoryAllocation) {
-    cudaGetLastError();
-    return fail(NWGPU_ERR_OUT_OF_MEMORY, "%s: %s", what, cudaGetErrorString(e));
-  }
+  cudaGetLastError();
+  if (e == cudaErrorMemoryAllocation) return fail(NWGPU_ERR_OUT_OF_MEMORY, "%s: %s", what, cudaGetErrorString(e));
   return fail(NWGPU_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
-#define CK(call, what)                       \
-  do {                                       \
-    cudaError_t _e = (call);                 \
+#define CK(call, what)                                 \
+  do {                                                 \
+    cudaError_t _e = (call);                           \
     if (_e != cudaSuccess) return cuda_fail(_e, what); \
   } while (0)
 
-int default_ipt() { return 8; }
+constexpr int kDefaultIpt = 8;
+
+std::once_flag g_config_once;
+cudaError_t    g_config_err = cudaSuccess;
 
 }  // namespace
 
@@ -55,43 +57,40 @@ struct nwgpu_graph {
   int          sms = 148;
   cudaStream_t stream = nullptr;
   uint64_t     n = 0, nnz = 0;
-  uint32_t*    row_ptr = nullptr;
-  uint32_t*    col = nullptr;
-  float*       weights = nullptr;
-  uint32_t*    t_row_ptr = nullptr;  // out-row CSR (adjacency<0>) for the adjoint
-  uint32_t*    t_col = nullptr;
-  uint32_t*    t_perm = nullptr;     // t_col entry -> entry of the in-row CSR
+  bool         relabelled = false;
+  Relabelled   g;  // device CSR (relabelled, or the input order with perm/inv null)
   Tiling       tiling{};
-  int          grid = 0;
+  int          grid = 0;         // persistent sweep CTAs
+  int          finish_grid = 1;  // finishing-kernel CTAs
   uint64_t     device_bytes = 0;
 
   // Plain-solve buffers, allocated on first use and kept.
-  bool         solve_ready = false;
-  float*       rank = nullptr;
-  float*       contrib[2] = {nullptr, nullptr};
-  uint32_t*    deg = nullptr;
-  float*       cpart = nullptr;
-  float*       epart = nullptr;
-  uint32_t*    cnt = nullptr;
-  double*      res_part = nullptr;
-  PrState*     st = nullptr;
-  double*      err_hist = nullptr;
-  uint32_t     err_cap = 4096;
-  PrState*     h_st = nullptr;               // pinned mirror of *st
-  unsigned int* h_abort = nullptr;           // mapped pinned abort word
+  bool          solve_ready = false;
+  float*        rank = nullptr;
+  float*        contrib[2] = {nullptr, nullptr};
+  uint32_t*     deg = nullptr;
+  uint32_t*     stage_u32 = nullptr;  // host <-> device staging in input order
+  float*        cpart = nullptr;
+  float*        epart = nullptr;
+  double*       res_part = nullptr;
+  PrState*      st = nullptr;
+  double*       err_hist = nullptr;
+  uint32_t      err_cap = 4096;
+  PrState*      h_st = nullptr;     // pinned mirror of *st
+  unsigned int* h_abort = nullptr;  // mapped pinned abort word
   unsigned int* d_abort = nullptr;
-  cudaEvent_t  ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t   ev0 = nullptr, ev1 = nullptr;
 
-  // CUDA graph of the sweep loop (arm node -> while node { sweep }).
+  // CUDA graph of the sweep loop (arm node -> while node { sweep; finish }).
   cudaGraph_t     cg = nullptr;
   cudaGraphExec_t cg_exec = nullptr;
-  float           cg_damping = 0.f, cg_base = 0.f;  // scalars baked into cg_exec
+  SweepArgs       cg_args{};  // arguments baked into cg_exec
 
   ~nwgpu_graph() {
     if (cg_exec) cudaGraphExecDestroy(cg_exec);
     if (cg) cudaGraphDestroy(cg);
-    void* dev_ptrs[] = {row_ptr, col, weights, t_row_ptr, t_col, t_perm, tiling.tile_row, tiling.tile_nnz, rank,
-                        contrib[0], contrib[1], deg, cpart, epart, cnt, res_part, st, err_hist};
+    void* dev_ptrs[] = {g.row_ptr, g.col, g.w, g.perm, g.inv, tiling.tile_row, tiling.tile_nnz, rank, contrib[0],
+                        contrib[1], deg, stage_u32, cpart, epart, res_part, st, err_hist};
     for (void* p : dev_ptrs)
       if (p) cudaFree(p);
     if (h_st) cudaFreeHost(h_st);
@@ -106,14 +105,17 @@ namespace {
 
 template <class T>
 cudaError_t dalloc(nwgpu_graph* g, T** p, uint64_t count) {
-  const uint64_t bytes = (count ? count : 1) * sizeof(T);
+  const uint64_t bytes = (count + kPad) * sizeof(T);
   cudaError_t    e = cudaMalloc((void**)p, bytes);
-  if (e == cudaSuccess) g->device_bytes += bytes;
+  if (e == cudaSuccess) {
+    g->device_bytes += bytes;
+    e = cudaMemsetAsync(*p, 0, bytes, g->stream);
+  }
   return e;
 }
 
 int check_device(int* dev_out, int* sms_out) {
-  int dev = 0, count = 0;
+  int         dev = 0, count = 0;
   cudaError_t e = cudaGetDeviceCount(&count);
   if (e != cudaSuccess || count == 0) {
     cudaGetLastError();
@@ -124,6 +126,8 @@ int check_device(int* dev_out, int* sms_out) {
   CK(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev), "cudaDeviceGetAttribute");
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
   if (major != 10) return fail(NWGPU_ERR_NO_DEVICE, "device %d is sm_%d0, this build targets sm_100a only", dev, major);
+  std::call_once(g_config_once, [] { g_config_err = configure_sweep_kernels(); });
+  if (g_config_err != cudaSuccess) return cuda_fail(g_config_err, "configure kernels");
   *dev_out = dev;
   *sms_out = sms;
   return NWGPU_OK;
@@ -136,51 +140,52 @@ int ensure_solve_buffers(nwgpu_graph* g) {
   CK(dalloc(g, &g->contrib[0], n), "cudaMalloc(contrib)");
   CK(dalloc(g, &g->contrib[1], n), "cudaMalloc(contrib)");
   CK(dalloc(g, &g->deg, n), "cudaMalloc(deg)");
+  CK(dalloc(g, &g->stage_u32, n), "cudaMalloc(staging)");
   CK(dalloc(g, &g->cpart, T + 1), "cudaMalloc(cpart)");
   CK(dalloc(g, &g->epart, T + 1), "cudaMalloc(epart)");
-  CK(dalloc(g, &g->cnt, T + 1), "cudaMalloc(cnt)");
-  CK(dalloc(g, &g->res_part, (uint64_t)g->grid), "cudaMalloc(res_part)");
+  CK(dalloc(g, &g->res_part, (uint64_t)g->grid + (uint64_t)g->finish_grid), "cudaMalloc(res_part)");
   CK(dalloc(g, &g->st, 1), "cudaMalloc(state)");
   CK(dalloc(g, &g->err_hist, g->err_cap), "cudaMalloc(err_hist)");
-  CK(cudaMemsetAsync(g->cnt, 0, (T + 1) * sizeof(uint32_t), g->stream), "cudaMemset(cnt)");
-  CK(cudaMemsetAsync(g->st, 0, sizeof(PrState), g->stream), "cudaMemset(state)");
   CK(cudaHostAlloc((void**)&g->h_st, sizeof(PrState), cudaHostAllocDefault), "cudaHostAlloc(state)");
   CK(cudaHostAlloc((void**)&g->h_abort, sizeof(unsigned int), cudaHostAllocMapped), "cudaHostAlloc(abort)");
   *g->h_abort = 0;
   CK(cudaHostGetDevicePointer((void**)&g->d_abort, g->h_abort, 0), "cudaHostGetDevicePointer(abort)");
   CK(cudaEventCreate(&g->ev0), "cudaEventCreate");
   CK(cudaEventCreate(&g->ev1), "cudaEventCreate");
+  CK(cudaStreamSynchronize(g->stream), "solve buffers");
   g->solve_ready = true;
   return NWGPU_OK;
 }
 
-SweepArgs make_sweep_args(nwgpu_graph* g, float damping, float base, int use_cond, cudaGraphConditionalHandle cond) {
+SweepArgs make_sweep_args(nwgpu_graph* g, float damping, float base, int teleport, uint32_t seed) {
   SweepArgs a = {};
-  a.row_ptr = g->row_ptr;
-  a.col = g->col;
+  a.row_ptr = g->g.row_ptr;
+  a.col = g->g.col;
   a.tile_row = g->tiling.tile_row;
   a.tile_nnz = g->tiling.tile_nnz;
   a.num_tiles = g->tiling.num_tiles;
+  a.tile_items = (uint32_t)(kSweepThreads * g->tiling.items_per_thread);
   a.contrib0 = g->contrib[0];
   a.contrib1 = g->contrib[1];
   a.rank = g->rank;
   a.deg = g->deg;
   a.cpart = g->cpart;
   a.epart = g->epart;
-  a.cnt = g->cnt;
   a.res_part = g->res_part;
+  a.sweep_grid = (uint32_t)g->grid;
   a.st = g->st;
   a.err_hist = g->err_hist;
   a.err_cap = g->err_cap;
   a.abort_word = g->d_abort;
-  a.cond = cond;
-  a.use_cond = use_cond;
+  a.use_cond = 0;
   a.damping = damping;
   a.base = base;
+  a.teleport = teleport;
+  a.seed = seed;
   return a;
 }
 
-int build_loop_graph(nwgpu_graph* g, float damping, float base) {
+int build_loop_graph(nwgpu_graph* g, const SweepArgs& proto) {
   if (g->cg_exec) {
     cudaGraphExecDestroy(g->cg_exec);
     g->cg_exec = nullptr;
@@ -202,9 +207,51 @@ int build_loop_graph(nwgpu_graph* g, float damping, float base) {
   cudaGraphNode_t wnode;
   CK(cudaGraphAddNode(&wnode, g->cg, &arm, 1, &cp), "cudaGraphAddNode(while)");
   cudaGraph_t body = cp.conditional.phGraph_out[0];
-  SweepArgs   a = make_sweep_args(g, damping, base, 1, cond);
-  CK(add_pr_sweep_node(body, a, g->tiling.items_per_thread, g->grid), "cudaGraphAddKernelNode(sweep)");
+  SweepArgs   a = proto;
+  a.cond = cond;
+  a.use_cond = 1;
+  CK(add_pr_sweep_nodes(body, a, g->tiling.items_per_thread, g->grid, g->finish_grid), "cudaGraphAddKernelNode(sweep)");
   CK(cudaGraphInstantiate(&g->cg_exec, g->cg, 0), "cudaGraphInstantiate");
+  g->cg_args = proto;
+  return NWGPU_OK;
+}
+
+bool same_scalars(const SweepArgs& x, const SweepArgs& y) {
+  return x.damping == y.damping && x.base == y.base && x.teleport == y.teleport && x.seed == y.seed;
+}
+
+// Runs the sweep loop from the state already on the device; fills fin.
+int run_sweeps(nwgpu_graph* g, const SweepArgs& a, uint32_t launch, uint64_t max_iters, cudaStream_t s, PrState* fin) {
+  if (launch == NWGPU_LAUNCH_GRAPH) {
+    if (!g->cg_exec || !same_scalars(g->cg_args, a)) {
+      int rc = build_loop_graph(g, a);
+      if (rc) return rc;
+    }
+    const uint64_t max_launches = max_iters / kGraphChunk + 2;
+    for (uint64_t launches = 0;; ++launches) {
+      if (launches == max_launches)
+        return fail(NWGPU_ERR_CUDA, "sweep loop did not finish after %llu graph launches", (unsigned long long)launches);
+      CK(cudaGraphLaunch(g->cg_exec, s), "cudaGraphLaunch");
+      CK(cudaMemcpyAsync(g->h_st, g->st, sizeof(PrState), cudaMemcpyDeviceToHost, s), "copy state");
+      CK(cudaStreamSynchronize(s), "sweep loop");
+      if (g->h_st->done) break;
+    }
+  } else {
+    uint64_t launched = 0;
+    for (;;) {
+      const uint64_t batch = (max_iters - launched) < kGraphChunk ? (max_iters - launched) : kGraphChunk;
+      for (uint64_t b = 0; b < batch; ++b) {
+        CK(launch_pr_sweep(a, g->tiling.items_per_thread, g->grid, s), "pr_sweep");
+        CK(launch_pr_finish(a, g->finish_grid, s), "pr_finish");
+      }
+      launched += batch;
+      CK(cudaMemcpyAsync(g->h_st, g->st, sizeof(PrState), cudaMemcpyDeviceToHost, s), "copy state");
+      CK(cudaStreamSynchronize(s), "sweep loop");
+      if (g->h_st->done || launched >= max_iters) break;
+    }
+  }
+  *fin = *g->h_st;
+  if (fin->fault) return fail(NWGPU_ERR_CUDA, "a bounded device wait gave up (fault word %u)", fin->fault);
   return NWGPU_OK;
 }
 
@@ -230,8 +277,9 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
   *out = nullptr;
   if (!row_ptr) return fail(NWGPU_ERR_INVALID_ARG, "row_ptr is NULL");
   if (nnz && !col) return fail(NWGPU_ERR_INVALID_ARG, "col is NULL with nnz > 0");
-  if (n >= 0xFFFFFFFFull) return fail(NWGPU_ERR_INVALID_ARG, "n = %llu does not fit uint32 vertex ids", (unsigned long long)n);
-  if (nnz > 0xFFFFFFFFull) return fail(NWGPU_ERR_INVALID_ARG, "nnz = %llu does not fit uint32 row pointers", (unsigned long long)nnz);
+  if (n >= 0xFFFFFFF0ull) return fail(NWGPU_ERR_INVALID_ARG, "n = %llu does not fit uint32 vertex ids", (unsigned long long)n);
+  if (nnz > 0xFFFFFFF0ull)
+    return fail(NWGPU_ERR_INVALID_ARG, "nnz = %llu does not fit uint32 row pointers", (unsigned long long)nnz);
   if (flags & NWGPU_GRAPH_TRANSPOSE) return fail(NWGPU_ERR_UNSUPPORTED, "NWGPU_GRAPH_TRANSPOSE is not available in this build");
   int dev, sms;
   int rc = check_device(&dev, &sms);
@@ -250,37 +298,71 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
   cudaError_t e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) return bail(cuda_fail(e, "cudaStreamCreate"));
   const cudaMemcpyKind kind = (flags & NWGPU_GRAPH_DEVICE_PTRS) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-  if ((e = dalloc(g, &g->row_ptr, n + 1)) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(row_ptr)"));
-  if ((e = dalloc(g, &g->col, nnz)) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(col)"));
-  if ((e = cudaMemcpyAsync(g->row_ptr, row_ptr, (n + 1) * sizeof(uint32_t), kind, g->stream)) != cudaSuccess)
-    return bail(cuda_fail(e, "copy row_ptr"));
-  if (nnz && (e = cudaMemcpyAsync(g->col, col, nnz * sizeof(uint32_t), kind, g->stream)) != cudaSuccess)
-    return bail(cuda_fail(e, "copy col"));
+  // Upload into padded buffers.
+  Relabelled in;
+  if ((e = dalloc(g, &in.row_ptr, n + 1)) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(row_ptr)"));
+  if ((e = dalloc(g, &in.col, nnz)) != cudaSuccess) {
+    cudaFree(in.row_ptr);
+    return bail(cuda_fail(e, "cudaMalloc(col)"));
+  }
+  auto free_in = [&]() {
+    cudaFree(in.row_ptr);
+    cudaFree(in.col);
+    cudaFree(in.w);
+  };
+  if ((e = cudaMemcpyAsync(in.row_ptr, row_ptr, (n + 1) * sizeof(uint32_t), kind, g->stream)) != cudaSuccess ||
+      (nnz && (e = cudaMemcpyAsync(in.col, col, nnz * sizeof(uint32_t), kind, g->stream)) != cudaSuccess)) {
+    free_in();
+    return bail(cuda_fail(e, "upload CSR"));
+  }
   if (weights) {
-    if ((e = dalloc(g, &g->weights, nnz)) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(weights)"));
-    if (nnz && (e = cudaMemcpyAsync(g->weights, weights, nnz * sizeof(float), kind, g->stream)) != cudaSuccess)
-      return bail(cuda_fail(e, "copy weights"));
+    if ((e = dalloc(g, &in.w, nnz)) != cudaSuccess ||
+        (nnz && (e = cudaMemcpyAsync(in.w, weights, nnz * sizeof(float), kind, g->stream)) != cudaSuccess)) {
+      free_in();
+      return bail(cuda_fail(e, "upload weights"));
+    }
   }
   // Validate on the device before any kernel indexes with these arrays.
   unsigned int* d_err = nullptr;
   unsigned int  h_err = 0;
-  if ((e = cudaMalloc(&d_err, sizeof(unsigned int))) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(err)"));
+  if ((e = cudaMalloc(&d_err, sizeof(unsigned int))) != cudaSuccess) {
+    free_in();
+    return bail(cuda_fail(e, "cudaMalloc(err)"));
+  }
   cudaMemsetAsync(d_err, 0, sizeof(unsigned int), g->stream);
-  e = validate_csr(g->row_ptr, g->col, n, nnz, d_err, g->stream);
+  e = validate_csr(in.row_ptr, in.col, n, nnz, d_err, sms, g->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(&h_err, d_err, sizeof(unsigned int), cudaMemcpyDeviceToHost, g->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
   cudaFree(d_err);
-  if (e != cudaSuccess) return bail(cuda_fail(e, "validate"));
+  if (e != cudaSuccess) {
+    free_in();
+    return bail(cuda_fail(e, "validate"));
+  }
   if (h_err) {
-    return bail(fail(NWGPU_ERR_INVALID_GRAPH, "invalid CSR:%s%s%s", (h_err & 1u) ? " row_ptr[0] != 0 or row_ptr[n] != nnz;" : "",
+    free_in();
+    return bail(fail(NWGPU_ERR_INVALID_GRAPH, "invalid CSR:%s%s%s",
+                     (h_err & 1u) ? " row_ptr[0] != 0 or row_ptr[n] != nnz;" : "",
                      (h_err & 2u) ? " row_ptr decreases;" : "", (h_err & 4u) ? " col index >= n;" : ""));
   }
-  const int ipt = default_ipt();
-  if ((e = build_tiling(g->row_ptr, n, nnz, ipt, &g->tiling, g->stream)) != cudaSuccess)
+  if (!(flags & NWGPU_GRAPH_NO_RELABEL) && n > 1) {
+    e = build_relabelled(in.row_ptr, in.col, in.w, n, nnz, sms, &g->g, g->stream);
+    free_in();
+    if (e != cudaSuccess) return bail(cuda_fail(e, "relabel"));
+    g->relabelled = true;
+    g->device_bytes += (2 * (n + kPad) + (n + 1 + kPad)) * sizeof(uint32_t) + (nnz + kPad) * sizeof(uint32_t) +
+                       (weights ? (nnz + kPad) * sizeof(float) : 0);
+  } else {
+    g->g.row_ptr = in.row_ptr;
+    g->g.col = in.col;
+    g->g.w = in.w;
+  }
+  const int ipt = kDefaultIpt;
+  if ((e = build_tiling(g->g.row_ptr, n, nnz, ipt, &g->tiling, g->stream)) != cudaSuccess)
     return bail(cuda_fail(e, "build_tiling"));
-  g->device_bytes += 2ull * (g->tiling.num_tiles + 1) * sizeof(uint32_t);
+  g->device_bytes += 2ull * (g->tiling.num_tiles + 2) * sizeof(uint32_t);
   const uint64_t want = (uint64_t)sms * sweep_blocks_per_sm(ipt);
   g->grid = (int)(want < g->tiling.num_tiles ? want : (g->tiling.num_tiles ? g->tiling.num_tiles : 1));
+  g->finish_grid = finish_grid_for(g->tiling.num_tiles);
   if ((e = cudaStreamSynchronize(g->stream)) != cudaSuccess) return bail(cuda_fail(e, "graph create"));
   *out = g;
   return NWGPU_OK;
@@ -304,8 +386,8 @@ int nwgpu_graph_get_info(const nwgpu_graph* g, nwgpu_graph_info* info) {
   info->grid = (uint32_t)g->grid;
   info->device_bytes = g->device_bytes;
   info->device = g->device;
-  info->has_weights = g->weights != nullptr;
-  info->has_transpose = g->t_col != nullptr;
+  info->has_weights = g->g.w != nullptr;
+  info->has_transpose = 0;
   return NWGPU_OK;
 }
 
@@ -349,63 +431,45 @@ int nwgpu_pr_run(nwgpu_graph* g, const uint32_t* out_degree, float* ranks, float
   }
   int rc = ensure_solve_buffers(g);
   if (rc) return rc;
-  // A caller stream must first see the handle's set-up work.
   cudaStream_t s = opt.stream ? (cudaStream_t)opt.stream : g->stream;
-  if (s != g->stream) CK(cudaStreamSynchronize(g->stream), "handle stream");
   const cudaMemcpyKind in_kind = opt.device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   const cudaMemcpyKind out_kind = opt.device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
   *(volatile unsigned int*)g->h_abort = 0u;
 
-  CK(cudaMemcpyAsync(g->deg, out_degree, n * sizeof(uint32_t), in_kind, s), "copy out_degree");
+  // degrees into internal order
+  if (g->relabelled) {
+    const uint32_t* src = out_degree;
+    if (!opt.device_ptrs) {
+      CK(cudaMemcpyAsync(g->stage_u32, out_degree, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s), "copy out_degree");
+      src = g->stage_u32;
+    }
+    CK(launch_gather_u32(src, g->g.inv, g->deg, n, g->sms, s), "permute degrees");
+  } else {
+    CK(cudaMemcpyAsync(g->deg, out_degree, n * sizeof(uint32_t), in_kind, s), "copy out_degree");
+  }
   PrState h = {};
-  h.iter = 0;
   h.max_iters = max_iters;
   h.chunk_end = kGraphChunk;
   h.threshold = (double)threshold;
-  h.last_error = 0.0;
   h.done = (max_iters == 0) ? 1u : 0u;
   *g->h_st = h;
   CK(cudaMemcpyAsync(g->st, g->h_st, sizeof(PrState), cudaMemcpyHostToDevice, s), "copy state");
-  SweepArgs a = make_sweep_args(g, damping, base, 0, cudaGraphConditionalHandle{});
-  CK(launch_pr_init(a, n, init, s), "pr_init");
+  SweepArgs a = make_sweep_args(g, damping, base, kTeleportUniform, 0u);
+  CK(launch_pr_init(a, n, init, g->sms, s), "pr_init");
 
   CK(cudaEventRecord(g->ev0, s), "cudaEventRecord");
-  if (opt.launch == NWGPU_LAUNCH_GRAPH) {
-    // The loop graph bakes in damping and base; rebuild it when they change.
-    if (!g->cg_exec || g->cg_damping != damping || g->cg_base != base) {
-      rc = build_loop_graph(g, damping, base);
-      if (rc) return rc;
-      g->cg_damping = damping;
-      g->cg_base = base;
-    }
-    // Each launch runs at most kGraphChunk sweeps; the host checks the state
-    // between launches (one launch for max_iters <= kGraphChunk).
-    const uint64_t max_launches = max_iters / kGraphChunk + 2;
-    for (uint64_t launches = 0;; ++launches) {
-      if (launches == max_launches)
-        return fail(NWGPU_ERR_CUDA, "sweep loop did not finish after %llu graph launches",
-                    (unsigned long long)launches);
-      CK(cudaGraphLaunch(g->cg_exec, s), "cudaGraphLaunch");
-      CK(cudaMemcpyAsync(g->h_st, g->st, sizeof(PrState), cudaMemcpyDeviceToHost, s), "copy state");
-      CK(cudaStreamSynchronize(s), "sweep loop");
-      if (g->h_st->done) break;
-    }
-  } else {
-    // One kernel per sweep; sweeps queued after convergence exit immediately.
-    uint64_t launched = 0;
-    for (;;) {
-      const uint64_t batch = (max_iters - launched) < kGraphChunk ? (max_iters - launched) : kGraphChunk;
-      for (uint64_t b = 0; b < batch; ++b) CK(launch_pr_sweep(a, g->tiling.items_per_thread, g->grid, s), "pr_sweep");
-      launched += batch;
-      CK(cudaMemcpyAsync(g->h_st, g->st, sizeof(PrState), cudaMemcpyDeviceToHost, s), "copy state");
-      CK(cudaStreamSynchronize(s), "sweep loop");
-      if (g->h_st->done || launched >= max_iters) break;
-    }
-  }
+  PrState fin{};
+  rc = run_sweeps(g, a, opt.launch, max_iters, s, &fin);
+  if (rc) return rc;
   CK(cudaEventRecord(g->ev1, s), "cudaEventRecord");
-  CK(cudaMemcpyAsync(ranks, g->rank, n * sizeof(float), out_kind, s), "copy ranks");
+  if (g->relabelled) {
+    float* dst = opt.device_ptrs ? ranks : reinterpret_cast<float*>(g->stage_u32);
+    CK(launch_gather_f32(g->rank, g->g.perm, dst, n, g->sms, s), "permute ranks");
+    if (!opt.device_ptrs) CK(cudaMemcpyAsync(ranks, dst, n * sizeof(float), cudaMemcpyDeviceToHost, s), "copy ranks");
+  } else {
+    CK(cudaMemcpyAsync(ranks, g->rank, n * sizeof(float), out_kind, s), "copy ranks");
+  }
   CK(cudaStreamSynchronize(s), "copy ranks");
-  const PrState fin = *g->h_st;
   if (stats) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, g->ev0, g->ev1);

@@ -6,25 +6,48 @@
 
 namespace nwgpu {
 
+// Every device array is allocated with kPad spare elements so that 16-byte
+// aligned bulk copies that round a slice outward stay inside the allocation.
+constexpr uint64_t kPad = 16;
+constexpr int      kSweepThreads = 256;
+constexpr unsigned long long kGraphChunk = 4096;  // sweeps per graph launch, at most
+
 // Device-resident solve state; one per graph handle. Written by the host
-// before a solve and by the last CTA of each sweep.
+// before a solve and by the last CTA of each sweep's finishing kernel.
 struct PrState {
   unsigned long long iter;       // sweeps completed
   unsigned long long max_iters;  // sweep limit of this solve
   unsigned long long chunk_end;  // the graph loop stops after this sweep count (bounds one launch)
   double             threshold;  // stop when the sweep's L1 change < threshold
   double             last_error; // L1 change of the last sweep
-  unsigned int       ticket;     // CTA arrivals in the current sweep
-  unsigned int       done;       // 1 once converged, at max_iters, or aborted
+  unsigned int       ticket;     // CTA arrivals of the finishing kernel in the current sweep
+  unsigned int       done;       // 1 once converged, at max_iters, aborted or failed
   unsigned int       converged;
   unsigned int       aborted;
+  unsigned int       fault;      // nonzero: a bounded device wait gave up (bit pattern = where)
+  unsigned int       pad_;
 };
 
 struct Tiling {
-  int       items_per_thread;  // IPT; a tile holds NT * IPT rows + entries
-  uint32_t  num_tiles;
-  uint32_t* tile_row;  // num_tiles + 1 merge-path row coordinates
-  uint32_t* tile_nnz;  // num_tiles + 1 merge-path entry coordinates
+  int       items_per_thread = 0;  // IPT; a tile holds kSweepThreads * IPT rows + entries
+  uint32_t  num_tiles = 0;
+  uint32_t* tile_row = nullptr;    // num_tiles + 1 merge-path row coordinates
+  uint32_t* tile_nnz = nullptr;    // num_tiles + 1 merge-path entry coordinates
+};
+
+// The relabelled CSR (vertices in descending out-degree order).
+struct Relabelled {
+  uint32_t* row_ptr = nullptr;  // n + 1 (+ kPad)
+  uint32_t* col = nullptr;      // nnz (+ kPad)
+  float*    w = nullptr;        // nnz (+ kPad) or null
+  uint32_t* perm = nullptr;     // input id -> internal id
+  uint32_t* inv = nullptr;      // internal id -> input id
+};
+
+// Teleport term of the update r_i' = base_i + d * z_i.
+enum TeleportMode : int {
+  kTeleportUniform = 0,  // base_i = (1 - d) / n, page_rank.hpp:94
+  kTeleportSeed = 1,     // personalised, one-hot: base_i = (1 - d) if i == seed else 0
 };
 
 struct SweepArgs {
@@ -33,36 +56,47 @@ struct SweepArgs {
   const uint32_t* tile_row;
   const uint32_t* tile_nnz;
   uint32_t        num_tiles;
-  float*          contrib0;  // contribution vectors, ping-pong by sweep parity
+  uint32_t        tile_items;  // D = kSweepThreads * IPT
+  float*          contrib0;    // contribution vectors, ping-pong by sweep parity
   float*          contrib1;
   float*          rank;
   const uint32_t* deg;
-  float*          cpart;     // per tile: partial sum of the row it carries out
-  float*          epart;     // per tile: partial sum of the continued row it completes
-  uint32_t*       cnt;       // per tile: arrivals for the spanning row that starts there
-  double*         res_part;  // per CTA residual partials
+  float*          cpart;       // per tile: partial sum of the row it carries out
+  float*          epart;       // per tile: partial sum of the continued row it completes
+  double*         res_part;    // residual partials: [0, sweep_grid) sweep kernel, then finishing kernel
+  uint32_t        sweep_grid;
   PrState*        st;
-  double*         err_hist;  // per-sweep L1 errors (ring of err_cap)
+  double*         err_hist;    // per-sweep L1 errors (ring of err_cap)
   uint32_t        err_cap;
   const volatile unsigned int* abort_word;  // host-mapped; nonzero -> stop
   cudaGraphConditionalHandle   cond;
   int                          use_cond;
   float                        damping;
-  float                        base;
+  float                        base;       // uniform teleport term (1 - d) / n
+  int                          teleport;   // TeleportMode
+  uint32_t                     seed;       // internal id of the one-hot teleport vertex
 };
 
-constexpr int kSweepThreads = 256;
-constexpr unsigned long long kGraphChunk = 4096;  // sweeps per graph launch, at most
+// graph_build.cu
+cudaError_t validate_csr(const uint32_t* d_row_ptr, const uint32_t* d_col, uint64_t n, uint64_t nnz,
+                         unsigned int* d_err, int sms, cudaStream_t s);
+cudaError_t build_tiling(const uint32_t* d_row_ptr, uint64_t n, uint64_t nnz, int ipt, Tiling* t, cudaStream_t s);
+cudaError_t build_relabelled(const uint32_t* d_row_ptr, const uint32_t* d_col, const float* d_w, uint64_t n,
+                             uint64_t nnz, int sms, Relabelled* out, cudaStream_t s);
 
 // pr_plain.cu
-cudaError_t build_tiling(const uint32_t* d_row_ptr, uint64_t n, uint64_t nnz, int ipt, Tiling* t, cudaStream_t s);
-cudaError_t validate_csr(const uint32_t* d_row_ptr, const uint32_t* d_col, uint64_t n, uint64_t nnz,
-                         unsigned int* d_err, cudaStream_t s);
-cudaError_t launch_pr_init(const SweepArgs& a, uint64_t n, float init, cudaStream_t s);
+cudaError_t launch_gather_u32(const uint32_t* src, const uint32_t* idx, uint32_t* dst, uint64_t n, int sms,
+                              cudaStream_t s);
+cudaError_t launch_gather_f32(const float* src, const uint32_t* idx, float* dst, uint64_t n, int sms, cudaStream_t s);
+cudaError_t launch_pr_init(const SweepArgs& a, uint64_t n, float init, int sms, cudaStream_t s);
 cudaError_t launch_pr_sweep(const SweepArgs& a, int ipt, int grid, cudaStream_t s);
-cudaError_t add_pr_sweep_node(cudaGraph_t body, const SweepArgs& a, int ipt, int grid);
+cudaError_t launch_pr_finish(const SweepArgs& a, int grid, cudaStream_t s);
+cudaError_t add_pr_sweep_nodes(cudaGraph_t body, const SweepArgs& a, int ipt, int sweep_grid, int finish_grid);
 cudaError_t add_pr_arm_node(cudaGraph_t g, PrState* st, cudaGraphNode_t* node);
+cudaError_t configure_sweep_kernels();
+size_t      sweep_smem_bytes(int ipt);
 int         sweep_blocks_per_sm(int ipt);
 bool        ipt_supported(int ipt);
+int         finish_grid_for(uint32_t num_tiles);
 
 }  // namespace nwgpu

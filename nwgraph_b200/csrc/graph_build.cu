@@ -1,0 +1,227 @@
+// Graph set-up on the device: validation, degree-ordered relabelling and
+// merge-path tiling of the uploaded CSR.
+//
+// Relabelling: vertices are renumbered by descending out-degree (how often a
+// vertex's contribution is gathered), stably, so the few hub vertices that
+// most gathers hit share sectors and L1 lines. Row i of the relabelled CSR is
+// row inv[i] of the input with its entries in their original order and each
+// column id mapped through perm, so every row is summed over the same terms in
+// the same order as the input row (page_rank.hpp:129-131). Ranks go back to
+// input order when a solve finishes.
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include "common.cuh"
+#include "engine.h"
+
+namespace nwgpu {
+
+// ---------------------------------------------------------------------------
+// Validation: bit 0 row_ptr[0] != 0 or row_ptr[n] != nnz; bit 1 row_ptr
+// decreases; bit 2 some col >= n. Reads only in-bounds entries whatever the
+// contents, so it is safe on arbitrary input.
+// ---------------------------------------------------------------------------
+__global__ void validate_kernel(const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ col, uint64_t n,
+                                uint64_t nnz, unsigned int* err) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned int   bad = 0;
+  if (tid == 0 && (row_ptr[0] != 0 || (uint64_t)row_ptr[n] != nnz)) bad |= 1u;
+  for (uint64_t i = tid; i < n; i += stride)
+    if (row_ptr[i + 1] < row_ptr[i]) bad |= 2u;
+  for (uint64_t k = tid; k < nnz; k += stride)
+    if ((uint64_t)__ldcs(col + k) >= n) bad |= 4u;
+  bad = __reduce_or_sync(kFullMask, bad);
+  if ((threadIdx.x & 31) == 0 && bad) atomicOr(err, bad);
+}
+
+cudaError_t validate_csr(const uint32_t* d_row_ptr, const uint32_t* d_col, uint64_t n, uint64_t nnz,
+                         unsigned int* d_err, int sms, cudaStream_t s) {
+  validate_kernel<<<sms * 8, 256, 0, s>>>(d_row_ptr, d_col, n, nnz, d_err);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Merge-path tiling
+// ---------------------------------------------------------------------------
+// Row i such that the first d merge items are rows [0, i) and entries [0, d - i).
+__device__ __forceinline__ uint32_t merge_path_row(const uint32_t* row_ptr, uint64_t n, uint64_t nnz, uint64_t d) {
+  uint64_t lo = d > nnz ? d - nnz : 0;
+  uint64_t hi = d < n ? d : n;
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if ((uint64_t)row_ptr[mid + 1] + mid + 1 <= d)  // row mid's end item lies before d
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return (uint32_t)lo;
+}
+
+__global__ void tiling_kernel(const uint32_t* __restrict__ row_ptr, uint64_t n, uint64_t nnz, uint32_t D,
+                              uint32_t num_tiles, uint32_t* __restrict__ tile_row, uint32_t* __restrict__ tile_nnz) {
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t > num_tiles) return;
+  uint64_t d = t * D;
+  if (d > n + nnz) d = n + nnz;
+  const uint32_t i = merge_path_row(row_ptr, n, nnz, d);
+  tile_row[t] = i;
+  tile_nnz[t] = (uint32_t)(d - i);
+}
+
+cudaError_t build_tiling(const uint32_t* d_row_ptr, uint64_t n, uint64_t nnz, int ipt, Tiling* t, cudaStream_t s) {
+  const uint64_t D = (uint64_t)kSweepThreads * ipt;
+  const uint64_t tiles = (n + nnz + D - 1) / D;
+  if (tiles >= 0xFFFFFFF0ull) return cudaErrorInvalidValue;
+  t->items_per_thread = ipt;
+  t->num_tiles = (uint32_t)tiles;
+  cudaError_t e = cudaMalloc(&t->tile_row, (tiles + 2) * sizeof(uint32_t));
+  if (e != cudaSuccess) return e;
+  e = cudaMalloc(&t->tile_nnz, (tiles + 2) * sizeof(uint32_t));
+  if (e != cudaSuccess) return e;
+  const unsigned blocks = (unsigned)((tiles + 1 + 255) / 256);
+  tiling_kernel<<<blocks, 256, 0, s>>>(d_row_ptr, n, nnz, (uint32_t)D, (uint32_t)tiles, t->tile_row, t->tile_nnz);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Relabelling
+// ---------------------------------------------------------------------------
+__global__ void count_gathers_kernel(const uint32_t* __restrict__ col, uint64_t nnz, uint32_t* __restrict__ cnt) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += stride) atomicAdd(cnt + __ldcs(col + k), 1u);
+}
+
+__global__ void iota_kernel(uint32_t* __restrict__ v, uint64_t n) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) v[i] = (uint32_t)i;
+}
+
+// perm[inv[i]] = i; new row lengths.
+__global__ void invert_kernel(const uint32_t* __restrict__ inv, const uint32_t* __restrict__ row_ptr, uint64_t n,
+                              uint32_t* __restrict__ perm, uint32_t* __restrict__ new_len) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint32_t o = inv[i];
+    perm[o] = (uint32_t)i;
+    new_len[i] = row_ptr[o + 1] - row_ptr[o];
+  }
+}
+
+// Fill the relabelled CSR one merge-path tile of the NEW row_ptr at a time:
+// for new entry p in row i (new id), the source entry is
+// old_row_ptr[inv[i]] + (p - new_row_ptr[i]).
+template <int NT>
+__global__ void __launch_bounds__(NT) permute_entries_kernel(const uint32_t* __restrict__ new_row_ptr,
+                                                              const uint32_t* __restrict__ tile_row,
+                                                              const uint32_t* __restrict__ tile_nnz, uint32_t num_tiles,
+                                                              const uint32_t* __restrict__ inv,
+                                                              const uint32_t* __restrict__ perm,
+                                                              const uint32_t* __restrict__ old_row_ptr,
+                                                              const uint32_t* __restrict__ old_col,
+                                                              const float* __restrict__ old_w, uint32_t* __restrict__ col,
+                                                              float* __restrict__ w, uint32_t D) {
+  extern __shared__ uint32_t sm[];
+  uint32_t* s_new = sm;          // new_row_ptr[r0 .. r1+1]
+  uint32_t* s_old = sm + D + 2;  // old start of rows r0 .. r1
+  for (uint32_t t = blockIdx.x; t < num_tiles; t += gridDim.x) {
+    const uint32_t r0 = tile_row[t], r1 = tile_row[t + 1], k0 = tile_nnz[t], k1 = tile_nnz[t + 1];
+    const uint32_t rows = r1 - r0 + 1;  // includes the (possibly partial) row r1
+    for (uint32_t j = threadIdx.x; j <= rows; j += NT) s_new[j] = new_row_ptr[r0 + j];
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < rows; j += NT) {
+      const uint32_t r = r0 + j;
+      s_old[j] = (s_new[j] < s_new[j + 1]) ? old_row_ptr[inv[r]] : 0u;  // rows without entries here are never read
+    }
+    __syncthreads();
+    for (uint32_t p = k0 + threadIdx.x; p < k1; p += NT) {
+      // row of entry p among rows r0..r1: last j with s_new[j] <= p
+      uint32_t lo = 0, hi = rows;  // answer in [0, rows)
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (s_new[mid] <= p)
+          lo = mid;
+        else
+          hi = mid;
+      }
+      const uint32_t src = s_old[lo] + (p - s_new[lo]);
+      col[p] = perm[old_col[src]];
+      if (w) w[p] = old_w[src];
+    }
+    __syncthreads();
+  }
+}
+
+// Builds the relabelled copy. On success *out holds freshly allocated
+// row_ptr / col / (weights) / perm / inv arrays padded for 16-byte bulk loads.
+cudaError_t build_relabelled(const uint32_t* d_row_ptr, const uint32_t* d_col, const float* d_w, uint64_t n,
+                             uint64_t nnz, int sms, Relabelled* out, cudaStream_t s) {
+  cudaError_t e;
+  uint32_t *cnt = nullptr, *cnt_sorted = nullptr, *ids = nullptr, *new_len = nullptr;
+  void*     tmp = nullptr;
+  size_t    tmp_bytes = 0, scan_bytes = 0;
+  Tiling    nt{};
+  auto      cleanup = [&]() {
+    cudaFree(cnt);
+    cudaFree(cnt_sorted);
+    cudaFree(ids);
+    cudaFree(new_len);
+    cudaFree(tmp);
+    cudaFree(nt.tile_row);
+    cudaFree(nt.tile_nnz);
+  };
+#define RK(x)                \
+  do {                       \
+    if ((e = (x)) != cudaSuccess) { \
+      cleanup();             \
+      return e;              \
+    }                        \
+  } while (0)
+  const int grid = sms * 8;
+  RK(cudaMalloc(&cnt, (n + 1) * sizeof(uint32_t)));
+  RK(cudaMalloc(&cnt_sorted, (n + 1) * sizeof(uint32_t)));
+  RK(cudaMalloc(&ids, (n + 1) * sizeof(uint32_t)));
+  RK(cudaMalloc(&new_len, (n + 1) * sizeof(uint32_t)));
+  RK(cudaMalloc(&out->inv, (n + kPad) * sizeof(uint32_t)));
+  RK(cudaMalloc(&out->perm, (n + kPad) * sizeof(uint32_t)));
+  RK(cudaMalloc(&out->row_ptr, (n + 1 + kPad) * sizeof(uint32_t)));
+  RK(cudaMalloc(&out->col, (nnz + kPad) * sizeof(uint32_t)));
+  RK(cudaMemsetAsync(out->row_ptr, 0, (n + 1 + kPad) * sizeof(uint32_t), s));
+  RK(cudaMemsetAsync(out->col, 0, (nnz + kPad) * sizeof(uint32_t), s));
+  if (d_w) {
+    RK(cudaMalloc(&out->w, (nnz + kPad) * sizeof(float)));
+    RK(cudaMemsetAsync(out->w, 0, (nnz + kPad) * sizeof(float), s));
+  }
+  RK(cudaMemsetAsync(cnt, 0, (n + 1) * sizeof(uint32_t), s));
+  count_gathers_kernel<<<grid, 256, 0, s>>>(d_col, nnz, cnt);
+  RK(cudaGetLastError());
+  iota_kernel<<<grid, 256, 0, s>>>(ids, n);
+  RK(cudaGetLastError());
+  // stable descending sort of vertex ids by gather count
+  RK(cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp_bytes, cnt, cnt_sorted, ids, out->inv, (int64_t)n, 0, 32, s));
+  RK(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, new_len, out->row_ptr, (int64_t)(n + 1), s));
+  if (scan_bytes > tmp_bytes) tmp_bytes = scan_bytes;
+  RK(cudaMalloc(&tmp, tmp_bytes ? tmp_bytes : 1));
+  size_t b1 = tmp_bytes;
+  RK(cub::DeviceRadixSort::SortPairsDescending(tmp, b1, cnt, cnt_sorted, ids, out->inv, (int64_t)n, 0, 32, s));
+  invert_kernel<<<grid, 256, 0, s>>>(out->inv, d_row_ptr, n, out->perm, new_len);
+  RK(cudaGetLastError());
+  RK(cudaMemsetAsync(new_len + n, 0, sizeof(uint32_t), s));
+  size_t b2 = tmp_bytes;
+  RK(cub::DeviceScan::ExclusiveSum(tmp, b2, new_len, out->row_ptr, (int64_t)(n + 1), s));
+  // entries: tile the new CSR and copy each tile's entries
+  const int ipt = 8;
+  RK(build_tiling(out->row_ptr, n, nnz, ipt, &nt, s));
+  const uint32_t D = (uint32_t)(kSweepThreads * ipt);
+  const size_t   smem = (size_t)(2 * D + 4) * sizeof(uint32_t);
+  permute_entries_kernel<kSweepThreads><<<sms * 4, kSweepThreads, smem, s>>>(
+      out->row_ptr, nt.tile_row, nt.tile_nnz, nt.num_tiles, out->inv, out->perm, d_row_ptr, d_col, d_w, out->col,
+      out->w, D);
+  RK(cudaGetLastError());
+  RK(cudaStreamSynchronize(s));
+  cleanup();
+#undef RK
+  return cudaSuccess;
+}
+
+}  // namespace nwgpu

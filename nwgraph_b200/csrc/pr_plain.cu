@@ -1,28 +1,29 @@
-// Plain PageRank sweep kernels for sm_100a.
+// PageRank sweep kernels for sm_100a.
 //
 // One sweep = the body of page_rank_v10's iteration
 // (include/nwgraph/experimental/algorithms/page_rank.hpp:400-423):
-//   z_i   = sum_{k in row i} contrib[col[k]]          (pull gather, :413-415)
-//   r_i'  = base + d * z_i                            (:417)
-//   err  += |r_i' - r_i|   (FP64)                     (:418)
+//   z_i  = sum_{k in row i} contrib[col[k]]           (pull gather, :413-415)
+//   r_i' = base_i + d * z_i                           (:417)
+//   err += |r_i' - r_i|   (FP64)                      (:418)
 // fused with the next sweep's contrib_i = r_i' / deg_i (:401-405), written to
-// the other half of a ping-pong pair, so a sweep is one kernel.
+// the other half of a ping-pong pair.
 //
-// Work decomposition: merge-path tiles. The sweep is a merge of the n row-end
+// Work decomposition: merge-path tiles. A sweep is the merge of the n row-end
 // items with the nnz entry items; tile t owns items [t*D, (t+1)*D), D = NT*IPT,
-// so every tile does the same work whatever the degree skew. Per tile:
-//   1. coalesced loads of the tile's col[] slice and row ends, and the random
-//      gathers of contrib, staged in shared memory (IPT independent gathers per
-//      thread in flight);
-//   2. each thread walks IPT items of the merge path over shared memory;
-//      rows that cross threads are combined by a block-wide segmented scan;
-//   3. coalesced epilogue over the tile's complete rows (rank, degree, the
-//      new contribution, the FP64 residual).
-// A row that crosses tiles (power-law hubs) leaves one partial per tile; the
-// last tile to arrive (atomic counter keyed by the row's first tile) sums the
-// partials in tile order and runs that row's epilogue. No CTA ever waits on
-// another, so the kernel cannot deadlock whatever the grid size.
-// All sums have a fixed order: ranks are bit-reproducible run to run.
+// so every tile costs the same whatever the degree skew.
+//
+// pr_sweep_kernel (persistent, one CTA per tile at a time) pipelines tiles:
+//   * TMA bulk copies (cp.async.bulk + mbarrier) bring tile i+2's slices of
+//     col, row_ptr, rank and degree into shared memory,
+//   * the random gathers of contrib for tile i+1 are in flight in registers,
+//   * while tile i is reduced from shared memory: each thread walks IPT merge
+//     items, rows crossing threads are combined by a block-wide segmented scan,
+//     and complete rows run the epilogue (rank, contrib, FP64 |dr|).
+// A row that crosses a tile boundary leaves one FP32 partial per tile
+// (cpart / epart); pr_finish_kernel, launched right after, sums each such
+// row's partials in tile order, runs its epilogue, reduces the residual and
+// tests convergence on the device. All sums have a fixed order, so ranks are
+// bit-reproducible run to run. No CTA waits on another CTA.
 #include <cstdio>
 
 #include "common.cuh"
@@ -31,106 +32,435 @@
 namespace nwgpu {
 
 // ---------------------------------------------------------------------------
-// Graph set-up kernels
+// TMA bulk copy + mbarrier helpers (no multicast anywhere)
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// Merge-path coordinate of diagonal d: the row i such that the first d items
-// are rows [0, i) and entries [0, d - i).
-__device__ __forceinline__ uint32_t merge_path_row(const uint32_t* row_ptr, uint64_t n, uint64_t nnz, uint64_t d) {
-  uint64_t lo = d > nnz ? d - nnz : 0;
-  uint64_t hi = d < n ? d : n;
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar, uint64_t pol) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(pol)
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: gives up after ~2^20 suspended polls (well over a second).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+#pragma unroll 1
+  for (uint32_t it = 0; it < (1u << 20); ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ uint64_t policy_evict_first() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+
+// ---------------------------------------------------------------------------
+// Shared-memory layout of the sweep kernel
+// ---------------------------------------------------------------------------
+struct TileMeta {
+  uint32_t r0, r1, k0, k1;  // merge-path coordinates of the tile
+  uint32_t col_at;          // stage word holding col[k0]
+  uint32_t rp_at;           // stage word holding row_ptr[r0] (row_ptr[r0..r1] follow)
+  uint32_t rk_at;           // stage word holding rank[r0]
+  uint32_t dg_at;           // stage word holding deg[r0]
+};
+
+template <int NT, int IPT>
+struct SweepSmem {
+  static constexpr int D = NT * IPT;
+  static constexpr int NW = NT / 32;
+  // col (<= E+6 words) + row_ptr (<= R+7) + rank (<= R+6) + deg (<= R+6),
+  // each rounded to 16 bytes, with E + R <= D.
+  static constexpr int STG = 3 * D + 32;
+  uint32_t stage[2][STG];
+  float    val[2][D];  // gathered contributions of the tile being reduced / the next one
+  float    z[D];       // row sums of the tile
+  uint32_t wkey[NW];
+  float    wsum[NW];
+  double   red[NW];
+  uint64_t bar[2];
+  TileMeta meta[2];
+};
+
+template <int NT, int IPT>
+constexpr size_t sweep_smem() {
+  return sizeof(SweepSmem<NT, IPT>);
+}
+
+__device__ __forceinline__ float base_of(const SweepArgs& a, uint32_t r) {
+  if (a.teleport == kTeleportSeed) return (r == a.seed) ? a.base : 0.f;
+  return a.base;
+}
+
+// Thread 0: bring tile t's slices into stage `stg` and record where they landed.
+__device__ __forceinline__ void issue_tile(const SweepArgs& a, uint32_t t, uint32_t* stg, TileMeta* m, uint64_t* bar,
+                                           uint64_t pol) {
+  const uint32_t r0 = a.tile_row[t], r1 = a.tile_row[t + 1], k0 = a.tile_nnz[t], k1 = a.tile_nnz[t + 1];
+  const uint32_t ca0 = k0 & ~3u, ca1 = (k1 + 3u) & ~3u;  // col[k0, k1)
+  const uint32_t pa0 = r0 & ~3u, pa1 = (r1 + 4u) & ~3u;  // row_ptr[r0 .. r1]
+  const uint32_t va0 = r0 & ~3u, va1 = (r1 + 3u) & ~3u;  // rank / deg [r0, r1)
+  const uint32_t cw = ca1 - ca0, pw = pa1 - pa0, vw = (r1 > r0) ? va1 - va0 : 0u;
+  m->r0 = r0;
+  m->r1 = r1;
+  m->k0 = k0;
+  m->k1 = k1;
+  m->col_at = k0 - ca0;
+  m->rp_at = cw + (r0 - pa0);
+  m->rk_at = cw + pw + (r0 - va0);
+  m->dg_at = cw + pw + vw + (r0 - va0);
+  mbar_arrive_expect_tx(bar, 4u * (cw + pw + 2u * vw));
+  if (cw) bulk_load(stg, a.col + ca0, 4u * cw, bar, pol);
+  bulk_load(stg + cw, a.row_ptr + pa0, 4u * pw, bar, pol);
+  if (vw) {
+    bulk_load(stg + cw + pw, a.rank + va0, 4u * vw, bar, pol);
+    bulk_load(stg + cw + pw + vw, a.deg + va0, 4u * vw, bar, pol);
+  }
+}
+
+template <int NT, int IPT>
+__device__ __forceinline__ void gather_tile(const uint32_t* stg, const TileMeta& m, const float* __restrict__ cin,
+                                            float (&v)[IPT], uint64_t pol) {
+  const int       E = (int)(m.k1 - m.k0);
+  const uint32_t* c = stg + m.col_at;
+  uint32_t        idx[IPT];
+#pragma unroll
+  for (int u = 0; u < IPT; ++u) {
+    const int j = (int)threadIdx.x + u * NT;
+    idx[u] = (j < E) ? c[j] : 0u;
+  }
+#pragma unroll
+  for (int u = 0; u < IPT; ++u) {
+    const int j = (int)threadIdx.x + u * NT;
+    v[u] = (j < E) ? ld_gather(cin + idx[u], pol) : 0.f;
+  }
+}
+
+// Reduce the tile in stage s; returns this thread's FP64 |dr| sum.
+template <int NT, int IPT>
+__device__ __forceinline__ double reduce_tile(const SweepArgs& a, SweepSmem<NT, IPT>& S, int s, uint32_t t,
+                                              float* __restrict__ cout, uint64_t pol_keep) {
+  const TileMeta  m = S.meta[s];
+  const int       R = (int)(m.r1 - m.r0), E = (int)(m.k1 - m.k0);
+  const uint32_t* rp = S.stage[s] + m.rp_at;  // rp[j] = row_ptr[r0 + j], j = 0..R
+  const float*    val = S.val[s];
+  const int       tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+  // merge-path walk of IPT items over shared memory
+  const int total = R + E;
+  const int d0 = min(tid * IPT, total), d1 = min(d0 + IPT, total);
+  int       lo = max(0, d0 - E), hi = min(d0, R);
   while (lo < hi) {
-    uint64_t mid = (lo + hi) >> 1;
-    // row mid ends (row_ptr[mid+1]) at or before entry (d - mid - 1): it is consumed.
-    if ((uint64_t)row_ptr[mid + 1] + mid + 1 <= d)
+    const int mid = (lo + hi) >> 1;
+    if ((int)(rp[mid + 1] - m.k0) <= d0 - mid - 1)
       lo = mid + 1;
     else
       hi = mid;
   }
-  return (uint32_t)lo;
+  int   i = lo, k = d0 - lo, first = -1;
+  int   end_i = (i < R) ? (int)(rp[i + 1] - m.k0) : 0x7fffffff;
+  float acc = 0.f;
+#pragma unroll
+  for (int q = 0; q < IPT; ++q) {
+    if (d0 + q < d1) {
+      if (k < end_i) {
+        acc += val[k];
+        ++k;
+      } else {
+        S.z[i] = acc;
+        if (first < 0) first = i;
+        acc = 0.f;
+        ++i;
+        end_i = (i < R) ? (int)(rp[i + 1] - m.k0) : 0x7fffffff;
+      }
+    }
+  }
+  // segmented inclusive scan of the carries (key = row the thread ends in)
+  const uint32_t key = (uint32_t)i;
+  float          sv = acc;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t k2 = __shfl_up_sync(kFullMask, key, off);
+    const float    v2 = __shfl_up_sync(kFullMask, sv, off);
+    if (lane >= off && k2 == key) sv = v2 + sv;
+  }
+  if (lane == 31) {
+    S.wkey[warp] = key;
+    S.wsum[warp] = sv;
+  }
+  __syncthreads();
+  float inc = sv;  // inclusive over the whole block
+  {
+    int w0 = warp;
+    while (w0 > 0 && S.wkey[w0 - 1] == key) --w0;
+    if (w0 < warp) {
+      float pre = S.wsum[w0];
+      for (int w = w0 + 1; w < warp; ++w) pre += S.wsum[w];
+      inc = pre + sv;
+    }
+  }
+  uint32_t pkey = __shfl_up_sync(kFullMask, key, 1);
+  float    pinc = __shfl_up_sync(kFullMask, inc, 1);
+  if (lane == 0) {
+    if (warp == 0) {
+      pkey = 0xffffffffu;
+      pinc = 0.f;
+    } else {  // the previous warp's last thread, recomputed from the warp totals
+      pkey = S.wkey[warp - 1];
+      int w0 = warp - 1;
+      while (w0 > 0 && S.wkey[w0 - 1] == pkey) --w0;
+      float p = S.wsum[w0];
+      for (int w = w0 + 1; w <= warp - 1; ++w) p += S.wsum[w];
+      pinc = p;
+    }
+  }
+  if (first >= 0 && pkey == (uint32_t)first) S.z[first] = pinc + S.z[first];
+  __syncthreads();
+
+  // epilogue of the rows that start and end in this tile
+  const bool      is_cont = rp[0] < m.k0;  // row r0 began in an earlier tile
+  const bool      has_co = m.k1 > rp[R];   // row r1 continues into the next tile
+  const float*    rk = reinterpret_cast<const float*>(S.stage[s] + m.rk_at);
+  const uint32_t* dg = S.stage[s] + m.dg_at;
+  double          res = 0.0;
+  for (int j = (is_cont ? 1 : 0) + tid; j < R; j += NT) {
+    const uint32_t r = m.r0 + j;
+    const float    nr = fmaf(a.damping, S.z[j], base_of(a, r));
+    st_stream(a.rank + r, nr);
+    st_keep(cout + r, nr / (float)dg[j], pol_keep);
+    res += (double)fabsf(nr - rk[j]);
+  }
+  if (tid == 0 && is_cont && R >= 1) a.epart[t] = S.z[0];
+  if (tid == NT - 1 && has_co) a.cpart[t] = (key == (uint32_t)R) ? inc : 0.f;
+  return res;
 }
 
-__global__ void tiling_kernel(const uint32_t* __restrict__ row_ptr, uint64_t n, uint64_t nnz, uint32_t D,
-                              uint32_t num_tiles, uint32_t* __restrict__ tile_row, uint32_t* __restrict__ tile_nnz) {
-  uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t > num_tiles) return;
-  uint64_t d = t * D;
-  if (d > n + nnz) d = n + nnz;
-  uint32_t i = merge_path_row(row_ptr, n, nnz, d);
-  tile_row[t] = i;
-  tile_nnz[t] = (uint32_t)(d - i);
-}
+template <int NT, int IPT>
+__global__ void __launch_bounds__(NT) pr_sweep_kernel(const SweepArgs a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  auto&          S = *reinterpret_cast<SweepSmem<NT, IPT>*>(smem_raw);
+  const int      tid = threadIdx.x;
+  PrState*       st = a.st;
 
-cudaError_t build_tiling(const uint32_t* d_row_ptr, uint64_t n, uint64_t nnz, int ipt, Tiling* t, cudaStream_t s) {
-  const uint64_t D = (uint64_t)kSweepThreads * ipt;
-  const uint64_t tiles = (n + nnz + D - 1) / D;
-  if (tiles >= 0xFFFFFFFFull) return cudaErrorInvalidValue;
-  t->items_per_thread = ipt;
-  t->num_tiles = (uint32_t)tiles;
-  cudaError_t e = cudaMalloc(&t->tile_row, (tiles + 1) * sizeof(uint32_t));
-  if (e != cudaSuccess) return e;
-  e = cudaMalloc(&t->tile_nnz, (tiles + 1) * sizeof(uint32_t));
-  if (e != cudaSuccess) return e;
-  const int bs = 256;
-  const unsigned blocks = (unsigned)((tiles + 1 + bs - 1) / bs);
-  tiling_kernel<<<blocks, bs, 0, s>>>(d_row_ptr, n, nnz, (uint32_t)D, (uint32_t)tiles, t->tile_row, t->tile_nnz);
-  return cudaGetLastError();
-}
+  // Graph loop fail-safe: block 0 clears the loop condition before anything
+  // else; only the finishing kernel's last CTA sets it again.
+  if (a.use_cond && blockIdx.x == 0 && tid == 0) cudaGraphSetConditional(a.cond, 0u);
+  if (*(volatile unsigned int*)&st->done) return;  // stable for the whole sweep
 
-// Bit 0: row_ptr[0] != 0 or row_ptr[n] != nnz; bit 1: row_ptr decreasing;
-// bit 2: some col >= n.
-__global__ void validate_kernel(const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ col, uint64_t n,
-                                uint64_t nnz, unsigned int* err) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned int bad = 0;
-  if (tid == 0 && (row_ptr[0] != 0 || (uint64_t)row_ptr[n] != nnz)) bad |= 1u;
-  for (uint64_t i = tid; i < n; i += stride)
-    if (row_ptr[i + 1] < row_ptr[i]) bad |= 2u;
-  for (uint64_t k = tid; k < nnz; k += stride)
-    if ((uint64_t)__ldcs(col + k) >= n) bad |= 4u;
-  bad = __reduce_or_sync(kFullMask, bad);
-  if ((threadIdx.x & 31) == 0 && bad) atomicOr(err, bad);
-}
+  const unsigned long long it = *(volatile unsigned long long*)&st->iter;
+  const float* __restrict__ cin = (it & 1ull) ? a.contrib1 : a.contrib0;
+  float* __restrict__ cout = (it & 1ull) ? a.contrib0 : a.contrib1;
+  const uint64_t pol_keep = policy_evict_last();
+  const uint64_t pol_stream = policy_evict_first();
+  const uint32_t G = gridDim.x, T = a.num_tiles;
+  double         res = 0.0;
+  int            ok = 1;
 
-cudaError_t validate_csr(const uint32_t* d_row_ptr, const uint32_t* d_col, uint64_t n, uint64_t nnz,
-                         unsigned int* d_err, cudaStream_t s) {
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  validate_kernel<<<sms * 8, 256, 0, s>>>(d_row_ptr, d_col, n, nnz, d_err);
-  return cudaGetLastError();
-}
+  if (tid == 0) {
+    mbar_init(&S.bar[0], 1);
+    mbar_init(&S.bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  uint32_t t = blockIdx.x;
+  if (t < T) {
+    if (tid == 0) {
+      issue_tile(a, t, S.stage[0], &S.meta[0], &S.bar[0], pol_stream);
+      if (t + G < T) issue_tile(a, t + G, S.stage[1], &S.meta[1], &S.bar[1], pol_stream);
+    }
+    float v[IPT];
+    ok = mbar_wait(&S.bar[0], 0u);
+    if (ok) {
+      gather_tile<NT, IPT>(S.stage[0], S.meta[0], cin, v, pol_keep);
+#pragma unroll
+      for (int u = 0; u < IPT; ++u) S.val[0][tid + u * NT] = v[u];
+    }
+    ok = __syncthreads_and(ok);
+    for (int i = 0; ok && t < T; ++i, t += G) {
+      const int      s = i & 1;
+      const uint32_t tn = t + G;
+      if (tn < T) {
+        ok = mbar_wait(&S.bar[s ^ 1], (uint32_t)((i + 1) >> 1) & 1u);
+        if (ok) gather_tile<NT, IPT>(S.stage[s ^ 1], S.meta[s ^ 1], cin, v, pol_keep);
+      }
+      res += reduce_tile<NT, IPT>(a, S, s, t, cout, pol_keep);
+      if (tn < T && ok) {
+#pragma unroll
+        for (int u = 0; u < IPT; ++u) S.val[s ^ 1][tid + u * NT] = v[u];
+      }
+      ok = __syncthreads_and(ok);  // stage s and val[s] are free, val[s^1] is ready
+      if (ok && tid == 0 && t + 2 * G < T) issue_tile(a, t + 2 * G, S.stage[s], &S.meta[s], &S.bar[s], pol_stream);
+    }
+  }
 
-// ---------------------------------------------------------------------------
-// Solve kernels
-// ---------------------------------------------------------------------------
-
-// rank = init, contrib = init / deg (page_rank.hpp:100-104 and v10 :401-405
-// of the first sweep).
-__global__ void pr_init_kernel(float* __restrict__ rank, float* __restrict__ contrib, const uint32_t* __restrict__ deg,
-                               uint64_t n, float init) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    rank[i] = init;
-    contrib[i] = init / (float)deg[i];
+  // FP64 residual: fixed-order block reduction, one partial per CTA.
+  res = warp_sum_lane0(res);
+  if ((tid & 31) == 0) S.red[tid >> 5] = res;
+  __syncthreads();
+  if (tid == 0) {
+    double b = 0.0;
+#pragma unroll
+    for (int w = 0; w < SweepSmem<NT, IPT>::NW; ++w) b += S.red[w];
+    a.res_part[blockIdx.x] = b;
+    if (!ok) atomicOr(&st->fault, 1u);
   }
 }
 
-cudaError_t launch_pr_init(const SweepArgs& a, uint64_t n, float init, cudaStream_t s) {
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  uint64_t want = (n + 255) / 256;
-  unsigned blocks = (unsigned)(want < (uint64_t)sms * 16 ? (want ? want : 1) : (uint64_t)sms * 16);
-  pr_init_kernel<<<blocks, 256, 0, s>>>(a.rank, a.contrib0, a.deg, n, init);
+// Epilogue of one row read straight from global memory.
+__device__ __forceinline__ double row_epilogue(const SweepArgs& a, float* cout, uint32_t r, float z, uint64_t pol) {
+  const float nr = fmaf(a.damping, z, base_of(a, r));
+  const float old = a.rank[r];
+  a.rank[r] = nr;
+  st_keep(cout + r, nr / (float)a.deg[r], pol);
+  return (double)fabsf(nr - old);
+}
+
+// Rows that cross tile boundaries, the residual and the convergence test.
+// Thread ta handles the row carried out of tile ta when that row starts there.
+__global__ void __launch_bounds__(256) pr_finish_kernel(const SweepArgs a) {
+  __shared__ double s_red[8];
+  __shared__ int    s_last;
+  PrState*          st = a.st;
+  if (*(volatile unsigned int*)&st->done) return;
+  const unsigned long long it = *(volatile unsigned long long*)&st->iter;
+  float* __restrict__ cout = (it & 1ull) ? a.contrib0 : a.contrib1;
+  const uint64_t pol = policy_evict_last();
+  const uint32_t D = a.tile_items, T = a.num_tiles;
+  const int      tid = threadIdx.x, lane = tid & 31;
+  double         res = 0.0;
+
+  const uint32_t ta = blockIdx.x * blockDim.x + tid;
+  uint32_t       S = 0, tb = 0;
+  bool           mine = false;
+  if (ta + 1 < T) {
+    S = a.tile_row[ta + 1];
+    const uint32_t k1 = a.tile_nnz[ta + 1], rs = a.row_ptr[S];
+    if (k1 > rs && ((uint64_t)S + rs) / D == ta) {
+      mine = true;
+      tb = (uint32_t)(((uint64_t)S + a.row_ptr[S + 1]) / D);
+    }
+  }
+  const bool longspan = mine && (tb - ta > 8u);
+  if (mine && !longspan) {
+    float z = 0.f;
+    for (uint32_t u = ta; u < tb; ++u) z += __ldcg(a.cpart + u);
+    z += __ldcg(a.epart + tb);
+    res += row_epilogue(a, cout, S, z, pol);
+  }
+  unsigned mask = __ballot_sync(kFullMask, longspan);
+  while (mask) {
+    const int src = __ffs(mask) - 1;
+    mask &= mask - 1;
+    const uint32_t sS = __shfl_sync(kFullMask, S, src);
+    const uint32_t sa = __shfl_sync(kFullMask, ta, src);
+    const uint32_t sb = __shfl_sync(kFullMask, tb, src);
+    float          p = 0.f;
+    for (uint32_t u = sa + lane; u < sb; u += 32) p += __ldcg(a.cpart + u);
+    p = warp_sum_lane0(p);
+    if (lane == 0) res += row_epilogue(a, cout, sS, p + __ldcg(a.epart + sb), pol);
+  }
+
+  res = warp_sum_lane0(res);
+  if (lane == 0) s_red[tid >> 5] = res;
+  __syncthreads();
+  if (tid == 0) {
+    double b = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) b += s_red[w];
+    a.res_part[a.sweep_grid + blockIdx.x] = b;
+    __threadfence();
+    const unsigned prev = atomicAdd(&st->ticket, 1u);
+    s_last = (prev == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last || tid >= 32) return;
+
+  // Last CTA: reduce all partials in a fixed order and test convergence.
+  __threadfence();
+  const uint32_t parts = a.sweep_grid + gridDim.x;
+  double         e = 0.0;
+  for (uint32_t u = lane; u < parts; u += 32) e += __ldcg(a.res_part + u);
+  e = warp_sum_lane0(e);
+  if (lane == 0) {
+    const unsigned long long done_iters = it + 1ull;
+    st->iter = done_iters;
+    st->last_error = e;
+    if (a.err_hist) a.err_hist[it % a.err_cap] = e;
+    const bool conv = e < st->threshold;
+    const bool abort = a.abort_word && *a.abort_word;
+    const bool fault = *(volatile unsigned int*)&st->fault != 0u;
+    const bool done = conv || done_iters >= st->max_iters || abort || fault;
+    st->converged = conv ? 1u : 0u;
+    st->aborted = (abort && !conv) ? 1u : 0u;
+    st->done = done ? 1u : 0u;
+    st->ticket = 0u;
+    __threadfence();
+    if (a.use_cond && !done && done_iters < st->chunk_end) cudaGraphSetConditional(a.cond, 1u);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Solve set-up kernels
+// ---------------------------------------------------------------------------
+__global__ void gather_u32_kernel(const uint32_t* __restrict__ src, const uint32_t* __restrict__ idx,
+                                  uint32_t* __restrict__ dst, uint64_t n) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) dst[i] = src[idx[i]];
+}
+__global__ void gather_f32_kernel(const float* __restrict__ src, const uint32_t* __restrict__ idx,
+                                  float* __restrict__ dst, uint64_t n) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) dst[i] = src[idx[i]];
+}
+
+cudaError_t launch_gather_u32(const uint32_t* src, const uint32_t* idx, uint32_t* dst, uint64_t n, int sms,
+                              cudaStream_t s) {
+  if (!n) return cudaSuccess;
+  gather_u32_kernel<<<sms * 8, 256, 0, s>>>(src, idx, dst, n);
+  return cudaGetLastError();
+}
+cudaError_t launch_gather_f32(const float* src, const uint32_t* idx, float* dst, uint64_t n, int sms, cudaStream_t s) {
+  if (!n) return cudaSuccess;
+  gather_f32_kernel<<<sms * 8, 256, 0, s>>>(src, idx, dst, n);
+  return cudaGetLastError();
+}
+
+// rank = r0 (1/n, or the one-hot seed), contrib = rank / deg
+// (page_rank.hpp:100-104 and page_rank_v10's first :401-405).
+__global__ void pr_init_kernel(float* __restrict__ rank, float* __restrict__ contrib, const uint32_t* __restrict__ deg,
+                               uint64_t n, float init, int teleport, uint32_t seed) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const float r = (teleport == kTeleportSeed) ? ((i == seed) ? 1.0f : 0.0f) : init;
+    rank[i] = r;
+    contrib[i] = r / (float)deg[i];
+  }
+}
+
+cudaError_t launch_pr_init(const SweepArgs& a, uint64_t n, float init, int sms, cudaStream_t s) {
+  if (!n) return cudaSuccess;
+  pr_init_kernel<<<sms * 8, 256, 0, s>>>(a.rank, a.contrib0, a.deg, n, init, a.teleport, a.seed);
   return cudaGetLastError();
 }
 
 // Sets the sweep bound of one graph launch (first node of the graph).
-__global__ void pr_arm_kernel(PrState* st) {
-  st->chunk_end = st->iter + kGraphChunk;
-}
+__global__ void pr_arm_kernel(PrState* st) { st->chunk_end = st->iter + kGraphChunk; }
 
 cudaError_t add_pr_arm_node(cudaGraph_t g, PrState* st, cudaGraphNode_t* node) {
   cudaKernelNodeParams kp = {};
@@ -142,220 +472,9 @@ cudaError_t add_pr_arm_node(cudaGraph_t g, PrState* st, cudaGraphNode_t* node) {
   return cudaGraphAddKernelNode(node, g, nullptr, 0, &kp);
 }
 
-// Epilogue of one row: the update of page_rank.hpp:132-135 in Jacobi form.
-__device__ __forceinline__ double row_epilogue(const SweepArgs& a, float* cout, uint32_t r, float z, uint64_t pol) {
-  const float nr = fmaf(a.damping, z, a.base);
-  const float old = ld_stream(a.rank + r);
-  st_stream(a.rank + r, nr);
-  st_keep(cout + r, nr / (float)ld_stream(a.deg + r), pol);
-  return (double)fabsf(nr - old);
-}
-
-// A tile's share of row S, which spans tiles [ta, tb]. The last of the
-// (tb - ta + 1) contributors sums the shares in tile order and finishes S.
-// Called by a whole warp; returns this row's |dr| in lane 0 (0 elsewhere).
-template <int D>
-__device__ __forceinline__ double span_arrive(const SweepArgs& a, float* cout, uint32_t S, float part, float* slot,
-                                              uint64_t pol) {
-  const int lane = threadIdx.x & 31;
-  uint64_t  ta = 0, tb = 0;
-  int       fin = 0;
-  if (lane == 0) {
-    ta = ((uint64_t)S + a.row_ptr[S]) / D;
-    tb = ((uint64_t)S + a.row_ptr[S + 1]) / D;
-    *slot = part;
-    __threadfence();
-    unsigned prev = atomicAdd(a.cnt + ta, 1u);
-    fin = (prev == (unsigned)(tb - ta));
-  }
-  fin = __shfl_sync(kFullMask, fin, 0);
-  if (!fin) return 0.0;
-  ta = __shfl_sync(kFullMask, ta, 0);
-  tb = __shfl_sync(kFullMask, tb, 0);
-  __threadfence();
-  float s = 0.f;
-  for (uint64_t u = ta + lane; u < tb; u += 32) s += __ldcg(a.cpart + u);
-  s = warp_sum_lane0(s);
-  double dr = 0.0;
-  if (lane == 0) {
-    const float z = s + __ldcg(a.epart + tb);
-    dr = row_epilogue(a, cout, S, z, pol);
-    a.cnt[ta] = 0u;  // last arrival: nobody else touches this counter in this sweep
-  }
-  return dr;
-}
-
-template <int NT, int IPT>
-__global__ void __launch_bounds__(NT) pr_sweep_kernel(const SweepArgs a) {
-  constexpr int D = NT * IPT;
-  constexpr int NW = NT / 32;
-  __shared__ uint32_t s_buf[D + 1];  // row ends [0, R] (+ sentinel), then gathered values
-  __shared__ float    s_z[D];        // row sums of the tile
-  __shared__ uint32_t s_key[NT];     // segmented scan of per-thread carries
-  __shared__ float    s_sum[NT];
-  __shared__ uint32_t s_wkey[NW];
-  __shared__ float    s_wsum[NW];
-  __shared__ double   s_red[NW];
-  __shared__ int      s_last;
-
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  PrState*  st = a.st;
-
-  // Fail-safe for the graph loop: block 0 clears the loop condition before it
-  // arrives; only the last CTA of a sweep that must continue sets it again.
-  if (a.use_cond && blockIdx.x == 0 && tid == 0) cudaGraphSetConditional(a.cond, 0u);
-  if (*(volatile unsigned int*)&st->done) return;  // stable for the whole sweep
-
-  const unsigned long long it = *(volatile unsigned long long*)&st->iter;
-  const float* __restrict__ cin = (it & 1ull) ? a.contrib1 : a.contrib0;
-  float* __restrict__ cout = (it & 1ull) ? a.contrib0 : a.contrib1;
-  const uint64_t pol = policy_evict_last();
-  double         res = 0.0;
-
-  for (uint32_t t = blockIdx.x; t < a.num_tiles; t += gridDim.x) {
-    const uint32_t r0 = a.tile_row[t], r1 = a.tile_row[t + 1];
-    const uint32_t k0 = a.tile_nnz[t], k1 = a.tile_nnz[t + 1];
-    const int      R = (int)(r1 - r0), E = (int)(k1 - k0);
-    uint32_t*      s_end = s_buf;
-    float*         s_val = reinterpret_cast<float*>(s_buf + R + 1);
-
-    // 1. loads: row ends (relative to k0) and gathered contributions.
-    for (int j = tid; j < R; j += NT) s_end[j] = ld_stream(a.row_ptr + r0 + j + 1) - k0;
-    if (tid == 0) s_end[R] = 0x7fffffffu;
-    uint32_t c[IPT];
-#pragma unroll
-    for (int u = 0; u < IPT; ++u) {
-      const int j = tid + u * NT;
-      c[u] = (j < E) ? ld_stream(a.col + k0 + j) : 0u;
-    }
-    float v[IPT];
-#pragma unroll
-    for (int u = 0; u < IPT; ++u) {
-      const int j = tid + u * NT;
-      v[u] = (j < E) ? ld_gather(cin + c[u], pol) : 0.f;
-    }
-#pragma unroll
-    for (int u = 0; u < IPT; ++u) {
-      const int j = tid + u * NT;
-      if (j < E) s_val[j] = v[u];
-    }
-    __syncthreads();
-
-    // 2. merge-path walk over shared memory.
-    const int total = R + E;
-    const int d0 = min(tid * IPT, total);
-    const int d1 = min(d0 + IPT, total);
-    int       lo = max(0, d0 - E), hi = min(d0, R);
-    while (lo < hi) {
-      const int mid = (lo + hi) >> 1;
-      if ((int)s_end[mid] <= d0 - mid - 1)
-        lo = mid + 1;
-      else
-        hi = mid;
-    }
-    int   i = lo, k = d0 - lo, first = -1;
-    float acc = 0.f;
-#pragma unroll
-    for (int s = 0; s < IPT; ++s) {
-      if (d0 + s < d1) {
-        if (k < (int)s_end[i]) {
-          acc += s_val[k];
-          ++k;
-        } else {
-          s_z[i] = acc;
-          if (first < 0) first = i;
-          acc = 0.f;
-          ++i;
-        }
-      }
-    }
-    // Segmented inclusive scan of the carries (key = row the thread ends in).
-    uint32_t key = (uint32_t)i;
-    float    sv = acc;
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-      const uint32_t k2 = __shfl_up_sync(kFullMask, key, off);
-      const float    v2 = __shfl_up_sync(kFullMask, sv, off);
-      if (lane >= off && k2 == key) sv = v2 + sv;
-    }
-    if (lane == 31) {
-      s_wkey[warp] = key;
-      s_wsum[warp] = sv;
-    }
-    __syncthreads();
-    {
-      int w0 = warp;
-      while (w0 > 0 && s_wkey[w0 - 1] == key) --w0;
-      if (w0 < warp) {
-        float pre = s_wsum[w0];
-        for (int w = w0 + 1; w < warp; ++w) pre += s_wsum[w];
-        sv = pre + sv;
-      }
-    }
-    s_key[tid] = key;
-    s_sum[tid] = sv;
-    __syncthreads();
-    if (first >= 0 && tid > 0 && s_key[tid - 1] == (uint32_t)first) s_z[first] = s_sum[tid - 1] + s_z[first];
-    __syncthreads();
-
-    // 3. epilogue over the tile's complete rows.
-    const bool is_cont = ld_stream(a.row_ptr + r0) < k0;   // row r0 began in an earlier tile
-    const bool has_co = k1 > ld_stream(a.row_ptr + r1);     // row r1 continues into the next tile
-    for (int j = (is_cont ? 1 : 0) + tid; j < R; j += NT) res += row_epilogue(a, cout, r0 + j, s_z[j], pol);
-    if (warp == 0) {
-      if (is_cont && R >= 1) res += span_arrive<D>(a, cout, r0, s_z[0], a.epart + t, pol);
-      if (has_co) {
-        const float part = (s_key[NT - 1] == (uint32_t)R) ? s_sum[NT - 1] : 0.f;
-        res += span_arrive<D>(a, cout, r1, part, a.cpart + t, pol);
-      }
-    }
-    __syncthreads();  // shared buffers are reused by the next tile
-  }
-
-  // FP64 residual: fixed-order block reduction, one partial per CTA.
-  res = warp_sum_lane0(res);
-  if (lane == 0) s_red[warp] = res;
-  __syncthreads();
-  if (tid == 0) {
-    double b = 0.0;
-#pragma unroll
-    for (int w = 0; w < NW; ++w) b += s_red[w];
-    a.res_part[blockIdx.x] = b;
-    __threadfence();
-    const unsigned prev = atomicAdd(&st->ticket, 1u);
-    s_last = (prev == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!s_last || warp != 0) return;
-
-  // Last CTA: reduce the residual, record it, test convergence on the device.
-  __threadfence();
-  double e = 0.0;
-  for (unsigned u = lane; u < gridDim.x; u += 32) e += __ldcg(a.res_part + u);
-  e = warp_sum_lane0(e);
-  if (lane == 0) {
-    const unsigned long long done_iters = it + 1ull;
-    st->iter = done_iters;
-    st->last_error = e;
-    if (a.err_hist) a.err_hist[it % a.err_cap] = e;
-    const bool conv = e < st->threshold;
-    const bool abort = a.abort_word && *a.abort_word;
-    const bool done = conv || done_iters >= st->max_iters || abort;
-    st->converged = conv ? 1u : 0u;
-    st->aborted = (abort && !conv) ? 1u : 0u;
-    st->done = done ? 1u : 0u;
-    st->ticket = 0u;
-    __threadfence();
-    if (a.use_cond && !done && done_iters < st->chunk_end) cudaGraphSetConditional(a.cond, 1u);
-  }
-}
-
-template <int IPT>
-static cudaError_t launch_ipt(const SweepArgs& a, int grid, cudaStream_t s) {
-  pr_sweep_kernel<kSweepThreads, IPT><<<grid, kSweepThreads, 0, s>>>(a);
-  return cudaGetLastError();
-}
-
+// ---------------------------------------------------------------------------
+// Dispatch over the items-per-thread variants
+// ---------------------------------------------------------------------------
 template <int IPT>
 static void* sweep_fn() {
   return (void*)pr_sweep_kernel<kSweepThreads, IPT>;
@@ -367,42 +486,72 @@ static void* sweep_fn_for(int ipt) {
     case 6: return sweep_fn<6>();
     case 8: return sweep_fn<8>();
     case 12: return sweep_fn<12>();
-    case 16: return sweep_fn<16>();
     default: return nullptr;
+  }
+}
+
+size_t sweep_smem_bytes(int ipt) {
+  switch (ipt) {
+    case 4: return sweep_smem<kSweepThreads, 4>();
+    case 6: return sweep_smem<kSweepThreads, 6>();
+    case 8: return sweep_smem<kSweepThreads, 8>();
+    case 12: return sweep_smem<kSweepThreads, 12>();
+    default: return 0;
   }
 }
 
 bool ipt_supported(int ipt) { return sweep_fn_for(ipt) != nullptr; }
 
+cudaError_t configure_sweep_kernels() {
+  for (int ipt : {4, 6, 8, 12}) {
+    cudaError_t e = cudaFuncSetAttribute(sweep_fn_for(ipt), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sweep_smem_bytes(ipt));
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 int sweep_blocks_per_sm(int ipt) {
   void* fn = sweep_fn_for(ipt);
   int   nb = 0;
-  if (!fn || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kSweepThreads, 0) != cudaSuccess) return 1;
+  if (!fn || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kSweepThreads, sweep_smem_bytes(ipt)) != cudaSuccess)
+    return 1;
   return nb > 0 ? nb : 1;
 }
 
-cudaError_t launch_pr_sweep(const SweepArgs& a, int ipt, int grid, cudaStream_t s) {
-  switch (ipt) {
-    case 4: return launch_ipt<4>(a, grid, s);
-    case 6: return launch_ipt<6>(a, grid, s);
-    case 8: return launch_ipt<8>(a, grid, s);
-    case 12: return launch_ipt<12>(a, grid, s);
-    case 16: return launch_ipt<16>(a, grid, s);
-    default: return cudaErrorInvalidValue;
-  }
-}
+int finish_grid_for(uint32_t num_tiles) { return num_tiles ? (int)((num_tiles + 255u) / 256u) : 1; }
 
-cudaError_t add_pr_sweep_node(cudaGraph_t body, const SweepArgs& a, int ipt, int grid) {
+cudaError_t launch_pr_sweep(const SweepArgs& a, int ipt, int grid, cudaStream_t s) {
   void* fn = sweep_fn_for(ipt);
   if (!fn) return cudaErrorInvalidValue;
-  cudaKernelNodeParams kp = {};
+  void* args[] = {(void*)&a};
+  return cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(kSweepThreads), args, sweep_smem_bytes(ipt), s);
+}
+
+cudaError_t launch_pr_finish(const SweepArgs& a, int grid, cudaStream_t s) {
+  pr_finish_kernel<<<grid, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t add_pr_sweep_nodes(cudaGraph_t body, const SweepArgs& a, int ipt, int sweep_grid, int finish_grid) {
+  void* fn = sweep_fn_for(ipt);
+  if (!fn) return cudaErrorInvalidValue;
   void*                args[] = {(void*)&a};
+  cudaKernelNodeParams kp = {};
   kp.func = fn;
-  kp.gridDim = dim3((unsigned)grid);
+  kp.gridDim = dim3((unsigned)sweep_grid);
   kp.blockDim = dim3(kSweepThreads);
+  kp.sharedMemBytes = (unsigned)sweep_smem_bytes(ipt);
   kp.kernelParams = args;
-  cudaGraphNode_t node;
-  return cudaGraphAddKernelNode(&node, body, nullptr, 0, &kp);
+  cudaGraphNode_t sweep_node, finish_node;
+  cudaError_t     e = cudaGraphAddKernelNode(&sweep_node, body, nullptr, 0, &kp);
+  if (e != cudaSuccess) return e;
+  cudaKernelNodeParams fp = {};
+  fp.func = (void*)pr_finish_kernel;
+  fp.gridDim = dim3((unsigned)finish_grid);
+  fp.blockDim = dim3(256);
+  fp.kernelParams = args;
+  return cudaGraphAddKernelNode(&finish_node, body, &sweep_node, 1, &fp);
 }
 
 }  // namespace nwgpu

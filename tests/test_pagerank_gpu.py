@@ -28,8 +28,8 @@ ERR_ATOL = 1e-6
 ERR_RTOL = 1e-4
 
 
-def solve(rp, cl, deg, thr=0.0, iters=20, launch="graph", damping=0.85):
-    with Graph(rp, cl) as g:
+def solve(rp, cl, deg, thr=0.0, iters=20, launch="graph", damping=0.85, relabel=True):
+    with Graph(rp, cl, relabel=relabel) as g:
         out = np.empty(len(rp) - 1, np.float32)
         st = g.page_rank(deg, out, damping, thr, iters, launch=launch, record_errors=True)
     return out, st
@@ -39,6 +39,25 @@ def assert_close(a, b, max_abs=MAX_ABS, l1=L1):
     d = np.abs(a.astype(np.float64) - b.astype(np.float64))
     assert d.max() <= max_abs, f"max-abs {d.max():.3e}"
     assert d.sum() <= l1, f"L1 {d.sum():.3e}"
+
+
+def assert_parity_or_more_accurate(gpu, ref, rp, cl, iters, damping=0.85):
+    """For hub graphs where the reference's serial FP32 row sums are themselves
+    off by more than the tolerance: the engine must be within tolerance of the
+    reference or at least as close as the reference to exact arithmetic (FP64
+    Jacobi with the same sweep count)."""
+    exact, _, _ = O.pr_f64(rp, cl, damping=damping, tol=0.0, max_iters=iters)
+    e_ref = np.abs(ref.astype(np.float64) - exact)
+    e_gpu = np.abs(gpu.astype(np.float64) - exact)
+    d = np.abs(gpu.astype(np.float64) - ref.astype(np.float64))
+    if d.max() <= MAX_ABS and d.sum() <= L1:
+        return
+    assert e_ref.max() > MAX_ABS, "the reference is accurate here, so the engine must match it"
+    assert e_gpu.max() <= e_ref.max() * 1.01 + 1e-9, (e_gpu.max(), e_ref.max())
+    assert e_gpu.sum() <= e_ref.sum() * 1.01 + 1e-8, (e_gpu.sum(), e_ref.sum())
+
+
+HUB_GRAPHS = {"star"}
 
 
 def top_k_consistent(gpu, ref, k=100, tol=MAX_ABS):
@@ -63,14 +82,23 @@ def test_karate_golden(gpu, karate):
 @pytest.mark.parametrize("launch", ["graph", "stream"])
 def test_small_fixtures(gpu, small_graphs, name, launch):
     g = small_graphs[name]
+    close = (lambda a, b, k: assert_parity_or_more_accurate(a, b, g["row_ptr"], g["col"], k)) if name in HUB_GRAPHS \
+        else (lambda a, b, k: assert_close(a, b))
     r, st = solve(g["row_ptr"], g["col"], g["deg"], iters=20, launch=launch)
     assert st.iterations == 20
-    assert_close(r, g["v10_20"])
+    close(r, g["v10_20"], 20)
     top_k_consistent(r, g["v10_20"])
     r, st = solve(g["row_ptr"], g["col"], g["deg"], thr=1e-4, iters=100, launch=launch)
     assert st.iterations == int(g["v10_thr_iters"][0])
     assert np.allclose(st.errors, g["v10_thr_errors"], rtol=ERR_RTOL, atol=ERR_ATOL)
-    assert_close(r, g["v10_thr"])
+    close(r, g["v10_thr"], st.iterations)
+
+
+@pytest.mark.parametrize("name", ["rmat10", "directed", "isolated", "grid"])
+def test_relabel_off_matches(gpu, small_graphs, name):
+    g = small_graphs[name]
+    r, st = solve(g["row_ptr"], g["col"], g["deg"], iters=20, relabel=False)
+    assert_close(r, g["v10_20"])
 
 
 @pytest.mark.parametrize("scale", [12, 14, 16])
@@ -107,7 +135,7 @@ def test_hub_rows_span_many_tiles(gpu):
     deg = g.out_degree()
     ref, _, _ = O.jacobi_f32(g.row_ptr, g.col, deg, 0.85, 0.0, 30)
     r, _ = solve(g.row_ptr, g.col, deg, iters=30)
-    assert_close(r, ref)
+    assert_parity_or_more_accurate(r, ref, g.row_ptr, g.col, 30)
     # a few more hubs plus leaves, rows landing on arbitrary tile offsets
     rng = np.random.default_rng(0)
     hubs = rng.integers(0, 2000, size=6)
@@ -116,8 +144,9 @@ def test_hub_rows_span_many_tiles(gpu):
     g = G.from_edges(src, dst, 60_000, symmetrize=True)
     deg = g.out_degree()
     ref, _, _ = O.jacobi_f32(g.row_ptr, g.col, deg, 0.85, 0.0, 20)
-    r, _ = solve(g.row_ptr, g.col, deg)
-    assert_close(r, ref)
+    for relabel in (True, False):
+        r, _ = solve(g.row_ptr, g.col, deg, relabel=relabel)
+        assert_parity_or_more_accurate(r, ref, g.row_ptr, g.col, 20)
 
 
 def test_bitwise_reproducible_and_launch_modes_agree(gpu):
