@@ -120,6 +120,35 @@ typedef struct nwgpu_pr_stats {
 int nwgpu_pr_run(nwgpu_graph* g, const uint32_t* out_degree, float* ranks, float damping, float threshold,
                  uint64_t max_iters, const nwgpu_pr_options* options, nwgpu_pr_stats* stats);
 
+/* Personalised PageRank with a one-hot teleport at `seed` (input vertex id):
+ *   r = (1 - d) e_seed + d A^T D^{-1} r,  r(0) = e_seed,
+ * the plain update of page_rank.hpp:133 with base_i = (1 - d) [i == seed];
+ * same stopping rule, leak semantics and argument conventions as nwgpu_pr_run.
+ * No counterpart in the reference (personalised PageRank is an extension). */
+int nwgpu_ppr_run(nwgpu_graph* g, const uint32_t* out_degree, uint32_t seed, float* ranks, float damping,
+                  float threshold, uint64_t max_iters, const nwgpu_pr_options* options, nwgpu_pr_stats* stats);
+
+typedef struct nwgpu_ppr_stats {
+  uint64_t  iterations;     /* sweeps run (the slowest column) */
+  int32_t   all_converged;  /* every column met the threshold */
+  double    device_ms;      /* CUDA-event time of the sweep loop */
+  double    ms_per_iter;
+  double    bytes_per_iter; /* 4 nnz + 4 (n+1) + 4 n + 16 k n */
+  uint32_t* col_iterations; /* optional, caller-owned [k]: sweeps until column c stopped */
+  double*   col_errors;     /* optional, caller-owned [k]: L1 change of column c's last sweep */
+  int32_t*  col_converged;  /* optional, caller-owned [k] */
+} nwgpu_ppr_stats;
+
+/* k personalised vectors solved together (k <= 128): seeds[k] are input
+ * vertex ids, ranks_nxk is an n x k row-major FP32 matrix in input vertex
+ * order (column c = the vector of seeds[c]). Each column stops at its own
+ * first sweep whose FP64 L1 change is < threshold (its values then stay
+ * fixed) or at max_iters. One column-index load feeds all k gathers.
+ * No counterpart in the reference. */
+int nwgpu_ppr_batched(nwgpu_graph* g, const uint32_t* out_degree, const uint32_t* seeds, uint32_t k, float* ranks_nxk,
+                      float damping, float threshold, uint64_t max_iters, const nwgpu_pr_options* options,
+                      nwgpu_ppr_stats* stats);
+
 /* Ask a running solve on g to stop at its next sweep boundary; the solve
  * returns NWGPU_ERR_ABORTED. Safe to call from another host thread. */
 int nwgpu_abort(nwgpu_graph* g);

@@ -59,6 +59,13 @@ class PrStats(C.Structure):
                 ("gteps", C.c_double), ("errors", C.POINTER(C.c_double)), ("errors_cap", C.c_uint64)]
 
 
+class PprStats(C.Structure):
+    _fields_ = [("iterations", C.c_uint64), ("all_converged", C.c_int32), ("device_ms", C.c_double),
+                ("ms_per_iter", C.c_double), ("bytes_per_iter", C.c_double),
+                ("col_iterations", C.POINTER(C.c_uint32)), ("col_errors", C.POINTER(C.c_double)),
+                ("col_converged", C.POINTER(C.c_int32))]
+
+
 # Every symbol include/nwgpu.h declares, with its C signature.
 _vp = C.c_void_p
 SIGNATURES = {
@@ -69,6 +76,10 @@ SIGNATURES = {
     "nwgpu_graph_get_info": (C.c_int, [_vp, C.POINTER(GraphInfo)]),
     "nwgpu_pr_run": (C.c_int, [_vp, _vp, _vp, C.c_float, C.c_float, C.c_uint64, C.POINTER(PrOptions),
                                C.POINTER(PrStats)]),
+    "nwgpu_ppr_run": (C.c_int, [_vp, _vp, C.c_uint32, _vp, C.c_float, C.c_float, C.c_uint64, C.POINTER(PrOptions),
+                                C.POINTER(PrStats)]),
+    "nwgpu_ppr_batched": (C.c_int, [_vp, _vp, _vp, C.c_uint32, _vp, C.c_float, C.c_float, C.c_uint64,
+                                    C.POINTER(PrOptions), C.POINTER(PprStats)]),
     "nwgpu_abort": (C.c_int, [_vp]),
 }
 

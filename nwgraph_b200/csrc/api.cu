@@ -1,27 +1,27 @@
-// C ABI of the PageRank engine (declared in include/nwgpu.h).
+// C ABI of the PageRank engine (declared in include/nwgpu.h): graph handles
+// and the single-vector solves.
 //
-// Host side of the drop-in: nwgpu_graph_create uploads and validates the CSR
-// once, relabels it (hubs first) and tiles it on the device; nwgpu_pr_run
-// replaces the body of nw::graph::page_rank / page_rank_v10
-// (include/nwgraph/algorithms/page_rank.hpp:92-147,
+// nwgpu_graph_create uploads and validates the CSR once, relabels it (hubs
+// first) and tiles it on the device; nwgpu_pr_run replaces the body of
+// nw::graph::page_rank / page_rank_v10 (include/nwgraph/algorithms/page_rank.hpp:92-147,
 // include/nwgraph/experimental/algorithms/page_rank.hpp:383-431) with one
 // CUDA-graph launch whose while loop runs the sweep and finishing kernels
 // until the device-side test "error < threshold" or max_iters stops it.
-#include <cstdarg>
-#include <cstdio>
-#include <cstring>
 #include <mutex>
 #include <new>
-#include <string>
 
-#include "../../include/nwgpu.h"
-#include "engine.h"
+#include "handle.h"
 
 using namespace nwgpu;
 
-namespace {
+namespace nwgpu {
 
+namespace {
 thread_local std::string g_last_error;
+std::once_flag           g_config_once;
+cudaError_t              g_config_err = cudaSuccess;
+constexpr int            kDefaultIpt = 8;
+}  // namespace
 
 int fail(int code, const char* fmt, ...) {
   char    buf[512];
@@ -39,82 +39,11 @@ int cuda_fail(cudaError_t e, const char* what) {
   return fail(NWGPU_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
-#define CK(call, what)                                 \
-  do {                                                 \
-    cudaError_t _e = (call);                           \
-    if (_e != cudaSuccess) return cuda_fail(_e, what); \
-  } while (0)
+void clear_error() { g_last_error.clear(); }
 
-constexpr int kDefaultIpt = 8;
+const std::string& last_error_text() { return g_last_error; }
 
-std::once_flag g_config_once;
-cudaError_t    g_config_err = cudaSuccess;
-
-}  // namespace
-
-struct nwgpu_graph {
-  int          device = 0;
-  int          sms = 148;
-  cudaStream_t stream = nullptr;
-  uint64_t     n = 0, nnz = 0;
-  bool         relabelled = false;
-  Relabelled   g;  // device CSR (relabelled, or the input order with perm/inv null)
-  Tiling       tiling{};
-  int          grid = 0;         // persistent sweep CTAs
-  int          finish_grid = 1;  // finishing-kernel CTAs
-  uint64_t     device_bytes = 0;
-
-  // Plain-solve buffers, allocated on first use and kept.
-  bool          solve_ready = false;
-  float*        rank = nullptr;
-  float*        contrib[2] = {nullptr, nullptr};
-  uint32_t*     deg = nullptr;
-  uint32_t*     stage_u32 = nullptr;  // host <-> device staging in input order
-  float*        cpart = nullptr;
-  float*        epart = nullptr;
-  double*       res_part = nullptr;
-  PrState*      st = nullptr;
-  double*       err_hist = nullptr;
-  uint32_t      err_cap = 4096;
-  PrState*      h_st = nullptr;     // pinned mirror of *st
-  unsigned int* h_abort = nullptr;  // mapped pinned abort word
-  unsigned int* d_abort = nullptr;
-  cudaEvent_t   ev0 = nullptr, ev1 = nullptr;
-
-  // CUDA graph of the sweep loop (arm node -> while node { sweep; finish }).
-  cudaGraph_t     cg = nullptr;
-  cudaGraphExec_t cg_exec = nullptr;
-  SweepArgs       cg_args{};  // arguments baked into cg_exec
-
-  ~nwgpu_graph() {
-    if (cg_exec) cudaGraphExecDestroy(cg_exec);
-    if (cg) cudaGraphDestroy(cg);
-    void* dev_ptrs[] = {g.row_ptr, g.col, g.w, g.perm, g.inv, tiling.tile_row, tiling.tile_nnz, rank, contrib[0],
-                        contrib[1], deg, stage_u32, cpart, epart, res_part, st, err_hist};
-    for (void* p : dev_ptrs)
-      if (p) cudaFree(p);
-    if (h_st) cudaFreeHost(h_st);
-    if (h_abort) cudaFreeHost(h_abort);
-    if (ev0) cudaEventDestroy(ev0);
-    if (ev1) cudaEventDestroy(ev1);
-    if (stream) cudaStreamDestroy(stream);
-  }
-};
-
-namespace {
-
-template <class T>
-cudaError_t dalloc(nwgpu_graph* g, T** p, uint64_t count) {
-  const uint64_t bytes = (count + kPad) * sizeof(T);
-  cudaError_t    e = cudaMalloc((void**)p, bytes);
-  if (e == cudaSuccess) {
-    g->device_bytes += bytes;
-    e = cudaMemsetAsync(*p, 0, bytes, g->stream);
-  }
-  return e;
-}
-
-int check_device(int* dev_out, int* sms_out) {
+static int check_device(int* dev_out, int* sms_out) {
   int         dev = 0, count = 0;
   cudaError_t e = cudaGetDeviceCount(&count);
   if (e != cudaSuccess || count == 0) {
@@ -156,6 +85,27 @@ int ensure_solve_buffers(nwgpu_graph* g) {
   g->solve_ready = true;
   return NWGPU_OK;
 }
+
+int load_degrees(nwgpu_graph* g, const uint32_t* out_degree, bool device_ptrs, cudaStream_t s) {
+  const uint64_t n = g->n;
+  if (g->relabelled) {
+    const uint32_t* src = out_degree;
+    if (!device_ptrs) {
+      CK(cudaMemcpyAsync(g->stage_u32, out_degree, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s), "copy out_degree");
+      src = g->stage_u32;
+    }
+    CK(launch_gather_u32(src, g->g.inv, g->deg, n, g->sms, s), "permute degrees");
+  } else {
+    CK(cudaMemcpyAsync(g->deg, out_degree, n * sizeof(uint32_t),
+                       device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s),
+       "copy out_degree");
+  }
+  return NWGPU_OK;
+}
+
+}  // namespace nwgpu
+
+namespace {
 
 SweepArgs make_sweep_args(nwgpu_graph* g, float damping, float base, int teleport, uint32_t seed) {
   SweepArgs a = {};
@@ -255,6 +205,102 @@ int run_sweeps(nwgpu_graph* g, const SweepArgs& a, uint32_t launch, uint64_t max
   return NWGPU_OK;
 }
 
+nwgpu_pr_options read_options(const nwgpu_pr_options* options) {
+  nwgpu_pr_options opt = {};
+  if (options) memcpy(&opt, options, options->size && options->size < sizeof(opt) ? options->size : sizeof(opt));
+  return opt;
+}
+
+// Shared body of nwgpu_pr_run (uniform teleport) and nwgpu_ppr_run (one-hot).
+int solve_single(nwgpu_graph* g, const uint32_t* out_degree, float* ranks, float damping, float threshold,
+                 uint64_t max_iters, const nwgpu_pr_options* options, nwgpu_pr_stats* stats, int teleport,
+                 uint32_t seed_in) {
+  clear_error();
+  if (!g) return fail(NWGPU_ERR_INVALID_ARG, "graph is NULL");
+  if (g->n && (!out_degree || !ranks)) return fail(NWGPU_ERR_INVALID_ARG, "out_degree / ranks is NULL");
+  if (!(damping >= 0.0f && damping <= 1.0f)) return fail(NWGPU_ERR_INVALID_ARG, "damping %g outside [0, 1]", (double)damping);
+  if (teleport == kTeleportSeed && seed_in >= g->n)
+    return fail(NWGPU_ERR_INVALID_ARG, "seed %u >= n = %llu", seed_in, (unsigned long long)g->n);
+  const nwgpu_pr_options opt = read_options(options);
+  if (opt.mode != NWGPU_MODE_PARITY) return fail(NWGPU_ERR_UNSUPPORTED, "mode %u is not supported", opt.mode);
+  if (opt.launch > NWGPU_LAUNCH_STREAM) return fail(NWGPU_ERR_INVALID_ARG, "launch %u unknown", opt.launch);
+  const uint64_t n = g->n;
+  if (stats) {
+    double*  eb = stats->errors;
+    uint64_t ec = stats->errors_cap;
+    memset(stats, 0, sizeof(*stats));
+    stats->errors = eb;
+    stats->errors_cap = ec;
+    stats->bytes_per_iter = 4.0 * (double)g->nnz + 4.0 * (double)(n + 1) + 20.0 * (double)n;
+  }
+  // page_rank.hpp:92-94: N = graph.size(); constants in double, stored as Real.
+  const float init = (float)(1.0 / (double)n);
+  const float base = (teleport == kTeleportSeed) ? (float)(1.0 - (double)damping)
+                                                 : (float)((1.0 - (double)damping) / (double)n);
+  if (n == 0) {
+    // The reference's sweep reduces over an empty range: error 0.
+    const uint64_t its = (max_iters == 0) ? 0 : ((0.0 < (double)threshold) ? 1 : max_iters);
+    if (stats) {
+      stats->iterations = its;
+      stats->converged = its > 0 && 0.0 < (double)threshold;
+    }
+    return NWGPU_OK;
+  }
+  int rc = ensure_solve_buffers(g);
+  if (rc) return rc;
+  cudaStream_t s = opt.stream ? (cudaStream_t)opt.stream : g->stream;
+  *(volatile unsigned int*)g->h_abort = 0u;
+  if ((rc = load_degrees(g, out_degree, opt.device_ptrs != 0, s))) return rc;
+  uint32_t seed = seed_in;
+  if (teleport == kTeleportSeed && g->relabelled)
+    CK(cudaMemcpy(&seed, g->g.perm + seed_in, sizeof(uint32_t), cudaMemcpyDeviceToHost), "seed id");
+  PrState h = {};
+  h.max_iters = max_iters;
+  h.chunk_end = kGraphChunk;
+  h.threshold = (double)threshold;
+  h.done = (max_iters == 0) ? 1u : 0u;
+  *g->h_st = h;
+  CK(cudaMemcpyAsync(g->st, g->h_st, sizeof(PrState), cudaMemcpyHostToDevice, s), "copy state");
+  SweepArgs a = make_sweep_args(g, damping, base, teleport, seed);
+  CK(launch_pr_init(a, n, init, g->sms, s), "pr_init");
+
+  CK(cudaEventRecord(g->ev0, s), "cudaEventRecord");
+  PrState fin{};
+  rc = run_sweeps(g, a, opt.launch, max_iters, s, &fin);
+  if (rc) return rc;
+  CK(cudaEventRecord(g->ev1, s), "cudaEventRecord");
+  if (g->relabelled) {
+    float* dst = opt.device_ptrs ? ranks : reinterpret_cast<float*>(g->stage_u32);
+    CK(launch_gather_f32(g->rank, g->g.perm, dst, n, g->sms, s), "permute ranks");
+    if (!opt.device_ptrs) CK(cudaMemcpyAsync(ranks, dst, n * sizeof(float), cudaMemcpyDeviceToHost, s), "copy ranks");
+  } else {
+    CK(cudaMemcpyAsync(ranks, g->rank, n * sizeof(float), opt.device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                       s),
+       "copy ranks");
+  }
+  CK(cudaStreamSynchronize(s), "copy ranks");
+  if (stats) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+    stats->iterations = fin.iter;
+    stats->final_error = fin.last_error;
+    stats->converged = (int32_t)fin.converged;
+    stats->device_ms = ms;
+    stats->ms_per_iter = fin.iter ? ms / (double)fin.iter : 0.0;
+    stats->gteps = ms > 0 ? (double)g->nnz * (double)fin.iter / (ms * 1e6) : 0.0;
+    if (stats->errors && stats->errors_cap) {
+      uint64_t m = fin.iter < stats->errors_cap ? fin.iter : stats->errors_cap;
+      if (m > g->err_cap) m = g->err_cap;
+      if (m) {
+        CK(cudaMemcpyAsync(stats->errors, g->err_hist, m * sizeof(double), cudaMemcpyDeviceToHost, s), "copy errors");
+        CK(cudaStreamSynchronize(s), "copy errors");
+      }
+    }
+  }
+  if (fin.aborted) return fail(NWGPU_ERR_ABORTED, "solve aborted after %llu sweeps", (unsigned long long)fin.iter);
+  return NWGPU_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -262,17 +308,18 @@ extern "C" {
 int nwgpu_abi_version(void) { return NWGPU_ABI_VERSION; }
 
 int nwgpu_last_error(char* buf, size_t len) {
+  const std::string& e = last_error_text();
   if (buf && len) {
-    size_t m = g_last_error.size() < len - 1 ? g_last_error.size() : len - 1;
-    memcpy(buf, g_last_error.data(), m);
+    size_t m = e.size() < len - 1 ? e.size() : len - 1;
+    memcpy(buf, e.data(), m);
     buf[m] = '\0';
   }
-  return (int)g_last_error.size();
+  return (int)e.size();
 }
 
 int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float* weights, uint64_t n, uint64_t nnz,
                        uint32_t flags, nwgpu_graph** out) {
-  g_last_error.clear();
+  clear_error();
   if (!out) return fail(NWGPU_ERR_INVALID_ARG, "out is NULL");
   *out = nullptr;
   if (!row_ptr) return fail(NWGPU_ERR_INVALID_ARG, "row_ptr is NULL");
@@ -300,16 +347,15 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
   const cudaMemcpyKind kind = (flags & NWGPU_GRAPH_DEVICE_PTRS) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   // Upload into padded buffers.
   Relabelled in;
-  if ((e = dalloc(g, &in.row_ptr, n + 1)) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(row_ptr)"));
-  if ((e = dalloc(g, &in.col, nnz)) != cudaSuccess) {
-    cudaFree(in.row_ptr);
-    return bail(cuda_fail(e, "cudaMalloc(col)"));
-  }
-  auto free_in = [&]() {
+  auto       free_in = [&]() {
     cudaFree(in.row_ptr);
     cudaFree(in.col);
     cudaFree(in.w);
   };
+  if ((e = dalloc(g, &in.row_ptr, n + 1)) != cudaSuccess || (e = dalloc(g, &in.col, nnz)) != cudaSuccess) {
+    free_in();
+    return bail(cuda_fail(e, "cudaMalloc(CSR)"));
+  }
   if ((e = cudaMemcpyAsync(in.row_ptr, row_ptr, (n + 1) * sizeof(uint32_t), kind, g->stream)) != cudaSuccess ||
       (nnz && (e = cudaMemcpyAsync(in.col, col, nnz * sizeof(uint32_t), kind, g->stream)) != cudaSuccess)) {
     free_in();
@@ -349,8 +395,6 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
     free_in();
     if (e != cudaSuccess) return bail(cuda_fail(e, "relabel"));
     g->relabelled = true;
-    g->device_bytes += (2 * (n + kPad) + (n + 1 + kPad)) * sizeof(uint32_t) + (nnz + kPad) * sizeof(uint32_t) +
-                       (weights ? (nnz + kPad) * sizeof(float) : 0);
   } else {
     g->g.row_ptr = in.row_ptr;
     g->g.col = in.col;
@@ -359,7 +403,6 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
   const int ipt = kDefaultIpt;
   if ((e = build_tiling(g->g.row_ptr, n, nnz, ipt, &g->tiling, g->stream)) != cudaSuccess)
     return bail(cuda_fail(e, "build_tiling"));
-  g->device_bytes += 2ull * (g->tiling.num_tiles + 2) * sizeof(uint32_t);
   const uint64_t want = (uint64_t)sms * sweep_blocks_per_sm(ipt);
   g->grid = (int)(want < g->tiling.num_tiles ? want : (g->tiling.num_tiles ? g->tiling.num_tiles : 1));
   g->finish_grid = finish_grid_for(g->tiling.num_tiles);
@@ -369,7 +412,7 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
 }
 
 int nwgpu_graph_destroy(nwgpu_graph* g) {
-  g_last_error.clear();
+  clear_error();
   if (!g) return NWGPU_OK;
   if (g->stream) cudaStreamSynchronize(g->stream);
   delete g;
@@ -399,97 +442,12 @@ int nwgpu_abort(nwgpu_graph* g) {
 
 int nwgpu_pr_run(nwgpu_graph* g, const uint32_t* out_degree, float* ranks, float damping, float threshold,
                  uint64_t max_iters, const nwgpu_pr_options* options, nwgpu_pr_stats* stats) {
-  g_last_error.clear();
-  if (!g) return fail(NWGPU_ERR_INVALID_ARG, "graph is NULL");
-  if (g->n && (!out_degree || !ranks)) return fail(NWGPU_ERR_INVALID_ARG, "out_degree / ranks is NULL");
-  if (!(damping >= 0.0f && damping <= 1.0f)) return fail(NWGPU_ERR_INVALID_ARG, "damping %g outside [0, 1]", (double)damping);
-  nwgpu_pr_options opt = {};
-  if (options) memcpy(&opt, options, options->size && options->size < sizeof(opt) ? options->size : sizeof(opt));
-  if (opt.mode != NWGPU_MODE_PARITY) return fail(NWGPU_ERR_UNSUPPORTED, "mode %u is not supported", opt.mode);
-  if (opt.launch > NWGPU_LAUNCH_STREAM) return fail(NWGPU_ERR_INVALID_ARG, "launch %u unknown", opt.launch);
-  const uint64_t n = g->n;
-  const double   bytes_iter = 4.0 * (double)g->nnz + 4.0 * (double)(n + 1) + 20.0 * (double)n;
-  if (stats) {
-    double*  eb = stats->errors;
-    uint64_t ec = stats->errors_cap;
-    memset(stats, 0, sizeof(*stats));
-    stats->errors = eb;
-    stats->errors_cap = ec;
-    stats->bytes_per_iter = bytes_iter;
-  }
-  // page_rank.hpp:92-94: N = graph.size(); constants in double, stored as Real.
-  const float init = (float)(1.0 / (double)n);
-  const float base = (float)((1.0 - (double)damping) / (double)n);
-  if (n == 0) {
-    // The reference's sweep reduces over an empty range: error 0.
-    const uint64_t its = (max_iters == 0) ? 0 : ((0.0 < (double)threshold) ? 1 : max_iters);
-    if (stats) {
-      stats->iterations = its;
-      stats->converged = its > 0 && 0.0 < (double)threshold;
-    }
-    return NWGPU_OK;
-  }
-  int rc = ensure_solve_buffers(g);
-  if (rc) return rc;
-  cudaStream_t s = opt.stream ? (cudaStream_t)opt.stream : g->stream;
-  const cudaMemcpyKind in_kind = opt.device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-  const cudaMemcpyKind out_kind = opt.device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-  *(volatile unsigned int*)g->h_abort = 0u;
+  return solve_single(g, out_degree, ranks, damping, threshold, max_iters, options, stats, kTeleportUniform, 0u);
+}
 
-  // degrees into internal order
-  if (g->relabelled) {
-    const uint32_t* src = out_degree;
-    if (!opt.device_ptrs) {
-      CK(cudaMemcpyAsync(g->stage_u32, out_degree, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s), "copy out_degree");
-      src = g->stage_u32;
-    }
-    CK(launch_gather_u32(src, g->g.inv, g->deg, n, g->sms, s), "permute degrees");
-  } else {
-    CK(cudaMemcpyAsync(g->deg, out_degree, n * sizeof(uint32_t), in_kind, s), "copy out_degree");
-  }
-  PrState h = {};
-  h.max_iters = max_iters;
-  h.chunk_end = kGraphChunk;
-  h.threshold = (double)threshold;
-  h.done = (max_iters == 0) ? 1u : 0u;
-  *g->h_st = h;
-  CK(cudaMemcpyAsync(g->st, g->h_st, sizeof(PrState), cudaMemcpyHostToDevice, s), "copy state");
-  SweepArgs a = make_sweep_args(g, damping, base, kTeleportUniform, 0u);
-  CK(launch_pr_init(a, n, init, g->sms, s), "pr_init");
-
-  CK(cudaEventRecord(g->ev0, s), "cudaEventRecord");
-  PrState fin{};
-  rc = run_sweeps(g, a, opt.launch, max_iters, s, &fin);
-  if (rc) return rc;
-  CK(cudaEventRecord(g->ev1, s), "cudaEventRecord");
-  if (g->relabelled) {
-    float* dst = opt.device_ptrs ? ranks : reinterpret_cast<float*>(g->stage_u32);
-    CK(launch_gather_f32(g->rank, g->g.perm, dst, n, g->sms, s), "permute ranks");
-    if (!opt.device_ptrs) CK(cudaMemcpyAsync(ranks, dst, n * sizeof(float), cudaMemcpyDeviceToHost, s), "copy ranks");
-  } else {
-    CK(cudaMemcpyAsync(ranks, g->rank, n * sizeof(float), out_kind, s), "copy ranks");
-  }
-  CK(cudaStreamSynchronize(s), "copy ranks");
-  if (stats) {
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, g->ev0, g->ev1);
-    stats->iterations = fin.iter;
-    stats->final_error = fin.last_error;
-    stats->converged = (int32_t)fin.converged;
-    stats->device_ms = ms;
-    stats->ms_per_iter = fin.iter ? ms / (double)fin.iter : 0.0;
-    stats->gteps = ms > 0 ? (double)g->nnz * (double)fin.iter / (ms * 1e6) : 0.0;
-    if (stats->errors && stats->errors_cap) {
-      uint64_t m = fin.iter < stats->errors_cap ? fin.iter : stats->errors_cap;
-      if (m > g->err_cap) m = g->err_cap;
-      if (m) {
-        CK(cudaMemcpyAsync(stats->errors, g->err_hist, m * sizeof(double), cudaMemcpyDeviceToHost, s), "copy errors");
-        CK(cudaStreamSynchronize(s), "copy errors");
-      }
-    }
-  }
-  if (fin.aborted) return fail(NWGPU_ERR_ABORTED, "solve aborted after %llu sweeps", (unsigned long long)fin.iter);
-  return NWGPU_OK;
+int nwgpu_ppr_run(nwgpu_graph* g, const uint32_t* out_degree, uint32_t seed, float* ranks, float damping,
+                  float threshold, uint64_t max_iters, const nwgpu_pr_options* options, nwgpu_pr_stats* stats) {
+  return solve_single(g, out_degree, ranks, damping, threshold, max_iters, options, stats, kTeleportSeed, seed);
 }
 
 }  // extern "C"

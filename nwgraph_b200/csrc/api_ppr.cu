@@ -1,0 +1,190 @@
+// C ABI: batched personalised PageRank (nwgpu_ppr_batched, include/nwgpu.h).
+// No counterpart in the reference; the single-vector personalised solve is
+// nwgpu_ppr_run in api.cu, and the looped baseline calls it k times.
+#include "handle.h"
+
+namespace nwgpu {
+
+void PprBuffers::release() {
+  if (cg_exec) cudaGraphExecDestroy(cg_exec);
+  if (cg) cudaGraphDestroy(cg);
+  cg_exec = nullptr;
+  cg = nullptr;
+  void* ptrs[] = {tiling.tile_row, tiling.tile_nnz, rank, contrib[0], contrib[1], out, cpart, epart, res_part,
+                  seeds, seeds_in, col_done, col_conv, col_iters, col_err, st};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (h_st) cudaFreeHost(h_st);
+  *this = PprBuffers();
+}
+
+static int ensure_ppr(nwgpu_graph* g, int K) {
+  PprBuffers& b = g->ppr;
+  if (b.K == K) return NWGPU_OK;
+  b.release();
+  const uint64_t n = g->n, nk = g->n * (uint64_t)K;
+  CK(build_tiling(g->g.row_ptr, n, g->nnz, kPprTileItems / kSweepThreads, &b.tiling, g->stream), "ppr tiling");
+  const uint64_t T = b.tiling.num_tiles;
+  b.sweep_grid = ppr_sweep_grid(K, g->sms);
+  b.finish_grid = g->sms * 4;
+  CK(dalloc(g, &b.rank, nk), "cudaMalloc(ppr rank)");
+  CK(dalloc(g, &b.contrib[0], nk), "cudaMalloc(ppr contrib)");
+  CK(dalloc(g, &b.contrib[1], nk), "cudaMalloc(ppr contrib)");
+  CK(dalloc(g, &b.out, nk), "cudaMalloc(ppr out)");
+  CK(dalloc(g, &b.cpart, (T + 1) * K), "cudaMalloc(ppr cpart)");
+  CK(dalloc(g, &b.epart, (T + 1) * K), "cudaMalloc(ppr epart)");
+  CK(dalloc(g, &b.res_part, (uint64_t)(b.sweep_grid + b.finish_grid) * K), "cudaMalloc(ppr res)");
+  CK(dalloc(g, &b.seeds, (uint64_t)K), "cudaMalloc(seeds)");
+  CK(dalloc(g, &b.seeds_in, (uint64_t)K), "cudaMalloc(seeds)");
+  CK(dalloc(g, &b.col_done, (uint64_t)K), "cudaMalloc(col flags)");
+  CK(dalloc(g, &b.col_conv, (uint64_t)K), "cudaMalloc(col flags)");
+  CK(dalloc(g, &b.col_iters, (uint64_t)K), "cudaMalloc(col iters)");
+  CK(dalloc(g, &b.col_err, (uint64_t)K), "cudaMalloc(col err)");
+  CK(dalloc(g, &b.st, 1), "cudaMalloc(ppr state)");
+  CK(cudaHostAlloc((void**)&b.h_st, sizeof(PprState), cudaHostAllocDefault), "cudaHostAlloc(ppr state)");
+  CK(cudaStreamSynchronize(g->stream), "ppr buffers");
+  b.K = K;
+  return NWGPU_OK;
+}
+
+static PprArgs make_ppr_args(nwgpu_graph* g, float damping) {
+  PprBuffers& b = g->ppr;
+  PprArgs     a = {};
+  a.row_ptr = g->g.row_ptr;
+  a.col = g->g.col;
+  a.tile_row = b.tiling.tile_row;
+  a.tile_nnz = b.tiling.tile_nnz;
+  a.num_tiles = b.tiling.num_tiles;
+  a.tile_items = (uint32_t)kPprTileItems;
+  a.deg = g->deg;
+  a.rank = b.rank;
+  a.contrib0 = b.contrib[0];
+  a.contrib1 = b.contrib[1];
+  a.cpart = b.cpart;
+  a.epart = b.epart;
+  a.res_part = b.res_part;
+  a.sweep_grid = (uint32_t)b.sweep_grid;
+  a.seeds = b.seeds;
+  a.col_done = b.col_done;
+  a.col_conv = b.col_conv;
+  a.col_iters = b.col_iters;
+  a.col_err = b.col_err;
+  a.st = b.st;
+  a.abort_word = g->d_abort;
+  a.damping = damping;
+  a.one_minus_d = (float)(1.0 - (double)damping);
+  return a;
+}
+
+}  // namespace nwgpu
+
+using namespace nwgpu;
+
+extern "C" int nwgpu_ppr_batched(nwgpu_graph* g, const uint32_t* out_degree, const uint32_t* seeds, uint32_t k,
+                                 float* ranks_nxk, float damping, float threshold, uint64_t max_iters,
+                                 const nwgpu_pr_options* options, nwgpu_ppr_stats* stats) {
+  clear_error();
+  if (!g) return fail(NWGPU_ERR_INVALID_ARG, "graph is NULL");
+  if (k == 0 || k > 128) return fail(NWGPU_ERR_INVALID_ARG, "k = %u outside [1, 128]", k);
+  if (!seeds || (g->n && (!out_degree || !ranks_nxk))) return fail(NWGPU_ERR_INVALID_ARG, "NULL array argument");
+  if (!(damping >= 0.0f && damping <= 1.0f)) return fail(NWGPU_ERR_INVALID_ARG, "damping %g outside [0, 1]", (double)damping);
+  nwgpu_pr_options opt = {};
+  if (options) memcpy(&opt, options, options->size && options->size < sizeof(opt) ? options->size : sizeof(opt));
+  if (opt.launch > NWGPU_LAUNCH_STREAM) return fail(NWGPU_ERR_INVALID_ARG, "launch %u unknown", opt.launch);
+  uint32_t h_seeds[128];
+  if (opt.device_ptrs) {
+    CK(cudaMemcpy(h_seeds, seeds, k * sizeof(uint32_t), cudaMemcpyDeviceToHost), "copy seeds");
+  } else {
+    memcpy(h_seeds, seeds, k * sizeof(uint32_t));
+  }
+  for (uint32_t c = 0; c < k; ++c)
+    if (h_seeds[c] >= g->n) return fail(NWGPU_ERR_INVALID_ARG, "seeds[%u] = %u >= n", c, h_seeds[c]);
+  const int      K = ppr_padded_k(k);
+  const uint64_t n = g->n;
+  if (stats) {
+    uint32_t* ci = stats->col_iterations;
+    double*   ce = stats->col_errors;
+    int32_t*  cc = stats->col_converged;
+    memset(stats, 0, sizeof(*stats));
+    stats->col_iterations = ci;
+    stats->col_errors = ce;
+    stats->col_converged = cc;
+    stats->bytes_per_iter = 4.0 * (double)g->nnz + 4.0 * (double)(n + 1) + 4.0 * (double)n + 16.0 * k * (double)n;
+  }
+  int rc = ensure_solve_buffers(g);
+  if (rc) return rc;
+  if ((rc = ensure_ppr(g, K))) return rc;
+  PprBuffers&  b = g->ppr;
+  cudaStream_t s = opt.stream ? (cudaStream_t)opt.stream : g->stream;
+  *(volatile unsigned int*)g->h_abort = 0u;
+  if ((rc = load_degrees(g, out_degree, opt.device_ptrs != 0, s))) return rc;
+  PprArgs a = make_ppr_args(g, damping);
+  CK(cudaMemcpyAsync(b.seeds_in, h_seeds, k * sizeof(uint32_t), cudaMemcpyHostToDevice, s), "copy seeds");
+  CK(launch_ppr_seeds(b.seeds_in, k, K, g->relabelled ? g->g.perm : nullptr, a, s), "ppr seeds");
+  PprState h = {};
+  h.max_iters = max_iters;
+  h.chunk_end = kGraphChunk;
+  h.threshold = (double)threshold;
+  h.done = (max_iters == 0) ? 1u : 0u;
+  *b.h_st = h;
+  CK(cudaMemcpyAsync(b.st, b.h_st, sizeof(PprState), cudaMemcpyHostToDevice, s), "copy ppr state");
+  CK(launch_ppr_init(a, K, n, g->sms, s), "ppr init");
+  CK(cudaEventRecord(g->ev0, s), "cudaEventRecord");
+  if (opt.launch == NWGPU_LAUNCH_GRAPH) {
+    if (!b.cg_exec || b.cg_damping != damping) {
+      if (b.cg_exec) cudaGraphExecDestroy(b.cg_exec);
+      if (b.cg) cudaGraphDestroy(b.cg);
+      b.cg_exec = nullptr;
+      CK(cudaGraphCreate(&b.cg, 0), "cudaGraphCreate");
+      CK(build_ppr_graph(b.cg, a, K, b.sweep_grid, b.finish_grid, b.st, &b.cg_exec), "ppr graph");
+      b.cg_damping = damping;
+    }
+    const uint64_t max_launches = max_iters / kGraphChunk + 2;
+    for (uint64_t l = 0;; ++l) {
+      if (l == max_launches) return fail(NWGPU_ERR_CUDA, "ppr sweep loop did not finish");
+      CK(cudaGraphLaunch(b.cg_exec, s), "cudaGraphLaunch");
+      CK(cudaMemcpyAsync(b.h_st, b.st, sizeof(PprState), cudaMemcpyDeviceToHost, s), "copy ppr state");
+      CK(cudaStreamSynchronize(s), "ppr sweep loop");
+      if (b.h_st->done) break;
+    }
+  } else {
+    uint64_t launched = 0;
+    for (;;) {
+      const uint64_t batch = (max_iters - launched) < kGraphChunk ? (max_iters - launched) : kGraphChunk;
+      for (uint64_t i = 0; i < batch; ++i) CK(launch_ppr_sweep(a, K, b.sweep_grid, b.finish_grid, s), "ppr sweep");
+      launched += batch;
+      CK(cudaMemcpyAsync(b.h_st, b.st, sizeof(PprState), cudaMemcpyDeviceToHost, s), "copy ppr state");
+      CK(cudaStreamSynchronize(s), "ppr sweep loop");
+      if (b.h_st->done || launched >= max_iters) break;
+    }
+  }
+  CK(cudaEventRecord(g->ev1, s), "cudaEventRecord");
+  float* dst = opt.device_ptrs ? ranks_nxk : b.out;
+  CK(launch_ppr_output(b.rank, g->relabelled ? g->g.perm : nullptr, n, K, k, dst, g->sms, s), "ppr output");
+  if (!opt.device_ptrs)
+    CK(cudaMemcpyAsync(ranks_nxk, dst, n * k * sizeof(float), cudaMemcpyDeviceToHost, s), "copy ranks");
+  uint32_t h_iters[128], h_conv[128];
+  double   h_err[128];
+  CK(cudaMemcpyAsync(h_iters, b.col_iters, K * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "copy col iters");
+  CK(cudaMemcpyAsync(h_conv, b.col_conv, K * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "copy col flags");
+  CK(cudaMemcpyAsync(h_err, b.col_err, K * sizeof(double), cudaMemcpyDeviceToHost, s), "copy col err");
+  CK(cudaStreamSynchronize(s), "ppr output");
+  const PprState fin = *b.h_st;
+  if (stats) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+    stats->iterations = fin.iter;
+    stats->device_ms = ms;
+    stats->ms_per_iter = fin.iter ? ms / (double)fin.iter : 0.0;
+    int all = 1;
+    for (uint32_t c = 0; c < k; ++c) {
+      all &= (h_conv[c] != 0);
+      if (stats->col_iterations) stats->col_iterations[c] = h_iters[c];
+      if (stats->col_errors) stats->col_errors[c] = h_err[c];
+      if (stats->col_converged) stats->col_converged[c] = (int32_t)h_conv[c];
+    }
+    stats->all_converged = all;
+  }
+  if (fin.aborted) return fail(NWGPU_ERR_ABORTED, "batched solve aborted after %llu sweeps", (unsigned long long)fin.iter);
+  return NWGPU_OK;
+}

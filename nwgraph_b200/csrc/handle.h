@@ -1,0 +1,119 @@
+// Internal: the graph handle and host helpers shared by the C ABI files.
+#pragma once
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/nwgpu.h"
+#include "engine.h"
+#include "ppr.h"
+
+namespace nwgpu {
+
+int  fail(int code, const char* fmt, ...);
+int  cuda_fail(cudaError_t e, const char* what);
+void clear_error();
+const std::string& last_error_text();
+
+#define CK(call, what)                                         \
+  do {                                                         \
+    cudaError_t _e = (call);                                   \
+    if (_e != cudaSuccess) return ::nwgpu::cuda_fail(_e, what); \
+  } while (0)
+
+// Buffers of the batched personalised solve (K padded columns).
+struct PprBuffers {
+  int             K = 0;
+  Tiling          tiling{};  // warp tiles of kPprTileItems
+  int             sweep_grid = 0, finish_grid = 0;
+  float*          rank = nullptr;
+  float*          contrib[2] = {nullptr, nullptr};
+  float*          out = nullptr;  // n x K staging for the output
+  float*          cpart = nullptr;
+  float*          epart = nullptr;
+  double*         res_part = nullptr;
+  uint32_t*       seeds = nullptr;
+  uint32_t*       seeds_in = nullptr;
+  uint32_t*       col_done = nullptr;
+  uint32_t*       col_conv = nullptr;
+  uint32_t*       col_iters = nullptr;
+  double*         col_err = nullptr;
+  PprState*       st = nullptr;
+  PprState*       h_st = nullptr;
+  cudaGraph_t     cg = nullptr;
+  cudaGraphExec_t cg_exec = nullptr;
+  float           cg_damping = -1.f;
+  void            release();
+};
+
+}  // namespace nwgpu
+
+struct nwgpu_graph {
+  int          device = 0;
+  int          sms = 148;
+  cudaStream_t stream = nullptr;
+  uint64_t     n = 0, nnz = 0;
+  bool         relabelled = false;
+  nwgpu::Relabelled g;  // device CSR (relabelled, or the input order with perm/inv null)
+  nwgpu::Tiling tiling{};
+  int          grid = 0;         // persistent sweep CTAs
+  int          finish_grid = 1;  // finishing-kernel CTAs
+  uint64_t     device_bytes = 0;
+
+  // Plain-solve buffers, allocated on first use and kept.
+  bool          solve_ready = false;
+  float*        rank = nullptr;
+  float*        contrib[2] = {nullptr, nullptr};
+  uint32_t*     deg = nullptr;
+  uint32_t*     stage_u32 = nullptr;  // host <-> device staging in input order
+  float*        cpart = nullptr;
+  float*        epart = nullptr;
+  double*       res_part = nullptr;
+  nwgpu::PrState* st = nullptr;
+  double*       err_hist = nullptr;
+  uint32_t      err_cap = 4096;
+  nwgpu::PrState* h_st = nullptr;     // pinned mirror of *st
+  unsigned int* h_abort = nullptr;  // mapped pinned abort word
+  unsigned int* d_abort = nullptr;
+  cudaEvent_t   ev0 = nullptr, ev1 = nullptr;
+
+  // CUDA graph of the sweep loop (arm node -> while node { sweep; finish }).
+  cudaGraph_t     cg = nullptr;
+  cudaGraphExec_t cg_exec = nullptr;
+  nwgpu::SweepArgs cg_args{};  // arguments baked into cg_exec
+
+  nwgpu::PprBuffers ppr;
+
+  ~nwgpu_graph() {
+    ppr.release();
+    if (cg_exec) cudaGraphExecDestroy(cg_exec);
+    if (cg) cudaGraphDestroy(cg);
+    void* dev_ptrs[] = {g.row_ptr, g.col, g.w, g.perm, g.inv, tiling.tile_row, tiling.tile_nnz, rank, contrib[0],
+                        contrib[1], deg, stage_u32, cpart, epart, res_part, st, err_hist};
+    for (void* p : dev_ptrs)
+      if (p) cudaFree(p);
+    if (h_st) cudaFreeHost(h_st);
+    if (h_abort) cudaFreeHost(h_abort);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace nwgpu {
+template <class T>
+cudaError_t dalloc(nwgpu_graph* g, T** p, uint64_t count) {
+  const uint64_t bytes = (count + kPad) * sizeof(T);
+  cudaError_t    e = cudaMalloc((void**)p, bytes);
+  if (e == cudaSuccess) {
+    g->device_bytes += bytes;
+    e = cudaMemsetAsync(*p, 0, bytes, g->stream);
+  }
+  return e;
+}
+int ensure_solve_buffers(nwgpu_graph* g);
+// degrees (input order, host or device) -> g->deg (internal order)
+int load_degrees(nwgpu_graph* g, const uint32_t* out_degree, bool device_ptrs, cudaStream_t s);
+}  // namespace nwgpu

@@ -1,0 +1,62 @@
+// Internal interface of the batched personalised PageRank kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace nwgpu {
+
+constexpr int kPprTileItems = 512;  // merge items per warp tile
+constexpr int kPprPrefetch = 8;     // gathered rows in flight per warp
+
+struct PprState {
+  unsigned long long iter;
+  unsigned long long max_iters;
+  unsigned long long chunk_end;
+  double             threshold;
+  unsigned int       ticket;
+  unsigned int       done;
+  unsigned int       aborted;
+  unsigned int       pad_;
+};
+
+struct PprArgs {
+  const uint32_t* row_ptr;
+  const uint32_t* col;
+  const uint32_t* tile_row;  // warp tiles of kPprTileItems
+  const uint32_t* tile_nnz;
+  uint32_t        num_tiles;
+  uint32_t        tile_items;
+  const uint32_t* deg;
+  float*          rank;      // n x K
+  float*          contrib0;  // n x K, ping-pong
+  float*          contrib1;
+  float*          cpart;     // num_tiles x K
+  float*          epart;
+  double*         res_part;  // (sweep_grid + finish_grid) x K
+  uint32_t        sweep_grid;
+  const uint32_t* seeds;     // K internal seed ids (0xffffffff: padding column)
+  uint32_t*       col_done;  // K flags
+  uint32_t*       col_conv;  // K flags
+  uint32_t*       col_iters; // K sweep counts
+  double*         col_err;   // K last L1 changes
+  PprState*       st;
+  const volatile unsigned int* abort_word;
+  cudaGraphConditionalHandle   cond;
+  int                          use_cond;
+  float                        damping;
+  float                        one_minus_d;
+};
+
+int         ppr_padded_k(uint32_t k);
+int         ppr_sweep_grid(int K, int sms);
+cudaError_t launch_ppr_seeds(const uint32_t* seeds_in, uint32_t k, int K, const uint32_t* perm, const PprArgs& a,
+                             cudaStream_t s);
+cudaError_t launch_ppr_init(const PprArgs& a, int K, uint64_t n, int sms, cudaStream_t s);
+cudaError_t launch_ppr_output(const float* rank, const uint32_t* perm, uint64_t n, int K, uint32_t k, float* out,
+                              int sms, cudaStream_t s);
+cudaError_t launch_ppr_sweep(const PprArgs& a, int K, int sweep_grid, int finish_grid, cudaStream_t s);
+cudaError_t build_ppr_graph(cudaGraph_t g, const PprArgs& proto, int K, int sweep_grid, int finish_grid,
+                            PprState* st, cudaGraphExec_t* exec);
+
+}  // namespace nwgpu

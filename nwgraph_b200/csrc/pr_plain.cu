@@ -77,9 +77,9 @@ __device__ __forceinline__ uint64_t policy_evict_first() {
 // ---------------------------------------------------------------------------
 struct TileMeta {
   uint32_t r0, r1, k0, k1;  // merge-path coordinates of the tile
-  uint32_t col_at;          // stage word holding col[k0]
+  uint32_t col_at;          // stage word holding col[k0] (0..3)
   uint32_t rp_at;           // stage word holding row_ptr[r0] (row_ptr[r0..r1] follow)
-  uint32_t rk_at;           // stage word holding rank[r0]
+  uint32_t rk_at;           // stage word holding rank[r0], or ~0u when rank/deg are not staged
   uint32_t dg_at;           // stage word holding deg[r0]
 };
 
@@ -87,12 +87,13 @@ template <int NT, int IPT>
 struct SweepSmem {
   static constexpr int D = NT * IPT;
   static constexpr int NW = NT / 32;
-  // col (<= E+6 words) + row_ptr (<= R+7) + rank (<= R+6) + deg (<= R+6),
-  // each rounded to 16 bytes, with E + R <= D.
-  static constexpr int STG = 3 * D + 32;
+  // col[k0,k1) and row_ptr[r0..r1] rounded out to 16 bytes share D + 16 words
+  // (E + R <= D); rank and deg of the tile's rows follow when R <= D / 4
+  // (row-heavy tiles read them from global memory in the epilogue).
+  static constexpr int RV = D / 4;
+  static constexpr int STG = D + 16 + 2 * (RV + 8);
   uint32_t stage[2][STG];
-  float    val[2][D];  // gathered contributions of the tile being reduced / the next one
-  float    z[D];       // row sums of the tile
+  float    z[D];  // row sums of the tile
   uint32_t wkey[NW];
   float    wsum[NW];
   double   red[NW];
@@ -111,20 +112,23 @@ __device__ __forceinline__ float base_of(const SweepArgs& a, uint32_t r) {
 }
 
 // Thread 0: bring tile t's slices into stage `stg` and record where they landed.
+template <int NT, int IPT>
 __device__ __forceinline__ void issue_tile(const SweepArgs& a, uint32_t t, uint32_t* stg, TileMeta* m, uint64_t* bar,
                                            uint64_t pol) {
+  constexpr int  RV = SweepSmem<NT, IPT>::RV;
   const uint32_t r0 = a.tile_row[t], r1 = a.tile_row[t + 1], k0 = a.tile_nnz[t], k1 = a.tile_nnz[t + 1];
   const uint32_t ca0 = k0 & ~3u, ca1 = (k1 + 3u) & ~3u;  // col[k0, k1)
   const uint32_t pa0 = r0 & ~3u, pa1 = (r1 + 4u) & ~3u;  // row_ptr[r0 .. r1]
   const uint32_t va0 = r0 & ~3u, va1 = (r1 + 3u) & ~3u;  // rank / deg [r0, r1)
-  const uint32_t cw = ca1 - ca0, pw = pa1 - pa0, vw = (r1 > r0) ? va1 - va0 : 0u;
+  const bool     stage_rows = (r1 > r0) && (r1 - r0 <= (uint32_t)RV);
+  const uint32_t cw = ca1 - ca0, pw = pa1 - pa0, vw = stage_rows ? va1 - va0 : 0u;
   m->r0 = r0;
   m->r1 = r1;
   m->k0 = k0;
   m->k1 = k1;
   m->col_at = k0 - ca0;
   m->rp_at = cw + (r0 - pa0);
-  m->rk_at = cw + pw + (r0 - va0);
+  m->rk_at = stage_rows ? cw + pw + (r0 - va0) : ~0u;
   m->dg_at = cw + pw + vw + (r0 - va0);
   mbar_arrive_expect_tx(bar, 4u * (cw + pw + 2u * vw));
   if (cw) bulk_load(stg, a.col + ca0, 4u * cw, bar, pol);
@@ -135,66 +139,102 @@ __device__ __forceinline__ void issue_tile(const SweepArgs& a, uint32_t t, uint3
   }
 }
 
+// Each thread gathers the contributions of its IPT consecutive entries
+// [tid*IPT, tid*IPT + IPT) of the tile into registers. The column ids are read
+// as 16-byte words from the aligned stage and shifted by col_at (uniform).
 template <int NT, int IPT>
 __device__ __forceinline__ void gather_tile(const uint32_t* stg, const TileMeta& m, const float* __restrict__ cin,
                                             float (&v)[IPT], uint64_t pol) {
-  const int       E = (int)(m.k1 - m.k0);
-  const uint32_t* c = stg + m.col_at;
-  uint32_t        idx[IPT];
+  static_assert(IPT % 4 == 0, "IPT must be a multiple of 4");
+  const int  E = (int)(m.k1 - m.k0);
+  const int  e0 = (int)threadIdx.x * IPT;
+  uint32_t   w[IPT + 4];
+  const uint4* src = reinterpret_cast<const uint4*>(stg + e0);
 #pragma unroll
-  for (int u = 0; u < IPT; ++u) {
-    const int j = (int)threadIdx.x + u * NT;
-    idx[u] = (j < E) ? c[j] : 0u;
+  for (int q = 0; q < IPT / 4 + 1; ++q) {
+    const uint4 x = src[q];
+    w[4 * q + 0] = x.x;
+    w[4 * q + 1] = x.y;
+    w[4 * q + 2] = x.z;
+    w[4 * q + 3] = x.w;
+  }
+  uint32_t idx[IPT];
+  switch (m.col_at) {
+    case 0:
+#pragma unroll
+      for (int u = 0; u < IPT; ++u) idx[u] = w[u];
+      break;
+    case 1:
+#pragma unroll
+      for (int u = 0; u < IPT; ++u) idx[u] = w[u + 1];
+      break;
+    case 2:
+#pragma unroll
+      for (int u = 0; u < IPT; ++u) idx[u] = w[u + 2];
+      break;
+    default:
+#pragma unroll
+      for (int u = 0; u < IPT; ++u) idx[u] = w[u + 3];
+      break;
   }
 #pragma unroll
-  for (int u = 0; u < IPT; ++u) {
-    const int j = (int)threadIdx.x + u * NT;
-    v[u] = (j < E) ? ld_gather(cin + idx[u], pol) : 0.f;
-  }
+  for (int u = 0; u < IPT; ++u) v[u] = (e0 + u < E) ? ld_gather(cin + idx[u], pol) : 0.f;
 }
 
-// Reduce the tile in stage s; returns this thread's FP64 |dr| sum.
+// Reduce the tile in stage s from the gathered values v; returns this thread's
+// FP64 |dr| sum. Entry-parallel: thread tid owns entries [tid*IPT, tid*IPT+IPT),
+// finds the row of its first entry by binary search, and touches shared memory
+// only where a row ends. Rows crossing threads are combined by a block-wide
+// segmented scan of (row, partial) carries.
 template <int NT, int IPT>
 __device__ __forceinline__ double reduce_tile(const SweepArgs& a, SweepSmem<NT, IPT>& S, int s, uint32_t t,
-                                              float* __restrict__ cout, uint64_t pol_keep) {
+                                              const float (&v)[IPT], float* __restrict__ cout, uint64_t pol_keep) {
   const TileMeta  m = S.meta[s];
   const int       R = (int)(m.r1 - m.r0), E = (int)(m.k1 - m.k0);
   const uint32_t* rp = S.stage[s] + m.rp_at;  // rp[j] = row_ptr[r0 + j], j = 0..R
-  const float*    val = S.val[s];
   const int       tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int       e0 = tid * IPT;
 
-  // merge-path walk of IPT items over shared memory
-  const int total = R + E;
-  const int d0 = min(tid * IPT, total), d1 = min(d0 + IPT, total);
-  int       lo = max(0, d0 - E), hi = min(d0, R);
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if ((int)(rp[mid + 1] - m.k0) <= d0 - mid - 1)
-      lo = mid + 1;
-    else
-      hi = mid;
-  }
-  int   i = lo, k = d0 - lo, first = -1;
-  int   end_i = (i < R) ? (int)(rp[i + 1] - m.k0) : 0x7fffffff;
-  float acc = 0.f;
+  uint32_t key = 0xffffffffu;  // row this thread's range ends in (none without entries)
+  float    acc = 0.f;
+  int      first = -1;         // first row this thread finishes
+  if (e0 < E) {
+    const int e_end = min(e0 + IPT, E);
+    int       lo = 0, hi = R;  // largest i in [0, R] whose start (rp[i] - k0) <= e0
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if ((int)(rp[mid] - m.k0) <= e0)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    int i = lo;
+    int nxt = (i < R) ? (int)(rp[i + 1] - m.k0) : 0x7fffffff;
 #pragma unroll
-  for (int q = 0; q < IPT; ++q) {
-    if (d0 + q < d1) {
-      if (k < end_i) {
-        acc += val[k];
-        ++k;
-      } else {
-        S.z[i] = acc;
-        if (first < 0) first = i;
-        acc = 0.f;
-        ++i;
-        end_i = (i < R) ? (int)(rp[i + 1] - m.k0) : 0x7fffffff;
+    for (int u = 0; u < IPT; ++u) {
+      const int e = e0 + u;
+      if (e < e_end) {
+        while (e >= nxt) {
+          S.z[i] = acc;
+          if (first < 0) first = i;
+          acc = 0.f;
+          ++i;
+          nxt = (i < R) ? (int)(rp[i + 1] - m.k0) : 0x7fffffff;
+        }
+        acc += v[u];
       }
     }
+    while (e_end >= nxt) {  // rows ending exactly at the end of this range
+      S.z[i] = acc;
+      if (first < 0) first = i;
+      acc = 0.f;
+      ++i;
+      nxt = (i < R) ? (int)(rp[i + 1] - m.k0) : 0x7fffffff;
+    }
+    key = (uint32_t)i;
   }
-  // segmented inclusive scan of the carries (key = row the thread ends in)
-  const uint32_t key = (uint32_t)i;
-  float          sv = acc;
+  // segmented inclusive scan of the carries
+  float sv = acc;
 #pragma unroll
   for (int off = 1; off < 32; off <<= 1) {
     const uint32_t k2 = __shfl_up_sync(kFullMask, key, off);
@@ -220,7 +260,7 @@ __device__ __forceinline__ double reduce_tile(const SweepArgs& a, SweepSmem<NT, 
   float    pinc = __shfl_up_sync(kFullMask, inc, 1);
   if (lane == 0) {
     if (warp == 0) {
-      pkey = 0xffffffffu;
+      pkey = 0xfffffffeu;
       pinc = 0.f;
     } else {  // the previous warp's last thread, recomputed from the warp totals
       pkey = S.wkey[warp - 1];
@@ -234,26 +274,41 @@ __device__ __forceinline__ double reduce_tile(const SweepArgs& a, SweepSmem<NT, 
   if (first >= 0 && pkey == (uint32_t)first) S.z[first] = pinc + S.z[first];
   __syncthreads();
 
-  // epilogue of the rows that start and end in this tile
-  const bool      is_cont = rp[0] < m.k0;  // row r0 began in an earlier tile
-  const bool      has_co = m.k1 > rp[R];   // row r1 continues into the next tile
-  const float*    rk = reinterpret_cast<const float*>(S.stage[s] + m.rk_at);
-  const uint32_t* dg = S.stage[s] + m.dg_at;
-  double          res = 0.0;
-  for (int j = (is_cont ? 1 : 0) + tid; j < R; j += NT) {
-    const uint32_t r = m.r0 + j;
-    const float    nr = fmaf(a.damping, S.z[j], base_of(a, r));
-    st_stream(a.rank + r, nr);
-    st_keep(cout + r, nr / (float)dg[j], pol_keep);
-    res += (double)fabsf(nr - rk[j]);
+  // epilogue of the rows that start and end in this tile; rows without
+  // entries in the tile were never written and sum to zero
+  const bool is_cont = rp[0] < m.k0;  // row r0 began in an earlier tile
+  const bool has_co = m.k1 > rp[R];   // row r1 continues into the next tile
+  double     res = 0.0;
+  if (m.rk_at != ~0u) {
+    const float*    rk = reinterpret_cast<const float*>(S.stage[s] + m.rk_at);
+    const uint32_t* dg = S.stage[s] + m.dg_at;
+    for (int j = (is_cont ? 1 : 0) + tid; j < R; j += NT) {
+      const uint32_t r = m.r0 + j;
+      const float    z = (rp[j + 1] > rp[j]) ? S.z[j] : 0.f;
+      const float    nr = fmaf(a.damping, z, base_of(a, r));
+      st_stream(a.rank + r, nr);
+      st_keep(cout + r, nr / (float)dg[j], pol_keep);
+      res += (double)fabsf(nr - rk[j]);
+    }
+  } else {
+    for (int j = (is_cont ? 1 : 0) + tid; j < R; j += NT) {
+      const uint32_t r = m.r0 + j;
+      const float    z = (rp[j + 1] > rp[j]) ? S.z[j] : 0.f;
+      const float    nr = fmaf(a.damping, z, base_of(a, r));
+      const float    old = ld_stream(a.rank + r);
+      const uint32_t dg = ld_stream(a.deg + r);
+      st_stream(a.rank + r, nr);
+      st_keep(cout + r, nr / (float)dg, pol_keep);
+      res += (double)fabsf(nr - old);
+    }
   }
-  if (tid == 0 && is_cont && R >= 1) a.epart[t] = S.z[0];
-  if (tid == NT - 1 && has_co) a.cpart[t] = (key == (uint32_t)R) ? inc : 0.f;
+  if (tid == 0 && is_cont && R >= 1) a.epart[t] = (rp[1] > m.k0) ? S.z[0] : 0.f;
+  if (has_co && E > 0 && tid == (E - 1) / IPT) a.cpart[t] = (key == (uint32_t)R) ? inc : 0.f;
   return res;
 }
 
 template <int NT, int IPT>
-__global__ void __launch_bounds__(NT) pr_sweep_kernel(const SweepArgs a) {
+__global__ void __launch_bounds__(NT, 4) pr_sweep_kernel(const SweepArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   auto&          S = *reinterpret_cast<SweepSmem<NT, IPT>*>(smem_raw);
   const int      tid = threadIdx.x;
@@ -282,31 +337,38 @@ __global__ void __launch_bounds__(NT) pr_sweep_kernel(const SweepArgs a) {
   uint32_t t = blockIdx.x;
   if (t < T) {
     if (tid == 0) {
-      issue_tile(a, t, S.stage[0], &S.meta[0], &S.bar[0], pol_stream);
-      if (t + G < T) issue_tile(a, t + G, S.stage[1], &S.meta[1], &S.bar[1], pol_stream);
+      issue_tile<NT, IPT>(a, t, S.stage[0], &S.meta[0], &S.bar[0], pol_stream);
+      if (t + G < T) issue_tile<NT, IPT>(a, t + G, S.stage[1], &S.meta[1], &S.bar[1], pol_stream);
     }
-    float v[IPT];
+    float v0[IPT], v1[IPT];
     ok = mbar_wait(&S.bar[0], 0u);
-    if (ok) {
-      gather_tile<NT, IPT>(S.stage[0], S.meta[0], cin, v, pol_keep);
-#pragma unroll
-      for (int u = 0; u < IPT; ++u) S.val[0][tid + u * NT] = v[u];
-    }
+    if (ok) gather_tile<NT, IPT>(S.stage[0], S.meta[0], cin, v0, pol_keep);
     ok = __syncthreads_and(ok);
-    for (int i = 0; ok && t < T; ++i, t += G) {
-      const int      s = i & 1;
-      const uint32_t tn = t + G;
+    // two tiles per trip so the register sets alternate without copies
+    for (int i = 0; ok && t < T; i += 2) {
+      // even tile t in stage 0 (values v0); prefetch tile t+G into v1
+      uint32_t tn = t + G;
       if (tn < T) {
-        ok = mbar_wait(&S.bar[s ^ 1], (uint32_t)((i + 1) >> 1) & 1u);
-        if (ok) gather_tile<NT, IPT>(S.stage[s ^ 1], S.meta[s ^ 1], cin, v, pol_keep);
+        ok = mbar_wait(&S.bar[1], (uint32_t)(i >> 1) & 1u);
+        if (ok) gather_tile<NT, IPT>(S.stage[1], S.meta[1], cin, v1, pol_keep);
       }
-      res += reduce_tile<NT, IPT>(a, S, s, t, cout, pol_keep);
-      if (tn < T && ok) {
-#pragma unroll
-        for (int u = 0; u < IPT; ++u) S.val[s ^ 1][tid + u * NT] = v[u];
+      res += reduce_tile<NT, IPT>(a, S, 0, t, v0, cout, pol_keep);
+      ok = __syncthreads_and(ok);
+      if (ok && tid == 0 && t + 2 * G < T)
+        issue_tile<NT, IPT>(a, t + 2 * G, S.stage[0], &S.meta[0], &S.bar[0], pol_stream);
+      t = tn;
+      if (!ok || t >= T) break;
+      // odd tile t in stage 1 (values v1); prefetch tile t+G into v0
+      tn = t + G;
+      if (tn < T) {
+        ok = mbar_wait(&S.bar[0], (uint32_t)((i >> 1) + 1) & 1u);
+        if (ok) gather_tile<NT, IPT>(S.stage[0], S.meta[0], cin, v0, pol_keep);
       }
-      ok = __syncthreads_and(ok);  // stage s and val[s] are free, val[s^1] is ready
-      if (ok && tid == 0 && t + 2 * G < T) issue_tile(a, t + 2 * G, S.stage[s], &S.meta[s], &S.bar[s], pol_stream);
+      res += reduce_tile<NT, IPT>(a, S, 1, t, v1, cout, pol_keep);
+      ok = __syncthreads_and(ok);
+      if (ok && tid == 0 && t + 2 * G < T)
+        issue_tile<NT, IPT>(a, t + 2 * G, S.stage[1], &S.meta[1], &S.bar[1], pol_stream);
+      t = tn;
     }
   }
 
@@ -483,9 +545,9 @@ static void* sweep_fn() {
 static void* sweep_fn_for(int ipt) {
   switch (ipt) {
     case 4: return sweep_fn<4>();
-    case 6: return sweep_fn<6>();
     case 8: return sweep_fn<8>();
     case 12: return sweep_fn<12>();
+    case 16: return sweep_fn<16>();
     default: return nullptr;
   }
 }
@@ -493,9 +555,9 @@ static void* sweep_fn_for(int ipt) {
 size_t sweep_smem_bytes(int ipt) {
   switch (ipt) {
     case 4: return sweep_smem<kSweepThreads, 4>();
-    case 6: return sweep_smem<kSweepThreads, 6>();
     case 8: return sweep_smem<kSweepThreads, 8>();
     case 12: return sweep_smem<kSweepThreads, 12>();
+    case 16: return sweep_smem<kSweepThreads, 16>();
     default: return 0;
   }
 }
@@ -503,7 +565,7 @@ size_t sweep_smem_bytes(int ipt) {
 bool ipt_supported(int ipt) { return sweep_fn_for(ipt) != nullptr; }
 
 cudaError_t configure_sweep_kernels() {
-  for (int ipt : {4, 6, 8, 12}) {
+  for (int ipt : {4, 8, 12, 16}) {
     cudaError_t e = cudaFuncSetAttribute(sweep_fn_for(ipt), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)sweep_smem_bytes(ipt));
     if (e != cudaSuccess) return e;

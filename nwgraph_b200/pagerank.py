@@ -72,6 +72,18 @@ class PageRankStats:
     errors: np.ndarray | None = None
 
 
+@dataclass
+class PprBatchStats:
+    iterations: int
+    all_converged: bool
+    device_ms: float
+    ms_per_iter: float
+    bytes_per_iter: float
+    col_iterations: np.ndarray
+    col_errors: np.ndarray
+    col_converged: np.ndarray
+
+
 class Graph:
     """A CSR resident in HBM (one ``nwgpu_graph`` handle).
 
@@ -133,6 +145,78 @@ class Graph:
         N.check(N.lib().nwgpu_abort(self.handle))
 
     # ------------------------------------------------------------------
+    def _vectors(self, degrees, out, n_out):
+        if len(degrees) != self.n:
+            raise ValueError(f"degrees must have {self.n} entries")
+        dp, d_dev, keep = _ptr(degrees, np.uint32)
+        out_dev = _is_cuda_tensor(out)
+        if d_dev != out_dev:
+            raise ValueError("degrees and outputs must both be host arrays or both device tensors")
+        if out_dev:
+            if str(out.dtype) != "torch.float32" or not out.is_contiguous() or out.numel() != n_out:
+                raise TypeError(f"output must be a contiguous float32 tensor of {n_out} entries")
+            op = out.data_ptr()
+        else:
+            if not (isinstance(out, np.ndarray) and out.dtype == np.float32 and out.flags.c_contiguous
+                    and out.size == n_out):
+                raise TypeError(f"output must be a contiguous float32 numpy array of {n_out} entries (filled in place)")
+            op = out.ctypes.data
+        return dp, op, out_dev, keep
+
+    def _options(self, launch, device, stream):
+        opt = N.PrOptions(size=C.sizeof(N.PrOptions), mode=N.MODE_PARITY,
+                          launch=N.LAUNCH_STREAM if launch == "stream" else N.LAUNCH_GRAPH,
+                          device_ptrs=1 if device else 0)
+        if stream is not None:
+            opt.stream = int(getattr(stream, "cuda_stream", stream))
+        return opt
+
+    def ppr(self, degrees, seed, out, damping_factor=0.85, threshold=1e-6, max_iters=100, launch="graph",
+            record_errors=False, stream=None) -> PageRankStats:
+        """Personalised PageRank with a one-hot teleport at ``seed`` (nwgpu_ppr_run)."""
+        dp, op, dev, keep = self._vectors(degrees, out, self.n)
+        opt = self._options(launch, dev, stream)
+        st = N.PrStats()
+        errs = None
+        if record_errors:
+            cap = int(min(max(int(max_iters), 1), 4096))
+            errs = np.zeros(cap, np.float64)
+            st.errors = errs.ctypes.data_as(C.POINTER(C.c_double))
+            st.errors_cap = cap
+        N.check(N.lib().nwgpu_ppr_run(self.handle, dp, int(seed), op, C.c_float(damping_factor), C.c_float(threshold),
+                                      int(max_iters), C.byref(opt), C.byref(st)))
+        del keep
+        return PageRankStats(int(st.iterations), float(st.final_error), bool(st.converged), float(st.device_ms),
+                             float(st.ms_per_iter), float(st.bytes_per_iter), float(st.gteps),
+                             None if errs is None else errs[: min(int(st.iterations), len(errs))])
+
+    def ppr_batched(self, degrees, seeds, out, damping_factor=0.85, threshold=1e-6, max_iters=100, launch="graph",
+                    stream=None) -> PprBatchStats:
+        """k personalised vectors at once (nwgpu_ppr_batched); ``out`` is n x k row-major float32."""
+        seeds_h = np.ascontiguousarray(np.asarray(seeds.cpu() if hasattr(seeds, "cpu") else seeds), np.uint32)
+        k = len(seeds_h)
+        dp, op, dev, keep = self._vectors(degrees, out, self.n * k)
+        if dev:
+            import torch
+            seeds_arg = torch.from_numpy(seeds_h.view(np.int32)).to(out.device)
+            sp = seeds_arg.data_ptr()
+        else:
+            seeds_arg = seeds_h
+            sp = seeds_h.ctypes.data
+        opt = self._options(launch, dev, stream)
+        ci = np.zeros(k, np.uint32)
+        ce = np.zeros(k, np.float64)
+        cc = np.zeros(k, np.int32)
+        st = N.PprStats()
+        st.col_iterations = ci.ctypes.data_as(C.POINTER(C.c_uint32))
+        st.col_errors = ce.ctypes.data_as(C.POINTER(C.c_double))
+        st.col_converged = cc.ctypes.data_as(C.POINTER(C.c_int32))
+        N.check(N.lib().nwgpu_ppr_batched(self.handle, dp, sp, k, op, C.c_float(damping_factor), C.c_float(threshold),
+                                          int(max_iters), C.byref(opt), C.byref(st)))
+        del keep, seeds_arg
+        return PprBatchStats(int(st.iterations), bool(st.all_converged), float(st.device_ms), float(st.ms_per_iter),
+                             float(st.bytes_per_iter), ci, ce, cc.astype(bool))
+
     def page_rank(self, degrees, page_rank, damping_factor=0.85, threshold=1e-4, max_iters=20,
                   launch: str = "graph", record_errors: bool = False, stream=None) -> PageRankStats:
         """Solve into ``page_rank`` (fully overwritten). Returns the stats.

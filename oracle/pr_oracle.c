@@ -67,6 +67,40 @@ int64_t orc_pr_jacobi_f32(const uint32_t* row_ptr, const uint32_t* col, uint64_t
 }
 
 /*
+ * Personalised variant of the restatement above (an extension with no
+ * reference counterpart): teleport one-hot at `seed`, so base_i = (1 - d)
+ * for i == seed (computed in double, stored as float) and 0 elsewhere, and
+ * r(0) = e_seed. Everything else is page_rank_v10's sweep.
+ */
+int64_t orc_ppr_jacobi_f32(const uint32_t* row_ptr, const uint32_t* col, uint64_t n, const uint32_t* deg,
+                           uint32_t seed, float* rank, float damping, float threshold, uint64_t max_iters,
+                           double* errors) {
+  const float base = (float)(1.0 - (double)damping);
+  float*      contrib = (float*)malloc((n ? n : 1) * sizeof(float));
+  if (!contrib) return -1;
+  for (uint64_t i = 0; i < n; ++i) rank[i] = (i == seed) ? 1.0f : 0.0f;
+  uint64_t it = 0;
+  for (; it < max_iters; ++it) {
+    for (uint64_t i = 0; i < n; ++i) contrib[i] = rank[i] / (float)deg[i];
+    double err = 0.0;
+    for (uint64_t i = 0; i < n; ++i) {
+      float z = 0.0f;
+      for (uint32_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k) z += contrib[col[k]];
+      float old = rank[i];
+      rank[i] = fmaf(damping, z, (i == seed) ? base : 0.0f);
+      err += (double)fabsf(rank[i] - old);
+    }
+    if (errors) errors[it] = err;
+    if (err < (double)threshold) {
+      ++it;
+      break;
+    }
+  }
+  free(contrib);
+  return (int64_t)it;
+}
+
+/*
  * Restates nw::graph::page_rank v11 (algorithms/page_rank.hpp:89-148) run on
  * one thread: Gauss-Seidel, contrib initialised once (:114-118) and rewritten
  * in place right after each row's update (:135), so later rows of the same
