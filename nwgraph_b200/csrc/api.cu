@@ -7,6 +7,7 @@
 // include/nwgraph/experimental/algorithms/page_rank.hpp:383-431) with one
 // CUDA-graph launch whose while loop runs the sweep and finishing kernels
 // until the device-side test "error < threshold" or max_iters stops it.
+#include <cstdlib>
 #include <mutex>
 #include <new>
 
@@ -21,6 +22,13 @@ thread_local std::string g_last_error;
 std::once_flag           g_config_once;
 cudaError_t              g_config_err = cudaSuccess;
 constexpr int            kDefaultIpt = 8;
+constexpr uint32_t       kDefaultHotIds = 32768;
+
+int env_int(const char* name, int dflt) {
+  const char* v = getenv(name);
+  if (!v || !*v) return dflt;
+  return atoi(v);
+}
 }  // namespace
 
 int fail(int code, const char* fmt, ...) {
@@ -132,6 +140,7 @@ SweepArgs make_sweep_args(nwgpu_graph* g, float damping, float base, int telepor
   a.base = base;
   a.teleport = teleport;
   a.seed = seed;
+  a.hot_ids = g->hot_ids;
   return a;
 }
 
@@ -400,10 +409,20 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
     g->g.col = in.col;
     g->g.w = in.w;
   }
-  const int ipt = kDefaultIpt;
+  // Launch shape (defaults; NWGPU_IPT / NWGPU_HOT_IDS / NWGPU_CTAS_PER_SM /
+  // NWGPU_CARVEOUT override them for tuning runs).
+  int ipt = env_int("NWGPU_IPT", kDefaultIpt);
+  if (!ipt_supported(ipt)) ipt = kDefaultIpt;
+  const long hot_env = env_int("NWGPU_HOT_IDS", -1);
+  g->hot_ids = hot_env >= 0 ? (uint32_t)hot_env : (g->relabelled ? kDefaultHotIds : 0xffffffffu);
+  const int carve = env_int("NWGPU_CARVEOUT", -1);
+  if (carve >= 0) set_sweep_carveout(ipt, carve);
   if ((e = build_tiling(g->g.row_ptr, n, nnz, ipt, &g->tiling, g->stream)) != cudaSuccess)
     return bail(cuda_fail(e, "build_tiling"));
-  const uint64_t want = (uint64_t)sms * sweep_blocks_per_sm(ipt);
+  int per_sm = sweep_blocks_per_sm(ipt);
+  const int cap = env_int("NWGPU_CTAS_PER_SM", 0);
+  if (cap > 0 && cap < per_sm) per_sm = cap;
+  const uint64_t want = (uint64_t)sms * per_sm;
   g->grid = (int)(want < g->tiling.num_tiles ? want : (g->tiling.num_tiles ? g->tiling.num_tiles : 1));
   g->finish_grid = finish_grid_for(g->tiling.num_tiles);
   if ((e = cudaStreamSynchronize(g->stream)) != cudaSuccess) return bail(cuda_fail(e, "graph create"));

@@ -26,6 +26,12 @@ __device__ __forceinline__ float ld_gather(const float* p, uint64_t pol) {
   asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
   return v;
 }
+// Cold gather: L2 evict-last, but no L1 allocation, so L1 keeps hot lines.
+__device__ __forceinline__ float ld_gather_cold(const float* p, uint64_t pol) {
+  float v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+  return v;
+}
 __device__ __forceinline__ float4 ld_gather4(const float4* p, uint64_t pol) {
   float4 v;
   asm volatile("ld.global.nc.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"

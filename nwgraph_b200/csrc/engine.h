@@ -75,6 +75,7 @@ struct SweepArgs {
   float                        base;       // uniform teleport term (1 - d) / n
   int                          teleport;   // TeleportMode
   uint32_t                     seed;       // internal id of the one-hot teleport vertex
+  uint32_t                     hot_ids;    // gathers of ids below this are cached in L1
 };
 
 // graph_build.cu
@@ -94,6 +95,7 @@ cudaError_t launch_pr_finish(const SweepArgs& a, int grid, cudaStream_t s);
 cudaError_t add_pr_sweep_nodes(cudaGraph_t body, const SweepArgs& a, int ipt, int sweep_grid, int finish_grid);
 cudaError_t add_pr_arm_node(cudaGraph_t g, PrState* st, cudaGraphNode_t* node);
 cudaError_t configure_sweep_kernels();
+cudaError_t set_sweep_carveout(int ipt, int percent);
 size_t      sweep_smem_bytes(int ipt);
 int         sweep_blocks_per_sm(int ipt);
 bool        ipt_supported(int ipt);

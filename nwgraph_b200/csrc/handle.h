@@ -59,6 +59,7 @@ struct nwgpu_graph {
   nwgpu::Relabelled g;  // device CSR (relabelled, or the input order with perm/inv null)
   nwgpu::Tiling tiling{};
   int          grid = 0;         // persistent sweep CTAs
+  uint32_t     hot_ids = 0;      // internal ids below this are gathered through L1
   int          finish_grid = 1;  // finishing-kernel CTAs
   uint64_t     device_bytes = 0;
 

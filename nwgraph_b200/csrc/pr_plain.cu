@@ -144,7 +144,7 @@ __device__ __forceinline__ void issue_tile(const SweepArgs& a, uint32_t t, uint3
 // as 16-byte words from the aligned stage and shifted by col_at (uniform).
 template <int NT, int IPT>
 __device__ __forceinline__ void gather_tile(const uint32_t* stg, const TileMeta& m, const float* __restrict__ cin,
-                                            float (&v)[IPT], uint64_t pol) {
+                                            float (&v)[IPT], uint64_t pol, uint32_t hot) {
   static_assert(IPT % 4 == 0, "IPT must be a multiple of 4");
   const int  E = (int)(m.k1 - m.k0);
   const int  e0 = (int)threadIdx.x * IPT;
@@ -177,8 +177,15 @@ __device__ __forceinline__ void gather_tile(const uint32_t* stg, const TileMeta&
       for (int u = 0; u < IPT; ++u) idx[u] = w[u + 3];
       break;
   }
+  // Vertices below hot_ids (the highest out-degrees after relabelling) are
+  // read through L1; the rest bypass L1 allocation so they cannot evict them.
+  const uint32_t H = hot;
 #pragma unroll
-  for (int u = 0; u < IPT; ++u) v[u] = (e0 + u < E) ? ld_gather(cin + idx[u], pol) : 0.f;
+  for (int u = 0; u < IPT; ++u) {
+    float x = 0.f;
+    if (e0 + u < E) x = (idx[u] < H) ? ld_gather(cin + idx[u], pol) : ld_gather_cold(cin + idx[u], pol);
+    v[u] = x;
+  }
 }
 
 // Reduce the tile in stage s from the gathered values v; returns this thread's
@@ -246,30 +253,26 @@ __device__ __forceinline__ double reduce_tile(const SweepArgs& a, SweepSmem<NT, 
     S.wsum[warp] = sv;
   }
   __syncthreads();
-  float inc = sv;  // inclusive over the whole block
-  {
-    int w0 = warp;
-    while (w0 > 0 && S.wkey[w0 - 1] == key) --w0;
-    if (w0 < warp) {
-      float pre = S.wsum[w0];
-      for (int w = w0 + 1; w < warp; ++w) pre += S.wsum[w];
-      inc = pre + sv;
-    }
+  // Every warp scans the NW warp totals itself (segmented, shuffles only):
+  // wk/wi at lane w = key and block-inclusive carry of warp w's last thread.
+  constexpr int NW = SweepSmem<NT, IPT>::NW;
+  uint32_t      wk = (lane < NW) ? S.wkey[lane] : 0xfffffffdu;
+  float         wi = (lane < NW) ? S.wsum[lane] : 0.f;
+#pragma unroll
+  for (int off = 1; off < NW; off <<= 1) {
+    const uint32_t k2 = __shfl_up_sync(kFullMask, wk, off);
+    const float    v2 = __shfl_up_sync(kFullMask, wi, off);
+    if (lane >= off && lane < NW && k2 == wk) wi = v2 + wi;
   }
-  uint32_t pkey = __shfl_up_sync(kFullMask, key, 1);
-  float    pinc = __shfl_up_sync(kFullMask, inc, 1);
+  // carry into this warp from earlier warps, for threads whose key continues it
+  const uint32_t prev_wk = __shfl_sync(kFullMask, wk, warp > 0 ? warp - 1 : 0);
+  const float    prev_wi = __shfl_sync(kFullMask, wi, warp > 0 ? warp - 1 : 0);
+  const float    inc = (warp > 0 && prev_wk == key) ? prev_wi + sv : sv;  // inclusive over the block
+  uint32_t       pkey = __shfl_up_sync(kFullMask, key, 1);
+  float          pinc = __shfl_up_sync(kFullMask, inc, 1);
   if (lane == 0) {
-    if (warp == 0) {
-      pkey = 0xfffffffeu;
-      pinc = 0.f;
-    } else {  // the previous warp's last thread, recomputed from the warp totals
-      pkey = S.wkey[warp - 1];
-      int w0 = warp - 1;
-      while (w0 > 0 && S.wkey[w0 - 1] == pkey) --w0;
-      float p = S.wsum[w0];
-      for (int w = w0 + 1; w <= warp - 1; ++w) p += S.wsum[w];
-      pinc = p;
-    }
+    pkey = (warp > 0) ? prev_wk : 0xfffffffeu;
+    pinc = (warp > 0) ? prev_wi : 0.f;
   }
   if (first >= 0 && pkey == (uint32_t)first) S.z[first] = pinc + S.z[first];
   __syncthreads();
@@ -342,7 +345,7 @@ __global__ void __launch_bounds__(NT, 4) pr_sweep_kernel(const SweepArgs a) {
     }
     float v0[IPT], v1[IPT];
     ok = mbar_wait(&S.bar[0], 0u);
-    if (ok) gather_tile<NT, IPT>(S.stage[0], S.meta[0], cin, v0, pol_keep);
+    if (ok) gather_tile<NT, IPT>(S.stage[0], S.meta[0], cin, v0, pol_keep, a.hot_ids);
     ok = __syncthreads_and(ok);
     // two tiles per trip so the register sets alternate without copies
     for (int i = 0; ok && t < T; i += 2) {
@@ -350,7 +353,7 @@ __global__ void __launch_bounds__(NT, 4) pr_sweep_kernel(const SweepArgs a) {
       uint32_t tn = t + G;
       if (tn < T) {
         ok = mbar_wait(&S.bar[1], (uint32_t)(i >> 1) & 1u);
-        if (ok) gather_tile<NT, IPT>(S.stage[1], S.meta[1], cin, v1, pol_keep);
+        if (ok) gather_tile<NT, IPT>(S.stage[1], S.meta[1], cin, v1, pol_keep, a.hot_ids);
       }
       res += reduce_tile<NT, IPT>(a, S, 0, t, v0, cout, pol_keep);
       ok = __syncthreads_and(ok);
@@ -362,7 +365,7 @@ __global__ void __launch_bounds__(NT, 4) pr_sweep_kernel(const SweepArgs a) {
       tn = t + G;
       if (tn < T) {
         ok = mbar_wait(&S.bar[0], (uint32_t)((i >> 1) + 1) & 1u);
-        if (ok) gather_tile<NT, IPT>(S.stage[0], S.meta[0], cin, v0, pol_keep);
+        if (ok) gather_tile<NT, IPT>(S.stage[0], S.meta[0], cin, v0, pol_keep, a.hot_ids);
       }
       res += reduce_tile<NT, IPT>(a, S, 1, t, v1, cout, pol_keep);
       ok = __syncthreads_and(ok);
@@ -571,6 +574,12 @@ cudaError_t configure_sweep_kernels() {
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
+}
+
+cudaError_t set_sweep_carveout(int ipt, int percent) {
+  void* fn = sweep_fn_for(ipt);
+  if (!fn) return cudaErrorInvalidValue;
+  return cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, percent);
 }
 
 int sweep_blocks_per_sm(int ipt) {
