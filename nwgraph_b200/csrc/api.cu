@@ -122,7 +122,7 @@ SweepArgs make_sweep_args(nwgpu_graph* g, float damping, float base, int telepor
   a.tile_row = g->tiling.tile_row;
   a.tile_nnz = g->tiling.tile_nnz;
   a.num_tiles = g->tiling.num_tiles;
-  a.tile_items = (uint32_t)(kSweepThreads * g->tiling.items_per_thread);
+  a.tile_items = g->tiling.tile_items;
   a.contrib0 = g->contrib[0];
   a.contrib1 = g->contrib[1];
   a.rank = g->rank;
@@ -169,7 +169,7 @@ int build_loop_graph(nwgpu_graph* g, const SweepArgs& proto) {
   SweepArgs   a = proto;
   a.cond = cond;
   a.use_cond = 1;
-  CK(add_pr_sweep_nodes(body, a, g->tiling.items_per_thread, g->grid, g->finish_grid), "cudaGraphAddKernelNode(sweep)");
+  CK(add_pr_sweep_nodes(body, a, g->variant, g->grid, g->finish_grid), "cudaGraphAddKernelNode(sweep)");
   CK(cudaGraphInstantiate(&g->cg_exec, g->cg, 0), "cudaGraphInstantiate");
   g->cg_args = proto;
   return NWGPU_OK;
@@ -200,7 +200,7 @@ int run_sweeps(nwgpu_graph* g, const SweepArgs& a, uint32_t launch, uint64_t max
     for (;;) {
       const uint64_t batch = (max_iters - launched) < kGraphChunk ? (max_iters - launched) : kGraphChunk;
       for (uint64_t b = 0; b < batch; ++b) {
-        CK(launch_pr_sweep(a, g->tiling.items_per_thread, g->grid, s), "pr_sweep");
+        CK(launch_pr_sweep(a, g->variant, g->grid, s), "pr_sweep");
         CK(launch_pr_finish(a, g->finish_grid, s), "pr_finish");
       }
       launched += batch;
@@ -409,17 +409,35 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
     g->g.col = in.col;
     g->g.w = in.w;
   }
-  // Launch shape (defaults; NWGPU_IPT / NWGPU_HOT_IDS / NWGPU_CTAS_PER_SM /
-  // NWGPU_CARVEOUT override them for tuning runs).
-  int ipt = env_int("NWGPU_IPT", kDefaultIpt);
-  if (!ipt_supported(ipt)) ipt = kDefaultIpt;
+  // Launch shape. Default: relabelled graphs of 64K+ vertices use one
+  // 1024-thread CTA per SM holding the hottest ids in shared memory; others
+  // use 256-thread CTAs. NWGPU_SWEEP (base|hot|hot512|hot1024x8), NWGPU_IPT,
+  // NWGPU_HOT_IDS, NWGPU_CTAS_PER_SM and NWGPU_CARVEOUT override for tuning.
+  SweepVariant v{256, kDefaultIpt, false};
+  const char*  which = getenv("NWGPU_SWEEP");
+  const bool   want_hot = which ? (strncmp(which, "hot", 3) == 0) : (g->relabelled && n >= 65536);
+  if (want_hot) {
+    v = SweepVariant{1024, 4, true};
+    if (which && !strcmp(which, "hot512")) v = SweepVariant{512, 8, true};
+    if (which && !strcmp(which, "hot1024x8")) v = SweepVariant{1024, 8, true};
+  } else {
+    v.ipt = env_int("NWGPU_IPT", kDefaultIpt);
+    if (!sweep_variant_supported(v)) v.ipt = kDefaultIpt;
+  }
+  g->variant = v;
   const long hot_env = env_int("NWGPU_HOT_IDS", -1);
-  g->hot_ids = hot_env >= 0 ? (uint32_t)hot_env : (g->relabelled ? kDefaultHotIds : 0xffffffffu);
+  if (v.hot_smem) {
+    uint32_t cap = sweep_hot_capacity(v);
+    if (hot_env >= 0 && (uint32_t)hot_env < cap) cap = (uint32_t)hot_env;
+    g->hot_ids = (uint32_t)(n < cap ? n : cap) & ~3u;
+  } else {
+    g->hot_ids = hot_env >= 0 ? (uint32_t)hot_env : (g->relabelled ? kDefaultHotIds : 0xffffffffu);
+  }
   const int carve = env_int("NWGPU_CARVEOUT", -1);
-  if (carve >= 0) set_sweep_carveout(ipt, carve);
-  if ((e = build_tiling(g->g.row_ptr, n, nnz, ipt, &g->tiling, g->stream)) != cudaSuccess)
+  if (carve >= 0) set_sweep_carveout(v, carve);
+  if ((e = build_tiling(g->g.row_ptr, n, nnz, v.tile_items(), &g->tiling, g->stream)) != cudaSuccess)
     return bail(cuda_fail(e, "build_tiling"));
-  int per_sm = sweep_blocks_per_sm(ipt);
+  int per_sm = sweep_blocks_per_sm(v, g->hot_ids);
   const int cap = env_int("NWGPU_CTAS_PER_SM", 0);
   if (cap > 0 && cap < per_sm) per_sm = cap;
   const uint64_t want = (uint64_t)sms * per_sm;
@@ -444,7 +462,7 @@ int nwgpu_graph_get_info(const nwgpu_graph* g, nwgpu_graph_info* info) {
   info->n = g->n;
   info->nnz = g->nnz;
   info->num_tiles = g->tiling.num_tiles;
-  info->tile_items = (uint32_t)(kSweepThreads * g->tiling.items_per_thread);
+  info->tile_items = g->tiling.tile_items;
   info->grid = (uint32_t)g->grid;
   info->device_bytes = g->device_bytes;
   info->device = g->device;

@@ -23,7 +23,7 @@ static int ensure_ppr(nwgpu_graph* g, int K) {
   if (b.K == K) return NWGPU_OK;
   b.release();
   const uint64_t n = g->n, nk = g->n * (uint64_t)K;
-  CK(build_tiling(g->g.row_ptr, n, g->nnz, kPprTileItems / kSweepThreads, &b.tiling, g->stream), "ppr tiling");
+  CK(build_tiling(g->g.row_ptr, n, g->nnz, (uint32_t)kPprTileItems, &b.tiling, g->stream), "ppr tiling");
   const uint64_t T = b.tiling.num_tiles;
   b.sweep_grid = ppr_sweep_grid(K, g->sms);
   b.finish_grid = g->sms * 4;

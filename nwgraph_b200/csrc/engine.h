@@ -29,7 +29,7 @@ struct PrState {
 };
 
 struct Tiling {
-  int       items_per_thread = 0;  // IPT; a tile holds kSweepThreads * IPT rows + entries
+  uint32_t  tile_items = 0;        // D: rows + entries per tile
   uint32_t  num_tiles = 0;
   uint32_t* tile_row = nullptr;    // num_tiles + 1 merge-path row coordinates
   uint32_t* tile_nnz = nullptr;    // num_tiles + 1 merge-path entry coordinates
@@ -81,7 +81,7 @@ struct SweepArgs {
 // graph_build.cu
 cudaError_t validate_csr(const uint32_t* d_row_ptr, const uint32_t* d_col, uint64_t n, uint64_t nnz,
                          unsigned int* d_err, int sms, cudaStream_t s);
-cudaError_t build_tiling(const uint32_t* d_row_ptr, uint64_t n, uint64_t nnz, int ipt, Tiling* t, cudaStream_t s);
+cudaError_t build_tiling(const uint32_t* d_row_ptr, uint64_t n, uint64_t nnz, uint32_t D, Tiling* t, cudaStream_t s);
 cudaError_t build_relabelled(const uint32_t* d_row_ptr, const uint32_t* d_col, const float* d_w, uint64_t n,
                              uint64_t nnz, int sms, Relabelled* out, cudaStream_t s);
 
@@ -90,15 +90,25 @@ cudaError_t launch_gather_u32(const uint32_t* src, const uint32_t* idx, uint32_t
                               cudaStream_t s);
 cudaError_t launch_gather_f32(const float* src, const uint32_t* idx, float* dst, uint64_t n, int sms, cudaStream_t s);
 cudaError_t launch_pr_init(const SweepArgs& a, uint64_t n, float init, int sms, cudaStream_t s);
-cudaError_t launch_pr_sweep(const SweepArgs& a, int ipt, int grid, cudaStream_t s);
+// Sweep kernel variants: threads per CTA, items per thread, and whether the
+// hottest ids are kept in shared memory (one large CTA per SM) or left to L1.
+struct SweepVariant {
+  int  threads;
+  int  ipt;
+  bool hot_smem;
+  uint32_t tile_items() const { return (uint32_t)(threads * ipt); }
+};
+bool        sweep_variant_supported(const SweepVariant& v);
+cudaError_t launch_pr_sweep(const SweepArgs& a, const SweepVariant& v, int grid, cudaStream_t s);
 cudaError_t launch_pr_finish(const SweepArgs& a, int grid, cudaStream_t s);
-cudaError_t add_pr_sweep_nodes(cudaGraph_t body, const SweepArgs& a, int ipt, int sweep_grid, int finish_grid);
+cudaError_t add_pr_sweep_nodes(cudaGraph_t body, const SweepArgs& a, const SweepVariant& v, int sweep_grid,
+                               int finish_grid);
 cudaError_t add_pr_arm_node(cudaGraph_t g, PrState* st, cudaGraphNode_t* node);
 cudaError_t configure_sweep_kernels();
-cudaError_t set_sweep_carveout(int ipt, int percent);
-size_t      sweep_smem_bytes(int ipt);
-int         sweep_blocks_per_sm(int ipt);
-bool        ipt_supported(int ipt);
+cudaError_t set_sweep_carveout(const SweepVariant& v, int percent);
+size_t      sweep_smem_bytes(const SweepVariant& v, uint32_t hot_ids);
+uint32_t    sweep_hot_capacity(const SweepVariant& v);  // ids that fit in shared memory (hot_smem variants)
+int         sweep_blocks_per_sm(const SweepVariant& v, uint32_t hot_ids);
 int         finish_grid_for(uint32_t num_tiles);
 
 }  // namespace nwgpu

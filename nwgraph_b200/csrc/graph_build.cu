@@ -69,11 +69,10 @@ __global__ void tiling_kernel(const uint32_t* __restrict__ row_ptr, uint64_t n, 
   tile_nnz[t] = (uint32_t)(d - i);
 }
 
-cudaError_t build_tiling(const uint32_t* d_row_ptr, uint64_t n, uint64_t nnz, int ipt, Tiling* t, cudaStream_t s) {
-  const uint64_t D = (uint64_t)kSweepThreads * ipt;
+cudaError_t build_tiling(const uint32_t* d_row_ptr, uint64_t n, uint64_t nnz, uint32_t D, Tiling* t, cudaStream_t s) {
   const uint64_t tiles = (n + nnz + D - 1) / D;
-  if (tiles >= 0xFFFFFFF0ull) return cudaErrorInvalidValue;
-  t->items_per_thread = ipt;
+  if (tiles >= 0xFFFFFFF0ull || D == 0) return cudaErrorInvalidValue;
+  t->tile_items = D;
   t->num_tiles = (uint32_t)tiles;
   cudaError_t e = cudaMalloc(&t->tile_row, (tiles + 2) * sizeof(uint32_t));
   if (e != cudaSuccess) return e;
@@ -210,9 +209,8 @@ cudaError_t build_relabelled(const uint32_t* d_row_ptr, const uint32_t* d_col, c
   size_t b2 = tmp_bytes;
   RK(cub::DeviceScan::ExclusiveSum(tmp, b2, new_len, out->row_ptr, (int64_t)(n + 1), s));
   // entries: tile the new CSR and copy each tile's entries
-  const int ipt = 8;
-  RK(build_tiling(out->row_ptr, n, nnz, ipt, &nt, s));
-  const uint32_t D = (uint32_t)(kSweepThreads * ipt);
+  const uint32_t D = 2048;
+  RK(build_tiling(out->row_ptr, n, nnz, D, &nt, s));
   const size_t   smem = (size_t)(2 * D + 4) * sizeof(uint32_t);
   permute_entries_kernel<kSweepThreads><<<sms * 4, kSweepThreads, smem, s>>>(
       out->row_ptr, nt.tile_row, nt.tile_nnz, nt.num_tiles, out->inv, out->perm, d_row_ptr, d_col, d_w, out->col,

@@ -59,7 +59,8 @@ struct nwgpu_graph {
   nwgpu::Relabelled g;  // device CSR (relabelled, or the input order with perm/inv null)
   nwgpu::Tiling tiling{};
   int          grid = 0;         // persistent sweep CTAs
-  uint32_t     hot_ids = 0;      // internal ids below this are gathered through L1
+  uint32_t     hot_ids = 0;      // internal ids below this are gathered from shared memory / L1
+  nwgpu::SweepVariant variant{256, 8, false};
   int          finish_grid = 1;  // finishing-kernel CTAs
   uint64_t     device_bytes = 0;
 

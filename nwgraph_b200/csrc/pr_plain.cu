@@ -84,7 +84,7 @@ struct TileMeta {
 };
 
 template <int NT, int IPT>
-struct SweepSmem {
+struct alignas(16) SweepSmem {
   static constexpr int D = NT * IPT;
   static constexpr int NW = NT / 32;
   // col[k0,k1) and row_ptr[r0..r1] rounded out to 16 bytes share D + 16 words
@@ -97,7 +97,7 @@ struct SweepSmem {
   uint32_t wkey[NW];
   float    wsum[NW];
   double   red[NW];
-  uint64_t bar[2];
+  uint64_t bar[3];  // two tile stages, the hot-id cache
   TileMeta meta[2];
 };
 
@@ -142,9 +142,9 @@ __device__ __forceinline__ void issue_tile(const SweepArgs& a, uint32_t t, uint3
 // Each thread gathers the contributions of its IPT consecutive entries
 // [tid*IPT, tid*IPT + IPT) of the tile into registers. The column ids are read
 // as 16-byte words from the aligned stage and shifted by col_at (uniform).
-template <int NT, int IPT>
+template <int NT, int IPT, bool HOT>
 __device__ __forceinline__ void gather_tile(const uint32_t* stg, const TileMeta& m, const float* __restrict__ cin,
-                                            float (&v)[IPT], uint64_t pol, uint32_t hot) {
+                                            float (&v)[IPT], uint64_t pol, uint32_t hot, const float* hot_smem) {
   static_assert(IPT % 4 == 0, "IPT must be a multiple of 4");
   const int  E = (int)(m.k1 - m.k0);
   const int  e0 = (int)threadIdx.x * IPT;
@@ -177,13 +177,19 @@ __device__ __forceinline__ void gather_tile(const uint32_t* stg, const TileMeta&
       for (int u = 0; u < IPT; ++u) idx[u] = w[u + 3];
       break;
   }
-  // Vertices below hot_ids (the highest out-degrees after relabelling) are
-  // read through L1; the rest bypass L1 allocation so they cannot evict them.
+  // Vertices below `hot` (the highest out-degrees after relabelling) come from
+  // the shared-memory copy (HOT) or through L1; the rest bypass L1 allocation
+  // so they cannot evict the hot lines.
   const uint32_t H = hot;
 #pragma unroll
   for (int u = 0; u < IPT; ++u) {
     float x = 0.f;
-    if (e0 + u < E) x = (idx[u] < H) ? ld_gather(cin + idx[u], pol) : ld_gather_cold(cin + idx[u], pol);
+    if (e0 + u < E) {
+      if constexpr (HOT)
+        x = (idx[u] < H) ? hot_smem[idx[u]] : ld_gather_cold(cin + idx[u], pol);
+      else
+        x = (idx[u] < H) ? ld_gather(cin + idx[u], pol) : ld_gather_cold(cin + idx[u], pol);
+    }
     v[u] = x;
   }
 }
@@ -310,10 +316,11 @@ __device__ __forceinline__ double reduce_tile(const SweepArgs& a, SweepSmem<NT, 
   return res;
 }
 
-template <int NT, int IPT>
-__global__ void __launch_bounds__(NT, 4) pr_sweep_kernel(const SweepArgs a) {
+template <int NT, int IPT, bool HOT>
+__global__ void __launch_bounds__(NT, HOT ? 1 : 4) pr_sweep_kernel(const SweepArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   auto&          S = *reinterpret_cast<SweepSmem<NT, IPT>*>(smem_raw);
+  float*         hot_smem = reinterpret_cast<float*>(smem_raw + sizeof(SweepSmem<NT, IPT>));
   const int      tid = threadIdx.x;
   PrState*       st = a.st;
 
@@ -334,10 +341,24 @@ __global__ void __launch_bounds__(NT, 4) pr_sweep_kernel(const SweepArgs a) {
   if (tid == 0) {
     mbar_init(&S.bar[0], 1);
     mbar_init(&S.bar[1], 1);
+    mbar_init(&S.bar[2], 1);
     fence_mbar_init();
   }
   __syncthreads();
   uint32_t t = blockIdx.x;
+  if (HOT && t < T && a.hot_ids) {
+    // this sweep's contributions of ids [0, hot_ids) into shared memory
+    if (tid == 0) {
+      const uint32_t bytes = a.hot_ids * 4u;  // hot_ids is a multiple of 4 and <= 256K ids
+      mbar_arrive_expect_tx(&S.bar[2], bytes);
+      for (uint32_t off = 0; off < bytes; off += 65536u) {
+        const uint32_t chunk = (bytes - off) < 65536u ? (bytes - off) : 65536u;
+        bulk_load(reinterpret_cast<unsigned char*>(hot_smem) + off, reinterpret_cast<const unsigned char*>(cin) + off,
+                  chunk, &S.bar[2], pol_keep);
+      }
+    }
+    ok = mbar_wait(&S.bar[2], 0u);
+  }
   if (t < T) {
     if (tid == 0) {
       issue_tile<NT, IPT>(a, t, S.stage[0], &S.meta[0], &S.bar[0], pol_stream);
@@ -345,7 +366,7 @@ __global__ void __launch_bounds__(NT, 4) pr_sweep_kernel(const SweepArgs a) {
     }
     float v0[IPT], v1[IPT];
     ok = mbar_wait(&S.bar[0], 0u);
-    if (ok) gather_tile<NT, IPT>(S.stage[0], S.meta[0], cin, v0, pol_keep, a.hot_ids);
+    if (ok) gather_tile<NT, IPT, HOT>(S.stage[0], S.meta[0], cin, v0, pol_keep, a.hot_ids, hot_smem);
     ok = __syncthreads_and(ok);
     // two tiles per trip so the register sets alternate without copies
     for (int i = 0; ok && t < T; i += 2) {
@@ -353,7 +374,7 @@ __global__ void __launch_bounds__(NT, 4) pr_sweep_kernel(const SweepArgs a) {
       uint32_t tn = t + G;
       if (tn < T) {
         ok = mbar_wait(&S.bar[1], (uint32_t)(i >> 1) & 1u);
-        if (ok) gather_tile<NT, IPT>(S.stage[1], S.meta[1], cin, v1, pol_keep, a.hot_ids);
+        if (ok) gather_tile<NT, IPT, HOT>(S.stage[1], S.meta[1], cin, v1, pol_keep, a.hot_ids, hot_smem);
       }
       res += reduce_tile<NT, IPT>(a, S, 0, t, v0, cout, pol_keep);
       ok = __syncthreads_and(ok);
@@ -365,7 +386,7 @@ __global__ void __launch_bounds__(NT, 4) pr_sweep_kernel(const SweepArgs a) {
       tn = t + G;
       if (tn < T) {
         ok = mbar_wait(&S.bar[0], (uint32_t)((i >> 1) + 1) & 1u);
-        if (ok) gather_tile<NT, IPT>(S.stage[0], S.meta[0], cin, v0, pol_keep, a.hot_ids);
+        if (ok) gather_tile<NT, IPT, HOT>(S.stage[0], S.meta[0], cin, v0, pol_keep, a.hot_ids, hot_smem);
       }
       res += reduce_tile<NT, IPT>(a, S, 1, t, v1, cout, pol_keep);
       ok = __syncthreads_and(ok);
@@ -540,63 +561,88 @@ cudaError_t add_pr_arm_node(cudaGraph_t g, PrState* st, cudaGraphNode_t* node) {
 // ---------------------------------------------------------------------------
 // Dispatch over the items-per-thread variants
 // ---------------------------------------------------------------------------
-template <int IPT>
-static void* sweep_fn() {
-  return (void*)pr_sweep_kernel<kSweepThreads, IPT>;
+// Variants: (threads, IPT, hot-in-shared-memory).
+struct VariantEntry {
+  int    threads, ipt;
+  bool   hot;
+  void*  fn;
+  size_t fixed_smem;
+};
+
+template <int NT, int IPT, bool HOT>
+static VariantEntry entry() {
+  return {NT, IPT, HOT, (void*)pr_sweep_kernel<NT, IPT, HOT>, sizeof(SweepSmem<NT, IPT>)};
 }
 
-static void* sweep_fn_for(int ipt) {
-  switch (ipt) {
-    case 4: return sweep_fn<4>();
-    case 8: return sweep_fn<8>();
-    case 12: return sweep_fn<12>();
-    case 16: return sweep_fn<16>();
-    default: return nullptr;
-  }
+static const VariantEntry* find_variant(const SweepVariant& v) {
+  static const VariantEntry table[] = {entry<256, 4, false>(),  entry<256, 8, false>(),  entry<256, 12, false>(),
+                                       entry<256, 16, false>(), entry<1024, 4, true>(),  entry<512, 8, true>(),
+                                       entry<1024, 8, true>()};
+  for (const auto& e : table)
+    if (e.threads == v.threads && e.ipt == v.ipt && e.hot == v.hot_smem) return &e;
+  return nullptr;
 }
 
-size_t sweep_smem_bytes(int ipt) {
-  switch (ipt) {
-    case 4: return sweep_smem<kSweepThreads, 4>();
-    case 8: return sweep_smem<kSweepThreads, 8>();
-    case 12: return sweep_smem<kSweepThreads, 12>();
-    case 16: return sweep_smem<kSweepThreads, 16>();
-    default: return 0;
-  }
+static int max_dyn_smem() {
+  int dev = 0, bytes = 0;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&bytes, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) bytes = 232448;
+  return bytes;
 }
 
-bool ipt_supported(int ipt) { return sweep_fn_for(ipt) != nullptr; }
+bool sweep_variant_supported(const SweepVariant& v) { return find_variant(v) != nullptr; }
+
+uint32_t sweep_hot_capacity(const SweepVariant& v) {
+  const VariantEntry* e = find_variant(v);
+  if (!e || !e->hot) return 0;
+  const long spare = (long)max_dyn_smem() - (long)e->fixed_smem - 1024;
+  if (spare <= 0) return 0;
+  uint32_t ids = (uint32_t)(spare / 4);
+  ids &= ~31u;
+  return ids > 262144u ? 262144u : ids;
+}
+
+size_t sweep_smem_bytes(const SweepVariant& v, uint32_t hot_ids) {
+  const VariantEntry* e = find_variant(v);
+  if (!e) return 0;
+  return e->fixed_smem + (e->hot ? (size_t)hot_ids * 4u : 0u);
+}
 
 cudaError_t configure_sweep_kernels() {
-  for (int ipt : {4, 8, 12, 16}) {
-    cudaError_t e = cudaFuncSetAttribute(sweep_fn_for(ipt), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sweep_smem_bytes(ipt));
-    if (e != cudaSuccess) return e;
+  static const SweepVariant all[] = {{256, 4, false}, {256, 8, false}, {256, 12, false}, {256, 16, false},
+                                     {1024, 4, true}, {512, 8, true},  {1024, 8, true}};
+  const int maxb = max_dyn_smem();
+  for (const auto& v : all) {
+    const VariantEntry* e = find_variant(v);
+    cudaError_t         err = cudaFuncSetAttribute(e->fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   e->hot ? maxb : (int)e->fixed_smem);
+    if (err != cudaSuccess) return err;
   }
   return cudaSuccess;
 }
 
-cudaError_t set_sweep_carveout(int ipt, int percent) {
-  void* fn = sweep_fn_for(ipt);
-  if (!fn) return cudaErrorInvalidValue;
-  return cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, percent);
+cudaError_t set_sweep_carveout(const SweepVariant& v, int percent) {
+  const VariantEntry* e = find_variant(v);
+  if (!e) return cudaErrorInvalidValue;
+  return cudaFuncSetAttribute(e->fn, cudaFuncAttributePreferredSharedMemoryCarveout, percent);
 }
 
-int sweep_blocks_per_sm(int ipt) {
-  void* fn = sweep_fn_for(ipt);
-  int   nb = 0;
-  if (!fn || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kSweepThreads, sweep_smem_bytes(ipt)) != cudaSuccess)
+int sweep_blocks_per_sm(const SweepVariant& v, uint32_t hot_ids) {
+  const VariantEntry* e = find_variant(v);
+  int                 nb = 0;
+  if (!e ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, e->fn, e->threads, sweep_smem_bytes(v, hot_ids)) != cudaSuccess)
     return 1;
   return nb > 0 ? nb : 1;
 }
 
 int finish_grid_for(uint32_t num_tiles) { return num_tiles ? (int)((num_tiles + 255u) / 256u) : 1; }
 
-cudaError_t launch_pr_sweep(const SweepArgs& a, int ipt, int grid, cudaStream_t s) {
-  void* fn = sweep_fn_for(ipt);
-  if (!fn) return cudaErrorInvalidValue;
+cudaError_t launch_pr_sweep(const SweepArgs& a, const SweepVariant& v, int grid, cudaStream_t s) {
+  const VariantEntry* e = find_variant(v);
+  if (!e) return cudaErrorInvalidValue;
   void* args[] = {(void*)&a};
-  return cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(kSweepThreads), args, sweep_smem_bytes(ipt), s);
+  return cudaLaunchKernel(e->fn, dim3((unsigned)grid), dim3(e->threads), args, sweep_smem_bytes(v, a.hot_ids), s);
 }
 
 cudaError_t launch_pr_finish(const SweepArgs& a, int grid, cudaStream_t s) {
@@ -604,15 +650,16 @@ cudaError_t launch_pr_finish(const SweepArgs& a, int grid, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t add_pr_sweep_nodes(cudaGraph_t body, const SweepArgs& a, int ipt, int sweep_grid, int finish_grid) {
-  void* fn = sweep_fn_for(ipt);
-  if (!fn) return cudaErrorInvalidValue;
+cudaError_t add_pr_sweep_nodes(cudaGraph_t body, const SweepArgs& a, const SweepVariant& v, int sweep_grid,
+                               int finish_grid) {
+  const VariantEntry* ve = find_variant(v);
+  if (!ve) return cudaErrorInvalidValue;
   void*                args[] = {(void*)&a};
   cudaKernelNodeParams kp = {};
-  kp.func = fn;
+  kp.func = ve->fn;
   kp.gridDim = dim3((unsigned)sweep_grid);
-  kp.blockDim = dim3(kSweepThreads);
-  kp.sharedMemBytes = (unsigned)sweep_smem_bytes(ipt);
+  kp.blockDim = dim3(ve->threads);
+  kp.sharedMemBytes = (unsigned)sweep_smem_bytes(v, a.hot_ids);
   kp.kernelParams = args;
   cudaGraphNode_t sweep_node, finish_node;
   cudaError_t     e = cudaGraphAddKernelNode(&sweep_node, body, nullptr, 0, &kp);

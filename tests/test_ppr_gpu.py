@@ -40,10 +40,11 @@ def test_single_seed_matches_restatement(gpu, rmat13):
             assert st.iterations == 25
             close(out, ref)
             assert np.allclose(st.errors, errs, rtol=1e-4, atol=1e-6)
-            # threshold run: same stopping sweep
+            # threshold run: at 1e-6 the L1 change of a sweep is within a few percent of the FP32
+            # rounding noise of O(1) ranks, so the stopping sweep may differ by one at a near-tie
             st = h.ppr(deg, int(s), out, 0.85, 1e-6, 200)
             ref, it, _ = O.ppr_jacobi_f32(g.row_ptr, g.col, deg, int(s), 0.85, 1e-6, 200)
-            assert st.iterations == it and st.converged
+            assert abs(st.iterations - it) <= 1 and st.converged
             close(out, ref)
 
 
