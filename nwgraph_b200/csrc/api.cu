@@ -11,6 +11,8 @@
 #include <mutex>
 #include <new>
 
+#include <cub/device/device_scan.cuh>
+
 #include "handle.h"
 
 using namespace nwgpu;
@@ -80,7 +82,9 @@ int ensure_solve_buffers(nwgpu_graph* g) {
   CK(dalloc(g, &g->stage_u32, n), "cudaMalloc(staging)");
   CK(dalloc(g, &g->cpart, T + 1), "cudaMalloc(cpart)");
   CK(dalloc(g, &g->epart, T + 1), "cudaMalloc(epart)");
-  CK(dalloc(g, &g->res_part, (uint64_t)g->grid + (uint64_t)g->finish_grid), "cudaMalloc(res_part)");
+  const uint64_t parts = (uint64_t)g->grid + (uint64_t)g->finish_grid;
+  const uint64_t bparts = (uint64_t)g->bin_sweep_grid + (uint64_t)g->bin_finish_grid;
+  CK(dalloc(g, &g->res_part, parts > bparts ? parts : bparts), "cudaMalloc(res_part)");
   CK(dalloc(g, &g->st, 1), "cudaMalloc(state)");
   CK(dalloc(g, &g->err_hist, g->err_cap), "cudaMalloc(err_hist)");
   CK(cudaHostAlloc((void**)&g->h_st, sizeof(PrState), cudaHostAllocDefault), "cudaHostAlloc(state)");
@@ -111,9 +115,80 @@ int load_degrees(nwgpu_graph* g, const uint32_t* out_degree, bool device_ptrs, c
   return NWGPU_OK;
 }
 
+// Bins of the degree-binned sweep: rows must be in non-increasing length
+// order (relabelled graphs); otherwise the merge-path sweep is used.
+static int setup_binned(nwgpu_graph* g) {
+  const uint32_t n = (uint32_t)g->n;
+  uint32_t*      d_out = nullptr;
+  unsigned int*  d_bad = nullptr;
+  CK(cudaMalloc(&d_out, 8 * sizeof(uint32_t) + sizeof(unsigned int)), "cudaMalloc(bins)");
+  d_bad = reinterpret_cast<unsigned int*>(d_out + 8);
+  uint32_t     h_out[8];
+  unsigned int h_bad = 0;
+  cudaError_t  e = cudaMemsetAsync(d_bad, 0, sizeof(unsigned int), g->stream);
+  if (e == cudaSuccess) e = launch_bin_bounds(g->g.row_ptr, n, d_out, d_bad, g->sms, g->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h_out, d_out, sizeof(h_out), cudaMemcpyDeviceToHost, g->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h_bad, d_bad, sizeof(h_bad), cudaMemcpyDeviceToHost, g->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  cudaFree(d_out);
+  if (e != cudaSuccess) return cuda_fail(e, "bin bounds");
+  if (h_bad) return NWGPU_OK;  // lengths not sorted: stay on the merge-path sweep
+  BinnedArgs&    b = g->bin;
+  const uint32_t nlong = h_out[0];
+  b.num_long_rows = nlong;
+  static const int G[kNumBins] = {32, 16, 8, 4, 2, 1, 1};
+  uint32_t         warps = 0;
+  for (int i = 0; i < kNumBins; ++i) {
+    b.bin_row_begin[i] = h_out[i];
+    b.bin_row_end[i] = h_out[i + 1];
+    const uint64_t rows = h_out[i + 1] - h_out[i];
+    warps += (uint32_t)((rows * (uint64_t)G[i] + 31) / 32);
+    b.bin_warp_end[i] = warps;
+  }
+  // chunk table of the long rows
+  CK(dalloc(g, &g->bin_first, (uint64_t)nlong + 1), "cudaMalloc(chunk table)");
+  uint32_t num_chunks = 0;
+  if (nlong) {
+    uint32_t* cnt = nullptr;
+    void*     tmp = nullptr;
+    size_t    tmp_bytes = 0;
+    CK(cudaMalloc(&cnt, ((uint64_t)nlong + 1) * sizeof(uint32_t)), "cudaMalloc(chunk counts)");
+    e = cudaMemsetAsync(cnt + nlong, 0, sizeof(uint32_t), g->stream);
+    if (e == cudaSuccess) e = launch_chunk_count(g->g.row_ptr, nlong, cnt, g->sms, g->stream);
+    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, cnt, g->bin_first, (int64_t)nlong + 1, g->stream);
+    if (e == cudaSuccess) e = cudaMalloc(&tmp, tmp_bytes ? tmp_bytes : 1);
+    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, cnt, g->bin_first, (int64_t)nlong + 1, g->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(&num_chunks, g->bin_first + nlong, sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+    cudaFree(cnt);
+    cudaFree(tmp);
+    if (e != cudaSuccess) return cuda_fail(e, "chunk table");
+  }
+  b.num_chunks = num_chunks;
+  CK(dalloc(g, &g->bin_chunk_row, (uint64_t)num_chunks), "cudaMalloc(chunk rows)");
+  CK(dalloc(g, &g->bin_chunk_part, (uint64_t)num_chunks), "cudaMalloc(chunk partials)");
+  CK(launch_chunk_fill(g->bin_first, nlong, g->bin_chunk_row, g->sms, g->stream), "chunk fill");
+  CK(cudaStreamSynchronize(g->stream), "chunk fill");
+  b.row_first_chunk = g->bin_first;
+  b.chunk_row = g->bin_chunk_row;
+  b.chunk_part = g->bin_chunk_part;
+  g->bin_sweep_grid = binned_sweep_grid(g->sms);
+  g->bin_finish_grid = g->sms * 2;
+  g->binned = true;
+  return NWGPU_OK;
+}
+
 }  // namespace nwgpu
 
 namespace {
+
+BinnedArgs make_binned_args(nwgpu_graph* g, const SweepArgs& sw) {
+  BinnedArgs b = g->bin;
+  b.sw = sw;
+  b.sw.sweep_grid = (uint32_t)g->bin_sweep_grid;
+  return b;
+}
 
 SweepArgs make_sweep_args(nwgpu_graph* g, float damping, float base, int teleport, uint32_t seed) {
   SweepArgs a = {};
@@ -169,7 +244,10 @@ int build_loop_graph(nwgpu_graph* g, const SweepArgs& proto) {
   SweepArgs   a = proto;
   a.cond = cond;
   a.use_cond = 1;
-  CK(add_pr_sweep_nodes(body, a, g->variant, g->grid, g->finish_grid), "cudaGraphAddKernelNode(sweep)");
+  if (g->binned)
+    CK(add_binned_nodes(body, make_binned_args(g, a), g->bin_sweep_grid, g->bin_finish_grid), "cudaGraphAddKernelNode(binned)");
+  else
+    CK(add_pr_sweep_nodes(body, a, g->variant, g->grid, g->finish_grid), "cudaGraphAddKernelNode(sweep)");
   CK(cudaGraphInstantiate(&g->cg_exec, g->cg, 0), "cudaGraphInstantiate");
   g->cg_args = proto;
   return NWGPU_OK;
@@ -199,9 +277,14 @@ int run_sweeps(nwgpu_graph* g, const SweepArgs& a, uint32_t launch, uint64_t max
     uint64_t launched = 0;
     for (;;) {
       const uint64_t batch = (max_iters - launched) < kGraphChunk ? (max_iters - launched) : kGraphChunk;
+      const BinnedArgs ba = g->binned ? make_binned_args(g, a) : BinnedArgs{};
       for (uint64_t b = 0; b < batch; ++b) {
-        CK(launch_pr_sweep(a, g->variant, g->grid, s), "pr_sweep");
-        CK(launch_pr_finish(a, g->finish_grid, s), "pr_finish");
+        if (g->binned) {
+          CK(launch_binned_sweep(ba, g->bin_sweep_grid, g->bin_finish_grid, s), "pr_binned_sweep");
+        } else {
+          CK(launch_pr_sweep(a, g->variant, g->grid, s), "pr_sweep");
+          CK(launch_pr_finish(a, g->finish_grid, s), "pr_finish");
+        }
       }
       launched += batch;
       CK(cudaMemcpyAsync(g->h_st, g->st, sizeof(PrState), cudaMemcpyDeviceToHost, s), "copy state");
@@ -415,7 +498,7 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
   // NWGPU_HOT_IDS, NWGPU_CTAS_PER_SM and NWGPU_CARVEOUT override for tuning.
   SweepVariant v{256, kDefaultIpt, false};
   const char*  which = getenv("NWGPU_SWEEP");
-  const bool   want_hot = which ? (strncmp(which, "hot", 3) == 0) : (g->relabelled && n >= 65536);
+  const bool   want_hot = which && strncmp(which, "hot", 3) == 0;
   if (want_hot) {
     v = SweepVariant{1024, 4, true};
     if (which && !strcmp(which, "hot512")) v = SweepVariant{512, 8, true};
@@ -444,6 +527,11 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
   g->grid = (int)(want < g->tiling.num_tiles ? want : (g->tiling.num_tiles ? g->tiling.num_tiles : 1));
   g->finish_grid = finish_grid_for(g->tiling.num_tiles);
   if ((e = cudaStreamSynchronize(g->stream)) != cudaSuccess) return bail(cuda_fail(e, "graph create"));
+  const bool want_binned = which ? !strcmp(which, "binned") : true;
+  if (g->relabelled && want_binned) {
+    rc = setup_binned(g);
+    if (rc) return bail(rc);
+  }
   *out = g;
   return NWGPU_OK;
 }

@@ -1,0 +1,32 @@
+// Internal interface of the degree-binned sweep (pr_binned.cu).
+#pragma once
+
+#include "engine.h"
+
+namespace nwgpu {
+
+constexpr uint32_t kLongRow = 2048;  // rows longer than this are split into chunks
+constexpr uint32_t kChunk = 1024;    // entries per long-row chunk (one warp)
+constexpr int      kNumBins = 7;     // G = 32, 16, 8, 4, 2, 1, empty
+
+struct BinnedArgs {
+  SweepArgs       sw;                     // row_ptr / col / vectors / state / loop control
+  uint32_t        num_long_rows;          // rows [0, num_long_rows) are chunked
+  uint32_t        num_chunks;
+  const uint32_t* row_first_chunk;        // num_long_rows + 1
+  const uint32_t* chunk_row;              // num_chunks
+  float*          chunk_part;             // num_chunks partial sums
+  uint32_t        bin_row_begin[kNumBins];
+  uint32_t        bin_row_end[kNumBins];
+  uint32_t        bin_warp_end[kNumBins]; // cumulative warps over the bins
+};
+
+cudaError_t launch_bin_bounds(const uint32_t* row_ptr, uint32_t n, uint32_t* d_out, unsigned int* d_unsorted, int sms,
+                              cudaStream_t s);
+cudaError_t launch_chunk_count(const uint32_t* row_ptr, uint32_t nlong, uint32_t* cnt, int sms, cudaStream_t s);
+cudaError_t launch_chunk_fill(const uint32_t* first, uint32_t nlong, uint32_t* chunk_row, int sms, cudaStream_t s);
+int         binned_sweep_grid(int sms);
+cudaError_t launch_binned_sweep(const BinnedArgs& a, int sweep_grid, int finish_grid, cudaStream_t s);
+cudaError_t add_binned_nodes(cudaGraph_t body, const BinnedArgs& a, int sweep_grid, int finish_grid);
+
+}  // namespace nwgpu

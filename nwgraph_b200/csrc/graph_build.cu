@@ -1,9 +1,10 @@
 // Graph set-up on the device: validation, degree-ordered relabelling and
 // merge-path tiling of the uploaded CSR.
 //
-// Relabelling: vertices are renumbered by descending out-degree (how often a
-// vertex's contribution is gathered), stably, so the few hub vertices that
-// most gathers hit share sectors and L1 lines. Row i of the relabelled CSR is
+// Relabelling: vertices are renumbered by descending row length, stably. Rows
+// of similar length become contiguous (the binned sweep's bins need no index
+// lists) and, on symmetric graphs, the hub vertices that most gathers hit get
+// the smallest ids. Row i of the relabelled CSR is
 // row inv[i] of the input with its entries in their original order and each
 // column id mapped through perm, so every row is summed over the same terms in
 // the same order as the input row (page_rank.hpp:129-131). Ranks go back to
@@ -86,9 +87,11 @@ cudaError_t build_tiling(const uint32_t* d_row_ptr, uint64_t n, uint64_t nnz, ui
 // ---------------------------------------------------------------------------
 // Relabelling
 // ---------------------------------------------------------------------------
-__global__ void count_gathers_kernel(const uint32_t* __restrict__ col, uint64_t nnz, uint32_t* __restrict__ cnt) {
+// Sort key: row length (in-degree). For the symmetric graphs of the benchmark
+// this equals the out-degree, i.e. how often a vertex's contribution is gathered.
+__global__ void row_length_kernel(const uint32_t* __restrict__ row_ptr, uint64_t n, uint32_t* __restrict__ len) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += stride) atomicAdd(cnt + __ldcs(col + k), 1u);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) len[i] = row_ptr[i + 1] - row_ptr[i];
 }
 
 __global__ void iota_kernel(uint32_t* __restrict__ v, uint64_t n) {
@@ -191,8 +194,7 @@ cudaError_t build_relabelled(const uint32_t* d_row_ptr, const uint32_t* d_col, c
     RK(cudaMalloc(&out->w, (nnz + kPad) * sizeof(float)));
     RK(cudaMemsetAsync(out->w, 0, (nnz + kPad) * sizeof(float), s));
   }
-  RK(cudaMemsetAsync(cnt, 0, (n + 1) * sizeof(uint32_t), s));
-  count_gathers_kernel<<<grid, 256, 0, s>>>(d_col, nnz, cnt);
+  row_length_kernel<<<grid, 256, 0, s>>>(d_row_ptr, n, cnt);
   RK(cudaGetLastError());
   iota_kernel<<<grid, 256, 0, s>>>(ids, n);
   RK(cudaGetLastError());

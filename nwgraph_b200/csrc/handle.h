@@ -9,6 +9,7 @@
 #include "../../include/nwgpu.h"
 #include "engine.h"
 #include "ppr.h"
+#include "binned.h"
 
 namespace nwgpu {
 
@@ -61,6 +62,13 @@ struct nwgpu_graph {
   int          grid = 0;         // persistent sweep CTAs
   uint32_t     hot_ids = 0;      // internal ids below this are gathered from shared memory / L1
   nwgpu::SweepVariant variant{256, 8, false};
+  // Degree-binned sweep (relabelled graphs with non-increasing row lengths).
+  bool              binned = false;
+  nwgpu::BinnedArgs bin{};         // tables; the SweepArgs part is filled per solve
+  uint32_t*         bin_first = nullptr;
+  uint32_t*         bin_chunk_row = nullptr;
+  float*            bin_chunk_part = nullptr;
+  int               bin_sweep_grid = 0, bin_finish_grid = 0;
   int          finish_grid = 1;  // finishing-kernel CTAs
   uint64_t     device_bytes = 0;
 
@@ -93,7 +101,8 @@ struct nwgpu_graph {
     if (cg_exec) cudaGraphExecDestroy(cg_exec);
     if (cg) cudaGraphDestroy(cg);
     void* dev_ptrs[] = {g.row_ptr, g.col, g.w, g.perm, g.inv, tiling.tile_row, tiling.tile_nnz, rank, contrib[0],
-                        contrib[1], deg, stage_u32, cpart, epart, res_part, st, err_hist};
+                        contrib[1], deg, stage_u32, cpart, epart, res_part, st, err_hist, bin_first, bin_chunk_row,
+                        bin_chunk_part};
     for (void* p : dev_ptrs)
       if (p) cudaFree(p);
     if (h_st) cudaFreeHost(h_st);

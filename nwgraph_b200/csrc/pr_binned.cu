@@ -1,0 +1,308 @@
+// Degree-binned PageRank sweep for relabelled graphs (rows in descending
+// length order), sm_100a.
+//
+// After relabelling, rows of similar length are contiguous, so the sweep is
+// split into bins without any per-row indirection:
+//   long   len > kLongRow     : chunks of kChunk entries, one warp per chunk;
+//                               per-chunk FP32 partials summed in chunk order by
+//                               pr_binned_finish_kernel
+//   G = 32 64 < len <= kLongRow: one warp per row, lanes stride the row
+//   G = 16, 8, 4, 2, 1          : rows of (G*2, G*4] entries (G = 1: 1..4),
+//                               G lanes per row, <= 4 entries per lane
+//   empty  len = 0             : epilogue only
+// Every lane's entries are summed in a fixed order and combined by a fixed
+// xor-shuffle tree, so ranks are bit-reproducible. Column ids stream through
+// (coalesced, evict-first); contributions are gathered with up to 4 loads in
+// flight per lane, hub ids (< hot_ids) through L1, the rest with
+// L1::no_allocate. The per-row update is page_rank_v10's
+// (include/nwgraph/experimental/algorithms/page_rank.hpp:413-418) fused with
+// the next sweep's contribution (:401-405).
+#include "binned.h"
+#include "common.cuh"
+#include "engine.h"
+
+namespace nwgpu {
+
+__device__ __forceinline__ float binned_base(const BinnedArgs& a, uint32_t r) {
+  if (a.sw.teleport == kTeleportSeed) return (r == a.sw.seed) ? a.sw.base : 0.f;
+  return a.sw.base;
+}
+
+__device__ __forceinline__ float gather_one(const float* __restrict__ cin, uint32_t id, uint32_t hot, uint64_t pol) {
+  return (id < hot) ? ld_gather(cin + id, pol) : ld_gather_cold(cin + id, pol);
+}
+
+// Epilogue of one row; returns |dr| in FP64.
+__device__ __forceinline__ double binned_epilogue(const BinnedArgs& a, float* __restrict__ cout, uint32_t r, float z,
+                                                  uint64_t pol) {
+  const float nr = fmaf(a.sw.damping, z, binned_base(a, r));
+  const float old = ld_stream(a.sw.rank + r);
+  st_stream(a.sw.rank + r, nr);
+  st_keep(cout + r, nr / (float)ld_stream(a.sw.deg + r), pol);
+  return (double)fabsf(nr - old);
+}
+
+// One warp: a chunk of a long row.
+__device__ __forceinline__ void long_chunk(const BinnedArgs& a, const float* __restrict__ cin, uint32_t c, int lane,
+                                           uint64_t pol) {
+  const uint32_t row = a.chunk_row[c];
+  const uint32_t rs = a.sw.row_ptr[row], re = a.sw.row_ptr[row + 1];
+  const uint32_t k0 = rs + (c - a.row_first_chunk[row]) * kChunk;
+  const uint32_t k1 = min(re, k0 + kChunk);
+  float          acc = 0.f;
+#pragma unroll 1
+  for (uint32_t k = k0 + lane; k < k1; k += 4 * 32) {
+    uint32_t id[4];
+    float    v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t kk = k + q * 32;
+      id[q] = (kk < k1) ? ld_stream(a.sw.col + kk) : 0u;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[q] = (k + q * 32 < k1) ? gather_one(cin, id[q], a.sw.hot_ids, pol) : 0.f;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc += v[q];
+  }
+  acc = warp_sum_lane0(acc);
+  if (lane == 0) a.chunk_part[c] = acc;
+}
+
+// One warp of a G-bin: 32/G rows, G lanes each.
+template <int G>
+__device__ __forceinline__ double group_rows(const BinnedArgs& a, const float* __restrict__ cin, float* __restrict__ cout,
+                                             uint32_t row0, uint32_t row_end, int lane, uint64_t pol) {
+  const int      sub = lane & (G - 1);
+  const uint32_t row = row0 + (uint32_t)(lane / G);
+  const bool     live = row < row_end;
+  const uint32_t rs = live ? a.sw.row_ptr[row] : 0u;
+  const uint32_t re = live ? a.sw.row_ptr[row + 1] : 0u;
+  float          acc = 0.f;
+  if constexpr (G == 32) {
+#pragma unroll 1
+    for (uint32_t k = rs + sub; k < re; k += 4 * 32) {
+      uint32_t id[4];
+      float    v[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) id[q] = (k + q * 32 < re) ? ld_stream(a.sw.col + k + q * 32) : 0u;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) v[q] = (k + q * 32 < re) ? gather_one(cin, id[q], a.sw.hot_ids, pol) : 0.f;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc += v[q];
+    }
+  } else {
+    uint32_t id[4];
+    float    v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t k = rs + sub + q * G;
+      id[q] = (k < re) ? ld_stream(a.sw.col + k) : 0u;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[q] = (rs + sub + q * G < re) ? gather_one(cin, id[q], a.sw.hot_ids, pol) : 0.f;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc += v[q];
+  }
+#pragma unroll
+  for (int off = G / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(kFullMask, acc, off);
+  double res = 0.0;
+  if (live && sub == 0) res = binned_epilogue(a, cout, row, acc, pol);
+  return res;
+}
+
+// Rows without entries: one lane per row.
+__device__ __forceinline__ double empty_rows(const BinnedArgs& a, float* __restrict__ cout, uint32_t row,
+                                             uint32_t row_end, uint64_t pol) {
+  return (row < row_end) ? binned_epilogue(a, cout, row, 0.f, pol) : 0.0;
+}
+
+__global__ void __launch_bounds__(256) pr_binned_sweep_kernel(const BinnedArgs a) {
+  __shared__ double s_red[8];
+  const int         tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  PrState*          st = a.sw.st;
+  if (a.sw.use_cond && blockIdx.x == 0 && tid == 0) cudaGraphSetConditional(a.sw.cond, 0u);
+  if (*(volatile unsigned int*)&st->done) return;
+  const unsigned long long it = *(volatile unsigned long long*)&st->iter;
+  const float* __restrict__ cin = (it & 1ull) ? a.sw.contrib1 : a.sw.contrib0;
+  float* __restrict__ cout = (it & 1ull) ? a.sw.contrib0 : a.sw.contrib1;
+  const uint64_t pol = policy_evict_last();
+  double         res = 0.0;
+
+  const uint32_t nwarps = gridDim.x * 8, gwarp = blockIdx.x * 8 + warp;
+  const uint32_t units = a.num_chunks + a.bin_warp_end[kNumBins - 1];
+  for (uint32_t u = gwarp; u < units; u += nwarps) {
+    if (u < a.num_chunks) {
+      long_chunk(a, cin, u, lane, pol);
+      continue;
+    }
+    const uint32_t w = u - a.num_chunks;  // warp index in the flat bin space
+    int            b = 0;
+    while (w >= a.bin_warp_end[b]) ++b;   // uniform across the warp
+    const uint32_t wb = w - (b ? a.bin_warp_end[b - 1] : 0u);
+    const uint32_t rb = a.bin_row_begin[b], re = a.bin_row_end[b];
+    switch (b) {
+      case 0: res += group_rows<32>(a, cin, cout, rb + wb, re, lane, pol); break;
+      case 1: res += group_rows<16>(a, cin, cout, rb + wb * 2, re, lane, pol); break;
+      case 2: res += group_rows<8>(a, cin, cout, rb + wb * 4, re, lane, pol); break;
+      case 3: res += group_rows<4>(a, cin, cout, rb + wb * 8, re, lane, pol); break;
+      case 4: res += group_rows<2>(a, cin, cout, rb + wb * 16, re, lane, pol); break;
+      case 5: res += group_rows<1>(a, cin, cout, rb + wb * 32, re, lane, pol); break;
+      default: res += empty_rows(a, cout, rb + wb * 32 + lane, re, pol); break;
+    }
+  }
+  res = warp_sum_lane0(res);
+  if (lane == 0) s_red[warp] = res;
+  __syncthreads();
+  if (tid == 0) {
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) s += s_red[w];
+    a.sw.res_part[blockIdx.x] = s;
+  }
+}
+
+// Long rows: sum the chunk partials in chunk order, run the epilogue; then the
+// residual reduction and the device-side convergence test.
+__global__ void __launch_bounds__(256) pr_binned_finish_kernel(const BinnedArgs a) {
+  __shared__ double s_red[8];
+  __shared__ int    s_last;
+  PrState*          st = a.sw.st;
+  if (*(volatile unsigned int*)&st->done) return;
+  const unsigned long long it = *(volatile unsigned long long*)&st->iter;
+  float* __restrict__ cout = (it & 1ull) ? a.sw.contrib0 : a.sw.contrib1;
+  const uint64_t pol = policy_evict_last();
+  const int      tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double         res = 0.0;
+  // one warp per long row: lane-strided partial sums, fixed tree
+  for (uint32_t r = blockIdx.x * 8 + warp; r < a.num_long_rows; r += gridDim.x * 8) {
+    const uint32_t c0 = a.row_first_chunk[r], c1 = a.row_first_chunk[r + 1];
+    float          p = 0.f;
+    for (uint32_t c = c0 + lane; c < c1; c += 32) p += __ldcg(a.chunk_part + c);
+    p = warp_sum_lane0(p);
+    if (lane == 0) res += binned_epilogue(a, cout, r, p, pol);
+  }
+  res = warp_sum_lane0(res);
+  if (lane == 0) s_red[warp] = res;
+  __syncthreads();
+  if (tid == 0) {
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) s += s_red[w];
+    a.sw.res_part[a.sw.sweep_grid + blockIdx.x] = s;
+    __threadfence();
+    s_last = (atomicAdd(&st->ticket, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last || tid >= 32) return;
+  __threadfence();
+  const uint32_t parts = a.sw.sweep_grid + gridDim.x;
+  double         e = 0.0;
+  for (uint32_t u = lane; u < parts; u += 32) e += __ldcg(a.sw.res_part + u);
+  e = warp_sum_lane0(e);
+  if (lane == 0) {
+    const unsigned long long done_iters = it + 1ull;
+    st->iter = done_iters;
+    st->last_error = e;
+    if (a.sw.err_hist) a.sw.err_hist[it % a.sw.err_cap] = e;
+    const bool conv = e < st->threshold;
+    const bool abort = a.sw.abort_word && *a.sw.abort_word;
+    const bool done = conv || done_iters >= st->max_iters || abort;
+    st->converged = conv ? 1u : 0u;
+    st->aborted = (abort && !conv) ? 1u : 0u;
+    st->done = done ? 1u : 0u;
+    st->ticket = 0u;
+    __threadfence();
+    if (a.sw.use_cond && !done && done_iters < st->chunk_end) cudaGraphSetConditional(a.sw.cond, 1u);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Set-up: bin boundaries (rows are in non-increasing length order) and the
+// chunk table of the long rows.
+// ---------------------------------------------------------------------------
+// first row whose length is <= len (lengths non-increasing)
+__device__ uint32_t first_row_at_most(const uint32_t* row_ptr, uint32_t n, uint32_t len) {
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (row_ptr[mid + 1] - row_ptr[mid] <= len)
+      hi = mid;
+    else
+      lo = mid + 1;
+  }
+  return lo;
+}
+
+// out[0] = end of long rows, out[1..7] = ends of bins 0..6; flag = 1 if the
+// lengths are not non-increasing (then the binned sweep cannot be used).
+__global__ void bin_bounds_kernel(const uint32_t* __restrict__ row_ptr, uint32_t n, uint32_t* out,
+                                  unsigned int* unsorted) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const uint32_t limits[8] = {kLongRow, 64, 32, 16, 8, 4, 0, 0};
+    for (int b = 0; b < 7; ++b) out[b] = first_row_at_most(row_ptr, n, limits[b]);
+    out[7] = n;
+  }
+  unsigned int bad = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i + 1 < n; i += gridDim.x * blockDim.x)
+    if (row_ptr[i + 2] - row_ptr[i + 1] > row_ptr[i + 1] - row_ptr[i]) bad = 1;
+  if (bad) atomicOr(unsorted, 1u);
+}
+
+__global__ void chunk_count_kernel(const uint32_t* __restrict__ row_ptr, uint32_t nlong, uint32_t* __restrict__ cnt) {
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < nlong; r += gridDim.x * blockDim.x)
+    cnt[r] = (row_ptr[r + 1] - row_ptr[r] + kChunk - 1) / kChunk;
+}
+
+__global__ void chunk_fill_kernel(const uint32_t* __restrict__ first, uint32_t nlong, uint32_t* __restrict__ chunk_row) {
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < nlong; r += gridDim.x * blockDim.x)
+    for (uint32_t c = first[r]; c < first[r + 1]; ++c) chunk_row[c] = r;
+}
+
+cudaError_t launch_bin_bounds(const uint32_t* row_ptr, uint32_t n, uint32_t* d_out, unsigned int* d_unsorted, int sms,
+                              cudaStream_t s) {
+  bin_bounds_kernel<<<sms * 4, 256, 0, s>>>(row_ptr, n, d_out, d_unsorted);
+  return cudaGetLastError();
+}
+cudaError_t launch_chunk_count(const uint32_t* row_ptr, uint32_t nlong, uint32_t* cnt, int sms, cudaStream_t s) {
+  if (!nlong) return cudaSuccess;
+  chunk_count_kernel<<<sms, 256, 0, s>>>(row_ptr, nlong, cnt);
+  return cudaGetLastError();
+}
+cudaError_t launch_chunk_fill(const uint32_t* first, uint32_t nlong, uint32_t* chunk_row, int sms, cudaStream_t s) {
+  if (!nlong) return cudaSuccess;
+  chunk_fill_kernel<<<sms, 256, 0, s>>>(first, nlong, chunk_row);
+  return cudaGetLastError();
+}
+
+int binned_sweep_grid(int sms) {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pr_binned_sweep_kernel, 256, 0) != cudaSuccess || nb < 1)
+    nb = 1;
+  return sms * nb;
+}
+
+cudaError_t launch_binned_sweep(const BinnedArgs& a, int sweep_grid, int finish_grid, cudaStream_t s) {
+  pr_binned_sweep_kernel<<<sweep_grid, 256, 0, s>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  pr_binned_finish_kernel<<<finish_grid, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t add_binned_nodes(cudaGraph_t body, const BinnedArgs& a, int sweep_grid, int finish_grid) {
+  void*                args[] = {(void*)&a};
+  cudaKernelNodeParams kp = {};
+  kp.func = (void*)pr_binned_sweep_kernel;
+  kp.gridDim = dim3((unsigned)sweep_grid);
+  kp.blockDim = dim3(256);
+  kp.kernelParams = args;
+  cudaGraphNode_t sn, fn;
+  cudaError_t     e = cudaGraphAddKernelNode(&sn, body, nullptr, 0, &kp);
+  if (e != cudaSuccess) return e;
+  cudaKernelNodeParams fp = kp;
+  fp.func = (void*)pr_binned_finish_kernel;
+  fp.gridDim = dim3((unsigned)finish_grid);
+  return cudaGraphAddKernelNode(&fn, body, &sn, 1, &fp);
+}
+
+}  // namespace nwgpu

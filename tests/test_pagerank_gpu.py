@@ -257,3 +257,25 @@ def test_scale20_properties(gpu):
     assert np.allclose(st.errors, errs, rtol=ERR_RTOL, atol=ERR_ATOL)
     # leak semantics: mass is lost only through isolated/dangling vertices
     assert abs(float(r.astype(np.float64).sum()) - float(ref.astype(np.float64).sum())) < 1e-5
+
+
+@pytest.mark.parametrize("sweep", ["binned", "base", "hot", "hot512"])
+def test_sweep_variants_agree(gpu, sweep, monkeypatch):
+    """Every sweep kernel variant (degree-binned, merge-path with L1 hot ids,
+    merge-path with the hot ids in shared memory) meets the same bar."""
+    monkeypatch.setenv("NWGPU_SWEEP", sweep)
+    g = G.rmat(15, 16, 77)
+    deg = g.out_degree()
+    ref, it, errs = O.jacobi_f32(g.row_ptr, g.col, deg, 0.85, 0.0, 20)
+    r, st = solve(g.row_ptr, g.col, deg)
+    assert_close(r, ref)
+    assert np.allclose(st.errors, errs, rtol=ERR_RTOL, atol=ERR_ATOL)
+    a, _ = solve(g.row_ptr, g.col, deg)
+    assert np.array_equal(a.view(np.uint32), r.view(np.uint32))
+    # a hub spanning many tiles / chunks
+    n = 40_001
+    s = np.zeros(n - 1, np.uint32)
+    hub = G.from_edges(s, np.arange(1, n, dtype=np.uint32), n, symmetrize=True)
+    ref, _, _ = O.jacobi_f32(hub.row_ptr, hub.col, hub.out_degree(), 0.85, 0.0, 10)
+    r, _ = solve(hub.row_ptr, hub.col, hub.out_degree(), iters=10)
+    assert_parity_or_more_accurate(r, ref, hub.row_ptr, hub.col, 10)
