@@ -136,13 +136,14 @@ static int setup_binned(nwgpu_graph* g) {
   BinnedArgs&    b = g->bin;
   const uint32_t nlong = h_out[0];
   b.num_long_rows = nlong;
-  static const int G[kNumBins] = {32, 16, 8, 4, 2, 1, 1};
-  uint32_t         warps = 0;
+  // rows one warp handles in each bin (pr_binned.cu: warp_row, group_rows<G>, empty_rows)
+  static const uint32_t rows_per_warp[kNumBins] = {1, 4, 8, 16, 32, 64, 128};
+  uint32_t              warps = 0;
   for (int i = 0; i < kNumBins; ++i) {
     b.bin_row_begin[i] = h_out[i];
     b.bin_row_end[i] = h_out[i + 1];
     const uint64_t rows = h_out[i + 1] - h_out[i];
-    warps += (uint32_t)((rows * (uint64_t)G[i] + 31) / 32);
+    warps += (uint32_t)((rows + rows_per_warp[i] - 1) / rows_per_warp[i]);
     b.bin_warp_end[i] = warps;
   }
   // chunk table of the long rows

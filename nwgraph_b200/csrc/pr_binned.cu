@@ -32,14 +32,37 @@ __device__ __forceinline__ float gather_one(const float* __restrict__ cin, uint3
   return (id < hot) ? ld_gather(cin + id, pol) : ld_gather_cold(cin + id, pol);
 }
 
-// Epilogue of one row; returns |dr| in FP64.
+// Epilogue of one row with its old rank and degree already loaded; returns
+// |dr| in FP64.
+__device__ __forceinline__ double binned_update(const BinnedArgs& a, float* __restrict__ cout, uint32_t r, float z,
+                                                float old, uint32_t dg, uint64_t pol) {
+  const float nr = fmaf(a.sw.damping, z, binned_base(a, r));
+  st_stream(a.sw.rank + r, nr);
+  st_keep(cout + r, nr / (float)dg, pol);
+  return (double)fabsf(nr - old);
+}
 __device__ __forceinline__ double binned_epilogue(const BinnedArgs& a, float* __restrict__ cout, uint32_t r, float z,
                                                   uint64_t pol) {
-  const float nr = fmaf(a.sw.damping, z, binned_base(a, r));
-  const float old = ld_stream(a.sw.rank + r);
-  st_stream(a.sw.rank + r, nr);
-  st_keep(cout + r, nr / (float)ld_stream(a.sw.deg + r), pol);
-  return (double)fabsf(nr - old);
+  return binned_update(a, cout, r, z, ld_stream(a.sw.rank + r), ld_stream(a.sw.deg + r), pol);
+}
+
+// Sum of entries [k, k_end) taken U at a time, lanes `stride` apart.
+template <int U>
+__device__ __forceinline__ float strided_sum(const BinnedArgs& a, const float* __restrict__ cin, uint32_t k,
+                                             uint32_t k_end, uint32_t stride, uint64_t pol) {
+  float acc = 0.f;
+#pragma unroll 1
+  for (; k < k_end; k += U * stride) {
+    uint32_t id[U];
+    float    v[U];
+#pragma unroll
+    for (int q = 0; q < U; ++q) id[q] = (k + q * stride < k_end) ? ld_stream(a.sw.col + k + q * stride) : 0u;
+#pragma unroll
+    for (int q = 0; q < U; ++q) v[q] = (k + q * stride < k_end) ? gather_one(cin, id[q], a.sw.hot_ids, pol) : 0.f;
+#pragma unroll
+    for (int q = 0; q < U; ++q) acc += v[q];
+  }
+  return acc;
 }
 
 // One warp: a chunk of a long row.
@@ -49,74 +72,94 @@ __device__ __forceinline__ void long_chunk(const BinnedArgs& a, const float* __r
   const uint32_t rs = a.sw.row_ptr[row], re = a.sw.row_ptr[row + 1];
   const uint32_t k0 = rs + (c - a.row_first_chunk[row]) * kChunk;
   const uint32_t k1 = min(re, k0 + kChunk);
-  float          acc = 0.f;
-#pragma unroll 1
-  for (uint32_t k = k0 + lane; k < k1; k += 4 * 32) {
-    uint32_t id[4];
-    float    v[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const uint32_t kk = k + q * 32;
-      id[q] = (kk < k1) ? ld_stream(a.sw.col + kk) : 0u;
-    }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) v[q] = (k + q * 32 < k1) ? gather_one(cin, id[q], a.sw.hot_ids, pol) : 0.f;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) acc += v[q];
-  }
+  float          acc = strided_sum<8>(a, cin, k0 + lane, k1, 32u, pol);
   acc = warp_sum_lane0(acc);
   if (lane == 0) a.chunk_part[c] = acc;
 }
 
-// One warp of a G-bin: 32/G rows, G lanes each.
+// One warp, G = 32: one row of 65..kLongRow entries.
+__device__ __forceinline__ double warp_row(const BinnedArgs& a, const float* __restrict__ cin, float* __restrict__ cout,
+                                           uint32_t row, uint32_t row_end, int lane, uint64_t pol) {
+  if (row >= row_end) return 0.0;  // uniform across the warp
+  const uint32_t rs = a.sw.row_ptr[row], re = a.sw.row_ptr[row + 1];
+  float          old = 0.f;
+  uint32_t       dg = 1u;
+  if (lane == 0) {
+    old = ld_stream(a.sw.rank + row);
+    dg = ld_stream(a.sw.deg + row);
+  }
+  float acc = strided_sum<8>(a, cin, rs + lane, re, 32u, pol);
+  acc = warp_sum_lane0(acc);
+  return (lane == 0) ? binned_update(a, cout, row, acc, old, dg, pol) : 0.0;
+}
+
+// One warp of a G-bin, G < 32: 2 * 32/G rows, G lanes per row, each lane two
+// rows and at most 4 entries of each (8 gathers in flight).
 template <int G>
 __device__ __forceinline__ double group_rows(const BinnedArgs& a, const float* __restrict__ cin, float* __restrict__ cout,
                                              uint32_t row0, uint32_t row_end, int lane, uint64_t pol) {
-  const int      sub = lane & (G - 1);
-  const uint32_t row = row0 + (uint32_t)(lane / G);
-  const bool     live = row < row_end;
-  const uint32_t rs = live ? a.sw.row_ptr[row] : 0u;
-  const uint32_t re = live ? a.sw.row_ptr[row + 1] : 0u;
-  float          acc = 0.f;
-  if constexpr (G == 32) {
-#pragma unroll 1
-    for (uint32_t k = rs + sub; k < re; k += 4 * 32) {
-      uint32_t id[4];
-      float    v[4];
+  constexpr uint32_t PER = 32 / G;  // rows per half
+  const int          sub = lane & (G - 1);
+  uint32_t           row[2], rs[2], re[2];
+  float              old[2];
+  uint32_t           dg[2];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) id[q] = (k + q * 32 < re) ? ld_stream(a.sw.col + k + q * 32) : 0u;
+  for (int h = 0; h < 2; ++h) {
+    row[h] = row0 + h * PER + (uint32_t)(lane / G);
+    const bool live = row[h] < row_end;
+    rs[h] = live ? a.sw.row_ptr[row[h]] : 0u;
+    re[h] = live ? a.sw.row_ptr[row[h] + 1] : 0u;
+    old[h] = (live && sub == 0) ? ld_stream(a.sw.rank + row[h]) : 0.f;
+    dg[h] = (live && sub == 0) ? ld_stream(a.sw.deg + row[h]) : 1u;
+  }
+  uint32_t id[2][4];
+  float    v[2][4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) v[q] = (k + q * 32 < re) ? gather_one(cin, id[q], a.sw.hot_ids, pol) : 0.f;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) acc += v[q];
-    }
-  } else {
-    uint32_t id[4];
-    float    v[4];
+  for (int h = 0; h < 2; ++h)
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const uint32_t k = rs + sub + q * G;
-      id[q] = (k < re) ? ld_stream(a.sw.col + k) : 0u;
+      const uint32_t k = rs[h] + sub + q * G;
+      id[h][q] = (k < re[h]) ? ld_stream(a.sw.col + k) : 0u;
     }
 #pragma unroll
-    for (int q = 0; q < 4; ++q) v[q] = (rs + sub + q * G < re) ? gather_one(cin, id[q], a.sw.hot_ids, pol) : 0.f;
+  for (int h = 0; h < 2; ++h)
 #pragma unroll
-    for (int q = 0; q < 4; ++q) acc += v[q];
-  }
-#pragma unroll
-  for (int off = G / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(kFullMask, acc, off);
+    for (int q = 0; q < 4; ++q)
+      v[h][q] = (rs[h] + sub + q * G < re[h]) ? gather_one(cin, id[h][q], a.sw.hot_ids, pol) : 0.f;
   double res = 0.0;
-  if (live && sub == 0) res = binned_epilogue(a, cout, row, acc, pol);
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    float acc = 0.f;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc += v[h][q];
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(kFullMask, acc, off);
+    if (row[h] < row_end && sub == 0) res += binned_update(a, cout, row[h], acc, old[h], dg[h], pol);
+  }
   return res;
 }
 
-// Rows without entries: one lane per row.
-__device__ __forceinline__ double empty_rows(const BinnedArgs& a, float* __restrict__ cout, uint32_t row,
-                                             uint32_t row_end, uint64_t pol) {
-  return (row < row_end) ? binned_epilogue(a, cout, row, 0.f, pol) : 0.0;
+// Rows without entries: four rows per lane.
+__device__ __forceinline__ double empty_rows(const BinnedArgs& a, float* __restrict__ cout, uint32_t row0,
+                                             uint32_t row_end, int lane, uint64_t pol) {
+  double   res = 0.0;
+  float    old[4];
+  uint32_t dg[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const uint32_t r = row0 + q * 32 + lane;
+    old[q] = (r < row_end) ? ld_stream(a.sw.rank + r) : 0.f;
+    dg[q] = (r < row_end) ? ld_stream(a.sw.deg + r) : 1u;
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const uint32_t r = row0 + q * 32 + lane;
+    if (r < row_end) res += binned_update(a, cout, r, 0.f, old[q], dg[q], pol);
+  }
+  return res;
 }
 
-__global__ void __launch_bounds__(256) pr_binned_sweep_kernel(const BinnedArgs a) {
+__global__ void __launch_bounds__(256, 4) pr_binned_sweep_kernel(const BinnedArgs a) {
   __shared__ double s_red[8];
   const int         tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   PrState*          st = a.sw.st;
@@ -141,13 +184,13 @@ __global__ void __launch_bounds__(256) pr_binned_sweep_kernel(const BinnedArgs a
     const uint32_t wb = w - (b ? a.bin_warp_end[b - 1] : 0u);
     const uint32_t rb = a.bin_row_begin[b], re = a.bin_row_end[b];
     switch (b) {
-      case 0: res += group_rows<32>(a, cin, cout, rb + wb, re, lane, pol); break;
-      case 1: res += group_rows<16>(a, cin, cout, rb + wb * 2, re, lane, pol); break;
-      case 2: res += group_rows<8>(a, cin, cout, rb + wb * 4, re, lane, pol); break;
-      case 3: res += group_rows<4>(a, cin, cout, rb + wb * 8, re, lane, pol); break;
-      case 4: res += group_rows<2>(a, cin, cout, rb + wb * 16, re, lane, pol); break;
-      case 5: res += group_rows<1>(a, cin, cout, rb + wb * 32, re, lane, pol); break;
-      default: res += empty_rows(a, cout, rb + wb * 32 + lane, re, pol); break;
+      case 0: res += warp_row(a, cin, cout, rb + wb, re, lane, pol); break;
+      case 1: res += group_rows<16>(a, cin, cout, rb + wb * 4, re, lane, pol); break;
+      case 2: res += group_rows<8>(a, cin, cout, rb + wb * 8, re, lane, pol); break;
+      case 3: res += group_rows<4>(a, cin, cout, rb + wb * 16, re, lane, pol); break;
+      case 4: res += group_rows<2>(a, cin, cout, rb + wb * 32, re, lane, pol); break;
+      case 5: res += group_rows<1>(a, cin, cout, rb + wb * 64, re, lane, pol); break;
+      default: res += empty_rows(a, cout, rb + wb * 128, re, lane, pol); break;
     }
   }
   res = warp_sum_lane0(res);
