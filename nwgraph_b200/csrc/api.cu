@@ -7,6 +7,7 @@
 // include/nwgraph/experimental/algorithms/page_rank.hpp:383-431) with one
 // CUDA-graph launch whose while loop runs the sweep and finishing kernels
 // until the device-side test "error < threshold" or max_iters stops it.
+#include <chrono>
 #include <cstdlib>
 #include <mutex>
 #include <new>
@@ -25,6 +26,24 @@ std::once_flag           g_config_once;
 cudaError_t              g_config_err = cudaSuccess;
 constexpr int            kDefaultIpt = 8;
 constexpr uint32_t       kDefaultHotIds = 32768;
+
+// NWGPU_TRACE=1 prints "# [ phase ]: X ms" lines to stderr, like the
+// reference's life_timer (include/nwgraph/util/timer.hpp:120-133).
+struct PhaseTimer {
+  bool                                           on;
+  cudaStream_t                                   s;
+  std::chrono::high_resolution_clock::time_point t0;
+  explicit PhaseTimer(cudaStream_t st) : on(getenv("NWGPU_TRACE") != nullptr), s(st) {
+    if (on) t0 = std::chrono::high_resolution_clock::now();
+  }
+  void mark(const char* what) {
+    if (!on) return;
+    cudaStreamSynchronize(s);
+    auto t1 = std::chrono::high_resolution_clock::now();
+    fprintf(stderr, "# [ nwgpu %s ]: %.3f ms\n", what, std::chrono::duration<double, std::milli>(t1 - t0).count());
+    t0 = t1;
+  }
+};
 
 int env_int(const char* name, int dflt) {
   const char* v = getenv(name);
@@ -339,10 +358,12 @@ int solve_single(nwgpu_graph* g, const uint32_t* out_degree, float* ranks, float
     }
     return NWGPU_OK;
   }
-  int rc = ensure_solve_buffers(g);
-  if (rc) return rc;
   cudaStream_t s = opt.stream ? (cudaStream_t)opt.stream : g->stream;
+  PhaseTimer   trace(s);
+  int          rc = ensure_solve_buffers(g);
+  if (rc) return rc;
   *(volatile unsigned int*)g->h_abort = 0u;
+  trace.mark("solve buffers");
   if ((rc = load_degrees(g, out_degree, opt.device_ptrs != 0, s))) return rc;
   uint32_t seed = seed_in;
   if (teleport == kTeleportSeed && g->relabelled)
@@ -357,11 +378,13 @@ int solve_single(nwgpu_graph* g, const uint32_t* out_degree, float* ranks, float
   SweepArgs a = make_sweep_args(g, damping, base, teleport, seed);
   CK(launch_pr_init(a, n, init, g->sms, s), "pr_init");
 
+  trace.mark("degrees + init");
   CK(cudaEventRecord(g->ev0, s), "cudaEventRecord");
   PrState fin{};
   rc = run_sweeps(g, a, opt.launch, max_iters, s, &fin);
   if (rc) return rc;
   CK(cudaEventRecord(g->ev1, s), "cudaEventRecord");
+  trace.mark("sweeps");
   if (g->relabelled) {
     float* dst = opt.device_ptrs ? ranks : reinterpret_cast<float*>(g->stage_u32);
     CK(launch_gather_f32(g->rank, g->g.perm, dst, n, g->sms, s), "permute ranks");
@@ -372,6 +395,7 @@ int solve_single(nwgpu_graph* g, const uint32_t* out_degree, float* ranks, float
        "copy ranks");
   }
   CK(cudaStreamSynchronize(s), "copy ranks");
+  trace.mark("ranks out");
   if (stats) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, g->ev0, g->ev1);
@@ -438,6 +462,7 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
   cudaError_t e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) return bail(cuda_fail(e, "cudaStreamCreate"));
   const cudaMemcpyKind kind = (flags & NWGPU_GRAPH_DEVICE_PTRS) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  PhaseTimer           trace(g->stream);
   // Upload into padded buffers.
   Relabelled in;
   auto       free_in = [&]() {
@@ -461,6 +486,7 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
       return bail(cuda_fail(e, "upload weights"));
     }
   }
+  trace.mark("upload");
   // Validate on the device before any kernel indexes with these arrays.
   unsigned int* d_err = nullptr;
   unsigned int  h_err = 0;
@@ -483,6 +509,7 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
                      (h_err & 1u) ? " row_ptr[0] != 0 or row_ptr[n] != nnz;" : "",
                      (h_err & 2u) ? " row_ptr decreases;" : "", (h_err & 4u) ? " col index >= n;" : ""));
   }
+  trace.mark("validate");
   if (!(flags & NWGPU_GRAPH_NO_RELABEL) && n > 1) {
     e = build_relabelled(in.row_ptr, in.col, in.w, n, nnz, sms, &g->g, g->stream);
     free_in();
@@ -493,6 +520,7 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
     g->g.col = in.col;
     g->g.w = in.w;
   }
+  trace.mark("relabel");
   // Launch shape. Default: relabelled graphs of 64K+ vertices use one
   // 1024-thread CTA per SM holding the hottest ids in shared memory; others
   // use 256-thread CTAs. NWGPU_SWEEP (base|hot|hot512|hot1024x8), NWGPU_IPT,
@@ -528,11 +556,13 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
   g->grid = (int)(want < g->tiling.num_tiles ? want : (g->tiling.num_tiles ? g->tiling.num_tiles : 1));
   g->finish_grid = finish_grid_for(g->tiling.num_tiles);
   if ((e = cudaStreamSynchronize(g->stream)) != cudaSuccess) return bail(cuda_fail(e, "graph create"));
+  trace.mark("tiling");
   const bool want_binned = which ? !strcmp(which, "binned") : true;
   if (g->relabelled && want_binned) {
     rc = setup_binned(g);
     if (rc) return bail(rc);
   }
+  trace.mark("bins");
   *out = g;
   return NWGPU_OK;
 }
@@ -541,7 +571,9 @@ int nwgpu_graph_destroy(nwgpu_graph* g) {
   clear_error();
   if (!g) return NWGPU_OK;
   if (g->stream) cudaStreamSynchronize(g->stream);
+  PhaseTimer trace(nullptr);
   delete g;
+  trace.mark("destroy");
   return NWGPU_OK;
 }
 
