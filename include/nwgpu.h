@@ -149,6 +149,42 @@ int nwgpu_ppr_batched(nwgpu_graph* g, const uint32_t* out_degree, const uint32_t
                       float damping, float threshold, uint64_t max_iters, const nwgpu_pr_options* options,
                       nwgpu_ppr_stats* stats);
 
+/* PageRank without any allocation. No counterpart in the reference.
+ *
+ * For callers that must not allocate:
+ *  - code running under a memory manager that owns the device's memory (an
+ *    application pool, a process with a fixed memory cap), where a cudaMalloc
+ *    from a library would fail or break the owner's accounting;
+ *  - callers on a latency path, where cudaMalloc / cudaFree could synchronise
+ *    the device.
+ * The call allocates nothing on the device or the host. The caller passes the
+ * CSR, the degrees and the output, all in device memory. The engine's own
+ * working memory lives in one statically sized device array inside this
+ * library (about 8.8 MB, present on every device once the library's kernels
+ * are loaded). That array bounds the graph:
+ *   n   <= NWGPU_NOALLOC_MAX_VERTICES,  nnz <= NWGPU_NOALLOC_MAX_ENTRIES.
+ * Larger graphs, and pointers that are not 16-byte-aligned device memory, are
+ * rejected with NWGPU_ERR_INVALID_ARG and a message naming the limit.
+ *
+ * Semantics are those of nwgpu_pr_run with NWGPU_GRAPH_NO_RELABEL and
+ * NWGPU_LAUNCH_STREAM:
+ *  - the same sweep, stopping rule and stats;
+ *  - device_ms is host time around the sweep loop;
+ *  - the CSR is validated on each call.
+ * `stream` is a cudaStream_t (NULL = the default stream). The call returns
+ * when the solve has finished.
+ *
+ * The first call on a device looks up that device's copy of the array. Make
+ * that first call before any stream capture on the device. The working array
+ * is shared by every call on a device: calls whose GPU work overlaps (from two
+ * host threads, or on two streams at once) race, and both results are
+ * undefined. Serialise them. */
+#define NWGPU_NOALLOC_MAX_VERTICES 1048576u
+#define NWGPU_NOALLOC_MAX_ENTRIES 33554432u
+int nwgpu_pr_run_noalloc(const uint32_t* row_ptr, const uint32_t* col, uint64_t n, uint64_t nnz,
+                         const uint32_t* out_degree, float* ranks, float damping, float threshold, uint64_t max_iters,
+                         void* stream, nwgpu_pr_stats* stats);
+
 /* Ask a running solve on g to stop at its next sweep boundary; the solve
  * returns NWGPU_ERR_ABORTED. Safe to call from another host thread. */
 int nwgpu_abort(nwgpu_graph* g);

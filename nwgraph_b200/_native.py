@@ -24,6 +24,8 @@ ERR_UNSUPPORTED = 7
 GRAPH_DEVICE_PTRS = 0x1
 GRAPH_TRANSPOSE = 0x2
 GRAPH_NO_RELABEL = 0x4
+NOALLOC_MAX_VERTICES = 1048576
+NOALLOC_MAX_ENTRIES = 33554432
 
 MODE_PARITY = 0
 LAUNCH_GRAPH = 0
@@ -80,6 +82,8 @@ SIGNATURES = {
                                 C.POINTER(PrStats)]),
     "nwgpu_ppr_batched": (C.c_int, [_vp, _vp, _vp, C.c_uint32, _vp, C.c_float, C.c_float, C.c_uint64,
                                     C.POINTER(PrOptions), C.POINTER(PprStats)]),
+    "nwgpu_pr_run_noalloc": (C.c_int, [_vp, _vp, C.c_uint64, C.c_uint64, _vp, _vp, C.c_float, C.c_float,
+                                       C.c_uint64, _vp, C.POINTER(PrStats)]),
     "nwgpu_abort": (C.c_int, [_vp]),
 }
 

@@ -72,7 +72,7 @@ void clear_error() { g_last_error.clear(); }
 
 const std::string& last_error_text() { return g_last_error; }
 
-static int check_device(int* dev_out, int* sms_out) {
+int check_device(int* dev_out, int* sms_out) {
   int         dev = 0, count = 0;
   cudaError_t e = cudaGetDeviceCount(&count);
   if (e != cudaSuccess || count == 0) {

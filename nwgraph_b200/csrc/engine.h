@@ -82,6 +82,9 @@ struct SweepArgs {
 cudaError_t validate_csr(const uint32_t* d_row_ptr, const uint32_t* d_col, uint64_t n, uint64_t nnz,
                          unsigned int* d_err, int sms, cudaStream_t s);
 cudaError_t build_tiling(const uint32_t* d_row_ptr, uint64_t n, uint64_t nnz, uint32_t D, Tiling* t, cudaStream_t s);
+// Merge-path coordinates into caller-owned tile_row / tile_nnz (num_tiles + 1 each).
+cudaError_t fill_tiling(const uint32_t* d_row_ptr, uint64_t n, uint64_t nnz, uint32_t D, uint32_t num_tiles,
+                        uint32_t* tile_row, uint32_t* tile_nnz, cudaStream_t s);
 cudaError_t build_relabelled(const uint32_t* d_row_ptr, const uint32_t* d_col, const float* d_w, uint64_t n,
                              uint64_t nnz, int sms, Relabelled* out, cudaStream_t s);
 

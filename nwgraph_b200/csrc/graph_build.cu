@@ -84,6 +84,14 @@ cudaError_t build_tiling(const uint32_t* d_row_ptr, uint64_t n, uint64_t nnz, ui
   return cudaGetLastError();
 }
 
+cudaError_t fill_tiling(const uint32_t* d_row_ptr, uint64_t n, uint64_t nnz, uint32_t D, uint32_t num_tiles,
+                        uint32_t* tile_row, uint32_t* tile_nnz, cudaStream_t s) {
+  if (D == 0 || (uint64_t)num_tiles * D < n + nnz) return cudaErrorInvalidValue;
+  const unsigned blocks = (unsigned)(((uint64_t)num_tiles + 1 + 255) / 256);
+  tiling_kernel<<<blocks, 256, 0, s>>>(d_row_ptr, n, nnz, D, num_tiles, tile_row, tile_nnz);
+  return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 // Relabelling
 // ---------------------------------------------------------------------------

@@ -17,6 +17,9 @@ int  fail(int code, const char* fmt, ...);
 int  cuda_fail(cudaError_t e, const char* what);
 void clear_error();
 const std::string& last_error_text();
+// Current device (must be compute capability 10.x) and its SM count; configures
+// the sweep kernels once per process.
+int  check_device(int* dev_out, int* sms_out);
 
 #define CK(call, what)                                         \
   do {                                                         \
