@@ -27,6 +27,10 @@
  *    computes it (bench/gapbs/common.hpp:110-121).
  *  - A handle owns one CUDA stream; calls on one handle are serialised by the
  *    caller, calls on distinct handles may run concurrently.
+ *  - Device memory of handles comes from one stream-ordered pool per device
+ *    that keeps freed blocks mapped: creating and destroying handles again
+ *    and again does not map and unmap pages each time.
+ *    nwgpu_release_cached_memory() returns the unused blocks to the driver.
  *  - There is no CPU fallback: without a usable sm_100 device every call that
  *    needs one returns NWGPU_ERR_CUDA / NWGPU_ERR_NO_DEVICE.
  */
@@ -188,6 +192,10 @@ int nwgpu_pr_run_noalloc(const uint32_t* row_ptr, const uint32_t* col, uint64_t 
 /* Ask a running solve on g to stop at its next sweep boundary; the solve
  * returns NWGPU_ERR_ABORTED. Safe to call from another host thread. */
 int nwgpu_abort(nwgpu_graph* g);
+
+/* Return the device memory that destroyed handles left in the pool to the
+ * driver (all devices). Handles still alive keep theirs. */
+int nwgpu_release_cached_memory(void);
 
 /* Thread-local message for the last failing call (empty if none). Returns
  * the message length. */

@@ -140,7 +140,7 @@ static int setup_binned(nwgpu_graph* g) {
   const uint32_t n = (uint32_t)g->n;
   uint32_t*      d_out = nullptr;
   unsigned int*  d_bad = nullptr;
-  CK(cudaMalloc(&d_out, 8 * sizeof(uint32_t) + sizeof(unsigned int)), "cudaMalloc(bins)");
+  CK(pool_alloc((void**)&d_out, 8 * sizeof(uint32_t) + sizeof(unsigned int), g->stream), "cudaMalloc(bins)");
   d_bad = reinterpret_cast<unsigned int*>(d_out + 8);
   uint32_t     h_out[8];
   unsigned int h_bad = 0;
@@ -149,7 +149,7 @@ static int setup_binned(nwgpu_graph* g) {
   if (e == cudaSuccess) e = cudaMemcpyAsync(h_out, d_out, sizeof(h_out), cudaMemcpyDeviceToHost, g->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(&h_bad, d_bad, sizeof(h_bad), cudaMemcpyDeviceToHost, g->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
-  cudaFree(d_out);
+  pool_free(d_out, g->stream);
   if (e != cudaSuccess) return cuda_fail(e, "bin bounds");
   if (h_bad) return NWGPU_OK;  // lengths not sorted: stay on the merge-path sweep
   BinnedArgs&    b = g->bin;
@@ -172,17 +172,17 @@ static int setup_binned(nwgpu_graph* g) {
     uint32_t* cnt = nullptr;
     void*     tmp = nullptr;
     size_t    tmp_bytes = 0;
-    CK(cudaMalloc(&cnt, ((uint64_t)nlong + 1) * sizeof(uint32_t)), "cudaMalloc(chunk counts)");
+    CK(pool_alloc_n(&cnt, (uint64_t)nlong + 1, g->stream), "cudaMalloc(chunk counts)");
     e = cudaMemsetAsync(cnt + nlong, 0, sizeof(uint32_t), g->stream);
     if (e == cudaSuccess) e = launch_chunk_count(g->g.row_ptr, nlong, cnt, g->sms, g->stream);
     if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, cnt, g->bin_first, (int64_t)nlong + 1, g->stream);
-    if (e == cudaSuccess) e = cudaMalloc(&tmp, tmp_bytes ? tmp_bytes : 1);
+    if (e == cudaSuccess) e = pool_alloc(&tmp, tmp_bytes, g->stream);
     if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, cnt, g->bin_first, (int64_t)nlong + 1, g->stream);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(&num_chunks, g->bin_first + nlong, sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
-    cudaFree(cnt);
-    cudaFree(tmp);
+    pool_free(cnt, g->stream);
+    pool_free(tmp, g->stream);
     if (e != cudaSuccess) return cuda_fail(e, "chunk table");
   }
   b.num_chunks = num_chunks;
@@ -466,9 +466,9 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
   // Upload into padded buffers.
   Relabelled in;
   auto       free_in = [&]() {
-    cudaFree(in.row_ptr);
-    cudaFree(in.col);
-    cudaFree(in.w);
+    pool_free(in.row_ptr, g->stream);
+    pool_free(in.col, g->stream);
+    pool_free(in.w, g->stream);
   };
   if ((e = dalloc(g, &in.row_ptr, n + 1)) != cudaSuccess || (e = dalloc(g, &in.col, nnz)) != cudaSuccess) {
     free_in();
@@ -490,7 +490,7 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
   // Validate on the device before any kernel indexes with these arrays.
   unsigned int* d_err = nullptr;
   unsigned int  h_err = 0;
-  if ((e = cudaMalloc(&d_err, sizeof(unsigned int))) != cudaSuccess) {
+  if ((e = pool_alloc_n(&d_err, 1, g->stream)) != cudaSuccess) {
     free_in();
     return bail(cuda_fail(e, "cudaMalloc(err)"));
   }
@@ -498,7 +498,7 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
   e = validate_csr(in.row_ptr, in.col, n, nnz, d_err, sms, g->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(&h_err, d_err, sizeof(unsigned int), cudaMemcpyDeviceToHost, g->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
-  cudaFree(d_err);
+  pool_free(d_err, g->stream);
   if (e != cudaSuccess) {
     free_in();
     return bail(cuda_fail(e, "validate"));

@@ -5,15 +5,14 @@
 
 namespace nwgpu {
 
-void PprBuffers::release() {
+void PprBuffers::release(cudaStream_t s) {
   if (cg_exec) cudaGraphExecDestroy(cg_exec);
   if (cg) cudaGraphDestroy(cg);
   cg_exec = nullptr;
   cg = nullptr;
   void* ptrs[] = {tiling.tile_row, tiling.tile_nnz, rank, contrib[0], contrib[1], out, cpart, epart, res_part,
                   seeds, seeds_in, col_done, col_conv, col_iters, col_err, st};
-  for (void* p : ptrs)
-    if (p) cudaFree(p);
+  for (void* p : ptrs) pool_free(p, s);
   if (h_st) cudaFreeHost(h_st);
   *this = PprBuffers();
 }
@@ -21,7 +20,7 @@ void PprBuffers::release() {
 static int ensure_ppr(nwgpu_graph* g, int K) {
   PprBuffers& b = g->ppr;
   if (b.K == K) return NWGPU_OK;
-  b.release();
+  b.release(g->stream);
   const uint64_t n = g->n, nk = g->n * (uint64_t)K;
   CK(build_tiling(g->g.row_ptr, n, g->nnz, (uint32_t)kPprTileItems, &b.tiling, g->stream), "ppr tiling");
   const uint64_t T = b.tiling.num_tiles;

@@ -78,6 +78,14 @@ struct SweepArgs {
   uint32_t                     hot_ids;    // gathers of ids below this are cached in L1
 };
 
+// devmem.cu: the per-device stream-ordered pool that every handle allocation uses
+cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t s);
+void        pool_free(void* p, cudaStream_t s);
+template <class T>
+cudaError_t pool_alloc_n(T** p, uint64_t count, cudaStream_t s) {
+  return pool_alloc(reinterpret_cast<void**>(p), (size_t)count * sizeof(T), s);
+}
+
 // graph_build.cu
 cudaError_t validate_csr(const uint32_t* d_row_ptr, const uint32_t* d_col, uint64_t n, uint64_t nnz,
                          unsigned int* d_err, int sms, cudaStream_t s);

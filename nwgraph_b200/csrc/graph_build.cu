@@ -75,9 +75,9 @@ cudaError_t build_tiling(const uint32_t* d_row_ptr, uint64_t n, uint64_t nnz, ui
   if (tiles >= 0xFFFFFFF0ull || D == 0) return cudaErrorInvalidValue;
   t->tile_items = D;
   t->num_tiles = (uint32_t)tiles;
-  cudaError_t e = cudaMalloc(&t->tile_row, (tiles + 2) * sizeof(uint32_t));
+  cudaError_t e = pool_alloc_n(&t->tile_row, tiles + 2, s);
   if (e != cudaSuccess) return e;
-  e = cudaMalloc(&t->tile_nnz, (tiles + 2) * sizeof(uint32_t));
+  e = pool_alloc_n(&t->tile_nnz, tiles + 2, s);
   if (e != cudaSuccess) return e;
   const unsigned blocks = (unsigned)((tiles + 1 + 255) / 256);
   tiling_kernel<<<blocks, 256, 0, s>>>(d_row_ptr, n, nnz, (uint32_t)D, (uint32_t)tiles, t->tile_row, t->tile_nnz);
@@ -172,13 +172,13 @@ cudaError_t build_relabelled(const uint32_t* d_row_ptr, const uint32_t* d_col, c
   size_t    tmp_bytes = 0, scan_bytes = 0;
   Tiling    nt{};
   auto      cleanup = [&]() {
-    cudaFree(cnt);
-    cudaFree(cnt_sorted);
-    cudaFree(ids);
-    cudaFree(new_len);
-    cudaFree(tmp);
-    cudaFree(nt.tile_row);
-    cudaFree(nt.tile_nnz);
+    pool_free(cnt, s);
+    pool_free(cnt_sorted, s);
+    pool_free(ids, s);
+    pool_free(new_len, s);
+    pool_free(tmp, s);
+    pool_free(nt.tile_row, s);
+    pool_free(nt.tile_nnz, s);
   };
 #define RK(x)                \
   do {                       \
@@ -188,18 +188,18 @@ cudaError_t build_relabelled(const uint32_t* d_row_ptr, const uint32_t* d_col, c
     }                        \
   } while (0)
   const int grid = sms * 8;
-  RK(cudaMalloc(&cnt, (n + 1) * sizeof(uint32_t)));
-  RK(cudaMalloc(&cnt_sorted, (n + 1) * sizeof(uint32_t)));
-  RK(cudaMalloc(&ids, (n + 1) * sizeof(uint32_t)));
-  RK(cudaMalloc(&new_len, (n + 1) * sizeof(uint32_t)));
-  RK(cudaMalloc(&out->inv, (n + kPad) * sizeof(uint32_t)));
-  RK(cudaMalloc(&out->perm, (n + kPad) * sizeof(uint32_t)));
-  RK(cudaMalloc(&out->row_ptr, (n + 1 + kPad) * sizeof(uint32_t)));
-  RK(cudaMalloc(&out->col, (nnz + kPad) * sizeof(uint32_t)));
+  RK(pool_alloc_n(&cnt, n + 1, s));
+  RK(pool_alloc_n(&cnt_sorted, n + 1, s));
+  RK(pool_alloc_n(&ids, n + 1, s));
+  RK(pool_alloc_n(&new_len, n + 1, s));
+  RK(pool_alloc_n(&out->inv, n + kPad, s));
+  RK(pool_alloc_n(&out->perm, n + kPad, s));
+  RK(pool_alloc_n(&out->row_ptr, n + 1 + kPad, s));
+  RK(pool_alloc_n(&out->col, nnz + kPad, s));
   RK(cudaMemsetAsync(out->row_ptr, 0, (n + 1 + kPad) * sizeof(uint32_t), s));
   RK(cudaMemsetAsync(out->col, 0, (nnz + kPad) * sizeof(uint32_t), s));
   if (d_w) {
-    RK(cudaMalloc(&out->w, (nnz + kPad) * sizeof(float)));
+    RK(pool_alloc_n(&out->w, nnz + kPad, s));
     RK(cudaMemsetAsync(out->w, 0, (nnz + kPad) * sizeof(float), s));
   }
   row_length_kernel<<<grid, 256, 0, s>>>(d_row_ptr, n, cnt);
@@ -210,7 +210,7 @@ cudaError_t build_relabelled(const uint32_t* d_row_ptr, const uint32_t* d_col, c
   RK(cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp_bytes, cnt, cnt_sorted, ids, out->inv, (int64_t)n, 0, 32, s));
   RK(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, new_len, out->row_ptr, (int64_t)(n + 1), s));
   if (scan_bytes > tmp_bytes) tmp_bytes = scan_bytes;
-  RK(cudaMalloc(&tmp, tmp_bytes ? tmp_bytes : 1));
+  RK(pool_alloc(&tmp, tmp_bytes, s));
   size_t b1 = tmp_bytes;
   RK(cub::DeviceRadixSort::SortPairsDescending(tmp, b1, cnt, cnt_sorted, ids, out->inv, (int64_t)n, 0, 32, s));
   invert_kernel<<<grid, 256, 0, s>>>(out->inv, d_row_ptr, n, out->perm, new_len);

@@ -49,7 +49,7 @@ struct PprBuffers {
   cudaGraph_t     cg = nullptr;
   cudaGraphExec_t cg_exec = nullptr;
   float           cg_damping = -1.f;
-  void            release();
+  void            release(cudaStream_t s);  // returns the buffers to the pool on stream s
 };
 
 }  // namespace nwgpu
@@ -100,14 +100,14 @@ struct nwgpu_graph {
   nwgpu::PprBuffers ppr;
 
   ~nwgpu_graph() {
-    ppr.release();
+    ppr.release(stream);
     if (cg_exec) cudaGraphExecDestroy(cg_exec);
     if (cg) cudaGraphDestroy(cg);
     void* dev_ptrs[] = {g.row_ptr, g.col, g.w, g.perm, g.inv, tiling.tile_row, tiling.tile_nnz, rank, contrib[0],
                         contrib[1], deg, stage_u32, cpart, epart, res_part, st, err_hist, bin_first, bin_chunk_row,
                         bin_chunk_part};
-    for (void* p : dev_ptrs)
-      if (p) cudaFree(p);
+    for (void* p : dev_ptrs) nwgpu::pool_free(p, stream);
+    cudaStreamSynchronize(stream);  // the blocks are free for the next handle at once
     if (h_st) cudaFreeHost(h_st);
     if (h_abort) cudaFreeHost(h_abort);
     if (ev0) cudaEventDestroy(ev0);
@@ -120,7 +120,7 @@ namespace nwgpu {
 template <class T>
 cudaError_t dalloc(nwgpu_graph* g, T** p, uint64_t count) {
   const uint64_t bytes = (count + kPad) * sizeof(T);
-  cudaError_t    e = cudaMalloc((void**)p, bytes);
+  cudaError_t    e = pool_alloc((void**)p, bytes, g->stream);
   if (e == cudaSuccess) {
     g->device_bytes += bytes;
     e = cudaMemsetAsync(*p, 0, bytes, g->stream);
