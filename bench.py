@@ -84,9 +84,11 @@ def peaks():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def sweep_traffic_per_launch():
-    """DRAM bytes per sweep launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "pr_sweep_scale24.md")
+def sweep_traffic_per_launch(args):
+    """DRAM bytes per sweep launch from the committed ncu summary (RMAT-24, edge factor 16, relabelled)."""
+    if args.scale != 24 or args.edge_factor != 16 or args.no_relabel:
+        return None
+    path = os.path.join(ROOT, "profiles", "pr_binned_sweep_rmat24_traffic.md")
     try:
         m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
         return float(m.group(1)) if m else None
@@ -366,7 +368,7 @@ def run_ours(args):
                    "tile_items": info["tile_items"], "grid": info["grid"], "num_tiles": info["num_tiles"],
                    "launch": args.launch, "relabel": not args.no_relabel},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": sweep_traffic_per_launch(), "peak_kind": peak_kind,
+                     "traffic": sweep_traffic_per_launch(args), "peak_kind": peak_kind,
                      "bytes_per_sweep": B, "sweep_ms": t_sweep_ms},
         "gteps_per_sweep_kernel": nnz / (t_sweep_ms * 1e-3) / 1e9,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(4 * (n + 1) + 4 * nnz + 4 * n),
