@@ -26,6 +26,8 @@ std::once_flag           g_config_once;
 cudaError_t              g_config_err = cudaSuccess;
 constexpr int            kDefaultIpt = 8;
 constexpr uint32_t       kDefaultHotIds = 32768;
+constexpr uint32_t       kHotL1Ids = 16384;   // ids past the staged ones that still go through L1 (hot variant)
+constexpr uint32_t       kHotSmemIds = 32768; // staged ids by default (128 KB of shared memory)
 
 // NWGPU_TRACE=1 prints "# [ phase ]: X ms" lines to stderr, like the
 // reference's life_timer (include/nwgraph/util/timer.hpp:120-133).
@@ -84,7 +86,10 @@ int check_device(int* dev_out, int* sms_out) {
   CK(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev), "cudaDeviceGetAttribute");
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
   if (major != 10) return fail(NWGPU_ERR_NO_DEVICE, "device %d is sm_%d0, this build targets sm_100a only", dev, major);
-  std::call_once(g_config_once, [] { g_config_err = configure_sweep_kernels(); });
+  std::call_once(g_config_once, [] {
+    g_config_err = configure_sweep_kernels();
+    if (g_config_err == cudaSuccess) g_config_err = configure_binned_kernels();
+  });
   if (g_config_err != cudaSuccess) return cuda_fail(g_config_err, "configure kernels");
   *dev_out = dev;
   *sms_out = sms;
@@ -193,7 +198,23 @@ static int setup_binned(nwgpu_graph* g) {
   b.row_first_chunk = g->bin_first;
   b.chunk_row = g->bin_chunk_row;
   b.chunk_part = g->bin_chunk_part;
-  g->bin_sweep_grid = binned_sweep_grid(g->sms);
+  // Variant: NWGPU_SWEEP=binned_hot stages the hub contributions in shared
+  // memory (NWGPU_HOT_IDS of them, default kHotSmemIds: half the SM's L1/shared
+  // capacity, which leaves L1 room for the next tier of hubs).
+  const char* which = getenv("NWGPU_SWEEP");
+  g->bin_hot = which && !strcmp(which, "binned_hot");
+  if (g->bin_hot) {
+    const uint32_t lim = binned_hot_capacity();
+    const long     want = env_int("NWGPU_HOT_IDS", -1);
+    uint32_t       cap = want >= 0 ? (uint32_t)want & ~3u : kHotSmemIds;
+    if (cap > lim) cap = lim;
+    b.smem_ids = (uint32_t)(g->n < cap ? g->n & ~3ull : cap);
+    b.l1_ids = b.smem_ids + kHotL1Ids;
+  } else {
+    b.smem_ids = 0;
+    b.l1_ids = g->hot_ids;
+  }
+  g->bin_sweep_grid = binned_sweep_grid(g->sms, g->bin_hot);
   g->bin_finish_grid = g->sms * 2;
   g->binned = true;
   return NWGPU_OK;
@@ -265,7 +286,8 @@ int build_loop_graph(nwgpu_graph* g, const SweepArgs& proto) {
   a.cond = cond;
   a.use_cond = 1;
   if (g->binned)
-    CK(add_binned_nodes(body, make_binned_args(g, a), g->bin_sweep_grid, g->bin_finish_grid), "cudaGraphAddKernelNode(binned)");
+    CK(add_binned_nodes(body, make_binned_args(g, a), g->bin_hot, g->bin_sweep_grid, g->bin_finish_grid),
+       "cudaGraphAddKernelNode(binned)");
   else
     CK(add_pr_sweep_nodes(body, a, g->variant, g->grid, g->finish_grid), "cudaGraphAddKernelNode(sweep)");
   CK(cudaGraphInstantiate(&g->cg_exec, g->cg, 0), "cudaGraphInstantiate");
@@ -300,7 +322,7 @@ int run_sweeps(nwgpu_graph* g, const SweepArgs& a, uint32_t launch, uint64_t max
       const BinnedArgs ba = g->binned ? make_binned_args(g, a) : BinnedArgs{};
       for (uint64_t b = 0; b < batch; ++b) {
         if (g->binned) {
-          CK(launch_binned_sweep(ba, g->bin_sweep_grid, g->bin_finish_grid, s), "pr_binned_sweep");
+          CK(launch_binned_sweep(ba, g->bin_hot, g->bin_sweep_grid, g->bin_finish_grid, s), "pr_binned_sweep");
         } else {
           CK(launch_pr_sweep(a, g->variant, g->grid, s), "pr_sweep");
           CK(launch_pr_finish(a, g->finish_grid, s), "pr_finish");
@@ -557,7 +579,7 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
   g->finish_grid = finish_grid_for(g->tiling.num_tiles);
   if ((e = cudaStreamSynchronize(g->stream)) != cudaSuccess) return bail(cuda_fail(e, "graph create"));
   trace.mark("tiling");
-  const bool want_binned = which ? !strcmp(which, "binned") : true;
+  const bool want_binned = which ? (!strcmp(which, "binned") || !strcmp(which, "binned_hot")) : true;
   if (g->relabelled && want_binned) {
     rc = setup_binned(g);
     if (rc) return bail(rc);

@@ -19,14 +19,24 @@ struct BinnedArgs {
   uint32_t        bin_row_begin[kNumBins];
   uint32_t        bin_row_end[kNumBins];
   uint32_t        bin_warp_end[kNumBins]; // cumulative warps over the bins
+  uint32_t        smem_ids;               // hot variant: contrib[0, smem_ids) is staged in shared memory
+  uint32_t        l1_ids;                 // ids in [smem_ids, l1_ids) are gathered through L1 (evict-last)
 };
+
+// Launch shapes of the binned sweep: 256-thread CTAs, four per SM, hub ids
+// through L1; or one 1024-thread CTA per SM with the hub contributions staged
+// in shared memory at the start of every sweep.
+constexpr int kBinnedThreads = 256;
+constexpr int kBinnedHotThreads = 1024;
 
 cudaError_t launch_bin_bounds(const uint32_t* row_ptr, uint32_t n, uint32_t* d_out, unsigned int* d_unsorted, int sms,
                               cudaStream_t s);
 cudaError_t launch_chunk_count(const uint32_t* row_ptr, uint32_t nlong, uint32_t* cnt, int sms, cudaStream_t s);
 cudaError_t launch_chunk_fill(const uint32_t* first, uint32_t nlong, uint32_t* chunk_row, int sms, cudaStream_t s);
-int         binned_sweep_grid(int sms);
-cudaError_t launch_binned_sweep(const BinnedArgs& a, int sweep_grid, int finish_grid, cudaStream_t s);
-cudaError_t add_binned_nodes(cudaGraph_t body, const BinnedArgs& a, int sweep_grid, int finish_grid);
+int         binned_sweep_grid(int sms, bool hot);
+uint32_t    binned_hot_capacity();  // ids the hot variant can stage (a multiple of 4)
+cudaError_t configure_binned_kernels();
+cudaError_t launch_binned_sweep(const BinnedArgs& a, bool hot, int sweep_grid, int finish_grid, cudaStream_t s);
+cudaError_t add_binned_nodes(cudaGraph_t body, const BinnedArgs& a, bool hot, int sweep_grid, int finish_grid);
 
 }  // namespace nwgpu

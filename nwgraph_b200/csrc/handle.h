@@ -67,6 +67,7 @@ struct nwgpu_graph {
   nwgpu::SweepVariant variant{256, 8, false};
   // Degree-binned sweep (relabelled graphs with non-increasing row lengths).
   bool              binned = false;
+  bool              bin_hot = false;   // hub contributions staged in shared memory
   nwgpu::BinnedArgs bin{};         // tables; the SweepArgs part is filled per solve
   uint32_t*         bin_first = nullptr;
   uint32_t*         bin_chunk_row = nullptr;

@@ -12,9 +12,22 @@
 //   empty  len = 0             : epilogue only
 // Every lane's entries are summed in a fixed order and combined by a fixed
 // xor-shuffle tree, so ranks are bit-reproducible. Column ids stream through
-// (coalesced, evict-first); contributions are gathered with up to 4 loads in
-// flight per lane, hub ids (< hot_ids) through L1, the rest with
-// L1::no_allocate. The per-row update is page_rank_v10's
+// (coalesced, evict-first); contributions are gathered with 8 loads in flight
+// per lane.
+//
+// Where the gathered values come from (ids are in descending-degree order, so
+// small ids are the hubs):
+//   HOT = false: ids < l1_ids through L1 with an evict-last policy, the rest
+//                with L1::no_allocate;
+//   HOT = true:  one 1024-thread CTA per SM copies contrib[0, smem_ids) into
+//                shared memory at the start of the sweep and gathers those ids
+//                from there; [smem_ids, l1_ids) through L1, the rest
+//                L1::no_allocate.
+// A warp load whose lanes mix L1 hits and misses costs the L1 as much as one
+// that misses in every lane, while shared-memory loads use a separate, much
+// wider path; staging the hubs in shared memory leaves the L1->L2 request
+// path to the misses alone. Both variants sum the same values in the same
+// order, so their ranks are bitwise equal. The per-row update is page_rank_v10's
 // (include/nwgraph/experimental/algorithms/page_rank.hpp:413-418) fused with
 // the next sweep's contribution (:401-405).
 #include "binned.h"
@@ -28,8 +41,19 @@ __device__ __forceinline__ float binned_base(const BinnedArgs& a, uint32_t r) {
   return a.sw.base;
 }
 
-__device__ __forceinline__ float gather_one(const float* __restrict__ cin, uint32_t id, uint32_t hot, uint64_t pol) {
-  return (id < hot) ? ld_gather(cin + id, pol) : ld_gather_cold(cin + id, pol);
+// Gather source of one contribution: shared memory (hot variant), L1, or L2.
+struct Src {
+  const float* __restrict__ cin;
+  const float* s_hot;   // staged contrib[0, smem_ids); null in the plain variant
+  uint32_t     smem_ids;
+  uint32_t     l1_ids;
+  uint64_t     pol;
+};
+
+template <bool HOT>
+__device__ __forceinline__ float gather_one(const Src& s, uint32_t id) {
+  if (HOT && id < s.smem_ids) return s.s_hot[id];
+  return (id < s.l1_ids) ? ld_gather(s.cin + id, s.pol) : ld_gather_cold(s.cin + id, s.pol);
 }
 
 // Epilogue of one row with its old rank and degree already loaded; returns
@@ -47,9 +71,9 @@ __device__ __forceinline__ double binned_epilogue(const BinnedArgs& a, float* __
 }
 
 // Sum of entries [k, k_end) taken U at a time, lanes `stride` apart.
-template <int U>
-__device__ __forceinline__ float strided_sum(const BinnedArgs& a, const float* __restrict__ cin, uint32_t k,
-                                             uint32_t k_end, uint32_t stride, uint64_t pol) {
+template <bool HOT, int U>
+__device__ __forceinline__ float strided_sum(const BinnedArgs& a, const Src& src, uint32_t k, uint32_t k_end,
+                                             uint32_t stride) {
   float acc = 0.f;
 #pragma unroll 1
   for (; k < k_end; k += U * stride) {
@@ -58,7 +82,7 @@ __device__ __forceinline__ float strided_sum(const BinnedArgs& a, const float* _
 #pragma unroll
     for (int q = 0; q < U; ++q) id[q] = (k + q * stride < k_end) ? ld_stream(a.sw.col + k + q * stride) : 0u;
 #pragma unroll
-    for (int q = 0; q < U; ++q) v[q] = (k + q * stride < k_end) ? gather_one(cin, id[q], a.sw.hot_ids, pol) : 0.f;
+    for (int q = 0; q < U; ++q) v[q] = (k + q * stride < k_end) ? gather_one<HOT>(src, id[q]) : 0.f;
 #pragma unroll
     for (int q = 0; q < U; ++q) acc += v[q];
   }
@@ -66,20 +90,21 @@ __device__ __forceinline__ float strided_sum(const BinnedArgs& a, const float* _
 }
 
 // One warp: a chunk of a long row.
-__device__ __forceinline__ void long_chunk(const BinnedArgs& a, const float* __restrict__ cin, uint32_t c, int lane,
-                                           uint64_t pol) {
+template <bool HOT>
+__device__ __forceinline__ void long_chunk(const BinnedArgs& a, const Src& src, uint32_t c, int lane) {
   const uint32_t row = a.chunk_row[c];
   const uint32_t rs = a.sw.row_ptr[row], re = a.sw.row_ptr[row + 1];
   const uint32_t k0 = rs + (c - a.row_first_chunk[row]) * kChunk;
   const uint32_t k1 = min(re, k0 + kChunk);
-  float          acc = strided_sum<8>(a, cin, k0 + lane, k1, 32u, pol);
+  float          acc = strided_sum<HOT, 8>(a, src, k0 + lane, k1, 32u);
   acc = warp_sum_lane0(acc);
   if (lane == 0) a.chunk_part[c] = acc;
 }
 
 // One warp, G = 32: one row of 65..kLongRow entries.
-__device__ __forceinline__ double warp_row(const BinnedArgs& a, const float* __restrict__ cin, float* __restrict__ cout,
-                                           uint32_t row, uint32_t row_end, int lane, uint64_t pol) {
+template <bool HOT>
+__device__ __forceinline__ double warp_row(const BinnedArgs& a, const Src& src, float* __restrict__ cout, uint32_t row,
+                                           uint32_t row_end, int lane) {
   if (row >= row_end) return 0.0;  // uniform across the warp
   const uint32_t rs = a.sw.row_ptr[row], re = a.sw.row_ptr[row + 1];
   float          old = 0.f;
@@ -88,16 +113,16 @@ __device__ __forceinline__ double warp_row(const BinnedArgs& a, const float* __r
     old = ld_stream(a.sw.rank + row);
     dg = ld_stream(a.sw.deg + row);
   }
-  float acc = strided_sum<8>(a, cin, rs + lane, re, 32u, pol);
+  float acc = strided_sum<HOT, 8>(a, src, rs + lane, re, 32u);
   acc = warp_sum_lane0(acc);
-  return (lane == 0) ? binned_update(a, cout, row, acc, old, dg, pol) : 0.0;
+  return (lane == 0) ? binned_update(a, cout, row, acc, old, dg, src.pol) : 0.0;
 }
 
 // One warp of a G-bin, G < 32: 2 * 32/G rows, G lanes per row, each lane two
 // rows and at most 4 entries of each (8 gathers in flight).
-template <int G>
-__device__ __forceinline__ double group_rows(const BinnedArgs& a, const float* __restrict__ cin, float* __restrict__ cout,
-                                             uint32_t row0, uint32_t row_end, int lane, uint64_t pol) {
+template <bool HOT, int G>
+__device__ __forceinline__ double group_rows(const BinnedArgs& a, const Src& src, float* __restrict__ cout, uint32_t row0,
+                                             uint32_t row_end, int lane) {
   constexpr uint32_t PER = 32 / G;  // rows per half
   const int          sub = lane & (G - 1);
   uint32_t           row[2], rs[2], re[2];
@@ -125,7 +150,7 @@ __device__ __forceinline__ double group_rows(const BinnedArgs& a, const float* _
   for (int h = 0; h < 2; ++h)
 #pragma unroll
     for (int q = 0; q < 4; ++q)
-      v[h][q] = (rs[h] + sub + q * G < re[h]) ? gather_one(cin, id[h][q], a.sw.hot_ids, pol) : 0.f;
+      v[h][q] = (rs[h] + sub + q * G < re[h]) ? gather_one<HOT>(src, id[h][q]) : 0.f;
   double res = 0.0;
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
@@ -134,7 +159,7 @@ __device__ __forceinline__ double group_rows(const BinnedArgs& a, const float* _
     for (int q = 0; q < 4; ++q) acc += v[h][q];
 #pragma unroll
     for (int off = G / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(kFullMask, acc, off);
-    if (row[h] < row_end && sub == 0) res += binned_update(a, cout, row[h], acc, old[h], dg[h], pol);
+    if (row[h] < row_end && sub == 0) res += binned_update(a, cout, row[h], acc, old[h], dg[h], src.pol);
   }
   return res;
 }
@@ -159,8 +184,11 @@ __device__ __forceinline__ double empty_rows(const BinnedArgs& a, float* __restr
   return res;
 }
 
-__global__ void __launch_bounds__(256, 4) pr_binned_sweep_kernel(const BinnedArgs a) {
-  __shared__ double s_red[8];
+template <int NT, bool HOT>
+__global__ void __launch_bounds__(NT, 1024 / NT) pr_binned_sweep_kernel(const BinnedArgs a) {
+  constexpr int     NW = NT / 32;
+  __shared__ double s_red[NW];
+  extern __shared__ float4 s_hot4[];  // HOT: contrib[0, smem_ids)
   const int         tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   PrState*          st = a.sw.st;
   if (a.sw.use_cond && blockIdx.x == 0 && tid == 0) cudaGraphSetConditional(a.sw.cond, 0u);
@@ -168,14 +196,22 @@ __global__ void __launch_bounds__(256, 4) pr_binned_sweep_kernel(const BinnedArg
   const unsigned long long it = *(volatile unsigned long long*)&st->iter;
   const float* __restrict__ cin = (it & 1ull) ? a.sw.contrib1 : a.sw.contrib0;
   float* __restrict__ cout = (it & 1ull) ? a.sw.contrib0 : a.sw.contrib1;
-  const uint64_t pol = policy_evict_last();
-  double         res = 0.0;
+  Src src{cin, nullptr, 0u, a.l1_ids, policy_evict_last()};
+  if constexpr (HOT) {
+    // smem_ids is a multiple of 4 and contrib is 16-byte aligned
+    const float4* g4 = reinterpret_cast<const float4*>(cin);
+    for (uint32_t i = tid; i < a.smem_ids / 4u; i += NT) s_hot4[i] = __ldcg(g4 + i);
+    __syncthreads();
+    src.s_hot = reinterpret_cast<const float*>(s_hot4);
+    src.smem_ids = a.smem_ids;
+  }
+  double res = 0.0;
 
-  const uint32_t nwarps = gridDim.x * 8, gwarp = blockIdx.x * 8 + warp;
+  const uint32_t nwarps = gridDim.x * NW, gwarp = blockIdx.x * NW + warp;
   const uint32_t units = a.num_chunks + a.bin_warp_end[kNumBins - 1];
   for (uint32_t u = gwarp; u < units; u += nwarps) {
     if (u < a.num_chunks) {
-      long_chunk(a, cin, u, lane, pol);
+      long_chunk<HOT>(a, src, u, lane);
       continue;
     }
     const uint32_t w = u - a.num_chunks;  // warp index in the flat bin space
@@ -184,13 +220,13 @@ __global__ void __launch_bounds__(256, 4) pr_binned_sweep_kernel(const BinnedArg
     const uint32_t wb = w - (b ? a.bin_warp_end[b - 1] : 0u);
     const uint32_t rb = a.bin_row_begin[b], re = a.bin_row_end[b];
     switch (b) {
-      case 0: res += warp_row(a, cin, cout, rb + wb, re, lane, pol); break;
-      case 1: res += group_rows<16>(a, cin, cout, rb + wb * 4, re, lane, pol); break;
-      case 2: res += group_rows<8>(a, cin, cout, rb + wb * 8, re, lane, pol); break;
-      case 3: res += group_rows<4>(a, cin, cout, rb + wb * 16, re, lane, pol); break;
-      case 4: res += group_rows<2>(a, cin, cout, rb + wb * 32, re, lane, pol); break;
-      case 5: res += group_rows<1>(a, cin, cout, rb + wb * 64, re, lane, pol); break;
-      default: res += empty_rows(a, cout, rb + wb * 128, re, lane, pol); break;
+      case 0: res += warp_row<HOT>(a, src, cout, rb + wb, re, lane); break;
+      case 1: res += group_rows<HOT, 16>(a, src, cout, rb + wb * 4, re, lane); break;
+      case 2: res += group_rows<HOT, 8>(a, src, cout, rb + wb * 8, re, lane); break;
+      case 3: res += group_rows<HOT, 4>(a, src, cout, rb + wb * 16, re, lane); break;
+      case 4: res += group_rows<HOT, 2>(a, src, cout, rb + wb * 32, re, lane); break;
+      case 5: res += group_rows<HOT, 1>(a, src, cout, rb + wb * 64, re, lane); break;
+      default: res += empty_rows(a, cout, rb + wb * 128, re, lane, src.pol); break;
     }
   }
   res = warp_sum_lane0(res);
@@ -199,7 +235,7 @@ __global__ void __launch_bounds__(256, 4) pr_binned_sweep_kernel(const BinnedArg
   if (tid == 0) {
     double s = 0.0;
 #pragma unroll
-    for (int w = 0; w < 8; ++w) s += s_red[w];
+    for (int w = 0; w < NW; ++w) s += s_red[w];
     a.sw.res_part[blockIdx.x] = s;
   }
 }
@@ -317,34 +353,62 @@ cudaError_t launch_chunk_fill(const uint32_t* first, uint32_t nlong, uint32_t* c
   return cudaGetLastError();
 }
 
-int binned_sweep_grid(int sms) {
+// Dynamic shared memory of the hot variant: the largest opt-in size less the
+// kernel's static shared memory and a margin.
+static int binned_hot_smem_bytes() {
+  int dev = 0, bytes = 0;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&bytes, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) bytes = 232448;
+  bytes -= 1024;
+  return bytes > 0 ? bytes & ~15 : 0;
+}
+
+uint32_t binned_hot_capacity() { return (uint32_t)(binned_hot_smem_bytes() / 4) & ~3u; }
+
+cudaError_t configure_binned_kernels() {
+  return cudaFuncSetAttribute(pr_binned_sweep_kernel<kBinnedHotThreads, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              binned_hot_smem_bytes());
+}
+
+int binned_sweep_grid(int sms, bool hot) {
+  if (hot) return sms;
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pr_binned_sweep_kernel, 256, 0) != cudaSuccess || nb < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pr_binned_sweep_kernel<kBinnedThreads, false>, kBinnedThreads, 0) !=
+          cudaSuccess ||
+      nb < 1)
     nb = 1;
   return sms * nb;
 }
 
-cudaError_t launch_binned_sweep(const BinnedArgs& a, int sweep_grid, int finish_grid, cudaStream_t s) {
-  pr_binned_sweep_kernel<<<sweep_grid, 256, 0, s>>>(a);
-  cudaError_t e = cudaGetLastError();
+static void* binned_fn(bool hot) {
+  return hot ? (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true> : (void*)pr_binned_sweep_kernel<kBinnedThreads, false>;
+}
+
+cudaError_t launch_binned_sweep(const BinnedArgs& a, bool hot, int sweep_grid, int finish_grid, cudaStream_t s) {
+  void*       args[] = {(void*)&a};
+  cudaError_t e = cudaLaunchKernel(binned_fn(hot), dim3((unsigned)sweep_grid), dim3(hot ? kBinnedHotThreads : kBinnedThreads),
+                                   args, hot ? (size_t)a.smem_ids * 4u : 0u, s);
   if (e != cudaSuccess) return e;
   pr_binned_finish_kernel<<<finish_grid, 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 
-cudaError_t add_binned_nodes(cudaGraph_t body, const BinnedArgs& a, int sweep_grid, int finish_grid) {
+cudaError_t add_binned_nodes(cudaGraph_t body, const BinnedArgs& a, bool hot, int sweep_grid, int finish_grid) {
   void*                args[] = {(void*)&a};
   cudaKernelNodeParams kp = {};
-  kp.func = (void*)pr_binned_sweep_kernel;
+  kp.func = binned_fn(hot);
   kp.gridDim = dim3((unsigned)sweep_grid);
-  kp.blockDim = dim3(256);
+  kp.blockDim = dim3(hot ? kBinnedHotThreads : kBinnedThreads);
+  kp.sharedMemBytes = hot ? (unsigned)a.smem_ids * 4u : 0u;
   kp.kernelParams = args;
   cudaGraphNode_t sn, fn;
   cudaError_t     e = cudaGraphAddKernelNode(&sn, body, nullptr, 0, &kp);
   if (e != cudaSuccess) return e;
-  cudaKernelNodeParams fp = kp;
+  cudaKernelNodeParams fp = {};
   fp.func = (void*)pr_binned_finish_kernel;
   fp.gridDim = dim3((unsigned)finish_grid);
+  fp.blockDim = dim3(256);
+  fp.kernelParams = args;
   return cudaGraphAddKernelNode(&fn, body, &sn, 1, &fp);
 }
 

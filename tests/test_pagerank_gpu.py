@@ -259,7 +259,7 @@ def test_scale20_properties(gpu):
     assert abs(float(r.astype(np.float64).sum()) - float(ref.astype(np.float64).sum())) < 1e-5
 
 
-@pytest.mark.parametrize("sweep", ["binned", "base", "hot", "hot512"])
+@pytest.mark.parametrize("sweep", ["binned", "binned_hot", "base", "hot", "hot512"])
 def test_sweep_variants_agree(gpu, sweep, monkeypatch):
     """Every sweep kernel variant (degree-binned, merge-path with L1 hot ids,
     merge-path with the hot ids in shared memory) meets the same bar."""
@@ -279,3 +279,19 @@ def test_sweep_variants_agree(gpu, sweep, monkeypatch):
     ref, _, _ = O.jacobi_f32(hub.row_ptr, hub.col, hub.out_degree(), 0.85, 0.0, 10)
     r, _ = solve(hub.row_ptr, hub.col, hub.out_degree(), iters=10)
     assert_parity_or_more_accurate(r, ref, hub.row_ptr, hub.col, 10)
+
+
+@pytest.mark.parametrize("hot_ids", ["-1", "0", "4", "1000", "40000"])
+def test_binned_hot_staging_is_exact(gpu, hot_ids, monkeypatch):
+    """Staging the hub contributions in shared memory changes where each value
+    is read from, not which values are summed or in what order: the ranks equal
+    the plain binned sweep's bit for bit, whatever the staged id count."""
+    g = G.rmat(16, 16, 5)
+    deg = g.out_degree()
+    monkeypatch.setenv("NWGPU_SWEEP", "binned")
+    a, _ = solve(g.row_ptr, g.col, deg)
+    monkeypatch.setenv("NWGPU_SWEEP", "binned_hot")
+    if hot_ids != "-1":
+        monkeypatch.setenv("NWGPU_HOT_IDS", hot_ids)
+    b, _ = solve(g.row_ptr, g.col, deg)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
