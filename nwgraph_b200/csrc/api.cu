@@ -145,9 +145,9 @@ static int setup_binned(nwgpu_graph* g) {
   const uint32_t n = (uint32_t)g->n;
   uint32_t*      d_out = nullptr;
   unsigned int*  d_bad = nullptr;
-  CK(pool_alloc((void**)&d_out, 8 * sizeof(uint32_t) + sizeof(unsigned int), g->stream), "cudaMalloc(bins)");
-  d_bad = reinterpret_cast<unsigned int*>(d_out + 8);
-  uint32_t     h_out[8];
+  CK(pool_alloc((void**)&d_out, (kNumBins + 1) * sizeof(uint32_t) + sizeof(unsigned int), g->stream), "cudaMalloc(bins)");
+  d_bad = reinterpret_cast<unsigned int*>(d_out + kNumBins + 1);
+  uint32_t     h_out[kNumBins + 1];
   unsigned int h_bad = 0;
   cudaError_t  e = cudaMemsetAsync(d_bad, 0, sizeof(unsigned int), g->stream);
   if (e == cudaSuccess) e = launch_bin_bounds(g->g.row_ptr, n, d_out, d_bad, g->sms, g->stream);
@@ -161,7 +161,7 @@ static int setup_binned(nwgpu_graph* g) {
   const uint32_t nlong = h_out[0];
   b.num_long_rows = nlong;
   // rows one warp handles in each bin (pr_binned.cu: warp_row, group_rows<G>, empty_rows)
-  static const uint32_t rows_per_warp[kNumBins] = {1, 4, 8, 16, 32, 64, 128};
+  static const uint32_t rows_per_warp[kNumBins] = {1, 2, 4, 8, 16, 32, 64, 128};
   uint32_t              warps = 0;
   for (int i = 0; i < kNumBins; ++i) {
     b.bin_row_begin[i] = h_out[i];
@@ -198,22 +198,24 @@ static int setup_binned(nwgpu_graph* g) {
   b.row_first_chunk = g->bin_first;
   b.chunk_row = g->bin_chunk_row;
   b.chunk_part = g->bin_chunk_part;
-  // Variant: NWGPU_SWEEP=binned_hot stages the hub contributions in shared
-  // memory (NWGPU_HOT_IDS of them, default kHotSmemIds: half the SM's L1/shared
-  // capacity, which leaves L1 room for the next tier of hubs).
+  // Variant: by default (or NWGPU_SWEEP=binned_hot) the hub contributions are
+  // staged in shared memory, NWGPU_HOT_IDS of them (default kHotSmemIds: half
+  // the SM's L1/shared capacity, which leaves L1 room for the next tier of
+  // hubs); NWGPU_SWEEP=binned keeps them in L1 only.
   const char* which = getenv("NWGPU_SWEEP");
-  g->bin_hot = which && !strcmp(which, "binned_hot");
+  g->bin_hot = !which || !strcmp(which, "binned_hot");
   if (g->bin_hot) {
     const uint32_t lim = binned_hot_capacity();
     const long     want = env_int("NWGPU_HOT_IDS", -1);
     uint32_t       cap = want >= 0 ? (uint32_t)want & ~3u : kHotSmemIds;
     if (cap > lim) cap = lim;
     b.smem_ids = (uint32_t)(g->n < cap ? g->n & ~3ull : cap);
-    b.l1_ids = b.smem_ids + kHotL1Ids;
+    b.l1_ids = b.smem_ids + (uint32_t)env_int("NWGPU_HOT_L1_IDS", (int)kHotL1Ids);
   } else {
     b.smem_ids = 0;
     b.l1_ids = g->hot_ids;
   }
+  b.pipe = env_int("NWGPU_BINNED_PIPE", 1) ? 1u : 0u;
   g->bin_sweep_grid = binned_sweep_grid(g->sms, g->bin_hot);
   g->bin_finish_grid = g->sms * 2;
   g->binned = true;
@@ -543,10 +545,11 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
     g->g.w = in.w;
   }
   trace.mark("relabel");
-  // Launch shape. Default: relabelled graphs of 64K+ vertices use one
-  // 1024-thread CTA per SM holding the hottest ids in shared memory; others
-  // use 256-thread CTAs. NWGPU_SWEEP (base|hot|hot512|hot1024x8), NWGPU_IPT,
-  // NWGPU_HOT_IDS, NWGPU_CTAS_PER_SM and NWGPU_CARVEOUT override for tuning.
+  // Merge-path sweep (graphs kept in input order, or NWGPU_SWEEP naming a
+  // merge-path variant): 256-thread CTAs by default. NWGPU_SWEEP
+  // (base|hot|hot512|hot1024x8), NWGPU_IPT, NWGPU_HOT_IDS, NWGPU_CTAS_PER_SM and
+  // NWGPU_CARVEOUT override for tuning. Relabelled graphs use the degree-binned
+  // sweep (set up below) unless NWGPU_SWEEP names a merge-path variant.
   SweepVariant v{256, kDefaultIpt, false};
   const char*  which = getenv("NWGPU_SWEEP");
   const bool   want_hot = which && strncmp(which, "hot", 3) == 0;

@@ -7,7 +7,7 @@ namespace nwgpu {
 
 constexpr uint32_t kLongRow = 2048;  // rows longer than this are split into chunks
 constexpr uint32_t kChunk = 1024;    // entries per long-row chunk (one warp)
-constexpr int      kNumBins = 7;     // G = 32, 16, 8, 4, 2, 1, empty
+constexpr int      kNumBins = 8;     // warp per row, then G = 32, 16, 8, 4, 2, 1, empty
 
 struct BinnedArgs {
   SweepArgs       sw;                     // row_ptr / col / vectors / state / loop control
@@ -19,8 +19,12 @@ struct BinnedArgs {
   uint32_t        bin_row_begin[kNumBins];
   uint32_t        bin_row_end[kNumBins];
   uint32_t        bin_warp_end[kNumBins]; // cumulative warps over the bins
+  // bin 0: 129..kLongRow entries, one warp per row; bins 1-6: G = 32..1 lanes
+  // per row, two rows per lane group, rows of (2G, 4G] entries (G = 1: 1..4);
+  // bin 7: empty rows
   uint32_t        smem_ids;               // hot variant: contrib[0, smem_ids) is staged in shared memory
   uint32_t        l1_ids;                 // ids in [smem_ids, l1_ids) are gathered through L1 (evict-last)
+  uint32_t        pipe;                   // 1: software-pipelined walk of the bins
 };
 
 // Launch shapes of the binned sweep: 256-thread CTAs, four per SM, hub ids

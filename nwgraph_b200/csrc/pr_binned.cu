@@ -6,9 +6,10 @@
 //   long   len > kLongRow     : chunks of kChunk entries, one warp per chunk;
 //                               per-chunk FP32 partials summed in chunk order by
 //                               pr_binned_finish_kernel
-//   G = 32 64 < len <= kLongRow: one warp per row, lanes stride the row
-//   G = 16, 8, 4, 2, 1          : rows of (G*2, G*4] entries (G = 1: 1..4),
-//                               G lanes per row, <= 4 entries per lane
+//   bin 0  128 < len <= kLongRow: one warp per row, lanes stride the row
+//   G = 32, 16, 8, 4, 2, 1      : rows of (G*2, G*4] entries (G = 1: 1..4),
+//                               G lanes per row, two rows per lane group,
+//                               <= 4 entries of each per lane
 //   empty  len = 0             : epilogue only
 // Every lane's entries are summed in a fixed order and combined by a fixed
 // xor-shuffle tree, so ranks are bit-reproducible. Column ids stream through
@@ -101,7 +102,7 @@ __device__ __forceinline__ void long_chunk(const BinnedArgs& a, const Src& src, 
   if (lane == 0) a.chunk_part[c] = acc;
 }
 
-// One warp, G = 32: one row of 65..kLongRow entries.
+// One warp: one row of 129..kLongRow entries.
 template <bool HOT>
 __device__ __forceinline__ double warp_row(const BinnedArgs& a, const Src& src, float* __restrict__ cout, uint32_t row,
                                            uint32_t row_end, int lane) {
@@ -118,8 +119,8 @@ __device__ __forceinline__ double warp_row(const BinnedArgs& a, const Src& src, 
   return (lane == 0) ? binned_update(a, cout, row, acc, old, dg, src.pol) : 0.0;
 }
 
-// One warp of a G-bin, G < 32: 2 * 32/G rows, G lanes per row, each lane two
-// rows and at most 4 entries of each (8 gathers in flight).
+// One warp of a G-bin: 2 * 32/G rows, G lanes per row, each lane two rows and
+// at most 4 entries of each (8 gathers in flight).
 template <bool HOT, int G>
 __device__ __forceinline__ double group_rows(const BinnedArgs& a, const Src& src, float* __restrict__ cout, uint32_t row0,
                                              uint32_t row_end, int lane) {
@@ -184,7 +185,185 @@ __device__ __forceinline__ double empty_rows(const BinnedArgs& a, float* __restr
   return res;
 }
 
-template <int NT, bool HOT>
+// ---------------------------------------------------------------------------
+// Software-pipelined bin walkers (PIPE = true). A warp takes the units of one
+// bin at a time, in the same order as the flat grid-stride walk above (unit
+// u of the flat space goes to warp u mod nwarps). While the gathers of one
+// step are in flight, the column ids of the next step and the row bounds of
+// the unit after it are already loading: a warp keeps loads of two or three
+// stages outstanding instead of waiting through row_ptr -> col -> contrib in
+// turn. Every lane sums the same entries in the same order as the plain walk,
+// so the results are bitwise equal.
+// ---------------------------------------------------------------------------
+// First unit (bin-local index) of warp gwarp in a bin that starts at flat unit `begin`.
+__device__ __forceinline__ uint32_t first_unit(uint32_t gwarp, uint32_t nwarps, uint32_t begin) {
+  const uint32_t r = begin % nwarps;
+  return gwarp >= r ? gwarp - r : gwarp + nwarps - r;
+}
+
+// Units that are entry ranges, one warp each, walked in steps of 8 x 32
+// entries. CHUNK: unit c = chunk c of a long row, partial sum to chunk_part[c].
+// Otherwise: unit w = row rb + w (bin 0), epilogue.
+template <bool HOT, bool CHUNK>
+__device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src, float* __restrict__ cout, uint32_t rb,
+                                            uint32_t nunits, uint32_t w, uint32_t nwarps, int lane) {
+  constexpr int      U = 8;
+  constexpr uint32_t STEP = U * 32;
+  if (w >= nunits) return 0.0;
+  auto bounds = [&](uint32_t unit, uint32_t& k0, uint32_t& k1) {
+    if (CHUNK) {
+      const uint32_t row = a.chunk_row[unit];
+      const uint32_t rs = a.sw.row_ptr[row], re = a.sw.row_ptr[row + 1];
+      k0 = rs + (unit - a.row_first_chunk[row]) * kChunk;
+      k1 = min(re, k0 + kChunk);
+    } else {
+      k0 = ld_stream(a.sw.row_ptr + rb + unit);
+      k1 = ld_stream(a.sw.row_ptr + rb + unit + 1);
+    }
+  };
+  auto load_ids = [&](uint32_t base, uint32_t end, uint32_t(&dst)[U]) {
+#pragma unroll
+    for (int q = 0; q < U; ++q) {
+      const uint32_t k = base + (uint32_t)lane + (uint32_t)q * 32u;
+      dst[q] = (k < end) ? ld_stream(a.sw.col + k) : 0u;
+    }
+  };
+  uint32_t k0, k1, nk0 = 0, nk1 = 0;
+  bounds(w, k0, k1);
+  if (w + nwarps < nunits) bounds(w + nwarps, nk0, nk1);
+  uint32_t id[U];
+  uint32_t base = k0;
+  load_ids(base, k1, id);
+  float    old = 0.f;
+  uint32_t dg = 1u;
+  if (!CHUNK && lane == 0) {
+    old = ld_stream(a.sw.rank + rb + w);
+    dg = ld_stream(a.sw.deg + rb + w);
+  }
+  float  acc = 0.f;
+  double res = 0.0;
+#pragma unroll 1
+  for (;;) {
+    float v[U];
+#pragma unroll
+    for (int q = 0; q < U; ++q) {
+      const uint32_t k = base + (uint32_t)lane + (uint32_t)q * 32u;
+      v[q] = (k < k1) ? gather_one<HOT>(src, id[q]) : 0.f;
+    }
+    // the next step: the rest of this unit, or the first step of the next one
+    const bool     more = base + STEP < k1;  // warp-uniform
+    const bool     has_next = w + nwarps < nunits;
+    const uint32_t nbase = more ? base + STEP : nk0;
+    const uint32_t nend = more ? k1 : (has_next ? nk1 : 0u);
+    load_ids(nbase, nend, id);
+#pragma unroll
+    for (int q = 0; q < U; ++q) acc += v[q];
+    if (!more) {
+      const float z = warp_sum_lane0(acc);
+      if (CHUNK) {
+        if (lane == 0) a.chunk_part[w] = z;
+      } else if (lane == 0) {
+        res += binned_update(a, cout, rb + w, z, old, dg, src.pol);
+      }
+      acc = 0.f;
+      w += nwarps;
+      if (w >= nunits) break;
+      k1 = nk1;
+      if (w + nwarps < nunits) bounds(w + nwarps, nk0, nk1);
+      if (!CHUNK && lane == 0) {
+        old = ld_stream(a.sw.rank + rb + w);
+        dg = ld_stream(a.sw.deg + rb + w);
+      }
+    }
+    base = nbase;
+  }
+  return res;
+}
+
+// Row bounds of the two rows a lane owns in unit w of a G-bin (len 0: no row).
+template <int G>
+__device__ __forceinline__ void group_bounds(const BinnedArgs& a, uint32_t rb, uint32_t re_bin, uint32_t w,
+                                             uint32_t nunits, int lane, uint32_t (&rs)[2], uint32_t (&len)[2]) {
+  constexpr uint32_t PER = 32 / G;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    rs[h] = 0u;
+    len[h] = 0u;
+    if (w < nunits) {
+      const uint32_t row = rb + w * (2u * PER) + (uint32_t)h * PER + (uint32_t)lane / G;
+      if (row < re_bin) {
+        const uint32_t s0 = ld_stream(a.sw.row_ptr + row);
+        rs[h] = s0;
+        len[h] = ld_stream(a.sw.row_ptr + row + 1) - s0;
+      }
+    }
+  }
+}
+
+template <int G>
+__device__ __forceinline__ void group_ids(const BinnedArgs& a, const uint32_t (&rs)[2], const uint32_t (&len)[2], int sub,
+                                          uint32_t (&id)[2][4]) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t o = (uint32_t)sub + (uint32_t)q * G;
+      id[h][q] = (o < len[h]) ? ld_stream(a.sw.col + rs[h] + o) : 0u;
+    }
+}
+
+// G-bins: a unit is 2 * 32/G consecutive rows, G lanes per row, each lane two
+// rows and at most 4 entries of each.
+template <bool HOT, int G>
+__device__ __forceinline__ double group_bin(const BinnedArgs& a, const Src& src, float* __restrict__ cout, uint32_t rb,
+                                            uint32_t re_bin, uint32_t nunits, uint32_t w, uint32_t nwarps, int lane) {
+  constexpr uint32_t PER = 32 / G;
+  if (w >= nunits) return 0.0;
+  const int sub = lane & (G - 1);
+  uint32_t  rs[2], len[2], nrs[2], nlen[2], id[2][4];
+  group_bounds<G>(a, rb, re_bin, w, nunits, lane, rs, len);
+  group_ids<G>(a, rs, len, sub, id);
+  group_bounds<G>(a, rb, re_bin, w + nwarps, nunits, lane, nrs, nlen);
+  double res = 0.0;
+#pragma unroll 1
+  for (; w < nunits; w += nwarps) {
+    uint32_t row[2], dg[2];
+    float    old[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      row[h] = rb + w * (2u * PER) + (uint32_t)h * PER + (uint32_t)lane / G;
+      const bool mine = row[h] < re_bin && sub == 0;
+      old[h] = mine ? ld_stream(a.sw.rank + row[h]) : 0.f;
+      dg[h] = mine ? ld_stream(a.sw.deg + row[h]) : 1u;
+    }
+    float v[2][4];
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        v[h][q] = ((uint32_t)sub + (uint32_t)q * G < len[h]) ? gather_one<HOT>(src, id[h][q]) : 0.f;
+    // the next unit's column ids, the bounds of the unit after it
+    group_ids<G>(a, nrs, nlen, sub, id);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      rs[h] = nrs[h];
+      len[h] = nlen[h];
+    }
+    group_bounds<G>(a, rb, re_bin, w + 2u * nwarps, nunits, lane, nrs, nlen);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      float acc = 0.f;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc += v[h][q];
+#pragma unroll
+      for (int off = G / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(kFullMask, acc, off);
+      if (row[h] < re_bin && sub == 0) res += binned_update(a, cout, row[h], acc, old[h], dg[h], src.pol);
+    }
+  }
+  return res;
+}
+
+template <int NT, bool HOT, bool PIPE>
 __global__ void __launch_bounds__(NT, 1024 / NT) pr_binned_sweep_kernel(const BinnedArgs a) {
   constexpr int     NW = NT / 32;
   __shared__ double s_red[NW];
@@ -209,7 +388,30 @@ __global__ void __launch_bounds__(NT, 1024 / NT) pr_binned_sweep_kernel(const Bi
 
   const uint32_t nwarps = gridDim.x * NW, gwarp = blockIdx.x * NW + warp;
   const uint32_t units = a.num_chunks + a.bin_warp_end[kNumBins - 1];
-  for (uint32_t u = gwarp; u < units; u += nwarps) {
+  if constexpr (PIPE) {
+    res += range_bin<HOT, true>(a, src, cout, 0u, a.num_chunks, gwarp, nwarps, lane);
+    uint32_t begin = a.num_chunks;  // flat index of the bin's first unit
+#pragma unroll 1
+    for (int b = 0; b < kNumBins; ++b) {
+      const uint32_t nu = a.bin_warp_end[b] - (b ? a.bin_warp_end[b - 1] : 0u);
+      const uint32_t w0 = first_unit(gwarp, nwarps, begin);
+      const uint32_t rb = a.bin_row_begin[b], re = a.bin_row_end[b];
+      switch (b) {
+        case 0: res += range_bin<HOT, false>(a, src, cout, rb, nu, w0, nwarps, lane); break;
+        case 1: res += group_bin<HOT, 32>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
+        case 2: res += group_bin<HOT, 16>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
+        case 3: res += group_bin<HOT, 8>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
+        case 4: res += group_bin<HOT, 4>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
+        case 5: res += group_bin<HOT, 2>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
+        case 6: res += group_bin<HOT, 1>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
+        default:
+          for (uint32_t w = w0; w < nu; w += nwarps) res += empty_rows(a, cout, rb + w * 128u, re, lane, src.pol);
+          break;
+      }
+      begin += nu;
+    }
+  }
+  for (uint32_t u = PIPE ? units : gwarp; u < units; u += nwarps) {
     if (u < a.num_chunks) {
       long_chunk<HOT>(a, src, u, lane);
       continue;
@@ -221,11 +423,12 @@ __global__ void __launch_bounds__(NT, 1024 / NT) pr_binned_sweep_kernel(const Bi
     const uint32_t rb = a.bin_row_begin[b], re = a.bin_row_end[b];
     switch (b) {
       case 0: res += warp_row<HOT>(a, src, cout, rb + wb, re, lane); break;
-      case 1: res += group_rows<HOT, 16>(a, src, cout, rb + wb * 4, re, lane); break;
-      case 2: res += group_rows<HOT, 8>(a, src, cout, rb + wb * 8, re, lane); break;
-      case 3: res += group_rows<HOT, 4>(a, src, cout, rb + wb * 16, re, lane); break;
-      case 4: res += group_rows<HOT, 2>(a, src, cout, rb + wb * 32, re, lane); break;
-      case 5: res += group_rows<HOT, 1>(a, src, cout, rb + wb * 64, re, lane); break;
+      case 1: res += group_rows<HOT, 32>(a, src, cout, rb + wb * 2, re, lane); break;
+      case 2: res += group_rows<HOT, 16>(a, src, cout, rb + wb * 4, re, lane); break;
+      case 3: res += group_rows<HOT, 8>(a, src, cout, rb + wb * 8, re, lane); break;
+      case 4: res += group_rows<HOT, 4>(a, src, cout, rb + wb * 16, re, lane); break;
+      case 5: res += group_rows<HOT, 2>(a, src, cout, rb + wb * 32, re, lane); break;
+      case 6: res += group_rows<HOT, 1>(a, src, cout, rb + wb * 64, re, lane); break;
       default: res += empty_rows(a, cout, rb + wb * 128, re, lane, src.pol); break;
     }
   }
@@ -312,14 +515,15 @@ __device__ uint32_t first_row_at_most(const uint32_t* row_ptr, uint32_t n, uint3
   return lo;
 }
 
-// out[0] = end of long rows, out[1..7] = ends of bins 0..6; flag = 1 if the
-// lengths are not non-increasing (then the binned sweep cannot be used).
+// out[0] = end of long rows, out[1..kNumBins] = ends of bins 0..kNumBins-1;
+// flag = 1 if the lengths are not non-increasing (then the binned sweep cannot
+// be used).
 __global__ void bin_bounds_kernel(const uint32_t* __restrict__ row_ptr, uint32_t n, uint32_t* out,
                                   unsigned int* unsorted) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    const uint32_t limits[8] = {kLongRow, 64, 32, 16, 8, 4, 0, 0};
-    for (int b = 0; b < 7; ++b) out[b] = first_row_at_most(row_ptr, n, limits[b]);
-    out[7] = n;
+    const uint32_t limits[kNumBins] = {kLongRow, 128, 64, 32, 16, 8, 4, 0};
+    for (int b = 0; b < kNumBins; ++b) out[b] = first_row_at_most(row_ptr, n, limits[b]);
+    out[kNumBins] = n;
   }
   unsigned int bad = 0;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i + 1 < n; i += gridDim.x * blockDim.x)
@@ -366,27 +570,34 @@ static int binned_hot_smem_bytes() {
 uint32_t binned_hot_capacity() { return (uint32_t)(binned_hot_smem_bytes() / 4) & ~3u; }
 
 cudaError_t configure_binned_kernels() {
-  return cudaFuncSetAttribute(pr_binned_sweep_kernel<kBinnedHotThreads, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              binned_hot_smem_bytes());
+  cudaError_t e = cudaFuncSetAttribute(pr_binned_sweep_kernel<kBinnedHotThreads, true, false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, binned_hot_smem_bytes());
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(pr_binned_sweep_kernel<kBinnedHotThreads, true, true>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, binned_hot_smem_bytes());
 }
 
 int binned_sweep_grid(int sms, bool hot) {
   if (hot) return sms;
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pr_binned_sweep_kernel<kBinnedThreads, false>, kBinnedThreads, 0) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pr_binned_sweep_kernel<kBinnedThreads, false, true>, kBinnedThreads, 0) !=
           cudaSuccess ||
       nb < 1)
     nb = 1;
   return sms * nb;
 }
 
-static void* binned_fn(bool hot) {
-  return hot ? (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true> : (void*)pr_binned_sweep_kernel<kBinnedThreads, false>;
+static void* binned_fn(bool hot, bool pipe) {
+  if (pipe)
+    return hot ? (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, true>
+               : (void*)pr_binned_sweep_kernel<kBinnedThreads, false, true>;
+  return hot ? (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, false>
+             : (void*)pr_binned_sweep_kernel<kBinnedThreads, false, false>;
 }
 
 cudaError_t launch_binned_sweep(const BinnedArgs& a, bool hot, int sweep_grid, int finish_grid, cudaStream_t s) {
   void*       args[] = {(void*)&a};
-  cudaError_t e = cudaLaunchKernel(binned_fn(hot), dim3((unsigned)sweep_grid), dim3(hot ? kBinnedHotThreads : kBinnedThreads),
+  cudaError_t e = cudaLaunchKernel(binned_fn(hot, a.pipe != 0), dim3((unsigned)sweep_grid), dim3(hot ? kBinnedHotThreads : kBinnedThreads),
                                    args, hot ? (size_t)a.smem_ids * 4u : 0u, s);
   if (e != cudaSuccess) return e;
   pr_binned_finish_kernel<<<finish_grid, 256, 0, s>>>(a);
@@ -396,7 +607,7 @@ cudaError_t launch_binned_sweep(const BinnedArgs& a, bool hot, int sweep_grid, i
 cudaError_t add_binned_nodes(cudaGraph_t body, const BinnedArgs& a, bool hot, int sweep_grid, int finish_grid) {
   void*                args[] = {(void*)&a};
   cudaKernelNodeParams kp = {};
-  kp.func = binned_fn(hot);
+  kp.func = binned_fn(hot, a.pipe != 0);
   kp.gridDim = dim3((unsigned)sweep_grid);
   kp.blockDim = dim3(hot ? kBinnedHotThreads : kBinnedThreads);
   kp.sharedMemBytes = hot ? (unsigned)a.smem_ids * 4u : 0u;
