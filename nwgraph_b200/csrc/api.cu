@@ -145,9 +145,9 @@ static int setup_binned(nwgpu_graph* g) {
   const uint32_t n = (uint32_t)g->n;
   uint32_t*      d_out = nullptr;
   unsigned int*  d_bad = nullptr;
-  CK(pool_alloc((void**)&d_out, (kNumBins + 1) * sizeof(uint32_t) + sizeof(unsigned int), g->stream), "cudaMalloc(bins)");
-  d_bad = reinterpret_cast<unsigned int*>(d_out + kNumBins + 1);
-  uint32_t     h_out[kNumBins + 1];
+  CK(pool_alloc((void**)&d_out, (kNumBins + 2) * sizeof(uint32_t) + sizeof(unsigned int), g->stream), "cudaMalloc(bins)");
+  d_bad = reinterpret_cast<unsigned int*>(d_out + kNumBins + 2);
+  uint32_t     h_out[kNumBins + 2];
   unsigned int h_bad = 0;
   cudaError_t  e = cudaMemsetAsync(d_bad, 0, sizeof(unsigned int), g->stream);
   if (e == cudaSuccess) e = launch_bin_bounds(g->g.row_ptr, n, d_out, d_bad, g->sms, g->stream);
@@ -160,6 +160,7 @@ static int setup_binned(nwgpu_graph* g) {
   BinnedArgs&    b = g->bin;
   const uint32_t nlong = h_out[0];
   b.num_long_rows = nlong;
+  b.num_big_rows = h_out[kNumBins + 1] < nlong ? h_out[kNumBins + 1] : nlong;
   // rows one warp handles in each bin (pr_binned.cu: warp_row, group_rows<G>, empty_rows)
   static const uint32_t rows_per_warp[kNumBins] = {1, 2, 4, 8, 16, 32, 64, 128};
   uint32_t              warps = 0;
@@ -215,9 +216,8 @@ static int setup_binned(nwgpu_graph* g) {
     b.smem_ids = 0;
     b.l1_ids = g->hot_ids;
   }
-  b.pipe = env_int("NWGPU_BINNED_PIPE", 1) ? 1u : 0u;
   g->bin_sweep_grid = binned_sweep_grid(g->sms, g->bin_hot);
-  g->bin_finish_grid = g->sms * 2;
+  g->bin_finish_grid = binned_finish_grid(b);
   g->binned = true;
   return NWGPU_OK;
 }

@@ -12,6 +12,7 @@ constexpr int      kNumBins = 8;     // warp per row, then G = 32, 16, 8, 4, 2, 
 struct BinnedArgs {
   SweepArgs       sw;                     // row_ptr / col / vectors / state / loop control
   uint32_t        num_long_rows;          // rows [0, num_long_rows) are chunked
+  uint32_t        num_big_rows;           // rows [0, num_big_rows) have more than 32 chunks
   uint32_t        num_chunks;
   const uint32_t* row_first_chunk;        // num_long_rows + 1
   const uint32_t* chunk_row;              // num_chunks
@@ -24,7 +25,6 @@ struct BinnedArgs {
   // bin 7: empty rows
   uint32_t        smem_ids;               // hot variant: contrib[0, smem_ids) is staged in shared memory
   uint32_t        l1_ids;                 // ids in [smem_ids, l1_ids) are gathered through L1 (evict-last)
-  uint32_t        pipe;                   // 1: software-pipelined walk of the bins
 };
 
 // Launch shapes of the binned sweep: 256-thread CTAs, four per SM, hub ids
@@ -40,6 +40,7 @@ cudaError_t launch_chunk_fill(const uint32_t* first, uint32_t nlong, uint32_t* c
 int         binned_sweep_grid(int sms, bool hot);
 uint32_t    binned_hot_capacity();  // ids the hot variant can stage (a multiple of 4)
 cudaError_t configure_binned_kernels();
+int         binned_finish_grid(const BinnedArgs& a);
 cudaError_t launch_binned_sweep(const BinnedArgs& a, bool hot, int sweep_grid, int finish_grid, cudaStream_t s);
 cudaError_t add_binned_nodes(cudaGraph_t body, const BinnedArgs& a, bool hot, int sweep_grid, int finish_grid);
 

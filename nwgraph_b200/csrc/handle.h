@@ -72,7 +72,7 @@ struct nwgpu_graph {
   uint32_t*         bin_first = nullptr;
   uint32_t*         bin_chunk_row = nullptr;
   float*            bin_chunk_part = nullptr;
-  int               bin_sweep_grid = 0, bin_finish_grid = 0;
+  int               bin_sweep_grid = 0, bin_finish_grid = 1;
   int          finish_grid = 1;  // finishing-kernel CTAs
   uint64_t     device_bytes = 0;
 

@@ -4,8 +4,8 @@
 // After relabelling, rows of similar length are contiguous, so the sweep is
 // split into bins without any per-row indirection:
 //   long   len > kLongRow     : chunks of kChunk entries, one warp per chunk;
-//                               per-chunk FP32 partials summed in chunk order by
-//                               pr_binned_finish_kernel
+//                               pr_binned_finish_kernel sums each row's chunk
+//                               partials in chunk order
 //   bin 0  128 < len <= kLongRow: one warp per row, lanes stride the row
 //   G = 32, 16, 8, 4, 2, 1      : rows of (G*2, G*4] entries (G = 1: 1..4),
 //                               G lanes per row, two rows per lane group,
@@ -14,12 +14,21 @@
 // Every lane's entries are summed in a fixed order and combined by a fixed
 // xor-shuffle tree, so ranks are bit-reproducible. Column ids stream through
 // (coalesced, evict-first); contributions are gathered with 8 loads in flight
-// per lane.
+// per lane. Each warp walks its units software-pipelined: while the gathers of
+// one step are in flight, the column ids of the next step and the row bounds
+// of the unit after it are already loading.
+//
+// pr_binned_finish_kernel, launched right after, finishes the long rows; its
+// last CTA to finish (a ticket) reduces all FP64 residual partials in a fixed
+// order and runs the convergence test on the device. Completing a long row
+// inside the sweep (the warp of its last chunk) needs a memory fence per
+// chunk, and a fence drains the warp's loads in flight: measured slower than
+// the second, short kernel.
 //
 // Where the gathered values come from (ids are in descending-degree order, so
 // small ids are the hubs):
-//   HOT = false: ids < l1_ids through L1 with an evict-last policy, the rest
-//                with L1::no_allocate;
+//   HOT = false: 256-thread CTAs, four per SM; ids < l1_ids through L1 with
+//                an evict-last policy, the rest with L1::no_allocate;
 //   HOT = true:  one 1024-thread CTA per SM copies contrib[0, smem_ids) into
 //                shared memory at the start of the sweep and gathers those ids
 //                from there; [smem_ids, l1_ids) through L1, the rest
@@ -71,100 +80,6 @@ __device__ __forceinline__ double binned_epilogue(const BinnedArgs& a, float* __
   return binned_update(a, cout, r, z, ld_stream(a.sw.rank + r), ld_stream(a.sw.deg + r), pol);
 }
 
-// Sum of entries [k, k_end) taken U at a time, lanes `stride` apart.
-template <bool HOT, int U>
-__device__ __forceinline__ float strided_sum(const BinnedArgs& a, const Src& src, uint32_t k, uint32_t k_end,
-                                             uint32_t stride) {
-  float acc = 0.f;
-#pragma unroll 1
-  for (; k < k_end; k += U * stride) {
-    uint32_t id[U];
-    float    v[U];
-#pragma unroll
-    for (int q = 0; q < U; ++q) id[q] = (k + q * stride < k_end) ? ld_stream(a.sw.col + k + q * stride) : 0u;
-#pragma unroll
-    for (int q = 0; q < U; ++q) v[q] = (k + q * stride < k_end) ? gather_one<HOT>(src, id[q]) : 0.f;
-#pragma unroll
-    for (int q = 0; q < U; ++q) acc += v[q];
-  }
-  return acc;
-}
-
-// One warp: a chunk of a long row.
-template <bool HOT>
-__device__ __forceinline__ void long_chunk(const BinnedArgs& a, const Src& src, uint32_t c, int lane) {
-  const uint32_t row = a.chunk_row[c];
-  const uint32_t rs = a.sw.row_ptr[row], re = a.sw.row_ptr[row + 1];
-  const uint32_t k0 = rs + (c - a.row_first_chunk[row]) * kChunk;
-  const uint32_t k1 = min(re, k0 + kChunk);
-  float          acc = strided_sum<HOT, 8>(a, src, k0 + lane, k1, 32u);
-  acc = warp_sum_lane0(acc);
-  if (lane == 0) a.chunk_part[c] = acc;
-}
-
-// One warp: one row of 129..kLongRow entries.
-template <bool HOT>
-__device__ __forceinline__ double warp_row(const BinnedArgs& a, const Src& src, float* __restrict__ cout, uint32_t row,
-                                           uint32_t row_end, int lane) {
-  if (row >= row_end) return 0.0;  // uniform across the warp
-  const uint32_t rs = a.sw.row_ptr[row], re = a.sw.row_ptr[row + 1];
-  float          old = 0.f;
-  uint32_t       dg = 1u;
-  if (lane == 0) {
-    old = ld_stream(a.sw.rank + row);
-    dg = ld_stream(a.sw.deg + row);
-  }
-  float acc = strided_sum<HOT, 8>(a, src, rs + lane, re, 32u);
-  acc = warp_sum_lane0(acc);
-  return (lane == 0) ? binned_update(a, cout, row, acc, old, dg, src.pol) : 0.0;
-}
-
-// One warp of a G-bin: 2 * 32/G rows, G lanes per row, each lane two rows and
-// at most 4 entries of each (8 gathers in flight).
-template <bool HOT, int G>
-__device__ __forceinline__ double group_rows(const BinnedArgs& a, const Src& src, float* __restrict__ cout, uint32_t row0,
-                                             uint32_t row_end, int lane) {
-  constexpr uint32_t PER = 32 / G;  // rows per half
-  const int          sub = lane & (G - 1);
-  uint32_t           row[2], rs[2], re[2];
-  float              old[2];
-  uint32_t           dg[2];
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    row[h] = row0 + h * PER + (uint32_t)(lane / G);
-    const bool live = row[h] < row_end;
-    rs[h] = live ? a.sw.row_ptr[row[h]] : 0u;
-    re[h] = live ? a.sw.row_ptr[row[h] + 1] : 0u;
-    old[h] = (live && sub == 0) ? ld_stream(a.sw.rank + row[h]) : 0.f;
-    dg[h] = (live && sub == 0) ? ld_stream(a.sw.deg + row[h]) : 1u;
-  }
-  uint32_t id[2][4];
-  float    v[2][4];
-#pragma unroll
-  for (int h = 0; h < 2; ++h)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const uint32_t k = rs[h] + sub + q * G;
-      id[h][q] = (k < re[h]) ? ld_stream(a.sw.col + k) : 0u;
-    }
-#pragma unroll
-  for (int h = 0; h < 2; ++h)
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-      v[h][q] = (rs[h] + sub + q * G < re[h]) ? gather_one<HOT>(src, id[h][q]) : 0.f;
-  double res = 0.0;
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    float acc = 0.f;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) acc += v[h][q];
-#pragma unroll
-    for (int off = G / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(kFullMask, acc, off);
-    if (row[h] < row_end && sub == 0) res += binned_update(a, cout, row[h], acc, old[h], dg[h], src.pol);
-  }
-  return res;
-}
-
 // Rows without entries: four rows per lane.
 __device__ __forceinline__ double empty_rows(const BinnedArgs& a, float* __restrict__ cout, uint32_t row0,
                                              uint32_t row_end, int lane, uint64_t pol) {
@@ -186,14 +101,12 @@ __device__ __forceinline__ double empty_rows(const BinnedArgs& a, float* __restr
 }
 
 // ---------------------------------------------------------------------------
-// Software-pipelined bin walkers (PIPE = true). A warp takes the units of one
-// bin at a time, in the same order as the flat grid-stride walk above (unit
-// u of the flat space goes to warp u mod nwarps). While the gathers of one
-// step are in flight, the column ids of the next step and the row bounds of
-// the unit after it are already loading: a warp keeps loads of two or three
-// stages outstanding instead of waiting through row_ptr -> col -> contrib in
-// turn. Every lane sums the same entries in the same order as the plain walk,
-// so the results are bitwise equal.
+// Bin walkers. Units are numbered in one flat space (long-row chunks, then
+// bins 0..7) and unit u goes to warp u mod nwarps; a warp takes the units of
+// one bin at a time. While the gathers of one step are in flight, the column
+// ids of the next step and the row bounds of the unit after it are already
+// loading: a warp keeps loads of two or three stages outstanding instead of
+// waiting through row_ptr -> col -> contrib in turn.
 // ---------------------------------------------------------------------------
 // First unit (bin-local index) of warp gwarp in a bin that starts at flat unit `begin`.
 __device__ __forceinline__ uint32_t first_unit(uint32_t gwarp, uint32_t nwarps, uint32_t begin) {
@@ -210,13 +123,14 @@ __device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src,
   constexpr int      U = 8;
   constexpr uint32_t STEP = U * 32;
   if (w >= nunits) return 0.0;
-  auto bounds = [&](uint32_t unit, uint32_t& k0, uint32_t& k1) {
+  auto bounds = [&](uint32_t unit, uint32_t& k0, uint32_t& k1, uint32_t& row) {
     if (CHUNK) {
-      const uint32_t row = a.chunk_row[unit];
+      row = a.chunk_row[unit];
       const uint32_t rs = a.sw.row_ptr[row], re = a.sw.row_ptr[row + 1];
       k0 = rs + (unit - a.row_first_chunk[row]) * kChunk;
       k1 = min(re, k0 + kChunk);
     } else {
+      row = rb + unit;
       k0 = ld_stream(a.sw.row_ptr + rb + unit);
       k1 = ld_stream(a.sw.row_ptr + rb + unit + 1);
     }
@@ -228,17 +142,17 @@ __device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src,
       dst[q] = (k < end) ? ld_stream(a.sw.col + k) : 0u;
     }
   };
-  uint32_t k0, k1, nk0 = 0, nk1 = 0;
-  bounds(w, k0, k1);
-  if (w + nwarps < nunits) bounds(w + nwarps, nk0, nk1);
+  uint32_t k0, k1, row, nk0 = 0, nk1 = 0, nrow = 0;
+  bounds(w, k0, k1, row);
+  if (w + nwarps < nunits) bounds(w + nwarps, nk0, nk1, nrow);
   uint32_t id[U];
   uint32_t base = k0;
   load_ids(base, k1, id);
   float    old = 0.f;
   uint32_t dg = 1u;
   if (!CHUNK && lane == 0) {
-    old = ld_stream(a.sw.rank + rb + w);
-    dg = ld_stream(a.sw.deg + rb + w);
+    old = ld_stream(a.sw.rank + row);
+    dg = ld_stream(a.sw.deg + row);
   }
   float  acc = 0.f;
   double res = 0.0;
@@ -263,16 +177,17 @@ __device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src,
       if (CHUNK) {
         if (lane == 0) a.chunk_part[w] = z;
       } else if (lane == 0) {
-        res += binned_update(a, cout, rb + w, z, old, dg, src.pol);
+        res += binned_update(a, cout, row, z, old, dg, src.pol);
       }
       acc = 0.f;
       w += nwarps;
       if (w >= nunits) break;
       k1 = nk1;
-      if (w + nwarps < nunits) bounds(w + nwarps, nk0, nk1);
+      row = nrow;
+      if (w + nwarps < nunits) bounds(w + nwarps, nk0, nk1, nrow);
       if (!CHUNK && lane == 0) {
-        old = ld_stream(a.sw.rank + rb + w);
-        dg = ld_stream(a.sw.deg + rb + w);
+        old = ld_stream(a.sw.rank + row);
+        dg = ld_stream(a.sw.deg + row);
       }
     }
     base = nbase;
@@ -363,7 +278,7 @@ __device__ __forceinline__ double group_bin(const BinnedArgs& a, const Src& src,
   return res;
 }
 
-template <int NT, bool HOT, bool PIPE>
+template <int NT, bool HOT>
 __global__ void __launch_bounds__(NT, 1024 / NT) pr_binned_sweep_kernel(const BinnedArgs a) {
   constexpr int     NW = NT / 32;
   __shared__ double s_red[NW];
@@ -384,54 +299,30 @@ __global__ void __launch_bounds__(NT, 1024 / NT) pr_binned_sweep_kernel(const Bi
     src.s_hot = reinterpret_cast<const float*>(s_hot4);
     src.smem_ids = a.smem_ids;
   }
-  double res = 0.0;
-
+  double         res = 0.0;
   const uint32_t nwarps = gridDim.x * NW, gwarp = blockIdx.x * NW + warp;
-  const uint32_t units = a.num_chunks + a.bin_warp_end[kNumBins - 1];
-  if constexpr (PIPE) {
-    res += range_bin<HOT, true>(a, src, cout, 0u, a.num_chunks, gwarp, nwarps, lane);
-    uint32_t begin = a.num_chunks;  // flat index of the bin's first unit
+  res += range_bin<HOT, true>(a, src, cout, 0u, a.num_chunks, gwarp, nwarps, lane);
+  uint32_t begin = a.num_chunks;  // flat index of the bin's first unit
 #pragma unroll 1
-    for (int b = 0; b < kNumBins; ++b) {
-      const uint32_t nu = a.bin_warp_end[b] - (b ? a.bin_warp_end[b - 1] : 0u);
-      const uint32_t w0 = first_unit(gwarp, nwarps, begin);
-      const uint32_t rb = a.bin_row_begin[b], re = a.bin_row_end[b];
-      switch (b) {
-        case 0: res += range_bin<HOT, false>(a, src, cout, rb, nu, w0, nwarps, lane); break;
-        case 1: res += group_bin<HOT, 32>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
-        case 2: res += group_bin<HOT, 16>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
-        case 3: res += group_bin<HOT, 8>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
-        case 4: res += group_bin<HOT, 4>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
-        case 5: res += group_bin<HOT, 2>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
-        case 6: res += group_bin<HOT, 1>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
-        default:
-          for (uint32_t w = w0; w < nu; w += nwarps) res += empty_rows(a, cout, rb + w * 128u, re, lane, src.pol);
-          break;
-      }
-      begin += nu;
-    }
-  }
-  for (uint32_t u = PIPE ? units : gwarp; u < units; u += nwarps) {
-    if (u < a.num_chunks) {
-      long_chunk<HOT>(a, src, u, lane);
-      continue;
-    }
-    const uint32_t w = u - a.num_chunks;  // warp index in the flat bin space
-    int            b = 0;
-    while (w >= a.bin_warp_end[b]) ++b;   // uniform across the warp
-    const uint32_t wb = w - (b ? a.bin_warp_end[b - 1] : 0u);
+  for (int b = 0; b < kNumBins; ++b) {
+    const uint32_t nu = a.bin_warp_end[b] - (b ? a.bin_warp_end[b - 1] : 0u);
+    const uint32_t w0 = first_unit(gwarp, nwarps, begin);
     const uint32_t rb = a.bin_row_begin[b], re = a.bin_row_end[b];
     switch (b) {
-      case 0: res += warp_row<HOT>(a, src, cout, rb + wb, re, lane); break;
-      case 1: res += group_rows<HOT, 32>(a, src, cout, rb + wb * 2, re, lane); break;
-      case 2: res += group_rows<HOT, 16>(a, src, cout, rb + wb * 4, re, lane); break;
-      case 3: res += group_rows<HOT, 8>(a, src, cout, rb + wb * 8, re, lane); break;
-      case 4: res += group_rows<HOT, 4>(a, src, cout, rb + wb * 16, re, lane); break;
-      case 5: res += group_rows<HOT, 2>(a, src, cout, rb + wb * 32, re, lane); break;
-      case 6: res += group_rows<HOT, 1>(a, src, cout, rb + wb * 64, re, lane); break;
-      default: res += empty_rows(a, cout, rb + wb * 128, re, lane, src.pol); break;
+      case 0: res += range_bin<HOT, false>(a, src, cout, rb, nu, w0, nwarps, lane); break;
+      case 1: res += group_bin<HOT, 32>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
+      case 2: res += group_bin<HOT, 16>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
+      case 3: res += group_bin<HOT, 8>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
+      case 4: res += group_bin<HOT, 4>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
+      case 5: res += group_bin<HOT, 2>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
+      case 6: res += group_bin<HOT, 1>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
+      default:
+        for (uint32_t w = w0; w < nu; w += nwarps) res += empty_rows(a, cout, rb + w * 128u, re, lane, src.pol);
+        break;
     }
+    begin += nu;
   }
+
   res = warp_sum_lane0(res);
   if (lane == 0) s_red[warp] = res;
   __syncthreads();
@@ -443,8 +334,11 @@ __global__ void __launch_bounds__(NT, 1024 / NT) pr_binned_sweep_kernel(const Bi
   }
 }
 
-// Long rows: sum the chunk partials in chunk order, run the epilogue; then the
-// residual reduction and the device-side convergence test.
+// Long rows, after the sweep: rows [0, num_big_rows) have more than 32 chunks
+// and get a warp each (lane-strided partial sums, fixed tree); the other long
+// rows get a thread each (partials in chunk order). Then the residual
+// reduction over the sweep's and this kernel's CTA partials in a fixed order,
+// and the device-side convergence test (page_rank.hpp:125-134).
 __global__ void __launch_bounds__(256) pr_binned_finish_kernel(const BinnedArgs a) {
   __shared__ double s_red[8];
   __shared__ int    s_last;
@@ -454,14 +348,23 @@ __global__ void __launch_bounds__(256) pr_binned_finish_kernel(const BinnedArgs 
   float* __restrict__ cout = (it & 1ull) ? a.sw.contrib0 : a.sw.contrib1;
   const uint64_t pol = policy_evict_last();
   const int      tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t gt = blockIdx.x * 256u + (uint32_t)tid, gw = gt / 32u;
   double         res = 0.0;
-  // one warp per long row: lane-strided partial sums, fixed tree
-  for (uint32_t r = blockIdx.x * 8 + warp; r < a.num_long_rows; r += gridDim.x * 8) {
-    const uint32_t c0 = a.row_first_chunk[r], c1 = a.row_first_chunk[r + 1];
+  if (gw < a.num_big_rows) {
+    const uint32_t c0 = a.row_first_chunk[gw], c1 = a.row_first_chunk[gw + 1];
     float          p = 0.f;
-    for (uint32_t c = c0 + lane; c < c1; c += 32) p += __ldcg(a.chunk_part + c);
+    for (uint32_t c = c0 + (uint32_t)lane; c < c1; c += 32u) p += __ldcg(a.chunk_part + c);
     p = warp_sum_lane0(p);
-    if (lane == 0) res += binned_epilogue(a, cout, r, p, pol);
+    if (lane == 0) res = binned_epilogue(a, cout, gw, p, pol);
+  } else {
+    const uint32_t r = a.num_big_rows + (gt - a.num_big_rows * 32u);
+    if (r < a.num_long_rows) {
+      const uint32_t c0 = a.row_first_chunk[r], c1 = a.row_first_chunk[r + 1];
+      float          p = 0.f;
+#pragma unroll 4
+      for (uint32_t c = c0; c < c1; ++c) p += __ldcg(a.chunk_part + c);
+      res = binned_epilogue(a, cout, r, p, pol);
+    }
   }
   res = warp_sum_lane0(res);
   if (lane == 0) s_red[warp] = res;
@@ -472,14 +375,14 @@ __global__ void __launch_bounds__(256) pr_binned_finish_kernel(const BinnedArgs 
     for (int w = 0; w < 8; ++w) s += s_red[w];
     a.sw.res_part[a.sw.sweep_grid + blockIdx.x] = s;
     __threadfence();
-    s_last = (atomicAdd(&st->ticket, 1u) == gridDim.x - 1);
+    s_last = (atomicAdd(&st->ticket, 1u) == gridDim.x - 1u);
   }
   __syncthreads();
   if (!s_last || tid >= 32) return;
   __threadfence();
   const uint32_t parts = a.sw.sweep_grid + gridDim.x;
   double         e = 0.0;
-  for (uint32_t u = lane; u < parts; u += 32) e += __ldcg(a.sw.res_part + u);
+  for (uint32_t u = lane; u < parts; u += 32u) e += __ldcg(a.sw.res_part + u);
   e = warp_sum_lane0(e);
   if (lane == 0) {
     const unsigned long long done_iters = it + 1ull;
@@ -515,15 +418,16 @@ __device__ uint32_t first_row_at_most(const uint32_t* row_ptr, uint32_t n, uint3
   return lo;
 }
 
-// out[0] = end of long rows, out[1..kNumBins] = ends of bins 0..kNumBins-1;
-// flag = 1 if the lengths are not non-increasing (then the binned sweep cannot
-// be used).
+// out[0] = end of long rows, out[1..kNumBins] = ends of bins 0..kNumBins-1,
+// out[kNumBins + 1] = end of the rows of more than 32 chunks; flag = 1 if the
+// lengths are not non-increasing (then the binned sweep cannot be used).
 __global__ void bin_bounds_kernel(const uint32_t* __restrict__ row_ptr, uint32_t n, uint32_t* out,
                                   unsigned int* unsorted) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     const uint32_t limits[kNumBins] = {kLongRow, 128, 64, 32, 16, 8, 4, 0};
     for (int b = 0; b < kNumBins; ++b) out[b] = first_row_at_most(row_ptr, n, limits[b]);
     out[kNumBins] = n;
+    out[kNumBins + 1] = first_row_at_most(row_ptr, n, 32u * kChunk);  // rows of more than 32 chunks
   }
   unsigned int bad = 0;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i + 1 < n; i += gridDim.x * blockDim.x)
@@ -570,34 +474,33 @@ static int binned_hot_smem_bytes() {
 uint32_t binned_hot_capacity() { return (uint32_t)(binned_hot_smem_bytes() / 4) & ~3u; }
 
 cudaError_t configure_binned_kernels() {
-  cudaError_t e = cudaFuncSetAttribute(pr_binned_sweep_kernel<kBinnedHotThreads, true, false>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, binned_hot_smem_bytes());
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(pr_binned_sweep_kernel<kBinnedHotThreads, true, true>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, binned_hot_smem_bytes());
+  return cudaFuncSetAttribute(pr_binned_sweep_kernel<kBinnedHotThreads, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              binned_hot_smem_bytes());
 }
 
 int binned_sweep_grid(int sms, bool hot) {
   if (hot) return sms;
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pr_binned_sweep_kernel<kBinnedThreads, false, true>, kBinnedThreads, 0) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pr_binned_sweep_kernel<kBinnedThreads, false>, kBinnedThreads, 0) !=
           cudaSuccess ||
       nb < 1)
     nb = 1;
   return sms * nb;
 }
 
-static void* binned_fn(bool hot, bool pipe) {
-  if (pipe)
-    return hot ? (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, true>
-               : (void*)pr_binned_sweep_kernel<kBinnedThreads, false, true>;
-  return hot ? (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, false>
-             : (void*)pr_binned_sweep_kernel<kBinnedThreads, false, false>;
+static void* binned_fn(bool hot) {
+  return hot ? (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true> : (void*)pr_binned_sweep_kernel<kBinnedThreads, false>;
+}
+
+int binned_finish_grid(const BinnedArgs& a) {
+  const uint64_t threads = (uint64_t)a.num_big_rows * 32u + (a.num_long_rows - a.num_big_rows);
+  const uint64_t blocks = (threads + 255u) / 256u;
+  return blocks ? (int)blocks : 1;
 }
 
 cudaError_t launch_binned_sweep(const BinnedArgs& a, bool hot, int sweep_grid, int finish_grid, cudaStream_t s) {
   void*       args[] = {(void*)&a};
-  cudaError_t e = cudaLaunchKernel(binned_fn(hot, a.pipe != 0), dim3((unsigned)sweep_grid), dim3(hot ? kBinnedHotThreads : kBinnedThreads),
+  cudaError_t e = cudaLaunchKernel(binned_fn(hot), dim3((unsigned)sweep_grid), dim3(hot ? kBinnedHotThreads : kBinnedThreads),
                                    args, hot ? (size_t)a.smem_ids * 4u : 0u, s);
   if (e != cudaSuccess) return e;
   pr_binned_finish_kernel<<<finish_grid, 256, 0, s>>>(a);
@@ -607,7 +510,7 @@ cudaError_t launch_binned_sweep(const BinnedArgs& a, bool hot, int sweep_grid, i
 cudaError_t add_binned_nodes(cudaGraph_t body, const BinnedArgs& a, bool hot, int sweep_grid, int finish_grid) {
   void*                args[] = {(void*)&a};
   cudaKernelNodeParams kp = {};
-  kp.func = binned_fn(hot, a.pipe != 0);
+  kp.func = binned_fn(hot);
   kp.gridDim = dim3((unsigned)sweep_grid);
   kp.blockDim = dim3(hot ? kBinnedHotThreads : kBinnedThreads);
   kp.sharedMemBytes = hot ? (unsigned)a.smem_ids * 4u : 0u;
