@@ -3,7 +3,7 @@
 Launched by tests/test_multirank.py through torch.distributed.run, the way
 bench.py is launched for N > 1, but with the gloo backend: each rank reports
 per-rank timings that differ, takes the maximum over ranks with bench's own
-helper, and prints what it got as one JSON line.
+helper, and writes what it got to <outdir>/rank<r>.json.
 """
 import datetime
 import json
@@ -27,8 +27,9 @@ def main():
     e2e, = bench.max_over_ranks([50.0 * (rank + 1)], dist)
     dist.barrier()
     dist.destroy_process_group()
-    print(json.dumps({"rank": rank, "world": world, "total": total, "sweep": sweep, "e2e": e2e,
-                      "gteps": bench.job_gteps(world, 1_000_000, bench.SWEEPS, total / 10)}), flush=True)
+    with open(os.path.join(sys.argv[1], f"rank{rank}.json"), "w") as f:
+        json.dump({"rank": rank, "world": world, "total": total, "sweep": sweep, "e2e": e2e,
+                   "gteps": bench.job_gteps(world, 1_000_000, bench.SWEEPS, total / 10)}, f)
 
 
 if __name__ == "__main__":

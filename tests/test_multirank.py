@@ -34,11 +34,11 @@ def json_lines(text):
     return [json.loads(line) for line in text.splitlines() if line.startswith("{")]
 
 
-def test_step_times_are_max_over_ranks():
-    out = torchrun([os.path.join("tests", "multirank_worker.py")])
+def test_step_times_are_max_over_ranks(tmp_path):
+    out = torchrun([os.path.join("tests", "multirank_worker.py"), str(tmp_path)])
     assert out.returncode == 0, out.stderr[-2000:]
-    lines = json_lines(out.stdout)
-    assert sorted(d["rank"] for d in lines) == [0, 1]
+    lines = [json.loads((tmp_path / f"rank{r}.json").read_text()) for r in range(2)]
+    assert [d["rank"] for d in lines] == [0, 1]
     for d in lines:
         assert d["world"] == 2
         assert (d["total"], d["sweep"], d["e2e"]) == (110.0, 2.0, 100.0)
