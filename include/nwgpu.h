@@ -61,7 +61,7 @@ typedef struct nwgpu_graph nwgpu_graph;
 
 /* nwgpu_graph_create flags */
 #define NWGPU_GRAPH_DEVICE_PTRS 0x1u /* row_ptr / col / weights are device pointers (copied device-to-device) */
-#define NWGPU_GRAPH_TRANSPOSE 0x2u   /* also keep the out-row CSR (adjacency<0>) needed by nwgpu_pr_vjp */
+#define NWGPU_GRAPH_TRANSPOSE 0x2u   /* build the out-row CSR (adjacency<0>) of nwgpu_pr_vjp at creation, not on first use */
 #define NWGPU_GRAPH_NO_RELABEL 0x4u  /* keep the input vertex order on the device (default: hubs first) */
 
 /* Upload a CSR once (replaces the per-call use of graph.indices_ /
@@ -188,6 +188,32 @@ int nwgpu_ppr_batched(nwgpu_graph* g, const uint32_t* out_degree, const uint32_t
 int nwgpu_pr_run_noalloc(const uint32_t* row_ptr, const uint32_t* col, uint64_t n, uint64_t nnz,
                          const uint32_t* out_degree, float* ranks, float damping, float threshold, uint64_t max_iters,
                          void* stream, nwgpu_pr_stats* stats);
+
+/* Weighted PageRank (no counterpart in the reference, whose page_rank is
+ * unweighted). g must carry edge weights (nwgpu_graph_create's `weights`,
+ * w_k > 0 for the edge col[k] -> row of k) and be relabelled (the default).
+ * With s_j the out-weight sum of j:
+ *   r_i = (1 - d) t_i + d sum_{k in row i} w_k r_{col[k]} / s_{col[k]},  r(0) = t
+ * teleport[n] (input order) is a distribution over the vertices; NULL means
+ * uniform 1/n. The update, stopping rule (FP64 L1 change < threshold), leak
+ * semantics and argument conventions are nwgpu_pr_run's. */
+int nwgpu_wpr_run(nwgpu_graph* g, const float* teleport, float* ranks, float damping, float threshold, uint64_t max_iters,
+                  const nwgpu_pr_options* options, nwgpu_pr_stats* stats);
+
+/* Vector-Jacobian product of the weighted PageRank fixed point (no
+ * counterpart in the reference). For L = sum_v dL_dr[v] r_v, with ranks[n]
+ * the converged output of nwgpu_wpr_run (same damping), it solves the adjoint
+ *   l_j = dL_dr_j + d sum_{k: col[k] = j} (w_k / s_j) l_{row(k)}
+ * by implicit differentiation, with the same sweep over the out-row CSR (no
+ * forward iterates are stored), to an FP64 L1 change < threshold, then writes
+ *   dL_dt[v] = (1 - d) l_v                                (n, may be NULL)
+ *   dL_dw[k] = d r_j / s_j (l_i - q_j),  q_j = (l_j - dL_dr_j) / d
+ * for entry k of row i with col[k] = j, in the input entry order (nnz, may be
+ * NULL). stats describe the adjoint solve. The out-rows must be in the
+ * relabelled length order, which holds for symmetric graphs; otherwise
+ * NWGPU_ERR_UNSUPPORTED. */
+int nwgpu_pr_vjp(nwgpu_graph* g, const float* ranks, const float* dL_dr, float* dL_dw, float* dL_dt, float damping,
+                 float threshold, uint64_t max_iters, const nwgpu_pr_options* options, nwgpu_pr_stats* stats);
 
 /* Ask a running solve on g to stop at its next sweep boundary; the solve
  * returns NWGPU_ERR_ABORTED. Safe to call from another host thread. */

@@ -86,6 +86,10 @@ SIGNATURES = {
                                        C.c_uint64, _vp, C.POINTER(PrStats)]),
     "nwgpu_abort": (C.c_int, [_vp]),
     "nwgpu_release_cached_memory": (C.c_int, []),
+    "nwgpu_wpr_run": (C.c_int, [_vp, _vp, _vp, C.c_float, C.c_float, C.c_uint64, C.POINTER(PrOptions),
+                                C.POINTER(PrStats)]),
+    "nwgpu_pr_vjp": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_float, C.c_float, C.c_uint64, C.POINTER(PrOptions),
+                               C.POINTER(PrStats)]),
 }
 
 _lib = None

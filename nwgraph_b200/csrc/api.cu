@@ -107,7 +107,7 @@ int ensure_solve_buffers(nwgpu_graph* g) {
   CK(dalloc(g, &g->cpart, T + 1), "cudaMalloc(cpart)");
   CK(dalloc(g, &g->epart, T + 1), "cudaMalloc(epart)");
   const uint64_t parts = (uint64_t)g->grid + (uint64_t)g->finish_grid;
-  const uint64_t bparts = (uint64_t)g->bin_sweep_grid + (uint64_t)g->bin_finish_grid;
+  const uint64_t bparts = (uint64_t)g->plan.sweep_grid + (uint64_t)g->plan.finish_grid;
   CK(dalloc(g, &g->res_part, parts > bparts ? parts : bparts), "cudaMalloc(res_part)");
   CK(dalloc(g, &g->st, 1), "cudaMalloc(state)");
   CK(dalloc(g, &g->err_hist, g->err_cap), "cudaMalloc(err_hist)");
@@ -139,10 +139,12 @@ int load_degrees(nwgpu_graph* g, const uint32_t* out_degree, bool device_ptrs, c
   return NWGPU_OK;
 }
 
-// Bins of the degree-binned sweep: rows must be in non-increasing length
-// order (relabelled graphs); otherwise the merge-path sweep is used.
-static int setup_binned(nwgpu_graph* g) {
-  const uint32_t n = (uint32_t)g->n;
+// Bin tables of the CSR (row_ptr, n rows) for the degree-binned sweep. Rows
+// must be in non-increasing length order (relabelled graphs); otherwise
+// p->ok stays false and the caller uses another sweep. hot: the launch shape
+// with the hub contributions staged in shared memory.
+int build_bin_plan(nwgpu_graph* g, const uint32_t* row_ptr, uint64_t n64, bool hot, BinPlan* p) {
+  const uint32_t n = (uint32_t)n64;
   uint32_t*      d_out = nullptr;
   unsigned int*  d_bad = nullptr;
   CK(pool_alloc((void**)&d_out, (kNumBins + 2) * sizeof(uint32_t) + sizeof(unsigned int), g->stream), "cudaMalloc(bins)");
@@ -150,18 +152,18 @@ static int setup_binned(nwgpu_graph* g) {
   uint32_t     h_out[kNumBins + 2];
   unsigned int h_bad = 0;
   cudaError_t  e = cudaMemsetAsync(d_bad, 0, sizeof(unsigned int), g->stream);
-  if (e == cudaSuccess) e = launch_bin_bounds(g->g.row_ptr, n, d_out, d_bad, g->sms, g->stream);
+  if (e == cudaSuccess) e = launch_bin_bounds(row_ptr, n, d_out, d_bad, g->sms, g->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(h_out, d_out, sizeof(h_out), cudaMemcpyDeviceToHost, g->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(&h_bad, d_bad, sizeof(h_bad), cudaMemcpyDeviceToHost, g->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
   pool_free(d_out, g->stream);
   if (e != cudaSuccess) return cuda_fail(e, "bin bounds");
-  if (h_bad) return NWGPU_OK;  // lengths not sorted: stay on the merge-path sweep
-  BinnedArgs&    b = g->bin;
+  if (h_bad) return NWGPU_OK;  // lengths not sorted
+  BinnedArgs&    b = p->bin;
   const uint32_t nlong = h_out[0];
   b.num_long_rows = nlong;
   b.num_big_rows = h_out[kNumBins + 1] < nlong ? h_out[kNumBins + 1] : nlong;
-  // rows one warp handles in each bin (pr_binned.cu: warp_row, group_rows<G>, empty_rows)
+  // rows one warp handles in each bin (pr_binned.cu: range_bin, group_bin<G>, empty_rows)
   static const uint32_t rows_per_warp[kNumBins] = {1, 2, 4, 8, 16, 32, 64, 128};
   uint32_t              warps = 0;
   for (int i = 0; i < kNumBins; ++i) {
@@ -172,7 +174,7 @@ static int setup_binned(nwgpu_graph* g) {
     b.bin_warp_end[i] = warps;
   }
   // chunk table of the long rows
-  CK(dalloc(g, &g->bin_first, (uint64_t)nlong + 1), "cudaMalloc(chunk table)");
+  CK(dalloc(g, &p->first, (uint64_t)nlong + 1), "cudaMalloc(chunk table)");
   uint32_t num_chunks = 0;
   if (nlong) {
     uint32_t* cnt = nullptr;
@@ -180,56 +182,63 @@ static int setup_binned(nwgpu_graph* g) {
     size_t    tmp_bytes = 0;
     CK(pool_alloc_n(&cnt, (uint64_t)nlong + 1, g->stream), "cudaMalloc(chunk counts)");
     e = cudaMemsetAsync(cnt + nlong, 0, sizeof(uint32_t), g->stream);
-    if (e == cudaSuccess) e = launch_chunk_count(g->g.row_ptr, nlong, cnt, g->sms, g->stream);
-    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, cnt, g->bin_first, (int64_t)nlong + 1, g->stream);
+    if (e == cudaSuccess) e = launch_chunk_count(row_ptr, nlong, cnt, g->sms, g->stream);
+    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, cnt, p->first, (int64_t)nlong + 1, g->stream);
     if (e == cudaSuccess) e = pool_alloc(&tmp, tmp_bytes, g->stream);
-    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, cnt, g->bin_first, (int64_t)nlong + 1, g->stream);
+    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, cnt, p->first, (int64_t)nlong + 1, g->stream);
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(&num_chunks, g->bin_first + nlong, sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream);
+      e = cudaMemcpyAsync(&num_chunks, p->first + nlong, sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
     pool_free(cnt, g->stream);
     pool_free(tmp, g->stream);
     if (e != cudaSuccess) return cuda_fail(e, "chunk table");
   }
   b.num_chunks = num_chunks;
-  CK(dalloc(g, &g->bin_chunk_row, (uint64_t)num_chunks), "cudaMalloc(chunk rows)");
-  CK(dalloc(g, &g->bin_chunk_part, (uint64_t)num_chunks), "cudaMalloc(chunk partials)");
-  CK(launch_chunk_fill(g->bin_first, nlong, g->bin_chunk_row, g->sms, g->stream), "chunk fill");
+  CK(dalloc(g, &p->chunk_row, (uint64_t)num_chunks), "cudaMalloc(chunk rows)");
+  CK(dalloc(g, &p->chunk_part, (uint64_t)num_chunks), "cudaMalloc(chunk partials)");
+  CK(launch_chunk_fill(p->first, nlong, p->chunk_row, g->sms, g->stream), "chunk fill");
   CK(cudaStreamSynchronize(g->stream), "chunk fill");
-  b.row_first_chunk = g->bin_first;
-  b.chunk_row = g->bin_chunk_row;
-  b.chunk_part = g->bin_chunk_part;
-  // Variant: by default (or NWGPU_SWEEP=binned_hot) the hub contributions are
-  // staged in shared memory, NWGPU_HOT_IDS of them (default kHotSmemIds: half
-  // the SM's L1/shared capacity, which leaves L1 room for the next tier of
-  // hubs); NWGPU_SWEEP=binned keeps them in L1 only.
-  const char* which = getenv("NWGPU_SWEEP");
-  g->bin_hot = !which || !strcmp(which, "binned_hot");
-  if (g->bin_hot) {
+  b.row_first_chunk = p->first;
+  b.chunk_row = p->chunk_row;
+  b.chunk_part = p->chunk_part;
+  // Hot shape: the first NWGPU_HOT_IDS contributions (default kHotSmemIds:
+  // half the SM's L1/shared capacity, which leaves L1 room for the next tier
+  // of hubs) are staged in shared memory. Otherwise hubs go through L1 only.
+  p->hot = hot;
+  if (hot) {
     const uint32_t lim = binned_hot_capacity();
     const long     want = env_int("NWGPU_HOT_IDS", -1);
     uint32_t       cap = want >= 0 ? (uint32_t)want & ~3u : kHotSmemIds;
     if (cap > lim) cap = lim;
-    b.smem_ids = (uint32_t)(g->n < cap ? g->n & ~3ull : cap);
+    b.smem_ids = (uint32_t)(n64 < cap ? n64 & ~3ull : cap);
     b.l1_ids = b.smem_ids + (uint32_t)env_int("NWGPU_HOT_L1_IDS", (int)kHotL1Ids);
   } else {
     b.smem_ids = 0;
     b.l1_ids = g->hot_ids;
   }
-  g->bin_sweep_grid = binned_sweep_grid(g->sms, g->bin_hot);
-  g->bin_finish_grid = binned_finish_grid(b);
-  g->binned = true;
+  p->sweep_grid = binned_sweep_grid(g->sms, hot);
+  p->finish_grid = binned_finish_grid(b);
+  p->ok = true;
   return NWGPU_OK;
 }
 
-}  // namespace nwgpu
+void BinPlan::release(cudaStream_t s) {
+  pool_free(first, s);
+  pool_free(chunk_row, s);
+  pool_free(chunk_part, s);
+  *this = BinPlan();
+}
 
-namespace {
+// Sweep grid of a binned solve: the plan's, except the weighted and adjoint
+// sweeps, which always run in the hot launch shape.
+int binned_grid(nwgpu_graph* g, const BinPlan& p, int mode) {
+  return mode == kModePlain ? p.sweep_grid : binned_sweep_grid(g->sms, true);
+}
 
-BinnedArgs make_binned_args(nwgpu_graph* g, const SweepArgs& sw) {
-  BinnedArgs b = g->bin;
+BinnedArgs make_binned_args(nwgpu_graph* g, const BinPlan& p, const SweepArgs& sw, int mode) {
+  BinnedArgs b = p.bin;
   b.sw = sw;
-  b.sw.sweep_grid = (uint32_t)g->bin_sweep_grid;
+  b.sw.sweep_grid = (uint32_t)binned_grid(g, p, mode);
   return b;
 }
 
@@ -262,7 +271,7 @@ SweepArgs make_sweep_args(nwgpu_graph* g, float damping, float base, int telepor
   return a;
 }
 
-int build_loop_graph(nwgpu_graph* g, const SweepArgs& proto) {
+int build_loop_graph(nwgpu_graph* g, const SweepArgs& proto, const BinPlan* plan, int mode) {
   if (g->cg_exec) {
     cudaGraphExecDestroy(g->cg_exec);
     g->cg_exec = nullptr;
@@ -287,25 +296,33 @@ int build_loop_graph(nwgpu_graph* g, const SweepArgs& proto) {
   SweepArgs   a = proto;
   a.cond = cond;
   a.use_cond = 1;
-  if (g->binned)
-    CK(add_binned_nodes(body, make_binned_args(g, a), g->bin_hot, g->bin_sweep_grid, g->bin_finish_grid),
+  if (plan)
+    CK(add_binned_nodes(body, make_binned_args(g, *plan, a, mode), plan->hot, mode, binned_grid(g, *plan, mode),
+                        plan->finish_grid),
        "cudaGraphAddKernelNode(binned)");
   else
     CK(add_pr_sweep_nodes(body, a, g->variant, g->grid, g->finish_grid), "cudaGraphAddKernelNode(sweep)");
   CK(cudaGraphInstantiate(&g->cg_exec, g->cg, 0), "cudaGraphInstantiate");
   g->cg_args = proto;
+  g->cg_plan = plan;
+  g->cg_mode = mode;
   return NWGPU_OK;
 }
 
-bool same_scalars(const SweepArgs& x, const SweepArgs& y) {
-  return x.damping == y.damping && x.base == y.base && x.teleport == y.teleport && x.seed == y.seed;
+// The arguments a cached loop graph baked in.
+bool same_loop(const nwgpu_graph* g, const SweepArgs& y, const BinPlan* plan, int mode) {
+  const SweepArgs& x = g->cg_args;
+  return g->cg_plan == plan && g->cg_mode == mode && x.damping == y.damping && x.base == y.base &&
+         x.teleport == y.teleport && x.seed == y.seed && x.row_ptr == y.row_ptr && x.col == y.col && x.w == y.w &&
+         x.vbase == y.vbase && x.vaux == y.vaux;
 }
 
 // Runs the sweep loop from the state already on the device; fills fin.
-int run_sweeps(nwgpu_graph* g, const SweepArgs& a, uint32_t launch, uint64_t max_iters, cudaStream_t s, PrState* fin) {
+int run_sweeps(nwgpu_graph* g, const SweepArgs& a, uint32_t launch, uint64_t max_iters, cudaStream_t s, PrState* fin,
+               const BinPlan* plan, int mode) {
   if (launch == NWGPU_LAUNCH_GRAPH) {
-    if (!g->cg_exec || !same_scalars(g->cg_args, a)) {
-      int rc = build_loop_graph(g, a);
+    if (!g->cg_exec || !same_loop(g, a, plan, mode)) {
+      int rc = build_loop_graph(g, a, plan, mode);
       if (rc) return rc;
     }
     const uint64_t max_launches = max_iters / kGraphChunk + 2;
@@ -321,10 +338,10 @@ int run_sweeps(nwgpu_graph* g, const SweepArgs& a, uint32_t launch, uint64_t max
     uint64_t launched = 0;
     for (;;) {
       const uint64_t batch = (max_iters - launched) < kGraphChunk ? (max_iters - launched) : kGraphChunk;
-      const BinnedArgs ba = g->binned ? make_binned_args(g, a) : BinnedArgs{};
+      const BinnedArgs ba = plan ? make_binned_args(g, *plan, a, mode) : BinnedArgs{};
       for (uint64_t b = 0; b < batch; ++b) {
-        if (g->binned) {
-          CK(launch_binned_sweep(ba, g->bin_hot, g->bin_sweep_grid, g->bin_finish_grid, s), "pr_binned_sweep");
+        if (plan) {
+          CK(launch_binned_sweep(ba, plan->hot, mode, binned_grid(g, *plan, mode), plan->finish_grid, s), "pr_binned_sweep");
         } else {
           CK(launch_pr_sweep(a, g->variant, g->grid, s), "pr_sweep");
           CK(launch_pr_finish(a, g->finish_grid, s), "pr_finish");
@@ -405,7 +422,7 @@ int solve_single(nwgpu_graph* g, const uint32_t* out_degree, float* ranks, float
   trace.mark("degrees + init");
   CK(cudaEventRecord(g->ev0, s), "cudaEventRecord");
   PrState fin{};
-  rc = run_sweeps(g, a, opt.launch, max_iters, s, &fin);
+  rc = run_sweeps(g, a, opt.launch, max_iters, s, &fin, g->plan.ok ? &g->plan : nullptr, kModePlain);
   if (rc) return rc;
   CK(cudaEventRecord(g->ev1, s), "cudaEventRecord");
   trace.mark("sweeps");
@@ -468,7 +485,6 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
   if (n >= 0xFFFFFFF0ull) return fail(NWGPU_ERR_INVALID_ARG, "n = %llu does not fit uint32 vertex ids", (unsigned long long)n);
   if (nnz > 0xFFFFFFF0ull)
     return fail(NWGPU_ERR_INVALID_ARG, "nnz = %llu does not fit uint32 row pointers", (unsigned long long)nnz);
-  if (flags & NWGPU_GRAPH_TRANSPOSE) return fail(NWGPU_ERR_UNSUPPORTED, "NWGPU_GRAPH_TRANSPOSE is not available in this build");
   int dev, sms;
   int rc = check_device(&dev, &sms);
   if (rc) return rc;
@@ -584,10 +600,16 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
   trace.mark("tiling");
   const bool want_binned = which ? (!strcmp(which, "binned") || !strcmp(which, "binned_hot")) : true;
   if (g->relabelled && want_binned) {
-    rc = setup_binned(g);
+    // NWGPU_SWEEP=binned keeps the hubs in L1 only (256-thread CTAs)
+    rc = build_bin_plan(g, g->g.row_ptr, n, !which || strcmp(which, "binned") != 0, &g->plan);
     if (rc) return bail(rc);
   }
   trace.mark("bins");
+  if ((flags & NWGPU_GRAPH_TRANSPOSE) && weights && g->plan.ok) {
+    rc = ensure_wpr(g);
+    if (rc) return bail(rc);
+    trace.mark("out-row CSR");
+  }
   *out = g;
   return NWGPU_OK;
 }

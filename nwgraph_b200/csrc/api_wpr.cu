@@ -1,0 +1,204 @@
+// C ABI: weighted PageRank and the implicit adjoint of its fixed point
+// (nwgpu_wpr_run, nwgpu_pr_vjp in include/nwgpu.h). No counterpart in the
+// reference, whose page_rank is unweighted (page_rank.hpp:129-133); the
+// update, the stopping rule and the FP64 residual are its own, with weighted,
+// out-normalised contributions and a teleport vector. The adjoint solves
+//   l = c + d P^T l   (P_ij = w(j->i) / s_j)
+// with the same degree-binned sweep over the out-row CSR, so no forward
+// iterates are stored; the gradients are one pass over the entries
+// (pr_weighted.cu).
+#include <chrono>
+
+#include "handle.h"
+
+using namespace nwgpu;
+
+namespace nwgpu {
+
+void WprBuffers::release(cudaStream_t s) {
+  void* ptrs[] = {t.row_ptr, t.col, t.w, t.fwd, t.s, vbase, vaux, r_int, stage, stage2, res, gw};
+  for (void* p : ptrs) pool_free(p, s);
+  tplan.release(s);
+  *this = WprBuffers();
+}
+
+int ensure_wpr(nwgpu_graph* g) {
+  WprBuffers& b = g->wpr;
+  if (b.ready) return NWGPU_OK;
+  const uint64_t n = g->n, nnz = g->nnz;
+  CK(build_transpose(g->g.row_ptr, g->g.col, g->g.w, n, nnz, g->sms, &b.t, g->stream), "out-row CSR");
+  g->device_bytes += (3 * (nnz + kPad) + 2 * (n + kPad) + 1) * sizeof(uint32_t);
+  int rc = build_bin_plan(g, b.t.row_ptr, n, true, &b.tplan);
+  if (rc) return rc;
+  CK(dalloc(g, &b.vbase, n), "cudaMalloc(wpr base)");
+  CK(dalloc(g, &b.vaux, n), "cudaMalloc(wpr aux)");
+  CK(dalloc(g, &b.r_int, n), "cudaMalloc(wpr ranks)");
+  CK(dalloc(g, &b.stage, n), "cudaMalloc(wpr staging)");
+  CK(dalloc(g, &b.stage2, n), "cudaMalloc(wpr staging)");
+  const uint64_t parts = (uint64_t)binned_sweep_grid(g->sms, true) + (uint64_t)b.tplan.finish_grid;
+  CK(dalloc(g, &b.res, parts), "cudaMalloc(wpr residuals)");
+  CK(cudaStreamSynchronize(g->stream), "wpr buffers");
+  b.ready = true;
+  return NWGPU_OK;
+}
+
+namespace {
+
+// Arguments shared by both calls; returns the stream or sets an error.
+int check_common(nwgpu_graph* g, const void* out, float damping, const nwgpu_pr_options& opt) {
+  if (!g) return fail(NWGPU_ERR_INVALID_ARG, "graph is NULL");
+  if (g->n && !out) return fail(NWGPU_ERR_INVALID_ARG, "output is NULL");
+  if (!(damping >= 0.0f && damping <= 1.0f)) return fail(NWGPU_ERR_INVALID_ARG, "damping %g outside [0, 1]", (double)damping);
+  if (opt.mode != NWGPU_MODE_PARITY) return fail(NWGPU_ERR_UNSUPPORTED, "mode %u is not supported", opt.mode);
+  if (opt.launch > NWGPU_LAUNCH_STREAM) return fail(NWGPU_ERR_INVALID_ARG, "launch %u unknown", opt.launch);
+  if (!g->g.w) return fail(NWGPU_ERR_UNSUPPORTED, "the graph has no edge weights (pass them to nwgpu_graph_create)");
+  if (!g->relabelled || !g->plan.ok)
+    return fail(NWGPU_ERR_UNSUPPORTED, "weighted PageRank runs on the degree-binned sweep: create the graph relabelled");
+  return NWGPU_OK;
+}
+
+int start_state(nwgpu_graph* g, uint64_t max_iters, float threshold, cudaStream_t s) {
+  PrState h = {};
+  h.max_iters = max_iters;
+  h.chunk_end = kGraphChunk;
+  h.threshold = (double)threshold;
+  h.done = (max_iters == 0) ? 1u : 0u;
+  *g->h_st = h;
+  *(volatile unsigned int*)g->h_abort = 0u;
+  CK(cudaMemcpyAsync(g->st, g->h_st, sizeof(PrState), cudaMemcpyHostToDevice, s), "copy state");
+  return NWGPU_OK;
+}
+
+void init_stats(nwgpu_pr_stats* stats, double bytes) {
+  if (!stats) return;
+  double*  eb = stats->errors;
+  uint64_t ec = stats->errors_cap;
+  memset(stats, 0, sizeof(*stats));
+  stats->errors = eb;
+  stats->errors_cap = ec;
+  stats->bytes_per_iter = bytes;
+}
+
+int finish_stats(nwgpu_graph* g, const PrState& fin, float ms, nwgpu_pr_stats* stats, cudaStream_t s) {
+  if (!stats) return NWGPU_OK;
+  stats->iterations = fin.iter;
+  stats->final_error = fin.last_error;
+  stats->converged = (int32_t)fin.converged;
+  stats->device_ms = ms;
+  stats->ms_per_iter = fin.iter ? ms / (double)fin.iter : 0.0;
+  stats->gteps = ms > 0 ? (double)g->nnz * (double)fin.iter / (ms * 1e6) : 0.0;
+  if (stats->errors && stats->errors_cap) {
+    uint64_t m = fin.iter < stats->errors_cap ? fin.iter : stats->errors_cap;
+    if (m > g->err_cap) m = g->err_cap;
+    if (m) {
+      CK(cudaMemcpyAsync(stats->errors, g->err_hist, m * sizeof(double), cudaMemcpyDeviceToHost, s), "copy errors");
+      CK(cudaStreamSynchronize(s), "copy errors");
+    }
+  }
+  return NWGPU_OK;
+}
+
+// An n-vector argument on the device: the caller's pointer, or a copy of the
+// host vector in `stage`.
+int device_vector(const float* v, float* stage, uint64_t n, bool device_ptrs, cudaStream_t s, const float** out) {
+  if (!v || device_ptrs) {
+    *out = v;
+    return NWGPU_OK;
+  }
+  CK(cudaMemcpyAsync(stage, v, n * sizeof(float), cudaMemcpyHostToDevice, s), "copy vector");
+  *out = stage;
+  return NWGPU_OK;
+}
+
+}  // namespace
+}  // namespace nwgpu
+
+extern "C" int nwgpu_wpr_run(nwgpu_graph* g, const float* teleport, float* ranks, float damping, float threshold,
+                             uint64_t max_iters, const nwgpu_pr_options* options, nwgpu_pr_stats* stats) {
+  clear_error();
+  const nwgpu_pr_options opt = read_options(options);
+  int                    rc = check_common(g, ranks, damping, opt);
+  if (rc) return rc;
+  const uint64_t n = g->n;
+  // weights per entry on top of the plain sweep's bytes, plus the base term per row
+  init_stats(stats, 8.0 * (double)g->nnz + 4.0 * (double)(n + 1) + 24.0 * (double)n);
+  if (n == 0) return NWGPU_OK;
+  cudaStream_t s = opt.stream ? (cudaStream_t)opt.stream : g->stream;
+  if ((rc = ensure_solve_buffers(g)) || (rc = ensure_wpr(g))) return rc;
+  WprBuffers&  b = g->wpr;
+  const float* t = nullptr;
+  if ((rc = device_vector(teleport, b.stage, n, opt.device_ptrs != 0, s, &t))) return rc;
+  CK(launch_wpr_prepare(t, g->g.inv, b.t.s, n, damping, b.vbase, g->rank, g->contrib[0], g->sms, s), "wpr prepare");
+  if ((rc = start_state(g, max_iters, threshold, s))) return rc;
+  SweepArgs a = make_sweep_args(g, damping, 0.f, kTeleportUniform, 0u);
+  a.w = g->g.w;
+  a.vbase = b.vbase;
+  a.vaux = b.t.s;
+  CK(cudaEventRecord(g->ev0, s), "cudaEventRecord");
+  PrState fin{};
+  if ((rc = run_sweeps(g, a, opt.launch, max_iters, s, &fin, &g->plan, kModeWeighted))) return rc;
+  CK(cudaEventRecord(g->ev1, s), "cudaEventRecord");
+  float* dst = opt.device_ptrs ? ranks : b.stage;
+  CK(launch_gather_f32(g->rank, g->g.perm, dst, n, g->sms, s), "permute ranks");
+  if (!opt.device_ptrs) CK(cudaMemcpyAsync(ranks, dst, n * sizeof(float), cudaMemcpyDeviceToHost, s), "copy ranks");
+  CK(cudaStreamSynchronize(s), "copy ranks");
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+  if ((rc = finish_stats(g, fin, ms, stats, s))) return rc;
+  if (fin.aborted) return fail(NWGPU_ERR_ABORTED, "solve aborted after %llu sweeps", (unsigned long long)fin.iter);
+  return NWGPU_OK;
+}
+
+extern "C" int nwgpu_pr_vjp(nwgpu_graph* g, const float* ranks, const float* dL_dr, float* dL_dw, float* dL_dt, float damping,
+                            float threshold, uint64_t max_iters, const nwgpu_pr_options* options, nwgpu_pr_stats* stats) {
+  clear_error();
+  const nwgpu_pr_options opt = read_options(options);
+  int                    rc = check_common(g, ranks, damping, opt);
+  if (rc) return rc;
+  const uint64_t n = g->n, nnz = g->nnz;
+  if (n && !dL_dr) return fail(NWGPU_ERR_INVALID_ARG, "dL_dr is NULL");
+  init_stats(stats, 8.0 * (double)nnz + 4.0 * (double)(n + 1) + 24.0 * (double)n);
+  if (n == 0) return NWGPU_OK;
+  cudaStream_t s = opt.stream ? (cudaStream_t)opt.stream : g->stream;
+  if ((rc = ensure_solve_buffers(g)) || (rc = ensure_wpr(g))) return rc;
+  WprBuffers& b = g->wpr;
+  if (!b.tplan.ok)
+    return fail(NWGPU_ERR_UNSUPPORTED,
+                "the adjoint sweep needs the out-rows in the relabelled (non-increasing length) order; "
+                "this holds for symmetric graphs");
+  const float *r = nullptr, *c = nullptr;
+  if ((rc = device_vector(ranks, b.stage, n, opt.device_ptrs != 0, s, &r))) return rc;
+  if ((rc = device_vector(dL_dr, b.stage2, n, opt.device_ptrs != 0, s, &c))) return rc;
+  CK(launch_vjp_prepare(r, c, g->g.inv, b.t.s, n, damping, b.r_int, b.vbase, b.vaux, g->rank, g->contrib[0], g->sms, s),
+     "vjp prepare");
+  if ((rc = start_state(g, max_iters, threshold, s))) return rc;
+  SweepArgs a = make_sweep_args(g, damping, 0.f, kTeleportUniform, 0u);
+  a.row_ptr = b.t.row_ptr;
+  a.col = b.t.col;
+  a.w = b.t.w;
+  a.vbase = b.vbase;
+  a.vaux = b.vaux;
+  a.res_part = b.res;
+  CK(cudaEventRecord(g->ev0, s), "cudaEventRecord");
+  PrState fin{};
+  if ((rc = run_sweeps(g, a, opt.launch, max_iters, s, &fin, &b.tplan, kModeAdjoint))) return rc;
+  // gradients from the adjoint l (in g->rank)
+  if (dL_dw) {
+    if (!opt.device_ptrs && !b.gw) CK(dalloc(g, &b.gw, nnz), "cudaMalloc(dL/dw staging)");
+    float* dst = opt.device_ptrs ? dL_dw : b.gw;
+    CK(launch_vjp_grad_w(b.t, g->g.emap, b.r_int, g->rank, b.vbase, n, nnz, damping, dst, g->sms, s), "dL/dw");
+    if (!opt.device_ptrs) CK(cudaMemcpyAsync(dL_dw, dst, nnz * sizeof(float), cudaMemcpyDeviceToHost, s), "copy dL/dw");
+  }
+  if (dL_dt) {
+    float* dst = opt.device_ptrs ? dL_dt : b.stage;
+    CK(launch_vjp_grad_t(g->rank, g->g.perm, n, damping, dst, g->sms, s), "dL/dt");
+    if (!opt.device_ptrs) CK(cudaMemcpyAsync(dL_dt, dst, n * sizeof(float), cudaMemcpyDeviceToHost, s), "copy dL/dt");
+  }
+  CK(cudaEventRecord(g->ev1, s), "cudaEventRecord");
+  CK(cudaStreamSynchronize(s), "vjp");
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+  if ((rc = finish_stats(g, fin, ms, stats, s))) return rc;
+  if (fin.aborted) return fail(NWGPU_ERR_ABORTED, "solve aborted after %llu sweeps", (unsigned long long)fin.iter);
+  return NWGPU_OK;
+}

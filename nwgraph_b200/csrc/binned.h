@@ -41,7 +41,9 @@ int         binned_sweep_grid(int sms, bool hot);
 uint32_t    binned_hot_capacity();  // ids the hot variant can stage (a multiple of 4)
 cudaError_t configure_binned_kernels();
 int         binned_finish_grid(const BinnedArgs& a);
-cudaError_t launch_binned_sweep(const BinnedArgs& a, bool hot, int sweep_grid, int finish_grid, cudaStream_t s);
-cudaError_t add_binned_nodes(cudaGraph_t body, const BinnedArgs& a, bool hot, int sweep_grid, int finish_grid);
+// mode: SweepMode. The weighted and adjoint sweeps always use the hot shape
+// (sweep_grid = binned_sweep_grid(sms, true)).
+cudaError_t launch_binned_sweep(const BinnedArgs& a, bool hot, int mode, int sweep_grid, int finish_grid, cudaStream_t s);
+cudaError_t add_binned_nodes(cudaGraph_t body, const BinnedArgs& a, bool hot, int mode, int sweep_grid, int finish_grid);
 
 }  // namespace nwgpu

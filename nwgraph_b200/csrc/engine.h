@@ -42,12 +42,30 @@ struct Relabelled {
   float*    w = nullptr;        // nnz (+ kPad) or null
   uint32_t* perm = nullptr;     // input id -> internal id
   uint32_t* inv = nullptr;      // internal id -> input id
+  uint32_t* emap = nullptr;     // nnz: internal entry -> input entry (weighted graphs; null = identity)
+};
+
+// The out-row CSR (adjacency<0>) of the internal graph, for the adjoint:
+// row j lists the entries whose column is j, in internal entry order.
+struct Transposed {
+  uint32_t* row_ptr = nullptr;  // n + 1
+  uint32_t* col = nullptr;      // nnz: row (destination) of the forward entry
+  float*    w = nullptr;        // nnz: weight of the forward entry
+  uint32_t* fwd = nullptr;      // nnz: the forward entry
+  float*    s = nullptr;        // n: out-weight sums, FP64 row sums of w rounded to FP32
 };
 
 // Teleport term of the update r_i' = base_i + d * z_i.
 enum TeleportMode : int {
   kTeleportUniform = 0,  // base_i = (1 - d) / n, page_rank.hpp:94
   kTeleportSeed = 1,     // personalised, one-hot: base_i = (1 - d) if i == seed else 0
+};
+
+// Update the binned sweep applies (page_rank.hpp:133-135 for kModePlain).
+enum SweepMode : int {
+  kModePlain = 0,     // z = sum contrib;      r = base + d z;          contrib' = r / deg
+  kModeWeighted = 1,  // z = sum w * contrib;  r = vbase + d z;         contrib' = r / vaux  (vaux = out-weight sum)
+  kModeAdjoint = 2,   // z = sum w * lambda;   l = vbase + vaux * z;    contrib' = l         (vaux = d / out-weight sum)
 };
 
 struct SweepArgs {
@@ -76,6 +94,9 @@ struct SweepArgs {
   int                          teleport;   // TeleportMode
   uint32_t                     seed;       // internal id of the one-hot teleport vertex
   uint32_t                     hot_ids;    // gathers of ids below this are cached in L1
+  const float*                 w;          // kModeWeighted / kModeAdjoint: entry weights of the swept CSR
+  const float*                 vbase;      // per-row base term (weighted: (1-d) t; adjoint: c)
+  const float*                 vaux;       // per-row factor (weighted: out-weight sum; adjoint: d / out-weight sum)
 };
 
 // devmem.cu: the per-device stream-ordered pool that every handle allocation uses
@@ -95,6 +116,20 @@ cudaError_t fill_tiling(const uint32_t* d_row_ptr, uint64_t n, uint64_t nnz, uin
                         uint32_t* tile_row, uint32_t* tile_nnz, cudaStream_t s);
 cudaError_t build_relabelled(const uint32_t* d_row_ptr, const uint32_t* d_col, const float* d_w, uint64_t n,
                              uint64_t nnz, int sms, Relabelled* out, cudaStream_t s);
+cudaError_t build_transpose(const uint32_t* d_row_ptr, const uint32_t* d_col, const float* d_w, uint64_t n, uint64_t nnz,
+                            int sms, Transposed* out, cudaStream_t s);
+
+// pr_weighted.cu: set-up and gradient kernels of the weighted solve and its adjoint
+cudaError_t launch_wpr_prepare(const float* t, const uint32_t* inv, const float* s, uint64_t n, float damping,
+                               float* vbase, float* rank, float* contrib, int sms, cudaStream_t st);
+cudaError_t launch_vjp_prepare(const float* r, const float* c, const uint32_t* inv, const float* s, uint64_t n,
+                               float damping, float* r_int, float* vbase, float* vaux, float* lam, float* contrib, int sms,
+                               cudaStream_t st);
+cudaError_t launch_vjp_grad_w(const Transposed& t, const uint32_t* emap, const float* r_int, const float* lam,
+                              const float* c_int, uint64_t n, uint64_t nnz, float damping, float* d_w, int sms,
+                              cudaStream_t st);
+cudaError_t launch_vjp_grad_t(const float* lam, const uint32_t* perm, uint64_t n, float damping, float* d_t, int sms,
+                              cudaStream_t st);
 
 // pr_plain.cu
 cudaError_t launch_gather_u32(const uint32_t* src, const uint32_t* idx, uint32_t* dst, uint64_t n, int sms,

@@ -130,7 +130,8 @@ __global__ void __launch_bounds__(NT) permute_entries_kernel(const uint32_t* __r
                                                               const uint32_t* __restrict__ old_row_ptr,
                                                               const uint32_t* __restrict__ old_col,
                                                               const float* __restrict__ old_w, uint32_t* __restrict__ col,
-                                                              float* __restrict__ w, uint32_t D) {
+                                                              float* __restrict__ w, uint32_t* __restrict__ emap,
+                                                              uint32_t D) {
   extern __shared__ uint32_t sm[];
   uint32_t* s_new = sm;          // new_row_ptr[r0 .. r1+1]
   uint32_t* s_old = sm + D + 2;  // old start of rows r0 .. r1
@@ -157,6 +158,7 @@ __global__ void __launch_bounds__(NT) permute_entries_kernel(const uint32_t* __r
       const uint32_t src = s_old[lo] + (p - s_new[lo]);
       col[p] = perm[old_col[src]];
       if (w) w[p] = old_w[src];
+      if (emap) emap[p] = src;
     }
     __syncthreads();
   }
@@ -201,6 +203,8 @@ cudaError_t build_relabelled(const uint32_t* d_row_ptr, const uint32_t* d_col, c
   if (d_w) {
     RK(pool_alloc_n(&out->w, nnz + kPad, s));
     RK(cudaMemsetAsync(out->w, 0, (nnz + kPad) * sizeof(float), s));
+    RK(pool_alloc_n(&out->emap, nnz + kPad, s));
+    RK(cudaMemsetAsync(out->emap, 0, (nnz + kPad) * sizeof(uint32_t), s));
   }
   row_length_kernel<<<grid, 256, 0, s>>>(d_row_ptr, n, cnt);
   RK(cudaGetLastError());
@@ -224,11 +228,124 @@ cudaError_t build_relabelled(const uint32_t* d_row_ptr, const uint32_t* d_col, c
   const size_t   smem = (size_t)(2 * D + 4) * sizeof(uint32_t);
   permute_entries_kernel<kSweepThreads><<<sms * 4, kSweepThreads, smem, s>>>(
       out->row_ptr, nt.tile_row, nt.tile_nnz, nt.num_tiles, out->inv, out->perm, d_row_ptr, d_col, d_w, out->col,
-      out->w, D);
+      out->w, out->emap, D);
   RK(cudaGetLastError());
   RK(cudaStreamSynchronize(s));
   cleanup();
 #undef RK
+  return cudaSuccess;
+}
+
+// ---------------------------------------------------------------------------
+// Transposed CSR (out-rows), for the adjoint solve
+// ---------------------------------------------------------------------------
+// Row of each entry: the last row whose start is <= k.
+__global__ void entry_row_kernel(const uint32_t* __restrict__ row_ptr, uint64_t n, uint64_t nnz,
+                                 uint32_t* __restrict__ erow) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += stride) {
+    uint64_t lo = 0, hi = n;  // row_ptr[lo] <= k < row_ptr[hi]
+    while (hi - lo > 1) {
+      const uint64_t mid = (lo + hi) >> 1;
+      if (row_ptr[mid] <= k)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    erow[k] = (uint32_t)lo;
+  }
+}
+
+__global__ void count_cols_kernel(const uint32_t* __restrict__ col, uint64_t nnz, uint32_t* __restrict__ cnt) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += stride) atomicAdd(cnt + col[k], 1u);
+}
+
+// Out-entry e is forward entry fwd[e]: its destination row and weight.
+__global__ void transpose_fill_kernel(const uint32_t* __restrict__ fwd, const uint32_t* __restrict__ erow,
+                                      const float* __restrict__ w, uint64_t nnz, uint32_t* __restrict__ tcol,
+                                      float* __restrict__ tw) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += stride) {
+    const uint32_t k = fwd[e];
+    tcol[e] = erow[k];
+    tw[e] = w ? w[k] : 1.0f;
+  }
+}
+
+// s_j = sum of the weights of out-row j, in entry order, in FP64.
+__global__ void out_weight_kernel(const uint32_t* __restrict__ trow, const float* __restrict__ tw, uint64_t n,
+                                  float* __restrict__ s) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+    double acc = 0.0;
+    for (uint32_t e = trow[j]; e < trow[j + 1]; ++e) acc += (double)tw[e];
+    s[j] = (float)acc;
+  }
+}
+
+cudaError_t build_transpose(const uint32_t* d_row_ptr, const uint32_t* d_col, const float* d_w, uint64_t n, uint64_t nnz,
+                            int sms, Transposed* out, cudaStream_t s) {
+  cudaError_t e;
+  uint32_t *erow = nullptr, *ids = nullptr, *keys = nullptr, *cnt = nullptr;
+  void*     tmp = nullptr;
+  size_t    sort_bytes = 0, scan_bytes = 0;
+  auto      cleanup = [&]() {
+    pool_free(erow, s);
+    pool_free(ids, s);
+    pool_free(keys, s);
+    pool_free(cnt, s);
+    pool_free(tmp, s);
+  };
+#define TK(x)                       \
+  do {                              \
+    if ((e = (x)) != cudaSuccess) { \
+      cleanup();                    \
+      return e;                     \
+    }                               \
+  } while (0)
+  const int grid = sms * 8;
+  TK(pool_alloc_n(&erow, nnz + kPad, s));
+  TK(pool_alloc_n(&ids, nnz + kPad, s));
+  TK(pool_alloc_n(&keys, nnz + kPad, s));
+  TK(pool_alloc_n(&cnt, n + 1, s));
+  TK(pool_alloc_n(&out->row_ptr, n + 1 + kPad, s));
+  TK(pool_alloc_n(&out->col, nnz + kPad, s));
+  TK(pool_alloc_n(&out->w, nnz + kPad, s));
+  TK(pool_alloc_n(&out->fwd, nnz + kPad, s));
+  TK(pool_alloc_n(&out->s, n + kPad, s));
+  TK(cudaMemsetAsync(out->row_ptr, 0, (n + 1 + kPad) * sizeof(uint32_t), s));
+  TK(cudaMemsetAsync(out->col, 0, (nnz + kPad) * sizeof(uint32_t), s));
+  TK(cudaMemsetAsync(out->w, 0, (nnz + kPad) * sizeof(float), s));
+  TK(cudaMemsetAsync(out->fwd, 0, (nnz + kPad) * sizeof(uint32_t), s));
+  TK(cudaMemsetAsync(out->s, 0, (n + kPad) * sizeof(float), s));
+  TK(cudaMemsetAsync(cnt, 0, (n + 1) * sizeof(uint32_t), s));
+  if (nnz) {
+    entry_row_kernel<<<grid, 256, 0, s>>>(d_row_ptr, n, nnz, erow);
+    TK(cudaGetLastError());
+    iota_kernel<<<grid, 256, 0, s>>>(ids, nnz);
+    TK(cudaGetLastError());
+    count_cols_kernel<<<grid, 256, 0, s>>>(d_col, nnz, cnt);
+    TK(cudaGetLastError());
+  }
+  // stable sort of the entries by column: out-row order, entries of one
+  // out-row in forward entry order
+  int bits = 1;
+  while (bits < 32 && (1ull << bits) < n) ++bits;
+  TK(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, d_col, keys, ids, out->fwd, (int64_t)nnz, 0, bits, s));
+  TK(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, cnt, out->row_ptr, (int64_t)(n + 1), s));
+  TK(pool_alloc(&tmp, sort_bytes > scan_bytes ? sort_bytes : scan_bytes, s));
+  if (nnz) TK(cub::DeviceRadixSort::SortPairs(tmp, sort_bytes, d_col, keys, ids, out->fwd, (int64_t)nnz, 0, bits, s));
+  TK(cub::DeviceScan::ExclusiveSum(tmp, scan_bytes, cnt, out->row_ptr, (int64_t)(n + 1), s));
+  if (nnz) {
+    transpose_fill_kernel<<<grid, 256, 0, s>>>(out->fwd, erow, d_w, nnz, out->col, out->w);
+    TK(cudaGetLastError());
+  }
+  out_weight_kernel<<<grid, 256, 0, s>>>(out->row_ptr, out->w, n, out->s);
+  TK(cudaGetLastError());
+  TK(cudaStreamSynchronize(s));
+  cleanup();
+#undef TK
   return cudaSuccess;
 }
 

@@ -27,6 +27,33 @@ int  check_device(int* dev_out, int* sms_out);
     if (_e != cudaSuccess) return ::nwgpu::cuda_fail(_e, what); \
   } while (0)
 
+// Bin tables of one CSR for the degree-binned sweep.
+struct BinPlan {
+  bool       ok = false;        // the rows are in non-increasing length order and the tables exist
+  bool       hot = false;       // hub contributions staged in shared memory
+  BinnedArgs bin{};             // tables; the SweepArgs part is filled per solve
+  uint32_t*  first = nullptr;   // row_first_chunk
+  uint32_t*  chunk_row = nullptr;
+  float*     chunk_part = nullptr;
+  int        sweep_grid = 0, finish_grid = 1;
+  void       release(cudaStream_t s);
+};
+
+// Buffers of the weighted solve and its adjoint (created on first use).
+struct WprBuffers {
+  bool       ready = false;
+  Transposed t{};                // out-row CSR, out-weight sums
+  BinPlan    tplan;              // bins of the out-row CSR (adjoint sweeps)
+  float*     vbase = nullptr;    // n: (1-d) t (forward) or c (adjoint), internal order
+  float*     vaux = nullptr;     // n: d / s (adjoint)
+  float*     r_int = nullptr;    // n: forward ranks, internal order
+  float*     stage = nullptr;    // n: input-order staging
+  float*     stage2 = nullptr;   // n: input-order staging
+  double*    res = nullptr;      // residual partials of the adjoint sweep
+  float*     gw = nullptr;       // nnz: dL/dw staging for host outputs
+  void       release(cudaStream_t s);
+};
+
 // Buffers of the batched personalised solve (K padded columns).
 struct PprBuffers {
   int             K = 0;
@@ -66,13 +93,7 @@ struct nwgpu_graph {
   uint32_t     hot_ids = 0;      // internal ids below this are gathered from shared memory / L1
   nwgpu::SweepVariant variant{256, 8, false};
   // Degree-binned sweep (relabelled graphs with non-increasing row lengths).
-  bool              binned = false;
-  bool              bin_hot = false;   // hub contributions staged in shared memory
-  nwgpu::BinnedArgs bin{};         // tables; the SweepArgs part is filled per solve
-  uint32_t*         bin_first = nullptr;
-  uint32_t*         bin_chunk_row = nullptr;
-  float*            bin_chunk_part = nullptr;
-  int               bin_sweep_grid = 0, bin_finish_grid = 1;
+  nwgpu::BinPlan plan;
   int          finish_grid = 1;  // finishing-kernel CTAs
   uint64_t     device_bytes = 0;
 
@@ -97,16 +118,20 @@ struct nwgpu_graph {
   cudaGraph_t     cg = nullptr;
   cudaGraphExec_t cg_exec = nullptr;
   nwgpu::SweepArgs cg_args{};  // arguments baked into cg_exec
+  const nwgpu::BinPlan* cg_plan = nullptr;
+  int             cg_mode = 0;
 
   nwgpu::PprBuffers ppr;
+  nwgpu::WprBuffers wpr;
 
   ~nwgpu_graph() {
     ppr.release(stream);
+    wpr.release(stream);
+    plan.release(stream);
     if (cg_exec) cudaGraphExecDestroy(cg_exec);
     if (cg) cudaGraphDestroy(cg);
-    void* dev_ptrs[] = {g.row_ptr, g.col, g.w, g.perm, g.inv, tiling.tile_row, tiling.tile_nnz, rank, contrib[0],
-                        contrib[1], deg, stage_u32, cpart, epart, res_part, st, err_hist, bin_first, bin_chunk_row,
-                        bin_chunk_part};
+    void* dev_ptrs[] = {g.row_ptr, g.col, g.w, g.perm, g.inv, g.emap, tiling.tile_row, tiling.tile_nnz, rank, contrib[0],
+                        contrib[1], deg, stage_u32, cpart, epart, res_part, st, err_hist};
     for (void* p : dev_ptrs) nwgpu::pool_free(p, stream);
     cudaStreamSynchronize(stream);  // the blocks are free for the next handle at once
     if (h_st) cudaFreeHost(h_st);
@@ -129,6 +154,16 @@ cudaError_t dalloc(nwgpu_graph* g, T** p, uint64_t count) {
   return e;
 }
 int ensure_solve_buffers(nwgpu_graph* g);
+int build_bin_plan(nwgpu_graph* g, const uint32_t* row_ptr, uint64_t n, bool hot, BinPlan* p);
+// Sweep arguments over the handle's forward CSR and solve buffers.
+SweepArgs make_sweep_args(nwgpu_graph* g, float damping, float base, int teleport, uint32_t seed);
+// Runs the sweep loop from the state already on the device (CUDA graph or one
+// launch per sweep); plan: the binned sweep's tables (null: merge-path sweep).
+int run_sweeps(nwgpu_graph* g, const SweepArgs& a, uint32_t launch, uint64_t max_iters, cudaStream_t s, PrState* fin,
+               const BinPlan* plan, int mode);
+nwgpu_pr_options read_options(const nwgpu_pr_options* options);
+// Out-row CSR, its bins and the buffers of the weighted solve and its adjoint.
+int ensure_wpr(nwgpu_graph* g);
 // degrees (input order, host or device) -> g->deg (internal order)
 int load_degrees(nwgpu_graph* g, const uint32_t* out_degree, bool device_ptrs, cudaStream_t s);
 }  // namespace nwgpu

@@ -66,36 +66,82 @@ __device__ __forceinline__ float gather_one(const Src& s, uint32_t id) {
   return (id < s.l1_ids) ? ld_gather(s.cin + id, s.pol) : ld_gather_cold(s.cin + id, s.pol);
 }
 
-// Epilogue of one row with its old rank and degree already loaded; returns
-// |dr| in FP64.
-__device__ __forceinline__ double binned_update(const BinnedArgs& a, float* __restrict__ cout, uint32_t r, float z,
-                                                float old, uint32_t dg, uint64_t pol) {
-  const float nr = fmaf(a.sw.damping, z, binned_base(a, r));
-  st_stream(a.sw.rank + r, nr);
-  st_keep(cout + r, nr / (float)dg, pol);
-  return (double)fabsf(nr - old);
+// What a row's epilogue reads besides its sum: the old value and, by mode,
+// the out-degree (plain) or the per-row factor and base term (weighted,
+// adjoint). Loaded early, while the row's gathers are in flight.
+struct RowIn {
+  float    old;
+  uint32_t dg;    // kModePlain: out-degree
+  float    aux;   // kModeWeighted: out-weight sum; kModeAdjoint: d / out-weight sum
+  float    base;  // kModeWeighted: (1-d) t; kModeAdjoint: c
+};
+
+template <int MODE>
+__device__ __forceinline__ RowIn load_row_in(const BinnedArgs& a, uint32_t r) {
+  RowIn x;
+  x.old = ld_stream(a.sw.rank + r);
+  if constexpr (MODE == kModePlain) {
+    x.dg = ld_stream(a.sw.deg + r);
+    x.aux = 1.f;
+    x.base = 0.f;
+  } else {
+    x.dg = 1u;
+    x.aux = ld_stream(a.sw.vaux + r);
+    x.base = ld_stream(a.sw.vbase + r);
+  }
+  return x;
 }
+__device__ __forceinline__ RowIn no_row_in() { return RowIn{0.f, 1u, 1.f, 0.f}; }
+
+// Epilogue of one row: new value, the next sweep's contribution, |dr| in FP64.
+template <int MODE>
+__device__ __forceinline__ double binned_update(const BinnedArgs& a, float* __restrict__ cout, uint32_t r, float z,
+                                                const RowIn& in, uint64_t pol) {
+  float nr, c;
+  if constexpr (MODE == kModePlain) {
+    nr = fmaf(a.sw.damping, z, binned_base(a, r));
+    c = nr / (float)in.dg;
+  } else if constexpr (MODE == kModeWeighted) {
+    nr = fmaf(a.sw.damping, z, in.base);
+    c = nr / in.aux;
+  } else {
+    nr = fmaf(in.aux, z, in.base);
+    c = nr;
+  }
+  st_stream(a.sw.rank + r, nr);
+  st_keep(cout + r, c, pol);
+  return (double)fabsf(nr - in.old);
+}
+template <int MODE>
 __device__ __forceinline__ double binned_epilogue(const BinnedArgs& a, float* __restrict__ cout, uint32_t r, float z,
                                                   uint64_t pol) {
-  return binned_update(a, cout, r, z, ld_stream(a.sw.rank + r), ld_stream(a.sw.deg + r), pol);
+  return binned_update<MODE>(a, cout, r, z, load_row_in<MODE>(a, r), pol);
+}
+
+// One term of a row sum: the gathered contribution, times the entry's weight
+// in the weighted and adjoint modes.
+template <bool HOT, int MODE>
+__device__ __forceinline__ float term(const BinnedArgs& a, const Src& src, uint32_t id, uint32_t k) {
+  const float c = gather_one<HOT>(src, id);
+  if constexpr (MODE == kModePlain) return c;
+  else return ld_stream(a.sw.w + k) * c;
 }
 
 // Rows without entries: four rows per lane.
+template <int MODE>
 __device__ __forceinline__ double empty_rows(const BinnedArgs& a, float* __restrict__ cout, uint32_t row0,
                                              uint32_t row_end, int lane, uint64_t pol) {
-  double   res = 0.0;
-  float    old[4];
-  uint32_t dg[4];
+  double res = 0.0;
+  RowIn  in[4];
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const uint32_t r = row0 + q * 32 + lane;
-    old[q] = (r < row_end) ? ld_stream(a.sw.rank + r) : 0.f;
-    dg[q] = (r < row_end) ? ld_stream(a.sw.deg + r) : 1u;
+    in[q] = (r < row_end) ? load_row_in<MODE>(a, r) : no_row_in();
   }
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const uint32_t r = row0 + q * 32 + lane;
-    if (r < row_end) res += binned_update(a, cout, r, 0.f, old[q], dg[q], pol);
+    if (r < row_end) res += binned_update<MODE>(a, cout, r, 0.f, in[q], pol);
   }
   return res;
 }
@@ -117,7 +163,7 @@ __device__ __forceinline__ uint32_t first_unit(uint32_t gwarp, uint32_t nwarps, 
 // Units that are entry ranges, one warp each, walked in steps of 8 x 32
 // entries. CHUNK: unit c = chunk c of a long row, partial sum to chunk_part[c].
 // Otherwise: unit w = row rb + w (bin 0), epilogue.
-template <bool HOT, bool CHUNK>
+template <bool HOT, bool CHUNK, int MODE>
 __device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src, float* __restrict__ cout, uint32_t rb,
                                             uint32_t nunits, uint32_t w, uint32_t nwarps, int lane) {
   constexpr int      U = 8;
@@ -148,12 +194,8 @@ __device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src,
   uint32_t id[U];
   uint32_t base = k0;
   load_ids(base, k1, id);
-  float    old = 0.f;
-  uint32_t dg = 1u;
-  if (!CHUNK && lane == 0) {
-    old = ld_stream(a.sw.rank + row);
-    dg = ld_stream(a.sw.deg + row);
-  }
+  RowIn in = no_row_in();
+  if (!CHUNK && lane == 0) in = load_row_in<MODE>(a, row);
   float  acc = 0.f;
   double res = 0.0;
 #pragma unroll 1
@@ -162,7 +204,7 @@ __device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src,
 #pragma unroll
     for (int q = 0; q < U; ++q) {
       const uint32_t k = base + (uint32_t)lane + (uint32_t)q * 32u;
-      v[q] = (k < k1) ? gather_one<HOT>(src, id[q]) : 0.f;
+      v[q] = (k < k1) ? term<HOT, MODE>(a, src, id[q], k) : 0.f;
     }
     // the next step: the rest of this unit, or the first step of the next one
     const bool     more = base + STEP < k1;  // warp-uniform
@@ -177,7 +219,7 @@ __device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src,
       if (CHUNK) {
         if (lane == 0) a.chunk_part[w] = z;
       } else if (lane == 0) {
-        res += binned_update(a, cout, row, z, old, dg, src.pol);
+        res += binned_update<MODE>(a, cout, row, z, in, src.pol);
       }
       acc = 0.f;
       w += nwarps;
@@ -185,10 +227,7 @@ __device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src,
       k1 = nk1;
       row = nrow;
       if (w + nwarps < nunits) bounds(w + nwarps, nk0, nk1, nrow);
-      if (!CHUNK && lane == 0) {
-        old = ld_stream(a.sw.rank + row);
-        dg = ld_stream(a.sw.deg + row);
-      }
+      if (!CHUNK && lane == 0) in = load_row_in<MODE>(a, row);
     }
     base = nbase;
   }
@@ -229,7 +268,7 @@ __device__ __forceinline__ void group_ids(const BinnedArgs& a, const uint32_t (&
 
 // G-bins: a unit is 2 * 32/G consecutive rows, G lanes per row, each lane two
 // rows and at most 4 entries of each.
-template <bool HOT, int G>
+template <bool HOT, int G, int MODE>
 __device__ __forceinline__ double group_bin(const BinnedArgs& a, const Src& src, float* __restrict__ cout, uint32_t rb,
                                             uint32_t re_bin, uint32_t nunits, uint32_t w, uint32_t nwarps, int lane) {
   constexpr uint32_t PER = 32 / G;
@@ -242,21 +281,21 @@ __device__ __forceinline__ double group_bin(const BinnedArgs& a, const Src& src,
   double res = 0.0;
 #pragma unroll 1
   for (; w < nunits; w += nwarps) {
-    uint32_t row[2], dg[2];
-    float    old[2];
+    uint32_t row[2];
+    RowIn    in[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       row[h] = rb + w * (2u * PER) + (uint32_t)h * PER + (uint32_t)lane / G;
-      const bool mine = row[h] < re_bin && sub == 0;
-      old[h] = mine ? ld_stream(a.sw.rank + row[h]) : 0.f;
-      dg[h] = mine ? ld_stream(a.sw.deg + row[h]) : 1u;
+      in[h] = (row[h] < re_bin && sub == 0) ? load_row_in<MODE>(a, row[h]) : no_row_in();
     }
     float v[2][4];
 #pragma unroll
     for (int h = 0; h < 2; ++h)
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        v[h][q] = ((uint32_t)sub + (uint32_t)q * G < len[h]) ? gather_one<HOT>(src, id[h][q]) : 0.f;
+        v[h][q] = ((uint32_t)sub + (uint32_t)q * G < len[h])
+                      ? term<HOT, MODE>(a, src, id[h][q], rs[h] + (uint32_t)sub + (uint32_t)q * G)
+                      : 0.f;
     // the next unit's column ids, the bounds of the unit after it
     group_ids<G>(a, nrs, nlen, sub, id);
 #pragma unroll
@@ -272,13 +311,13 @@ __device__ __forceinline__ double group_bin(const BinnedArgs& a, const Src& src,
       for (int q = 0; q < 4; ++q) acc += v[h][q];
 #pragma unroll
       for (int off = G / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(kFullMask, acc, off);
-      if (row[h] < re_bin && sub == 0) res += binned_update(a, cout, row[h], acc, old[h], dg[h], src.pol);
+      if (row[h] < re_bin && sub == 0) res += binned_update<MODE>(a, cout, row[h], acc, in[h], src.pol);
     }
   }
   return res;
 }
 
-template <int NT, bool HOT>
+template <int NT, bool HOT, int MODE>
 __global__ void __launch_bounds__(NT, 1024 / NT) pr_binned_sweep_kernel(const BinnedArgs a) {
   constexpr int     NW = NT / 32;
   __shared__ double s_red[NW];
@@ -301,7 +340,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) pr_binned_sweep_kernel(const Bi
   }
   double         res = 0.0;
   const uint32_t nwarps = gridDim.x * NW, gwarp = blockIdx.x * NW + warp;
-  res += range_bin<HOT, true>(a, src, cout, 0u, a.num_chunks, gwarp, nwarps, lane);
+  res += range_bin<HOT, true, MODE>(a, src, cout, 0u, a.num_chunks, gwarp, nwarps, lane);
   uint32_t begin = a.num_chunks;  // flat index of the bin's first unit
 #pragma unroll 1
   for (int b = 0; b < kNumBins; ++b) {
@@ -309,15 +348,15 @@ __global__ void __launch_bounds__(NT, 1024 / NT) pr_binned_sweep_kernel(const Bi
     const uint32_t w0 = first_unit(gwarp, nwarps, begin);
     const uint32_t rb = a.bin_row_begin[b], re = a.bin_row_end[b];
     switch (b) {
-      case 0: res += range_bin<HOT, false>(a, src, cout, rb, nu, w0, nwarps, lane); break;
-      case 1: res += group_bin<HOT, 32>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
-      case 2: res += group_bin<HOT, 16>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
-      case 3: res += group_bin<HOT, 8>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
-      case 4: res += group_bin<HOT, 4>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
-      case 5: res += group_bin<HOT, 2>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
-      case 6: res += group_bin<HOT, 1>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
+      case 0: res += range_bin<HOT, false, MODE>(a, src, cout, rb, nu, w0, nwarps, lane); break;
+      case 1: res += group_bin<HOT, 32, MODE>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
+      case 2: res += group_bin<HOT, 16, MODE>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
+      case 3: res += group_bin<HOT, 8, MODE>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
+      case 4: res += group_bin<HOT, 4, MODE>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
+      case 5: res += group_bin<HOT, 2, MODE>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
+      case 6: res += group_bin<HOT, 1, MODE>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
       default:
-        for (uint32_t w = w0; w < nu; w += nwarps) res += empty_rows(a, cout, rb + w * 128u, re, lane, src.pol);
+        for (uint32_t w = w0; w < nu; w += nwarps) res += empty_rows<MODE>(a, cout, rb + w * 128u, re, lane, src.pol);
         break;
     }
     begin += nu;
@@ -339,6 +378,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) pr_binned_sweep_kernel(const Bi
 // rows get a thread each (partials in chunk order). Then the residual
 // reduction over the sweep's and this kernel's CTA partials in a fixed order,
 // and the device-side convergence test (page_rank.hpp:125-134).
+template <int MODE>
 __global__ void __launch_bounds__(256) pr_binned_finish_kernel(const BinnedArgs a) {
   __shared__ double s_red[8];
   __shared__ int    s_last;
@@ -355,7 +395,7 @@ __global__ void __launch_bounds__(256) pr_binned_finish_kernel(const BinnedArgs 
     float          p = 0.f;
     for (uint32_t c = c0 + (uint32_t)lane; c < c1; c += 32u) p += __ldcg(a.chunk_part + c);
     p = warp_sum_lane0(p);
-    if (lane == 0) res = binned_epilogue(a, cout, gw, p, pol);
+    if (lane == 0) res = binned_epilogue<MODE>(a, cout, gw, p, pol);
   } else {
     const uint32_t r = a.num_big_rows + (gt - a.num_big_rows * 32u);
     if (r < a.num_long_rows) {
@@ -363,7 +403,7 @@ __global__ void __launch_bounds__(256) pr_binned_finish_kernel(const BinnedArgs 
       float          p = 0.f;
 #pragma unroll 4
       for (uint32_t c = c0; c < c1; ++c) p += __ldcg(a.chunk_part + c);
-      res = binned_epilogue(a, cout, r, p, pol);
+      res = binned_epilogue<MODE>(a, cout, r, p, pol);
     }
   }
   res = warp_sum_lane0(res);
@@ -474,23 +514,41 @@ static int binned_hot_smem_bytes() {
 uint32_t binned_hot_capacity() { return (uint32_t)(binned_hot_smem_bytes() / 4) & ~3u; }
 
 cudaError_t configure_binned_kernels() {
-  return cudaFuncSetAttribute(pr_binned_sweep_kernel<kBinnedHotThreads, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              binned_hot_smem_bytes());
+  void* const hot[] = {(void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModePlain>,
+                       (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModeWeighted>,
+                       (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModeAdjoint>};
+  for (void* fn : hot) {
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, binned_hot_smem_bytes());
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 int binned_sweep_grid(int sms, bool hot) {
   if (hot) return sms;
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pr_binned_sweep_kernel<kBinnedThreads, false>, kBinnedThreads, 0) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pr_binned_sweep_kernel<kBinnedThreads, false, kModePlain>,
+                                                    kBinnedThreads, 0) !=
           cudaSuccess ||
       nb < 1)
     nb = 1;
   return sms * nb;
 }
 
-static void* binned_fn(bool hot) {
-  return hot ? (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true> : (void*)pr_binned_sweep_kernel<kBinnedThreads, false>;
+// Plain sweeps come in both launch shapes; the weighted and adjoint sweeps in
+// the hot shape only.
+static void* binned_fn(bool hot, int mode) {
+  if (mode == kModeWeighted) return (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModeWeighted>;
+  if (mode == kModeAdjoint) return (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModeAdjoint>;
+  return hot ? (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModePlain>
+             : (void*)pr_binned_sweep_kernel<kBinnedThreads, false, kModePlain>;
 }
+static void* binned_finish_fn(int mode) {
+  if (mode == kModeWeighted) return (void*)pr_binned_finish_kernel<kModeWeighted>;
+  if (mode == kModeAdjoint) return (void*)pr_binned_finish_kernel<kModeAdjoint>;
+  return (void*)pr_binned_finish_kernel<kModePlain>;
+}
+static bool binned_shape_hot(bool hot, int mode) { return hot || mode != kModePlain; }
 
 int binned_finish_grid(const BinnedArgs& a) {
   const uint64_t threads = (uint64_t)a.num_big_rows * 32u + (a.num_long_rows - a.num_big_rows);
@@ -498,28 +556,29 @@ int binned_finish_grid(const BinnedArgs& a) {
   return blocks ? (int)blocks : 1;
 }
 
-cudaError_t launch_binned_sweep(const BinnedArgs& a, bool hot, int sweep_grid, int finish_grid, cudaStream_t s) {
+cudaError_t launch_binned_sweep(const BinnedArgs& a, bool hot, int mode, int sweep_grid, int finish_grid, cudaStream_t s) {
   void*       args[] = {(void*)&a};
-  cudaError_t e = cudaLaunchKernel(binned_fn(hot), dim3((unsigned)sweep_grid), dim3(hot ? kBinnedHotThreads : kBinnedThreads),
-                                   args, hot ? (size_t)a.smem_ids * 4u : 0u, s);
+  const bool  h = binned_shape_hot(hot, mode);
+  cudaError_t e = cudaLaunchKernel(binned_fn(hot, mode), dim3((unsigned)sweep_grid),
+                                   dim3(h ? kBinnedHotThreads : kBinnedThreads), args, h ? (size_t)a.smem_ids * 4u : 0u, s);
   if (e != cudaSuccess) return e;
-  pr_binned_finish_kernel<<<finish_grid, 256, 0, s>>>(a);
-  return cudaGetLastError();
+  return cudaLaunchKernel(binned_finish_fn(mode), dim3((unsigned)finish_grid), dim3(256), args, 0, s);
 }
 
-cudaError_t add_binned_nodes(cudaGraph_t body, const BinnedArgs& a, bool hot, int sweep_grid, int finish_grid) {
+cudaError_t add_binned_nodes(cudaGraph_t body, const BinnedArgs& a, bool hot, int mode, int sweep_grid, int finish_grid) {
   void*                args[] = {(void*)&a};
+  const bool           h = binned_shape_hot(hot, mode);
   cudaKernelNodeParams kp = {};
-  kp.func = binned_fn(hot);
+  kp.func = binned_fn(hot, mode);
   kp.gridDim = dim3((unsigned)sweep_grid);
-  kp.blockDim = dim3(hot ? kBinnedHotThreads : kBinnedThreads);
-  kp.sharedMemBytes = hot ? (unsigned)a.smem_ids * 4u : 0u;
+  kp.blockDim = dim3(h ? kBinnedHotThreads : kBinnedThreads);
+  kp.sharedMemBytes = h ? (unsigned)a.smem_ids * 4u : 0u;
   kp.kernelParams = args;
   cudaGraphNode_t sn, fn;
   cudaError_t     e = cudaGraphAddKernelNode(&sn, body, nullptr, 0, &kp);
   if (e != cudaSuccess) return e;
   cudaKernelNodeParams fp = {};
-  fp.func = (void*)pr_binned_finish_kernel;
+  fp.func = binned_finish_fn(mode);
   fp.gridDim = dim3((unsigned)finish_grid);
   fp.blockDim = dim3(256);
   fp.kernelParams = args;

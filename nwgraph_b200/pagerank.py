@@ -261,6 +261,78 @@ class Graph:
                              None if errs is None else errs[: min(int(st.iterations), len(errs))])
 
 
+    # ------------------------------------------------------------------
+    def _f32_vectors(self, arrays, sizes):
+        """Addresses of float32 vectors that are all host arrays or all CUDA
+        tensors (None allowed); outputs are filled in place."""
+        dev = {_is_cuda_tensor(x) for x in arrays if x is not None}
+        if len(dev) > 1:
+            raise ValueError("vectors must all be host arrays or all device tensors")
+        on_dev = dev.pop() if dev else False
+        ptrs, keep = [], []
+        for x, size in zip(arrays, sizes):
+            if x is None:
+                ptrs.append(None)
+                continue
+            if len(x) != size:
+                raise ValueError(f"expected {size} entries, got {len(x)}")
+            if on_dev:
+                if str(x.dtype) != "torch.float32" or not x.is_contiguous():
+                    raise TypeError("device vectors must be contiguous float32 tensors")
+                ptrs.append(x.data_ptr())
+            else:
+                if not (isinstance(x, np.ndarray) and x.dtype == np.float32 and x.flags.c_contiguous):
+                    raise TypeError("host vectors must be contiguous float32 numpy arrays")
+                ptrs.append(x.ctypes.data)
+            keep.append(x)
+        return ptrs, on_dev, keep
+
+    @staticmethod
+    def _stats(st, errs):
+        return PageRankStats(int(st.iterations), float(st.final_error), bool(st.converged), float(st.device_ms),
+                             float(st.ms_per_iter), float(st.bytes_per_iter), float(st.gteps),
+                             None if errs is None else errs[: min(int(st.iterations), len(errs))])
+
+    @staticmethod
+    def _error_buffer(st, record, max_iters):
+        if not record:
+            return None
+        cap = int(min(max(int(max_iters), 1), 4096))
+        errs = np.zeros(cap, np.float64)
+        st.errors = errs.ctypes.data_as(C.POINTER(C.c_double))
+        st.errors_cap = cap
+        return errs
+
+    def weighted_page_rank(self, teleport, out, damping_factor=0.85, threshold=1e-6, max_iters=100, launch="graph",
+                           record_errors=False, stream=None) -> PageRankStats:
+        """Weighted PageRank with a teleport distribution (nwgpu_wpr_run):
+        r = (1-d) t + d W^T D_s^-1 r over the edge weights given at creation.
+        ``teleport`` has n entries (None: uniform 1/n); ``out`` is filled in place."""
+        (tp, op), dev, keep = self._f32_vectors([teleport, out], [self.n, self.n])
+        opt = self._options(launch, dev, stream)
+        st = N.PrStats()
+        errs = self._error_buffer(st, record_errors, max_iters)
+        N.check(N.lib().nwgpu_wpr_run(self.handle, tp, op, C.c_float(damping_factor), C.c_float(threshold),
+                                      int(max_iters), C.byref(opt), C.byref(st)))
+        del keep
+        return self._stats(st, errs)
+
+    def page_rank_vjp(self, ranks, dL_dr, dL_dw=None, dL_dt=None, damping_factor=0.85, threshold=1e-7,
+                      max_iters=1000, launch="graph", record_errors=False, stream=None) -> PageRankStats:
+        """Gradients of L = dL_dr . r at the weighted fixed point ``ranks``
+        (nwgpu_pr_vjp): dL/dw (nnz, input entry order) and dL/dt (n), each
+        filled in place when given. Returns the adjoint solve's stats."""
+        (rp, cp, wp, tp), dev, keep = self._f32_vectors([ranks, dL_dr, dL_dw, dL_dt],
+                                                        [self.n, self.n, self.nnz, self.n])
+        opt = self._options(launch, dev, stream)
+        st = N.PrStats()
+        errs = self._error_buffer(st, record_errors, max_iters)
+        N.check(N.lib().nwgpu_pr_vjp(self.handle, rp, cp, wp, tp, C.c_float(damping_factor), C.c_float(threshold),
+                                     int(max_iters), C.byref(opt), C.byref(st)))
+        del keep
+        return self._stats(st, errs)
+
+
 def page_rank(graph, degrees, page_rank, damping_factor=0.85, threshold=1e-4, max_iters=20, num_threads=None):
     """Drop-in for ``nw::graph::page_rank`` (page_rank.hpp:89-148).
 
