@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--no-relabel", action="store_true", help="keep the input vertex order on the device")
     ap.add_argument("--ppr-scale", type=int, default=22, help="graph scale of the batched-PPR comparison (0: skip)")
     ap.add_argument("--ppr-k", type=int, default=64)
+    ap.add_argument("--vjp-scale", type=int, default=20,
+                    help="graph scale of the weighted forward vs adjoint (backward) timing (0: skip)")
     ap.add_argument("--launch", default="graph", choices=["graph", "stream"],
                     help="sweep loop as a CUDA graph with a device-side while loop, or one launch per sweep")
     return ap.parse_args()
@@ -235,6 +237,45 @@ def ppr_batched_vs_looped(scale, k, stream):
             "all_converged": stb.all_converged, "max_abs_batched_vs_looped": worst}
 
 
+def vjp_vs_forward(scale, stream):
+    """Weighted PageRank forward and its implicit-adjoint backward on RMAT
+    `scale` (weights U(0.1, 1) seed 1234, uniform teleport, L = c . r with
+    c ~ N(0,1) seed 99). Each side runs to an FP64 L1 change of 1e-6 times its
+    own scale (1 for the ranks, sum |c| for the adjoint). Times with CUDA
+    events on `stream`."""
+    import torch
+    from nwgraph_b200 import Graph, graphs as G
+    g = G.rmat(scale, 16, 42)
+    dev = stream.device
+    w = torch.from_numpy(G.edge_weights(g.nnz, seed=1234)).to(dev)
+    c = torch.from_numpy(np.random.default_rng(99).standard_normal(g.n).astype(np.float32)).to(dev)
+    rp = torch.from_numpy(g.row_ptr.view(np.int32)).to(dev)
+    cl = torch.from_numpy(g.col.view(np.int32)).to(dev)
+    r = torch.empty(g.n, dtype=torch.float32, device=dev)
+    dw = torch.empty(g.nnz, dtype=torch.float32, device=dev)
+    dt = torch.empty(g.n, dtype=torch.float32, device=dev)
+    thr_b = 1e-6 * float(c.abs().sum())
+    with Graph(rp, cl, weights=w) as h:
+        fwd = lambda: h.weighted_page_rank(None, r, DAMPING, 1e-6, 1000, stream=stream)  # noqa: E731
+        bwd = lambda: h.page_rank_vjp(r, c, dw, dt, DAMPING, thr_b, 1000, stream=stream)  # noqa: E731
+        for _ in range(2):
+            fwd()
+            bwd()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        torch.cuda.synchronize()
+        e[0].record(stream)
+        sf = fwd()
+        e[1].record(stream)
+        sb = bwd()
+        e[2].record(stream)
+        torch.cuda.synchronize()
+    t_f, t_b = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
+    return {"graph": f"rmat{scale}_ef16_weighted", "n": g.n, "nnz": g.nnz, "forward_ms": t_f, "backward_ms": t_b,
+            "bwd_over_fwd": t_b / t_f, "forward_sweeps": sf.iterations, "adjoint_sweeps": sb.iterations,
+            "forward_ms_per_sweep": sf.ms_per_iter, "adjoint_ms_per_sweep": sb.ms_per_iter,
+            "backward_includes": "adjoint solve on the out-row CSR + dL/dw (nnz) + dL/dt (n)"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -364,6 +405,7 @@ def run_ours(args):
     h.release()
     del rp_h, cl_h, deg_h, out_h
     ppr = ppr_batched_vs_looped(args.ppr_scale, args.ppr_k, stream) if args.ppr_scale > 0 else None
+    vjp = vjp_vs_forward(args.vjp_scale, stream) if args.vjp_scale > 0 else None
 
     peak, peak_kind = peaks()
     achieved = B / (t_sweep_ms * 1e-3) / 1e9
@@ -399,6 +441,8 @@ def run_ours(args):
     }
     if ppr:
         line["ppr_batched_vs_looped"] = ppr
+    if vjp:
+        line["vjp_vs_forward"] = vjp
     if cpu:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)

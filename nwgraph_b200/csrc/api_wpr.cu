@@ -7,6 +7,15 @@
 // with the same degree-binned sweep over the out-row CSR, so no forward
 // iterates are stored; the gradients are one pass over the entries
 // (pr_weighted.cu).
+//
+// The adjoint is solved by restarted GMRES (Saad & Schultz 1986) with
+// classical Gram-Schmidt applied twice, an FP32 Krylov basis and FP64
+// reductions; one operator application A v = v - d P^T v is one adjoint
+// sweep. The plain fixed-point iteration converges at rate d on every mode
+// of P^T with eigenvalue 1 (one per connected component) and -1 (one per
+// bipartite component); GMRES removes each such cluster with one polynomial
+// factor and needs about as many sweeps as the forward solve.
+// NWGPU_VJP_SOLVER=jacobi selects the fixed-point iteration instead.
 #include <chrono>
 
 #include "handle.h"
@@ -16,7 +25,8 @@ using namespace nwgpu;
 namespace nwgpu {
 
 void WprBuffers::release(cudaStream_t s) {
-  void* ptrs[] = {t.row_ptr, t.col, t.w, t.fwd, t.s, vbase, vaux, r_int, stage, stage2, res, gw};
+  void* ptrs[] = {t.row_ptr, t.col, t.w, t.fwd, t.s, t.erow, vbase, vaux, r_int, stage, stage2, res, gw, basis, w, vneg,
+                  part, dout, f, q};
   for (void* p : ptrs) pool_free(p, s);
   tplan.release(s);
   *this = WprBuffers();
@@ -27,7 +37,7 @@ int ensure_wpr(nwgpu_graph* g) {
   if (b.ready) return NWGPU_OK;
   const uint64_t n = g->n, nnz = g->nnz;
   CK(build_transpose(g->g.row_ptr, g->g.col, g->g.w, n, nnz, g->sms, &b.t, g->stream), "out-row CSR");
-  g->device_bytes += (3 * (nnz + kPad) + 2 * (n + kPad) + 1) * sizeof(uint32_t);
+  g->device_bytes += (4 * (nnz + kPad) + 2 * (n + kPad) + 1) * sizeof(uint32_t);
   int rc = build_bin_plan(g, b.t.row_ptr, n, true, &b.tplan);
   if (rc) return rc;
   CK(dalloc(g, &b.vbase, n), "cudaMalloc(wpr base)");
@@ -35,6 +45,8 @@ int ensure_wpr(nwgpu_graph* g) {
   CK(dalloc(g, &b.r_int, n), "cudaMalloc(wpr ranks)");
   CK(dalloc(g, &b.stage, n), "cudaMalloc(wpr staging)");
   CK(dalloc(g, &b.stage2, n), "cudaMalloc(wpr staging)");
+  CK(dalloc(g, &b.f, n), "cudaMalloc(dL/dw factors)");
+  CK(dalloc(g, &b.q, n), "cudaMalloc(dL/dw offsets)");
   const uint64_t parts = (uint64_t)binned_sweep_grid(g->sms, true) + (uint64_t)b.tplan.finish_grid;
   CK(dalloc(g, &b.res, parts), "cudaMalloc(wpr residuals)");
   CK(cudaStreamSynchronize(g->stream), "wpr buffers");
@@ -110,6 +122,141 @@ int device_vector(const float* v, float* stage, uint64_t n, bool device_ptrs, cu
   return NWGPU_OK;
 }
 
+constexpr int kGmresRestart = 30;
+static_assert(kGmresRestart <= kGmresMaxBasis, "more basis vectors than the update kernel takes");
+
+int ensure_gmres(nwgpu_graph* g) {
+  WprBuffers& b = g->wpr;
+  if (b.basis) return NWGPU_OK;
+  const uint64_t n = g->n;
+  b.ld = (n + kPad + 3) & ~3ull;
+  const VecGrid vg = vec_grid(n, g->sms);
+  CK(dalloc(g, &b.basis, b.ld * (kGmresRestart + 1)), "cudaMalloc(Krylov basis)");
+  CK(dalloc(g, &b.w, n), "cudaMalloc(gmres work)");
+  CK(dalloc(g, &b.vneg, n), "cudaMalloc(gmres -d/s)");
+  CK(dalloc(g, &b.part, (uint64_t)vg.blocks * (kGmresRestart + 1)), "cudaMalloc(gmres partials)");
+  CK(dalloc(g, &b.dout, (uint64_t)kGmresRestart + 2), "cudaMalloc(gmres dots)");
+  return NWGPU_OK;
+}
+
+// out = A v = v - d P^T v: one adjoint sweep over the out-row CSR with
+// vbase = v and vaux = -d/s, reading v as the contribution vector.
+int apply_adjoint_op(nwgpu_graph* g, const SweepArgs& proto, const float* v, float* out, cudaStream_t s) {
+  WprBuffers& b = g->wpr;
+  SweepArgs   a = proto;
+  a.vbase = v;
+  a.vaux = b.vneg;
+  a.contrib0 = const_cast<float*>(v);
+  a.contrib1 = out;
+  a.rank = out;
+  CK(launch_op_state(g->st, s), "operator state");
+  const BinnedArgs ba = make_binned_args(g, b.tplan, a, kModeAdjoint);
+  CK(launch_binned_sweep(ba, b.tplan.hot, kModeAdjoint, binned_grid(g, b.tplan, kModeAdjoint), b.tplan.finish_grid, s),
+     "adjoint operator");
+  return NWGPU_OK;
+}
+
+int read_doubles(const double* d, double* h, int count, cudaStream_t s) {
+  CK(cudaMemcpyAsync(h, d, (size_t)count * sizeof(double), cudaMemcpyDeviceToHost, s), "copy reduction");
+  CK(cudaStreamSynchronize(s), "reduction");
+  return NWGPU_OK;
+}
+
+// Restarted GMRES for A x = c (c = vbase, internal order), x in/out (x0 on
+// entry). Stops when the L1 norm of the true residual c - A x, evaluated in
+// FP64 at the start of each cycle, is below thr, or after max_ops operator
+// applications. *ops = operator applications, *res_l1 = last true residual.
+int gmres_adjoint(nwgpu_graph* g, const SweepArgs& proto, const float* c, float* x, double thr, uint64_t max_ops,
+                  cudaStream_t s, uint64_t* ops, double* res_l1, bool* converged) {
+  WprBuffers&    b = g->wpr;
+  const uint64_t n = g->n;
+  const VecGrid  vg = vec_grid(n, g->sms);
+  const int      m = kGmresRestart;
+  auto           V = [&](int i) { return b.basis + (uint64_t)i * b.ld; };
+  double         H[kGmresRestart + 1][kGmresRestart], cs[kGmresRestart], sn[kGmresRestart], gv[kGmresRestart + 1];
+  double         h[kGmresRestart + 2];
+  float          coef[kGmresMaxBasis];
+  *ops = 0;
+  *converged = false;
+  int rc;
+  for (;;) {
+    // r = c - A x, its L1 norm (the fixed-point iteration's L1 change) and 2-norm
+    if ((rc = apply_adjoint_op(g, proto, x, b.w, s))) return rc;
+    ++*ops;
+    CK(launch_vec_axpby(1.f, c, 0.f, V(0), n, vg, b.part, nullptr, s), "residual");
+    CK(launch_vec_axpby(-1.f, b.w, 1.f, V(0), n, vg, b.part, b.dout, s), "residual");
+    CK(launch_vec_dots(V(0), b.ld, 1, V(0), n, vg, b.part, b.dout + 1, s), "residual norm");
+    if ((rc = read_doubles(b.dout, h, 2, s))) return rc;
+    *res_l1 = h[0];
+    if (h[0] < thr) {
+      *converged = true;
+      return NWGPU_OK;
+    }
+    if (*ops >= max_ops) return NWGPU_OK;
+    const double beta = sqrt(h[1]);
+    if (!(beta > 0.0)) return NWGPU_OK;
+    const double l1_per_l2 = h[0] / beta;  // how the L1 norm scales with the 2-norm this cycle
+    CK(launch_vec_axpby((float)(1.0 / beta), V(0), 0.f, V(0), n, vg, b.part, nullptr, s), "normalise");
+    for (int i = 0; i <= m; ++i) gv[i] = 0.0;
+    gv[0] = beta;
+    int k = 0;  // basis vectors used this cycle
+    for (int j = 0; j < m; ++j) {
+      if ((rc = apply_adjoint_op(g, proto, V(j), b.w, s))) return rc;
+      ++*ops;
+      // classical Gram-Schmidt, twice: h1 = V^T w; w' = w - V h1 with h2 = V^T w'
+      // and |w'|^2 in the same pass; the new vector (w' - V h2) / |w' - V h2|,
+      // whose norm is sqrt(|w'|^2 - |h2|^2)
+      double hj[kGmresRestart + 1] = {0.0};
+      CK(launch_vec_dots(V(0), b.ld, j + 1, b.w, n, vg, b.part, b.dout, s), "Gram-Schmidt dots");
+      if ((rc = read_doubles(b.dout, h, j + 1, s))) return rc;
+      for (int i = 0; i <= j; ++i) {
+        hj[i] = h[i];
+        coef[i] = (float)h[i];
+      }
+      CK(launch_vec_update(b.w, b.w, V(0), b.ld, j + 1, coef, 1.f, n, vg, b.part, b.dout, s), "Gram-Schmidt update");
+      if ((rc = read_doubles(b.dout, h, j + 2, s))) return rc;
+      double h2sq = 0.0;
+      for (int i = 0; i <= j; ++i) {
+        hj[i] += h[i];
+        coef[i] = (float)h[i];
+        h2sq += h[i] * h[i];
+      }
+      const double nrm2 = h[j + 1] - h2sq;
+      hj[j + 1] = nrm2 > 0.0 ? sqrt(nrm2) : 0.0;
+      // apply the previous rotations, then a new one that zeroes hj[j + 1]
+      for (int i = 0; i < j; ++i) {
+        const double t = cs[i] * hj[i] + sn[i] * hj[i + 1];
+        hj[i + 1] = -sn[i] * hj[i] + cs[i] * hj[i + 1];
+        hj[i] = t;
+      }
+      const double hn = hj[j + 1];
+      const double r = sqrt(hj[j] * hj[j] + hn * hn);
+      cs[j] = r > 0.0 ? hj[j] / r : 1.0;
+      sn[j] = r > 0.0 ? hn / r : 0.0;
+      hj[j] = r;
+      gv[j + 1] = -sn[j] * gv[j];
+      gv[j] = cs[j] * gv[j];
+      for (int i = 0; i <= j; ++i) H[i][j] = hj[i];
+      k = j + 1;
+      const bool breakdown = !(hn > 1e-30 * beta);
+      if (!breakdown)
+        CK(launch_vec_update(b.w, V(j + 1), V(0), b.ld, j + 1, coef, (float)(1.0 / hn), n, vg, b.part, nullptr, s),
+           "new basis vector");
+      // estimated L1 residual: the 2-norm estimate |g_{j+1}| scaled like this cycle's start
+      if (breakdown || fabs(gv[j + 1]) * l1_per_l2 < 0.5 * thr || *ops >= max_ops) break;
+    }
+    // x += V y, H y = g (upper triangular)
+    double y[kGmresRestart];
+    for (int i = k - 1; i >= 0; --i) {
+      double t = gv[i];
+      for (int l = i + 1; l < k; ++l) t -= H[i][l] * y[l];
+      y[i] = H[i][i] != 0.0 ? t / H[i][i] : 0.0;
+    }
+    for (int i = 0; i < k; ++i) coef[i] = (float)-y[i];
+    CK(launch_vec_update(x, x, V(0), b.ld, k, coef, 1.f, n, vg, b.part, nullptr, s), "update solution");
+  }
+}
+
 }  // namespace
 }  // namespace nwgpu
 
@@ -171,7 +318,6 @@ extern "C" int nwgpu_pr_vjp(nwgpu_graph* g, const float* ranks, const float* dL_
   if ((rc = device_vector(dL_dr, b.stage2, n, opt.device_ptrs != 0, s, &c))) return rc;
   CK(launch_vjp_prepare(r, c, g->g.inv, b.t.s, n, damping, b.r_int, b.vbase, b.vaux, g->rank, g->contrib[0], g->sms, s),
      "vjp prepare");
-  if ((rc = start_state(g, max_iters, threshold, s))) return rc;
   SweepArgs a = make_sweep_args(g, damping, 0.f, kTeleportUniform, 0u);
   a.row_ptr = b.t.row_ptr;
   a.col = b.t.col;
@@ -179,14 +325,31 @@ extern "C" int nwgpu_pr_vjp(nwgpu_graph* g, const float* ranks, const float* dL_
   a.vbase = b.vbase;
   a.vaux = b.vaux;
   a.res_part = b.res;
-  CK(cudaEventRecord(g->ev0, s), "cudaEventRecord");
-  PrState fin{};
-  if ((rc = run_sweeps(g, a, opt.launch, max_iters, s, &fin, &b.tplan, kModeAdjoint))) return rc;
+  const char* solver = getenv("NWGPU_VJP_SOLVER");
+  const bool  jacobi = solver && !strcmp(solver, "jacobi");
+  PrState     fin{};
+  if (jacobi) {
+    if ((rc = start_state(g, max_iters, threshold, s))) return rc;
+    CK(cudaEventRecord(g->ev0, s), "cudaEventRecord");
+    if ((rc = run_sweeps(g, a, opt.launch, max_iters, s, &fin, &b.tplan, kModeAdjoint))) return rc;
+  } else {
+    if ((rc = ensure_gmres(g))) return rc;
+    CK(launch_neg_dinv(b.t.s, n, damping, b.vneg, g->sms, s), "-d/s");
+    CK(cudaEventRecord(g->ev0, s), "cudaEventRecord");
+    uint64_t ops = 0;
+    double   res = 0.0;
+    bool     conv = false;
+    if ((rc = gmres_adjoint(g, a, b.vbase, g->rank, (double)threshold, max_iters, s, &ops, &res, &conv))) return rc;
+    fin.iter = ops;
+    fin.last_error = res;
+    fin.converged = conv ? 1u : 0u;
+  }
   // gradients from the adjoint l (in g->rank)
   if (dL_dw) {
     if (!opt.device_ptrs && !b.gw) CK(dalloc(g, &b.gw, nnz), "cudaMalloc(dL/dw staging)");
     float* dst = opt.device_ptrs ? dL_dw : b.gw;
-    CK(launch_vjp_grad_w(b.t, g->g.emap, b.r_int, g->rank, b.vbase, n, nnz, damping, dst, g->sms, s), "dL/dw");
+    CK(launch_vjp_grad_w(b.t, g->g.col, g->g.emap, b.r_int, g->rank, b.vbase, n, nnz, damping, b.f, b.q, dst, g->sms, s),
+       "dL/dw");
     if (!opt.device_ptrs) CK(cudaMemcpyAsync(dL_dw, dst, nnz * sizeof(float), cudaMemcpyDeviceToHost, s), "copy dL/dw");
   }
   if (dL_dt) {

@@ -53,6 +53,7 @@ struct Transposed {
   float*    w = nullptr;        // nnz: weight of the forward entry
   uint32_t* fwd = nullptr;      // nnz: the forward entry
   float*    s = nullptr;        // n: out-weight sums, FP64 row sums of w rounded to FP32
+  uint32_t* erow = nullptr;     // nnz: row of each forward entry
 };
 
 // Teleport term of the update r_i' = base_i + d * z_i.
@@ -125,11 +126,34 @@ cudaError_t launch_wpr_prepare(const float* t, const uint32_t* inv, const float*
 cudaError_t launch_vjp_prepare(const float* r, const float* c, const uint32_t* inv, const float* s, uint64_t n,
                                float damping, float* r_int, float* vbase, float* vaux, float* lam, float* contrib, int sms,
                                cudaStream_t st);
-cudaError_t launch_vjp_grad_w(const Transposed& t, const uint32_t* emap, const float* r_int, const float* lam,
-                              const float* c_int, uint64_t n, uint64_t nnz, float damping, float* d_w, int sms,
-                              cudaStream_t st);
+// dL/dw over the forward entries (col: the forward CSR's columns); f, q: n-float scratch
+cudaError_t launch_vjp_grad_w(const Transposed& t, const uint32_t* col, const uint32_t* emap, const float* r_int,
+                              const float* lam, const float* c_int, uint64_t n, uint64_t nnz, float damping, float* f,
+                              float* q, float* d_w, int sms, cudaStream_t st);
 cudaError_t launch_vjp_grad_t(const float* lam, const uint32_t* perm, uint64_t n, float damping, float* d_t, int sms,
                               cudaStream_t st);
+
+// Vector kernels of the GMRES adjoint solve (pr_weighted.cu). A VecGrid
+// splits n into contiguous per-block ranges; reductions are FP64, fixed order.
+constexpr int kGmresMaxBasis = 32;
+struct VecGrid {
+  int      blocks;
+  uint64_t chunk;
+};
+VecGrid     vec_grid(uint64_t n, int sms);
+// out[0..nv) = V_i . x for the nv (1..kGmresMaxBasis) vectors of V (stride
+// ld), out[nv] = x . x; part: blocks * (nv + 1) doubles
+cudaError_t launch_vec_dots(const float* V, uint64_t ld, int nv, const float* x, uint64_t n, const VecGrid& vg,
+                            double* part, double* out, cudaStream_t st);
+// y = scale * (x - sum_i coef[i] V_i) (x and y may alias); with out: the dots
+// of the V_i with y, and y . y, as launch_vec_dots writes them
+cudaError_t launch_vec_update(const float* x, float* y, const float* V, uint64_t ld, int nv, const float* coef, float scale,
+                              uint64_t n, const VecGrid& vg, double* part, double* out, cudaStream_t st);
+// y = alpha x + beta y; with l1_out: ||y||_1 after the update
+cudaError_t launch_vec_axpby(float alpha, const float* x, float beta, float* y, uint64_t n, const VecGrid& vg,
+                             double* part, double* l1_out, cudaStream_t st);
+cudaError_t launch_neg_dinv(const float* s, uint64_t n, float damping, float* vaux, int sms, cudaStream_t st);
+cudaError_t launch_op_state(PrState* st, cudaStream_t s);
 
 // pr_plain.cu
 cudaError_t launch_gather_u32(const uint32_t* src, const uint32_t* idx, uint32_t* dst, uint64_t n, int sms,

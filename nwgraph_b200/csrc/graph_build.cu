@@ -287,11 +287,10 @@ __global__ void out_weight_kernel(const uint32_t* __restrict__ trow, const float
 cudaError_t build_transpose(const uint32_t* d_row_ptr, const uint32_t* d_col, const float* d_w, uint64_t n, uint64_t nnz,
                             int sms, Transposed* out, cudaStream_t s) {
   cudaError_t e;
-  uint32_t *erow = nullptr, *ids = nullptr, *keys = nullptr, *cnt = nullptr;
+  uint32_t *ids = nullptr, *keys = nullptr, *cnt = nullptr;
   void*     tmp = nullptr;
   size_t    sort_bytes = 0, scan_bytes = 0;
   auto      cleanup = [&]() {
-    pool_free(erow, s);
     pool_free(ids, s);
     pool_free(keys, s);
     pool_free(cnt, s);
@@ -305,7 +304,8 @@ cudaError_t build_transpose(const uint32_t* d_row_ptr, const uint32_t* d_col, co
     }                               \
   } while (0)
   const int grid = sms * 8;
-  TK(pool_alloc_n(&erow, nnz + kPad, s));
+  TK(pool_alloc_n(&out->erow, nnz + kPad, s));
+  uint32_t* erow = out->erow;
   TK(pool_alloc_n(&ids, nnz + kPad, s));
   TK(pool_alloc_n(&keys, nnz + kPad, s));
   TK(pool_alloc_n(&cnt, n + 1, s));

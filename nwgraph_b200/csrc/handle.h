@@ -51,6 +51,16 @@ struct WprBuffers {
   float*     stage2 = nullptr;   // n: input-order staging
   double*    res = nullptr;      // residual partials of the adjoint sweep
   float*     gw = nullptr;       // nnz: dL/dw staging for host outputs
+  // GMRES adjoint: Krylov basis (kGmresRestart + 1 vectors of stride ld),
+  // operator output, -d/s, per-block reduction partials, reduction results
+  float*     basis = nullptr;
+  uint64_t   ld = 0;
+  float*     w = nullptr;
+  float*     vneg = nullptr;
+  double*    part = nullptr;
+  double*    dout = nullptr;
+  float*     f = nullptr;        // n: dL/dw factors d r_j / s_j
+  float*     q = nullptr;        // n: dL/dw offsets q_j
   void       release(cudaStream_t s);
 };
 
@@ -155,6 +165,10 @@ cudaError_t dalloc(nwgpu_graph* g, T** p, uint64_t count) {
 }
 int ensure_solve_buffers(nwgpu_graph* g);
 int build_bin_plan(nwgpu_graph* g, const uint32_t* row_ptr, uint64_t n, bool hot, BinPlan* p);
+// Sweep grid of a binned solve (the weighted and adjoint sweeps always use the
+// hot launch shape) and the kernel arguments of one.
+int        binned_grid(nwgpu_graph* g, const BinPlan& p, int mode);
+BinnedArgs make_binned_args(nwgpu_graph* g, const BinPlan& p, const SweepArgs& sw, int mode);
 // Sweep arguments over the handle's forward CSR and solve buffers.
 SweepArgs make_sweep_args(nwgpu_graph* g, float damping, float base, int teleport, uint32_t seed);
 // Runs the sweep loop from the state already on the device (CUDA graph or one
