@@ -62,7 +62,8 @@ static PprArgs make_ppr_args(nwgpu_graph* g, float damping) {
   a.cpart = b.cpart;
   a.epart = b.epart;
   a.res_part = b.res_part;
-  a.sweep_grid = (uint32_t)b.sweep_grid;
+  a.epi_grid = (uint32_t)b.finish_grid;
+  a.n = g->n;
   a.seeds = b.seeds;
   a.col_done = b.col_done;
   a.col_conv = b.col_conv;
@@ -135,7 +136,7 @@ extern "C" int nwgpu_ppr_batched(nwgpu_graph* g, const uint32_t* out_degree, con
       if (b.cg) cudaGraphDestroy(b.cg);
       b.cg_exec = nullptr;
       CK(cudaGraphCreate(&b.cg, 0), "cudaGraphCreate");
-      CK(build_ppr_graph(b.cg, a, K, b.sweep_grid, b.finish_grid, b.st, &b.cg_exec), "ppr graph");
+      CK(build_ppr_graph(b.cg, a, K, b.sweep_grid, b.st, &b.cg_exec), "ppr graph");
       b.cg_damping = damping;
     }
     const uint64_t max_launches = max_iters / kGraphChunk + 2;
@@ -150,7 +151,7 @@ extern "C" int nwgpu_ppr_batched(nwgpu_graph* g, const uint32_t* out_degree, con
     uint64_t launched = 0;
     for (;;) {
       const uint64_t batch = (max_iters - launched) < kGraphChunk ? (max_iters - launched) : kGraphChunk;
-      for (uint64_t i = 0; i < batch; ++i) CK(launch_ppr_sweep(a, K, b.sweep_grid, b.finish_grid, s), "ppr sweep");
+      for (uint64_t i = 0; i < batch; ++i) CK(launch_ppr_sweep(a, K, b.sweep_grid, s), "ppr sweep");
       launched += batch;
       CK(cudaMemcpyAsync(b.h_st, b.st, sizeof(PprState), cudaMemcpyDeviceToHost, s), "copy ppr state");
       CK(cudaStreamSynchronize(s), "ppr sweep loop");

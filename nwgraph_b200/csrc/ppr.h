@@ -7,7 +7,6 @@
 namespace nwgpu {
 
 constexpr int kPprTileItems = 512;  // merge items per warp tile
-constexpr int kPprPrefetch = 8;     // gathered rows in flight per warp
 
 struct PprState {
   unsigned long long iter;
@@ -33,8 +32,9 @@ struct PprArgs {
   float*          contrib1;
   float*          cpart;     // num_tiles x K
   float*          epart;
-  double*         res_part;  // (sweep_grid + finish_grid) x K
-  uint32_t        sweep_grid;
+  double*         res_part;  // epi_grid x K: the epilogue's per-CTA column residuals
+  uint32_t        epi_grid;
+  uint64_t        n;
   const uint32_t* seeds;     // K internal seed ids (0xffffffff: padding column)
   uint32_t*       col_done;  // K flags
   uint32_t*       col_conv;  // K flags
@@ -55,8 +55,8 @@ cudaError_t launch_ppr_seeds(const uint32_t* seeds_in, uint32_t k, int K, const 
 cudaError_t launch_ppr_init(const PprArgs& a, int K, uint64_t n, int sms, cudaStream_t s);
 cudaError_t launch_ppr_output(const float* rank, const uint32_t* perm, uint64_t n, int K, uint32_t k, float* out,
                               int sms, cudaStream_t s);
-cudaError_t launch_ppr_sweep(const PprArgs& a, int K, int sweep_grid, int finish_grid, cudaStream_t s);
-cudaError_t build_ppr_graph(cudaGraph_t g, const PprArgs& proto, int K, int sweep_grid, int finish_grid,
-                            PprState* st, cudaGraphExec_t* exec);
+cudaError_t launch_ppr_sweep(const PprArgs& a, int K, int sweep_grid, cudaStream_t s);
+cudaError_t build_ppr_graph(cudaGraph_t g, const PprArgs& proto, int K, int sweep_grid, PprState* st,
+                            cudaGraphExec_t* exec);
 
 }  // namespace nwgpu

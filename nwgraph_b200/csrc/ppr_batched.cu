@@ -10,11 +10,12 @@
 // whose FP64 L1 change is below the threshold; its values are then frozen
 // while the other columns continue.
 //
-// Work decomposition: merge-path tiles of W items per WARP (lanes own K/32
-// columns each). A warp walks its tile's entries in order with U gathers in
-// flight, finishing rows as their end items come up; rows that cross tiles
-// leave a K-vector partial per tile, summed in tile order by the finishing
-// kernel, which also reduces the per-column residuals and tests convergence.
+// One sweep is four kernels: the gather (merge-path tiles of W items per
+// warp, lanes owning K/32 columns each, rows of the contribution matrix
+// loaded U at a time with the next group in flight), the fix-up of rows that
+// cross tiles, a streaming epilogue over the n x K matrix (update, FP64
+// per-column residual, next contributions) and the per-column convergence
+// test.
 #include "common.cuh"
 #include "engine.h"
 #include "ppr.h"
@@ -47,35 +48,34 @@ __device__ __forceinline__ void load_row(Cols<K>& out, const float* __restrict__
   }
 }
 
-// Row epilogue for the K columns of internal row r; returns nothing, adds the
-// per-column |dr| into res.
-template <int K>
-__device__ __forceinline__ void ppr_row_epilogue(const PprArgs& a, float* __restrict__ cout, uint32_t r,
-                                                 const Cols<K>& z, double (&res)[Cols<K>::PER_LANE], int lane,
-                                                 uint32_t active_bits, const uint32_t (&seed)[Cols<K>::PER_LANE]) {
-  constexpr int P = Cols<K>::PER_LANE;
-  const float   dg = (float)__ldg(a.deg + r);
-  float*        rk = a.rank + (uint64_t)r * K + lane * P;
-  float*        co = cout + (uint64_t)r * K + lane * P;
+// ---------------------------------------------------------------------------
+// Gather: merge-path tiles of W items per warp. A warp walks its tile's
+// entries in order, U rows of the contribution matrix per group, and loads
+// the next group while it sums the current one (2 * U * K * 4 bytes in flight
+// per warp: 4 KB for every K). Column ids and row ends of the tile are staged
+// in shared memory; the next row end sits in a register. A finished row only
+// stores its K sums (z) into the output contribution matrix: the update, the
+// residual and the next contributions are the epilogue kernel's, so nothing
+// in this loop waits on a load other than the gathers. The first row of a
+// tile that started in an earlier tile leaves its partial in epart[t], the
+// last row that continues past the tile in cpart[t].
+// ---------------------------------------------------------------------------
+template <int K, int U>
+__device__ __forceinline__ void load_group(Cols<K> (&v)[U], const float* __restrict__ cin, const uint32_t* s_col, int g,
+                                           int E, int lane, uint64_t pol) {
 #pragma unroll
-  for (int q = 0; q < P; ++q) {
-    if (!((active_bits >> q) & 1u)) continue;
-    const float tele = (seed[q] == r) ? a.one_minus_d : 0.f;
-    const float nr = fmaf(a.damping, z.v[q], tele);
-    const float old = rk[q];
-    rk[q] = nr;
-    co[q] = nr / dg;
-    res[q] += (double)fabsf(nr - old);
+  for (int u = 0; u < U; ++u) {
+    const int e = g * U + u;
+    if (e < E) load_row<K>(v[u], cin, s_col[e], lane, pol);
   }
 }
 
 template <int K, int W, int U>
-__global__ void __launch_bounds__(256) ppr_sweep_kernel(const PprArgs a) {
+__global__ void __launch_bounds__(256) ppr_gather_kernel(const PprArgs a) {
   constexpr int P = Cols<K>::PER_LANE;
   constexpr int NWARP = 256 / 32;
   __shared__ uint32_t s_col[NWARP][W + 1];
   __shared__ uint32_t s_rp[NWARP][W + 2];
-  __shared__ double   s_res[NWARP][K];
   const int           lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   PprState*           st = a.st;
   if (a.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.cond, 0u);
@@ -84,18 +84,6 @@ __global__ void __launch_bounds__(256) ppr_sweep_kernel(const PprArgs a) {
   const float* __restrict__ cin = (it & 1ull) ? a.contrib1 : a.contrib0;
   float* __restrict__ cout = (it & 1ull) ? a.contrib0 : a.contrib1;
   const uint64_t pol = policy_evict_last();
-
-  // this lane's columns: active mask and internal seeds
-  uint32_t active = 0, seed[P];
-#pragma unroll
-  for (int q = 0; q < P; ++q) {
-    const int c = lane * P + q;
-    seed[q] = a.seeds[c];
-    if (!a.col_done[c]) active |= 1u << q;
-  }
-  double res[P];
-#pragma unroll
-  for (int q = 0; q < P; ++q) res[q] = 0.0;
 
   const uint32_t gwarp = blockIdx.x * NWARP + warp, nwarps = gridDim.x * NWARP;
   for (uint32_t t = gwarp; t < a.num_tiles; t += nwarps) {
@@ -109,120 +97,129 @@ __global__ void __launch_bounds__(256) ppr_sweep_kernel(const PprArgs a) {
     Cols<K>    acc;
 #pragma unroll
     for (int q = 0; q < P; ++q) acc.v[q] = 0.f;
-    int i = 0;  // next row (relative) whose end item has not been consumed
-    // finish rows whose end comes before entry index `upto` (relative)
-    auto finish_rows = [&](int upto) {
-      while (i < R && (int)(s_rp[warp][i + 1] - k0) <= upto) {
-        if (i == 0 && is_cont) {
+    int i = 0;  // next row (relative) to finish
+    int next_end = (R > 0) ? (int)(s_rp[warp][1] - k0) : 0x7fffffff;
+    auto flush = [&]() {
+      float* dst = (i == 0 && is_cont) ? a.epart + (uint64_t)t * K : cout + (uint64_t)(r0 + i) * K;
 #pragma unroll
-          for (int q = 0; q < P; ++q) a.epart[(uint64_t)t * K + lane * P + q] = acc.v[q];
-        } else {
-          ppr_row_epilogue<K>(a, cout, r0 + i, acc, res, lane, active, seed);
-        }
-#pragma unroll
-        for (int q = 0; q < P; ++q) acc.v[q] = 0.f;
-        ++i;
+      for (int q = 0; q < P; ++q) {
+        dst[lane * P + q] = acc.v[q];
+        acc.v[q] = 0.f;
       }
+      ++i;
+      next_end = (i < R) ? (int)(s_rp[warp][i + 1] - k0) : 0x7fffffff;
     };
-    for (int kk = 0; kk < E; kk += U) {
-      Cols<K> v[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u)
-        if (kk + u < E) load_row<K>(v[u], cin, s_col[warp][kk + u], lane, pol);
+    auto consume = [&](const Cols<K>(&v)[U], int g) {
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        if (kk + u < E) {
-          finish_rows(kk + u);
+        const int e = g * U + u;
+        if (e < E) {
+          while (next_end <= e) flush();
 #pragma unroll
           for (int q = 0; q < P; ++q) acc.v[q] += v[u].v[q];
         }
       }
+    };
+    Cols<K> va[U], vb[U];
+    load_group<K, U>(va, cin, s_col[warp], 0, E, lane, pol);
+    for (int g = 0; g * U < E; g += 2) {
+      load_group<K, U>(vb, cin, s_col[warp], g + 1, E, lane, pol);
+      consume(va, g);
+      if ((g + 1) * U >= E) break;
+      load_group<K, U>(va, cin, s_col[warp], g + 2, E, lane, pol);
+      consume(vb, g + 1);
     }
-    finish_rows(0x7fffffff);
+    while (next_end <= E) flush();  // rows ending at the tile's last entry, and empty rows after it
     if (has_co) {
 #pragma unroll
       for (int q = 0; q < P; ++q) a.cpart[(uint64_t)t * K + lane * P + q] = acc.v[q];
     }
     __syncwarp();
   }
-  // per-column residual: warps -> CTA partial (fixed order)
-#pragma unroll
-  for (int q = 0; q < P; ++q) s_res[warp][lane * P + q] = res[q];
-  __syncthreads();
-  for (int c = threadIdx.x; c < K; c += blockDim.x) {
-    double b = 0.0;
-#pragma unroll
-    for (int w = 0; w < NWARP; ++w) b += s_res[w][c];
-    a.res_part[(uint64_t)blockIdx.x * K + c] = b;
-  }
 }
 
-// Rows crossing warp tiles, per-column residual reduction and convergence.
+// Rows that cross warp tiles: one warp per tile boundary ta whose carried-out
+// row S starts in ta; z(S) = sum of its tile partials in tile order.
 template <int K>
-__global__ void __launch_bounds__(256) ppr_finish_kernel(const PprArgs a) {
+__global__ void __launch_bounds__(256) ppr_fixup_kernel(const PprArgs a) {
   constexpr int P = Cols<K>::PER_LANE;
-  constexpr int NWARP = 256 / 32;
-  __shared__ double s_res[NWARP][K];
-  __shared__ int    s_last;
-  const int         lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  PprState*         st = a.st;
+  PprState*     st = a.st;
   if (*(volatile unsigned int*)&st->done) return;
   const unsigned long long it = *(volatile unsigned long long*)&st->iter;
   float* __restrict__ cout = (it & 1ull) ? a.contrib0 : a.contrib1;
   const uint32_t D = a.tile_items, T = a.num_tiles;
-  uint32_t       active = 0, seed[P];
-#pragma unroll
-  for (int q = 0; q < P; ++q) {
-    const int c = lane * P + q;
-    seed[q] = a.seeds[c];
-    if (!a.col_done[c]) active |= 1u << q;
-  }
-  double res[P];
-#pragma unroll
-  for (int q = 0; q < P; ++q) res[q] = 0.0;
-  // one warp per tile boundary: the row carried out of tile ta, if it starts there
-  const uint32_t gwarp = blockIdx.x * NWARP + warp, nwarps = gridDim.x * NWARP;
+  const int      lane = threadIdx.x & 31;
+  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t ta = gwarp; ta + 1 < T; ta += nwarps) {
     const uint32_t S = a.tile_row[ta + 1];
     const uint32_t k1 = a.tile_nnz[ta + 1], rs = a.row_ptr[S];
     if (!(k1 > rs && ((uint64_t)S + rs) / D == ta)) continue;
     const uint32_t tb = (uint32_t)(((uint64_t)S + a.row_ptr[S + 1]) / D);
-    Cols<K>        z;
+    float          z[P];
 #pragma unroll
-    for (int q = 0; q < P; ++q) z.v[q] = 0.f;
+    for (int q = 0; q < P; ++q) z[q] = 0.f;
     for (uint32_t u = ta; u < tb; ++u)
 #pragma unroll
-      for (int q = 0; q < P; ++q) z.v[q] += __ldcg(a.cpart + (uint64_t)u * K + lane * P + q);
+      for (int q = 0; q < P; ++q) z[q] += __ldcg(a.cpart + (uint64_t)u * K + lane * P + q);
 #pragma unroll
-    for (int q = 0; q < P; ++q) z.v[q] += __ldcg(a.epart + (uint64_t)tb * K + lane * P + q);
-    ppr_row_epilogue<K>(a, cout, S, z, res, lane, active, seed);
+    for (int q = 0; q < P; ++q) cout[(uint64_t)S * K + lane * P + q] = z[q] + __ldcg(a.epart + (uint64_t)tb * K + lane * P + q);
   }
-#pragma unroll
-  for (int q = 0; q < P; ++q) s_res[warp][lane * P + q] = res[q];
+}
+
+// Epilogue, streaming over the n x K matrix: for each active column c,
+// r' = (1 - d)[i == seed_c] + d z, contrib = r' / deg_i, FP64 |r' - r| into
+// per-CTA column partials. Converged columns keep their ranks. The grid
+// stride is a multiple of K, so every thread stays on one column.
+template <int K>
+__global__ void __launch_bounds__(256) ppr_epilogue_kernel(const PprArgs a, uint64_t n) {
+  __shared__ double s_res[256];
+  PprState*         st = a.st;
+  if (*(volatile unsigned int*)&st->done) return;
+  const unsigned long long it = *(volatile unsigned long long*)&st->iter;
+  float* __restrict__ cout = (it & 1ull) ? a.contrib0 : a.contrib1;
+  const uint64_t total = n * K, stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t x0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int      c = (int)(x0 % K);
+  const bool     active = a.col_done[c] == 0u;
+  const uint32_t seed = a.seeds[c];
+  double         res = 0.0;
+  if (active) {
+    for (uint64_t x = x0; x < total; x += stride) {
+      const uint32_t i = (uint32_t)(x / K);
+      const float    z = __ldcs(cout + x);
+      const float    tele = (seed == i) ? a.one_minus_d : 0.f;
+      const float    nr = fmaf(a.damping, z, tele);
+      const float    old = __ldcs(a.rank + x);
+      __stcs(a.rank + x, nr);
+      st_keep(cout + x, nr / (float)__ldg(a.deg + i), policy_evict_last());
+      res += (double)fabsf(nr - old);
+    }
+  }
+  s_res[threadIdx.x] = res;
   __syncthreads();
-  for (int c = threadIdx.x; c < K; c += blockDim.x) {
+  if (threadIdx.x < K) {
     double b = 0.0;
-#pragma unroll
-    for (int w = 0; w < NWARP; ++w) b += s_res[w][c];
-    a.res_part[(uint64_t)(a.sweep_grid + blockIdx.x) * K + c] = b;
+    for (int j = threadIdx.x; j < (int)blockDim.x; j += K) b += s_res[j];
+    a.res_part[(uint64_t)blockIdx.x * K + threadIdx.x] = b;
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    s_last = (atomicAdd(&st->ticket, 1u) == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  // last CTA: one warp per column sums the CTA partials (lane-strided, fixed tree)
+}
+
+// Per-column residuals over the epilogue's CTAs (one warp per column,
+// lane-strided, fixed tree) and the per-column convergence test.
+template <int K>
+__global__ void __launch_bounds__(256) ppr_finish_kernel(const PprArgs a) {
+  constexpr int NWARP = 256 / 32;
   __shared__ int s_all_done;
+  PprState*      st = a.st;
+  if (*(volatile unsigned int*)&st->done) return;
+  const unsigned long long it = *(volatile unsigned long long*)&st->iter;
+  const int      lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) s_all_done = 1;
   __syncthreads();
-  const uint32_t parts = a.sweep_grid + gridDim.x;
   for (int c = warp; c < K; c += NWARP) {
     if (a.col_done[c]) continue;  // uniform across the warp
     double e = 0.0;
-    for (uint32_t u = lane; u < parts; u += 32) e += __ldcg(a.res_part + (uint64_t)u * K + c);
+    for (uint32_t u = lane; u < a.epi_grid; u += 32) e += __ldcg(a.res_part + (uint64_t)u * K + c);
     e = warp_sum_lane0(e);
     if (lane == 0) {
       a.col_err[c] = e;
@@ -243,7 +240,6 @@ __global__ void __launch_bounds__(256) ppr_finish_kernel(const PprArgs a) {
     const bool done = s_all_done || done_iters >= st->max_iters || abort;
     st->aborted = (abort && !s_all_done) ? 1u : 0u;
     st->done = done ? 1u : 0u;
-    st->ticket = 0u;
     __threadfence();
     if (a.use_cond && !done && done_iters < st->chunk_end) cudaGraphSetConditional(a.cond, 1u);
   }
@@ -303,34 +299,43 @@ cudaError_t launch_ppr_seeds(const uint32_t* seeds_in, uint32_t k, int K, const 
 
 __global__ void ppr_arm_kernel(PprState* st) { st->chunk_end = st->iter + kGraphChunk; }
 
+// Rows per group: U * K = 512 floats, 2 KB of rows per group (16 floats per lane).
 template <int K>
 struct PprKernels {
-  static void* sweep() { return (void*)ppr_sweep_kernel<K, kPprTileItems, kPprPrefetch>; }
-  static void* finish() { return (void*)ppr_finish_kernel<K>; }
+  static constexpr int U = 512 / K;
+  static void*         gather() { return (void*)ppr_gather_kernel<K, kPprTileItems, U>; }
+  static void*         fixup() { return (void*)ppr_fixup_kernel<K>; }
+  static void*         epilogue() { return (void*)ppr_epilogue_kernel<K>; }
+  static void*         finish() { return (void*)ppr_finish_kernel<K>; }
 };
 
-static void* ppr_sweep_fn(int K) {
+// kernel 0 gather, 1 fix-up, 2 epilogue, 3 finish
+static void* ppr_fn(int K, int which) {
   switch (K) {
-    case 32: return PprKernels<32>::sweep();
-    case 64: return PprKernels<64>::sweep();
-    case 128: return PprKernels<128>::sweep();
+    case 32: return which == 0 ? PprKernels<32>::gather() : which == 1 ? PprKernels<32>::fixup()
+                    : which == 2 ? PprKernels<32>::epilogue() : PprKernels<32>::finish();
+    case 64: return which == 0 ? PprKernels<64>::gather() : which == 1 ? PprKernels<64>::fixup()
+                    : which == 2 ? PprKernels<64>::epilogue() : PprKernels<64>::finish();
+    case 128: return which == 0 ? PprKernels<128>::gather() : which == 1 ? PprKernels<128>::fixup()
+                     : which == 2 ? PprKernels<128>::epilogue() : PprKernels<128>::finish();
     default: return nullptr;
   }
 }
-static void* ppr_finish_fn(int K) {
-  switch (K) {
-    case 32: return PprKernels<32>::finish();
-    case 64: return PprKernels<64>::finish();
-    case 128: return PprKernels<128>::finish();
-    default: return nullptr;
-  }
+
+// Grid of each kernel: gather persistent at its occupancy, fix-up one warp
+// per tile boundary, epilogue epi_grid CTAs, finish one CTA.
+static dim3 ppr_grid(const PprArgs& a, int which, int sweep_grid) {
+  if (which == 0) return dim3((unsigned)sweep_grid);
+  if (which == 1) return dim3((a.num_tiles + 7u) / 8u ? (a.num_tiles + 7u) / 8u : 1u);
+  if (which == 2) return dim3(a.epi_grid);
+  return dim3(1);
 }
 
 int ppr_padded_k(uint32_t k) { return k <= 32 ? 32 : (k <= 64 ? 64 : (k <= 128 ? 128 : 0)); }
 
 int ppr_sweep_grid(int K, int sms) {
   int nb = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppr_sweep_fn(K), 256, 0) != cudaSuccess || nb < 1) nb = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppr_fn(K, 0), 256, 0) != cudaSuccess || nb < 1) nb = 1;
   return sms * nb;
 }
 
@@ -355,15 +360,19 @@ cudaError_t launch_ppr_output(const float* rank, const uint32_t* perm, uint64_t 
   return cudaGetLastError();
 }
 
-cudaError_t launch_ppr_sweep(const PprArgs& a, int K, int sweep_grid, int finish_grid, cudaStream_t s) {
+cudaError_t launch_ppr_sweep(const PprArgs& a, int K, int sweep_grid, cudaStream_t s) {
   void* args[] = {(void*)&a};
-  cudaError_t e = cudaLaunchKernel(ppr_sweep_fn(K), dim3(sweep_grid), dim3(256), args, 0, s);
-  if (e != cudaSuccess) return e;
-  return cudaLaunchKernel(ppr_finish_fn(K), dim3(finish_grid), dim3(256), args, 0, s);
+  for (int w = 0; w < 4; ++w) {
+    uint64_t    n = a.n;
+    void*       eargs[] = {(void*)&a, (void*)&n};
+    cudaError_t e = cudaLaunchKernel(ppr_fn(K, w), ppr_grid(a, w, sweep_grid), dim3(256), w == 2 ? eargs : args, 0, s);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
-cudaError_t build_ppr_graph(cudaGraph_t g, const PprArgs& proto, int K, int sweep_grid, int finish_grid,
-                            PprState* st, cudaGraphExec_t* exec) {
+cudaError_t build_ppr_graph(cudaGraph_t g, const PprArgs& proto, int K, int sweep_grid, PprState* st,
+                            cudaGraphExec_t* exec) {
   cudaGraphNode_t      arm;
   cudaKernelNodeParams kp = {};
   void*                sargs[] = {(void*)&st};
@@ -386,18 +395,20 @@ cudaError_t build_ppr_graph(cudaGraph_t g, const PprArgs& proto, int K, int swee
   PprArgs     a = proto;
   a.cond = cond;
   a.use_cond = 1;
+  uint64_t             n = a.n;
   void*                args[] = {(void*)&a};
-  cudaKernelNodeParams sp = {};
-  sp.func = ppr_sweep_fn(K);
-  sp.gridDim = dim3(sweep_grid);
-  sp.blockDim = dim3(256);
-  sp.kernelParams = args;
-  cudaGraphNode_t sn, fn;
-  if ((e = cudaGraphAddKernelNode(&sn, body, nullptr, 0, &sp)) != cudaSuccess) return e;
-  cudaKernelNodeParams fp = sp;
-  fp.func = ppr_finish_fn(K);
-  fp.gridDim = dim3(finish_grid);
-  if ((e = cudaGraphAddKernelNode(&fn, body, &sn, 1, &fp)) != cudaSuccess) return e;
+  void*                eargs[] = {(void*)&a, (void*)&n};
+  cudaGraphNode_t      prev = nullptr;
+  for (int w = 0; w < 4; ++w) {
+    cudaKernelNodeParams kp2 = {};
+    kp2.func = ppr_fn(K, w);
+    kp2.gridDim = ppr_grid(a, w, sweep_grid);
+    kp2.blockDim = dim3(256);
+    kp2.kernelParams = w == 2 ? eargs : args;
+    cudaGraphNode_t node;
+    if ((e = cudaGraphAddKernelNode(&node, body, prev ? &prev : nullptr, prev ? 1 : 0, &kp2)) != cudaSuccess) return e;
+    prev = node;
+  }
   return cudaGraphInstantiate(exec, g, 0);
 }
 
