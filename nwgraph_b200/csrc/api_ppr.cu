@@ -64,6 +64,7 @@ static PprArgs make_ppr_args(nwgpu_graph* g, float damping) {
   a.res_part = b.res_part;
   a.epi_grid = (uint32_t)b.finish_grid;
   a.n = g->n;
+
   a.seeds = b.seeds;
   a.col_done = b.col_done;
   a.col_conv = b.col_conv;

@@ -20,6 +20,12 @@ __device__ __forceinline__ uint64_t policy_evict_last() {
   asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
   return pol;
 }
+// L2 evict-first policy for data read or written once per sweep.
+__device__ __forceinline__ uint64_t policy_evict_first() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
 // Read-only gather through L1 with the L2 evict-last hint.
 __device__ __forceinline__ float ld_gather(const float* p, uint64_t pol) {
   float v;
@@ -42,6 +48,12 @@ __device__ __forceinline__ float4 ld_gather4(const float4* p, uint64_t pol) {
 // Store of the next sweep's gather source, kept in L2.
 __device__ __forceinline__ void st_keep(float* p, float v, uint64_t pol) {
   asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(p), "f"(v), "l"(pol) : "memory");
+}
+
+__device__ __forceinline__ void st_keep4(float4* p, float4 v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(p), "f"(v.x), "f"(v.y), "f"(v.z),
+               "f"(v.w), "l"(pol)
+               : "memory");
 }
 
 // Deterministic warp sum: fixed shuffle-down tree, result valid in lane 0.

@@ -63,10 +63,13 @@ __device__ __forceinline__ void load_row(Cols<K>& out, const float* __restrict__
 template <int K, int U>
 __device__ __forceinline__ void load_group(Cols<K> (&v)[U], const float* __restrict__ cin, const uint32_t* s_col, int g,
                                            int E, int lane, uint64_t pol) {
+  if ((g + 1) * U <= E) {  // a full group: no bounds checks
 #pragma unroll
-  for (int u = 0; u < U; ++u) {
-    const int e = g * U + u;
-    if (e < E) load_row<K>(v[u], cin, s_col[e], lane, pol);
+    for (int u = 0; u < U; ++u) load_row<K>(v[u], cin, s_col[g * U + u], lane, pol);
+  } else {
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (g * U + u < E) load_row<K>(v[u], cin, s_col[g * U + u], lane, pol);
   }
 }
 
@@ -110,9 +113,17 @@ __global__ void __launch_bounds__(256) ppr_gather_kernel(const PprArgs a) {
       next_end = (i < R) ? (int)(s_rp[warp][i + 1] - k0) : 0x7fffffff;
     };
     auto consume = [&](const Cols<K>(&v)[U], int g) {
+      const int e0 = g * U;
+      if (next_end >= e0 + U && e0 + U <= E) {  // a full group inside the current row
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+          for (int q = 0; q < P; ++q) acc.v[q] += v[u].v[q];
+        return;
+      }
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const int e = g * U + u;
+        const int e = e0 + u;
         if (e < E) {
           while (next_end <= e) flush();
 #pragma unroll
@@ -166,40 +177,59 @@ __global__ void __launch_bounds__(256) ppr_fixup_kernel(const PprArgs a) {
   }
 }
 
-// Epilogue, streaming over the n x K matrix: for each active column c,
-// r' = (1 - d)[i == seed_c] + d z, contrib = r' / deg_i, FP64 |r' - r| into
-// per-CTA column partials. Converged columns keep their ranks. The grid
-// stride is a multiple of K, so every thread stays on one column.
+// Epilogue, streaming over the n x K matrix, four columns per thread (16-byte
+// loads and stores): for each active column c, r' = (1 - d)[i == seed_c] + d z,
+// FP64 |r' - r| into per-CTA column partials; converged columns keep their
+// ranks. contrib = r' / deg_i for every column. The grid stride is a multiple
+// of K / 4, so every thread stays on one group of four columns.
 template <int K>
 __global__ void __launch_bounds__(256) ppr_epilogue_kernel(const PprArgs a, uint64_t n) {
-  __shared__ double s_res[256];
+  constexpr int     C4 = K / 4;
+  __shared__ double s_res[256][4];
   PprState*         st = a.st;
   if (*(volatile unsigned int*)&st->done) return;
   const unsigned long long it = *(volatile unsigned long long*)&st->iter;
   float* __restrict__ cout = (it & 1ull) ? a.contrib0 : a.contrib1;
-  const uint64_t total = n * K, stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t total = n * C4, stride = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t x0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int      c = (int)(x0 % K);
-  const bool     active = a.col_done[c] == 0u;
-  const uint32_t seed = a.seeds[c];
-  double         res = 0.0;
-  if (active) {
+  const int      c0 = (int)(x0 % C4) * 4;
+  bool           act[4];
+  uint32_t       seed[4];
+  bool           any = false;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    act[q] = a.col_done[c0 + q] == 0u;
+    seed[q] = a.seeds[c0 + q];
+    any = any || act[q];
+  }
+  const uint64_t pol = policy_evict_last();
+  double         res[4] = {0.0, 0.0, 0.0, 0.0};
+  if (any) {
     for (uint64_t x = x0; x < total; x += stride) {
-      const uint32_t i = (uint32_t)(x / K);
-      const float    z = __ldcs(cout + x);
-      const float    tele = (seed == i) ? a.one_minus_d : 0.f;
-      const float    nr = fmaf(a.damping, z, tele);
-      const float    old = __ldcs(a.rank + x);
-      __stcs(a.rank + x, nr);
-      st_keep(cout + x, nr / (float)__ldg(a.deg + i), policy_evict_last());
-      res += (double)fabsf(nr - old);
+      const uint32_t i = (uint32_t)(x / C4);
+      const float4   z = __ldcs(reinterpret_cast<const float4*>(cout) + x);
+      const float4   old = __ldcs(reinterpret_cast<const float4*>(a.rank) + x);
+      const float    dg = (float)__ldg(a.deg + i);
+      const float    zv[4] = {z.x, z.y, z.z, z.w}, ov[4] = {old.x, old.y, old.z, old.w};
+      float          nr[4], co[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const float tele = (seed[q] == i) ? a.one_minus_d : 0.f;
+        nr[q] = act[q] ? fmaf(a.damping, zv[q], tele) : ov[q];
+        co[q] = nr[q] / dg;
+        if (act[q]) res[q] += (double)fabsf(nr[q] - ov[q]);
+      }
+      __stcs(reinterpret_cast<float4*>(a.rank) + x, make_float4(nr[0], nr[1], nr[2], nr[3]));
+      st_keep4(reinterpret_cast<float4*>(cout) + x, make_float4(co[0], co[1], co[2], co[3]), pol);
     }
   }
-  s_res[threadIdx.x] = res;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) s_res[threadIdx.x][q] = res[q];
   __syncthreads();
   if (threadIdx.x < K) {
-    double b = 0.0;
-    for (int j = threadIdx.x; j < (int)blockDim.x; j += K) b += s_res[j];
+    const int g = threadIdx.x / 4, q = threadIdx.x % 4;
+    double    b = 0.0;
+    for (int j = g; j < (int)blockDim.x; j += C4) b += s_res[j][q];
     a.res_part[(uint64_t)blockIdx.x * K + threadIdx.x] = b;
   }
 }
