@@ -11,7 +11,7 @@ void PprBuffers::release(cudaStream_t s) {
   cg_exec = nullptr;
   cg = nullptr;
   void* ptrs[] = {tiling.tile_row, tiling.tile_nnz, rank, contrib[0], contrib[1], out, cpart, epart, res_part,
-                  seeds, seeds_in, col_done, col_conv, col_iters, col_err, st};
+                  spans, seeds, seeds_in, col_done, col_conv, col_iters, col_err, st};
   for (void* p : ptrs) pool_free(p, s);
   if (h_st) cudaFreeHost(h_st);
   *this = PprBuffers();
@@ -40,6 +40,20 @@ static int ensure_ppr(nwgpu_graph* g, int K) {
   CK(dalloc(g, &b.col_iters, (uint64_t)K), "cudaMalloc(col iters)");
   CK(dalloc(g, &b.col_err, (uint64_t)K), "cudaMalloc(col err)");
   CK(dalloc(g, &b.st, 1), "cudaMalloc(ppr state)");
+  // rows crossing warp tiles, once per graph (counted in the state's ticket word, reset below)
+  CK(dalloc(g, &b.spans, T + 1), "cudaMalloc(ppr spans)");
+  {
+    unsigned int* cnt = &b.st->ticket;
+    CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned int), g->stream), "ppr spans");
+    CK(launch_ppr_spans(g->g.row_ptr, b.tiling.tile_row, b.tiling.tile_nnz, b.tiling.num_tiles, (uint32_t)kPprTileItems,
+                        b.spans, cnt, g->sms, g->stream),
+       "ppr spans");
+    unsigned int h_cnt = 0;
+    CK(cudaMemcpyAsync(&h_cnt, cnt, sizeof(h_cnt), cudaMemcpyDeviceToHost, g->stream), "ppr spans");
+    CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned int), g->stream), "ppr spans");
+    CK(cudaStreamSynchronize(g->stream), "ppr spans");
+    b.num_spans = h_cnt;
+  }
   CK(cudaHostAlloc((void**)&b.h_st, sizeof(PprState), cudaHostAllocDefault), "cudaHostAlloc(ppr state)");
   CK(cudaStreamSynchronize(g->stream), "ppr buffers");
   b.K = K;
@@ -64,6 +78,9 @@ static PprArgs make_ppr_args(nwgpu_graph* g, float damping) {
   a.res_part = b.res_part;
   a.epi_grid = (uint32_t)b.finish_grid;
   a.n = g->n;
+  a.K = (uint32_t)b.K;
+  a.spans = b.spans;
+  a.num_spans = b.num_spans;
 
   a.seeds = b.seeds;
   a.col_done = b.col_done;

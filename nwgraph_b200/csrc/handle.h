@@ -75,6 +75,8 @@ struct PprBuffers {
   float*          cpart = nullptr;
   float*          epart = nullptr;
   double*         res_part = nullptr;
+  uint4*          spans = nullptr;  // rows crossing warp tiles
+  uint32_t        num_spans = 0;
   uint32_t*       seeds = nullptr;
   uint32_t*       seeds_in = nullptr;
   uint32_t*       col_done = nullptr;

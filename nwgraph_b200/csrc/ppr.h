@@ -35,6 +35,9 @@ struct PprArgs {
   double*         res_part;  // epi_grid x K: the epilogue's per-CTA column residuals
   uint32_t        epi_grid;
   uint64_t        n;
+  uint32_t        K;          // padded column count
+  const uint4*    spans;      // rows crossing warp tiles: (row, first tile, last tile)
+  uint32_t        num_spans;
   const uint32_t* seeds;     // K internal seed ids (0xffffffff: padding column)
   uint32_t*       col_done;  // K flags
   uint32_t*       col_conv;  // K flags
@@ -49,6 +52,9 @@ struct PprArgs {
 };
 
 int         ppr_padded_k(uint32_t k);
+// Rows crossing warp tiles (spans[count] = (row, first tile, last tile), any order).
+cudaError_t launch_ppr_spans(const uint32_t* row_ptr, const uint32_t* tile_row, const uint32_t* tile_nnz, uint32_t T,
+                             uint32_t D, uint4* spans, unsigned int* count, int sms, cudaStream_t s);
 int         ppr_sweep_grid(int K, int sms);
 cudaError_t launch_ppr_seeds(const uint32_t* seeds_in, uint32_t k, int K, const uint32_t* perm, const PprArgs& a,
                              cudaStream_t s);

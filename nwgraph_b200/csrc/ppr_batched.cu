@@ -149,8 +149,21 @@ __global__ void __launch_bounds__(256) ppr_gather_kernel(const PprArgs a) {
   }
 }
 
-// Rows that cross warp tiles: one warp per tile boundary ta whose carried-out
-// row S starts in ta; z(S) = sum of its tile partials in tile order.
+// Rows that cross warp tiles are fixed by the tiling: listed once per graph
+// as (row, first tile, last tile). One warp per listed row sums its tile
+// partials in tile order into z.
+__global__ void ppr_spans_kernel(const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ tile_row,
+                                 const uint32_t* __restrict__ tile_nnz, uint32_t T, uint32_t D, uint4* __restrict__ spans,
+                                 unsigned int* __restrict__ count) {
+  for (uint32_t ta = blockIdx.x * blockDim.x + threadIdx.x; ta + 1 < T; ta += gridDim.x * blockDim.x) {
+    const uint32_t S = tile_row[ta + 1];
+    const uint32_t k1 = tile_nnz[ta + 1], rs = row_ptr[S];
+    if (!(k1 > rs && ((uint64_t)S + rs) / D == ta)) continue;  // the carried-out row does not start in ta
+    const uint32_t tb = (uint32_t)(((uint64_t)S + row_ptr[S + 1]) / D);
+    spans[atomicAdd(count, 1u)] = make_uint4(S, ta, tb, 0u);
+  }
+}
+
 template <int K>
 __global__ void __launch_bounds__(256) ppr_fixup_kernel(const PprArgs a) {
   constexpr int P = Cols<K>::PER_LANE;
@@ -158,22 +171,34 @@ __global__ void __launch_bounds__(256) ppr_fixup_kernel(const PprArgs a) {
   if (*(volatile unsigned int*)&st->done) return;
   const unsigned long long it = *(volatile unsigned long long*)&st->iter;
   float* __restrict__ cout = (it & 1ull) ? a.contrib0 : a.contrib1;
-  const uint32_t D = a.tile_items, T = a.num_tiles;
   const int      lane = threadIdx.x & 31;
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t ta = gwarp; ta + 1 < T; ta += nwarps) {
-    const uint32_t S = a.tile_row[ta + 1];
-    const uint32_t k1 = a.tile_nnz[ta + 1], rs = a.row_ptr[S];
-    if (!(k1 > rs && ((uint64_t)S + rs) / D == ta)) continue;
-    const uint32_t tb = (uint32_t)(((uint64_t)S + a.row_ptr[S + 1]) / D);
-    float          z[P];
+  for (uint32_t sp = gwarp; sp < a.num_spans; sp += nwarps) {
+    const uint4 span = a.spans[sp];
+    // 8 interleaved partial sums (tile u goes to sum (u - first) % 8), combined in order
+    float z[8][P];
 #pragma unroll
-    for (int q = 0; q < P; ++q) z[q] = 0.f;
-    for (uint32_t u = ta; u < tb; ++u)
+    for (int j = 0; j < 8; ++j)
 #pragma unroll
-      for (int q = 0; q < P; ++q) z[q] += __ldcg(a.cpart + (uint64_t)u * K + lane * P + q);
+      for (int q = 0; q < P; ++q) z[j][q] = 0.f;
+    uint32_t u = span.y;
+    for (; u + 8 <= span.z; u += 8)
 #pragma unroll
-    for (int q = 0; q < P; ++q) cout[(uint64_t)S * K + lane * P + q] = z[q] + __ldcg(a.epart + (uint64_t)tb * K + lane * P + q);
+      for (int j = 0; j < 8; ++j)
+#pragma unroll
+        for (int q = 0; q < P; ++q) z[j][q] += __ldcg(a.cpart + (uint64_t)(u + j) * K + lane * P + q);
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      if (u + j < span.z)
+#pragma unroll
+        for (int q = 0; q < P; ++q) z[j][q] += __ldcg(a.cpart + (uint64_t)(u + j) * K + lane * P + q);
+#pragma unroll
+    for (int q = 0; q < P; ++q) {
+      float t = 0.f;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) t += z[j][q];
+      cout[(uint64_t)span.x * K + lane * P + q] = t + __ldcg(a.epart + (uint64_t)span.z * K + lane * P + q);
+    }
   }
 }
 
@@ -234,20 +259,17 @@ __global__ void __launch_bounds__(256) ppr_epilogue_kernel(const PprArgs a, uint
   }
 }
 
-// Per-column residuals over the epilogue's CTAs (one warp per column,
-// lane-strided, fixed tree) and the per-column convergence test.
+// Per-column residuals over the epilogue's CTAs and the per-column
+// convergence test: one warp per column (K / 8 CTAs), lane-strided over the
+// partials with a fixed tree; the last CTA to arrive updates the solve state.
 template <int K>
 __global__ void __launch_bounds__(256) ppr_finish_kernel(const PprArgs a) {
-  constexpr int NWARP = 256 / 32;
-  __shared__ int s_all_done;
+  __shared__ int s_last;
   PprState*      st = a.st;
   if (*(volatile unsigned int*)&st->done) return;
   const unsigned long long it = *(volatile unsigned long long*)&st->iter;
-  const int      lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (threadIdx.x == 0) s_all_done = 1;
-  __syncthreads();
-  for (int c = warp; c < K; c += NWARP) {
-    if (a.col_done[c]) continue;  // uniform across the warp
+  const int      lane = threadIdx.x & 31, c = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (c < K && !a.col_done[c]) {  // uniform across the warp
     double e = 0.0;
     for (uint32_t u = lane; u < a.epi_grid; u += 32) e += __ldcg(a.res_part + (uint64_t)u * K + c);
     e = warp_sum_lane0(e);
@@ -257,22 +279,28 @@ __global__ void __launch_bounds__(256) ppr_finish_kernel(const PprArgs a) {
       if (e < st->threshold) {
         a.col_done[c] = 1u;
         a.col_conv[c] = 1u;
-      } else {
-        s_all_done = 0;
       }
     }
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    const unsigned long long done_iters = it + 1ull;
-    st->iter = done_iters;
-    const bool abort = a.abort_word && *a.abort_word;
-    const bool done = s_all_done || done_iters >= st->max_iters || abort;
-    st->aborted = (abort && !s_all_done) ? 1u : 0u;
-    st->done = done ? 1u : 0u;
     __threadfence();
-    if (a.use_cond && !done && done_iters < st->chunk_end) cudaGraphSetConditional(a.cond, 1u);
+    s_last = (atomicAdd(&st->ticket, 1u) == gridDim.x - 1u);
   }
+  __syncthreads();
+  if (!s_last || threadIdx.x != 0) return;
+  __threadfence();
+  bool all_done = true;
+  for (int q = 0; q < K; ++q) all_done = all_done && *(volatile uint32_t*)&a.col_done[q] != 0u;
+  const unsigned long long done_iters = it + 1ull;
+  st->iter = done_iters;
+  const bool abort = a.abort_word && *a.abort_word;
+  const bool done = all_done || done_iters >= st->max_iters || abort;
+  st->aborted = (abort && !all_done) ? 1u : 0u;
+  st->done = done ? 1u : 0u;
+  st->ticket = 0u;
+  __threadfence();
+  if (a.use_cond && !done && done_iters < st->chunk_end) cudaGraphSetConditional(a.cond, 1u);
 }
 
 // rank(i, c) = [i == seed_c], contrib = rank / deg.
@@ -321,6 +349,13 @@ __global__ void ppr_seed_kernel(const uint32_t* __restrict__ seeds_in, uint32_t 
   a.col_err[c] = 0.0;
 }
 
+cudaError_t launch_ppr_spans(const uint32_t* row_ptr, const uint32_t* tile_row, const uint32_t* tile_nnz, uint32_t T,
+                             uint32_t D, uint4* spans, unsigned int* count, int sms, cudaStream_t s) {
+  if (T < 2) return cudaSuccess;
+  ppr_spans_kernel<<<sms * 4, 256, 0, s>>>(row_ptr, tile_row, tile_nnz, T, D, spans, count);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_ppr_seeds(const uint32_t* seeds_in, uint32_t k, int K, const uint32_t* perm, const PprArgs& a,
                              cudaStream_t s) {
   ppr_seed_kernel<<<1, 128, 0, s>>>(seeds_in, k, K, perm, a);
@@ -353,12 +388,13 @@ static void* ppr_fn(int K, int which) {
 }
 
 // Grid of each kernel: gather persistent at its occupancy, fix-up one warp
-// per tile boundary, epilogue epi_grid CTAs, finish one CTA.
+// per row crossing tiles, epilogue epi_grid CTAs, finish one warp per column.
+static int K_of(const PprArgs& a) { return (int)a.K; }
 static dim3 ppr_grid(const PprArgs& a, int which, int sweep_grid) {
   if (which == 0) return dim3((unsigned)sweep_grid);
-  if (which == 1) return dim3((a.num_tiles + 7u) / 8u ? (a.num_tiles + 7u) / 8u : 1u);
+  if (which == 1) return dim3(a.num_spans ? (a.num_spans + 7u) / 8u : 1u);
   if (which == 2) return dim3(a.epi_grid);
-  return dim3(1);
+  return dim3((unsigned)(K_of(a) / 8));
 }
 
 int ppr_padded_k(uint32_t k) { return k <= 32 ? 32 : (k <= 64 ? 64 : (k <= 128 ? 128 : 0)); }
