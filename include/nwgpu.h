@@ -219,6 +219,46 @@ int nwgpu_pr_vjp(nwgpu_graph* g, const float* ranks, const float* dL_dr, float* 
  * returns NWGPU_ERR_ABORTED. Safe to call from another host thread. */
 int nwgpu_abort(nwgpu_graph* g);
 
+/* ---- Ragged batches: many independent graphs in one solve ----------------
+ * No counterpart in the reference: each graph's result is what page_rank
+ * (page_rank.hpp:92-147) gives for that graph alone, and each graph stops at
+ * its own first sweep whose FP64 L1 change is < threshold (or max_iters);
+ * graphs that stopped are skipped by later sweeps.
+ *
+ * Graph g (0 <= g < num_graphs) has n_g = vertex_offsets[g+1] -
+ * vertex_offsets[g] vertices and nnz_g = entry_offsets[g+1] - entry_offsets[g]
+ * entries, as a CSR with local ids: its n_g + 1 row pointers (local entry
+ * offsets, first 0, last nnz_g) are row_ptr[vertex_offsets[g] + g ...], its
+ * column ids (local vertex ids < n_g) are col[entry_offsets[g] ...]. So
+ * row_ptr holds vertex_offsets[num_graphs] + num_graphs words and col
+ * entry_offsets[num_graphs]. vertex_offsets / entry_offsets are host arrays
+ * of num_graphs + 1 non-decreasing values starting at 0; row_ptr / col are
+ * host pointers unless flags has NWGPU_GRAPH_DEVICE_PTRS. Per graph n_g and
+ * nnz_g must be below 2^32 - 16; the batch totals are 64-bit. */
+typedef struct nwgpu_batch nwgpu_batch;
+int nwgpu_batch_create(uint64_t num_graphs, const uint64_t* vertex_offsets, const uint64_t* entry_offsets,
+                       const uint32_t* row_ptr, const uint32_t* col, uint32_t flags, nwgpu_batch** out);
+int nwgpu_batch_destroy(nwgpu_batch* b);
+
+typedef struct nwgpu_batch_stats {
+  uint64_t  sweeps;           /* batch sweeps run (the last graph to stop) */
+  uint64_t  converged_graphs; /* graphs whose last L1 change was < threshold */
+  double    device_ms;        /* CUDA-event time of the sweep loop */
+  double    entries_swept;    /* sum over graphs of nnz_g x the graph's sweeps */
+  double    gteps;            /* entries_swept / device time */
+  uint32_t* graph_iterations; /* optional, caller-owned [num_graphs]: sweeps until graph g stopped */
+  double*   graph_errors;     /* optional [num_graphs]: L1 change of graph g's last sweep */
+  int32_t*  graph_converged;  /* optional [num_graphs] */
+} nwgpu_batch_stats;
+
+/* PageRank of every graph of the batch. out_degree and ranks hold
+ * vertex_offsets[num_graphs] values, graph g's at vertex_offsets[g] (local
+ * vertex order); host pointers unless options->device_ptrs. damping,
+ * threshold and max_iters apply to every graph, with nwgpu_pr_run's meaning
+ * and update. A graph with no vertices has error 0 at every sweep. */
+int nwgpu_pr_ragged(nwgpu_batch* b, const uint32_t* out_degree, float* ranks, float damping, float threshold,
+                    uint64_t max_iters, const nwgpu_pr_options* options, nwgpu_batch_stats* stats);
+
 /* Return the device memory that destroyed handles left in the pool to the
  * driver (all devices). Handles still alive keep theirs. */
 int nwgpu_release_cached_memory(void);

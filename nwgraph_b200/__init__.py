@@ -9,6 +9,6 @@ The CUDA library (``libnwgpu.so``, C ABI in ``include/nwgpu.h``) is loaded on
 first use; there is no CPU fallback.
 """
 from ._native import NwgpuError
-from .pagerank import Graph, PageRankStats, PprBatchStats, page_rank
+from .pagerank import Graph, GraphBatch, PageRankStats, PprBatchStats, RaggedStats, page_rank
 
-__all__ = ["Graph", "PageRankStats", "PprBatchStats", "NwgpuError", "page_rank"]
+__all__ = ["Graph", "GraphBatch", "PageRankStats", "PprBatchStats", "RaggedStats", "NwgpuError", "page_rank"]

@@ -68,6 +68,13 @@ class PprStats(C.Structure):
                 ("col_converged", C.POINTER(C.c_int32))]
 
 
+class BatchStats(C.Structure):
+    _fields_ = [("sweeps", C.c_uint64), ("converged_graphs", C.c_uint64), ("device_ms", C.c_double),
+                ("entries_swept", C.c_double), ("gteps", C.c_double),
+                ("graph_iterations", C.POINTER(C.c_uint32)), ("graph_errors", C.POINTER(C.c_double)),
+                ("graph_converged", C.POINTER(C.c_int32))]
+
+
 # Every symbol include/nwgpu.h declares, with its C signature.
 _vp = C.c_void_p
 SIGNATURES = {
@@ -90,6 +97,10 @@ SIGNATURES = {
                                 C.POINTER(PrStats)]),
     "nwgpu_pr_vjp": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_float, C.c_float, C.c_uint64, C.POINTER(PrOptions),
                                C.POINTER(PrStats)]),
+    "nwgpu_batch_create": (C.c_int, [C.c_uint64, _vp, _vp, _vp, _vp, C.c_uint32, C.POINTER(_vp)]),
+    "nwgpu_batch_destroy": (C.c_int, [_vp]),
+    "nwgpu_pr_ragged": (C.c_int, [_vp, _vp, _vp, C.c_float, C.c_float, C.c_uint64, C.POINTER(PrOptions),
+                                  C.POINTER(BatchStats)]),
 }
 
 _lib = None

@@ -1,0 +1,361 @@
+// C ABI: ragged batches of independent graphs (nwgpu_batch_create,
+// nwgpu_pr_ragged, nwgpu_batch_destroy; include/nwgpu.h).
+//
+// No counterpart in the reference, whose page_rank (page_rank.hpp:92-147)
+// takes one graph: each graph of a batch gets exactly that solve (Jacobi,
+// leak semantics, init 1/n_g, base (1-d)/n_g, FP64 L1 stopping test), but all
+// graphs advance together in one sweep loop. Each graph keeps its local CSR;
+// 64-bit per-graph bases locate its slices of the batch arrays, so a batch is
+// limited only by device memory, not by 32-bit totals. The merge-path tiles of
+// a graph never cross into the next graph, so every tile's L1 change belongs
+// to one graph and the per-graph errors are sums of tile residuals in tile
+// order. Graphs that stopped keep their ranks; their tiles issue no loads.
+#include <new>
+#include <vector>
+
+#include "handle.h"
+
+namespace nwgpu {
+
+struct RaggedBatch {
+  int          device = 0, sms = 0;
+  cudaStream_t stream = nullptr;
+  uint32_t     num_graphs = 0;
+  uint64_t     nv = 0, nnz = 0, nrp = 0;  // vertices, entries, row pointers of the batch
+  uint32_t     num_tiles = 0;
+  uint64_t     device_bytes = 0;
+  std::vector<RaggedGraph> h_graphs;
+  RaggedGraph* graphs = nullptr;
+  uint32_t *   row_ptr = nullptr, *col = nullptr;
+  uint32_t *   tile_graph = nullptr, *tile_row = nullptr, *tile_nnz = nullptr;
+  float *      rank = nullptr, *contrib[2] = {nullptr, nullptr};
+  uint32_t*    deg = nullptr;
+  float *      cpart = nullptr, *epart = nullptr, *base = nullptr;
+  double *     res_tile = nullptr, *res_part = nullptr, *err_hist = nullptr;
+  uint32_t     err_cap = 4096;
+  RaggedState  rs{};
+  PrState*     st = nullptr;
+  PrState*     h_st = nullptr;
+  unsigned int* h_abort = nullptr;
+  unsigned int* d_abort = nullptr;
+  int          sweep_grid = 1, finish_grid = 1, conv_grid = 1;
+  cudaEvent_t  ev0 = nullptr, ev1 = nullptr;
+  cudaGraph_t  cg = nullptr;
+  cudaGraphExec_t cg_exec = nullptr;
+  float        cg_damping = -1.f;
+
+  template <class T>
+  cudaError_t alloc(T** p, uint64_t count) {
+    const uint64_t bytes = (count + kPad) * sizeof(T);
+    cudaError_t    e = pool_alloc((void**)p, bytes, stream);
+    if (e == cudaSuccess) {
+      device_bytes += bytes;
+      e = cudaMemsetAsync(*p, 0, bytes, stream);
+    }
+    return e;
+  }
+  ~RaggedBatch() {
+    if (stream) cudaStreamSynchronize(stream);
+    if (cg_exec) cudaGraphExecDestroy(cg_exec);
+    if (cg) cudaGraphDestroy(cg);
+    void* ptrs[] = {graphs,   row_ptr,  col,      tile_graph, tile_row, tile_nnz, rank,     contrib[0], contrib[1],
+                    deg,      cpart,    epart,    base,       res_tile, res_part, err_hist, rs.done,    rs.iters,
+                    rs.err,   rs.conv,  st};
+    for (void* p : ptrs) pool_free(p, stream);
+    if (stream) cudaStreamSynchronize(stream);
+    if (h_st) cudaFreeHost(h_st);
+    if (h_abort) cudaFreeHost(h_abort);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+SweepArgs ragged_args(const RaggedBatch* b, float damping) {
+  SweepArgs a = {};
+  a.row_ptr = b->row_ptr;
+  a.col = b->col;
+  a.tile_row = b->tile_row;
+  a.tile_nnz = b->tile_nnz;
+  a.num_tiles = b->num_tiles;
+  a.tile_items = kRaggedTileItems;
+  a.contrib0 = b->contrib[0];
+  a.contrib1 = b->contrib[1];
+  a.rank = b->rank;
+  a.deg = b->deg;
+  a.cpart = b->cpart;
+  a.epart = b->epart;
+  a.res_part = b->res_part;
+  a.sweep_grid = (uint32_t)b->sweep_grid;
+  a.st = b->st;
+  a.err_hist = b->err_hist;
+  a.err_cap = b->err_cap;
+  a.abort_word = b->d_abort;
+  a.damping = damping;
+  a.hot_ids = 0u;
+  a.graphs = b->graphs;
+  a.tile_graph = b->tile_graph;
+  a.graph_base = b->base;
+  a.graph_done = b->rs.done;
+  a.res_tile = b->res_tile;
+  return a;
+}
+
+int build_ragged_graph(RaggedBatch* b, const SweepArgs& proto) {
+  if (b->cg_exec) {
+    cudaGraphExecDestroy(b->cg_exec);
+    b->cg_exec = nullptr;
+  }
+  if (b->cg) {
+    cudaGraphDestroy(b->cg);
+    b->cg = nullptr;
+  }
+  CK(cudaGraphCreate(&b->cg, 0), "cudaGraphCreate");
+  cudaGraphNode_t arm;
+  CK(add_pr_arm_node(b->cg, b->st, &arm), "cudaGraphAddKernelNode(arm)");
+  cudaGraphConditionalHandle cond;
+  CK(cudaGraphConditionalHandleCreate(&cond, b->cg, 1u, cudaGraphCondAssignDefault), "cudaGraphConditionalHandleCreate");
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = cond;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t wnode;
+  CK(cudaGraphAddNode(&wnode, b->cg, &arm, 1, &cp), "cudaGraphAddNode(while)");
+  SweepArgs a = proto;
+  a.cond = cond;
+  a.use_cond = 1;
+  CK(add_ragged_nodes(cp.conditional.phGraph_out[0], a, b->sweep_grid, b->finish_grid, b->num_graphs, b->rs,
+                      b->conv_grid),
+     "cudaGraphAddKernelNode(ragged)");
+  CK(cudaGraphInstantiate(&b->cg_exec, b->cg, 0), "cudaGraphInstantiate");
+  b->cg_damping = proto.damping;
+  return NWGPU_OK;
+}
+
+}  // namespace
+}  // namespace nwgpu
+
+struct nwgpu_batch : nwgpu::RaggedBatch {};
+
+using namespace nwgpu;
+
+extern "C" {
+
+int nwgpu_batch_create(uint64_t num_graphs, const uint64_t* vertex_offsets, const uint64_t* entry_offsets,
+                       const uint32_t* row_ptr, const uint32_t* col, uint32_t flags, nwgpu_batch** out) {
+  clear_error();
+  if (!out) return fail(NWGPU_ERR_INVALID_ARG, "out is NULL");
+  *out = nullptr;
+  if (num_graphs == 0 || num_graphs >= 0x7FFFFFFFull)
+    return fail(NWGPU_ERR_INVALID_ARG, "num_graphs = %llu outside [1, 2^31)", (unsigned long long)num_graphs);
+  if (!vertex_offsets || !entry_offsets) return fail(NWGPU_ERR_INVALID_ARG, "vertex_offsets / entry_offsets is NULL");
+  if (vertex_offsets[0] != 0 || entry_offsets[0] != 0)
+    return fail(NWGPU_ERR_INVALID_ARG, "vertex_offsets[0] and entry_offsets[0] must be 0");
+  // Per-graph slices and tiles, checked on the host (the offsets are host arrays).
+  std::vector<RaggedGraph> hg(num_graphs);
+  uint64_t                 tiles = 0;
+  for (uint64_t g = 0; g < num_graphs; ++g) {
+    if (vertex_offsets[g + 1] < vertex_offsets[g] || entry_offsets[g + 1] < entry_offsets[g])
+      return fail(NWGPU_ERR_INVALID_ARG, "offsets decrease at graph %llu", (unsigned long long)g);
+    const uint64_t n = vertex_offsets[g + 1] - vertex_offsets[g], m = entry_offsets[g + 1] - entry_offsets[g];
+    if (n >= 0xFFFFFFF0ull || m >= 0xFFFFFFF0ull)
+      return fail(NWGPU_ERR_INVALID_ARG, "graph %llu: n = %llu, nnz = %llu do not fit uint32 local ids",
+                  (unsigned long long)g, (unsigned long long)n, (unsigned long long)m);
+    RaggedGraph& R = hg[g];
+    R.v0 = vertex_offsets[g];
+    R.e0 = entry_offsets[g];
+    R.p0 = vertex_offsets[g] + g;
+    R.n = (uint32_t)n;
+    R.nnz = (uint32_t)m;
+    R.tile0 = (uint32_t)tiles;
+    R.tiles = (uint32_t)((n + m + kRaggedTileItems - 1) / kRaggedTileItems);
+    tiles += R.tiles;
+    if (tiles + num_graphs >= 0xFFFFFFF0ull) return fail(NWGPU_ERR_INVALID_ARG, "batch has too many tiles");
+  }
+  const uint64_t nv = vertex_offsets[num_graphs], nnz = entry_offsets[num_graphs], nrp = nv + num_graphs;
+  if (!row_ptr) return fail(NWGPU_ERR_INVALID_ARG, "row_ptr is NULL");
+  if (nnz && !col) return fail(NWGPU_ERR_INVALID_ARG, "col is NULL with entries");
+  int dev, sms;
+  int rc = check_device(&dev, &sms);
+  if (rc) return rc;
+
+  nwgpu_batch* b = new (std::nothrow) nwgpu_batch();
+  if (!b) return fail(NWGPU_ERR_OUT_OF_MEMORY, "host allocation failed");
+  auto bail = [&](int code) {
+    delete b;
+    return code;
+  };
+  b->device = dev;
+  b->sms = sms;
+  b->num_graphs = (uint32_t)num_graphs;
+  b->nv = nv;
+  b->nnz = nnz;
+  b->nrp = nrp;
+  b->num_tiles = (uint32_t)tiles;
+  b->h_graphs = std::move(hg);
+  cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return bail(cuda_fail(e, "cudaStreamCreate"));
+  const cudaMemcpyKind kind = (flags & NWGPU_GRAPH_DEVICE_PTRS) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  const uint64_t       T = tiles, G = num_graphs;
+#define BK(call, what)                                    \
+  do {                                                    \
+    cudaError_t _e = (call);                              \
+    if (_e != cudaSuccess) return bail(cuda_fail(_e, what)); \
+  } while (0)
+  BK(b->alloc(&b->graphs, G), "cudaMalloc(graphs)");
+  BK(b->alloc(&b->row_ptr, nrp), "cudaMalloc(row_ptr)");
+  BK(b->alloc(&b->col, nnz), "cudaMalloc(col)");
+  BK(cudaMemcpyAsync(b->graphs, b->h_graphs.data(), G * sizeof(RaggedGraph), cudaMemcpyHostToDevice, b->stream),
+     "upload graphs");
+  BK(cudaMemcpyAsync(b->row_ptr, row_ptr, nrp * sizeof(uint32_t), kind, b->stream), "upload row_ptr");
+  if (nnz) BK(cudaMemcpyAsync(b->col, col, nnz * sizeof(uint32_t), kind, b->stream), "upload col");
+  // Validate on the device before any kernel indexes with these arrays.
+  unsigned int* d_err = nullptr;
+  unsigned int  h_err = 0;
+  BK(pool_alloc_n(&d_err, 1, b->stream), "cudaMalloc(err)");
+  e = cudaMemsetAsync(d_err, 0, sizeof(unsigned int), b->stream);
+  if (e == cudaSuccess) e = validate_ragged(b->graphs, b->num_graphs, b->row_ptr, b->col, nrp, nnz, d_err, sms, b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h_err, d_err, sizeof(unsigned int), cudaMemcpyDeviceToHost, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  pool_free(d_err, b->stream);
+  if (e != cudaSuccess) return bail(cuda_fail(e, "validate"));
+  if (h_err)
+    return bail(fail(NWGPU_ERR_INVALID_GRAPH, "invalid batch CSR:%s%s%s",
+                     (h_err & 1u) ? " a graph's row pointers do not start at 0 or end at its nnz;" : "",
+                     (h_err & 2u) ? " row pointers decrease;" : "", (h_err & 4u) ? " column id >= the graph's n;" : ""));
+  // Tiles and solve buffers.
+  BK(b->alloc(&b->tile_graph, T), "cudaMalloc(tile_graph)");
+  BK(b->alloc(&b->tile_row, T + G), "cudaMalloc(tile_row)");
+  BK(b->alloc(&b->tile_nnz, T + G), "cudaMalloc(tile_nnz)");
+  BK(fill_ragged_tiling(b->graphs, b->num_graphs, b->row_ptr, b->num_tiles, b->tile_graph, b->tile_row, b->tile_nnz,
+                        sms, b->stream),
+     "ragged tiling");
+  BK(b->alloc(&b->rank, nv), "cudaMalloc(rank)");
+  BK(b->alloc(&b->contrib[0], nv), "cudaMalloc(contrib)");
+  BK(b->alloc(&b->contrib[1], nv), "cudaMalloc(contrib)");
+  BK(b->alloc(&b->deg, nv), "cudaMalloc(deg)");
+  BK(b->alloc(&b->cpart, T + 1), "cudaMalloc(cpart)");
+  BK(b->alloc(&b->epart, T + 1), "cudaMalloc(epart)");
+  BK(b->alloc(&b->res_tile, T + 1), "cudaMalloc(res_tile)");
+  BK(b->alloc(&b->base, G), "cudaMalloc(base)");
+  BK(b->alloc(&b->rs.done, G), "cudaMalloc(graph state)");
+  BK(b->alloc(&b->rs.iters, G), "cudaMalloc(graph state)");
+  BK(b->alloc(&b->rs.err, G), "cudaMalloc(graph state)");
+  BK(b->alloc(&b->rs.conv, G), "cudaMalloc(graph state)");
+  BK(b->alloc(&b->err_hist, b->err_cap), "cudaMalloc(err_hist)");
+  BK(b->alloc(&b->st, 1), "cudaMalloc(state)");
+  // Grids: 4 resident 256-thread CTAs per SM for the sweep; the converge
+  // kernel has one warp per graph up to 16 CTAs per SM.
+  const uint64_t want = (uint64_t)sms * 4;
+  b->sweep_grid = (int)(T == 0 ? 1 : (want < T ? want : T));
+  b->finish_grid = (int)(T == 0 ? 1 : (T + 255) / 256);
+  const uint64_t cg = (G + 7) / 8, cap = (uint64_t)sms * 16;
+  b->conv_grid = (int)(cg < cap ? cg : cap);
+  BK(b->alloc(&b->res_part, (uint64_t)b->conv_grid), "cudaMalloc(res_part)");
+  BK(cudaHostAlloc((void**)&b->h_st, sizeof(PrState), cudaHostAllocDefault), "cudaHostAlloc(state)");
+  BK(cudaHostAlloc((void**)&b->h_abort, sizeof(unsigned int), cudaHostAllocMapped), "cudaHostAlloc(abort)");
+  *b->h_abort = 0;
+  BK(cudaHostGetDevicePointer((void**)&b->d_abort, b->h_abort, 0), "cudaHostGetDevicePointer(abort)");
+  BK(cudaEventCreate(&b->ev0), "cudaEventCreate");
+  BK(cudaEventCreate(&b->ev1), "cudaEventCreate");
+  BK(cudaStreamSynchronize(b->stream), "batch create");
+#undef BK
+  *out = b;
+  return NWGPU_OK;
+}
+
+int nwgpu_batch_destroy(nwgpu_batch* b) {
+  clear_error();
+  delete b;
+  return NWGPU_OK;
+}
+
+int nwgpu_pr_ragged(nwgpu_batch* b, const uint32_t* out_degree, float* ranks, float damping, float threshold,
+                    uint64_t max_iters, const nwgpu_pr_options* options, nwgpu_batch_stats* stats) {
+  clear_error();
+  if (!b) return fail(NWGPU_ERR_INVALID_ARG, "batch is NULL");
+  if (b->nv && (!out_degree || !ranks)) return fail(NWGPU_ERR_INVALID_ARG, "out_degree / ranks is NULL");
+  if (!(damping >= 0.0f && damping <= 1.0f)) return fail(NWGPU_ERR_INVALID_ARG, "damping %g outside [0, 1]", (double)damping);
+  const nwgpu_pr_options opt = read_options(options);
+  if (opt.mode != NWGPU_MODE_PARITY) return fail(NWGPU_ERR_UNSUPPORTED, "mode %u is not supported", opt.mode);
+  if (opt.launch > NWGPU_LAUNCH_STREAM) return fail(NWGPU_ERR_INVALID_ARG, "launch %u unknown", opt.launch);
+  cudaStream_t   s = opt.stream ? (cudaStream_t)opt.stream : b->stream;
+  const uint64_t nv = b->nv, G = b->num_graphs;
+  const bool     dptr = opt.device_ptrs != 0;
+  *(volatile unsigned int*)b->h_abort = 0u;
+  if (nv)
+    CK(cudaMemcpyAsync(b->deg, out_degree, nv * sizeof(uint32_t), dptr ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                       s),
+       "copy out_degree");
+  PrState h = {};
+  h.max_iters = max_iters;
+  h.chunk_end = kGraphChunk;
+  h.threshold = (double)threshold;
+  h.done = (max_iters == 0) ? 1u : 0u;
+  *b->h_st = h;
+  CK(cudaMemcpyAsync(b->st, b->h_st, sizeof(PrState), cudaMemcpyHostToDevice, s), "copy state");
+  const SweepArgs a = ragged_args(b, damping);
+  CK(launch_ragged_init(a, b->rs, b->num_graphs, nv, damping, h.done, b->sms, s), "ragged init");
+  CK(cudaEventRecord(b->ev0, s), "cudaEventRecord");
+  if (opt.launch == NWGPU_LAUNCH_GRAPH) {
+    if (!b->cg_exec || b->cg_damping != damping) {
+      int rc = build_ragged_graph(b, a);
+      if (rc) return rc;
+    }
+    const uint64_t max_launches = max_iters / kGraphChunk + 2;
+    for (uint64_t launches = 0; !b->h_st->done; ++launches) {
+      if (launches == max_launches)
+        return fail(NWGPU_ERR_CUDA, "sweep loop did not finish after %llu graph launches", (unsigned long long)launches);
+      CK(cudaGraphLaunch(b->cg_exec, s), "cudaGraphLaunch");
+      CK(cudaMemcpyAsync(b->h_st, b->st, sizeof(PrState), cudaMemcpyDeviceToHost, s), "copy state");
+      CK(cudaStreamSynchronize(s), "sweep loop");
+    }
+  } else {
+    uint64_t launched = 0;
+    while (!b->h_st->done && launched < max_iters) {
+      const uint64_t batch = (max_iters - launched) < kGraphChunk ? (max_iters - launched) : kGraphChunk;
+      for (uint64_t k = 0; k < batch; ++k)
+        CK(launch_ragged_sweep(a, b->sweep_grid, b->finish_grid, b->num_graphs, b->rs, b->conv_grid, s), "ragged sweep");
+      launched += batch;
+      CK(cudaMemcpyAsync(b->h_st, b->st, sizeof(PrState), cudaMemcpyDeviceToHost, s), "copy state");
+      CK(cudaStreamSynchronize(s), "sweep loop");
+    }
+  }
+  CK(cudaEventRecord(b->ev1, s), "cudaEventRecord");
+  const PrState fin = *b->h_st;
+  if (fin.fault) return fail(NWGPU_ERR_CUDA, "a bounded device wait gave up (fault word %u)", fin.fault);
+  if (nv)
+    CK(cudaMemcpyAsync(ranks, b->rank, nv * sizeof(float), dptr ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s),
+       "copy ranks");
+  std::vector<uint32_t> iters(G);
+  std::vector<uint32_t> conv(G);
+  CK(cudaMemcpyAsync(iters.data(), b->rs.iters, G * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "copy graph state");
+  CK(cudaMemcpyAsync(conv.data(), b->rs.conv, G * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "copy graph state");
+  if (stats && stats->graph_errors)
+    CK(cudaMemcpyAsync(stats->graph_errors, b->rs.err, G * sizeof(double), cudaMemcpyDeviceToHost, s), "copy graph errors");
+  CK(cudaStreamSynchronize(s), "copy ranks");
+  if (stats) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    double   swept = 0.0;
+    uint64_t nconv = 0;
+    for (uint64_t g = 0; g < G; ++g) {
+      swept += (double)b->h_graphs[g].nnz * (double)iters[g];
+      nconv += conv[g] ? 1u : 0u;
+      if (stats->graph_iterations) stats->graph_iterations[g] = iters[g];
+      if (stats->graph_converged) stats->graph_converged[g] = conv[g] ? 1 : 0;
+    }
+    stats->sweeps = fin.iter;
+    stats->converged_graphs = nconv;
+    stats->device_ms = ms;
+    stats->entries_swept = swept;
+    stats->gteps = ms > 0 ? swept / (ms * 1e6) : 0.0;
+  }
+  if (fin.aborted) return fail(NWGPU_ERR_ABORTED, "solve aborted after %llu sweeps", (unsigned long long)fin.iter);
+  return NWGPU_OK;
+}
+
+}  // extern "C"

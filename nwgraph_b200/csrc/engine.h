@@ -25,7 +25,7 @@ struct PrState {
   unsigned int       converged;
   unsigned int       aborted;
   unsigned int       fault;      // nonzero: a bounded device wait gave up (bit pattern = where)
-  unsigned int       pad_;
+  unsigned int       pending;    // ragged batches: graphs still running after the current sweep
 };
 
 struct Tiling {
@@ -54,6 +54,23 @@ struct Transposed {
   uint32_t* fwd = nullptr;      // nnz: the forward entry
   float*    s = nullptr;        // n: out-weight sums, FP64 row sums of w rounded to FP32
   uint32_t* erow = nullptr;     // nnz: row of each forward entry
+};
+
+// One graph of a ragged batch: where its slices of the batch arrays start.
+// Graph g has n local vertices and nnz entries; its row pointers (n + 1,
+// local entry offsets) start at p0 = v0 + g, its column ids (local vertex
+// ids) at e0, its ranks / contributions / degrees at v0, and its merge-path
+// tiles (local diagonals, D items each, the last one partial) are tiles
+// [tile0, tile0 + tiles) of the batch. Tile t's coordinates sit at index
+// t + g of the tile tables, its end at t + g + 1.
+struct RaggedGraph {
+  uint64_t v0;
+  uint64_t e0;
+  uint64_t p0;
+  uint32_t n;
+  uint32_t nnz;
+  uint32_t tile0;
+  uint32_t tiles;
 };
 
 // Teleport term of the update r_i' = base_i + d * z_i.
@@ -98,6 +115,20 @@ struct SweepArgs {
   const float*                 w;          // kModeWeighted / kModeAdjoint: entry weights of the swept CSR
   const float*                 vbase;      // per-row base term (weighted: (1-d) t; adjoint: c)
   const float*                 vaux;       // per-row factor (weighted: out-weight sum; adjoint: d / out-weight sum)
+  // Ragged batches only (the RAGGED sweep variant):
+  const RaggedGraph*           graphs;
+  const uint32_t*              tile_graph;  // graph of each tile
+  const float*                 graph_base;  // per graph: (1 - d) / n
+  const uint32_t*              graph_done;  // per graph: nonzero once it stopped; its tiles are skipped
+  double*                      res_tile;    // per tile: FP64 L1 change of the rows the tile completes
+};
+
+// Per-graph results of a ragged solve, written by the convergence kernel.
+struct RaggedState {
+  uint32_t* done;   // stopped (converged, at max_iters, aborted or failed)
+  uint32_t* iters;  // sweeps run
+  double*   err;    // L1 change of the last sweep
+  uint32_t* conv;   // err < threshold
 };
 
 // devmem.cu: the per-device stream-ordered pool that every handle allocation uses
@@ -177,6 +208,26 @@ cudaError_t add_pr_arm_node(cudaGraph_t g, PrState* st, cudaGraphNode_t* node);
 cudaError_t configure_sweep_kernels();
 cudaError_t set_sweep_carveout(const SweepVariant& v, int percent);
 size_t      sweep_smem_bytes(const SweepVariant& v, uint32_t hot_ids);
+// Ragged batches (pr_plain.cu): the merge-path sweep over per-graph tiles,
+// the rows crossing tiles, then per-graph convergence and the loop condition.
+constexpr uint32_t kRaggedTileItems = 2048;  // D of the ragged sweep (256 threads x 8 items)
+cudaError_t launch_ragged_sweep(const SweepArgs& a, int sweep_grid, int finish_grid, uint32_t num_graphs,
+                                const RaggedState& rs, int conv_grid, cudaStream_t s);
+cudaError_t add_ragged_nodes(cudaGraph_t body, const SweepArgs& a, int sweep_grid, int finish_grid, uint32_t num_graphs,
+                             const RaggedState& rs, int conv_grid);
+// rank = 1/n_g, contrib = rank / deg over the batch's vertices; per-graph base
+// terms and state reset
+cudaError_t launch_ragged_init(const SweepArgs& a, const RaggedState& rs, uint32_t num_graphs, uint64_t num_vertices,
+                               float damping, uint32_t stopped, int sms, cudaStream_t s);
+// graph_build.cu: merge-path coordinates of every graph's tiles (num_tiles +
+// num_graphs entries) and the graph of each tile
+cudaError_t fill_ragged_tiling(const RaggedGraph* graphs, uint32_t num_graphs, const uint32_t* row_ptr,
+                               uint32_t num_tiles, uint32_t* tile_graph, uint32_t* tile_row, uint32_t* tile_nnz,
+                               int sms, cudaStream_t s);
+// Checks every graph's row pointers (first 0, last nnz, non-decreasing) and
+// column ids (< n); sets the bits validate_csr sets.
+cudaError_t validate_ragged(const RaggedGraph* graphs, uint32_t num_graphs, const uint32_t* row_ptr, const uint32_t* col,
+                            uint64_t num_row_ptrs, uint64_t num_entries, unsigned int* err, int sms, cudaStream_t s);
 uint32_t    sweep_hot_capacity(const SweepVariant& v);  // ids that fit in shared memory (hot_smem variants)
 int         sweep_blocks_per_sm(const SweepVariant& v, uint32_t hot_ids);
 int         finish_grid_for(uint32_t num_tiles);

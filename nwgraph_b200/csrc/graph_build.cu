@@ -93,6 +93,83 @@ cudaError_t fill_tiling(const uint32_t* d_row_ptr, uint64_t n, uint64_t nnz, uin
 }
 
 // ---------------------------------------------------------------------------
+// Ragged batches: per-graph tiling and validation
+// ---------------------------------------------------------------------------
+// Last graph g whose key(g) <= x, for a key non-decreasing in g.
+template <class Key>
+__device__ __forceinline__ uint32_t last_graph_at_or_below(uint32_t num_graphs, uint64_t x, Key key) {
+  uint32_t lo = 0, hi = num_graphs - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) >> 1;
+    if (key(mid) <= x)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// Entry e of the tile tables belongs to the graph g with tile0 + g <= e <
+// tile0 + g + tiles + 1 (each graph has its tiles plus one end entry).
+__global__ void ragged_tiling_kernel(const RaggedGraph* __restrict__ graphs, uint32_t num_graphs,
+                                     const uint32_t* __restrict__ row_ptr, uint32_t D, uint64_t entries,
+                                     uint32_t* __restrict__ tile_graph, uint32_t* __restrict__ tile_row,
+                                     uint32_t* __restrict__ tile_nnz) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < entries; e += stride) {
+    const uint32_t g = last_graph_at_or_below(num_graphs, e, [&](uint32_t x) { return (uint64_t)graphs[x].tile0 + x; });
+    const RaggedGraph R = graphs[g];
+    const uint64_t    j = e - ((uint64_t)R.tile0 + g);
+    const uint64_t    items = (uint64_t)R.n + R.nnz;
+    const uint64_t    d = j * D < items ? j * D : items;
+    const uint32_t    i = merge_path_row(row_ptr + R.p0, R.n, R.nnz, d);
+    tile_row[e] = i;
+    tile_nnz[e] = (uint32_t)(d - i);
+    if (j < R.tiles) tile_graph[R.tile0 + j] = g;
+  }
+}
+
+cudaError_t fill_ragged_tiling(const RaggedGraph* graphs, uint32_t num_graphs, const uint32_t* row_ptr,
+                               uint32_t num_tiles, uint32_t* tile_graph, uint32_t* tile_row, uint32_t* tile_nnz,
+                               int sms, cudaStream_t s) {
+  if (!num_graphs) return cudaSuccess;
+  ragged_tiling_kernel<<<sms * 8, 256, 0, s>>>(graphs, num_graphs, row_ptr, kRaggedTileItems,
+                                                (uint64_t)num_tiles + num_graphs, tile_graph, tile_row, tile_nnz);
+  return cudaGetLastError();
+}
+
+// Bits as validate_kernel: 1 a graph's row pointers do not start at 0 or end
+// at its nnz, 2 they decrease, 4 a column id >= the graph's n.
+__global__ void validate_ragged_kernel(const RaggedGraph* __restrict__ graphs, uint32_t num_graphs,
+                                       const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ col,
+                                       uint64_t num_row_ptrs, uint64_t num_entries, unsigned int* err) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned int   bad = 0;
+  for (uint64_t q = tid; q < num_row_ptrs; q += stride) {
+    const uint32_t g = last_graph_at_or_below(num_graphs, q, [&](uint32_t x) { return graphs[x].p0; });
+    const uint64_t i = q - graphs[g].p0;
+    const uint32_t v = row_ptr[q];
+    if (i == 0 && v != 0u) bad |= 1u;
+    if (i == graphs[g].n && v != graphs[g].nnz) bad |= 1u;
+    if (i < graphs[g].n && row_ptr[q + 1] < v) bad |= 2u;
+  }
+  for (uint64_t k = tid; k < num_entries; k += stride) {
+    const uint32_t g = last_graph_at_or_below(num_graphs, k, [&](uint32_t x) { return graphs[x].e0; });
+    if (__ldcs(col + k) >= graphs[g].n) bad |= 4u;
+  }
+  bad = __reduce_or_sync(kFullMask, bad);
+  if ((threadIdx.x & 31) == 0 && bad) atomicOr(err, bad);
+}
+
+cudaError_t validate_ragged(const RaggedGraph* graphs, uint32_t num_graphs, const uint32_t* row_ptr, const uint32_t* col,
+                            uint64_t num_row_ptrs, uint64_t num_entries, unsigned int* err, int sms, cudaStream_t s) {
+  if (!num_graphs) return cudaSuccess;
+  validate_ragged_kernel<<<sms * 8, 256, 0, s>>>(graphs, num_graphs, row_ptr, col, num_row_ptrs, num_entries, err);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // Relabelling
 // ---------------------------------------------------------------------------
 // Sort key: row length (in-degree). For the symmetric graphs of the benchmark

@@ -76,6 +76,9 @@ struct TileMeta {
   uint32_t rp_at;           // stage word holding row_ptr[r0] (row_ptr[r0..r1] follow)
   uint32_t rk_at;           // stage word holding rank[r0], or ~0u when rank/deg are not staged
   uint32_t dg_at;           // stage word holding deg[r0]
+  float    base;            // ragged batches: the tile's graph's base term
+  uint32_t pad_;
+  uint64_t v0;              // ragged batches: the tile's graph's first vertex
 };
 
 template <int NT, int IPT>
@@ -104,6 +107,53 @@ constexpr size_t sweep_smem() {
 __device__ __forceinline__ float base_of(const SweepArgs& a, uint32_t r) {
   if (a.teleport == kTeleportSeed) return (r == a.seed) ? a.base : 0.f;
   return a.base;
+}
+
+// Thread 0, ragged batches: tile t of graph g in local coordinates; the
+// slices start at the graph's 64-bit bases and are rounded out to 16 bytes
+// of the batch arrays. A stopped graph's tiles get an empty meta (no rows, no
+// entries) and arrive with no bytes.
+template <int NT, int IPT>
+__device__ __forceinline__ void issue_ragged_tile(const SweepArgs& a, uint32_t t, uint32_t* stg, TileMeta* m,
+                                                  uint64_t* bar, uint64_t pol) {
+  constexpr int  RV = SweepSmem<NT, IPT>::RV;
+  const uint32_t g = a.tile_graph[t];
+  const RaggedGraph* G = a.graphs + g;
+  m->base = a.graph_base[g];
+  m->v0 = G->v0;
+  if (*(const volatile uint32_t*)(a.graph_done + g)) {
+    m->r0 = m->r1 = 0u;
+    m->k0 = m->k1 = 0u;
+    m->col_at = 0u;
+    m->rp_at = 0u;
+    m->rk_at = ~0u;
+    m->dg_at = 0u;
+    mbar_arrive_expect_tx(bar, 0u);
+    return;
+  }
+  const uint32_t e = t + g;
+  const uint32_t r0 = a.tile_row[e], r1 = a.tile_row[e + 1], k0 = a.tile_nnz[e], k1 = a.tile_nnz[e + 1];
+  const uint64_t K0 = G->e0 + k0, P0 = G->p0 + r0, V0 = G->v0 + r0;
+  const uint64_t ca0 = K0 & ~3ull, ca1 = (G->e0 + k1 + 3ull) & ~3ull;  // col[k0, k1)
+  const uint64_t pa0 = P0 & ~3ull, pa1 = (G->p0 + r1 + 4ull) & ~3ull;  // row_ptr[r0 .. r1]
+  const uint64_t va0 = V0 & ~3ull, va1 = (G->v0 + r1 + 3ull) & ~3ull;  // rank / deg [r0, r1)
+  const bool     stage_rows = (r1 > r0) && (r1 - r0 <= (uint32_t)RV);
+  const uint32_t cw = (uint32_t)(ca1 - ca0), pw = (uint32_t)(pa1 - pa0), vw = stage_rows ? (uint32_t)(va1 - va0) : 0u;
+  m->r0 = r0;
+  m->r1 = r1;
+  m->k0 = k0;
+  m->k1 = k1;
+  m->col_at = (uint32_t)(K0 - ca0);
+  m->rp_at = cw + (uint32_t)(P0 - pa0);
+  m->rk_at = stage_rows ? cw + pw + (uint32_t)(V0 - va0) : ~0u;
+  m->dg_at = cw + pw + vw + (uint32_t)(V0 - va0);
+  mbar_arrive_expect_tx(bar, 4u * (cw + pw + 2u * vw));
+  if (cw) bulk_load(stg, a.col + ca0, 4u * cw, bar, pol);
+  bulk_load(stg + cw, a.row_ptr + pa0, 4u * pw, bar, pol);
+  if (vw) {
+    bulk_load(stg + cw + pw, a.rank + va0, 4u * vw, bar, pol);
+    bulk_load(stg + cw + pw + vw, a.deg + va0, 4u * vw, bar, pol);
+  }
 }
 
 // Thread 0: bring tile t's slices into stage `stg` and record where they landed.
@@ -194,10 +244,14 @@ __device__ __forceinline__ void gather_tile(const uint32_t* stg, const TileMeta&
 // finds the row of its first entry by binary search, and touches shared memory
 // only where a row ends. Rows crossing threads are combined by a block-wide
 // segmented scan of (row, partial) carries.
-template <int NT, int IPT>
+template <int NT, int IPT, bool RAGGED>
 __device__ __forceinline__ double reduce_tile(const SweepArgs& a, SweepSmem<NT, IPT>& S, int s, uint32_t t,
                                               const float (&v)[IPT], float* __restrict__ cout, uint64_t pol_keep) {
   const TileMeta  m = S.meta[s];
+  // ragged batches: the tile's rows are local ids of its graph
+  float* const    rank = RAGGED ? a.rank + m.v0 : a.rank;
+  const uint32_t* degv = RAGGED ? a.deg + m.v0 : a.deg;
+  if (RAGGED) cout += m.v0;
   const int       R = (int)(m.r1 - m.r0), E = (int)(m.k1 - m.k0);
   const uint32_t* rp = S.stage[s] + m.rp_at;  // rp[j] = row_ptr[r0 + j], j = 0..R
   const int       tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -289,8 +343,8 @@ __device__ __forceinline__ double reduce_tile(const SweepArgs& a, SweepSmem<NT, 
     for (int j = (is_cont ? 1 : 0) + tid; j < R; j += NT) {
       const uint32_t r = m.r0 + j;
       const float    z = (rp[j + 1] > rp[j]) ? S.z[j] : 0.f;
-      const float    nr = fmaf(a.damping, z, base_of(a, r));
-      st_stream(a.rank + r, nr);
+      const float    nr = fmaf(a.damping, z, RAGGED ? m.base : base_of(a, r));
+      st_stream(rank + r, nr);
       st_keep(cout + r, nr / (float)dg[j], pol_keep);
       res += (double)fabsf(nr - rk[j]);
     }
@@ -298,10 +352,10 @@ __device__ __forceinline__ double reduce_tile(const SweepArgs& a, SweepSmem<NT, 
     for (int j = (is_cont ? 1 : 0) + tid; j < R; j += NT) {
       const uint32_t r = m.r0 + j;
       const float    z = (rp[j + 1] > rp[j]) ? S.z[j] : 0.f;
-      const float    nr = fmaf(a.damping, z, base_of(a, r));
-      const float    old = ld_stream(a.rank + r);
-      const uint32_t dg = ld_stream(a.deg + r);
-      st_stream(a.rank + r, nr);
+      const float    nr = fmaf(a.damping, z, RAGGED ? m.base : base_of(a, r));
+      const float    old = ld_stream(rank + r);
+      const uint32_t dg = ld_stream(degv + r);
+      st_stream(rank + r, nr);
       st_keep(cout + r, nr / (float)dg, pol_keep);
       res += (double)fabsf(nr - old);
     }
@@ -311,7 +365,38 @@ __device__ __forceinline__ double reduce_tile(const SweepArgs& a, SweepSmem<NT, 
   return res;
 }
 
-template <int NT, int IPT, bool HOT>
+template <int NT, int IPT, bool RAGGED>
+__device__ __forceinline__ void issue_any(const SweepArgs& a, uint32_t t, uint32_t* stg, TileMeta* m, uint64_t* bar,
+                                          uint64_t pol) {
+  if constexpr (RAGGED)
+    issue_ragged_tile<NT, IPT>(a, t, stg, m, bar, pol);
+  else
+    issue_tile<NT, IPT>(a, t, stg, m, bar, pol);
+}
+
+// Ragged batches: the FP64 L1 change of the rows tile t completes goes to
+// res_tile[t] (warp sums in shared memory, added in warp order by thread 0
+// after the barrier that follows). Every tile belongs to one graph, so the
+// per-graph sums need no atomics.
+template <int NT, int IPT, bool RAGGED>
+__device__ __forceinline__ double tile_residual(SweepSmem<NT, IPT>& S, double r) {
+  if constexpr (RAGGED) {
+    r = warp_sum_lane0(r);
+    if ((threadIdx.x & 31) == 0) S.red[threadIdx.x >> 5] = r;
+    return 0.0;
+  } else {
+    return r;
+  }
+}
+template <int NT, int IPT>
+__device__ __forceinline__ void store_tile_residual(const SweepArgs& a, const SweepSmem<NT, IPT>& S, uint32_t t) {
+  double b = 0.0;
+#pragma unroll
+  for (int w = 0; w < SweepSmem<NT, IPT>::NW; ++w) b += S.red[w];
+  a.res_tile[t] = b;
+}
+
+template <int NT, int IPT, bool HOT, bool RAGGED = false>
 __global__ void __launch_bounds__(NT, HOT ? 1 : 4) pr_sweep_kernel(const SweepArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   auto&          S = *reinterpret_cast<SweepSmem<NT, IPT>*>(smem_raw);
@@ -356,12 +441,14 @@ __global__ void __launch_bounds__(NT, HOT ? 1 : 4) pr_sweep_kernel(const SweepAr
   }
   if (t < T) {
     if (tid == 0) {
-      issue_tile<NT, IPT>(a, t, S.stage[0], &S.meta[0], &S.bar[0], pol_stream);
-      if (t + G < T) issue_tile<NT, IPT>(a, t + G, S.stage[1], &S.meta[1], &S.bar[1], pol_stream);
+      issue_any<NT, IPT, RAGGED>(a, t, S.stage[0], &S.meta[0], &S.bar[0], pol_stream);
+      if (t + G < T) issue_any<NT, IPT, RAGGED>(a, t + G, S.stage[1], &S.meta[1], &S.bar[1], pol_stream);
     }
     float v0[IPT], v1[IPT];
     ok = mbar_wait(&S.bar[0], 0u);
-    if (ok) gather_tile<NT, IPT, HOT>(S.stage[0], S.meta[0], cin, v0, pol_keep, a.hot_ids, hot_smem);
+    if (ok)
+      gather_tile<NT, IPT, HOT>(S.stage[0], S.meta[0], RAGGED ? cin + S.meta[0].v0 : cin, v0, pol_keep, a.hot_ids,
+                                hot_smem);
     ok = __syncthreads_and(ok);
     // two tiles per trip so the register sets alternate without copies
     for (int i = 0; ok && t < T; i += 2) {
@@ -369,28 +456,38 @@ __global__ void __launch_bounds__(NT, HOT ? 1 : 4) pr_sweep_kernel(const SweepAr
       uint32_t tn = t + G;
       if (tn < T) {
         ok = mbar_wait(&S.bar[1], (uint32_t)(i >> 1) & 1u);
-        if (ok) gather_tile<NT, IPT, HOT>(S.stage[1], S.meta[1], cin, v1, pol_keep, a.hot_ids, hot_smem);
+        if (ok)
+          gather_tile<NT, IPT, HOT>(S.stage[1], S.meta[1], RAGGED ? cin + S.meta[1].v0 : cin, v1, pol_keep, a.hot_ids,
+                                    hot_smem);
       }
-      res += reduce_tile<NT, IPT>(a, S, 0, t, v0, cout, pol_keep);
+      res += tile_residual<NT, IPT, RAGGED>(S, reduce_tile<NT, IPT, RAGGED>(a, S, 0, t, v0, cout, pol_keep));
       ok = __syncthreads_and(ok);
+      if (RAGGED && tid == 0) store_tile_residual<NT, IPT>(a, S, t);
       if (ok && tid == 0 && t + 2 * G < T)
-        issue_tile<NT, IPT>(a, t + 2 * G, S.stage[0], &S.meta[0], &S.bar[0], pol_stream);
+        issue_any<NT, IPT, RAGGED>(a, t + 2 * G, S.stage[0], &S.meta[0], &S.bar[0], pol_stream);
       t = tn;
       if (!ok || t >= T) break;
       // odd tile t in stage 1 (values v1); prefetch tile t+G into v0
       tn = t + G;
       if (tn < T) {
         ok = mbar_wait(&S.bar[0], (uint32_t)((i >> 1) + 1) & 1u);
-        if (ok) gather_tile<NT, IPT, HOT>(S.stage[0], S.meta[0], cin, v0, pol_keep, a.hot_ids, hot_smem);
+        if (ok)
+          gather_tile<NT, IPT, HOT>(S.stage[0], S.meta[0], RAGGED ? cin + S.meta[0].v0 : cin, v0, pol_keep, a.hot_ids,
+                                    hot_smem);
       }
-      res += reduce_tile<NT, IPT>(a, S, 1, t, v1, cout, pol_keep);
+      res += tile_residual<NT, IPT, RAGGED>(S, reduce_tile<NT, IPT, RAGGED>(a, S, 1, t, v1, cout, pol_keep));
       ok = __syncthreads_and(ok);
+      if (RAGGED && tid == 0) store_tile_residual<NT, IPT>(a, S, t);
       if (ok && tid == 0 && t + 2 * G < T)
-        issue_tile<NT, IPT>(a, t + 2 * G, S.stage[1], &S.meta[1], &S.bar[1], pol_stream);
+        issue_any<NT, IPT, RAGGED>(a, t + 2 * G, S.stage[1], &S.meta[1], &S.bar[1], pol_stream);
       t = tn;
     }
   }
 
+  if constexpr (RAGGED) {  // residuals went to res_tile; thread 0 may still be reading S.red
+    if (tid == 0 && !ok) atomicOr(&st->fault, 1u);
+    return;
+  }
   // FP64 residual: fixed-order block reduction, one partial per CTA.
   res = warp_sum_lane0(res);
   if ((tid & 31) == 0) S.red[tid >> 5] = res;
@@ -493,6 +590,174 @@ __global__ void __launch_bounds__(256) pr_finish_kernel(const SweepArgs a) {
     st->ticket = 0u;
     __threadfence();
     if (a.use_cond && !done && done_iters < st->chunk_end) cudaGraphSetConditional(a.cond, 1u);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Ragged batches: rows crossing tiles, per-graph convergence, set-up
+// ---------------------------------------------------------------------------
+// Thread ta completes the row carried out of tile ta when that row starts
+// there (local merge-path coordinates of the tile's graph; rows never cross
+// graphs) and adds its L1 change to res_tile[ta]. Spans of more than 8 tiles
+// are summed by the whole warp.
+__global__ void __launch_bounds__(256) pr_ragged_finish_kernel(const SweepArgs a) {
+  if (*(volatile unsigned int*)&a.st->done) return;
+  const unsigned long long it = *(volatile unsigned long long*)&a.st->iter;
+  float* __restrict__ cout = (it & 1ull) ? a.contrib0 : a.contrib1;
+  const uint64_t pol = policy_evict_last();
+  const uint32_t D = a.tile_items, T = a.num_tiles;
+  const int      lane = threadIdx.x & 31;
+  const uint32_t ta = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t       S = 0, tb = 0, g = 0;
+  bool           mine = false;
+  if (ta < T) {
+    g = a.tile_graph[ta];
+    if (!*(const volatile uint32_t*)(a.graph_done + g)) {
+      const RaggedGraph& G = a.graphs[g];
+      const uint32_t*    rp = a.row_ptr + G.p0;
+      S = a.tile_row[ta + g + 1];  // the tile's end; S = n at the graph's last tile
+      const uint32_t k1 = a.tile_nnz[ta + g + 1], rs = rp[S];
+      if (k1 > rs && ((uint64_t)S + rs) / D == ta - G.tile0) {
+        mine = true;
+        tb = G.tile0 + (uint32_t)(((uint64_t)S + rp[S + 1]) / D);
+      }
+    }
+  }
+  const bool longspan = mine && (tb - ta > 8u);
+  float      z = 0.f;
+  if (mine && !longspan) {
+    for (uint32_t u = ta; u < tb; ++u) z += __ldcg(a.cpart + u);
+    z += __ldcg(a.epart + tb);
+  }
+  unsigned mask = __ballot_sync(kFullMask, longspan);
+  while (mask) {
+    const int src = __ffs(mask) - 1;
+    mask &= mask - 1;
+    const uint32_t sa = __shfl_sync(kFullMask, ta, src);
+    const uint32_t sb = __shfl_sync(kFullMask, tb, src);
+    float          p = 0.f;
+    for (uint32_t u = sa + lane; u < sb; u += 32) p += __ldcg(a.cpart + u);
+    p = __shfl_sync(kFullMask, warp_sum_lane0(p), 0);
+    if (lane == src) z = p + __ldcg(a.epart + sb);
+  }
+  if (mine) {
+    const uint64_t v = a.graphs[g].v0 + S;
+    const float    nr = fmaf(a.damping, z, a.graph_base[g]);
+    const float    old = a.rank[v];
+    a.rank[v] = nr;
+    st_keep(cout + v, nr / (float)a.deg[v], pol);
+    a.res_tile[ta] += (double)fabsf(nr - old);
+  }
+}
+
+// One warp per running graph: its sweep error is the sum of its tiles'
+// residuals in tile order (lane-strided FP64 partials, then a fixed shuffle
+// tree); the graph stops on err < threshold, at max_iters, or when the solve
+// is aborted or failed. The last CTA advances the sweep count, records the
+// summed error of the sweep and ends the loop once no graph is running.
+__global__ void __launch_bounds__(256) pr_ragged_converge_kernel(const SweepArgs a, uint32_t num_graphs,
+                                                                 RaggedState rs) {
+  __shared__ double   s_err[8];
+  __shared__ uint32_t s_run[8];
+  __shared__ int      s_last;
+  PrState*            st = a.st;
+  if (*(volatile unsigned int*)&st->done) return;
+  const unsigned long long it = *(volatile unsigned long long*)&st->iter;
+  const int                tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const bool               abort = a.abort_word && *a.abort_word;
+  const bool               fault = *(volatile unsigned int*)&st->fault != 0u;
+  const bool               last_sweep = it + 1ull >= st->max_iters;
+  const double             thr = st->threshold;
+  double                   esum = 0.0;
+  uint32_t                 running = 0;
+  const uint32_t           nwarps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t g = blockIdx.x * (blockDim.x >> 5) + warp; g < num_graphs; g += nwarps) {
+    if (rs.done[g]) continue;
+    const uint32_t t0 = a.graphs[g].tile0, nt = a.graphs[g].tiles;
+    double         e = 0.0;
+    for (uint32_t u = lane; u < nt; u += 32) e += __ldcg(a.res_tile + t0 + u);
+    e = warp_sum_lane0(e);
+    if (lane == 0) {
+      const bool conv = e < thr;
+      const bool more = !conv && !last_sweep;  // the graph would take another sweep
+      rs.iters[g] = (uint32_t)(it + 1ull);
+      rs.err[g] = e;
+      rs.conv[g] = conv ? 1u : 0u;
+      rs.done[g] = (more && !abort && !fault) ? 0u : 1u;
+      esum += e;
+      running += more ? 1u : 0u;
+    }
+  }
+  if (lane == 0) {
+    s_err[warp] = esum;
+    s_run[warp] = running;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double   b = 0.0;
+    uint32_t r = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      b += s_err[w];
+      r += s_run[w];
+    }
+    a.res_part[blockIdx.x] = b;
+    if (r) atomicAdd(&st->pending, r);
+    __threadfence();
+    const unsigned prev = atomicAdd(&st->ticket, 1u);
+    s_last = (prev == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last || tid >= 32) return;
+  __threadfence();
+  double e = 0.0;
+  for (uint32_t u = lane; u < gridDim.x; u += 32) e += __ldcg(a.res_part + u);
+  e = warp_sum_lane0(e);
+  if (lane == 0) {
+    const unsigned long long done_iters = it + 1ull;
+    const unsigned int       pending = *(volatile unsigned int*)&st->pending;
+    st->iter = done_iters;
+    st->last_error = e;
+    if (a.err_hist) a.err_hist[it % a.err_cap] = e;
+    const bool done = pending == 0u || done_iters >= st->max_iters || abort || fault;
+    st->converged = 0u;
+    st->aborted = (abort && pending) ? 1u : 0u;  // graphs were still running
+    st->done = done ? 1u : 0u;
+    st->pending = 0u;
+    st->ticket = 0u;
+    __threadfence();
+    if (a.use_cond && !done && done_iters < st->chunk_end) cudaGraphSetConditional(a.cond, 1u);
+  }
+}
+
+// rank_v = 1/n_g (page_rank.hpp:100-104 per graph), contrib_v = rank_v / deg_v;
+// thread v finds its graph by binary search over the graphs' first vertices.
+// One warp per graph (grid-strided) sets the base term (1 - d)/n_g and resets
+// the graph's state: stopped = `stopped` (max_iters == 0), no sweeps yet.
+__global__ void ragged_init_kernel(const SweepArgs a, RaggedState rs, uint32_t num_graphs, uint64_t nv, float damping,
+                                   uint32_t stopped, float* __restrict__ base) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (uint64_t g = tid; g < num_graphs; g += stride) {
+    const uint32_t n = a.graphs[g].n;
+    // page_rank.hpp:93-94: constants in double, stored as float
+    base[g] = n ? (float)((1.0 - (double)damping) / (double)n) : 0.f;
+    rs.done[g] = stopped;
+    rs.iters[g] = 0u;
+    rs.err[g] = 0.0;
+    rs.conv[g] = 0u;
+  }
+  for (uint64_t v = tid; v < nv; v += stride) {
+    uint32_t lo = 0, hi = num_graphs - 1;  // last graph whose first vertex is <= v
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      if (a.graphs[mid].v0 <= v)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const float r = (float)(1.0 / (double)a.graphs[lo].n);
+    a.rank[v] = r;
+    a.contrib0[v] = r / (float)a.deg[v];
   }
 }
 
@@ -613,7 +878,8 @@ cudaError_t configure_sweep_kernels() {
                                                    e->hot ? maxb : (int)e->fixed_smem);
     if (err != cudaSuccess) return err;
   }
-  return cudaSuccess;
+  return cudaFuncSetAttribute((void*)pr_sweep_kernel<256, 8, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)sizeof(SweepSmem<256, 8>));
 }
 
 cudaError_t set_sweep_carveout(const SweepVariant& v, int percent) {
@@ -665,6 +931,60 @@ cudaError_t add_pr_sweep_nodes(cudaGraph_t body, const SweepArgs& a, const Sweep
   fp.blockDim = dim3(256);
   fp.kernelParams = args;
   return cudaGraphAddKernelNode(&finish_node, body, &sweep_node, 1, &fp);
+}
+
+// ---------------------------------------------------------------------------
+// Ragged batches: launches
+// ---------------------------------------------------------------------------
+static void* ragged_sweep_fn() { return (void*)pr_sweep_kernel<256, 8, false, true>; }
+static size_t ragged_sweep_smem() { return sizeof(SweepSmem<256, 8>); }
+
+cudaError_t launch_ragged_sweep(const SweepArgs& a, int sweep_grid, int finish_grid, uint32_t num_graphs,
+                                const RaggedState& rs, int conv_grid, cudaStream_t s) {
+  void*       args[] = {(void*)&a};
+  cudaError_t e = cudaLaunchKernel(ragged_sweep_fn(), dim3((unsigned)sweep_grid), dim3(256), args, ragged_sweep_smem(), s);
+  if (e != cudaSuccess) return e;
+  pr_ragged_finish_kernel<<<finish_grid, 256, 0, s>>>(a);
+  pr_ragged_converge_kernel<<<conv_grid, 256, 0, s>>>(a, num_graphs, rs);
+  return cudaGetLastError();
+}
+
+cudaError_t add_ragged_nodes(cudaGraph_t body, const SweepArgs& a, int sweep_grid, int finish_grid, uint32_t num_graphs,
+                             const RaggedState& rs, int conv_grid) {
+  void*                sargs[] = {(void*)&a};
+  cudaKernelNodeParams kp = {};
+  kp.func = ragged_sweep_fn();
+  kp.gridDim = dim3((unsigned)sweep_grid);
+  kp.blockDim = dim3(256);
+  kp.sharedMemBytes = (unsigned)ragged_sweep_smem();
+  kp.kernelParams = sargs;
+  cudaGraphNode_t sweep_node, finish_node, conv_node;
+  cudaError_t     e = cudaGraphAddKernelNode(&sweep_node, body, nullptr, 0, &kp);
+  if (e != cudaSuccess) return e;
+  cudaKernelNodeParams fp = {};
+  fp.func = (void*)pr_ragged_finish_kernel;
+  fp.gridDim = dim3((unsigned)finish_grid);
+  fp.blockDim = dim3(256);
+  fp.kernelParams = sargs;
+  e = cudaGraphAddKernelNode(&finish_node, body, &sweep_node, 1, &fp);
+  if (e != cudaSuccess) return e;
+  RaggedState          r = rs;
+  uint32_t             ng = num_graphs;
+  void*                cargs[] = {(void*)&a, (void*)&ng, (void*)&r};
+  cudaKernelNodeParams cp = {};
+  cp.func = (void*)pr_ragged_converge_kernel;
+  cp.gridDim = dim3((unsigned)conv_grid);
+  cp.blockDim = dim3(256);
+  cp.kernelParams = cargs;
+  return cudaGraphAddKernelNode(&conv_node, body, &finish_node, 1, &cp);
+}
+
+cudaError_t launch_ragged_init(const SweepArgs& a, const RaggedState& rs, uint32_t num_graphs, uint64_t num_vertices,
+                               float damping, uint32_t stopped, int sms, cudaStream_t s) {
+  if (!num_graphs) return cudaSuccess;
+  ragged_init_kernel<<<sms * 8, 256, 0, s>>>(a, rs, num_graphs, num_vertices, damping, stopped,
+                                              const_cast<float*>(a.graph_base));
+  return cudaGetLastError();
 }
 
 }  // namespace nwgpu

@@ -333,6 +333,133 @@ class Graph:
         return self._stats(st, errs)
 
 
+@dataclass
+class RaggedStats:
+    sweeps: int
+    converged_graphs: int
+    device_ms: float
+    entries_swept: float
+    gteps: float
+    graph_iterations: np.ndarray
+    graph_errors: np.ndarray
+    graph_converged: np.ndarray
+
+
+class GraphBatch:
+    """Many independent graphs resident in HBM (one ``nwgpu_batch`` handle),
+    solved together by :meth:`page_rank` with per-graph convergence.
+
+    Graph ``g`` is a CSR with local ids: ``row_ptr[vertex_offsets[g] + g :
+    vertex_offsets[g + 1] + g + 1]`` are its row pointers (first 0) and
+    ``col[entry_offsets[g] : entry_offsets[g + 1]]`` its column ids.
+    Per-vertex arrays (degrees, ranks) are concatenated in graph order, graph
+    ``g``'s at ``vertex_offsets[g]``. No counterpart in the reference: each
+    graph gets what ``page_rank`` (page_rank.hpp:92-147) gives for it alone.
+    """
+
+    def __init__(self, vertex_offsets, entry_offsets, row_ptr, col):
+        self.vertex_offsets = np.ascontiguousarray(vertex_offsets, np.uint64)
+        self.entry_offsets = np.ascontiguousarray(entry_offsets, np.uint64)
+        if self.vertex_offsets.shape != self.entry_offsets.shape or self.vertex_offsets.size < 2:
+            raise ValueError("vertex_offsets and entry_offsets need num_graphs + 1 entries each")
+        self.num_graphs = self.vertex_offsets.size - 1
+        self.n = int(self.vertex_offsets[-1])
+        self.nnz = int(self.entry_offsets[-1])
+        rp, rp_dev, k0 = _ptr(row_ptr, np.uint32)
+        cl, cl_dev, k1 = _ptr(col, np.uint32)
+        if self.nnz and rp_dev != cl_dev:
+            raise ValueError("row_ptr and col must both be on the host or both on the device")
+        if len(row_ptr) != self.n + self.num_graphs or len(col) != self.nnz:
+            raise ValueError("row_ptr needs n + num_graphs entries and col entry_offsets[-1]")
+        h = C.c_void_p()
+        N.check(N.lib().nwgpu_batch_create(self.num_graphs, self.vertex_offsets.ctypes.data,
+                                           self.entry_offsets.ctypes.data, rp, cl,
+                                           N.GRAPH_DEVICE_PTRS if rp_dev else 0, C.byref(h)))
+        self._h = h
+        del k0, k1
+
+    @classmethod
+    def from_graphs(cls, graphs):
+        """Batch of ``(row_ptr, col)`` pairs (or objects with ``row_ptr`` / ``col``)."""
+        rps, cols = [], []
+        for g in graphs:
+            rp, cl = (g if isinstance(g, tuple) else _csr_arrays(g))
+            rps.append(np.asarray(rp, np.uint32))
+            cols.append(np.asarray(cl, np.uint32))
+        vo = np.zeros(len(rps) + 1, np.uint64)
+        eo = np.zeros(len(rps) + 1, np.uint64)
+        vo[1:] = np.cumsum([len(r) - 1 for r in rps])
+        eo[1:] = np.cumsum([len(c) for c in cols])
+        return cls(vo, eo, np.concatenate(rps), np.concatenate(cols) if cols else np.zeros(0, np.uint32))
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise ValueError("batch was released")
+        return self._h
+
+    def release(self):
+        if getattr(self, "_h", None) is not None:
+            N.lib().nwgpu_batch_destroy(self._h)
+            self._h = None
+
+    close = release
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.release()
+
+    def split(self, values):
+        """Per-graph views of a concatenated per-vertex array."""
+        vo = self.vertex_offsets.astype(np.int64)
+        return [values[vo[g]:vo[g + 1]] for g in range(self.num_graphs)]
+
+    def page_rank(self, degrees, page_rank, damping_factor=0.85, threshold=1e-4, max_iters=20, launch="graph",
+                  stream=None) -> RaggedStats:
+        """Solve every graph into ``page_rank`` (concatenated, fully overwritten)."""
+        if len(degrees) != self.n or len(page_rank) != self.n:
+            raise ValueError(f"degrees/page_rank must have {self.n} entries")
+        dp, d_dev, keep = _ptr(degrees, np.uint32)
+        out_dev = _is_cuda_tensor(page_rank)
+        if self.n and d_dev != out_dev:
+            raise ValueError("degrees and page_rank must both be host arrays or both device tensors")
+        if out_dev:
+            if str(page_rank.dtype) != "torch.float32" or not page_rank.is_contiguous():
+                raise TypeError("page_rank must be a contiguous float32 tensor")
+            op = page_rank.data_ptr()
+        else:
+            if not (isinstance(page_rank, np.ndarray) and page_rank.dtype == np.float32
+                    and page_rank.flags.c_contiguous):
+                raise TypeError("page_rank must be a contiguous float32 numpy array (filled in place)")
+            op = page_rank.ctypes.data
+        opt = N.PrOptions(size=C.sizeof(N.PrOptions), mode=N.MODE_PARITY,
+                          launch=N.LAUNCH_STREAM if launch == "stream" else N.LAUNCH_GRAPH,
+                          device_ptrs=1 if out_dev else 0)
+        if stream is not None:
+            opt.stream = int(getattr(stream, "cuda_stream", stream))
+        G = self.num_graphs
+        gi = np.zeros(G, np.uint32)
+        ge = np.zeros(G, np.float64)
+        gc = np.zeros(G, np.int32)
+        st = N.BatchStats()
+        st.graph_iterations = gi.ctypes.data_as(C.POINTER(C.c_uint32))
+        st.graph_errors = ge.ctypes.data_as(C.POINTER(C.c_double))
+        st.graph_converged = gc.ctypes.data_as(C.POINTER(C.c_int32))
+        N.check(N.lib().nwgpu_pr_ragged(self.handle, dp, op, C.c_float(damping_factor), C.c_float(threshold),
+                                        int(max_iters), C.byref(opt), C.byref(st)))
+        del keep
+        return RaggedStats(int(st.sweeps), int(st.converged_graphs), float(st.device_ms), float(st.entries_swept),
+                           float(st.gteps), gi, ge, gc.astype(bool))
+
+
 def page_rank(graph, degrees, page_rank, damping_factor=0.85, threshold=1e-4, max_iters=20, num_threads=None):
     """Drop-in for ``nw::graph::page_rank`` (page_rank.hpp:89-148).
 

@@ -1,0 +1,203 @@
+"""Ragged batches: many independent graphs in one solve (nwgpu_pr_ragged).
+
+No counterpart in the reference; the bar is that every graph of a batch gets
+what page_rank_v10 gives for that graph alone: the oracle's jacobi_f32 per
+graph (pinned to the reference in test_oracle.py), within 1e-6 max-abs and
+1e-5 L1, stopping at the same sweep. Graphs mix symmetrised RMAT and
+4-neighbour grids as in the ragged configuration (smaller sizes), plus the
+edge cases: no vertices, no entries, one vertex, and a hub whose row spans
+more than eight tiles.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from nwgraph_b200 import GraphBatch, NwgpuError, graphs as G
+from nwgraph_b200 import _native as N
+
+pytestmark = pytest.mark.gpu
+
+D = 0.85
+MAX_ABS = 1e-6
+L1 = 1e-5
+# Per-sweep L1 errors sum n FP32 rank differences whose last bits depend on
+# the order of the row sums. Ranks form a distribution (sum 1), so iterates
+# that differ by one ulp per vertex give L1 changes that differ by at most
+# 2 * 2^-23 * sum(r) ~ 2.4e-7. A graph whose reference error lands that close
+# to the threshold may stop one sweep earlier or later.
+STOP_ATOL = 2.5e-7
+
+
+def star(n):
+    """Vertex 0 linked both ways with every other vertex."""
+    others = np.arange(1, n, dtype=np.uint32)
+    return G.from_edges(np.concatenate([others, np.zeros(n - 1, np.uint32)]),
+                        np.concatenate([np.zeros(n - 1, np.uint32), others]), n)
+
+
+def empty_graph(n):
+    return G.CSR(np.zeros(n + 1, np.uint32), np.zeros(0, np.uint32))
+
+
+def mixed_graphs(seed=11, count=40):
+    """RMAT (even) and grid (odd) graphs with log-uniform sizes, plus edge cases."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(np.exp(rng.uniform(np.log(64), np.log(20000))))
+        if i % 2 == 0:
+            scale = max(4, int(np.log2(n)))
+            out.append(G.rmat(scale, int(rng.integers(8, 33)), seed=int(rng.integers(1 << 30))))
+        else:
+            out.append(G.grid(n))
+    out[5:5] = [empty_graph(0), empty_graph(1), empty_graph(7), star(40000)]
+    return out
+
+
+def oracle_each(graphs, thr, iters, damping=D):
+    res = []
+    for g in graphs:
+        n = len(g.row_ptr) - 1
+        if n == 0:  # error 0 at every sweep
+            res.append((np.zeros(0, np.float32), 1 if thr > 0 else iters, np.zeros(0)))
+            continue
+        res.append(O.jacobi_f32(g.row_ptr, g.col, O.out_degree(g.row_ptr, g.col, n), damping, thr, iters))
+    return res
+
+
+def batch_degrees(graphs):
+    return np.concatenate([O.out_degree(g.row_ptr, g.col, len(g.row_ptr) - 1) for g in graphs] +
+                          [np.zeros(0, np.uint32)])
+
+
+def close(a, b):
+    d = np.abs(a.astype(np.float64) - b.astype(np.float64))
+    return d.size == 0 or (d.max() <= MAX_ABS and d.sum() <= L1)
+
+
+def check_batch(graphs, r, st, ref, thr, damping=D):
+    """Every graph against the oracle run alone. Graphs stop at the oracle's
+    sweep (one apart when its error is within STOP_ATOL of the threshold) with
+    ranks within tolerance; or, for hub rows whose serial FP32 sum in the
+    reference is itself off FP64 Jacobi by more than the tolerance (and then
+    freezes or cycles, so it stops at another sweep, or never), the engine's
+    ranks must be at least as close to FP64 Jacobi at its own sweep count as
+    the reference's are at theirs."""
+    offs = np.concatenate([[0], np.cumsum([len(g.row_ptr) - 1 for g in graphs])])
+    for i, (g, (rr, it, errs)) in enumerate(zip(graphs, ref)):
+        got = r[offs[i]:offs[i + 1]]
+        gi = int(st.graph_iterations[i])
+        assert bool(st.graph_converged[i]) == (thr > 0 and st.graph_errors[i] < thr), i
+        same_stop = gi == it or (thr > 0 and abs(gi - it) == 1 and abs(errs[min(gi, it) - 1] - thr) < STOP_ATOL)
+        if same_stop and close(got, rr):
+            if gi == it and len(errs):
+                assert np.isclose(st.graph_errors[i], errs[-1], rtol=1e-4, atol=STOP_ATOL), (i, st.graph_errors[i])
+            continue
+        e_ref = np.abs(rr.astype(np.float64) - O.pr_f64(g.row_ptr, g.col, damping=damping, tol=0.0, max_iters=it)[0])
+        e_gpu = np.abs(got.astype(np.float64) - O.pr_f64(g.row_ptr, g.col, damping=damping, tol=0.0, max_iters=gi)[0])
+        assert e_ref.max() > MAX_ABS, (i, gi, it, "the reference is accurate here, so the engine must match it")
+        assert e_gpu.max() <= e_ref.max() * 1.01 + 1e-9 and e_gpu.sum() <= e_ref.sum() * 1.01 + 1e-8, i
+
+
+@pytest.fixture(scope="module")
+def mixed():
+    gs = mixed_graphs()
+    return gs, batch_degrees(gs)
+
+
+def test_mixed_batch_converged_per_graph(gpu, mixed):
+    graphs, deg = mixed
+    thr, iters = 1e-6, 200
+    with GraphBatch.from_graphs([(g.row_ptr, g.col) for g in graphs]) as b:
+        r = np.empty(b.n, np.float32)
+        st = b.page_rank(deg, r, D, thr, iters)
+    ref = oracle_each(graphs, thr, iters)
+    check_batch(graphs, r, st, ref, thr)
+    # graphs stop at different sweeps; the batch runs until the last one stops
+    assert st.sweeps == int(st.graph_iterations.max())
+    assert len(set(st.graph_iterations.tolist())) > 3
+    assert st.converged_graphs == int(st.graph_converged.sum()) == len(graphs)
+    nnz = np.array([len(g.col) for g in graphs], np.float64)
+    assert st.entries_swept == pytest.approx(float((nnz * st.graph_iterations).sum()))
+
+
+def test_fixed_sweeps_and_launch_modes_agree(gpu, mixed):
+    graphs, deg = mixed
+    with GraphBatch.from_graphs([(g.row_ptr, g.col) for g in graphs]) as b:
+        r1 = np.empty(b.n, np.float32)
+        r2 = np.empty(b.n, np.float32)
+        st1 = b.page_rank(deg, r1, D, 0.0, 20)
+        st2 = b.page_rank(deg, r2, D, 0.0, 20, launch="stream")
+    assert np.array_equal(r1.view(np.uint32), r2.view(np.uint32))
+    assert np.all(st1.graph_iterations == 20) and np.all(st2.graph_iterations == 20)
+    assert st1.sweeps == 20 and st1.converged_graphs == 0
+    check_batch(graphs, r1, st1, oracle_each(graphs, 0.0, 20), 0.0)
+
+
+def test_thousands_of_small_graphs(gpu):
+    # graph boundaries inside nearly every tile; several converge CTAs
+    rng = np.random.default_rng(3)
+    graphs = []
+    for _ in range(3000):
+        n = int(rng.integers(1, 80))
+        m = int(rng.integers(0, 4 * n))
+        graphs.append(G.from_edges(rng.integers(0, n, m), rng.integers(0, n, m), n, symmetrize=True))
+    deg = batch_degrees(graphs)
+    with GraphBatch.from_graphs([(g.row_ptr, g.col) for g in graphs]) as b:
+        r = np.empty(b.n, np.float32)
+        st = b.page_rank(deg, r, D, 1e-6, 200)
+    check_batch(graphs, r, st, oracle_each(graphs, 1e-6, 200), 1e-6)
+
+
+def test_device_pointers_and_reuse(gpu, mixed):
+    import torch
+    graphs, deg = mixed
+    dev = torch.device("cuda")
+    b0 = GraphBatch.from_graphs([(g.row_ptr, g.col) for g in graphs])
+    rh = np.empty(b0.n, np.float32)
+    b0.page_rank(deg, rh, D, 1e-6, 200)
+    rp = np.concatenate([g.row_ptr for g in graphs])
+    cl = np.concatenate([g.col for g in graphs])
+    with GraphBatch(b0.vertex_offsets, b0.entry_offsets, torch.from_numpy(rp.view(np.int32)).to(dev),
+                    torch.from_numpy(cl.view(np.int32)).to(dev)) as b:
+        rd = torch.empty(b.n, dtype=torch.float32, device=dev)
+        b.page_rank(torch.from_numpy(deg.view(np.int32)).to(dev), rd, D, 1e-6, 200)
+        assert np.array_equal(rd.cpu().numpy(), rh)
+        # another damping on the same handle (the sweep loop is rebuilt)
+        r2 = np.empty(b.n, np.float32)
+        st = b.page_rank(deg, r2, 0.5, 1e-6, 200)
+        check_batch(graphs, r2, st, oracle_each(graphs, 1e-6, 200, 0.5), 1e-6, 0.5)
+    b0.release()
+
+
+def test_max_iters_zero_and_single_graph(gpu):
+    g = G.rmat(10, 16, 5)
+    deg = O.out_degree(g.row_ptr, g.col, g.n)
+    with GraphBatch.from_graphs([(g.row_ptr, g.col)]) as b:
+        r = np.empty(g.n, np.float32)
+        st = b.page_rank(deg, r, D, 1e-4, 0)
+        assert st.sweeps == 0 and np.all(r == np.float32(1.0 / g.n)) and st.graph_iterations[0] == 0
+        st = b.page_rank(deg, r, D, 1e-4, 20)
+    ref, it, _ = O.jacobi_f32(g.row_ptr, g.col, deg, D, 1e-4, 20)
+    assert st.graph_iterations[0] == it and close(r, ref)
+
+
+def test_invalid_batches_rejected(gpu):
+    a = G.grid(100)
+    b = G.grid(49)
+    ok = [(a.row_ptr, a.col), (b.row_ptr, b.col)]
+    bad_col = b.col.copy()
+    bad_col[3] = 60  # a valid id of the batch, but not of graph 1 (49 vertices)
+    with pytest.raises(NwgpuError) as ei:
+        GraphBatch.from_graphs([ok[0], (b.row_ptr, bad_col)])
+    assert ei.value.status == N.ERR_INVALID_GRAPH and "column" in str(ei.value)
+    bad_rp = b.row_ptr.copy()
+    bad_rp[-1] -= 1
+    with pytest.raises(NwgpuError) as ei:
+        GraphBatch.from_graphs([ok[0], (bad_rp, b.col)])
+    assert ei.value.status == N.ERR_INVALID_GRAPH
+    vo = np.array([0, 100, 90], np.uint64)
+    eo = np.array([0, len(a.col), len(a.col)], np.uint64)
+    with pytest.raises(NwgpuError) as ei:
+        GraphBatch(vo, eo, np.zeros(92, np.uint32), a.col)
+    assert ei.value.status == N.ERR_INVALID_ARG
