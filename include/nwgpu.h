@@ -219,6 +219,48 @@ int nwgpu_pr_vjp(nwgpu_graph* g, const float* ranks, const float* dL_dr, float* 
  * returns NWGPU_ERR_ABORTED. Safe to call from another host thread. */
 int nwgpu_abort(nwgpu_graph* g);
 
+/* ---- Graph construction on the device ------------------------------------
+ * CSR from an edge list (src[e] -> dst[e], m edges over n vertices): the
+ * reference's remove_self_loops (build.hpp:404-410), uniq (:394-402) and
+ * fill_directed / fill_undirected (:209-272), in that order, as flags, on
+ * the device. Rows
+ * are indexed by target (adjacency<1>, row v lists the sources of edges into
+ * v) unless NWGPU_EDGES_BY_SOURCE (adjacency<0>); entries of a row come out
+ * sorted ascending, as with fill(..., sort_adjacency = true). Writes
+ * row_ptr[n + 1], col[nnz] (col_capacity must be >= nnz; otherwise
+ * NWGPU_ERR_INVALID_ARG with *nnz set) and, when degrees is not NULL,
+ * degrees[n] = the number of entries whose column is v (the out-degree the
+ * bench's build_degrees computes for an adjacency<1>, common.hpp:110-121).
+ * Arrays are host pointers unless NWGPU_EDGES_DEVICE_PTRS. stream: a
+ * cudaStream_t, NULL for the default stream; the call returns when done. */
+#define NWGPU_EDGES_DEVICE_PTRS 0x1u       /* src, dst and the outputs are device pointers */
+#define NWGPU_EDGES_BY_SOURCE 0x2u         /* rows indexed by source (adjacency<0>) */
+#define NWGPU_EDGES_UNDIRECTED 0x4u        /* fill_undirected: every edge in both directions */
+#define NWGPU_EDGES_REMOVE_SELF_LOOPS 0x8u /* remove_self_loops */
+#define NWGPU_EDGES_UNIQUE 0x10u           /* uniq on the edge list: each (src, dst) pair once, before fill */
+#define NWGPU_EDGES_UNIQUE_ENTRIES 0x20u   /* one entry per (row, col) of the result (simple graph; not a
+                                              reference step: with UNDIRECTED, (u, v) and (v, u) both listed
+                                              otherwise give two entries per row, as in fill_undirected) */
+int nwgpu_csr_from_edges(const uint32_t* src, const uint32_t* dst, uint64_t m, uint64_t n, uint32_t flags,
+                         uint32_t* row_ptr, uint32_t* col, uint64_t col_capacity, uint64_t* nnz, uint32_t* degrees,
+                         void* stream);
+
+/* Seeded RMAT edge list on the device (no counterpart in the reference, which
+ * ships no generator): m samples over 2^scale ids, each descending `scale`
+ * levels with quadrant probabilities a, b, c (d = 1 - a - b - c) drawn from a
+ * counter-based hash of (seed, sample, level); the same samples as the host
+ * builder nwgen_rmat (include/nwgraph_gen.h). With 0 < n < 2^scale the ids
+ * are taken modulo n. src[m], dst[m] are device pointers. Asynchronous on
+ * stream. */
+int nwgpu_rmat_edges(uint32_t scale, uint64_t m, double a, double b, double c, uint64_t seed, uint64_t n, uint32_t* src,
+                     uint32_t* dst, void* stream);
+
+/* The side x side 4-neighbour grid as 2 side (side - 1) undirected edges
+ * (horizontal (v, v+1) first, then vertical (v, v+side)); device pointers,
+ * asynchronous on stream. Built with NWGPU_EDGES_UNDIRECTED it equals
+ * nwgen_grid(side * side). */
+int nwgpu_grid_edges(uint64_t side, uint32_t* src, uint32_t* dst, void* stream);
+
 /* ---- Ragged batches: many independent graphs in one solve ----------------
  * No counterpart in the reference: each graph's result is what page_rank
  * (page_rank.hpp:92-147) gives for that graph alone, and each graph stops at

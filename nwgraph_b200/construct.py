@@ -1,0 +1,112 @@
+"""Graph construction on the device (``nwgpu_csr_from_edges``,
+``nwgpu_rmat_edges``, ``nwgpu_grid_edges``).
+
+The reference builds its CSR on the host: an edge list, optionally
+``remove_self_loops`` and ``uniq`` (include/nwgraph/build.hpp:394-410), then
+``fill_directed`` / ``fill_undirected`` (:209-272) into ``adjacency<idx>``.
+:func:`csr_from_edges` does the same steps on the GPU as radix sorts of packed
+keys. :func:`rmat` and :func:`grid` generate their edge lists on the device
+with the host builder's samples (``graphs.rmat`` / ``graphs.grid``) and build
+them there, so they return the same CSR many times faster.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from .graphs import CSR, RMAT_ABC
+
+DEVICE_PTRS = 0x1
+BY_SOURCE = 0x2
+UNDIRECTED = 0x4
+REMOVE_SELF_LOOPS = 0x8
+UNIQUE = 0x10
+UNIQUE_ENTRIES = 0x20
+# the host builder's clean-up of generated graphs (graphgen.cpp): a simple symmetric graph
+SIMPLE_UNDIRECTED = UNDIRECTED | REMOVE_SELF_LOOPS | UNIQUE_ENTRIES
+
+
+def csr_from_edges(src, dst, n: int, flags: int = 0):
+    """CSR of the edge list ``src[e] -> dst[e]`` over ``n`` vertices.
+
+    Host arrays in, ``(CSR, degrees)`` out as numpy; CUDA tensors in, device
+    tensors ``(row_ptr, col, degrees)`` out. ``flags``: BY_SOURCE,
+    UNDIRECTED, REMOVE_SELF_LOOPS, UNIQUE, UNIQUE_ENTRIES (include/nwgpu.h).
+    """
+    m = len(src)
+    if hasattr(src, "is_cuda") and src.is_cuda:
+        import torch
+        total = 2 * m if flags & UNDIRECTED else m
+        rp = torch.empty(n + 1, dtype=torch.int32, device=src.device)
+        cl = torch.empty(max(total, 1), dtype=torch.int32, device=src.device)
+        deg = torch.empty(n, dtype=torch.int32, device=src.device)
+        nnz = C.c_uint64()
+        stream = torch.cuda.current_stream(src.device).cuda_stream
+        N.check(N.lib().nwgpu_csr_from_edges(src.data_ptr(), dst.data_ptr(), m, n, flags | DEVICE_PTRS, rp.data_ptr(),
+                                             cl.data_ptr(), cl.numel(), C.byref(nnz), deg.data_ptr(), stream))
+        return rp, cl[: nnz.value], deg
+    s = np.ascontiguousarray(src, np.uint32)
+    d = np.ascontiguousarray(dst, np.uint32)
+    total = 2 * m if flags & UNDIRECTED else m
+    rp = np.empty(n + 1, np.uint32)
+    cl = np.empty(max(total, 1), np.uint32)
+    deg = np.empty(n, np.uint32)
+    nnz = C.c_uint64()
+    N.check(N.lib().nwgpu_csr_from_edges(s.ctypes.data, d.ctypes.data, m, n, flags & ~DEVICE_PTRS, rp.ctypes.data,
+                                         cl.ctypes.data, cl.size, C.byref(nnz), deg.ctypes.data, None))
+    return CSR(rp, cl[: nnz.value].copy()), deg
+
+
+def _edges(m, device):
+    import torch
+    return (torch.empty(max(m, 1), dtype=torch.int32, device=device),
+            torch.empty(max(m, 1), dtype=torch.int32, device=device))
+
+
+def rmat_edges(scale: int, m: int, seed: int = 42, abc=RMAT_ABC, n: int = 0, device="cuda"):
+    """m seeded RMAT samples as two int32 device tensors (ids modulo n when 0 < n < 2^scale)."""
+    import torch
+    src, dst = _edges(m, device)
+    stream = torch.cuda.current_stream(src.device).cuda_stream
+    N.check(N.lib().nwgpu_rmat_edges(int(scale), int(m), abc[0], abc[1], abc[2], int(seed), int(n), src.data_ptr(),
+                                     dst.data_ptr(), stream))
+    return src[:m], dst[:m]
+
+
+def grid_edges(side: int, device="cuda"):
+    """The side x side 4-neighbour grid's 2 side (side - 1) edges on the device."""
+    import torch
+    m = 2 * side * (side - 1)
+    src, dst = _edges(m, device)
+    stream = torch.cuda.current_stream(src.device).cuda_stream
+    N.check(N.lib().nwgpu_grid_edges(int(side), src.data_ptr(), dst.data_ptr(), stream))
+    return src[:m], dst[:m]
+
+
+def rmat(scale: int, edge_factor: float = 16, seed: int = 42, abc=RMAT_ABC, device_out: bool = False):
+    """``graphs.rmat`` built on the device: the same symmetrised simple graph.
+    Returns a host CSR, or device tensors ``(row_ptr, col, degrees)``."""
+    m = int(np.floor(edge_factor * (1 << scale) + 0.5))  # llround, as the host builder
+    src, dst = rmat_edges(scale, m, seed, abc)
+    rp, cl, deg = csr_from_edges(src, dst, 1 << scale, SIMPLE_UNDIRECTED)
+    del src, dst
+    if device_out:
+        return rp, cl, deg
+    return CSR(rp.cpu().numpy().view(np.uint32), cl.cpu().numpy().view(np.uint32))
+
+
+def grid(n_target: int, device_out: bool = False):
+    """``graphs.grid`` built on the device."""
+    side = max(1, int(np.floor(np.sqrt(n_target))))
+    while (side + 1) * (side + 1) <= n_target:
+        side += 1
+    while side * side > n_target:
+        side -= 1
+    side = max(side, 1)
+    src, dst = grid_edges(side)
+    rp, cl, deg = csr_from_edges(src, dst, side * side, UNDIRECTED)
+    if device_out:
+        return rp, cl, deg
+    return CSR(rp.cpu().numpy().view(np.uint32), cl.cpu().numpy().view(np.uint32))

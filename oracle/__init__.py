@@ -102,6 +102,9 @@ def ref(fast: bool = False):
         L.nwref_build_degrees.argtypes = [_u32p, _u32p, C.c_uint64, _u32p, C.c_int]
         L.nwref_fill_adj1.restype = C.c_int
         L.nwref_fill_adj1.argtypes = [_u32p, _u32p, C.c_uint64, C.c_uint64, _u32p, _u32p]
+        L.nwref_build_csr.restype = C.c_int
+        L.nwref_build_csr.argtypes = [_u32p, _u32p, C.c_uint64, C.c_uint64, C.c_int, _u32p, _u32p, C.c_uint64,
+                                      C.POINTER(C.c_uint64)]
         L.nwref_load_mm.restype = C.c_void_p
         L.nwref_load_mm.argtypes = [C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
         L.nwref_copy_csr.restype = None
@@ -268,6 +271,61 @@ def ref_fill_adj1(src, dst, n):
     if rc != 0:
         raise RuntimeError("nwref_fill_adj1 failed")
     return rp, cl[:m]
+
+
+# Flags of the edge-list -> CSR build (the values of include/nwgpu.h's NWGPU_EDGES_*).
+BY_SOURCE, UNDIRECTED, REMOVE_SELF_LOOPS, UNIQUE, UNIQUE_ENTRIES = 0x2, 0x4, 0x8, 0x10, 0x20
+
+
+def build_csr(src, dst, n, flags):
+    """Edge list -> CSR restated: the reference's remove_self_loops
+    (build.hpp:404-410), lexical sort + uniq on the edge list (:58-69,
+    :394-402) and fill_directed / fill_undirected (:209-272) with
+    sort_adjacency (:311-321), i.e. rows indexed by target (by source with
+    BY_SOURCE), both directions of every edge with UNDIRECTED, rows sorted.
+    UNIQUE_ENTRIES then drops repeated (row, col) entries of the result (the
+    host builder's simple-graph clean-up, graphgen.cpp; not a reference step).
+    Returns (row_ptr, col, degrees) with degrees = column occurrences
+    (bench/gapbs/common.hpp:110-121)."""
+    s = np.asarray(src, np.uint64)
+    d = np.asarray(dst, np.uint64)
+    if flags & REMOVE_SELF_LOOPS:
+        keep = s != d
+        s, d = s[keep], d[keep]
+    if flags & UNIQUE:
+        pairs = np.unique(s << np.uint64(32) | d)
+        s, d = pairs >> np.uint64(32), pairs & np.uint64(0xFFFFFFFF)
+    row, col = (s, d) if flags & BY_SOURCE else (d, s)
+    if flags & UNDIRECTED:
+        row, col = np.concatenate([row, col]), np.concatenate([col, row])
+    keys = np.sort(row << np.uint64(32) | col)
+    if flags & UNIQUE_ENTRIES:
+        keys = np.unique(keys)
+    r = (keys >> np.uint64(32)).astype(np.int64)
+    c = (keys & np.uint64(0xFFFFFFFF)).astype(np.uint32)
+    rp = np.zeros(int(n) + 1, np.uint32)
+    rp[1:] = np.cumsum(np.bincount(r, minlength=int(n)))
+    return rp, c, np.bincount(c, minlength=int(n)).astype(np.uint32)
+
+
+def ref_build_csr(src, dst, n, flags):
+    """The same through the reference's own code (oracle/_ref); (row_ptr, col).
+    UNIQUE_ENTRIES is not a reference step and is refused."""
+    if flags & UNIQUE_ENTRIES:
+        raise ValueError("UNIQUE_ENTRIES has no reference counterpart")
+    flags = ((1 if flags & BY_SOURCE else 0) | (2 if flags & UNDIRECTED else 0) | (4 if flags & REMOVE_SELF_LOOPS else 0)
+             | (8 if flags & UNIQUE else 0))
+    src = np.ascontiguousarray(src, np.uint32)
+    dst = np.ascontiguousarray(dst, np.uint32)
+    m = len(src)
+    cap = 2 * m + 1
+    rp = np.empty(int(n) + 1, np.uint32)
+    cl = np.empty(cap, np.uint32)
+    nnz = C.c_uint64()
+    if ref().nwref_build_csr(_p(src, _u32p), _p(dst, _u32p), m, int(n), int(flags), _p(rp, _u32p), _p(cl, _u32p), cap,
+                             C.byref(nnz)) != 0:
+        raise RuntimeError("nwref_build_csr failed")
+    return rp, cl[: nnz.value]
 
 
 def ref_load_mm(path):

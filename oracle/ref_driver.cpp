@@ -11,6 +11,8 @@
 //   nw::graph::page_rank_v1         include/nwgraph/experimental/algorithms/page_rank.hpp:82-119 (serial Jacobi)
 //   nw::graph::bench::build_degrees bench/gapbs/common.hpp:110-121 (out-degree from adjacency<1>)
 //   nw::graph::read_mm              include/nwgraph/io/mmio.hpp:171-217 + adjacency<1> fill (build.hpp:209-232)
+//   edge clean-up and fill          remove_self_loops / lexical_sort_by / uniq (build.hpp:58-69, 394-410),
+//                                   adjacency<idx>(el, sort_adjacency) (adjacency.hpp:115-129, build.hpp:209-321)
 //
 // Per-iteration times come from the reference's own pagerank::trace lines
 // (page_rank.hpp:42-52, printed at :142), captured from std::cout.
@@ -133,6 +135,44 @@ int nwref_fill_adj1(const uint32_t* src, const uint32_t* dst, uint64_t m, uint64
   std::memcpy(row_ptr, g.indices_.data(), (n + 1) * sizeof(uint32_t));
   std::memcpy(col, std::get<0>(g.to_be_indexed_).data(), m * sizeof(uint32_t));
   return 0;
+}
+
+// Edge list -> CSR with the reference's own clean-up steps and fill, rows
+// sorted (sort_adjacency = true). flags: 1 by source (adjacency<0>), 2
+// undirected edge list (fill_undirected), 4 remove_self_loops, 8 lexical sort
+// + uniq. Returns -1 if col_cap is too small (nnz still set).
+}  // extern "C"
+template <nw::graph::directedness D, int idx>
+int build_csr(const uint32_t* src, const uint32_t* dst, uint64_t m, uint64_t n, int flags, uint32_t* row_ptr,
+              uint32_t* col, uint64_t col_cap, uint64_t* nnz) {
+  nw::graph::edge_list<D> el(n);
+  el.open_for_push_back();
+  for (uint64_t e = 0; e < m; ++e) el.push_back(src[e], dst[e]);
+  el.close_for_push_back();
+  CoutCapture cap;
+  if (flags & 4) nw::graph::remove_self_loops(el);
+  if (flags & 8) {
+    nw::graph::lexical_sort_by<0>(el);
+    nw::graph::uniq(el);
+  }
+  nw::graph::adjacency<idx> g(el, true);
+  *nnz = g.indices_.back();
+  if (g.indices_.size() != n + 1 || *nnz > col_cap) return -1;
+  std::memcpy(row_ptr, g.indices_.data(), (n + 1) * sizeof(uint32_t));
+  std::memcpy(col, std::get<0>(g.to_be_indexed_).data(), *nnz * sizeof(uint32_t));
+  return 0;
+}
+extern "C" {
+
+int nwref_build_csr(const uint32_t* src, const uint32_t* dst, uint64_t m, uint64_t n, int flags, uint32_t* row_ptr,
+                    uint32_t* col, uint64_t col_cap, uint64_t* nnz) {
+  using nw::graph::directedness;
+  const bool by_source = flags & 1, undirected = flags & 2;
+  if (undirected)
+    return by_source ? build_csr<directedness::undirected, 0>(src, dst, m, n, flags, row_ptr, col, col_cap, nnz)
+                     : build_csr<directedness::undirected, 1>(src, dst, m, n, flags, row_ptr, col, col_cap, nnz);
+  return by_source ? build_csr<directedness::directed, 0>(src, dst, m, n, flags, row_ptr, col, col_cap, nnz)
+                   : build_csr<directedness::directed, 1>(src, dst, m, n, flags, row_ptr, col, col_cap, nnz);
 }
 
 // A resident adjacency<1> + degrees, so timing runs do not re-copy the CSR.

@@ -30,6 +30,22 @@ def small_graphs():
     return out
 
 
+@pytest.fixture(scope="session")
+def csr_golden():
+    """Edge lists and the reference's CSRs for each clean-up flag set:
+    {name: {"src", "dst", "n", flags: {"row_ptr", "col", "deg"}}}."""
+    z = np.load(os.path.join(GOLDEN, "csr_build.npz"))
+    out = {}
+    for key in z.files:
+        parts = key.split("/")
+        g = out.setdefault(parts[0], {})
+        if len(parts) == 2:
+            g[parts[1]] = z[key] if parts[1] != "n" else int(z[key][0])
+        else:
+            g.setdefault(int(parts[1]), {})[parts[2]] = z[key]
+    return out
+
+
 def has_gpu():
     try:
         import torch

@@ -14,6 +14,11 @@ the reference tree; the GPU host only reads the committed .npz files).
   vertices) with NWGraph's FP32 page_rank_v10 (20 sweeps, threshold 0, and
   threshold 1e-4 with its sweep count and per-sweep errors) and page_rank v11
   on one thread.
+* ``csr_build.npz`` -- edge lists with repeated edges, reversed pairs and
+  self-loops (and the karate list), and the CSR the reference builds from
+  each with every combination of remove_self_loops, lexical sort + uniq, and
+  adjacency<0> / adjacency<1> over a directed or undirected edge list
+  (build.hpp:58-69, 209-272, 394-410; rows sorted).
 
 All reference outputs come from oracle/_ref/libnwref.so, built from the
 reference headers by oracle/Makefile.
@@ -82,11 +87,41 @@ def isolated_mix(n=700, seed=5):
     return G.from_edges(s, d, n, symmetrize=True)  # upper half of the ids is isolated
 
 
+CSR_FLAG_SETS = [f for f in range(0, 0x20, 2)]  # BY_SOURCE | UNDIRECTED | REMOVE_SELF_LOOPS | UNIQUE
+
+
+def csr_fixtures(karate_i, karate_j):
+    rng = np.random.default_rng(2024)
+    lists = {"karate": (karate_i, karate_j, 34)}
+    for name, n, m in (("small", 12, 60), ("medium", 200, 3000), ("sparse", 1000, 700)):
+        s = rng.integers(0, n, m).astype(np.uint32)
+        d = rng.integers(0, n, m).astype(np.uint32)
+        k = m // 10  # repeated edges, reversed pairs and self-loops
+        s[:k], d[:k] = s[k:2 * k], d[k:2 * k]
+        s[2 * k:3 * k], d[2 * k:3 * k] = d[3 * k:4 * k], s[3 * k:4 * k]
+        d[4 * k:4 * k + k // 2] = s[4 * k:4 * k + k // 2]
+        lists[name] = (s, d, n)
+    out = {}
+    for name, (s, d, n) in lists.items():
+        out[f"{name}/src"], out[f"{name}/dst"], out[f"{name}/n"] = s, d, np.array([n], np.int64)
+        for f in CSR_FLAG_SETS:
+            rp, cl = O.ref_build_csr(s, d, n, f)
+            out[f"{name}/{f}/row_ptr"], out[f"{name}/{f}/col"] = rp, cl
+            out[f"{name}/{f}/deg"] = O.ref_build_degrees(rp, cl)  # column occurrences
+    np.savez_compressed(os.path.join(HERE, "csr_build.npz"), **out)
+    print("csr_build:", len(lists), "edge lists x", len(CSR_FLAG_SETS), "flag sets")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=os.environ.get("NWGRAPH_REF", "/root/reference"))
+    ap.add_argument("--only", choices=["csr"], default=None, help="regenerate csr_build.npz alone")
     args = ap.parse_args()
     O.build(with_reference=True)
+    if args.only == "csr":
+        src = open(os.path.join(args.ref, "test", "page_rank_test.cpp")).read()
+        csr_fixtures(np.array(parse_vector(src, "i"), np.uint32), np.array(parse_vector(src, "j"), np.uint32))
+        return
 
     src = open(os.path.join(args.ref, "test", "page_rank_test.cpp")).read()
     i = np.array(parse_vector(src, "i"), np.uint32)
@@ -119,6 +154,7 @@ def main():
             out[f"{name}/{key}"] = val
         print(name, "n", g.n, "nnz", g.nnz, "v10 thr iters", int(out[f"{name}/v10_thr_iters"][0]))
     np.savez_compressed(os.path.join(HERE, "small_graphs.npz"), **out)
+    csr_fixtures(i, j)
 
 
 if __name__ == "__main__":

@@ -138,3 +138,14 @@ def test_vjp_fp64_matches_finite_differences_teleport():
         rm_, _, _ = O.pr_f64(g.row_ptr, g.col, weights=w, teleport=tm, tol=1e-15)
         fd = (cvec @ rp_ - cvec @ rm_) / (2 * h)
         assert abs(fd - dt[v]) <= 1e-6 * max(abs(dt).max(), 1e-12)
+
+
+def test_build_csr_restatement_matches_reference_golden(csr_golden):
+    """oracle.build_csr (edge clean-up + fill restated) against the CSRs the
+    reference's own remove_self_loops / uniq / fill built (csr_build.npz)."""
+    for name, g in csr_golden.items():
+        for f in range(0, 0x20, 2):
+            rp, cl, deg = O.build_csr(g["src"], g["dst"], g["n"], f)
+            assert np.array_equal(rp, g[f]["row_ptr"]), (name, f)
+            assert np.array_equal(cl, g[f]["col"]), (name, f)
+            assert np.array_equal(deg, g[f]["deg"]), (name, f)
