@@ -65,6 +65,9 @@ def parse():
     ap.add_argument("--no-relabel", action="store_true", help="keep the input vertex order on the device")
     ap.add_argument("--ppr-scale", type=int, default=22, help="graph scale of the batched-PPR comparison (0: skip)")
     ap.add_argument("--ppr-k", type=int, default=64)
+    ap.add_argument("--ragged-graphs", type=int, default=4096,
+                    help="graphs of the ragged-batch comparison (0: skip)")
+    ap.add_argument("--ragged-max-n", type=float, default=1e6, help="largest graph of the ragged batch")
     ap.add_argument("--vjp-scale", type=int, default=20,
                     help="graph scale of the weighted forward vs adjoint (backward) timing (0: skip)")
     ap.add_argument("--launch", default="graph", choices=["graph", "stream"],
@@ -168,10 +171,17 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_graph(args):
-    from nwgraph_b200 import graphs as G
+def make_graph(args, device=False):
+    """The RMAT workload graph: built on the GPU (nwgpu_rmat_edges +
+    nwgpu_csr_from_edges) for our arm, on the host for the reference arm;
+    both give the same CSR bit for bit (tests/test_construct_gpu.py)."""
     t0 = time.time()
-    g = G.rmat(args.scale, args.edge_factor, args.seed)
+    if device:
+        from nwgraph_b200 import construct as K
+        g = K.rmat(args.scale, args.edge_factor, args.seed)
+    else:
+        from nwgraph_b200 import graphs as G
+        g = G.rmat(args.scale, args.edge_factor, args.seed)
     return g, g.out_degree(), time.time() - t0
 
 
@@ -235,6 +245,81 @@ def ppr_batched_vs_looped(scale, k, stream):
             "batched_ms": t_batched, "looped_ms": t_looped, "speedup": t_looped / t_batched,
             "batched_sweeps": stb.iterations, "looped_sweeps_total": looped_sweeps,
             "all_converged": stb.all_converged, "max_abs_batched_vs_looped": worst}
+
+
+def ragged_batch(num_graphs, max_n, seed=11):
+    """The ragged configuration, built on the GPU: n_g log-uniform in
+    [1e3, max_n] (seed 11); even graph ids symmetrised RMAT (edge factor
+    U{8..32}, scale ceil(log2 n_g), ids taken modulo n_g, self-loops and
+    repeats dropped), odd ids floor(sqrt(n_g))^2 4-neighbour grids. Returns the
+    per-graph device CSRs and degrees."""
+    import math
+    from nwgraph_b200 import construct as K
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(np.log(1e3), np.log(max_n), num_graphs)).astype(np.int64)
+    efs = rng.integers(8, 33, num_graphs)
+    parts, degs = [], []
+    for g in range(num_graphs):
+        n = int(ns[g])
+        if g % 2 == 0:
+            src, dst = K.rmat_edges(max(1, math.ceil(math.log2(n))), int(efs[g]) * n, seed=seed + g, n=n)
+            rp, cl, dg = K.csr_from_edges(src, dst, n, K.SIMPLE_UNDIRECTED)
+            del src, dst
+        else:
+            rp, cl, dg = K.grid(n, device_out=True)
+        parts.append((rp, cl))
+        degs.append(dg)
+    return parts, degs
+
+
+def ragged_vs_looped(num_graphs, max_n, stream, sample_mod=16):
+    """One ragged-batch solve of every graph (per-graph L1 < 1e-6, at most 200
+    sweeps) against looped single-graph solves on the same engine, timed on a
+    sample (graph ids = 0 or 1 mod sample_mod: RMAT and grid alike) and
+    scaled to the batch."""
+    import torch
+    from nwgraph_b200 import Graph, construct as K
+    t0 = time.time()
+    parts, degs = ragged_batch(num_graphs, max_n)
+    torch.cuda.synchronize()
+    build_s = time.time() - t0
+    nv = sum(int(p[0].numel()) - 1 for p in parts)
+    nnz = sum(int(p[1].numel()) for p in parts)
+    sample = [g for g in range(num_graphs) if g % sample_mod in (0, 1)]
+    kept = [(parts[g][0].clone(), parts[g][1].clone(), degs[g].clone()) for g in sample]
+    b, deg = K.batch_from_device_csrs(parts, degs)
+    out = torch.empty(max(b.n, 1), dtype=torch.float32, device="cuda")
+    b.page_rank(deg, out, DAMPING, 1e-6, 200, stream=stream)  # warm-up
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    st = b.page_rank(deg, out, DAMPING, 1e-6, 200, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_batched = e0.elapsed_time(e1)
+    b.release()
+    del out, deg, b
+    looped_ms, looped_swept = 0.0, 0.0
+    for rp, cl, dg in kept:
+        with Graph(rp, cl) as h:
+            o = torch.empty(rp.numel() - 1, dtype=torch.float32, device="cuda")
+            h.page_rank(dg, o, DAMPING, 1e-6, 200, stream=stream)  # warm-up
+            torch.cuda.synchronize()
+            e0.record(stream)
+            s1 = h.page_rank(dg, o, DAMPING, 1e-6, 200, stream=stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            looped_ms += e0.elapsed_time(e1)
+            looped_swept += float(cl.numel()) * s1.iterations
+    scale = num_graphs / len(sample)
+    return {"graphs": num_graphs, "n_range": [1000, int(max_n)], "vertices": nv, "entries": nnz,
+            "threshold": 1e-6, "max_iters": 200, "build_s": build_s, "batched_ms": t_batched,
+            "batched_sweeps": st.sweeps, "converged_graphs": st.converged_graphs,
+            "graph_sweeps_median": int(np.median(st.graph_iterations)), "entries_swept": st.entries_swept,
+            "batched_gteps": st.entries_swept / (t_batched * 1e6),
+            "looped_ms_est": looped_ms * scale, "looped_sample": f"{len(sample)} of {num_graphs} graphs "
+            f"(ids 0, 1 mod {sample_mod}), summed and scaled x{scale:g}",
+            "speedup_est": looped_ms * scale / t_batched}
 
 
 def vjp_vs_forward(scale, stream):
@@ -339,7 +424,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
 
     from nwgraph_b200 import Graph
-    g, deg, gen_s = make_graph(args)
+    g, deg, gen_s = make_graph(args, device=True)
     n, nnz = g.n, g.nnz
     B = graded_bytes(n, nnz)
     stream = torch.cuda.current_stream(dev)
@@ -406,6 +491,7 @@ def run_ours(args):
     del rp_h, cl_h, deg_h, out_h
     ppr = ppr_batched_vs_looped(args.ppr_scale, args.ppr_k, stream) if args.ppr_scale > 0 else None
     vjp = vjp_vs_forward(args.vjp_scale, stream) if args.vjp_scale > 0 else None
+    ragged = ragged_vs_looped(args.ragged_graphs, args.ragged_max_n, stream) if args.ragged_graphs > 0 else None
 
     peak, peak_kind = peaks()
     achieved = B / (t_sweep_ms * 1e-3) / 1e9
@@ -443,6 +529,8 @@ def run_ours(args):
         line["ppr_batched_vs_looped"] = ppr
     if vjp:
         line["vjp_vs_forward"] = vjp
+    if ragged:
+        line["ragged_batch_vs_looped"] = ragged
     if cpu:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)

@@ -110,3 +110,39 @@ def grid(n_target: int, device_out: bool = False):
     if device_out:
         return rp, cl, deg
     return CSR(rp.cpu().numpy().view(np.uint32), cl.cpu().numpy().view(np.uint32))
+
+
+def batch_from_device_csrs(parts, degrees=None):
+    """A :class:`GraphBatch` from device-built graphs ``[(row_ptr, col), ...]``
+    (int32 CUDA tensors, local ids), concatenated on the device in order.
+    Releases ``parts`` as it goes (the list is emptied). With ``degrees`` (a
+    list of per-graph degree tensors, emptied likewise) also returns their
+    concatenation."""
+    import torch
+    from .pagerank import GraphBatch
+    dev = parts[0][0].device
+    ns = np.array([int(rp.numel()) - 1 for rp, _ in parts], np.uint64)
+    ms = np.array([int(cl.numel()) for _, cl in parts], np.uint64)
+    vo = np.zeros(len(parts) + 1, np.uint64)
+    eo = np.zeros(len(parts) + 1, np.uint64)
+    vo[1:] = np.cumsum(ns)
+    eo[1:] = np.cumsum(ms)
+    rp_all = torch.empty(int(vo[-1]) + len(parts), dtype=torch.int32, device=dev)
+    cl_all = torch.empty(max(int(eo[-1]), 1), dtype=torch.int32, device=dev)
+    deg_all = torch.empty(max(int(vo[-1]), 1), dtype=torch.int32, device=dev) if degrees is not None else None
+    for g in range(len(parts)):
+        rp, cl = parts[g]
+        p0 = int(vo[g]) + g
+        rp_all[p0:p0 + rp.numel()] = rp
+        cl_all[int(eo[g]):int(eo[g + 1])] = cl
+        parts[g] = None
+        if degrees is not None:
+            deg_all[int(vo[g]):int(vo[g + 1])] = degrees[g]
+            degrees[g] = None
+    parts.clear()
+    if degrees is not None:
+        degrees.clear()
+    torch.cuda.empty_cache()  # the freed parts, for the batch's own copy
+    b = GraphBatch(vo, eo, rp_all, cl_all[: int(eo[-1])])
+    del rp_all, cl_all
+    return (b, deg_all[: int(vo[-1])]) if degrees is not None else b

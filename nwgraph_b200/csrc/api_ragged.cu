@@ -9,7 +9,10 @@
 // limited only by device memory, not by 32-bit totals. The merge-path tiles of
 // a graph never cross into the next graph, so every tile's L1 change belongs
 // to one graph and the per-graph errors are sums of tile residuals in tile
-// order. Graphs that stopped keep their ranks; their tiles issue no loads.
+// order. Graphs that stopped keep their ranks: each sweep walks a list of the
+// running graphs' tiles, rebuilt after every sweep by the convergence kernel.
+#include <cstdlib>
+#include <cstring>
 #include <new>
 #include <vector>
 
@@ -25,9 +28,10 @@ struct RaggedBatch {
   uint32_t     num_tiles = 0;
   uint64_t     device_bytes = 0;
   std::vector<RaggedGraph> h_graphs;
+  std::vector<uint32_t>    h_act;  // staging of the initial tile-list offsets
   RaggedGraph* graphs = nullptr;
   uint32_t *   row_ptr = nullptr, *col = nullptr;
-  uint32_t *   tile_graph = nullptr, *tile_row = nullptr, *tile_nnz = nullptr;
+  uint32_t *   tile_row = nullptr, *tile_nnz = nullptr;
   float *      rank = nullptr, *contrib[2] = {nullptr, nullptr};
   uint32_t*    deg = nullptr;
   float *      cpart = nullptr, *epart = nullptr, *base = nullptr;
@@ -58,9 +62,9 @@ struct RaggedBatch {
     if (stream) cudaStreamSynchronize(stream);
     if (cg_exec) cudaGraphExecDestroy(cg_exec);
     if (cg) cudaGraphDestroy(cg);
-    void* ptrs[] = {graphs,   row_ptr,  col,      tile_graph, tile_row, tile_nnz, rank,     contrib[0], contrib[1],
+    void* ptrs[] = {graphs,   row_ptr,  col,      tile_row, tile_nnz, rank,     contrib[0], contrib[1],
                     deg,      cpart,    epart,    base,       res_tile, res_part, err_hist, rs.done,    rs.iters,
-                    rs.err,   rs.conv,  st};
+                    rs.err,   rs.conv,  rs.act_off, rs.act_list, st};
     for (void* p : ptrs) pool_free(p, stream);
     if (stream) cudaStreamSynchronize(stream);
     if (h_st) cudaFreeHost(h_st);
@@ -94,12 +98,15 @@ SweepArgs ragged_args(const RaggedBatch* b, float damping) {
   a.err_cap = b->err_cap;
   a.abort_word = b->d_abort;
   a.damping = damping;
-  a.hot_ids = 0u;
+  // gathers allocate in L1 (every id counts as hot) unless NWGPU_RAGGED_GATHER=l2
+  const char* gm = getenv("NWGPU_RAGGED_GATHER");
+  a.hot_ids = (gm && !strcmp(gm, "l2")) ? 0u : 0xFFFFFFFFu;
   a.graphs = b->graphs;
-  a.tile_graph = b->tile_graph;
   a.graph_base = b->base;
-  a.graph_done = b->rs.done;
   a.res_tile = b->res_tile;
+  a.act_off = b->rs.act_off;
+  a.act_list = b->rs.act_list;
+  a.num_graphs = b->num_graphs;
   return a;
 }
 
@@ -227,11 +234,9 @@ int nwgpu_batch_create(uint64_t num_graphs, const uint64_t* vertex_offsets, cons
                      (h_err & 1u) ? " a graph's row pointers do not start at 0 or end at its nnz;" : "",
                      (h_err & 2u) ? " row pointers decrease;" : "", (h_err & 4u) ? " column id >= the graph's n;" : ""));
   // Tiles and solve buffers.
-  BK(b->alloc(&b->tile_graph, T), "cudaMalloc(tile_graph)");
   BK(b->alloc(&b->tile_row, T + G), "cudaMalloc(tile_row)");
   BK(b->alloc(&b->tile_nnz, T + G), "cudaMalloc(tile_nnz)");
-  BK(fill_ragged_tiling(b->graphs, b->num_graphs, b->row_ptr, b->num_tiles, b->tile_graph, b->tile_row, b->tile_nnz,
-                        sms, b->stream),
+  BK(fill_ragged_tiling(b->graphs, b->num_graphs, b->row_ptr, b->num_tiles, b->tile_row, b->tile_nnz, sms, b->stream),
      "ragged tiling");
   BK(b->alloc(&b->rank, nv), "cudaMalloc(rank)");
   BK(b->alloc(&b->contrib[0], nv), "cudaMalloc(contrib)");
@@ -245,6 +250,8 @@ int nwgpu_batch_create(uint64_t num_graphs, const uint64_t* vertex_offsets, cons
   BK(b->alloc(&b->rs.iters, G), "cudaMalloc(graph state)");
   BK(b->alloc(&b->rs.err, G), "cudaMalloc(graph state)");
   BK(b->alloc(&b->rs.conv, G), "cudaMalloc(graph state)");
+  BK(b->alloc(&b->rs.act_off, G + 1), "cudaMalloc(graph state)");
+  BK(b->alloc(&b->rs.act_list, T), "cudaMalloc(tile list)");
   BK(b->alloc(&b->err_hist, b->err_cap), "cudaMalloc(err_hist)");
   BK(b->alloc(&b->st, 1), "cudaMalloc(state)");
   // Grids: 4 resident 256-thread CTAs per SM for the sweep; the converge
@@ -297,8 +304,14 @@ int nwgpu_pr_ragged(nwgpu_batch* b, const uint32_t* out_degree, float* ranks, fl
   h.done = (max_iters == 0) ? 1u : 0u;
   *b->h_st = h;
   CK(cudaMemcpyAsync(b->st, b->h_st, sizeof(PrState), cudaMemcpyHostToDevice, s), "copy state");
+  // every graph starts running: the tile list is all tiles
+  b->h_act.resize(G + 1);
+  for (uint64_t g = 0; g <= G; ++g) b->h_act[g] = g < G ? b->h_graphs[g].tile0 : b->num_tiles;
+  CK(cudaMemcpyAsync(b->rs.act_off, b->h_act.data(), (G + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, s),
+     "copy tile list");
   const SweepArgs a = ragged_args(b, damping);
   CK(launch_ragged_init(a, b->rs, b->num_graphs, nv, damping, h.done, b->sms, s), "ragged init");
+  CK(launch_ragged_list(a, b->rs, b->sms, s), "ragged tile list");
   CK(cudaEventRecord(b->ev0, s), "cudaEventRecord");
   if (opt.launch == NWGPU_LAUNCH_GRAPH) {
     if (!b->cg_exec || b->cg_damping != damping) {

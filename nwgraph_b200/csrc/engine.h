@@ -117,18 +117,25 @@ struct SweepArgs {
   const float*                 vaux;       // per-row factor (weighted: out-weight sum; adjoint: d / out-weight sum)
   // Ragged batches only (the RAGGED sweep variant):
   const RaggedGraph*           graphs;
-  const uint32_t*              tile_graph;  // graph of each tile
   const float*                 graph_base;  // per graph: (1 - d) / n
-  const uint32_t*              graph_done;  // per graph: nonzero once it stopped; its tiles are skipped
   double*                      res_tile;    // per tile: FP64 L1 change of the rows the tile completes
+  // Tiles of the running graphs: running graph g's tiles are entries
+  // [act_off[g], act_off[g + 1]) of the sweep's tile list act_list, as
+  // (tile, graph) pairs (act_off[num_graphs] = their count); stopped graphs
+  // have none.
+  const uint32_t*              act_off;
+  const uint2*                 act_list;
+  uint32_t                     num_graphs;
 };
 
 // Per-graph results of a ragged solve, written by the convergence kernel.
 struct RaggedState {
-  uint32_t* done;   // stopped (converged, at max_iters, aborted or failed)
-  uint32_t* iters;  // sweeps run
-  double*   err;    // L1 change of the last sweep
-  uint32_t* conv;   // err < threshold
+  uint32_t* done;     // stopped (converged, at max_iters, aborted or failed)
+  uint32_t* iters;    // sweeps run
+  double*   err;      // L1 change of the last sweep
+  uint32_t* conv;     // err < threshold
+  uint32_t* act_off;  // num_graphs + 1: running graphs' tile-list offsets (SweepArgs::act_off)
+  uint2*    act_list; // the tile list (SweepArgs::act_list)
 };
 
 // devmem.cu: the per-device stream-ordered pool that every handle allocation uses
@@ -215,15 +222,16 @@ cudaError_t launch_ragged_sweep(const SweepArgs& a, int sweep_grid, int finish_g
                                 const RaggedState& rs, int conv_grid, cudaStream_t s);
 cudaError_t add_ragged_nodes(cudaGraph_t body, const SweepArgs& a, int sweep_grid, int finish_grid, uint32_t num_graphs,
                              const RaggedState& rs, int conv_grid);
+// The running graphs' (tile, graph) list from act_off and the done flags
+cudaError_t launch_ragged_list(const SweepArgs& a, const RaggedState& rs, int sms, cudaStream_t s);
 // rank = 1/n_g, contrib = rank / deg over the batch's vertices; per-graph base
 // terms and state reset
 cudaError_t launch_ragged_init(const SweepArgs& a, const RaggedState& rs, uint32_t num_graphs, uint64_t num_vertices,
                                float damping, uint32_t stopped, int sms, cudaStream_t s);
 // graph_build.cu: merge-path coordinates of every graph's tiles (num_tiles +
-// num_graphs entries) and the graph of each tile
+// num_graphs entries)
 cudaError_t fill_ragged_tiling(const RaggedGraph* graphs, uint32_t num_graphs, const uint32_t* row_ptr,
-                               uint32_t num_tiles, uint32_t* tile_graph, uint32_t* tile_row, uint32_t* tile_nnz,
-                               int sms, cudaStream_t s);
+                               uint32_t num_tiles, uint32_t* tile_row, uint32_t* tile_nnz, int sms, cudaStream_t s);
 // Checks every graph's row pointers (first 0, last nnz, non-decreasing) and
 // column ids (< n); sets the bits validate_csr sets.
 cudaError_t validate_ragged(const RaggedGraph* graphs, uint32_t num_graphs, const uint32_t* row_ptr, const uint32_t* col,

@@ -113,8 +113,7 @@ __device__ __forceinline__ uint32_t last_graph_at_or_below(uint32_t num_graphs, 
 // tile0 + g + tiles + 1 (each graph has its tiles plus one end entry).
 __global__ void ragged_tiling_kernel(const RaggedGraph* __restrict__ graphs, uint32_t num_graphs,
                                      const uint32_t* __restrict__ row_ptr, uint32_t D, uint64_t entries,
-                                     uint32_t* __restrict__ tile_graph, uint32_t* __restrict__ tile_row,
-                                     uint32_t* __restrict__ tile_nnz) {
+                                     uint32_t* __restrict__ tile_row, uint32_t* __restrict__ tile_nnz) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < entries; e += stride) {
     const uint32_t g = last_graph_at_or_below(num_graphs, e, [&](uint32_t x) { return (uint64_t)graphs[x].tile0 + x; });
@@ -125,16 +124,14 @@ __global__ void ragged_tiling_kernel(const RaggedGraph* __restrict__ graphs, uin
     const uint32_t    i = merge_path_row(row_ptr + R.p0, R.n, R.nnz, d);
     tile_row[e] = i;
     tile_nnz[e] = (uint32_t)(d - i);
-    if (j < R.tiles) tile_graph[R.tile0 + j] = g;
   }
 }
 
 cudaError_t fill_ragged_tiling(const RaggedGraph* graphs, uint32_t num_graphs, const uint32_t* row_ptr,
-                               uint32_t num_tiles, uint32_t* tile_graph, uint32_t* tile_row, uint32_t* tile_nnz,
-                               int sms, cudaStream_t s) {
+                               uint32_t num_tiles, uint32_t* tile_row, uint32_t* tile_nnz, int sms, cudaStream_t s) {
   if (!num_graphs) return cudaSuccess;
   ragged_tiling_kernel<<<sms * 8, 256, 0, s>>>(graphs, num_graphs, row_ptr, kRaggedTileItems,
-                                                (uint64_t)num_tiles + num_graphs, tile_graph, tile_row, tile_nnz);
+                                                (uint64_t)num_tiles + num_graphs, tile_row, tile_nnz);
   return cudaGetLastError();
 }
 

@@ -77,7 +77,7 @@ struct TileMeta {
   uint32_t rk_at;           // stage word holding rank[r0], or ~0u when rank/deg are not staged
   uint32_t dg_at;           // stage word holding deg[r0]
   float    base;            // ragged batches: the tile's graph's base term
-  uint32_t pad_;
+  uint32_t tile;            // ragged batches: the tile (the sweep walks the running graphs' tile list)
   uint64_t v0;              // ragged batches: the tile's graph's first vertex
 };
 
@@ -109,28 +109,19 @@ __device__ __forceinline__ float base_of(const SweepArgs& a, uint32_t r) {
   return a.base;
 }
 
-// Thread 0, ragged batches: tile t of graph g in local coordinates; the
-// slices start at the graph's 64-bit bases and are rounded out to 16 bytes
-// of the batch arrays. A stopped graph's tiles get an empty meta (no rows, no
-// entries) and arrive with no bytes.
+// Thread 0, ragged batches: entry i of the running graphs' tile list, tile t
+// of graph g, in local coordinates; the slices start at the graph's 64-bit
+// bases and are rounded out to 16 bytes of the batch arrays.
 template <int NT, int IPT>
-__device__ __forceinline__ void issue_ragged_tile(const SweepArgs& a, uint32_t t, uint32_t* stg, TileMeta* m,
+__device__ __forceinline__ void issue_ragged_tile(const SweepArgs& a, uint32_t i, uint32_t* stg, TileMeta* m,
                                                   uint64_t* bar, uint64_t pol) {
   constexpr int  RV = SweepSmem<NT, IPT>::RV;
-  const uint32_t g = a.tile_graph[t];
+  const uint2    tg = __ldcg(a.act_list + i);
+  const uint32_t t = tg.x, g = tg.y;
   const RaggedGraph* G = a.graphs + g;
   m->base = a.graph_base[g];
   m->v0 = G->v0;
-  if (*(const volatile uint32_t*)(a.graph_done + g)) {
-    m->r0 = m->r1 = 0u;
-    m->k0 = m->k1 = 0u;
-    m->col_at = 0u;
-    m->rp_at = 0u;
-    m->rk_at = ~0u;
-    m->dg_at = 0u;
-    mbar_arrive_expect_tx(bar, 0u);
-    return;
-  }
+  m->tile = t;
   const uint32_t e = t + g;
   const uint32_t r0 = a.tile_row[e], r1 = a.tile_row[e + 1], k0 = a.tile_nnz[e], k1 = a.tile_nnz[e + 1];
   const uint64_t K0 = G->e0 + k0, P0 = G->p0 + r0, V0 = G->v0 + r0;
@@ -248,7 +239,8 @@ template <int NT, int IPT, bool RAGGED>
 __device__ __forceinline__ double reduce_tile(const SweepArgs& a, SweepSmem<NT, IPT>& S, int s, uint32_t t,
                                               const float (&v)[IPT], float* __restrict__ cout, uint64_t pol_keep) {
   const TileMeta  m = S.meta[s];
-  // ragged batches: the tile's rows are local ids of its graph
+  // ragged batches: t is the tile list entry; the tile's rows are local ids of its graph
+  if (RAGGED) t = m.tile;
   float* const    rank = RAGGED ? a.rank + m.v0 : a.rank;
   const uint32_t* degv = RAGGED ? a.deg + m.v0 : a.deg;
   if (RAGGED) cout += m.v0;
@@ -414,7 +406,8 @@ __global__ void __launch_bounds__(NT, HOT ? 1 : 4) pr_sweep_kernel(const SweepAr
   float* __restrict__ cout = (it & 1ull) ? a.contrib0 : a.contrib1;
   const uint64_t pol_keep = policy_evict_last();
   const uint64_t pol_stream = policy_evict_first();
-  const uint32_t G = gridDim.x, T = a.num_tiles;
+  // ragged batches walk the running graphs' tile list
+  const uint32_t G = gridDim.x, T = RAGGED ? *(const volatile uint32_t*)(a.act_off + a.num_graphs) : a.num_tiles;
   double         res = 0.0;
   int            ok = 1;
 
@@ -462,7 +455,7 @@ __global__ void __launch_bounds__(NT, HOT ? 1 : 4) pr_sweep_kernel(const SweepAr
       }
       res += tile_residual<NT, IPT, RAGGED>(S, reduce_tile<NT, IPT, RAGGED>(a, S, 0, t, v0, cout, pol_keep));
       ok = __syncthreads_and(ok);
-      if (RAGGED && tid == 0) store_tile_residual<NT, IPT>(a, S, t);
+      if (RAGGED && tid == 0) store_tile_residual<NT, IPT>(a, S, S.meta[0].tile);
       if (ok && tid == 0 && t + 2 * G < T)
         issue_any<NT, IPT, RAGGED>(a, t + 2 * G, S.stage[0], &S.meta[0], &S.bar[0], pol_stream);
       t = tn;
@@ -477,7 +470,7 @@ __global__ void __launch_bounds__(NT, HOT ? 1 : 4) pr_sweep_kernel(const SweepAr
       }
       res += tile_residual<NT, IPT, RAGGED>(S, reduce_tile<NT, IPT, RAGGED>(a, S, 1, t, v1, cout, pol_keep));
       ok = __syncthreads_and(ok);
-      if (RAGGED && tid == 0) store_tile_residual<NT, IPT>(a, S, t);
+      if (RAGGED && tid == 0) store_tile_residual<NT, IPT>(a, S, S.meta[1].tile);
       if (ok && tid == 0 && t + 2 * G < T)
         issue_any<NT, IPT, RAGGED>(a, t + 2 * G, S.stage[1], &S.meta[1], &S.bar[1], pol_stream);
       t = tn;
@@ -596,31 +589,33 @@ __global__ void __launch_bounds__(256) pr_finish_kernel(const SweepArgs a) {
 // ---------------------------------------------------------------------------
 // Ragged batches: rows crossing tiles, per-graph convergence, set-up
 // ---------------------------------------------------------------------------
-// Thread ta completes the row carried out of tile ta when that row starts
-// there (local merge-path coordinates of the tile's graph; rows never cross
-// graphs) and adds its L1 change to res_tile[ta]. Spans of more than 8 tiles
-// are summed by the whole warp.
+// Thread i takes entry i of the running graphs' tile list, tile ta, and
+// completes the row carried out of ta when that row starts there (local
+// merge-path coordinates of the tile's graph; rows never cross graphs),
+// adding its L1 change to res_tile[ta]. Spans of more than 8 tiles are summed
+// by the whole warp.
 __global__ void __launch_bounds__(256) pr_ragged_finish_kernel(const SweepArgs a) {
   if (*(volatile unsigned int*)&a.st->done) return;
   const unsigned long long it = *(volatile unsigned long long*)&a.st->iter;
   float* __restrict__ cout = (it & 1ull) ? a.contrib0 : a.contrib1;
   const uint64_t pol = policy_evict_last();
-  const uint32_t D = a.tile_items, T = a.num_tiles;
+  const uint32_t D = a.tile_items;
   const int      lane = threadIdx.x & 31;
-  const uint32_t ta = blockIdx.x * blockDim.x + threadIdx.x;
-  uint32_t       S = 0, tb = 0, g = 0;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;  // entry of the running graphs' tile list
+  const uint32_t L = *(const volatile uint32_t*)(a.act_off + a.num_graphs);
+  uint32_t       S = 0, ta = 0, tb = 0, g = 0;
   bool           mine = false;
-  if (ta < T) {
-    g = a.tile_graph[ta];
-    if (!*(const volatile uint32_t*)(a.graph_done + g)) {
-      const RaggedGraph& G = a.graphs[g];
-      const uint32_t*    rp = a.row_ptr + G.p0;
-      S = a.tile_row[ta + g + 1];  // the tile's end; S = n at the graph's last tile
-      const uint32_t k1 = a.tile_nnz[ta + g + 1], rs = rp[S];
-      if (k1 > rs && ((uint64_t)S + rs) / D == ta - G.tile0) {
-        mine = true;
-        tb = G.tile0 + (uint32_t)(((uint64_t)S + rp[S + 1]) / D);
-      }
+  if (i < L) {
+    const uint2 tg = __ldcg(a.act_list + i);
+    ta = tg.x;
+    g = tg.y;
+    const RaggedGraph& G = a.graphs[g];
+    const uint32_t*    rp = a.row_ptr + G.p0;
+    S = a.tile_row[ta + g + 1];  // the tile's end; S = n at the graph's last tile
+    const uint32_t k1 = a.tile_nnz[ta + g + 1], rs = rp[S];
+    if (k1 > rs && ((uint64_t)S + rs) / D == ta - G.tile0) {
+      mine = true;
+      tb = G.tile0 + (uint32_t)(((uint64_t)S + rp[S + 1]) / D);
     }
   }
   const bool longspan = mine && (tb - ta > 8u);
@@ -653,8 +648,9 @@ __global__ void __launch_bounds__(256) pr_ragged_finish_kernel(const SweepArgs a
 // One warp per running graph: its sweep error is the sum of its tiles'
 // residuals in tile order (lane-strided FP64 partials, then a fixed shuffle
 // tree); the graph stops on err < threshold, at max_iters, or when the solve
-// is aborted or failed. The last CTA advances the sweep count, records the
-// summed error of the sweep and ends the loop once no graph is running.
+// is aborted or failed. The last CTA rebuilds the running graphs' tile list
+// offsets for the next sweep, advances the sweep count, records the summed
+// error of the sweep and ends the loop once no graph is running.
 __global__ void __launch_bounds__(256) pr_ragged_converge_kernel(const SweepArgs a, uint32_t num_graphs,
                                                                  RaggedState rs) {
   __shared__ double   s_err[8];
@@ -707,8 +703,33 @@ __global__ void __launch_bounds__(256) pr_ragged_converge_kernel(const SweepArgs
     s_last = (prev == gridDim.x - 1);
   }
   __syncthreads();
-  if (!s_last || tid >= 32) return;
+  if (!s_last) return;
   __threadfence();
+  {
+    // act_off = exclusive scan over the graphs of (running ? tiles : 0):
+    // thread tid owns graphs [tid * per, tid * per + per)
+    __shared__ uint32_t s_wsum[8];
+    const uint32_t      per = (num_graphs + blockDim.x - 1) / blockDim.x;
+    const uint32_t      g0 = tid * per, g1 = min(num_graphs, g0 + per);
+    uint32_t            mine = 0;
+    for (uint32_t g = g0; g < g1; ++g) mine += *(volatile uint32_t*)(rs.done + g) ? 0u : a.graphs[g].tiles;
+    uint32_t incl = mine;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(kFullMask, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_wsum[warp] = incl;
+    __syncthreads();
+    uint32_t before = 0;
+    for (int w = 0; w < warp; ++w) before += s_wsum[w];
+    uint32_t off = before + incl - mine;
+    for (uint32_t g = g0; g < g1; ++g) {
+      rs.act_off[g] = off;
+      off += *(volatile uint32_t*)(rs.done + g) ? 0u : a.graphs[g].tiles;
+    }
+    if (tid == blockDim.x - 1) rs.act_off[num_graphs] = before + incl;
+  }
+  if (tid >= 32) return;
   double e = 0.0;
   for (uint32_t u = lane; u < gridDim.x; u += 32) e += __ldcg(a.res_part + u);
   e = warp_sum_lane0(e);
@@ -726,6 +747,18 @@ __global__ void __launch_bounds__(256) pr_ragged_converge_kernel(const SweepArgs
     st->ticket = 0u;
     __threadfence();
     if (a.use_cond && !done && done_iters < st->chunk_end) cudaGraphSetConditional(a.cond, 1u);
+  }
+}
+
+// One warp per running graph writes its entries of the tile list.
+__global__ void ragged_list_kernel(const RaggedGraph* __restrict__ graphs, uint32_t num_graphs,
+                                   const uint32_t* __restrict__ done, const uint32_t* __restrict__ act_off,
+                                   uint2* __restrict__ list) {
+  const uint32_t lane = threadIdx.x & 31, nwarps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < num_graphs; g += nwarps) {
+    if (done[g]) continue;
+    const uint32_t t0 = graphs[g].tile0, nt = graphs[g].tiles, o = act_off[g];
+    for (uint32_t j = lane; j < nt; j += 32) list[o + j] = make_uint2(t0 + j, g);
   }
 }
 
@@ -939,6 +972,15 @@ cudaError_t add_pr_sweep_nodes(cudaGraph_t body, const SweepArgs& a, const Sweep
 static void* ragged_sweep_fn() { return (void*)pr_sweep_kernel<256, 8, false, true>; }
 static size_t ragged_sweep_smem() { return sizeof(SweepSmem<256, 8>); }
 
+static int ragged_list_grid(uint32_t num_graphs) { return (int)((num_graphs + 7) / 8 < 4096 ? (num_graphs + 7) / 8 : 4096); }
+
+cudaError_t launch_ragged_list(const SweepArgs& a, const RaggedState& rs, int sms, cudaStream_t s) {
+  (void)sms;
+  ragged_list_kernel<<<ragged_list_grid(a.num_graphs), 256, 0, s>>>(a.graphs, a.num_graphs, rs.done, rs.act_off,
+                                                                     rs.act_list);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_ragged_sweep(const SweepArgs& a, int sweep_grid, int finish_grid, uint32_t num_graphs,
                                 const RaggedState& rs, int conv_grid, cudaStream_t s) {
   void*       args[] = {(void*)&a};
@@ -946,6 +988,8 @@ cudaError_t launch_ragged_sweep(const SweepArgs& a, int sweep_grid, int finish_g
   if (e != cudaSuccess) return e;
   pr_ragged_finish_kernel<<<finish_grid, 256, 0, s>>>(a);
   pr_ragged_converge_kernel<<<conv_grid, 256, 0, s>>>(a, num_graphs, rs);
+  ragged_list_kernel<<<ragged_list_grid(num_graphs), 256, 0, s>>>(a.graphs, num_graphs, rs.done, rs.act_off,
+                                                                   rs.act_list);
   return cudaGetLastError();
 }
 
@@ -976,7 +1020,20 @@ cudaError_t add_ragged_nodes(cudaGraph_t body, const SweepArgs& a, int sweep_gri
   cp.gridDim = dim3((unsigned)conv_grid);
   cp.blockDim = dim3(256);
   cp.kernelParams = cargs;
-  return cudaGraphAddKernelNode(&conv_node, body, &finish_node, 1, &cp);
+  e = cudaGraphAddKernelNode(&conv_node, body, &finish_node, 1, &cp);
+  if (e != cudaSuccess) return e;
+  const RaggedGraph*   gr = a.graphs;
+  const uint32_t*      dn = rs.done;
+  const uint32_t*      ao = rs.act_off;
+  uint2*               al = rs.act_list;
+  void*                largs[] = {(void*)&gr, (void*)&ng, (void*)&dn, (void*)&ao, (void*)&al};
+  cudaKernelNodeParams lp = {};
+  lp.func = (void*)ragged_list_kernel;
+  lp.gridDim = dim3((unsigned)ragged_list_grid(num_graphs));
+  lp.blockDim = dim3(256);
+  lp.kernelParams = largs;
+  cudaGraphNode_t list_node;
+  return cudaGraphAddKernelNode(&list_node, body, &conv_node, 1, &lp);
 }
 
 cudaError_t launch_ragged_init(const SweepArgs& a, const RaggedState& rs, uint32_t num_graphs, uint64_t num_vertices,
