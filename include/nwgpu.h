@@ -63,6 +63,10 @@ typedef struct nwgpu_graph nwgpu_graph;
 #define NWGPU_GRAPH_DEVICE_PTRS 0x1u /* row_ptr / col / weights are device pointers (copied device-to-device) */
 #define NWGPU_GRAPH_TRANSPOSE 0x2u   /* build the out-row CSR (adjacency<0>) of nwgpu_pr_vjp at creation, not on first use */
 #define NWGPU_GRAPH_NO_RELABEL 0x4u  /* keep the input vertex order on the device (default: hubs first) */
+#define NWGPU_GRAPH_AUTOTUNE 0x8u    /* pick the sweep's launch shape and hub tiers by timing a few sweeps of
+                                        each candidate (or reuse the choice cached for graphs of the same
+                                        signature; NWGPU_TUNE_CACHE=<file> keeps the cache across processes).
+                                        Every choice gives bitwise-equal ranks. Also set by NWGPU_AUTOTUNE=1 */
 
 /* Upload a CSR once (replaces the per-call use of graph.indices_ /
  * to_be_indexed_ at page_rank.hpp:129). Validates it on the device
@@ -85,6 +89,13 @@ typedef struct nwgpu_graph_info {
   uint64_t device_bytes; /* HBM held by the handle */
   int32_t  device;
   int32_t  has_weights, has_transpose;
+  int32_t  binned;         /* 1: the degree-binned sweep (relabelled graphs); 0: merge-path tiles */
+  uint32_t sweep_threads;  /* threads per CTA of the sweep */
+  uint32_t sweep_grid;     /* CTAs of the sweep */
+  uint32_t hub_smem_ids;   /* binned: contributions [0, hub_smem_ids) staged in shared memory each sweep */
+  uint32_t hub_l1_ids;     /* binned: ids [hub_smem_ids, hub_l1_ids) gathered through L1 */
+  int32_t  tuned;          /* 0 defaults, 1 timed at creation, 2 taken from the tuning cache */
+  float    tuned_us_per_sweep;
 } nwgpu_graph_info;
 int nwgpu_graph_get_info(const nwgpu_graph* g, nwgpu_graph_info* info);
 

@@ -24,6 +24,7 @@ ERR_UNSUPPORTED = 7
 GRAPH_DEVICE_PTRS = 0x1
 GRAPH_TRANSPOSE = 0x2
 GRAPH_NO_RELABEL = 0x4
+GRAPH_AUTOTUNE = 0x8
 NOALLOC_MAX_VERTICES = 1048576
 NOALLOC_MAX_ENTRIES = 33554432
 
@@ -47,7 +48,9 @@ class NwgpuError(RuntimeError):
 class GraphInfo(C.Structure):
     _fields_ = [("n", C.c_uint64), ("nnz", C.c_uint64), ("num_tiles", C.c_uint64), ("tile_items", C.c_uint32),
                 ("grid", C.c_uint32), ("device_bytes", C.c_uint64), ("device", C.c_int32),
-                ("has_weights", C.c_int32), ("has_transpose", C.c_int32)]
+                ("has_weights", C.c_int32), ("has_transpose", C.c_int32), ("binned", C.c_int32),
+                ("sweep_threads", C.c_uint32), ("sweep_grid", C.c_uint32), ("hub_smem_ids", C.c_uint32),
+                ("hub_l1_ids", C.c_uint32), ("tuned", C.c_int32), ("tuned_us_per_sweep", C.c_float)]
 
 
 class PrOptions(C.Structure):

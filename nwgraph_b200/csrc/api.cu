@@ -605,6 +605,16 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
     if (rc) return bail(rc);
   }
   trace.mark("bins");
+  {
+    // explicit launch settings in the environment take precedence over tuning
+    const char* tune = getenv("NWGPU_AUTOTUNE");
+    const bool  want_tune = (flags & NWGPU_GRAPH_AUTOTUNE) || (tune && !strcmp(tune, "1"));
+    if (want_tune && g->plan.ok && !which && !getenv("NWGPU_HOT_IDS") && !getenv("NWGPU_HOT_L1_IDS")) {
+      rc = autotune_binned(g);
+      if (rc) return bail(rc);
+      trace.mark("autotune");
+    }
+  }
   if ((flags & NWGPU_GRAPH_TRANSPOSE) && weights && g->plan.ok) {
     rc = ensure_wpr(g);
     if (rc) return bail(rc);
@@ -635,7 +645,19 @@ int nwgpu_graph_get_info(const nwgpu_graph* g, nwgpu_graph_info* info) {
   info->device_bytes = g->device_bytes;
   info->device = g->device;
   info->has_weights = g->g.w != nullptr;
-  info->has_transpose = 0;
+  info->has_transpose = g->wpr.ready ? 1 : 0;
+  info->binned = g->plan.ok ? 1 : 0;
+  if (g->plan.ok) {
+    info->sweep_threads = g->plan.hot ? kBinnedHotThreads : kBinnedThreads;
+    info->sweep_grid = (uint32_t)g->plan.sweep_grid;
+    info->hub_smem_ids = g->plan.bin.smem_ids;
+    info->hub_l1_ids = g->plan.bin.l1_ids;
+  } else {
+    info->sweep_threads = (uint32_t)g->variant.threads;
+    info->sweep_grid = (uint32_t)g->grid;
+  }
+  info->tuned = g->tuned;
+  info->tuned_us_per_sweep = g->tune_us;
   return NWGPU_OK;
 }
 

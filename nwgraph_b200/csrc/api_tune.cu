@@ -1,0 +1,201 @@
+// Autotuner of the degree-binned sweep's launch parameters.
+//
+// No counterpart in the reference (its page_rank has no tunables beyond the
+// TBB grain). The binned sweep's runtime knobs are the launch shape (one
+// 1024-thread CTA per SM with the hub contributions staged in shared memory,
+// or four 256-thread CTAs per SM with the hubs in L1), how many hub
+// contributions the hot shape stages, and how many more ids go through L1
+// with an evict-last policy. Every choice gives bitwise-equal ranks (the
+// summation order does not depend on where a contribution is read from), so
+// the tuner only times: a few sweeps of each candidate on the resident graph
+// with unit degrees, and keeps the fastest.
+//
+// Choices are cached per graph signature -- the SM count, log2 of the vertex
+// count in half steps, the average degree, and the share of entries in
+// chunked long rows and in warp-per-row rows (5% steps) -- in the process and,
+// when NWGPU_TUNE_CACHE names a file, in that file (one line per signature),
+// so a graph like one already tuned reuses its choice without timing.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "handle.h"
+
+namespace nwgpu {
+namespace {
+
+struct Choice {
+  int      hot = 1;
+  uint32_t smem_ids = 0, l1_ids = 0;
+  float    us = 0.f;  // measured time per sweep
+};
+
+std::mutex                    g_mu;
+std::map<std::string, Choice> g_cache;
+bool                          g_loaded = false;
+
+const char* cache_path() {
+  const char* p = getenv("NWGPU_TUNE_CACHE");
+  return (p && *p) ? p : nullptr;
+}
+
+void load_locked() {
+  if (g_loaded) return;
+  g_loaded = true;
+  const char* path = cache_path();
+  if (!path) return;
+  FILE* f = fopen(path, "r");
+  if (!f) return;
+  char line[512];
+  while (fgets(line, sizeof line, f)) {
+    char*  tab = strchr(line, '\t');
+    Choice c;
+    if (!tab) continue;
+    *tab = 0;
+    if (sscanf(tab + 1, "%d %u %u %f", &c.hot, &c.smem_ids, &c.l1_ids, &c.us) == 4) g_cache[line] = c;
+  }
+  fclose(f);
+}
+
+void store_locked(const std::string& sig, const Choice& c) {
+  g_cache[sig] = c;
+  const char* path = cache_path();
+  if (!path) return;
+  FILE* f = fopen(path, "a");
+  if (!f) return;
+  fprintf(f, "%s\t%d %u %u %.2f\n", sig.c_str(), c.hot, c.smem_ids, c.l1_ids, c.us);
+  fclose(f);
+}
+
+__global__ void fill_u32_kernel(uint32_t* __restrict__ p, uint64_t n, uint32_t v) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) p[i] = v;
+}
+
+int signature(nwgpu_graph* g, std::string* out) {
+  const BinnedArgs& b = g->plan.bin;
+  uint32_t          at[2] = {0, 0};  // row_ptr at the end of the long rows and of bin 0
+  CK(cudaMemcpyAsync(&at[0], g->g.row_ptr + b.num_long_rows, sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream),
+     "signature");
+  CK(cudaMemcpyAsync(&at[1], g->g.row_ptr + b.bin_row_end[0], sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream),
+     "signature");
+  CK(cudaStreamSynchronize(g->stream), "signature");
+  const double nnz = g->nnz ? (double)g->nnz : 1.0;
+  const double n = g->n ? (double)g->n : 1.0;
+  auto         pct5 = [&](double x) { return (int)(std::lround(20.0 * x / nnz) * 5); };
+  char         buf[160];
+  snprintf(buf, sizeof buf, "binned sms=%d log2n=%.1f deg=%ld long=%d%% warp=%d%%", g->sms,
+           std::round(2.0 * std::log2(n)) / 2.0, std::lround(nnz / n), pct5(at[0]), pct5((double)at[1] - at[0]));
+  *out = buf;
+  return NWGPU_OK;
+}
+
+void apply(nwgpu_graph* g, const Choice& c) {
+  BinPlan& p = g->plan;
+  p.hot = c.hot != 0;
+  p.bin.smem_ids = c.smem_ids;
+  p.bin.l1_ids = c.l1_ids;
+  p.sweep_grid = binned_sweep_grid(g->sms, p.hot);
+}
+
+// Microseconds per sweep of the plan's current settings (after one warm sweep).
+int time_plan(nwgpu_graph* g, const SweepArgs& a, int sweeps, float* us) {
+  const BinPlan&   p = g->plan;
+  const BinnedArgs ba = make_binned_args(g, p, a, kModePlain);
+  CK(launch_binned_sweep(ba, p.hot, kModePlain, p.sweep_grid, p.finish_grid, g->stream), "tune sweep");
+  CK(cudaEventRecord(g->ev0, g->stream), "cudaEventRecord");
+  for (int i = 0; i < sweeps; ++i)
+    CK(launch_binned_sweep(ba, p.hot, kModePlain, p.sweep_grid, p.finish_grid, g->stream), "tune sweep");
+  CK(cudaEventRecord(g->ev1, g->stream), "cudaEventRecord");
+  CK(cudaEventSynchronize(g->ev1), "tune sweep");
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, g->ev0, g->ev1), "cudaEventElapsedTime");
+  *us = 1e3f * ms / (float)sweeps;
+  return NWGPU_OK;
+}
+
+}  // namespace
+
+int autotune_binned(nwgpu_graph* g) {
+  if (!g->plan.ok || g->n == 0) return NWGPU_OK;
+  std::string sig;
+  int         rc = signature(g, &sig);
+  if (rc) return rc;
+  const uint32_t lim = binned_hot_capacity();
+  const uint32_t n = (uint32_t)g->n;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    load_locked();
+    auto it = g_cache.find(sig);
+    if (it != g_cache.end()) {
+      Choice c = it->second;
+      if (c.smem_ids > lim) c.smem_ids = lim;
+      if (c.smem_ids > n) c.smem_ids = n & ~3u;
+      if (c.l1_ids < c.smem_ids) c.l1_ids = c.smem_ids;
+      apply(g, c);
+      g->tuned = 2;
+      g->tune_us = c.us;
+      return NWGPU_OK;
+    }
+  }
+  // Candidates: the hot shape with 16K / 32K / 48K staged ids (as the shared
+  // memory allows) and an L1 tier of 0 / 16K / 32K more; the 256-thread shape
+  // with 16K / 32K / 64K ids through L1.
+  std::vector<Choice> cands;
+  for (uint32_t s : {16384u, 32768u, 49152u}) {
+    uint32_t st = s < lim ? s : lim;
+    if (st > n) st = n & ~3u;
+    for (uint32_t l1 : {0u, 16384u, 32768u}) {
+      Choice c;
+      c.hot = 1;
+      c.smem_ids = st;
+      c.l1_ids = st + l1;
+      bool dup = false;
+      for (const Choice& d : cands) dup |= d.hot == 1 && d.smem_ids == c.smem_ids && d.l1_ids == c.l1_ids;
+      if (!dup) cands.push_back(c);
+    }
+  }
+  for (uint32_t l1 : {16384u, 32768u, 65536u}) {
+    Choice c;
+    c.hot = 0;
+    c.l1_ids = l1;
+    cands.push_back(c);
+  }
+  // Timing state: unit degrees, uniform start, a sweep limit never reached,
+  // threshold 0 (never converged).
+  rc = ensure_solve_buffers(g);
+  if (rc) return rc;
+  fill_u32_kernel<<<g->sms * 4, 256, 0, g->stream>>>(g->deg, g->n, 1u);
+  CK(cudaGetLastError(), "tune degrees");
+  PrState h = {};
+  h.max_iters = ~0ull;
+  h.chunk_end = ~0ull;
+  h.threshold = 0.0;
+  *g->h_st = h;
+  CK(cudaMemcpyAsync(g->st, g->h_st, sizeof(PrState), cudaMemcpyHostToDevice, g->stream), "tune state");
+  const float     base = (float)(0.15 / (double)g->n);
+  const SweepArgs a = make_sweep_args(g, 0.85f, base, kTeleportUniform, 0u);
+  CK(launch_pr_init(a, g->n, (float)(1.0 / (double)g->n), g->sms, g->stream), "tune init");
+  const int sweeps = g->nnz > (1u << 26) ? 3 : 8;
+  Choice    best;
+  best.us = 3.4e38f;
+  for (Choice c : cands) {
+    apply(g, c);
+    float us = 0.f;
+    if ((rc = time_plan(g, a, sweeps, &us))) return rc;
+    c.us = us;
+    if (us < best.us) best = c;
+  }
+  apply(g, best);
+  g->tuned = 1;
+  g->tune_us = best.us;
+  std::lock_guard<std::mutex> lk(g_mu);
+  store_locked(sig, best);
+  return NWGPU_OK;
+}
+
+}  // namespace nwgpu

@@ -104,6 +104,8 @@ struct nwgpu_graph {
   int          grid = 0;         // persistent sweep CTAs
   uint32_t     hot_ids = 0;      // internal ids below this are gathered from shared memory / L1
   nwgpu::SweepVariant variant{256, 8, false};
+  int          tuned = 0;        // binned launch parameters: 0 defaults, 1 timed at creation, 2 from the tuning cache
+  float        tune_us = 0.f;    // the chosen parameters' time per sweep when tuned
   // Degree-binned sweep (relabelled graphs with non-increasing row lengths).
   nwgpu::BinPlan plan;
   int          finish_grid = 1;  // finishing-kernel CTAs
@@ -180,6 +182,9 @@ int run_sweeps(nwgpu_graph* g, const SweepArgs& a, uint32_t launch, uint64_t max
 nwgpu_pr_options read_options(const nwgpu_pr_options* options);
 // Out-row CSR, its bins and the buffers of the weighted solve and its adjoint.
 int ensure_wpr(nwgpu_graph* g);
+// api_tune.cu: picks the binned sweep's launch shape and hub tiers for g
+// (timed, or from the per-signature cache) and sets g->plan accordingly.
+int autotune_binned(nwgpu_graph* g);
 // degrees (input order, host or device) -> g->deg (internal order)
 int load_degrees(nwgpu_graph* g, const uint32_t* out_degree, bool device_ptrs, cudaStream_t s);
 }  // namespace nwgpu

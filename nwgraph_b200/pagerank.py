@@ -92,7 +92,7 @@ class Graph:
     copied, validated and tiled on the device at construction.
     """
 
-    def __init__(self, row_ptr, col, weights=None, n=None, nnz=None, relabel=True):
+    def __init__(self, row_ptr, col, weights=None, n=None, nnz=None, relabel=True, autotune=False):
         rp, rp_dev, self._k0 = _ptr(row_ptr, np.uint32)
         cl, cl_dev, self._k1 = _ptr(col, np.uint32)
         w, w_dev, self._k2 = _ptr(weights, np.float32)
@@ -100,7 +100,8 @@ class Graph:
             raise ValueError("row_ptr, col and weights must all be on the host or all on the device")
         self.n = int(n if n is not None else len(row_ptr) - 1)
         self.nnz = int(nnz if nnz is not None else len(col))
-        flags = (N.GRAPH_DEVICE_PTRS if rp_dev else 0) | (0 if relabel else N.GRAPH_NO_RELABEL)
+        flags = ((N.GRAPH_DEVICE_PTRS if rp_dev else 0) | (0 if relabel else N.GRAPH_NO_RELABEL)
+                 | (N.GRAPH_AUTOTUNE if autotune else 0))
         h = C.c_void_p()
         N.check(N.lib().nwgpu_graph_create(rp, cl, w, self.n, self.nnz, flags, C.byref(h)))
         self._h = h

@@ -1,0 +1,80 @@
+"""Autotuner of the binned sweep (NWGPU_GRAPH_AUTOTUNE): every candidate gives
+bitwise-equal ranks, so a tuned graph must reproduce the default graph's
+ranks bit for bit; choices are cached per graph signature in the process and,
+with NWGPU_TUNE_CACHE, in a file that a later process reuses."""
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+import oracle as O
+from nwgraph_b200 import Graph, graphs as G
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def solve(g, deg, **kw):
+    with Graph(g.row_ptr, g.col, **kw) as h:
+        out = np.empty(g.n, np.float32)
+        h.page_rank(deg, out, 0.85, 0.0, 20)
+        return out, h.info()
+
+
+def test_tuned_ranks_are_bitwise_equal_and_cached(gpu, monkeypatch):
+    monkeypatch.delenv("NWGPU_TUNE_CACHE", raising=False)
+    g = G.rmat(17, 16, 5)
+    deg = g.out_degree()
+    r0, i0 = solve(g, deg)
+    r1, i1 = solve(g, deg, autotune=True)
+    r2, i2 = solve(g, deg, autotune=True)
+    assert i0["tuned"] == 0 and i0["binned"] == 1
+    assert i1["tuned"] in (1, 2) and i1["tuned_us_per_sweep"] > 0
+    assert i2["tuned"] == 2  # same signature: taken from the cache
+    for k in ("sweep_threads", "hub_smem_ids", "hub_l1_ids"):
+        assert i1[k] == i2[k]
+    assert np.array_equal(r0.view(np.uint32), r1.view(np.uint32))
+    assert np.array_equal(r0.view(np.uint32), r2.view(np.uint32))
+    ref, _, _ = O.jacobi_f32(g.row_ptr, g.col, deg, 0.85, 0.0, 20)
+    assert np.abs(r1.astype(np.float64) - ref).max() <= 1e-6
+
+
+def test_environment_settings_take_precedence(gpu, monkeypatch):
+    monkeypatch.setenv("NWGPU_SWEEP", "binned")
+    g = G.rmat(12, 16, 9)
+    _, info = solve(g, g.out_degree(), autotune=True)
+    assert info["tuned"] == 0 and info["sweep_threads"] == 256
+
+
+CHILD = r"""
+import json, sys
+sys.path.insert(0, {root!r})
+import numpy as np
+from nwgraph_b200 import Graph, graphs as G
+g = G.grid(90000)
+with Graph(g.row_ptr, g.col, autotune=True) as h:
+    out = np.empty(g.n, np.float32)
+    h.page_rank(g.out_degree(), out, 0.85, 0.0, 5)
+    print(json.dumps(h.info()))
+"""
+
+
+def test_cache_file_is_reused_by_another_process(gpu, tmp_path):
+    path = tmp_path / "tune.txt"
+    env = dict(os.environ, NWGPU_TUNE_CACHE=str(path))
+    env.pop("NWGPU_SWEEP", None)
+    code = CHILD.format(root=ROOT)
+    a = json.loads(subprocess.run([sys.executable, "-c", code], env=env, check=True, capture_output=True,
+                                  text=True).stdout.strip().splitlines()[-1])
+    assert a["tuned"] == 1 and path.exists()
+    lines = path.read_text().strip().splitlines()
+    assert len(lines) == 1 and lines[0].startswith("binned sms=")
+    b = json.loads(subprocess.run([sys.executable, "-c", code], env=env, check=True, capture_output=True,
+                                  text=True).stdout.strip().splitlines()[-1])
+    assert b["tuned"] == 2
+    for k in ("sweep_threads", "hub_smem_ids", "hub_l1_ids"):
+        assert a[k] == b[k]
