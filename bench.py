@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--cpu-sample-sweeps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-relabel", action="store_true", help="keep the input vertex order on the device")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="default launch settings instead of the tuned ones (tuning runs at graph creation)")
     ap.add_argument("--ppr-scale", type=int, default=22, help="graph scale of the batched-PPR comparison (0: skip)")
     ap.add_argument("--ppr-k", type=int, default=64)
     ap.add_argument("--ragged-graphs", type=int, default=4096,
@@ -434,7 +436,7 @@ def run_ours(args):
     cl_d = torch.from_numpy(g.col.view(np.int32)).to(dev)
     deg_d = torch.from_numpy(deg.view(np.int32)).to(dev)
     out_d = torch.empty(n, dtype=torch.float32, device=dev)
-    h = Graph(rp_d, cl_d, relabel=not args.no_relabel)
+    h = Graph(rp_d, cl_d, relabel=not args.no_relabel, autotune=not args.no_autotune)
     del rp_d, cl_d
     for _ in range(max(args.warmup, 3)):
         h.page_rank(deg_d, out_d, DAMPING, 0.0, SWEEPS, stream=stream, launch=args.launch)
@@ -467,7 +469,7 @@ def run_ours(args):
     e2e_steps = max(1, args.e2e_steps)
 
     def e2e_step():
-        with Graph(rp_h, cl_h, relabel=not args.no_relabel) as hh:
+        with Graph(rp_h, cl_h, relabel=not args.no_relabel, autotune=not args.no_autotune) as hh:
             hh.page_rank(deg_h, out_h, DAMPING, 0.0, SWEEPS, launch=args.launch)
 
     e2e_step()  # warm-up (context, allocator)
@@ -511,7 +513,9 @@ def run_ours(args):
                    "sweeps_per_step": SWEEPS, "threshold": 0.0, "damping": DAMPING,
                    "l2": "inputs larger than L2 (col 4*nnz bytes), no flush", "parallelism": f"replicas{world}",
                    "tile_items": info["tile_items"], "grid": info["grid"], "num_tiles": info["num_tiles"],
-                   "launch": args.launch, "relabel": not args.no_relabel},
+                   "launch": args.launch, "relabel": not args.no_relabel,
+                   "sweep": {k: info[k] for k in ("binned", "sweep_threads", "sweep_grid", "hub_smem_ids",
+                                                  "hub_l1_ids", "tuned", "tuned_us_per_sweep")}},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": sweep_traffic_per_launch(args), "peak_kind": peak_kind,
                      "bytes_per_sweep": B, "sweep_ms": t_sweep_ms},
