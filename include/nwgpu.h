@@ -272,6 +272,40 @@ int nwgpu_rmat_edges(uint32_t scale, uint64_t m, double a, double b, double c, u
  * nwgen_grid(side * side). */
 int nwgpu_grid_edges(uint64_t side, uint32_t* src, uint32_t* dst, void* stream);
 
+/* ---- Row-sharded PageRank across GPUs (one shard per rank) --------------
+ * The sweep of page_rank.hpp:92-147 split by destination rows over `world`
+ * ranks, one GPU each. Every rank passes the whole graph; it is relabelled
+ * the same way on every rank (descending row length, stably) and rank q
+ * keeps the internal rows [bounds[q], bounds[q+1]). Contributions live in a
+ * padded layout of world * stride floats, rank q's rows at q * stride, so
+ * one equal-count all-gather of the ranks' slices (stride floats each)
+ * rebuilds the whole vector between sweeps. The caller runs that exchange and
+ * the sum of the ranks' FP64 L1 changes (nwgraph_b200/shard.py does it over
+ * NCCL through torch.distributed) and decides when to stop. bounds[world+1]
+ * (host) must run from 0 to n, stride be a multiple of 4 and at least every
+ * rank's row count; every rank passes the same bounds and stride.
+ * All vectors below are device pointers; stream is a cudaStream_t, NULL
+ * meaning the CUDA default stream (as torch's default stream is). */
+typedef struct nwgpu_shard nwgpu_shard;
+int nwgpu_shard_create(const uint32_t* row_ptr, const uint32_t* col, uint64_t n, uint64_t nnz, uint32_t world,
+                       uint32_t rank, const uint64_t* bounds, uint64_t stride, uint32_t flags, nwgpu_shard** out);
+int nwgpu_shard_destroy(nwgpu_shard* s);
+/* ranks of this rank's rows = 1/n; their contributions rank / out_degree into
+ * contrib_slice[stride]. out_degree[n] is in input order (host unless
+ * device_ptrs). */
+int nwgpu_shard_start(nwgpu_shard* s, const uint32_t* out_degree, int device_ptrs, float* contrib_slice, void* stream);
+/* One Jacobi sweep of this rank's rows from contrib_all[world * stride] (the
+ * gathered slices): new ranks kept in the shard, new contributions into
+ * contrib_slice, and the FP64 L1 change of these rows into *l1 (one double,
+ * device; NaN if a bounded device wait gave up). */
+int nwgpu_shard_sweep(nwgpu_shard* s, const float* contrib_all, float* contrib_slice, float damping, double* l1,
+                      void* stream);
+/* This rank's ranks into rank_slice[stride]; after the caller gathers every
+ * slice into ranks_all[world * stride], nwgpu_shard_unpermute writes the
+ * ranks in input order into ranks[n]. */
+int nwgpu_shard_rank_slice(nwgpu_shard* s, float* rank_slice, void* stream);
+int nwgpu_shard_unpermute(nwgpu_shard* s, const float* ranks_all, float* ranks, void* stream);
+
 /* ---- Ragged batches: many independent graphs in one solve ----------------
  * No counterpart in the reference: each graph's result is what page_rank
  * (page_rank.hpp:92-147) gives for that graph alone, and each graph stops at

@@ -105,6 +105,13 @@ SIGNATURES = {
     "nwgpu_rmat_edges": (C.c_int, [C.c_uint32, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_uint64,
                                    C.c_uint64, _vp, _vp, _vp]),
     "nwgpu_grid_edges": (C.c_int, [C.c_uint64, _vp, _vp, _vp]),
+    "nwgpu_shard_create": (C.c_int, [_vp, _vp, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32, _vp, C.c_uint64,
+                                     C.c_uint32, C.POINTER(_vp)]),
+    "nwgpu_shard_destroy": (C.c_int, [_vp]),
+    "nwgpu_shard_start": (C.c_int, [_vp, _vp, C.c_int, _vp, _vp]),
+    "nwgpu_shard_sweep": (C.c_int, [_vp, _vp, _vp, C.c_float, _vp, _vp]),
+    "nwgpu_shard_rank_slice": (C.c_int, [_vp, _vp, _vp]),
+    "nwgpu_shard_unpermute": (C.c_int, [_vp, _vp, _vp, _vp]),
     "nwgpu_batch_create": (C.c_int, [C.c_uint64, _vp, _vp, _vp, _vp, C.c_uint32, C.POINTER(_vp)]),
     "nwgpu_batch_destroy": (C.c_int, [_vp]),
     "nwgpu_pr_ragged": (C.c_int, [_vp, _vp, _vp, C.c_float, C.c_float, C.c_uint64, C.POINTER(PrOptions),
