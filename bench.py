@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--cpu-sample-sweeps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-relabel", action="store_true", help="keep the input vertex order on the device")
+    ap.add_argument("--shard", action="store_true",
+                    help="with N > 1 GPUs also time the row-sharded solve of the one graph across the ranks "
+                         "(all-gather over NCCL each sweep); at N = 1 a one-shard solve is always timed")
     ap.add_argument("--no-autotune", action="store_true",
                     help="default launch settings instead of the tuned ones (tuning runs at graph creation)")
     ap.add_argument("--ppr-scale", type=int, default=22, help="graph scale of the batched-PPR comparison (0: skip)")
@@ -363,6 +366,45 @@ def vjp_vs_forward(scale, stream):
             "backward_includes": "adjoint solve on the out-row CSR + dL/dw (nnz) + dL/dt (n)"}
 
 
+def row_sharded(g, deg, dev, dist, steps):
+    """The row-sharded solve (nwgraph_b200.shard) of the whole graph: 20
+    fixed sweeps per step, each followed by the all-gather of the ranks'
+    contribution slices and the all-reduce of their L1 changes (one shard and
+    plain copies on one GPU). Strong scaling: every rank holds 1/N of the rows."""
+    import torch
+    from nwgraph_b200 import shard as S
+    rp = torch.from_numpy(g.row_ptr.view(np.int32)).to(dev)
+    cl = torch.from_numpy(g.col.view(np.int32)).to(dev)
+    dg = torch.from_numpy(deg.view(np.int32)).to(dev)
+    out = torch.empty(g.n, dtype=torch.float32, device=dev)
+    if dist:
+        sg = S.ShardedGraph(rp, cl)
+        solve = lambda: sg.page_rank(dg, out, DAMPING, 0.0, SWEEPS)  # noqa: E731
+        world, bounds = sg.world, sg.bounds
+    else:
+        bounds, stride = S.shard_bounds(g.row_ptr, 1)
+        sh = S.GpuShard(rp, cl, 1, 0, bounds, stride)
+        solve = lambda: S.run([sh], S.LocalExchange(), dg, out, DAMPING, 0.0, SWEEPS, device=dev)  # noqa: E731
+        world = 1
+    del rp, cl
+    for _ in range(3):
+        solve()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        solve()
+    e1.record()
+    torch.cuda.synchronize()
+    ms, = max_over_ranks([e0.elapsed_time(e1) / steps], dist, dev)
+    return {"world": world, "ms_per_step": ms, "ms_per_sweep": ms / SWEEPS,
+            "gteps": g.nnz * SWEEPS / (ms * 1e-3) / 1e9, "scaling": "strong",
+            "rows_per_rank": np.diff(np.asarray(bounds, np.int64)).tolist(),
+            "exchange": "all_gather_into_tensor + all_reduce (NCCL)" if dist else "one shard, copies"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -494,6 +536,7 @@ def run_ours(args):
     ppr = ppr_batched_vs_looped(args.ppr_scale, args.ppr_k, stream) if args.ppr_scale > 0 else None
     vjp = vjp_vs_forward(args.vjp_scale, stream) if args.vjp_scale > 0 else None
     ragged = ragged_vs_looped(args.ragged_graphs, args.ragged_max_n, stream) if args.ragged_graphs > 0 else None
+    sharded = row_sharded(g, deg, dev, dist, args.steps) if (world == 1 or args.shard) else None
 
     peak, peak_kind = peaks()
     achieved = B / (t_sweep_ms * 1e-3) / 1e9
@@ -535,6 +578,8 @@ def run_ours(args):
         line["vjp_vs_forward"] = vjp
     if ragged:
         line["ragged_batch_vs_looped"] = ragged
+    if sharded:
+        line["row_sharded"] = sharded
     if cpu:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
