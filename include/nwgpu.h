@@ -226,6 +226,16 @@ int nwgpu_wpr_run(nwgpu_graph* g, const float* teleport, float* ranks, float dam
 int nwgpu_pr_vjp(nwgpu_graph* g, const float* ranks, const float* dL_dr, float* dL_dw, float* dL_dt, float damping,
                  float threshold, uint64_t max_iters, const nwgpu_pr_options* options, nwgpu_pr_stats* stats);
 
+/* Weighted sparse matrix-vector product over the graph's rows:
+ *   y[i] = sum over the entries k of row i of weights[k] * x[col[k]]
+ * (bench/abstraction_penalty/spmv.cpp:52-62, the reference's SpMV kernel
+ * `y[i] += x[idx[j]] * dat[j]` from y = 0), as one sweep of the weighted
+ * PageRank kernel. x[n] and y[n] are in input order, host pointers unless
+ * options->device_ptrs. The graph must carry weights and be relabelled (the
+ * default); otherwise NWGPU_ERR_UNSUPPORTED. Row sums are FP32 in the
+ * kernel's fixed order, not the reference's serial order. */
+int nwgpu_spmv(nwgpu_graph* g, const float* x, float* y, const nwgpu_pr_options* options);
+
 /* Ask a running solve on g to stop at its next sweep boundary; the solve
  * returns NWGPU_ERR_ABORTED. Safe to call from another host thread. */
 int nwgpu_abort(nwgpu_graph* g);

@@ -365,3 +365,51 @@ extern "C" int nwgpu_pr_vjp(nwgpu_graph* g, const float* ranks, const float* dL_
   if (fin.aborted) return fail(NWGPU_ERR_ABORTED, "solve aborted after %llu sweeps", (unsigned long long)fin.iter);
   return NWGPU_OK;
 }
+
+namespace nwgpu {
+__global__ void spmv_fill_kernel(float* __restrict__ p, uint64_t n, float v) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) p[i] = v;
+}
+}  // namespace nwgpu
+
+// y = A x over the graph's rows: one sweep of the weighted binned kernel with
+// damping 1, base terms 0 and out-weight sums 1, so each row's update
+// fmaf(1, z, 0) is its weighted sum z = sum_k w_k x[col_k] exactly.
+extern "C" int nwgpu_spmv(nwgpu_graph* g, const float* x, float* y, const nwgpu_pr_options* options) {
+  clear_error();
+  const nwgpu_pr_options opt = read_options(options);
+  int                    rc = check_common(g, y, 1.0f, opt);
+  if (rc) return rc;
+  const uint64_t n = g->n;
+  if (n && !x) return fail(NWGPU_ERR_INVALID_ARG, "x is NULL");
+  if (n == 0) return NWGPU_OK;
+  cudaStream_t s = opt.stream ? (cudaStream_t)opt.stream : g->stream;
+  if ((rc = ensure_solve_buffers(g))) return rc;
+  if (!g->unit) {
+    CK(dalloc(g, &g->unit, n), "cudaMalloc(spmv ones)");
+    CK(dalloc(g, &g->zero, n), "cudaMalloc(spmv zeros)");
+    spmv_fill_kernel<<<g->sms * 4, 256, 0, g->stream>>>(g->unit, n, 1.0f);
+    CK(cudaGetLastError(), "spmv ones");
+    CK(cudaStreamSynchronize(g->stream), "spmv buffers");
+  }
+  // x in internal order as the sweep's contributions
+  const float* xd = x;
+  if (!opt.device_ptrs) {
+    CK(cudaMemcpyAsync(g->stage_u32, x, n * sizeof(float), cudaMemcpyHostToDevice, s), "copy x");
+    xd = reinterpret_cast<const float*>(g->stage_u32);
+  }
+  CK(launch_gather_f32(xd, g->g.inv, g->contrib[0], n, g->sms, s), "permute x");
+  if ((rc = start_state(g, 1, -1.0f, s))) return rc;
+  SweepArgs a = make_sweep_args(g, 1.0f, 0.f, kTeleportUniform, 0u);
+  a.w = g->g.w;
+  a.vbase = g->zero;
+  a.vaux = g->unit;
+  PrState fin{};
+  if ((rc = run_sweeps(g, a, NWGPU_LAUNCH_STREAM, 1, s, &fin, &g->plan, kModeWeighted))) return rc;
+  float* dst = opt.device_ptrs ? y : reinterpret_cast<float*>(g->stage_u32);
+  CK(launch_gather_f32(g->rank, g->g.perm, dst, n, g->sms, s), "permute y");
+  if (!opt.device_ptrs) CK(cudaMemcpyAsync(y, dst, n * sizeof(float), cudaMemcpyDeviceToHost, s), "copy y");
+  CK(cudaStreamSynchronize(s), "spmv");
+  return NWGPU_OK;
+}

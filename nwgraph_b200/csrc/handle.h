@@ -137,6 +137,8 @@ struct nwgpu_graph {
 
   nwgpu::PprBuffers ppr;
   nwgpu::WprBuffers wpr;
+  float*        unit = nullptr;  // n ones (nwgpu_spmv: out-weight sums of 1)
+  float*        zero = nullptr;  // n zeros (nwgpu_spmv: base terms of 0)
 
   ~nwgpu_graph() {
     ppr.release(stream);
@@ -145,7 +147,7 @@ struct nwgpu_graph {
     if (cg_exec) cudaGraphExecDestroy(cg_exec);
     if (cg) cudaGraphDestroy(cg);
     void* dev_ptrs[] = {g.row_ptr, g.col, g.w, g.perm, g.inv, g.emap, tiling.tile_row, tiling.tile_nnz, rank, contrib[0],
-                        contrib[1], deg, stage_u32, cpart, epart, res_part, st, err_hist};
+                        contrib[1], deg, stage_u32, cpart, epart, res_part, st, err_hist, unit, zero};
     for (void* p : dev_ptrs) nwgpu::pool_free(p, stream);
     cudaStreamSynchronize(stream);  // the blocks are free for the next handle at once
     if (h_st) cudaFreeHost(h_st);

@@ -318,6 +318,13 @@ class Graph:
         del keep
         return self._stats(st, errs)
 
+    def spmv(self, x, y, stream=None):
+        """y = A x over the rows (nwgpu_spmv): y[i] = sum_k weights[k] * x[col[k]] for row i's entries."""
+        (xp, yp), dev, keep = self._f32_vectors([x, y], [self.n, self.n])
+        opt = self._options("stream", dev, stream)
+        N.check(N.lib().nwgpu_spmv(self.handle, xp, yp, C.byref(opt)))
+        del keep
+
     def page_rank_vjp(self, ranks, dL_dr, dL_dw=None, dL_dt=None, damping_factor=0.85, threshold=1e-7,
                       max_iters=1000, launch="graph", record_errors=False, stream=None) -> PageRankStats:
         """Gradients of L = dL_dr . r at the weighted fixed point ``ranks``
