@@ -266,6 +266,34 @@ int nwgpu_csr_from_edges(const uint32_t* src, const uint32_t* dst, uint64_t m, u
                          uint32_t* row_ptr, uint32_t* col, uint64_t col_capacity, uint64_t* nnz, uint32_t* degrees,
                          void* stream);
 
+/* Graph files: the reference driver's load_graph (bench/gapbs/common.hpp:83-100)
+ * reads a serialized NW edge list (edge_list.hpp:237-280) or a Matrix Market
+ * coordinate file through read_mm<directed> (io/mmio.hpp:86-103, 171-208).
+ * These read both on all host cores into the same edge list, in the same
+ * order (Matrix Market: entry (i, j) gives edge (i-1, j-1), and symmetric
+ * files add (j-1, i-1) for i != j; only general / symmetric coordinate files,
+ * as read_mm). Build the CSR with nwgpu_csr_from_edges (no flags: the
+ * reference driver's adjacency<1>). Host code only: no device is needed.
+ * probe: the format, vertex count, an upper bound on the edges (capacity for
+ * read) and whether the file holds values. read: src/dst[capacity] and, if
+ * not NULL, values[capacity] (1.0 for pattern files); *m = edges read;
+ * nthreads <= 0 uses every core. write_nw: the NW edge-list layout that
+ * edge_list::deserialize reads (sources and targets, no attributes). */
+#define NWGPU_FILE_MATRIX_MARKET 1
+#define NWGPU_FILE_NW_EDGE_LIST 2
+typedef struct nwgpu_edge_file {
+  int32_t  format;     /* NWGPU_FILE_* */
+  int32_t  directed;   /* NW: the directedness written in the file; Matrix Market: 1 */
+  int32_t  has_values;
+  uint64_t n;          /* vertices */
+  uint64_t max_edges;  /* edges the file can yield (capacity for nwgpu_edge_file_read) */
+} nwgpu_edge_file;
+int nwgpu_edge_file_probe(const char* path, nwgpu_edge_file* info);
+int nwgpu_edge_file_read(const char* path, uint32_t* src, uint32_t* dst, float* values, uint64_t capacity,
+                         uint64_t* m, int nthreads);
+int nwgpu_edge_file_write_nw(const char* path, const uint32_t* src, const uint32_t* dst, uint64_t m, uint64_t n,
+                             int directed);
+
 /* Seeded RMAT edge list on the device (no counterpart in the reference, which
  * ships no generator): m samples over 2^scale ids, each descending `scale`
  * levels with quadrant probabilities a, b, c (d = 1 - a - b - c) drawn from a

@@ -78,6 +78,15 @@ class BatchStats(C.Structure):
                 ("graph_converged", C.POINTER(C.c_int32))]
 
 
+FILE_MATRIX_MARKET = 1
+FILE_NW_EDGE_LIST = 2
+
+
+class EdgeFile(C.Structure):
+    _fields_ = [("format", C.c_int32), ("directed", C.c_int32), ("has_values", C.c_int32), ("n", C.c_uint64),
+                ("max_edges", C.c_uint64)]
+
+
 # Every symbol include/nwgpu.h declares, with its C signature.
 _vp = C.c_void_p
 SIGNATURES = {
@@ -101,6 +110,9 @@ SIGNATURES = {
                                 C.POINTER(PrStats)]),
     "nwgpu_pr_vjp": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_float, C.c_float, C.c_uint64, C.POINTER(PrOptions),
                                C.POINTER(PrStats)]),
+    "nwgpu_edge_file_probe": (C.c_int, [C.c_char_p, C.POINTER(EdgeFile)]),
+    "nwgpu_edge_file_read": (C.c_int, [C.c_char_p, _vp, _vp, _vp, C.c_uint64, C.POINTER(C.c_uint64), C.c_int]),
+    "nwgpu_edge_file_write_nw": (C.c_int, [C.c_char_p, _vp, _vp, C.c_uint64, C.c_uint64, C.c_int]),
     "nwgpu_csr_from_edges": (C.c_int, [_vp, _vp, C.c_uint64, C.c_uint64, C.c_uint32, _vp, _vp, C.c_uint64,
                                        C.POINTER(C.c_uint64), _vp, _vp]),
     "nwgpu_rmat_edges": (C.c_int, [C.c_uint32, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_uint64,

@@ -146,3 +146,38 @@ def batch_from_device_csrs(parts, degrees=None):
     b = GraphBatch(vo, eo, rp_all, cl_all[: int(eo[-1])])
     del rp_all, cl_all
     return (b, deg_all[: int(vo[-1])]) if degrees is not None else b
+
+
+def read_edges(path: str, values: bool = False, nthreads: int = 0):
+    """The edge list of a graph file (Matrix Market or NW binary edge list),
+    as the reference driver's load_graph reads it: ``(src, dst, n)`` uint32
+    numpy arrays, plus the values when ``values``. Host code (no GPU)."""
+    info = N.EdgeFile()
+    N.check(N.lib().nwgpu_edge_file_probe(path.encode(), C.byref(info)))
+    cap = int(info.max_edges)
+    src = np.empty(max(cap, 1), np.uint32)
+    dst = np.empty(max(cap, 1), np.uint32)
+    val = np.empty(max(cap, 1), np.float32) if values else None
+    m = C.c_uint64()
+    N.check(N.lib().nwgpu_edge_file_read(path.encode(), src.ctypes.data, dst.ctypes.data,
+                                         val.ctypes.data if values else None, cap, C.byref(m), int(nthreads)))
+    k = m.value
+    out = (src[:k].copy(), dst[:k].copy(), int(info.n))
+    return out + (val[:k].copy(),) if values else out
+
+
+def write_nw_edges(path: str, src, dst, n: int, directed: bool = True):
+    """Write an NW binary edge list (what edge_list::deserialize reads)."""
+    s = np.ascontiguousarray(src, np.uint32)
+    d = np.ascontiguousarray(dst, np.uint32)
+    N.check(N.lib().nwgpu_edge_file_write_nw(path.encode(), s.ctypes.data, d.ctypes.data, len(s), int(n),
+                                             1 if directed else 0))
+
+
+def load_graph(path: str, nthreads: int = 0):
+    """The reference driver's graph input (bench/gapbs/common.hpp:83-100 then
+    build_adjacency<1>): the file's edge list built into adjacency<1> (row v
+    lists the sources of the edges into v, rows sorted) on the GPU. Returns
+    ``(CSR, degrees)`` on the host; degrees are build_degrees' out-degrees."""
+    src, dst, n = read_edges(path, nthreads=nthreads)
+    return csr_from_edges(src, dst, n, 0)

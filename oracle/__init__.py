@@ -102,6 +102,13 @@ def ref(fast: bool = False):
         L.nwref_build_degrees.argtypes = [_u32p, _u32p, C.c_uint64, _u32p, C.c_int]
         L.nwref_fill_adj1.restype = C.c_int
         L.nwref_fill_adj1.argtypes = [_u32p, _u32p, C.c_uint64, C.c_uint64, _u32p, _u32p]
+        L.nwref_read_mm_edges.restype = C.c_int
+        L.nwref_read_mm_edges.argtypes = [C.c_char_p, _u32p, _u32p, C.c_uint64, C.POINTER(C.c_uint64),
+                                          C.POINTER(C.c_uint64)]
+        L.nwref_read_nw_edges.restype = C.c_int
+        L.nwref_read_nw_edges.argtypes = L.nwref_read_mm_edges.argtypes
+        L.nwref_write_nw_edges.restype = C.c_int
+        L.nwref_write_nw_edges.argtypes = [C.c_char_p, _u32p, _u32p, C.c_uint64, C.c_uint64]
         L.nwref_build_csr.restype = C.c_int
         L.nwref_build_csr.argtypes = [_u32p, _u32p, C.c_uint64, C.c_uint64, C.c_int, _u32p, _u32p, C.c_uint64,
                                       C.POINTER(C.c_uint64)]
@@ -326,6 +333,33 @@ def ref_build_csr(src, dst, n, flags):
                              C.byref(nnz)) != 0:
         raise RuntimeError("nwref_build_csr failed")
     return rp, cl[: nnz.value]
+
+
+def _ref_edges(fn, path, cap):
+    src = np.empty(max(cap, 1), np.uint32)
+    dst = np.empty(max(cap, 1), np.uint32)
+    m, n = C.c_uint64(), C.c_uint64()
+    if fn(path.encode(), _p(src, _u32p), _p(dst, _u32p), cap, C.byref(m), C.byref(n)) != 0:
+        raise RuntimeError("reference edge reader failed")
+    return src[: m.value].copy(), dst[: m.value].copy(), int(n.value)
+
+
+def ref_read_mm_edges(path, cap):
+    """The edge list NWGraph's read_mm<directed> builds (oracle/_ref): (src, dst, n)."""
+    return _ref_edges(ref().nwref_read_mm_edges, path, cap)
+
+
+def ref_read_nw_edges(path, cap):
+    """The edge list NWGraph's edge_list::deserialize reads (oracle/_ref): (src, dst, n)."""
+    return _ref_edges(ref().nwref_read_nw_edges, path, cap)
+
+
+def ref_write_nw_edges(path, src, dst, n):
+    """NWGraph's edge_list::serialize of the edges (oracle/_ref)."""
+    s = np.ascontiguousarray(src, np.uint32)
+    d = np.ascontiguousarray(dst, np.uint32)
+    if ref().nwref_write_nw_edges(path.encode(), _p(s, _u32p), _p(d, _u32p), len(s), int(n)) != 0:
+        raise RuntimeError("nwref_write_nw_edges failed")
 
 
 def ref_load_mm(path):

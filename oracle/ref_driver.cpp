@@ -11,6 +11,8 @@
 //   nw::graph::page_rank_v1         include/nwgraph/experimental/algorithms/page_rank.hpp:82-119 (serial Jacobi)
 //   nw::graph::bench::build_degrees bench/gapbs/common.hpp:110-121 (out-degree from adjacency<1>)
 //   nw::graph::read_mm              include/nwgraph/io/mmio.hpp:171-217 + adjacency<1> fill (build.hpp:209-232)
+//   read_mm<directed> edge list     include/nwgraph/io/mmio.hpp:86-103, 171-208
+//   edge_list serialize/deserialize include/nwgraph/edge_list.hpp:237-280
 //   edge clean-up and fill          remove_self_loops / lexical_sort_by / uniq (build.hpp:58-69, 394-410),
 //                                   adjacency<idx>(el, sort_adjacency) (adjacency.hpp:115-129, build.hpp:209-321)
 //
@@ -173,6 +175,50 @@ int nwref_build_csr(const uint32_t* src, const uint32_t* dst, uint64_t m, uint64
                      : build_csr<directedness::undirected, 1>(src, dst, m, n, flags, row_ptr, col, col_cap, nnz);
   return by_source ? build_csr<directedness::directed, 0>(src, dst, m, n, flags, row_ptr, col, col_cap, nnz)
                    : build_csr<directedness::directed, 1>(src, dst, m, n, flags, row_ptr, col, col_cap, nnz);
+}
+
+// The edge list read_mm<directed> builds, in its order. Returns -1 if cap is
+// too small (m still set).
+int nwref_read_mm_edges(const char* path, uint32_t* src, uint32_t* dst, uint64_t cap, uint64_t* m, uint64_t* n) {
+  CoutCapture cap_out;
+  auto        el = nw::graph::read_mm<nw::graph::directedness::directed>(std::string(path));
+  *m             = el.size();
+  *n             = el.num_vertices()[0];
+  if (*m > cap) return -1;
+  uint64_t e = 0;
+  for (auto&& [u, v] : el) {
+    src[e] = u;
+    dst[e] = v;
+    ++e;
+  }
+  return 0;
+}
+
+// edge_list<directed>::serialize of the given edges.
+int nwref_write_nw_edges(const char* path, const uint32_t* src, const uint32_t* dst, uint64_t m, uint64_t n) {
+  nw::graph::edge_list<nw::graph::directedness::directed> el(n);
+  el.open_for_push_back();
+  for (uint64_t e = 0; e < m; ++e) el.push_back(src[e], dst[e]);
+  el.close_for_push_back();
+  el.serialize(std::string(path));
+  return 0;
+}
+
+// edge_list<directed>::deserialize, as load_graph does for "NW" files.
+int nwref_read_nw_edges(const char* path, uint32_t* src, uint32_t* dst, uint64_t cap, uint64_t* m, uint64_t* n) {
+  CoutCapture                                              cap_out;
+  nw::graph::edge_list<nw::graph::directedness::directed> el(0);
+  el.deserialize(std::string(path));
+  *m = el.size();
+  *n = el.num_vertices()[0];
+  if (*m > cap) return -1;
+  uint64_t e = 0;
+  for (auto&& [u, v] : el) {
+    src[e] = u;
+    dst[e] = v;
+    ++e;
+  }
+  return 0;
 }
 
 // A resident adjacency<1> + degrees, so timing runs do not re-copy the CSR.

@@ -19,6 +19,11 @@ the reference tree; the GPU host only reads the committed .npz files).
   each with every combination of remove_self_loops, lexical sort + uniq, and
   adjacency<0> / adjacency<1> over a directed or undirected edge list
   (build.hpp:58-69, 209-272, 394-410; rows sorted).
+* ``files/`` and ``loaders.npz`` -- small Matrix Market files written here
+  (general with real values and comments, symmetric pattern with self-loops,
+  the karate edge list) with the edge lists NWGraph's read_mm<directed> reads
+  from them (io/mmio.hpp:86-103, 171-208), and an NW binary edge list written
+  by NWGraph's edge_list::serialize (edge_list.hpp:237-255) with its edges.
 
 All reference outputs come from oracle/_ref/libnwref.so, built from the
 reference headers by oracle/Makefile.
@@ -112,15 +117,54 @@ def csr_fixtures(karate_i, karate_j):
     print("csr_build:", len(lists), "edge lists x", len(CSR_FLAG_SETS), "flag sets")
 
 
+def write_mtx(path, header, n, rows, comments=()):
+    with open(path, "w") as f:
+        f.write(header + "\n")
+        for c in comments:
+            f.write("%" + c + "\n")
+        f.write(f"{n} {n} {len(rows)}\n")
+        for r in rows:
+            f.write(" ".join(str(x) for x in r) + "\n")
+
+
+def loader_fixtures(karate_i, karate_j):
+    files = os.path.join(HERE, "files")
+    os.makedirs(files, exist_ok=True)
+    rng = np.random.default_rng(31)
+    n = 50
+    gi, gj = rng.integers(1, n + 1, 300), rng.integers(1, n + 1, 300)
+    gj[:20] = gi[:20]  # self-loops
+    gi[20:40], gj[20:40] = gi[40:60], gj[40:60]  # repeats
+    vals = np.round(rng.uniform(-2, 2, 300), 4)
+    write_mtx(os.path.join(files, "general_real.mtx"), "%%MatrixMarket matrix coordinate real general", n,
+              [(a, b, v) for a, b, v in zip(gi, gj, vals)], comments=(" written by make_golden.py", ""))
+    si, sj = rng.integers(1, 41, 150), rng.integers(1, 41, 150)
+    si, sj = np.maximum(si, sj), np.minimum(si, sj)  # lower triangle, diagonal included
+    write_mtx(os.path.join(files, "symmetric_pattern.mtx"), "%%MatrixMarket matrix coordinate pattern symmetric", 40,
+              list(zip(si, sj)))
+    write_mtx(os.path.join(files, "karate_pattern.mtx"), "%%MatrixMarket matrix coordinate pattern symmetric", 34,
+              list(zip(np.maximum(karate_i, karate_j) + 1, np.minimum(karate_i, karate_j) + 1)))
+    out = {}
+    for name in ("general_real", "symmetric_pattern", "karate_pattern"):
+        s, d, nn = O.ref_read_mm_edges(os.path.join(files, name + ".mtx"), 1000)
+        out[f"{name}/src"], out[f"{name}/dst"], out[f"{name}/n"] = s, d, np.array([nn], np.int64)
+    s, d = out["general_real/src"], out["general_real/dst"]
+    O.ref_write_nw_edges(os.path.join(files, "general_ref.nw"), s, d, n)
+    np.savez_compressed(os.path.join(HERE, "loaders.npz"), **out)
+    print("loaders:", sorted({k.split("/")[0] for k in out}), "+ general_ref.nw")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=os.environ.get("NWGRAPH_REF", "/root/reference"))
-    ap.add_argument("--only", choices=["csr"], default=None, help="regenerate csr_build.npz alone")
+    ap.add_argument("--only", choices=["csr", "loaders"], default=None,
+                    help="regenerate csr_build.npz, or files/ and loaders.npz, alone")
     args = ap.parse_args()
     O.build(with_reference=True)
-    if args.only == "csr":
+    if args.only:
         src = open(os.path.join(args.ref, "test", "page_rank_test.cpp")).read()
-        csr_fixtures(np.array(parse_vector(src, "i"), np.uint32), np.array(parse_vector(src, "j"), np.uint32))
+        ki, kj = np.array(parse_vector(src, "i"), np.uint32), np.array(parse_vector(src, "j"), np.uint32)
+        (csr_fixtures if args.only == "csr" else loader_fixtures)(ki, kj)
         return
 
     src = open(os.path.join(args.ref, "test", "page_rank_test.cpp")).read()
@@ -155,6 +199,7 @@ def main():
         print(name, "n", g.n, "nnz", g.nnz, "v10 thr iters", int(out[f"{name}/v10_thr_iters"][0]))
     np.savez_compressed(os.path.join(HERE, "small_graphs.npz"), **out)
     csr_fixtures(i, j)
+    loader_fixtures(i, j)
 
 
 if __name__ == "__main__":

@@ -87,3 +87,15 @@ def test_errors(gpu):
     assert st == N.ERR_INVALID_ARG and nnz.value == 6  # capacity 2 < 6 entries: refused, size reported
     with pytest.raises(NwgpuError):
         K.rmat_edges(0, 10)
+
+
+def test_load_graph_from_files(gpu):
+    """load_graph: a graph file's edges built into adjacency<1> on the device,
+    as the reference driver's load_graph + build_adjacency<1> (rows sorted)."""
+    import os
+    files = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "files")
+    for name in ("general_real.mtx", "symmetric_pattern.mtx", "karate_pattern.mtx", "general_ref.nw"):
+        csr, deg = K.load_graph(os.path.join(files, name))
+        s, d, n = K.read_edges(os.path.join(files, name))
+        rp, cl, dg = O.build_csr(s, d, n, 0)
+        assert np.array_equal(csr.row_ptr, rp) and np.array_equal(csr.col, cl) and np.array_equal(deg, dg), name
