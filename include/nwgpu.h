@@ -135,6 +135,20 @@ typedef struct nwgpu_pr_stats {
 int nwgpu_pr_run(nwgpu_graph* g, const uint32_t* out_degree, float* ranks, float damping, float threshold,
                  uint64_t max_iters, const nwgpu_pr_options* options, nwgpu_pr_stats* stats);
 
+/* Residual-push PageRank: page_rank_v13 (experimental/algorithms/page_rank.hpp:
+ * 552-625). Ranks start at 0 and every residual at (float)(1 - d). Each
+ * iteration pushes every residual above `threshold` into its vertex's rank
+ * and, for out-degree > 0, spreads residual * d / deg to the out-neighbours
+ * (FP32); each vertex's next residual is the sum of what it received. It stops
+ * after the first iteration in which no vertex with out-degree > 0 pushed, or
+ * after max_iters. The ranks are the reference's: not normalised (they sum to
+ * about n). stats->errors[i] / final_error count the vertices that pushed in
+ * iteration i / the last one; converged = no push in the last iteration.
+ * Needs a relabelled graph (the default). Sums run in the kernel's fixed
+ * order, not the reference's serial one. */
+int nwgpu_pr_residual_run(nwgpu_graph* g, const uint32_t* out_degree, float* ranks, float damping, float threshold,
+                          uint64_t max_iters, const nwgpu_pr_options* options, nwgpu_pr_stats* stats);
+
 /* Personalised PageRank with a one-hot teleport at `seed` (input vertex id):
  *   r = (1 - d) e_seed + d A^T D^{-1} r,  r(0) = e_seed,
  * the plain update of page_rank.hpp:133 with base_i = (1 - d) [i == seed];

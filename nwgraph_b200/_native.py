@@ -97,6 +97,8 @@ SIGNATURES = {
     "nwgpu_graph_get_info": (C.c_int, [_vp, C.POINTER(GraphInfo)]),
     "nwgpu_pr_run": (C.c_int, [_vp, _vp, _vp, C.c_float, C.c_float, C.c_uint64, C.POINTER(PrOptions),
                                C.POINTER(PrStats)]),
+    "nwgpu_pr_residual_run": (C.c_int, [_vp, _vp, _vp, C.c_float, C.c_float, C.c_uint64, C.POINTER(PrOptions),
+                                        C.POINTER(PrStats)]),
     "nwgpu_ppr_run": (C.c_int, [_vp, _vp, C.c_uint32, _vp, C.c_float, C.c_float, C.c_uint64, C.POINTER(PrOptions),
                                 C.POINTER(PrStats)]),
     "nwgpu_ppr_batched": (C.c_int, [_vp, _vp, _vp, C.c_uint32, _vp, C.c_float, C.c_float, C.c_uint64,

@@ -314,7 +314,7 @@ bool same_loop(const nwgpu_graph* g, const SweepArgs& y, const BinPlan* plan, in
   const SweepArgs& x = g->cg_args;
   return g->cg_plan == plan && g->cg_mode == mode && x.damping == y.damping && x.base == y.base &&
          x.teleport == y.teleport && x.seed == y.seed && x.row_ptr == y.row_ptr && x.col == y.col && x.w == y.w &&
-         x.vbase == y.vbase && x.vaux == y.vaux;
+         x.vbase == y.vbase && x.vaux == y.vaux && x.push_threshold == y.push_threshold;
 }
 
 // Runs the sweep loop from the state already on the device; fills fin.
@@ -670,6 +670,89 @@ int nwgpu_abort(nwgpu_graph* g) {
 int nwgpu_pr_run(nwgpu_graph* g, const uint32_t* out_degree, float* ranks, float damping, float threshold,
                  uint64_t max_iters, const nwgpu_pr_options* options, nwgpu_pr_stats* stats) {
   return solve_single(g, out_degree, ranks, damping, threshold, max_iters, options, stats, kTeleportUniform, 0u);
+}
+
+int nwgpu_pr_residual_run(nwgpu_graph* g, const uint32_t* out_degree, float* ranks, float damping, float threshold,
+                          uint64_t max_iters, const nwgpu_pr_options* options, nwgpu_pr_stats* stats) {
+  clear_error();
+  if (!g) return fail(NWGPU_ERR_INVALID_ARG, "graph is NULL");
+  if (g->n && (!out_degree || !ranks)) return fail(NWGPU_ERR_INVALID_ARG, "out_degree / ranks is NULL");
+  if (!(damping >= 0.0f && damping <= 1.0f)) return fail(NWGPU_ERR_INVALID_ARG, "damping %g outside [0, 1]", (double)damping);
+  const nwgpu_pr_options opt = read_options(options);
+  if (opt.launch > NWGPU_LAUNCH_STREAM) return fail(NWGPU_ERR_INVALID_ARG, "launch %u unknown", opt.launch);
+  const uint64_t n = g->n;
+  if (stats) {
+    double*  eb = stats->errors;
+    uint64_t ec = stats->errors_cap;
+    memset(stats, 0, sizeof(*stats));
+    stats->errors = eb;
+    stats->errors_cap = ec;
+    stats->bytes_per_iter = 4.0 * (double)g->nnz + 4.0 * (double)(n + 1) + 20.0 * (double)n;
+  }
+  if (n == 0) {  // no vertex pushes: the first iteration ends the loop
+    if (stats) stats->iterations = max_iters ? 1 : 0;
+    if (stats) stats->converged = max_iters ? 1 : 0;
+    return NWGPU_OK;
+  }
+  if (!g->plan.ok) return fail(NWGPU_ERR_UNSUPPORTED, "the residual-push solve runs on the binned sweep: relabel the graph");
+  cudaStream_t s = opt.stream ? (cudaStream_t)opt.stream : g->stream;
+  int          rc = ensure_solve_buffers(g);
+  if (rc) return rc;
+  *(volatile unsigned int*)g->h_abort = 0u;
+  if ((rc = load_degrees(g, out_degree, opt.device_ptrs != 0, s))) return rc;
+  // page_rank_v13's first iteration, first phase: every residual is (float)(1 - d)
+  const float r0 = (float)(1.0 - (double)damping);
+  PrState     h = {};
+  *g->h_st = h;
+  CK(cudaMemcpyAsync(g->st, g->h_st, sizeof(PrState), cudaMemcpyHostToDevice, s), "copy state");
+  CK(launch_residual_init(g->rank, g->contrib[0], g->deg, n, r0, damping, max_iters > 0 && r0 > threshold,
+                          &g->st->pending, g->sms, s),
+     "residual init");
+  CK(cudaMemcpyAsync(g->h_st, g->st, sizeof(PrState), cudaMemcpyDeviceToHost, s), "copy state");
+  CK(cudaStreamSynchronize(s), "residual init");
+  const uint64_t first = g->h_st->pending;  // vertices that pushed in the first iteration
+  CK(cudaEventRecord(g->ev0, s), "cudaEventRecord");
+  PrState fin{};
+  if (max_iters > 1 && first > 0) {
+    // each sweep: the second phase of one iteration and the first of the next;
+    // its "error" is the number of vertices that pushed, and no push ends the loop
+    h = {};
+    h.max_iters = max_iters - 1;
+    h.chunk_end = kGraphChunk;
+    h.threshold = 0.5;
+    *g->h_st = h;
+    CK(cudaMemcpyAsync(g->st, g->h_st, sizeof(PrState), cudaMemcpyHostToDevice, s), "copy state");
+    SweepArgs a = make_sweep_args(g, damping, 0.f, kTeleportUniform, 0u);
+    a.push_threshold = threshold;
+    if ((rc = run_sweeps(g, a, opt.launch, max_iters - 1, s, &fin, &g->plan, kModeResidual))) return rc;
+  }
+  CK(cudaEventRecord(g->ev1, s), "cudaEventRecord");
+  float* dst = opt.device_ptrs ? ranks : reinterpret_cast<float*>(g->stage_u32);
+  CK(launch_gather_f32(g->rank, g->g.perm, dst, n, g->sms, s), "permute ranks");
+  if (!opt.device_ptrs) CK(cudaMemcpyAsync(ranks, dst, n * sizeof(float), cudaMemcpyDeviceToHost, s), "copy ranks");
+  CK(cudaStreamSynchronize(s), "copy ranks");
+  if (stats) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+    const uint64_t its = max_iters == 0 ? 0 : 1 + fin.iter;
+    stats->iterations = its;
+    stats->final_error = fin.iter ? fin.last_error : (double)first;
+    stats->converged = max_iters > 0 && (fin.iter ? fin.converged != 0 : first == 0);
+    stats->device_ms = ms;
+    stats->ms_per_iter = fin.iter ? ms / (double)fin.iter : 0.0;
+    stats->gteps = ms > 0 ? (double)g->nnz * (double)fin.iter / (ms * 1e6) : 0.0;
+    if (stats->errors && stats->errors_cap && its) {
+      stats->errors[0] = (double)first;
+      uint64_t m = fin.iter < stats->errors_cap - 1 ? fin.iter : stats->errors_cap - 1;
+      if (m > g->err_cap) m = g->err_cap;
+      if (m) {
+        CK(cudaMemcpyAsync(stats->errors + 1, g->err_hist, m * sizeof(double), cudaMemcpyDeviceToHost, s), "copy errors");
+        CK(cudaStreamSynchronize(s), "copy errors");
+      }
+    }
+  }
+  if (fin.aborted) return fail(NWGPU_ERR_ABORTED, "solve aborted after %llu sweeps", (unsigned long long)fin.iter);
+  return NWGPU_OK;
 }
 
 int nwgpu_ppr_run(nwgpu_graph* g, const uint32_t* out_degree, uint32_t seed, float* ranks, float damping,

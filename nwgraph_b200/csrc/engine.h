@@ -84,6 +84,8 @@ enum SweepMode : int {
   kModePlain = 0,     // z = sum contrib;      r = base + d z;          contrib' = r / deg
   kModeWeighted = 1,  // z = sum w * contrib;  r = vbase + d z;         contrib' = r / vaux  (vaux = out-weight sum)
   kModeAdjoint = 2,   // z = sum w * lambda;   l = vbase + vaux * z;    contrib' = l         (vaux = d / out-weight sum)
+  kModeResidual = 3,  // residual push (page_rank_v13): z = sum delta; if z > push_threshold: r += z and
+                      // delta' = z d / deg (deg > 0), else delta' = 0; the sweep "error" counts pushes
 };
 
 struct SweepArgs {
@@ -115,6 +117,7 @@ struct SweepArgs {
   const float*                 w;          // kModeWeighted / kModeAdjoint: entry weights of the swept CSR
   const float*                 vbase;      // per-row base term (weighted: (1-d) t; adjoint: c)
   const float*                 vaux;       // per-row factor (weighted: out-weight sum; adjoint: d / out-weight sum)
+  float                        push_threshold;  // kModeResidual: residuals above this are pushed
   // Ragged batches only (the RAGGED sweep variant):
   const RaggedGraph*           graphs;
   const float*                 graph_base;  // per graph: (1 - d) / n
@@ -198,6 +201,10 @@ cudaError_t launch_gather_u32(const uint32_t* src, const uint32_t* idx, uint32_t
                               cudaStream_t s);
 cudaError_t launch_gather_f32(const float* src, const uint32_t* idx, float* dst, uint64_t n, int sms, cudaStream_t s);
 cudaError_t launch_pr_init(const SweepArgs& a, uint64_t n, float init, int sms, cudaStream_t s);
+// Residual push, first phase of the first iteration: rank = push ? r0 : 0,
+// delta = (push, deg > 0) ? r0 d / deg : 0, *pushed += vertices with both.
+cudaError_t launch_residual_init(float* rank, float* delta, const uint32_t* deg, uint64_t n, float r0, float damping,
+                                 bool push, unsigned int* pushed, int sms, cudaStream_t s);
 // Sweep kernel variants: threads per CTA, items per thread, and whether the
 // hottest ids are kept in shared memory (one large CTA per SM) or left to L1.
 struct SweepVariant {

@@ -80,7 +80,7 @@ template <int MODE>
 __device__ __forceinline__ RowIn load_row_in(const BinnedArgs& a, uint32_t r) {
   RowIn x;
   x.old = ld_stream(a.sw.rank + r);
-  if constexpr (MODE == kModePlain) {
+  if constexpr (MODE == kModePlain || MODE == kModeResidual) {
     x.dg = ld_stream(a.sw.deg + r);
     x.aux = 1.f;
     x.base = 0.f;
@@ -104,6 +104,19 @@ __device__ __forceinline__ double binned_update(const BinnedArgs& a, float* __re
   } else if constexpr (MODE == kModeWeighted) {
     nr = fmaf(a.sw.damping, z, in.base);
     c = nr / in.aux;
+  } else if constexpr (MODE == kModeResidual) {
+    // z is this row's new residual (page_rank_v13's second phase: the sum of
+    // the positive deltas, all deltas being >= 0); then its first phase for
+    // the next iteration: push a residual above the threshold into the rank
+    // and, with out-degree > 0, spread residual * d / deg (FP32, :576-589).
+    const float res = z > 0.f ? z : 0.f;
+    const bool  push = res > a.sw.push_threshold;
+    const bool  moved = push && in.dg > 0u;
+    nr = push ? in.old + res : in.old;
+    c = moved ? res * a.sw.damping / (float)in.dg : 0.f;
+    st_stream(a.sw.rank + r, nr);
+    st_keep(cout + r, c, pol);
+    return moved ? 1.0 : 0.0;
   } else {
     nr = fmaf(in.aux, z, in.base);
     c = nr;
@@ -123,7 +136,7 @@ __device__ __forceinline__ double binned_epilogue(const BinnedArgs& a, float* __
 template <bool HOT, int MODE>
 __device__ __forceinline__ float term(const BinnedArgs& a, const Src& src, uint32_t id, uint32_t k) {
   const float c = gather_one<HOT>(src, id);
-  if constexpr (MODE == kModePlain) return c;
+  if constexpr (MODE == kModePlain || MODE == kModeResidual) return c;
   else return ld_stream(a.sw.w + k) * c;
 }
 
@@ -516,7 +529,8 @@ uint32_t binned_hot_capacity() { return (uint32_t)(binned_hot_smem_bytes() / 4) 
 cudaError_t configure_binned_kernels() {
   void* const hot[] = {(void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModePlain>,
                        (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModeWeighted>,
-                       (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModeAdjoint>};
+                       (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModeAdjoint>,
+                       (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModeResidual>};
   for (void* fn : hot) {
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, binned_hot_smem_bytes());
     if (e != cudaSuccess) return e;
@@ -540,12 +554,14 @@ int binned_sweep_grid(int sms, bool hot) {
 static void* binned_fn(bool hot, int mode) {
   if (mode == kModeWeighted) return (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModeWeighted>;
   if (mode == kModeAdjoint) return (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModeAdjoint>;
+  if (mode == kModeResidual) return (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModeResidual>;
   return hot ? (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModePlain>
              : (void*)pr_binned_sweep_kernel<kBinnedThreads, false, kModePlain>;
 }
 static void* binned_finish_fn(int mode) {
   if (mode == kModeWeighted) return (void*)pr_binned_finish_kernel<kModeWeighted>;
   if (mode == kModeAdjoint) return (void*)pr_binned_finish_kernel<kModeAdjoint>;
+  if (mode == kModeResidual) return (void*)pr_binned_finish_kernel<kModeResidual>;
   return (void*)pr_binned_finish_kernel<kModePlain>;
 }
 static bool binned_shape_hot(bool hot, int mode) { return hot || mode != kModePlain; }

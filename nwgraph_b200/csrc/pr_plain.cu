@@ -838,6 +838,27 @@ cudaError_t launch_pr_init(const SweepArgs& a, uint64_t n, float init, int sms, 
   return cudaGetLastError();
 }
 
+__global__ void residual_init_kernel(float* __restrict__ rank, float* __restrict__ delta, const uint32_t* __restrict__ deg,
+                                     uint64_t n, float r0, float damping, int push, unsigned int* pushed) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  unsigned int   cnt = 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint32_t dg = deg[i];
+    const bool     moved = push && dg > 0u;
+    rank[i] = push ? r0 : 0.f;
+    delta[i] = moved ? r0 * damping / (float)dg : 0.f;
+    cnt += moved ? 1u : 0u;
+  }
+  cnt = __reduce_add_sync(kFullMask, cnt);
+  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(pushed, cnt);
+}
+
+cudaError_t launch_residual_init(float* rank, float* delta, const uint32_t* deg, uint64_t n, float r0, float damping,
+                                 bool push, unsigned int* pushed, int sms, cudaStream_t s) {
+  residual_init_kernel<<<sms * 8, 256, 0, s>>>(rank, delta, deg, n, r0, damping, push ? 1 : 0, pushed);
+  return cudaGetLastError();
+}
+
 // Sets the sweep bound of one graph launch (first node of the graph).
 __global__ void pr_arm_kernel(PrState* st) { st->chunk_end = st->iter + kGraphChunk; }
 

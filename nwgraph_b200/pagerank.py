@@ -172,6 +172,25 @@ class Graph:
             opt.stream = int(getattr(stream, "cuda_stream", stream))
         return opt
 
+    def page_rank_residual(self, degrees, out, damping_factor=0.85, threshold=1e-4, max_iters=20, launch="graph",
+                           record_errors=False, stream=None) -> PageRankStats:
+        """Residual-push PageRank (page_rank_v13; nwgpu_pr_residual_run). Ranks are not normalised."""
+        dp, op, dev, keep = self._vectors(degrees, out, self.n)
+        opt = self._options(launch, dev, stream)
+        st = N.PrStats()
+        errs = None
+        if record_errors:
+            cap = int(min(max(int(max_iters), 1), 4096))
+            errs = np.zeros(cap, np.float64)
+            st.errors = errs.ctypes.data_as(C.POINTER(C.c_double))
+            st.errors_cap = cap
+        N.check(N.lib().nwgpu_pr_residual_run(self.handle, dp, op, C.c_float(damping_factor), C.c_float(threshold),
+                                              int(max_iters), C.byref(opt), C.byref(st)))
+        del keep
+        return PageRankStats(int(st.iterations), float(st.final_error), bool(st.converged), float(st.device_ms),
+                             float(st.ms_per_iter), float(st.bytes_per_iter), float(st.gteps),
+                             None if errs is None else errs[: min(int(st.iterations), len(errs))])
+
     def ppr(self, degrees, seed, out, damping_factor=0.85, threshold=1e-6, max_iters=100, launch="graph",
             record_errors=False, stream=None) -> PageRankStats:
         """Personalised PageRank with a one-hot teleport at ``seed`` (nwgpu_ppr_run)."""

@@ -67,6 +67,8 @@ def lib():
         L.orc_ppr_jacobi_f32.restype = C.c_int64
         L.orc_ppr_jacobi_f32.argtypes = [_u32p, _u32p, C.c_uint64, _u32p, C.c_uint32, _f32p, C.c_float, C.c_float,
                                          C.c_uint64, _f64p]
+        L.orc_pr_residual_f32.restype = C.c_int64
+        L.orc_pr_residual_f32.argtypes = L.orc_pr_jacobi_f32.argtypes
         L.orc_pr_v1_f64.restype = C.c_int64
         L.orc_pr_v1_f64.argtypes = [_u32p, _u32p, C.c_uint64, _u32p, _f64p, C.c_double, C.c_double, C.c_uint64]
         L.orc_pr_f64.restype = C.c_int64
@@ -156,6 +158,16 @@ def ppr_jacobi_f32(row_ptr, col, deg, seed, damping=0.85, threshold=1e-6, max_it
     it = lib().orc_ppr_jacobi_f32(_p(row_ptr, _u32p), _p(col, _u32p), n, _p(deg, _u32p), int(seed), _p(r, _f32p),
                                   damping, threshold, int(max_iters), _p(errs, _f64p))
     return r, int(it), errs[: int(it)]
+
+
+def residual_f32(row_ptr, col, deg, damping=0.85, threshold=1e-4, max_iters=20):
+    """page_rank_v13 (residual push) restated. Returns (ranks, iterations, pushes per iteration)."""
+    n = len(row_ptr) - 1
+    r = np.empty(n, np.float32)
+    cnt = np.zeros(max(int(max_iters), 1), np.float64)
+    it = lib().orc_pr_residual_f32(_p(row_ptr, _u32p), _p(col, _u32p), n, _p(deg, _u32p), _p(r, _f32p), damping,
+                                   threshold, int(max_iters), _p(cnt, _f64p))
+    return r, int(it), cnt[: int(it)]
 
 
 def gauss_seidel_f32(row_ptr, col, deg, damping=0.85, threshold=1e-4, max_iters=20):

@@ -282,3 +282,61 @@ int64_t orc_pr_vjp_f64(const uint32_t* row_ptr, const uint32_t* col, uint64_t n,
   free(q);
   return (int64_t)it;
 }
+
+/*
+ * Restates nw::graph::page_rank_v13 (experimental/algorithms/page_rank.hpp:
+ * 552-625), the residual-push PageRank, on one thread: ranks start at 0 and
+ * every residual at (float)(1 - d) (:562-568). Per iteration: for every
+ * vertex, delta = 0, and if residual > threshold the residual moves into the
+ * rank and, for out-degree > 0, delta = residual * d / deg in FP32 (:576-589);
+ * then every row sums the positive deltas of its entries in CSR order, and
+ * its residual becomes that sum if > 0, else 0 (:593-605). It stops after the
+ * first iteration in which no vertex with out-degree > 0 pushed (:610-612).
+ * Returns the iterations run; changed[] (may be NULL) receives how many
+ * vertices pushed in each.
+ */
+int64_t orc_pr_residual_f32(const uint32_t* row_ptr, const uint32_t* col, uint64_t n, const uint32_t* deg, float* rank,
+                            float damping, float threshold, uint64_t max_iters, double* changed) {
+  float* delta = (float*)malloc((n ? n : 1) * sizeof(float));
+  float* residual = (float*)malloc((n ? n : 1) * sizeof(float));
+  if (!delta || !residual) {
+    free(delta);
+    free(residual);
+    return -1;
+  }
+  for (uint64_t i = 0; i < n; ++i) {
+    rank[i] = 0.0f;
+    delta[i] = 0.0f;
+    residual[i] = (float)(1.0 - (double)damping);
+  }
+  uint64_t it = 0;
+  for (; it < max_iters; ++it) {
+    uint64_t count = 0;
+    for (uint64_t s = 0; s < n; ++s) {
+      delta[s] = 0.0f;
+      if (residual[s] > threshold) {
+        const float old = residual[s];
+        rank[s] += old;
+        residual[s] = 0.0f;
+        if (deg[s] > 0) {
+          delta[s] = old * damping / (float)deg[s];
+          ++count;
+        }
+      }
+    }
+    for (uint64_t i = 0; i < n; ++i) {
+      float sum = 0.0f;
+      for (uint32_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k)
+        if (delta[col[k]] > 0) sum += delta[col[k]];
+      residual[i] = sum > 0 ? sum : 0.0f;
+    }
+    if (changed) changed[it] = (double)count;
+    if (count == 0) {
+      ++it;
+      break;
+    }
+  }
+  free(delta);
+  free(residual);
+  return (int64_t)it;
+}

@@ -9,6 +9,7 @@
 //   nw::graph::page_rank            include/nwgraph/algorithms/page_rank.hpp:89-148 (v11, Gauss-Seidel)
 //   nw::graph::page_rank_v10        include/nwgraph/experimental/algorithms/page_rank.hpp:377-432 (Jacobi)
 //   nw::graph::page_rank_v1         include/nwgraph/experimental/algorithms/page_rank.hpp:82-119 (serial Jacobi)
+//   nw::graph::page_rank_v13        include/nwgraph/experimental/algorithms/page_rank.hpp:552-625 (residual push)
 //   nw::graph::bench::build_degrees bench/gapbs/common.hpp:110-121 (out-degree from adjacency<1>)
 //   nw::graph::read_mm              include/nwgraph/io/mmio.hpp:171-217 + adjacency<1> fill (build.hpp:209-232)
 //   read_mm<directed> edge list     include/nwgraph/io/mmio.hpp:86-103, 171-208
@@ -94,6 +95,8 @@ int nwref_page_rank_f32(int version, const uint32_t* row_ptr, const uint32_t* co
       nw::graph::page_rank_v10(g, degrees, pr, damping, threshold, (size_t)max_iters, (size_t)nthreads);
     } else if (version == 1) {
       nw::graph::page_rank_v1(g, degrees, pr, damping, threshold, (size_t)max_iters);
+    } else if (version == 13) {
+      nw::graph::page_rank_v13(g, degrees, pr, damping, threshold, (size_t)max_iters, (size_t)nthreads);
     } else {
       return -1;
     }

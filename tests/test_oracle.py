@@ -149,3 +149,17 @@ def test_build_csr_restatement_matches_reference_golden(csr_golden):
             assert np.array_equal(rp, g[f]["row_ptr"]), (name, f)
             assert np.array_equal(cl, g[f]["col"]), (name, f)
             assert np.array_equal(deg, g[f]["deg"]), (name, f)
+
+
+def test_residual_restatement_matches_reference_v13():
+    """oracle.residual_f32 restates page_rank_v13 (experimental/algorithms/
+    page_rank.hpp:552-625): bit for bit against the compiled reference on one
+    thread, with its iteration count."""
+    if not O.ref_available():
+        pytest.skip("the reference build (oracle/_ref) is not present")
+    for g in (G.rmat(10, 16, 3), G.grid(1000)):
+        deg = g.out_degree()
+        for thr, iters in ((1e-4, 100), (0.0, 12), (1e-3, 5)):
+            r, it, _ = O.residual_f32(g.row_ptr, g.col, deg, 0.85, thr, iters)
+            rr, rit, _, _ = O.ref_page_rank(13, g.row_ptr, g.col, deg, 0.85, thr, iters, 1)
+            assert it == rit and np.array_equal(r.view(np.uint32), rr.view(np.uint32)), (g.n, thr)
