@@ -405,6 +405,45 @@ def row_sharded(g, deg, dev, dist, steps):
             "exchange": "all_gather_into_tensor + all_reduce (NCCL)" if dist else "one shard, copies"}
 
 
+def wppr_batched_vs_looped(scale, k, stream):
+    """The weighted configuration's batched variant: k teleport vectors
+    (random distributions, seed 99) on the RMAT graph with weights U(0.1, 1)
+    (seed 1234), per-column L1 < 1e-6, against k looped weighted solves."""
+    import torch
+    from nwgraph_b200 import Graph, graphs as G
+    g = G.rmat(scale, 16, 42)
+    w = G.edge_weights(g.nnz, seed=1234)
+    t = np.random.default_rng(99).uniform(0.0, 1.0, (g.n, k))
+    t = (t / t.sum(axis=0, keepdims=True)).astype(np.float32)
+    dev = torch.device("cuda")
+    td = torch.from_numpy(t).to(dev)
+    cols = [td[:, c].contiguous() for c in range(k)]
+    out = torch.empty((g.n, k), dtype=torch.float32, device=dev)
+    out1 = torch.empty(g.n, dtype=torch.float32, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Graph(g.row_ptr, g.col, weights=w) as h:
+        h.weighted_page_rank_batched(td, out, DAMPING, 1e-6, 300, stream=stream)  # warm-up (out-row CSR, buffers)
+        h.weighted_page_rank(cols[0], out1, DAMPING, 1e-6, 300, stream=stream)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        sb = h.weighted_page_rank_batched(td, out, DAMPING, 1e-6, 300, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_b = e0.elapsed_time(e1)
+        sweeps = 0
+        e0.record(stream)
+        for c in range(k):
+            sweeps += h.weighted_page_rank(cols[c], out1, DAMPING, 1e-6, 300, stream=stream).iterations
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_l = e0.elapsed_time(e1)
+        worst = float((out1 - out[:, k - 1]).abs().max())
+    return {"graph": f"rmat{scale}_ef16_weighted", "n": g.n, "nnz": g.nnz, "k": k, "threshold": 1e-6,
+            "batched_ms": t_b, "looped_ms": t_l, "speedup": t_l / t_b, "batched_sweeps": sb.iterations,
+            "looped_sweeps_total": sweeps, "all_converged": sb.all_converged,
+            "max_abs_batched_vs_looped_last_column": worst}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -535,6 +574,7 @@ def run_ours(args):
     del rp_h, cl_h, deg_h, out_h
     ppr = ppr_batched_vs_looped(args.ppr_scale, args.ppr_k, stream) if args.ppr_scale > 0 else None
     vjp = vjp_vs_forward(args.vjp_scale, stream) if args.vjp_scale > 0 else None
+    wppr = wppr_batched_vs_looped(args.vjp_scale, 16, stream) if args.vjp_scale > 0 else None
     ragged = ragged_vs_looped(args.ragged_graphs, args.ragged_max_n, stream) if args.ragged_graphs > 0 else None
     sharded = row_sharded(g, deg, dev, dist, args.steps) if (world == 1 or args.shard) else None
 
@@ -576,6 +616,8 @@ def run_ours(args):
         line["ppr_batched_vs_looped"] = ppr
     if vjp:
         line["vjp_vs_forward"] = vjp
+    if wppr:
+        line["wppr_batched_vs_looped"] = wppr
     if ragged:
         line["ragged_batch_vs_looped"] = ragged
     if sharded:

@@ -178,6 +178,18 @@ int nwgpu_ppr_batched(nwgpu_graph* g, const uint32_t* out_degree, const uint32_t
                       float damping, float threshold, uint64_t max_iters, const nwgpu_pr_options* options,
                       nwgpu_ppr_stats* stats);
 
+/* Weighted personalised PageRank for k <= 128 teleport vectors at once (no
+ * counterpart in the reference): column c solves nwgpu_wpr_run's problem
+ *   r_c = (1 - d) t_c + d sum_k w_k r_c[col[k]] / s_{col[k]},  r_c(0) = t_c
+ * with teleports[n x k] (row-major, input order) and writes ranks_nxk
+ * (row-major, input order). One index and weight load feeds all k gathers;
+ * each column stops at its own first sweep whose FP64 L1 change is below
+ * threshold (its values then stay fixed) or at max_iters. The graph must carry
+ * weights and be relabelled (the default). Arrays are host pointers unless
+ * options->device_ptrs. */
+int nwgpu_wppr_batched(nwgpu_graph* g, const float* teleports, uint32_t k, float* ranks_nxk, float damping,
+                       float threshold, uint64_t max_iters, const nwgpu_pr_options* options, nwgpu_ppr_stats* stats);
+
 /* PageRank without any allocation. No counterpart in the reference.
  *
  * For callers that must not allocate:

@@ -11,7 +11,7 @@ void PprBuffers::release(cudaStream_t s) {
   cg_exec = nullptr;
   cg = nullptr;
   void* ptrs[] = {tiling.tile_row, tiling.tile_nnz, rank, contrib[0], contrib[1], out, cpart, epart, res_part,
-                  spans, seeds, seeds_in, col_done, col_conv, col_iters, col_err, st};
+                  spans, seeds, seeds_in, col_done, col_conv, col_iters, col_err, st, vbase};
   for (void* p : ptrs) pool_free(p, s);
   if (h_st) cudaFreeHost(h_st);
   *this = PprBuffers();
@@ -59,6 +59,9 @@ static int ensure_ppr(nwgpu_graph* g, int K) {
   b.K = K;
   return NWGPU_OK;
 }
+
+int ppr_loop(nwgpu_graph* g, const PprArgs& a, int K, uint32_t k, float* ranks_nxk, float damping, uint64_t max_iters,
+             const nwgpu_pr_options& opt, nwgpu_ppr_stats* stats, cudaStream_t s);
 
 static PprArgs make_ppr_args(nwgpu_graph* g, float damping) {
   PprBuffers& b = g->ppr;
@@ -147,15 +150,27 @@ extern "C" int nwgpu_ppr_batched(nwgpu_graph* g, const uint32_t* out_degree, con
   *b.h_st = h;
   CK(cudaMemcpyAsync(b.st, b.h_st, sizeof(PprState), cudaMemcpyHostToDevice, s), "copy ppr state");
   CK(launch_ppr_init(a, K, n, g->sms, s), "ppr init");
+  return ppr_loop(g, a, K, k, ranks_nxk, damping, max_iters, opt, stats, s);
+}
+
+namespace nwgpu {
+// The batched sweep loop from the state on the device, then the output and
+// the per-column stats (both batched entry points).
+int ppr_loop(nwgpu_graph* g, const PprArgs& a, int K, uint32_t k, float* ranks_nxk, float damping, uint64_t max_iters,
+             const nwgpu_pr_options& opt, nwgpu_ppr_stats* stats, cudaStream_t s) {
+  PprBuffers&    b = g->ppr;
+  const uint64_t n = g->n;
+  const bool     weighted = a.w != nullptr;
   CK(cudaEventRecord(g->ev0, s), "cudaEventRecord");
   if (opt.launch == NWGPU_LAUNCH_GRAPH) {
-    if (!b.cg_exec || b.cg_damping != damping) {
+    if (!b.cg_exec || b.cg_damping != damping || b.cg_weighted != weighted) {
       if (b.cg_exec) cudaGraphExecDestroy(b.cg_exec);
       if (b.cg) cudaGraphDestroy(b.cg);
       b.cg_exec = nullptr;
       CK(cudaGraphCreate(&b.cg, 0), "cudaGraphCreate");
       CK(build_ppr_graph(b.cg, a, K, b.sweep_grid, b.st, &b.cg_exec), "ppr graph");
       b.cg_damping = damping;
+      b.cg_weighted = weighted;
     }
     const uint64_t max_launches = max_iters / kGraphChunk + 2;
     for (uint64_t l = 0;; ++l) {
@@ -205,4 +220,63 @@ extern "C" int nwgpu_ppr_batched(nwgpu_graph* g, const uint32_t* out_degree, con
   }
   if (fin.aborted) return fail(NWGPU_ERR_ABORTED, "batched solve aborted after %llu sweeps", (unsigned long long)fin.iter);
   return NWGPU_OK;
+}
+}  // namespace nwgpu
+
+extern "C" int nwgpu_wppr_batched(nwgpu_graph* g, const float* teleports, uint32_t k, float* ranks_nxk, float damping,
+                                  float threshold, uint64_t max_iters, const nwgpu_pr_options* options,
+                                  nwgpu_ppr_stats* stats) {
+  clear_error();
+  if (!g) return fail(NWGPU_ERR_INVALID_ARG, "graph is NULL");
+  if (k == 0 || k > 128) return fail(NWGPU_ERR_INVALID_ARG, "k = %u outside [1, 128]", k);
+  if (g->n && (!teleports || !ranks_nxk)) return fail(NWGPU_ERR_INVALID_ARG, "NULL array argument");
+  if (!(damping >= 0.0f && damping <= 1.0f)) return fail(NWGPU_ERR_INVALID_ARG, "damping %g outside [0, 1]", (double)damping);
+  if (!g->g.w) return fail(NWGPU_ERR_UNSUPPORTED, "the graph has no edge weights (pass them to nwgpu_graph_create)");
+  if (!g->relabelled || !g->plan.ok) return fail(NWGPU_ERR_UNSUPPORTED, "weighted solves need a relabelled graph");
+  nwgpu_pr_options opt = {};
+  if (options) memcpy(&opt, options, options->size && options->size < sizeof(opt) ? options->size : sizeof(opt));
+  if (opt.launch > NWGPU_LAUNCH_STREAM) return fail(NWGPU_ERR_INVALID_ARG, "launch %u unknown", opt.launch);
+  const int      K = ppr_padded_k(k);
+  const uint64_t n = g->n;
+  if (stats) {
+    uint32_t* ci = stats->col_iterations;
+    double*   ce = stats->col_errors;
+    int32_t*  cc = stats->col_converged;
+    memset(stats, 0, sizeof(*stats));
+    stats->col_iterations = ci;
+    stats->col_errors = ce;
+    stats->col_converged = cc;
+    stats->bytes_per_iter = 8.0 * (double)g->nnz + 4.0 * (double)(n + 1) + 4.0 * (double)n + 20.0 * k * (double)n;
+  }
+  if (n == 0) return NWGPU_OK;
+  int rc = ensure_solve_buffers(g);
+  if (rc) return rc;
+  if ((rc = ensure_wpr(g))) return rc;  // out-weight sums (internal order)
+  if ((rc = ensure_ppr(g, K))) return rc;
+  PprBuffers& b = g->ppr;
+  if (!b.vbase) CK(dalloc(g, &b.vbase, n * (uint64_t)K), "cudaMalloc(ppr base terms)");
+  cudaStream_t s = opt.stream ? (cudaStream_t)opt.stream : g->stream;
+  *(volatile unsigned int*)g->h_abort = 0u;
+  // teleports on the device (the output staging holds n x K >= n x k floats)
+  const float* t = teleports;
+  if (!opt.device_ptrs) {
+    CK(cudaMemcpyAsync(b.out, teleports, n * k * sizeof(float), cudaMemcpyHostToDevice, s), "copy teleports");
+    t = b.out;
+  }
+  PprArgs a = make_ppr_args(g, damping);
+  a.w = g->g.w;
+  a.vbase = b.vbase;
+  a.vaux = g->wpr.t.s;
+  // columns: the first k active, the padding ones stopped from the start
+  CK(cudaMemsetAsync(b.seeds_in, 0, k * sizeof(uint32_t), s), "ppr columns");
+  CK(launch_ppr_seeds(b.seeds_in, k, K, nullptr, a, s), "ppr columns");
+  PprState h = {};
+  h.max_iters = max_iters;
+  h.chunk_end = kGraphChunk;
+  h.threshold = (double)threshold;
+  h.done = (max_iters == 0) ? 1u : 0u;
+  *b.h_st = h;
+  CK(cudaMemcpyAsync(b.st, b.h_st, sizeof(PprState), cudaMemcpyHostToDevice, s), "copy ppr state");
+  CK(launch_ppr_winit(a, K, t, k, g->g.inv, n, b.vbase, g->sms, s), "weighted ppr init");
+  return ppr_loop(g, a, K, k, ranks_nxk, damping, max_iters, opt, stats, s);
 }

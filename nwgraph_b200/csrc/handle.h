@@ -88,6 +88,8 @@ struct PprBuffers {
   cudaGraph_t     cg = nullptr;
   cudaGraphExec_t cg_exec = nullptr;
   float           cg_damping = -1.f;
+  bool            cg_weighted = false;
+  float*          vbase = nullptr;  // weighted solves: n x K base terms (1 - d) t
   void            release(cudaStream_t s);  // returns the buffers to the pool on stream s
 };
 

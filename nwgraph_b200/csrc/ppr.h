@@ -49,6 +49,11 @@ struct PprArgs {
   int                          use_cond;
   float                        damping;
   float                        one_minus_d;
+  // Weighted solves (w != null): entry weights, base terms (1 - d) t (n x K)
+  // and out-weight sums (n), all in internal order.
+  const float*                 w;
+  const float*                 vbase;
+  const float*                 vaux;
 };
 
 int         ppr_padded_k(uint32_t k);
@@ -59,6 +64,10 @@ int         ppr_sweep_grid(int K, int sms);
 cudaError_t launch_ppr_seeds(const uint32_t* seeds_in, uint32_t k, int K, const uint32_t* perm, const PprArgs& a,
                              cudaStream_t s);
 cudaError_t launch_ppr_init(const PprArgs& a, int K, uint64_t n, int sms, cudaStream_t s);
+// Weighted start from teleports t_in (n x k row-major, input order; inv:
+// internal -> input id): vbase = (1 - d) t, rank = t, contrib = t / s per column.
+cudaError_t launch_ppr_winit(const PprArgs& a, int K, const float* t_in, uint32_t k, const uint32_t* inv, uint64_t n,
+                             float* vbase, int sms, cudaStream_t s);
 cudaError_t launch_ppr_output(const float* rank, const uint32_t* perm, uint64_t n, int K, uint32_t k, float* out,
                               int sms, cudaStream_t s);
 cudaError_t launch_ppr_sweep(const PprArgs& a, int K, int sweep_grid, cudaStream_t s);

@@ -72,8 +72,14 @@ __device__ __forceinline__ void load_group(Cols<K> (&v)[U], const float* __restr
       if (g * U + u < E) load_row<K>(v[u], cin, s_col[g * U + u], lane, pol);
   }
 }
+// Weighted solves: the group's entry weights (the same address in every lane).
+template <int U>
+__device__ __forceinline__ void load_weights(float (&wv)[U], const float* __restrict__ w, uint32_t k0, int g, int E) {
+#pragma unroll
+  for (int u = 0; u < U; ++u) wv[u] = (g * U + u < E) ? __ldg(w + k0 + g * U + u) : 0.f;
+}
 
-template <int K, int W, int U>
+template <int K, int W, int U, bool WEIGHTED>
 __global__ void __launch_bounds__(256) ppr_gather_kernel(const PprArgs a) {
   constexpr int P = Cols<K>::PER_LANE;
   constexpr int NWARP = 256 / 32;
@@ -112,13 +118,16 @@ __global__ void __launch_bounds__(256) ppr_gather_kernel(const PprArgs a) {
       ++i;
       next_end = (i < R) ? (int)(s_rp[warp][i + 1] - k0) : 0x7fffffff;
     };
-    auto consume = [&](const Cols<K>(&v)[U], int g) {
+    // one term: the gathered contribution (times the entry's weight when weighted)
+    auto add = [&](const Cols<K>& v, float wgt) {
+#pragma unroll
+      for (int q = 0; q < P; ++q) acc.v[q] = WEIGHTED ? fmaf(wgt, v.v[q], acc.v[q]) : acc.v[q] + v.v[q];
+    };
+    auto consume = [&](const Cols<K>(&v)[U], const float(&wv)[U], int g) {
       const int e0 = g * U;
       if (next_end >= e0 + U && e0 + U <= E) {  // a full group inside the current row
 #pragma unroll
-        for (int u = 0; u < U; ++u)
-#pragma unroll
-          for (int q = 0; q < P; ++q) acc.v[q] += v[u].v[q];
+        for (int u = 0; u < U; ++u) add(v[u], wv[u]);
         return;
       }
 #pragma unroll
@@ -126,19 +135,24 @@ __global__ void __launch_bounds__(256) ppr_gather_kernel(const PprArgs a) {
         const int e = e0 + u;
         if (e < E) {
           while (next_end <= e) flush();
-#pragma unroll
-          for (int q = 0; q < P; ++q) acc.v[q] += v[u].v[q];
+          add(v[u], wv[u]);
         }
       }
     };
     Cols<K> va[U], vb[U];
+    float   wa[U], wb[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) wa[u] = wb[u] = 1.f;
     load_group<K, U>(va, cin, s_col[warp], 0, E, lane, pol);
+    if (WEIGHTED) load_weights<U>(wa, a.w, k0, 0, E);
     for (int g = 0; g * U < E; g += 2) {
       load_group<K, U>(vb, cin, s_col[warp], g + 1, E, lane, pol);
-      consume(va, g);
+      if (WEIGHTED) load_weights<U>(wb, a.w, k0, g + 1, E);
+      consume(va, wa, g);
       if ((g + 1) * U >= E) break;
       load_group<K, U>(va, cin, s_col[warp], g + 2, E, lane, pol);
-      consume(vb, g + 1);
+      if (WEIGHTED) load_weights<U>(wa, a.w, k0, g + 2, E);
+      consume(vb, wb, g + 1);
     }
     while (next_end <= E) flush();  // rows ending at the tile's last entry, and empty rows after it
     if (has_co) {
@@ -207,7 +221,7 @@ __global__ void __launch_bounds__(256) ppr_fixup_kernel(const PprArgs a) {
 // FP64 |r' - r| into per-CTA column partials; converged columns keep their
 // ranks. contrib = r' / deg_i for every column. The grid stride is a multiple
 // of K / 4, so every thread stays on one group of four columns.
-template <int K>
+template <int K, bool WEIGHTED>
 __global__ void __launch_bounds__(256) ppr_epilogue_kernel(const PprArgs a, uint64_t n) {
   constexpr int     C4 = K / 4;
   __shared__ double s_res[256][4];
@@ -234,12 +248,16 @@ __global__ void __launch_bounds__(256) ppr_epilogue_kernel(const PprArgs a, uint
       const uint32_t i = (uint32_t)(x / C4);
       const float4   z = __ldcs(reinterpret_cast<const float4*>(cout) + x);
       const float4   old = __ldcs(reinterpret_cast<const float4*>(a.rank) + x);
-      const float    dg = (float)__ldg(a.deg + i);
+      // weighted: divide by the out-weight sum; the base terms are (1 - d) t
+      const float    dg = WEIGHTED ? __ldg(a.vaux + i) : (float)__ldg(a.deg + i);
+      float4         tb = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (WEIGHTED) tb = __ldg(reinterpret_cast<const float4*>(a.vbase) + x);
       const float    zv[4] = {z.x, z.y, z.z, z.w}, ov[4] = {old.x, old.y, old.z, old.w};
+      const float    bv[4] = {tb.x, tb.y, tb.z, tb.w};
       float          nr[4], co[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const float tele = (seed[q] == i) ? a.one_minus_d : 0.f;
+        const float tele = WEIGHTED ? bv[q] : ((seed[q] == i) ? a.one_minus_d : 0.f);
         nr[q] = act[q] ? fmaf(a.damping, zv[q], tele) : ov[q];
         co[q] = nr[q] / dg;
         if (act[q]) res[q] += (double)fabsf(nr[q] - ov[q]);
@@ -317,6 +335,25 @@ __global__ void ppr_init_kernel(const PprArgs a, uint64_t n) {
   }
 }
 
+// Weighted start: per column c < k, t = t_in[inv[i] * k + c]; vbase = (1 - d) t,
+// rank = t, contrib = t / s_i (the single weighted solve's start, per column);
+// padding columns are 0.
+template <int K>
+__global__ void ppr_winit_kernel(const PprArgs a, const float* __restrict__ t_in, uint32_t k,
+                                 const uint32_t* __restrict__ inv, uint64_t n, float* __restrict__ vbase) {
+  const uint64_t total = n * K;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total; x += stride) {
+    const uint64_t i = x / K;
+    const uint32_t c = (uint32_t)(x % K);
+    const uint64_t src = inv ? inv[i] : i;
+    const float    t = (c < k) ? t_in[src * k + c] : 0.f;
+    vbase[x] = a.one_minus_d * t;
+    a.rank[x] = t;
+    a.contrib0[x] = t / a.vaux[i];
+  }
+}
+
 // out[i * k + c] = rank[perm[i] * K + c] for c < k (input order, unpadded).
 template <int K>
 __global__ void ppr_output_kernel(const float* __restrict__ rank, const uint32_t* __restrict__ perm, uint64_t n,
@@ -365,24 +402,23 @@ cudaError_t launch_ppr_seeds(const uint32_t* seeds_in, uint32_t k, int K, const 
 __global__ void ppr_arm_kernel(PprState* st) { st->chunk_end = st->iter + kGraphChunk; }
 
 // Rows per group: U * K = 512 floats, 2 KB of rows per group (16 floats per lane).
-template <int K>
+template <int K, bool WEIGHTED>
 struct PprKernels {
   static constexpr int U = 512 / K;
-  static void*         gather() { return (void*)ppr_gather_kernel<K, kPprTileItems, U>; }
-  static void*         fixup() { return (void*)ppr_fixup_kernel<K>; }
-  static void*         epilogue() { return (void*)ppr_epilogue_kernel<K>; }
-  static void*         finish() { return (void*)ppr_finish_kernel<K>; }
+  static void*         fn(int which) {
+    return which == 0   ? (void*)ppr_gather_kernel<K, kPprTileItems, U, WEIGHTED>
+           : which == 1 ? (void*)ppr_fixup_kernel<K>
+           : which == 2 ? (void*)ppr_epilogue_kernel<K, WEIGHTED>
+                        : (void*)ppr_finish_kernel<K>;
+  }
 };
 
-// kernel 0 gather, 1 fix-up, 2 epilogue, 3 finish
-static void* ppr_fn(int K, int which) {
+// kernel 0 gather, 1 fix-up, 2 epilogue, 3 finish; weighted solves have their own gather and epilogue
+static void* ppr_fn(int K, int which, bool weighted = false) {
   switch (K) {
-    case 32: return which == 0 ? PprKernels<32>::gather() : which == 1 ? PprKernels<32>::fixup()
-                    : which == 2 ? PprKernels<32>::epilogue() : PprKernels<32>::finish();
-    case 64: return which == 0 ? PprKernels<64>::gather() : which == 1 ? PprKernels<64>::fixup()
-                    : which == 2 ? PprKernels<64>::epilogue() : PprKernels<64>::finish();
-    case 128: return which == 0 ? PprKernels<128>::gather() : which == 1 ? PprKernels<128>::fixup()
-                     : which == 2 ? PprKernels<128>::epilogue() : PprKernels<128>::finish();
+    case 32: return weighted ? PprKernels<32, true>::fn(which) : PprKernels<32, false>::fn(which);
+    case 64: return weighted ? PprKernels<64, true>::fn(which) : PprKernels<64, false>::fn(which);
+    case 128: return weighted ? PprKernels<128, true>::fn(which) : PprKernels<128, false>::fn(which);
     default: return nullptr;
   }
 }
@@ -415,6 +451,17 @@ cudaError_t launch_ppr_init(const PprArgs& a, int K, uint64_t n, int sms, cudaSt
   return cudaGetLastError();
 }
 
+cudaError_t launch_ppr_winit(const PprArgs& a, int K, const float* t_in, uint32_t k, const uint32_t* inv, uint64_t n,
+                             float* vbase, int sms, cudaStream_t s) {
+  switch (K) {
+    case 32: ppr_winit_kernel<32><<<sms * 8, 256, 0, s>>>(a, t_in, k, inv, n, vbase); break;
+    case 64: ppr_winit_kernel<64><<<sms * 8, 256, 0, s>>>(a, t_in, k, inv, n, vbase); break;
+    case 128: ppr_winit_kernel<128><<<sms * 8, 256, 0, s>>>(a, t_in, k, inv, n, vbase); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t launch_ppr_output(const float* rank, const uint32_t* perm, uint64_t n, int K, uint32_t k, float* out,
                               int sms, cudaStream_t s) {
   switch (K) {
@@ -431,7 +478,8 @@ cudaError_t launch_ppr_sweep(const PprArgs& a, int K, int sweep_grid, cudaStream
   for (int w = 0; w < 4; ++w) {
     uint64_t    n = a.n;
     void*       eargs[] = {(void*)&a, (void*)&n};
-    cudaError_t e = cudaLaunchKernel(ppr_fn(K, w), ppr_grid(a, w, sweep_grid), dim3(256), w == 2 ? eargs : args, 0, s);
+    cudaError_t e = cudaLaunchKernel(ppr_fn(K, w, a.w != nullptr), ppr_grid(a, w, sweep_grid), dim3(256),
+                                     w == 2 ? eargs : args, 0, s);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -467,7 +515,7 @@ cudaError_t build_ppr_graph(cudaGraph_t g, const PprArgs& proto, int K, int swee
   cudaGraphNode_t      prev = nullptr;
   for (int w = 0; w < 4; ++w) {
     cudaKernelNodeParams kp2 = {};
-    kp2.func = ppr_fn(K, w);
+    kp2.func = ppr_fn(K, w, a.w != nullptr);
     kp2.gridDim = ppr_grid(a, w, sweep_grid);
     kp2.blockDim = dim3(256);
     kp2.kernelParams = w == 2 ? eargs : args;

@@ -210,6 +210,28 @@ class Graph:
                              float(st.ms_per_iter), float(st.bytes_per_iter), float(st.gteps),
                              None if errs is None else errs[: min(int(st.iterations), len(errs))])
 
+    def weighted_page_rank_batched(self, teleports, out, damping_factor=0.85, threshold=1e-6, max_iters=100,
+                                   launch="graph", stream=None) -> PprBatchStats:
+        """k weighted personalised vectors at once (nwgpu_wppr_batched); ``teleports`` and ``out`` are n x k
+        row-major float32 (host arrays or CUDA tensors)."""
+        if len(teleports.shape) != 2 or tuple(out.shape) != tuple(teleports.shape):
+            raise ValueError("teleports and out must be n x k matrices")
+        k = int(teleports.shape[1])
+        (tp, op), dev, keep = self._f32_vectors([teleports.reshape(-1), out.reshape(-1)], [self.n * k, self.n * k])
+        opt = self._options(launch, dev, stream)
+        ci = np.zeros(k, np.uint32)
+        ce = np.zeros(k, np.float64)
+        cc = np.zeros(k, np.int32)
+        st = N.PprStats()
+        st.col_iterations = ci.ctypes.data_as(C.POINTER(C.c_uint32))
+        st.col_errors = ce.ctypes.data_as(C.POINTER(C.c_double))
+        st.col_converged = cc.ctypes.data_as(C.POINTER(C.c_int32))
+        N.check(N.lib().nwgpu_wppr_batched(self.handle, tp, k, op, C.c_float(damping_factor), C.c_float(threshold),
+                                           int(max_iters), C.byref(opt), C.byref(st)))
+        del keep
+        return PprBatchStats(int(st.iterations), bool(st.all_converged), float(st.device_ms), float(st.ms_per_iter),
+                             float(st.bytes_per_iter), ci, ce, cc.astype(bool))
+
     def ppr_batched(self, degrees, seeds, out, damping_factor=0.85, threshold=1e-6, max_iters=100, launch="graph",
                     stream=None) -> PprBatchStats:
         """k personalised vectors at once (nwgpu_ppr_batched); ``out`` is n x k row-major float32."""
