@@ -104,6 +104,15 @@ public:
     return st;
   }
 
+  /// One residual-push solve (page_rank_v13's semantics); returns the engine's statistics.
+  nwgpu_pr_stats run_residual(const std::uint32_t* out_degree, float* ranks, float damping, float threshold,
+                              std::uint64_t max_iters, const nwgpu_pr_options* opt = nullptr) const {
+    nwgpu_pr_stats st{};
+    detail::check(nwgpu_pr_residual_run(h_, out_degree, ranks, damping, threshold, max_iters, opt, &st),
+                  "nwgpu_pr_residual_run");
+    return st;
+  }
+
 private:
   nwgpu_graph* h_ = nullptr;
 };
@@ -197,6 +206,39 @@ void page_rank(const Graph& graph, const std::vector<typename Graph::vertex_id_t
   auto g = resident(graph);
   g->run(reinterpret_cast<const std::uint32_t*>(degrees.data()), page_rank.data(), damping_factor, threshold,
          max_iters);
+}
+
+/**
+ * Drop-in for nw::graph::page_rank_v10 (include/nwgraph/experimental/algorithms/
+ * page_rank.hpp:377-432), the Jacobi solve the engine implements: the same
+ * call as page_rank above.
+ */
+template <gpu_csr_graph Graph, typename Real>
+void page_rank_v10(const Graph& graph, const std::vector<typename Graph::vertex_id_type>& degrees,
+                   std::vector<Real>& page_rank, Real damping_factor, Real threshold, std::size_t max_iters,
+                   std::size_t num_threads) {
+  gpu::page_rank(graph, degrees, page_rank, damping_factor, threshold, max_iters, num_threads);
+}
+
+/**
+ * Drop-in for nw::graph::page_rank_v13 (include/nwgraph/experimental/algorithms/
+ * page_rank.hpp:552-625), the residual-push PageRank: ranks start at 0, every
+ * residual at 1 - d, residuals above threshold are pushed each iteration;
+ * the ranks are not normalised, as in the reference.
+ */
+template <gpu_csr_graph Graph, typename Real>
+void page_rank_v13(const Graph& graph, const std::vector<typename Graph::vertex_id_type>& degrees,
+                   std::vector<Real>& page_rank, Real damping_factor, Real threshold, std::size_t max_iters,
+                   std::size_t num_threads) {
+  static_assert(std::is_same_v<Real, float>, "the B200 engine computes FP32 scores (Real = float)");
+  static_assert(sizeof(typename Graph::vertex_id_type) == 4, "vertex ids must be 32-bit (default_vertex_id_type)");
+  (void)num_threads;
+  const std::size_t n = graph.indices_.size() - 1;
+  if (degrees.size() != n) throw gpu_error(NWGPU_ERR_INVALID_ARG, "degrees.size() != graph.size()");
+  if (page_rank.size() != n) throw gpu_error(NWGPU_ERR_INVALID_ARG, "page_rank.size() != graph.size()");
+  auto g = resident(graph);
+  g->run_residual(reinterpret_cast<const std::uint32_t*>(degrees.data()), page_rank.data(), damping_factor,
+                  threshold, max_iters);
 }
 
 }  // namespace nw::graph::gpu

@@ -68,9 +68,19 @@ int main(int argc, char** argv) {
     std::fprintf(stderr, "size mismatch did not throw\n");
     return 1;
   }
+  // page_rank_v10 is the same Jacobi solve; page_rank_v13 the residual push
+  std::vector<float> v10(g.size()), v13(g.size());
+  nw::graph::gpu::page_rank_v10(g, degrees, v10, 0.85f, 0.0f, 20, 1);
+  if (std::memcmp(ranks.data(), v10.data(), ranks.size() * sizeof(float)) != 0) {
+    std::fprintf(stderr, "page_rank_v10 differs from page_rank\n");
+    return 1;
+  }
+  nw::graph::gpu::page_rank_v13(g, degrees, v13, 0.85f, 1e-4f, 100, 1);
   nw::graph::gpu::release(g);
   std::ofstream out(dir + "/ranks.f32", std::ios::binary);
   out.write(reinterpret_cast<const char*>(ranks.data()), (std::streamsize)(ranks.size() * sizeof(float)));
+  std::ofstream out13(dir + "/ranks_v13.f32", std::ios::binary);
+  out13.write(reinterpret_cast<const char*>(v13.data()), (std::streamsize)(v13.size() * sizeof(float)));
   std::printf("dropin ok n=%zu\n", g.size());
   return 0;
 }

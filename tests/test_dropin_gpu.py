@@ -44,6 +44,10 @@ def test_cpp_dropin_standin_graph(gpu, tmp_path):
     ref, _, _ = O.jacobi_f32(g.row_ptr, g.col, deg, 0.85, 0.0, 20)
     d = np.abs(ranks.astype(np.float64) - ref)
     assert d.max() <= 1e-6 and d.sum() <= 1e-5
+    # gpu::page_rank_v13: the residual push, within a few thresholds of the reference's v13 (restated)
+    v13 = np.fromfile(tmp_path / "ranks_v13.f32", np.float32)
+    r13, _, _ = O.residual_f32(g.row_ptr, g.col, deg, 0.85, 1e-4, 100)
+    assert np.all(np.abs(v13.astype(np.float64) - r13) <= 4e-4 + 1e-5 * np.abs(r13))
 
 
 @pytest.mark.skipif(not os.path.exists(DROPIN_REF), reason="oracle/_ref/dropin_ref not built")
