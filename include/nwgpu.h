@@ -307,6 +307,7 @@ int nwgpu_csr_from_edges(const uint32_t* src, const uint32_t* dst, uint64_t m, u
  * edge_list::deserialize reads (sources and targets, no attributes). */
 #define NWGPU_FILE_MATRIX_MARKET 1
 #define NWGPU_FILE_NW_EDGE_LIST 2
+#define NWGPU_FILE_NW_ADJACENCY 3  /* a serialized adjacency<idx> (adjacency.hpp:176-191): a CSR; see below */
 typedef struct nwgpu_edge_file {
   int32_t  format;     /* NWGPU_FILE_* */
   int32_t  directed;   /* NW: the directedness written in the file; Matrix Market: 1 */
@@ -319,6 +320,12 @@ int nwgpu_edge_file_read(const char* path, uint32_t* src, uint32_t* dst, float* 
                          uint64_t* m, int nthreads);
 int nwgpu_edge_file_write_nw(const char* path, const uint32_t* src, const uint32_t* dst, uint64_t m, uint64_t n,
                              int directed);
+/* A serialized adjacency<idx> (index_adjacency::serialize, adjacency.hpp:
+ * 176-191 over compressed.hpp:377-413) read as its CSR: row_ptr[n + 1], col[nnz]
+ * and, if not NULL, values[nnz] (its first attribute, 1.0 without one). With
+ * row_ptr NULL only *n and *nnz are set. Host code only. */
+int nwgpu_adjacency_file_read(const char* path, uint32_t* row_ptr, uint32_t* col, float* values, uint64_t n_cap,
+                              uint64_t nnz_cap, uint64_t* n, uint64_t* nnz);
 
 /* Seeded RMAT edge list on the device (no counterpart in the reference, which
  * ships no generator): m samples over 2^scale ids, each descending `scale`

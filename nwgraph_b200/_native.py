@@ -80,6 +80,7 @@ class BatchStats(C.Structure):
 
 FILE_MATRIX_MARKET = 1
 FILE_NW_EDGE_LIST = 2
+FILE_NW_ADJACENCY = 3
 
 
 class EdgeFile(C.Structure):
@@ -117,6 +118,8 @@ SIGNATURES = {
     "nwgpu_edge_file_probe": (C.c_int, [C.c_char_p, C.POINTER(EdgeFile)]),
     "nwgpu_edge_file_read": (C.c_int, [C.c_char_p, _vp, _vp, _vp, C.c_uint64, C.POINTER(C.c_uint64), C.c_int]),
     "nwgpu_edge_file_write_nw": (C.c_int, [C.c_char_p, _vp, _vp, C.c_uint64, C.c_uint64, C.c_int]),
+    "nwgpu_adjacency_file_read": (C.c_int, [C.c_char_p, _vp, _vp, _vp, C.c_uint64, C.c_uint64,
+                                            C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "nwgpu_csr_from_edges": (C.c_int, [_vp, _vp, C.c_uint64, C.c_uint64, C.c_uint32, _vp, _vp, C.c_uint64,
                                        C.POINTER(C.c_uint64), _vp, _vp]),
     "nwgpu_rmat_edges": (C.c_int, [C.c_uint32, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_uint64,

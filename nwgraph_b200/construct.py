@@ -174,10 +174,26 @@ def write_nw_edges(path: str, src, dst, n: int, directed: bool = True):
                                              1 if directed else 0))
 
 
+def read_adjacency(path: str):
+    """A serialized NWGraph adjacency file as its CSR (host arrays)."""
+    n, nnz = C.c_uint64(), C.c_uint64()
+    N.check(N.lib().nwgpu_adjacency_file_read(path.encode(), None, None, None, 0, 0, C.byref(n), C.byref(nnz)))
+    rp = np.empty(n.value + 1, np.uint32)
+    cl = np.empty(max(nnz.value, 1), np.uint32)
+    N.check(N.lib().nwgpu_adjacency_file_read(path.encode(), rp.ctypes.data, cl.ctypes.data, None, n.value, nnz.value,
+                                              C.byref(n), C.byref(nnz)))
+    return CSR(rp, cl[: nnz.value].copy())
+
+
 def load_graph(path: str, nthreads: int = 0):
     """The reference driver's graph input (bench/gapbs/common.hpp:83-100 then
     build_adjacency<1>): the file's edge list built into adjacency<1> (row v
     lists the sources of the edges into v, rows sorted) on the GPU. Returns
     ``(CSR, degrees)`` on the host; degrees are build_degrees' out-degrees."""
+    info = N.EdgeFile()
+    N.check(N.lib().nwgpu_edge_file_probe(path.encode(), C.byref(info)))
+    if info.format == N.FILE_NW_ADJACENCY:  # already a CSR
+        g = read_adjacency(path)
+        return g, np.bincount(g.col, minlength=g.n).astype(np.uint32)
     src, dst, n = read_edges(path, nthreads=nthreads)
     return csr_from_edges(src, dst, n, 0)

@@ -21,6 +21,14 @@
 // (int), vertex count (size_t), open flag (bool), then the struct of arrays:
 // edge count, array count, and per array its length, element size and data
 // (sources and targets as uint32, then attributes).
+//
+// NW adjacency (adjacency.hpp:176-191 over compressed.hpp:377-413): vertex
+// count (size_t), open flag (bool), magic "NW GRAPH indexed_struct_of_arrays"
+// (34 bytes), N (8 bytes written from a 4-byte index, so only the low 4 carry
+// the value), the row pointers (length, element size, data), then the struct
+// of arrays of the entries (count, array count, per array length, element
+// size, data: column ids, then attributes). This is a CSR already: it is read
+// into row_ptr / col directly.
 #include <fcntl.h>
 #include <sys/mman.h>
 #include <sys/stat.h>
@@ -284,9 +292,95 @@ int parse_nw(const Mapped& f, NwLayout* L) {
   return NWGPU_OK;
 }
 
+// ---------------------------------------------------------------------------
+// NW binary adjacency
+// ---------------------------------------------------------------------------
+constexpr char   kNwAdjMagic[34] = "NW GRAPH indexed_struct_of_arrays";
+constexpr size_t kNwAdjMagicAt = 8 + 1;
+
+struct AdjLayout {
+  uint64_t n = 0, nnz = 0, arrays = 0;
+  size_t   rp = 0, col = 0, attr = 0;  // data offsets
+  uint64_t attr_size = 0;
+};
+
+bool is_nw_adjacency(const Mapped& f) {
+  return f.size >= kNwAdjMagicAt + sizeof(kNwAdjMagic) &&
+         memcmp(f.p + kNwAdjMagicAt, kNwAdjMagic, sizeof(kNwAdjMagic)) == 0;
+}
+
+int parse_adj(const Mapped& f, AdjLayout* L) {
+  const char* p = f.p;
+  size_t      at = kNwAdjMagicAt + sizeof(kNwAdjMagic);
+  auto        u64 = [&](uint64_t* v) {
+    if (at + 8 > f.size) return false;
+    memcpy(v, p + at, 8);
+    at += 8;
+    return true;
+  };
+  uint64_t N8 = 0, len = 0, el = 0;
+  if (!u64(&N8) || !u64(&len) || !u64(&el)) return fail(NWGPU_ERR_INVALID_GRAPH, "NW adjacency truncated");
+  L->n = N8 & 0xFFFFFFFFull;
+  if (len != L->n + 1 || el != 4) return fail(NWGPU_ERR_UNSUPPORTED, "NW adjacency with %llu row pointers of %llu bytes",
+                                              (unsigned long long)len, (unsigned long long)el);
+  L->rp = at;
+  if (at + 4 * len > f.size) return fail(NWGPU_ERR_INVALID_GRAPH, "NW adjacency truncated");
+  at += 4 * len;
+  if (!u64(&L->nnz) || !u64(&L->arrays) || L->arrays < 1 || L->arrays > 16)
+    return fail(NWGPU_ERR_INVALID_GRAPH, "NW adjacency entries header");
+  for (uint64_t a = 0; a < L->arrays; ++a) {
+    if (!u64(&len) || !u64(&el)) return fail(NWGPU_ERR_INVALID_GRAPH, "NW adjacency truncated");
+    if (len != L->nnz || el == 0 || at + len * el > f.size) return fail(NWGPU_ERR_INVALID_GRAPH, "NW adjacency array %llu",
+                                                                       (unsigned long long)a);
+    if (a == 0 && el != 4) return fail(NWGPU_ERR_UNSUPPORTED, "NW adjacency with %llu-byte column ids", (unsigned long long)el);
+    if (a == 0) L->col = at;
+    if (a == 1) {
+      L->attr = at;
+      L->attr_size = el;
+    }
+    at += len * el;
+  }
+  if (L->n >= 0xFFFFFFF0ull || L->nnz >= 0xFFFFFFF0ull) return fail(NWGPU_ERR_INVALID_GRAPH, "NW adjacency too large");
+  return NWGPU_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int nwgpu_adjacency_file_read(const char* path, uint32_t* row_ptr, uint32_t* col, float* values, uint64_t n_cap,
+                              uint64_t nnz_cap, uint64_t* n_out, uint64_t* nnz_out) {
+  nwgpu::clear_error();
+  if (!n_out || !nnz_out) return fail(NWGPU_ERR_INVALID_ARG, "n / nnz is NULL");
+  Mapped f;
+  int    rc = map_file(path, &f);
+  if (rc) return rc;
+  if (!is_nw_adjacency(f)) return fail(NWGPU_ERR_INVALID_GRAPH, "not an NW Graph adjacency file");
+  AdjLayout L;
+  if ((rc = parse_adj(f, &L))) return rc;
+  *n_out = L.n;
+  *nnz_out = L.nnz;
+  if (!row_ptr) return NWGPU_OK;  // sizes only
+  if (L.n > n_cap || L.nnz > nnz_cap || (L.nnz && !col))
+    return fail(NWGPU_ERR_INVALID_ARG, "the file holds n = %llu, nnz = %llu", (unsigned long long)L.n,
+                (unsigned long long)L.nnz);
+  memcpy(row_ptr, f.p + L.rp, (L.n + 1) * 4);
+  if (L.nnz) memcpy(col, f.p + L.col, L.nnz * 4);
+  if (values) {
+    for (uint64_t e = 0; e < L.nnz; ++e) {
+      if (L.attr_size == 4) {
+        memcpy(values + e, f.p + L.attr + 4 * e, 4);
+      } else if (L.attr_size == 8) {
+        double x;
+        memcpy(&x, f.p + L.attr + 8 * e, 8);
+        values[e] = (float)x;
+      } else {
+        values[e] = 1.0f;
+      }
+    }
+  }
+  return NWGPU_OK;
+}
 
 int nwgpu_edge_file_probe(const char* path, nwgpu_edge_file* info) {
   nwgpu::clear_error();
@@ -295,6 +389,16 @@ int nwgpu_edge_file_probe(const char* path, nwgpu_edge_file* info) {
   Mapped f;
   int    rc = map_file(path, &f);
   if (rc) return rc;
+  if (is_nw_adjacency(f)) {
+    AdjLayout A;
+    if ((rc = parse_adj(f, &A))) return rc;
+    info->format = NWGPU_FILE_NW_ADJACENCY;
+    info->n = A.n;
+    info->max_edges = A.nnz;
+    info->directed = 1;
+    info->has_values = A.attr_size == 4 || A.attr_size == 8;
+    return NWGPU_OK;
+  }
   if (f.size >= 2 && f.p[0] == 'N' && f.p[1] == 'W') {
     NwLayout L;
     if ((rc = parse_nw(f, &L))) return rc;

@@ -111,6 +111,8 @@ def ref(fast: bool = False):
         L.nwref_read_nw_edges.argtypes = L.nwref_read_mm_edges.argtypes
         L.nwref_write_nw_edges.restype = C.c_int
         L.nwref_write_nw_edges.argtypes = [C.c_char_p, _u32p, _u32p, C.c_uint64, C.c_uint64]
+        L.nwref_write_adj1.restype = C.c_int
+        L.nwref_write_adj1.argtypes = [C.c_char_p, _u32p, _u32p, C.c_uint64]
         L.nwref_build_csr.restype = C.c_int
         L.nwref_build_csr.argtypes = [_u32p, _u32p, C.c_uint64, C.c_uint64, C.c_int, _u32p, _u32p, C.c_uint64,
                                       C.POINTER(C.c_uint64)]
@@ -372,6 +374,14 @@ def ref_write_nw_edges(path, src, dst, n):
     d = np.ascontiguousarray(dst, np.uint32)
     if ref().nwref_write_nw_edges(path.encode(), _p(s, _u32p), _p(d, _u32p), len(s), int(n)) != 0:
         raise RuntimeError("nwref_write_nw_edges failed")
+
+
+def ref_write_adj1(path, row_ptr, col):
+    """NWGraph's adjacency<1>::serialize of the CSR (oracle/_ref)."""
+    rp = np.ascontiguousarray(row_ptr, np.uint32)
+    cl = np.ascontiguousarray(col, np.uint32)
+    if ref().nwref_write_adj1(path.encode(), _p(rp, _u32p), _p(cl, _u32p), len(rp) - 1) != 0:
+        raise RuntimeError("nwref_write_adj1 failed")
 
 
 def ref_load_mm(path):

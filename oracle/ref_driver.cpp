@@ -21,6 +21,7 @@
 // (page_rank.hpp:42-52, printed at :142), captured from std::cout.
 #include <cstdint>
 #include <cstring>
+#include <fstream>
 #include <iostream>
 #include <sstream>
 #include <string>
@@ -222,6 +223,18 @@ int nwref_read_nw_edges(const char* path, uint32_t* src, uint32_t* dst, uint64_t
     ++e;
   }
   return 0;
+}
+
+// What adjacency<1>::serialize (adjacency.hpp:180-184) writes for the CSR.
+// That member does not compile in the reference (it is const and calls the
+// non-const indexed_struct_of_arrays::serialize), so this makes its two calls
+// directly on a non-const graph.
+int nwref_write_adj1(const char* path, const uint32_t* row_ptr, const uint32_t* col, uint64_t n) {
+  Adj1          g = make_adj(row_ptr, col, n);
+  std::ofstream out(path, std::ofstream::binary);
+  static_cast<const nw::graph::unipartite_graph_base&>(g).serialize(out);
+  static_cast<nw::graph::indexed_struct_of_arrays<uint32_t, uint32_t>&>(g).serialize(out);
+  return out.good() ? 0 : -1;
 }
 
 // A resident adjacency<1> + degrees, so timing runs do not re-copy the CSR.

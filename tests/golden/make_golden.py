@@ -22,8 +22,9 @@ the reference tree; the GPU host only reads the committed .npz files).
 * ``files/`` and ``loaders.npz`` -- small Matrix Market files written here
   (general with real values and comments, symmetric pattern with self-loops,
   the karate edge list) with the edge lists NWGraph's read_mm<directed> reads
-  from them (io/mmio.hpp:86-103, 171-208), and an NW binary edge list written
-  by NWGraph's edge_list::serialize (edge_list.hpp:237-255) with its edges.
+  from them (io/mmio.hpp:86-103, 171-208), an NW binary edge list written
+  by NWGraph's edge_list::serialize (edge_list.hpp:237-255) with its edges,
+  and the karate adjacency<1> serialized as adjacency.hpp:180-184 writes it.
 
 All reference outputs come from oracle/_ref/libnwref.so, built from the
 reference headers by oracle/Makefile.
@@ -150,6 +151,10 @@ def loader_fixtures(karate_i, karate_j):
         out[f"{name}/src"], out[f"{name}/dst"], out[f"{name}/n"] = s, d, np.array([nn], np.int64)
     s, d = out["general_real/src"], out["general_real/dst"]
     O.ref_write_nw_edges(os.path.join(files, "general_ref.nw"), s, d, n)
+    # the reference's adjacency<1> of the karate edge list, serialized by the reference
+    rp, cl = O.ref_fill_adj1(karate_i, karate_j, 34)
+    O.ref_write_adj1(os.path.join(files, "karate_adj1_ref.nw"), rp, cl)
+    out["karate_adj1/row_ptr"], out["karate_adj1/col"] = rp, cl
     np.savez_compressed(os.path.join(HERE, "loaders.npz"), **out)
     print("loaders:", sorted({k.split("/")[0] for k in out}), "+ general_ref.nw")
 

@@ -113,3 +113,20 @@ def test_bad_files(tmp_path, text, status):
     with pytest.raises(NwgpuError) as ei:
         K.read_edges(str(path))
     assert ei.value.status == status
+
+
+def test_nw_adjacency_file(golden, tmp_path):
+    """A serialized adjacency<1> (adjacency.hpp:180-184, compressed.hpp:377-393)
+    written by the reference is read back as its CSR."""
+    path = os.path.join(FILES, "karate_adj1_ref.nw")
+    info = N.EdgeFile()
+    N.check(N.lib().nwgpu_edge_file_probe(path.encode(), C.byref(info)))
+    assert info.format == N.FILE_NW_ADJACENCY and info.n == 34 and info.max_edges == 156
+    g = K.read_adjacency(path)
+    assert np.array_equal(g.row_ptr, golden["karate_adj1/row_ptr"]) and np.array_equal(g.col, golden["karate_adj1/col"])
+    if O.ref_available():  # larger, straight from the reference
+        from nwgraph_b200 import graphs as G
+        big = G.rmat(12, 16, 5)
+        O.ref_write_adj1(str(tmp_path / "big.nw"), big.row_ptr, big.col)
+        r = K.read_adjacency(str(tmp_path / "big.nw"))
+        assert np.array_equal(r.row_ptr, big.row_ptr) and np.array_equal(r.col, big.col)
