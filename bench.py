@@ -486,11 +486,11 @@ def _time_port(g, deg):
 
 def launches_per_step(args):
     """Kernels one timed step launches: degrees to internal order (relabelled
-    graphs), rank init, the sweeps (one fused kernel each on the binned sweep,
-    sweep + finish on the merge-path one), the CUDA graph's arm kernel, ranks
-    back to input order (relabelled graphs)."""
-    per_sweep = 1 if not args.no_relabel else 2
-    return SWEEPS * per_sweep + 1 + (1 if args.launch == "graph" else 0) + (2 if not args.no_relabel else 0)
+    graphs), rank init, two per sweep (the sweep kernel and its finishing
+    kernel, on the binned and the merge-path sweep alike;
+    profiles/launches_rmat24_pagerank_stream.md lists them), the CUDA graph's
+    arm kernel, ranks back to input order (relabelled graphs)."""
+    return SWEEPS * 2 + 1 + (1 if args.launch == "graph" else 0) + (2 if not args.no_relabel else 0)
 
 
 def run_ours(args):
