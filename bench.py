@@ -487,8 +487,7 @@ def _time_port(g, deg):
 def launches_per_step(args):
     """Kernels one timed step launches: degrees to internal order (relabelled
     graphs), rank init, two per sweep (the sweep kernel and its finishing
-    kernel, on the binned and the merge-path sweep alike;
-    profiles/launches_rmat24_pagerank_stream.md lists them), the CUDA graph's
+    kernel, on the binned and the merge-path sweep alike), the CUDA graph's
     arm kernel, ranks back to input order (relabelled graphs)."""
     return SWEEPS * 2 + 1 + (1 if args.launch == "graph" else 0) + (2 if not args.no_relabel else 0)
 

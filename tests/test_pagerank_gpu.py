@@ -1,6 +1,6 @@
 """Parity of the B200 engine with NWGraph's page_rank, through the C ABI.
 
-Bar (BASELINE north star): FP32 scores within 1e-6 max-abs and 1e-5 L1 of the
+Bar: FP32 scores within 1e-6 max-abs and 1e-5 L1 of the
 reference after a fixed sweep count, the same top-100 order apart from ties
 inside that tolerance, and the same stopping sweep for threshold runs. The
 reference is page_rank_v10 (Jacobi; its outputs are the committed fixtures,
