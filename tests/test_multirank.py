@@ -4,7 +4,7 @@ bench.py --gpus N runs one rank per GPU: each rank solves its own replica,
 the step times are the maximum over ranks (one all-reduce per timing, in the
 same order on every rank), and rank 0 alone prints the JSON line. The
 reference arm runs on rank 0 only; the other ranks exit at once. Both are
-checked here with the launcher the driver uses, on CPU.
+checked here on CPU, launched as bench.py is for N > 1 (torch.distributed.run).
 """
 import json
 import os
