@@ -209,15 +209,20 @@ def cpu_reference_sample(g, deg, sweeps, nthreads):
             "sample": "1 sweep of the C restatement of page_rank_v10 on the full graph (includes init)"}
 
 
-def ppr_batched_vs_looped(scale, k, stream):
+def ppr_batched_vs_looped(scale, k, stream, dist=None):
     """Batched personalised PageRank (k one-hot seeds drawn among vertices with
     out-degree >= 1, per-column L1 < 1e-6, at most 100 sweeps) against k
-    looped single-seed solves on the same engine, all resident in HBM."""
+    looped single-seed solves on the same engine, all resident in HBM. Over
+    several ranks each solves its share of the seeds (even_bounds) with no
+    exchange, and the times are the slowest rank's."""
     import torch
-    from nwgraph_b200 import Graph, graphs as G
+    from nwgraph_b200 import Graph, graphs as G, shard as S
     g = G.rmat(scale, 16, 42)
     deg = g.out_degree()
-    seeds = G.random_sources(deg, k, seed=7)
+    world, rank = (dist.get_world_size(), dist.get_rank()) if dist else (1, 0)
+    cb = S.even_bounds(k, world)
+    seeds = G.random_sources(deg, k, seed=7)[cb[rank]:cb[rank + 1]]
+    k_all, k = k, int(cb[rank + 1] - cb[rank])
     dev = torch.device("cuda")
     rp = torch.from_numpy(g.row_ptr.view(np.int32)).to(dev)
     cl = torch.from_numpy(g.col.view(np.int32)).to(dev)
@@ -246,25 +251,34 @@ def ppr_batched_vs_looped(scale, k, stream):
         for c in range(0, k, 8):
             h.ppr(dg, int(seeds[c]), out_1, DAMPING, 1e-6, 100, stream=stream)
             worst = max(worst, float((out_1 - out_b[:, c]).abs().max()))
-    return {"graph": f"rmat{scale}_ef16", "n": g.n, "nnz": g.nnz, "k": k, "threshold": 1e-6,
+    t_batched, t_looped, worst = max_over_ranks([t_batched, t_looped, worst], dist, dev)
+    return {"graph": f"rmat{scale}_ef16", "n": g.n, "nnz": g.nnz, "k": k_all, "threshold": 1e-6,
+            "columns_per_rank": np.diff(cb).tolist(),
             "batched_ms": t_batched, "looped_ms": t_looped, "speedup": t_looped / t_batched,
             "batched_sweeps": stb.iterations, "looped_sweeps_total": looped_sweeps,
             "all_converged": stb.all_converged, "max_abs_batched_vs_looped": worst}
 
 
-def ragged_batch(num_graphs, max_n, seed=11):
+def ragged_sizes(num_graphs, max_n, seed=11):
+    """Vertex counts (log-uniform in [1e3, max_n]) and RMAT edge factors
+    (U{8..32}) of the ragged configuration's graphs."""
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(np.log(1e3), np.log(max_n), num_graphs)).astype(np.int64)
+    return ns, rng.integers(8, 33, num_graphs)
+
+
+def ragged_batch(num_graphs, max_n, seed=11, graphs=None):
     """The ragged configuration, built on the GPU: n_g log-uniform in
     [1e3, max_n] (seed 11); even graph ids symmetrised RMAT (edge factor
     U{8..32}, scale ceil(log2 n_g), ids taken modulo n_g, self-loops and
     repeats dropped), odd ids floor(sqrt(n_g))^2 4-neighbour grids. Returns the
-    per-graph device CSRs and degrees."""
+    device CSRs and degrees of the graphs ``graphs`` (a range of ids; all of
+    them by default)."""
     import math
     from nwgraph_b200 import construct as K
-    rng = np.random.default_rng(seed)
-    ns = np.exp(rng.uniform(np.log(1e3), np.log(max_n), num_graphs)).astype(np.int64)
-    efs = rng.integers(8, 33, num_graphs)
+    ns, efs = ragged_sizes(num_graphs, max_n, seed)
     parts, degs = [], []
-    for g in range(num_graphs):
+    for g in (range(num_graphs) if graphs is None else graphs):
         n = int(ns[g])
         if g % 2 == 0:
             src, dst = K.rmat_edges(max(1, math.ceil(math.log2(n))), int(efs[g]) * n, seed=seed + g, n=n)
@@ -277,21 +291,28 @@ def ragged_batch(num_graphs, max_n, seed=11):
     return parts, degs
 
 
-def ragged_vs_looped(num_graphs, max_n, stream, sample_mod=16):
+def ragged_vs_looped(num_graphs, max_n, stream, sample_mod=16, dist=None):
     """One ragged-batch solve of every graph (per-graph L1 < 1e-6, at most 200
     sweeps) against looped single-graph solves on the same engine, timed on a
     sample (graph ids = 0 or 1 mod sample_mod: RMAT and grid alike) and
-    scaled to the batch."""
+    scaled to the batch. Over several ranks each builds and solves its own
+    whole graphs (weighted_bounds over the expected rows plus entries) with no
+    exchange; times are the slowest rank's, counts are summed."""
     import torch
-    from nwgraph_b200 import Graph, construct as K
+    from nwgraph_b200 import Graph, construct as K, shard as S
+    world, rank = (dist.get_world_size(), dist.get_rank()) if dist else (1, 0)
+    ns, efs = ragged_sizes(num_graphs, max_n)
+    ids = np.arange(num_graphs)
+    gb = S.weighted_bounds(np.where(ids % 2 == 0, ns * (1 + 2 * efs), 5 * ns), world)
+    mine = range(int(gb[rank]), int(gb[rank + 1]))
     t0 = time.time()
-    parts, degs = ragged_batch(num_graphs, max_n)
+    parts, degs = ragged_batch(num_graphs, max_n, graphs=mine)
     torch.cuda.synchronize()
     build_s = time.time() - t0
     nv = sum(int(p[0].numel()) - 1 for p in parts)
     nnz = sum(int(p[1].numel()) for p in parts)
-    sample = [g for g in range(num_graphs) if g % sample_mod in (0, 1)]
-    kept = [(parts[g][0].clone(), parts[g][1].clone(), degs[g].clone()) for g in sample]
+    sample = [j for j, g in enumerate(mine) if g % sample_mod in (0, 1)]
+    kept = [(parts[j][0].clone(), parts[j][1].clone(), degs[j].clone()) for j in sample]
     b, deg = K.batch_from_device_csrs(parts, degs)
     out = torch.empty(max(b.n, 1), dtype=torch.float32, device="cuda")
     b.page_rank(deg, out, DAMPING, 1e-6, 200, stream=stream)  # warm-up
@@ -316,15 +337,24 @@ def ragged_vs_looped(num_graphs, max_n, stream, sample_mod=16):
             torch.cuda.synchronize()
             looped_ms += e0.elapsed_time(e1)
             looped_swept += float(cl.numel()) * s1.iterations
-    scale = num_graphs / len(sample)
-    return {"graphs": num_graphs, "n_range": [1000, int(max_n)], "vertices": nv, "entries": nnz,
+    scale = len(mine) / max(len(sample), 1)
+    looped_ms *= scale
+    swept, conv = st.entries_swept, st.converged_graphs
+    med = int(np.median(st.graph_iterations))
+    if dist:
+        dev = torch.device("cuda", torch.cuda.current_device())
+        sums = torch.tensor([nv, nnz, swept, conv], dtype=torch.float64, device=dev)
+        dist.all_reduce(sums, group=None)
+        nv, nnz, swept, conv = (int(sums[0]), int(sums[1]), float(sums[2]), int(sums[3]))
+        t_batched, looped_ms, build_s = max_over_ranks([t_batched, looped_ms, build_s], dist, dev)
+    return {"graphs": num_graphs, "graphs_per_rank": np.diff(gb).tolist(), "n_range": [1000, int(max_n)],
+            "vertices": nv, "entries": nnz,
             "threshold": 1e-6, "max_iters": 200, "build_s": build_s, "batched_ms": t_batched,
-            "batched_sweeps": st.sweeps, "converged_graphs": st.converged_graphs,
-            "graph_sweeps_median": int(np.median(st.graph_iterations)), "entries_swept": st.entries_swept,
-            "batched_gteps": st.entries_swept / (t_batched * 1e6),
-            "looped_ms_est": looped_ms * scale, "looped_sample": f"{len(sample)} of {num_graphs} graphs "
-            f"(ids 0, 1 mod {sample_mod}), summed and scaled x{scale:g}",
-            "speedup_est": looped_ms * scale / t_batched}
+            "batched_sweeps_rank0": st.sweeps, "converged_graphs": conv, "graph_sweeps_median_rank0": med,
+            "entries_swept": swept, "batched_gteps": swept / (t_batched * 1e6),
+            "looped_ms_est": looped_ms, "looped_sample": f"graph ids 0, 1 mod {sample_mod} of each rank's "
+            f"graphs, summed and scaled to the rank's graphs (x{scale:g} on rank 0)",
+            "speedup_est": looped_ms / t_batched}
 
 
 def vjp_vs_forward(scale, stream):
@@ -571,10 +601,11 @@ def run_ours(args):
     info = h.info()
     h.release()
     del rp_h, cl_h, deg_h, out_h
-    ppr = ppr_batched_vs_looped(args.ppr_scale, args.ppr_k, stream) if args.ppr_scale > 0 else None
+    ppr = ppr_batched_vs_looped(args.ppr_scale, args.ppr_k, stream, dist) if args.ppr_scale > 0 else None
     vjp = vjp_vs_forward(args.vjp_scale, stream) if args.vjp_scale > 0 else None
     wppr = wppr_batched_vs_looped(args.vjp_scale, 16, stream) if args.vjp_scale > 0 else None
-    ragged = ragged_vs_looped(args.ragged_graphs, args.ragged_max_n, stream) if args.ragged_graphs > 0 else None
+    ragged = (ragged_vs_looped(args.ragged_graphs, args.ragged_max_n, stream, dist=dist)
+              if args.ragged_graphs > 0 else None)
     sharded = row_sharded(g, deg, dev, dist, args.steps) if (world == 1 or args.shard) else None
 
     peak, peak_kind = peaks()

@@ -209,3 +209,165 @@ class ShardedGraph:
 
     def release(self):
         self.shard.release()
+
+
+# ---- batches: personalised columns and whole graphs shard without an exchange per sweep ----
+
+def even_bounds(count: int, world: int) -> np.ndarray:
+    """``world`` contiguous ranges over ``count`` items whose sizes differ by at
+    most one (the first ``count % world`` ranges hold one more). Returns
+    ``bounds[world + 1]`` (int64, from 0 to ``count``)."""
+    q, r = divmod(int(count), int(world))
+    sizes = np.full(int(world), q, np.int64)
+    sizes[:r] += 1
+    return np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+
+
+def weighted_bounds(weights, world: int) -> np.ndarray:
+    """``world`` contiguous ranges of whole items with weight sums as even as
+    whole items allow: cut q falls on the item boundary nearest to q / world
+    of the total weight. Returns ``bounds[world + 1]`` (int64)."""
+    ends = np.concatenate([[0.0], np.cumsum(np.asarray(weights, np.float64))])
+    total = ends[-1]
+    cuts = []
+    for q in range(1, int(world)):
+        t = q * total / world
+        j = int(np.searchsorted(ends, t))  # ends[j - 1] < t <= ends[j]
+        if j > 0 and t - ends[j - 1] <= ends[j] - t:
+            j -= 1
+        cuts.append(j)
+    return np.maximum.accumulate(np.array([0] + cuts + [len(ends) - 1], np.int64))
+
+
+def graph_bounds(vertex_offsets, entry_offsets, world: int) -> np.ndarray:
+    """Graph ranges of a ragged batch over ``world`` ranks: whole graphs,
+    balanced by rows plus entries (the merge-path items its sweep walks)."""
+    vo = np.asarray(vertex_offsets, np.int64)
+    eo = np.asarray(entry_offsets, np.int64)
+    return weighted_bounds(np.diff(vo) + np.diff(eo), world)
+
+
+def batch_slice(vertex_offsets, entry_offsets, row_ptr, col, lo: int, hi: int):
+    """Graphs ``[lo, hi)`` of a batch in the :class:`~nwgraph_b200.GraphBatch`
+    layout, as a batch of their own: ``(vertex_offsets, entry_offsets,
+    row_ptr, col)`` with the offsets rebased to 0 and the arrays sliced
+    (views: a graph's row pointers are local to it, so nothing is rewritten)."""
+    vo = np.asarray(vertex_offsets, np.uint64)
+    eo = np.asarray(entry_offsets, np.uint64)
+    v0, v1, e0, e1 = int(vo[lo]), int(vo[hi]), int(eo[lo]), int(eo[hi])
+    return vo[lo:hi + 1] - vo[lo], eo[lo:hi + 1] - eo[lo], row_ptr[v0 + lo:v1 + hi], col[e0:e1]
+
+
+def gather_rows(local, counts, exchange):
+    """The ranks' ``local`` blocks (rank q's holds ``counts[q]`` rows of one
+    trailing shape) concatenated in rank order, on every rank: each block is
+    padded to the largest count and one equal-size all-gather moves them."""
+    import torch
+    world = len(counts)
+    cmax = max(int(max(counts)), 1)
+    tail = tuple(local.shape[1:])
+    pad = torch.zeros((cmax,) + tail, dtype=local.dtype, device=local.device)
+    pad[:local.shape[0]] = local
+    full = torch.empty(world * pad.numel(), dtype=local.dtype, device=local.device)
+    exchange.gather(full, [pad.reshape(-1)])
+    full = full.view((world, cmax) + tail)
+    return torch.cat([full[q, :int(counts[q])] for q in range(world)], 0)
+
+
+def solve_columns(graph, degrees, seeds, out, bounds, rank: int, damping_factor=0.85, threshold=1e-6,
+                  max_iters=100, stream=None):
+    """Rank ``rank``'s share of a personalised batch: the seeds
+    ``[bounds[rank], bounds[rank + 1])`` solved by ``graph.ppr_batched`` into
+    ``out`` (n x that many, row-major). Returns its stats, or None for an empty
+    share. A converged column is frozen and every column is summed in the same
+    order whatever the other columns are, so the shares are the columns of
+    one whole batch."""
+    lo, hi = int(bounds[rank]), int(bounds[rank + 1])
+    if hi == lo:
+        return None
+    kw = {} if stream is None else {"stream": stream}
+    return graph.ppr_batched(degrees, seeds[lo:hi], out, damping_factor, threshold, max_iters, **kw)
+
+
+@dataclass
+class ShardedPprStats:
+    iterations: int  # the most sweeps any rank ran
+    all_converged: bool
+    device_ms: float  # the slowest rank's solve
+    columns: tuple  # this rank's [lo, hi)
+    col_iterations: np.ndarray  # every column, gathered
+    col_errors: np.ndarray
+    col_converged: np.ndarray
+
+
+def ppr_batched(graph, degrees, seeds, damping_factor=0.85, threshold=1e-6, max_iters=100, group=None,
+                gather=True, stream=None):
+    """Personalised PageRank for ``seeds`` with the columns split over the
+    ranks of ``group``: every rank holds the whole graph, solves its share of
+    the seeds (:func:`even_bounds`) with no exchange between sweeps, and with
+    ``gather`` the n x k row-major result is assembled on every rank at the
+    end (else each rank returns its n x share block). Returns ``(scores,
+    ShardedPprStats)``."""
+    import torch
+    ex = DistExchange(group)
+    k = len(seeds)
+    b = even_bounds(k, ex.world)
+    lo, hi = int(b[ex.rank]), int(b[ex.rank + 1])
+    dev = degrees.device
+    local = torch.empty((graph.n, hi - lo), dtype=torch.float32, device=dev)
+    st = solve_columns(graph, degrees, seeds, local, b, ex.rank, damping_factor, threshold, max_iters, stream)
+    per = torch.zeros((hi - lo, 3), dtype=torch.float64, device=dev)
+    if st is not None:
+        per[:, 0] = torch.from_numpy(np.asarray(st.col_iterations, np.float64))
+        per[:, 1] = torch.from_numpy(np.asarray(st.col_errors, np.float64))
+        per[:, 2] = torch.from_numpy(np.asarray(st.col_converged, np.float64))
+    counts = np.diff(b)
+    per = gather_rows(per, counts, ex).cpu().numpy()
+    mx = torch.tensor([st.iterations if st else 0, st.device_ms if st else 0.0,
+                       0.0 if (st is None or st.all_converged) else 1.0], dtype=torch.float64, device=dev)
+    ex.dist.all_reduce(mx, op=ex.dist.ReduceOp.MAX, group=ex.group)
+    mx = mx.cpu().tolist()
+    stats = ShardedPprStats(int(mx[0]), mx[2] == 0.0, float(mx[1]), (lo, hi), per[:, 0].astype(np.uint32),
+                            per[:, 1].copy(), per[:, 2].astype(bool))
+    if not gather:
+        return local, stats
+    return gather_rows(local.t().contiguous(), counts, ex).t().contiguous(), stats
+
+
+class ShardedBatch:
+    """This rank's graphs of a ragged batch: whole graphs ``[lo, hi)``
+    (:func:`graph_bounds`), solved with no exchange between sweeps. The batch
+    arrays, in the :class:`~nwgraph_b200.GraphBatch` layout, are passed whole on
+    every rank (host arrays or CUDA tensors); the rank keeps a batch of its own
+    graphs. :meth:`page_rank` takes and fills this rank's vertices
+    (``vertex_range`` of the concatenated per-vertex arrays), and
+    :meth:`gather` concatenates every rank's per-vertex results."""
+
+    def __init__(self, vertex_offsets, entry_offsets, row_ptr, col, group=None):
+        from .pagerank import GraphBatch
+        self.exchange = DistExchange(group)
+        self.world, self.rank = self.exchange.world, self.exchange.rank
+        vo = np.asarray(vertex_offsets, np.uint64)
+        eo = np.asarray(entry_offsets, np.uint64)
+        self.bounds = graph_bounds(vo, eo, self.world)
+        lo, hi = int(self.bounds[self.rank]), int(self.bounds[self.rank + 1])
+        self.graphs = (lo, hi)
+        self.vertex_range = (int(vo[lo]), int(vo[hi]))
+        self.vertex_counts = [int(vo[self.bounds[q + 1]] - vo[self.bounds[q]]) for q in range(self.world)]
+        self.batch = GraphBatch(*batch_slice(vo, eo, row_ptr, col, lo, hi)) if hi > lo else None
+
+    def page_rank(self, degrees, page_rank, damping_factor=0.85, threshold=1e-4, max_iters=20, launch="graph",
+                  stream=None):
+        """This rank's graphs solved into ``page_rank`` (this rank's vertices);
+        its RaggedStats, or None when the rank holds no graph."""
+        if self.batch is None:
+            return None
+        return self.batch.page_rank(degrees, page_rank, damping_factor, threshold, max_iters, launch, stream)
+
+    def gather(self, local):
+        """Every rank's per-vertex ``local`` values concatenated in graph order."""
+        return gather_rows(local, self.vertex_counts, self.exchange)
+
+    def release(self):
+        if self.batch is not None:
+            self.batch.release()
