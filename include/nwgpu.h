@@ -418,7 +418,8 @@ int nwgpu_pr_ragged(nwgpu_batch* b, const uint32_t* out_degree, float* ranks, fl
                     uint64_t max_iters, const nwgpu_pr_options* options, nwgpu_batch_stats* stats);
 
 /* Return the device memory that destroyed handles left in the pool to the
- * driver (all devices). Handles still alive keep theirs. */
+ * driver (all devices), and unpin the small host blocks they cached for their
+ * solve states. Handles still alive keep theirs. */
 int nwgpu_release_cached_memory(void);
 
 /* Thread-local message for the last failing call (empty if none). Returns

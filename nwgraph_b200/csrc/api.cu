@@ -7,10 +7,13 @@
 // include/nwgraph/experimental/algorithms/page_rank.hpp:383-431) with one
 // CUDA-graph launch whose while loop runs the sweep and finishing kernels
 // until the device-side test "error < threshold" or max_iters stops it.
+#include <algorithm>
 #include <chrono>
+#include <cstdio>
 #include <cstdlib>
 #include <mutex>
 #include <new>
+#include <vector>
 
 #include <cub/device/device_scan.cuh>
 
@@ -51,6 +54,102 @@ int env_int(const char* name, int dflt) {
   const char* v = getenv(name);
   if (!v || !*v) return dflt;
   return atoi(v);
+}
+
+// Column ids per upload chunk of the streamed build (NWGPU_UPLOAD_CHUNK_ENTRIES
+// overrides; CSRs with at most one chunk of entries are uploaded in one piece).
+constexpr uint64_t kUploadChunkEntries = 32ull << 20;
+constexpr uint64_t kMaxUploadChunks = 256;
+
+// Merge-path row of diagonal d over a host copy of the row pointers: rows
+// [0, i) end before item d (the device's merge_path_row). Indexes [0, n] only.
+uint64_t host_merge_row(const uint32_t* rp, uint64_t n, uint64_t nnz, uint64_t d) {
+  uint64_t lo = d > nnz ? d - nnz : 0, hi = d < n ? d : n;
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if ((uint64_t)rp[mid + 1] + mid + 1 <= d)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+const char* csr_error_text(unsigned int bits, char* buf, size_t len) {
+  snprintf(buf, len, "%s%s%s", (bits & 1u) ? " row_ptr[0] != 0 or row_ptr[n] != nnz;" : "",
+           (bits & 2u) ? " row_ptr decreases;" : "", (bits & 4u) ? " col index >= n;" : "");
+  return buf;
+}
+
+// Upload, validation and relabelling of a host CSR with the column ids still
+// in flight. The row pointers go first and are checked before any kernel
+// indexes with them. The column ids follow in merge-path chunks on a second
+// stream while the rows are sorted, and each chunk's entries are placed in the
+// relabelled CSR (ids checked) as soon as the chunk has arrived. The result is
+// the relabelled CSR of the one-piece path, entry for entry.
+int upload_streamed(nwgpu_graph* g, const uint32_t* h_row_ptr, const uint32_t* h_col, uint64_t n, uint64_t nnz,
+                    uint64_t chunk, PhaseTimer& trace) {
+  cudaStream_t             s = g->stream, cs = nullptr;
+  const uint64_t           C = std::min((nnz + chunk - 1) / chunk, kMaxUploadChunks);
+  std::vector<cudaEvent_t> ev(C, nullptr);
+  std::vector<uint64_t>    dg(C + 1), kk(C + 1);
+  uint32_t *               d_rp = nullptr, *d_col = nullptr;
+  unsigned int*            d_err = nullptr;
+  unsigned int             h_err = 0;
+  char                     why[160];
+  auto                     done = [&](int code) {
+    if (cs) cudaStreamSynchronize(cs);  // no copy may still write d_col when it is freed
+    cudaStreamSynchronize(s);
+    for (cudaEvent_t x : ev)
+      if (x) cudaEventDestroy(x);
+    if (cs) cudaStreamDestroy(cs);
+    pool_free(d_rp, s);
+    pool_free(d_col, s);
+    pool_free(d_err, s);
+    return code;
+  };
+  cudaError_t e;
+  if ((e = dalloc(g, &d_rp, n + 1)) != cudaSuccess || (e = pool_alloc_n(&d_col, nnz + kPad, s)) != cudaSuccess ||
+      (e = pool_alloc_n(&d_err, 1, s)) != cudaSuccess)
+    return done(cuda_fail(e, "cudaMalloc(CSR)"));
+  if ((e = cudaMemsetAsync(d_err, 0, sizeof(unsigned int), s)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(d_rp, h_row_ptr, (n + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+      (e = validate_row_ptr(d_rp, n, nnz, d_err, g->sms, s)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(&h_err, d_err, sizeof(unsigned int), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+    return done(cuda_fail(e, "upload row_ptr"));
+  // Chunk c holds merge-path items [dg[c], dg[c+1]) and so entries [kk[c], kk[c+1]).
+  // Clamped, so the copies stay inside col whatever the row pointers hold;
+  // with valid row pointers the clamps change nothing.
+  for (uint64_t c = 0; c <= C; ++c) {
+    dg[c] = (n + nnz) * c / C;
+    uint64_t k = c == C ? nnz : dg[c] - host_merge_row(h_row_ptr, n, nnz, dg[c]);
+    if (c && k < kk[c - 1]) k = kk[c - 1];
+    kk[c] = k < nnz ? k : nnz;
+  }
+  if ((e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking)) != cudaSuccess) return done(cuda_fail(e, "cudaStreamCreate"));
+  for (uint64_t c = 0; c < C; ++c) {
+    if ((e = cudaEventCreateWithFlags(&ev[c], cudaEventDisableTiming)) != cudaSuccess ||
+        (kk[c + 1] > kk[c] && (e = cudaMemcpyAsync(d_col + kk[c], h_col + kk[c], (kk[c + 1] - kk[c]) * sizeof(uint32_t),
+                                                   cudaMemcpyHostToDevice, cs)) != cudaSuccess) ||
+        (e = cudaEventRecord(ev[c], cs)) != cudaSuccess)
+      return done(cuda_fail(e, "upload col"));
+  }
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return done(cuda_fail(e, "validate row_ptr"));
+  if (h_err) return done(fail(NWGPU_ERR_INVALID_GRAPH, "invalid CSR:%s", csr_error_text(h_err, why, sizeof(why))));
+  trace.mark("upload row_ptr + validate");
+  if ((e = relabel_rows(d_rp, n, nnz, g->sms, false, false, &g->g, s)) != cudaSuccess) return done(cuda_fail(e, "relabel"));
+  for (uint64_t c = 0; c < C; ++c) {
+    if ((e = cudaStreamWaitEvent(s, ev[c], 0)) != cudaSuccess ||
+        (e = scatter_entries(d_rp, d_col, n, nnz, dg[c], dg[c + 1], g->g, d_err, g->sms, s)) != cudaSuccess)
+      return done(cuda_fail(e, "relabel entries"));
+  }
+  if ((e = cudaMemcpyAsync(&h_err, d_err, sizeof(unsigned int), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(s)) != cudaSuccess)
+    return done(cuda_fail(e, "relabel entries"));
+  if (h_err) return done(fail(NWGPU_ERR_INVALID_GRAPH, "invalid CSR:%s", csr_error_text(h_err, why, sizeof(why))));
+  g->relabelled = true;
+  trace.mark("upload col + relabel");
+  return done(NWGPU_OK);
 }
 }  // namespace
 
@@ -111,9 +210,9 @@ int ensure_solve_buffers(nwgpu_graph* g) {
   CK(dalloc(g, &g->res_part, parts > bparts ? parts : bparts), "cudaMalloc(res_part)");
   CK(dalloc(g, &g->st, 1), "cudaMalloc(state)");
   CK(dalloc(g, &g->err_hist, g->err_cap), "cudaMalloc(err_hist)");
-  CK(cudaHostAlloc((void**)&g->h_st, sizeof(PrState), cudaHostAllocDefault), "cudaHostAlloc(state)");
-  CK(cudaHostAlloc((void**)&g->h_abort, sizeof(unsigned int), cudaHostAllocMapped), "cudaHostAlloc(abort)");
-  *g->h_abort = 0;
+  static_assert(sizeof(PrState) <= kHostBlock, "state mirror fits a host block");
+  CK(host_block_get((void**)&g->h_st), "cudaHostAlloc(state)");
+  CK(host_block_get((void**)&g->h_abort), "cudaHostAlloc(abort)");
   CK(cudaHostGetDevicePointer((void**)&g->d_abort, g->h_abort, 0), "cudaHostGetDevicePointer(abort)");
   CK(cudaEventCreate(&g->ev0), "cudaEventCreate");
   CK(cudaEventCreate(&g->ev1), "cudaEventCreate");
@@ -475,6 +574,12 @@ int nwgpu_last_error(char* buf, size_t len) {
   return (int)e.size();
 }
 
+namespace {
+int upload_whole(nwgpu_graph* g, const uint32_t* row_ptr, const uint32_t* col, const float* weights, uint64_t n,
+                 uint64_t nnz, uint32_t flags, cudaMemcpyKind kind, PhaseTimer& trace);
+int finish_create(nwgpu_graph* g, const float* weights, uint32_t flags, nwgpu_graph** out, PhaseTimer& trace);
+}  // namespace
+
 int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float* weights, uint64_t n, uint64_t nnz,
                        uint32_t flags, nwgpu_graph** out) {
   clear_error();
@@ -503,6 +608,27 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
   if (e != cudaSuccess) return bail(cuda_fail(e, "cudaStreamCreate"));
   const cudaMemcpyKind kind = (flags & NWGPU_GRAPH_DEVICE_PTRS) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   PhaseTimer           trace(g->stream);
+  const long           chunk_env = env_int("NWGPU_UPLOAD_CHUNK_ENTRIES", 0);
+  const uint64_t       chunk = chunk_env > 0 ? (uint64_t)chunk_env : kUploadChunkEntries;
+  if (kind == cudaMemcpyHostToDevice && !weights && !(flags & NWGPU_GRAPH_NO_RELABEL) && n > 1 && nnz > chunk) {
+    rc = upload_streamed(g, row_ptr, col, n, nnz, chunk, trace);
+    if (rc) return bail(rc);
+  } else {
+    rc = upload_whole(g, row_ptr, col, weights, n, nnz, flags, kind, trace);
+    if (rc) return bail(rc);
+  }
+  rc = finish_create(g, weights, flags, out, trace);
+  return rc ? bail(rc) : NWGPU_OK;
+}
+
+namespace {
+// The CSR uploaded (or copied from device memory) in one piece, validated,
+// then relabelled unless NWGPU_GRAPH_NO_RELABEL.
+int upload_whole(nwgpu_graph* g, const uint32_t* row_ptr, const uint32_t* col, const float* weights, uint64_t n,
+                 uint64_t nnz, uint32_t flags, cudaMemcpyKind kind, PhaseTimer& trace) {
+  const int   sms = g->sms;
+  cudaError_t e;
+  auto        bail = [](int code) { return code; };
   // Upload into padded buffers.
   Relabelled in;
   auto       free_in = [&]() {
@@ -545,9 +671,8 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
   }
   if (h_err) {
     free_in();
-    return bail(fail(NWGPU_ERR_INVALID_GRAPH, "invalid CSR:%s%s%s",
-                     (h_err & 1u) ? " row_ptr[0] != 0 or row_ptr[n] != nnz;" : "",
-                     (h_err & 2u) ? " row_ptr decreases;" : "", (h_err & 4u) ? " col index >= n;" : ""));
+    char why[160];
+    return bail(fail(NWGPU_ERR_INVALID_GRAPH, "invalid CSR:%s", csr_error_text(h_err, why, sizeof(why))));
   }
   trace.mark("validate");
   if (!(flags & NWGPU_GRAPH_NO_RELABEL) && n > 1) {
@@ -561,6 +686,17 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
     g->g.w = in.w;
   }
   trace.mark("relabel");
+  return NWGPU_OK;
+}
+
+// Launch set-up of a handle whose CSR is in place: tiling, the bin plan, the
+// tuner, the out-row CSR.
+int finish_create(nwgpu_graph* g, const float* weights, uint32_t flags, nwgpu_graph** out, PhaseTimer& trace) {
+  const uint64_t n = g->n, nnz = g->nnz;
+  const int      sms = g->sms;
+  cudaError_t    e;
+  int            rc;
+  auto           bail = [](int code) { return code; };
   // Merge-path sweep (graphs kept in input order, or NWGPU_SWEEP naming a
   // merge-path variant): 256-thread CTAs by default. NWGPU_SWEEP
   // (base|hot|hot512|hot1024x8), NWGPU_IPT, NWGPU_HOT_IDS, NWGPU_CTAS_PER_SM and
@@ -623,6 +759,7 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
   *out = g;
   return NWGPU_OK;
 }
+}  // namespace
 
 int nwgpu_graph_destroy(nwgpu_graph* g) {
   clear_error();

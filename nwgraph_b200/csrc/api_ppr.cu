@@ -13,7 +13,10 @@ void PprBuffers::release(cudaStream_t s) {
   void* ptrs[] = {tiling.tile_row, tiling.tile_nnz, rank, contrib[0], contrib[1], out, cpart, epart, res_part,
                   spans, seeds, seeds_in, col_done, col_conv, col_iters, col_err, st, vbase};
   for (void* p : ptrs) pool_free(p, s);
-  if (h_st) cudaFreeHost(h_st);
+  if (h_st) {
+    cudaStreamSynchronize(s);  // no copy may still target the block when it is reused
+    host_block_put(h_st);
+  }
   *this = PprBuffers();
 }
 
@@ -54,7 +57,8 @@ static int ensure_ppr(nwgpu_graph* g, int K) {
     CK(cudaStreamSynchronize(g->stream), "ppr spans");
     b.num_spans = h_cnt;
   }
-  CK(cudaHostAlloc((void**)&b.h_st, sizeof(PprState), cudaHostAllocDefault), "cudaHostAlloc(ppr state)");
+  static_assert(sizeof(PprState) <= kHostBlock, "state mirror fits a host block");
+  CK(host_block_get((void**)&b.h_st), "cudaHostAlloc(ppr state)");
   CK(cudaStreamSynchronize(g->stream), "ppr buffers");
   b.K = K;
   return NWGPU_OK;

@@ -67,8 +67,8 @@ struct RaggedBatch {
                     rs.err,   rs.conv,  rs.act_off, rs.act_list, st};
     for (void* p : ptrs) pool_free(p, stream);
     if (stream) cudaStreamSynchronize(stream);
-    if (h_st) cudaFreeHost(h_st);
-    if (h_abort) cudaFreeHost(h_abort);
+    host_block_put(h_st);  // the stream is idle: no copy still targets them
+    host_block_put(h_abort);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
@@ -262,9 +262,8 @@ int nwgpu_batch_create(uint64_t num_graphs, const uint64_t* vertex_offsets, cons
   const uint64_t cg = (G + 7) / 8, cap = (uint64_t)sms * 16;
   b->conv_grid = (int)(cg < cap ? cg : cap);
   BK(b->alloc(&b->res_part, (uint64_t)b->conv_grid), "cudaMalloc(res_part)");
-  BK(cudaHostAlloc((void**)&b->h_st, sizeof(PrState), cudaHostAllocDefault), "cudaHostAlloc(state)");
-  BK(cudaHostAlloc((void**)&b->h_abort, sizeof(unsigned int), cudaHostAllocMapped), "cudaHostAlloc(abort)");
-  *b->h_abort = 0;
+  BK(host_block_get((void**)&b->h_st), "cudaHostAlloc(state)");
+  BK(host_block_get((void**)&b->h_abort), "cudaHostAlloc(abort)");
   BK(cudaHostGetDevicePointer((void**)&b->d_abort, b->h_abort, 0), "cudaHostGetDevicePointer(abort)");
   BK(cudaEventCreate(&b->ev0), "cudaEventCreate");
   BK(cudaEventCreate(&b->ev1), "cudaEventCreate");

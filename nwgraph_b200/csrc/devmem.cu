@@ -6,10 +6,13 @@
 // the device; on some machines that cost more than the upload and the solve
 // together. The pool keeps freed blocks mapped, so a program that creates
 // and destroys handles repeatedly (a service answering one graph per request,
-// a benchmark loop) pays the mapping once. nwgpu_release_cached_memory()
-// hands the unused blocks back to the driver.
+// a benchmark loop) pays the mapping once. The small pinned host blocks of
+// the handles' solve states are cached the same way. nwgpu_release_cached_memory()
+// hands the unused blocks of both back to the driver.
 #include <cstdint>
+#include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "handle.h"
 
@@ -57,6 +60,41 @@ void pool_free(void* p, cudaStream_t s) {
   if (p) cudaFreeAsync(p, s);
 }
 
+namespace {
+std::mutex         g_host_mu;
+std::vector<void*> g_host_free;  // cached blocks, each one cudaHostAlloc of kHostBlock bytes
+}  // namespace
+
+cudaError_t host_block_get(void** p) {
+  *p = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_host_mu);
+    if (!g_host_free.empty()) {
+      *p = g_host_free.back();
+      g_host_free.pop_back();
+    }
+  }
+  if (!*p) {
+    cudaError_t e = cudaHostAlloc(p, kHostBlock, cudaHostAllocMapped | cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+      *p = nullptr;
+      return e;
+    }
+  }
+  memset(*p, 0, kHostBlock);
+  return cudaSuccess;
+}
+
+void host_block_put(void* p) {
+  if (!p) return;
+  std::lock_guard<std::mutex> lock(g_host_mu);
+  try {
+    g_host_free.push_back(p);
+  } catch (...) {
+    cudaFreeHost(p);
+  }
+}
+
 }  // namespace nwgpu
 
 extern "C" int nwgpu_release_cached_memory(void) {
@@ -67,5 +105,8 @@ extern "C" int nwgpu_release_cached_memory(void) {
     cudaError_t e = cudaMemPoolTrimTo(nwgpu::g_pools[d], 0);
     if (e != cudaSuccess) return nwgpu::cuda_fail(e, "cudaMemPoolTrimTo");
   }
+  std::lock_guard<std::mutex> hlock(nwgpu::g_host_mu);
+  for (void* p : nwgpu::g_host_free) cudaFreeHost(p);
+  nwgpu::g_host_free.clear();
   return NWGPU_OK;
 }

@@ -149,6 +149,14 @@ cudaError_t pool_alloc_n(T** p, uint64_t count, cudaStream_t s) {
   return pool_alloc(reinterpret_cast<void**>(p), (size_t)count * sizeof(T), s);
 }
 
+// devmem.cu: small mapped pinned blocks (kHostBlock bytes, zeroed) for the
+// host mirrors of solve states and abort words, cached across handles: pinning
+// and unpinning memory costs milliseconds per call. A block goes back with
+// host_block_put only once no copy or kernel can still touch it.
+constexpr size_t kHostBlock = 256;
+cudaError_t host_block_get(void** p);
+void        host_block_put(void* p);
+
 // graph_build.cu
 cudaError_t validate_csr(const uint32_t* d_row_ptr, const uint32_t* d_col, uint64_t n, uint64_t nnz,
                          unsigned int* d_err, int sms, cudaStream_t s);
@@ -156,8 +164,18 @@ cudaError_t build_tiling(const uint32_t* d_row_ptr, uint64_t n, uint64_t nnz, ui
 // Merge-path coordinates into caller-owned tile_row / tile_nnz (num_tiles + 1 each).
 cudaError_t fill_tiling(const uint32_t* d_row_ptr, uint64_t n, uint64_t nnz, uint32_t D, uint32_t num_tiles,
                         uint32_t* tile_row, uint32_t* tile_nnz, cudaStream_t s);
+cudaError_t validate_row_ptr(const uint32_t* d_row_ptr, uint64_t n, uint64_t nnz, unsigned int* d_err, int sms,
+                             cudaStream_t s);
 cudaError_t build_relabelled(const uint32_t* d_row_ptr, const uint32_t* d_col, const float* d_w, uint64_t n,
                              uint64_t nnz, int sms, Relabelled* out, cudaStream_t s);
+// The two halves of build_relabelled for a CSR whose column ids arrive in
+// chunks: relabel_rows needs only the (validated) row pointers; scatter_entries
+// places the entries of merge-path items [d0, d1) of the input CSR once they
+// are on the device, setting bit 2 of *d_err for ids >= n.
+cudaError_t relabel_rows(const uint32_t* d_row_ptr, uint64_t n, uint64_t nnz, int sms, bool with_weights,
+                         bool clear_entries, Relabelled* out, cudaStream_t s);
+cudaError_t scatter_entries(const uint32_t* d_row_ptr, const uint32_t* d_col, uint64_t n, uint64_t nnz, uint64_t d0,
+                            uint64_t d1, const Relabelled& out, unsigned int* d_err, int sms, cudaStream_t s);
 cudaError_t build_transpose(const uint32_t* d_row_ptr, const uint32_t* d_col, const float* d_w, uint64_t n, uint64_t nnz,
                             int sms, Transposed* out, cudaStream_t s);
 

@@ -30,8 +30,9 @@ __global__ void validate_kernel(const uint32_t* __restrict__ row_ptr, const uint
   if (tid == 0 && (row_ptr[0] != 0 || (uint64_t)row_ptr[n] != nnz)) bad |= 1u;
   for (uint64_t i = tid; i < n; i += stride)
     if (row_ptr[i + 1] < row_ptr[i]) bad |= 2u;
-  for (uint64_t k = tid; k < nnz; k += stride)
-    if ((uint64_t)__ldcs(col + k) >= n) bad |= 4u;
+  if (col)
+    for (uint64_t k = tid; k < nnz; k += stride)
+      if ((uint64_t)__ldcs(col + k) >= n) bad |= 4u;
   bad = __reduce_or_sync(kFullMask, bad);
   if ((threadIdx.x & 31) == 0 && bad) atomicOr(err, bad);
 }
@@ -39,6 +40,14 @@ __global__ void validate_kernel(const uint32_t* __restrict__ row_ptr, const uint
 cudaError_t validate_csr(const uint32_t* d_row_ptr, const uint32_t* d_col, uint64_t n, uint64_t nnz,
                          unsigned int* d_err, int sms, cudaStream_t s) {
   validate_kernel<<<sms * 8, 256, 0, s>>>(d_row_ptr, d_col, n, nnz, d_err);
+  return cudaGetLastError();
+}
+
+// The row pointers alone (bits 0 and 1): the streamed build checks them before
+// any kernel indexes with them, while the column ids are still arriving.
+cudaError_t validate_row_ptr(const uint32_t* d_row_ptr, uint64_t n, uint64_t nnz, unsigned int* d_err, int sms,
+                             cudaStream_t s) {
+  validate_kernel<<<sms * 8, 256, 0, s>>>(d_row_ptr, nullptr, n, nnz, d_err);
   return cudaGetLastError();
 }
 
@@ -238,23 +247,76 @@ __global__ void __launch_bounds__(NT) permute_entries_kernel(const uint32_t* __r
   }
 }
 
-// Builds the relabelled copy. On success *out holds freshly allocated
-// row_ptr / col / (weights) / perm / inv arrays padded for 16-byte bulk loads.
-cudaError_t build_relabelled(const uint32_t* d_row_ptr, const uint32_t* d_col, const float* d_w, uint64_t n,
-                             uint64_t nnz, int sms, Relabelled* out, cudaStream_t s) {
+// The input entries of merge-path items [d0, d1) of the input CSR, each
+// copied to its place in the relabelled CSR with its id mapped: entry p of
+// input row o goes to new_row_ptr[perm[o]] + (p - old_row_ptr[o]). Reads the
+// input coalesced, so a chunk can be placed as soon as it has arrived; the
+// row pointers must be valid (validate_row_ptr). Ids >= n set bit 2 of *err
+// and are written as 0, so no load or store leaves its array.
+template <int NT>
+__global__ void __launch_bounds__(NT) scatter_entries_kernel(const uint32_t* __restrict__ old_row_ptr,
+                                                              const uint32_t* __restrict__ old_col, uint64_t n,
+                                                              uint64_t nnz, uint64_t d0, uint64_t d1,
+                                                              const uint32_t* __restrict__ perm,
+                                                              const uint32_t* __restrict__ new_row_ptr,
+                                                              uint32_t* __restrict__ col, unsigned int* err, uint32_t D) {
+  extern __shared__ uint32_t sm[];
+  __shared__ uint32_t        s_pt[2];
+  uint32_t*                  s_old = sm;          // old_row_ptr[i0 + j]
+  uint32_t*                  s_dst = sm + D + 2;  // new start of row i0 + j
+  unsigned int               bad = 0;
+  const uint64_t             tiles = (d1 - d0 + D - 1) / D;
+  for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const uint64_t a = d0 + t * D, b = min(a + (uint64_t)D, d1);
+    if (threadIdx.x < 2) s_pt[threadIdx.x] = merge_path_row(old_row_ptr, n, nnz, threadIdx.x ? b : a);
+    __syncthreads();
+    const uint32_t i0 = s_pt[0], i1 = s_pt[1];
+    const uint64_t k0 = a - i0, k1 = b - i1;
+    // rows i0 .. min(i1, n - 1) hold this tile's entries (at most D + 1 rows)
+    const uint32_t rows = (i1 < n ? i1 : (uint32_t)(n - 1)) - i0 + 1;
+    for (uint32_t j = threadIdx.x; j < rows; j += NT) {
+      s_old[j] = old_row_ptr[i0 + j];
+      s_dst[j] = new_row_ptr[perm[i0 + j]];
+    }
+    __syncthreads();
+    for (uint64_t p = k0 + threadIdx.x; p < k1; p += NT) {
+      uint32_t lo = 0, hi = rows;  // last j with s_old[j] <= p
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (s_old[mid] <= p)
+          lo = mid;
+        else
+          hi = mid;
+      }
+      uint32_t c = __ldcs(old_col + p);
+      if ((uint64_t)c >= n) {
+        bad |= 4u;
+        c = 0u;
+      }
+      col[s_dst[lo] + (p - s_old[lo])] = perm[c];
+    }
+    __syncthreads();
+  }
+  bad = __reduce_or_sync(kFullMask, bad);
+  if ((threadIdx.x & 31) == 0 && bad) atomicOr(err, bad);
+}
+
+// The row half of the relabelling: allocates *out's arrays (row_ptr, col,
+// perm, inv, and w / emap when with_weights) and computes the id maps and the
+// new row pointers. The entries are placed afterwards, all at once
+// (permute_entries_kernel) or chunk by chunk (scatter_entries).
+cudaError_t relabel_rows(const uint32_t* d_row_ptr, uint64_t n, uint64_t nnz, int sms, bool with_weights,
+                         bool clear_entries, Relabelled* out, cudaStream_t s) {
   cudaError_t e;
   uint32_t *cnt = nullptr, *cnt_sorted = nullptr, *ids = nullptr, *new_len = nullptr;
   void*     tmp = nullptr;
   size_t    tmp_bytes = 0, scan_bytes = 0;
-  Tiling    nt{};
   auto      cleanup = [&]() {
     pool_free(cnt, s);
     pool_free(cnt_sorted, s);
     pool_free(ids, s);
     pool_free(new_len, s);
     pool_free(tmp, s);
-    pool_free(nt.tile_row, s);
-    pool_free(nt.tile_nnz, s);
   };
 #define RK(x)                \
   do {                       \
@@ -273,8 +335,11 @@ cudaError_t build_relabelled(const uint32_t* d_row_ptr, const uint32_t* d_col, c
   RK(pool_alloc_n(&out->row_ptr, n + 1 + kPad, s));
   RK(pool_alloc_n(&out->col, nnz + kPad, s));
   RK(cudaMemsetAsync(out->row_ptr, 0, (n + 1 + kPad) * sizeof(uint32_t), s));
-  RK(cudaMemsetAsync(out->col, 0, (nnz + kPad) * sizeof(uint32_t), s));
-  if (d_w) {
+  if (clear_entries)
+    RK(cudaMemsetAsync(out->col, 0, (nnz + kPad) * sizeof(uint32_t), s));
+  else  // every entry is written by the scatter; only the padding is cleared here
+    RK(cudaMemsetAsync(out->col + nnz, 0, kPad * sizeof(uint32_t), s));
+  if (with_weights) {
     RK(pool_alloc_n(&out->w, nnz + kPad, s));
     RK(cudaMemsetAsync(out->w, 0, (nnz + kPad) * sizeof(float), s));
     RK(pool_alloc_n(&out->emap, nnz + kPad, s));
@@ -296,18 +361,42 @@ cudaError_t build_relabelled(const uint32_t* d_row_ptr, const uint32_t* d_col, c
   RK(cudaMemsetAsync(new_len + n, 0, sizeof(uint32_t), s));
   size_t b2 = tmp_bytes;
   RK(cub::DeviceScan::ExclusiveSum(tmp, b2, new_len, out->row_ptr, (int64_t)(n + 1), s));
-  // entries: tile the new CSR and copy each tile's entries
-  const uint32_t D = 2048;
-  RK(build_tiling(out->row_ptr, n, nnz, D, &nt, s));
-  const size_t   smem = (size_t)(2 * D + 4) * sizeof(uint32_t);
-  permute_entries_kernel<kSweepThreads><<<sms * 4, kSweepThreads, smem, s>>>(
-      out->row_ptr, nt.tile_row, nt.tile_nnz, nt.num_tiles, out->inv, out->perm, d_row_ptr, d_col, d_w, out->col,
-      out->w, out->emap, D);
-  RK(cudaGetLastError());
-  RK(cudaStreamSynchronize(s));
   cleanup();
 #undef RK
   return cudaSuccess;
+}
+
+cudaError_t scatter_entries(const uint32_t* d_row_ptr, const uint32_t* d_col, uint64_t n, uint64_t nnz, uint64_t d0,
+                            uint64_t d1, const Relabelled& out, unsigned int* d_err, int sms, cudaStream_t s) {
+  if (d1 <= d0 || n == 0) return cudaSuccess;
+  const uint32_t D = 2048;
+  const size_t   smem = (size_t)(2 * D + 4) * sizeof(uint32_t);
+  const uint64_t tiles = (d1 - d0 + D - 1) / D, cap = (uint64_t)sms * 4;
+  scatter_entries_kernel<kSweepThreads><<<(unsigned)(tiles < cap ? tiles : cap), kSweepThreads, smem, s>>>(
+      d_row_ptr, d_col, n, nnz, d0, d1, out.perm, out.row_ptr, out.col, d_err, D);
+  return cudaGetLastError();
+}
+
+// Builds the relabelled copy. On success *out holds freshly allocated
+// row_ptr / col / (weights) / perm / inv arrays padded for 16-byte bulk loads.
+cudaError_t build_relabelled(const uint32_t* d_row_ptr, const uint32_t* d_col, const float* d_w, uint64_t n,
+                             uint64_t nnz, int sms, Relabelled* out, cudaStream_t s) {
+  cudaError_t e = relabel_rows(d_row_ptr, n, nnz, sms, d_w != nullptr, true, out, s);
+  if (e != cudaSuccess) return e;
+  // entries: tile the new CSR and copy each tile's entries
+  const uint32_t D = 2048;
+  Tiling         nt{};
+  if ((e = build_tiling(out->row_ptr, n, nnz, D, &nt, s)) == cudaSuccess) {
+    const size_t smem = (size_t)(2 * D + 4) * sizeof(uint32_t);
+    permute_entries_kernel<kSweepThreads><<<sms * 4, kSweepThreads, smem, s>>>(
+        out->row_ptr, nt.tile_row, nt.tile_nnz, nt.num_tiles, out->inv, out->perm, d_row_ptr, d_col, d_w, out->col,
+        out->w, out->emap, D);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  }
+  pool_free(nt.tile_row, s);
+  pool_free(nt.tile_nnz, s);
+  return e;
 }
 
 // ---------------------------------------------------------------------------

@@ -152,8 +152,8 @@ struct nwgpu_graph {
                         contrib[1], deg, stage_u32, cpart, epart, res_part, st, err_hist, unit, zero};
     for (void* p : dev_ptrs) nwgpu::pool_free(p, stream);
     cudaStreamSynchronize(stream);  // the blocks are free for the next handle at once
-    if (h_st) cudaFreeHost(h_st);
-    if (h_abort) cudaFreeHost(h_abort);
+    nwgpu::host_block_put(h_st);  // the stream is idle: no copy still targets them
+    nwgpu::host_block_put(h_abort);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
