@@ -211,6 +211,21 @@ __device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src,
   if (!CHUNK && lane == 0) in = load_row_in<MODE>(a, row);
   float  acc = 0.f;
   double res = 0.0;
+  // A finished unit's reduction and epilogue wait one step, until the next
+  // step's gathers are in flight, so the shuffle tree and the update run
+  // under those loads instead of between them (warp-uniform).
+  bool     pending = false;
+  float    acc_done = 0.f;
+  uint32_t unit_done = 0u;
+  RowIn    in_done = no_row_in();
+  auto     finish = [&]() {
+    const float z = warp_sum_lane0(acc_done);
+    if (CHUNK) {
+      if (lane == 0) a.chunk_part[unit_done] = z;
+    } else if (lane == 0) {
+      res += binned_update<MODE>(a, cout, rb + unit_done, z, in_done, src.pol);
+    }
+  };
 #pragma unroll 1
   for (;;) {
     float v[U];
@@ -218,6 +233,10 @@ __device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src,
     for (int q = 0; q < U; ++q) {
       const uint32_t k = base + (uint32_t)lane + (uint32_t)q * 32u;
       v[q] = (k < k1) ? term<HOT, MODE>(a, src, id[q], k) : 0.f;
+    }
+    if (pending) {
+      finish();
+      pending = false;
     }
     // the next step: the rest of this unit, or the first step of the next one
     const bool     more = base + STEP < k1;  // warp-uniform
@@ -228,12 +247,10 @@ __device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src,
 #pragma unroll
     for (int q = 0; q < U; ++q) acc += v[q];
     if (!more) {
-      const float z = warp_sum_lane0(acc);
-      if (CHUNK) {
-        if (lane == 0) a.chunk_part[w] = z;
-      } else if (lane == 0) {
-        res += binned_update<MODE>(a, cout, row, z, in, src.pol);
-      }
+      pending = true;
+      acc_done = acc;
+      unit_done = w;
+      in_done = in;
       acc = 0.f;
       w += nwarps;
       if (w >= nunits) break;
@@ -244,6 +261,7 @@ __device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src,
     }
     base = nbase;
   }
+  if (pending) finish();
   return res;
 }
 
@@ -292,14 +310,31 @@ __device__ __forceinline__ double group_bin(const BinnedArgs& a, const Src& src,
   group_ids<G>(a, rs, len, sub, id);
   group_bounds<G>(a, rb, re_bin, w + nwarps, nunits, lane, nrs, nlen);
   double res = 0.0;
-#pragma unroll 1
-  for (; w < nunits; w += nwarps) {
-    uint32_t row[2];
-    RowIn    in[2];
+  // As in range_bin, a unit's shuffle tree and epilogue wait until the next
+  // unit's gathers are in flight; not in the weighted mode, whose wider
+  // per-row inputs would not fit the register budget.
+  constexpr bool kDefer = MODE != kModeWeighted;
+  bool     pending = false;
+  uint32_t unit_done = 0u;
+  float    acc_done[2] = {0.f, 0.f};
+  RowIn    in_done[2] = {no_row_in(), no_row_in()};
+  auto     finish = [&]() {
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      row[h] = rb + w * (2u * PER) + (uint32_t)h * PER + (uint32_t)lane / G;
-      in[h] = (row[h] < re_bin && sub == 0) ? load_row_in<MODE>(a, row[h]) : no_row_in();
+      float acc = acc_done[h];
+#pragma unroll
+      for (int off = G / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(kFullMask, acc, off);
+      const uint32_t r = rb + unit_done * (2u * PER) + (uint32_t)h * PER + (uint32_t)lane / G;
+      if (r < re_bin && sub == 0) res += binned_update<MODE>(a, cout, r, acc, in_done[h], src.pol);
+    }
+  };
+#pragma unroll 1
+  for (; w < nunits; w += nwarps) {
+    RowIn in[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const uint32_t r = rb + w * (2u * PER) + (uint32_t)h * PER + (uint32_t)lane / G;
+      in[h] = (r < re_bin && sub == 0) ? load_row_in<MODE>(a, r) : no_row_in();
     }
     float v[2][4];
 #pragma unroll
@@ -309,6 +344,7 @@ __device__ __forceinline__ double group_bin(const BinnedArgs& a, const Src& src,
         v[h][q] = ((uint32_t)sub + (uint32_t)q * G < len[h])
                       ? term<HOT, MODE>(a, src, id[h][q], rs[h] + (uint32_t)sub + (uint32_t)q * G)
                       : 0.f;
+    if (kDefer && pending) finish();
     // the next unit's column ids, the bounds of the unit after it
     group_ids<G>(a, nrs, nlen, sub, id);
 #pragma unroll
@@ -322,11 +358,17 @@ __device__ __forceinline__ double group_bin(const BinnedArgs& a, const Src& src,
       float acc = 0.f;
 #pragma unroll
       for (int q = 0; q < 4; ++q) acc += v[h][q];
-#pragma unroll
-      for (int off = G / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(kFullMask, acc, off);
-      if (row[h] < re_bin && sub == 0) res += binned_update<MODE>(a, cout, row[h], acc, in[h], src.pol);
+      acc_done[h] = acc;
+      in_done[h] = in[h];
+    }
+    unit_done = w;
+    pending = true;
+    if (!kDefer) {
+      finish();
+      pending = false;
     }
   }
+  if (pending) finish();
   return res;
 }
 
