@@ -11,7 +11,7 @@ void PprBuffers::release(cudaStream_t s) {
   cg_exec = nullptr;
   cg = nullptr;
   void* ptrs[] = {tiling.tile_row, tiling.tile_nnz, rank, contrib[0], contrib[1], out, cpart, epart, res_part,
-                  spans, seeds, seeds_in, col_done, col_conv, col_iters, col_err, st, vbase};
+                  spans, seeds, seeds_in, col_done, col_conv, col_iters, col_err, st, vbase, slot_map, slot_orig};
   for (void* p : ptrs) pool_free(p, s);
   if (h_st) {
     cudaStreamSynchronize(s);  // no copy may still target the block when it is reused
@@ -43,6 +43,8 @@ static int ensure_ppr(nwgpu_graph* g, int K) {
   CK(dalloc(g, &b.col_iters, (uint64_t)K), "cudaMalloc(col iters)");
   CK(dalloc(g, &b.col_err, (uint64_t)K), "cudaMalloc(col err)");
   CK(dalloc(g, &b.st, 1), "cudaMalloc(ppr state)");
+  CK(dalloc(g, &b.slot_map, (uint64_t)K), "cudaMalloc(ppr slots)");
+  CK(dalloc(g, &b.slot_orig, (uint64_t)K), "cudaMalloc(ppr slots)");
   // rows crossing warp tiles, once per graph (counted in the state's ticket word, reset below)
   CK(dalloc(g, &b.spans, T + 1), "cudaMalloc(ppr spans)");
   {
@@ -151,6 +153,7 @@ extern "C" int nwgpu_ppr_batched(nwgpu_graph* g, const uint32_t* out_degree, con
   h.chunk_end = kGraphChunk;
   h.threshold = (double)threshold;
   h.done = (max_iters == 0) ? 1u : 0u;
+  h.narrow_at = K > 32 ? (unsigned int)(K / 2) : 0u;
   *b.h_st = h;
   CK(cudaMemcpyAsync(b.st, b.h_st, sizeof(PprState), cudaMemcpyHostToDevice, s), "copy ppr state");
   CK(launch_ppr_init(a, K, n, g->sms, s), "ppr init");
@@ -160,11 +163,46 @@ extern "C" int nwgpu_ppr_batched(nwgpu_graph* g, const uint32_t* out_degree, con
 namespace nwgpu {
 // The batched sweep loop from the state on the device, then the output and
 // the per-column stats (both batched entry points).
-int ppr_loop(nwgpu_graph* g, const PprArgs& a, int K, uint32_t k, float* ranks_nxk, float damping, uint64_t max_iters,
+//
+// Narrowing (state narrow_at > 0): once at most narrow_at columns still run,
+// the device loop stops; every column's current ranks go to the output, the
+// running columns move into an n x K/2 layout (K' = 64 or 32), and the solve
+// goes on with the narrower kernels, launched from the host a few sweeps at a
+// time. The gather sums each column in the same order at every K, so the
+// result is the one the wide layout would give, at a fraction of the gather
+// traffic in the sweeps where most columns have stopped.
+int ppr_loop(nwgpu_graph* g, const PprArgs& a0, int K0, uint32_t k, float* ranks_nxk, float damping, uint64_t max_iters,
              const nwgpu_pr_options& opt, nwgpu_ppr_stats* stats, cudaStream_t s) {
-  PprBuffers&    b = g->ppr;
-  const uint64_t n = g->n;
-  const bool     weighted = a.w != nullptr;
+  PprBuffers&     b = g->ppr;
+  const uint64_t  n = g->n;
+  const bool      weighted = a0.w != nullptr;
+  const uint32_t* perm = g->relabelled ? g->g.perm : nullptr;
+  float*          dst = opt.device_ptrs ? ranks_nxk : b.out;
+  PprArgs         a = a0;
+  int             K = K0;
+  bool            narrowed_any = false;
+  // per slot: the caller's column it holds (>= k: padding); per caller's column: its stats
+  uint32_t orig[128], h_iters[128] = {}, h_conv[128] = {};
+  double   h_err[128] = {};
+  for (int j = 0; j < K0; ++j) orig[j] = (uint32_t)j < k ? (uint32_t)j : 0xffffffffu;
+  auto pull_stats = [&](uint32_t* done_out) -> int {
+    uint32_t it[128], cv[128], dn[128];
+    double   er[128];
+    CK(cudaMemcpyAsync(it, a.col_iters, K * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "copy col iters");
+    CK(cudaMemcpyAsync(cv, a.col_conv, K * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "copy col flags");
+    CK(cudaMemcpyAsync(er, a.col_err, K * sizeof(double), cudaMemcpyDeviceToHost, s), "copy col err");
+    CK(cudaMemcpyAsync(dn, a.col_done, K * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "copy col flags");
+    CK(cudaStreamSynchronize(s), "copy col stats");
+    for (int j = 0; j < K; ++j) {
+      if (orig[j] < k) {
+        h_iters[orig[j]] = it[j];
+        h_conv[orig[j]] = cv[j];
+        h_err[orig[j]] = er[j];
+      }
+      if (done_out) done_out[j] = dn[j];
+    }
+    return NWGPU_OK;
+  };
   CK(cudaEventRecord(g->ev0, s), "cudaEventRecord");
   if (opt.launch == NWGPU_LAUNCH_GRAPH) {
     if (!b.cg_exec || b.cg_damping != damping || b.cg_weighted != weighted) {
@@ -195,17 +233,65 @@ int ppr_loop(nwgpu_graph* g, const PprArgs& a, int K, uint32_t k, float* ranks_n
       if (b.h_st->done || launched >= max_iters) break;
     }
   }
+  while (b.h_st->narrowed) {
+    // the columns' current ranks to the output: the stopped ones are final
+    uint32_t done[128], map[128], orig2[128];
+    int      rc = pull_stats(done);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(b.slot_orig, orig, K * sizeof(uint32_t), cudaMemcpyHostToDevice, s), "copy slots");
+    CK(launch_ppr_output_slots(a.rank, perm, n, K, b.slot_orig, k, dst, g->sms, s), "ppr output");
+    uint32_t nact = 0;
+    for (int j = 0; j < K; ++j)
+      if (!done[j]) map[nact++] = (uint32_t)j;
+    const int K2 = ppr_padded_k(nact ? nact : 1);
+    if (K2 >= K) return fail(NWGPU_ERR_CUDA, "narrowing found %u running columns of %d", nact, K);
+    for (int j = 0; j < K2; ++j) orig2[j] = (uint32_t)j < nact ? orig[map[j]] : 0xffffffffu;
+    CK(cudaMemcpyAsync(b.slot_map, map, nact * sizeof(uint32_t), cudaMemcpyHostToDevice, s), "copy slots");
+    // ranks through the idle contribution buffer, then the current contributions into it
+    const uint64_t it = b.h_st->iter;
+    float*         cur = (it & 1ull) ? a.contrib1 : a.contrib0;  // the next sweep's input
+    float*         idle = (it & 1ull) ? a.contrib0 : a.contrib1;
+    CK(launch_ppr_repack(a.rank, idle, n, K, K2, b.slot_map, nact, g->sms, s), "ppr repack");
+    CK(cudaMemcpyAsync(a.rank, idle, n * (uint64_t)K2 * sizeof(float), cudaMemcpyDeviceToDevice, s), "ppr repack");
+    CK(launch_ppr_repack(cur, idle, n, K, K2, b.slot_map, nact, g->sms, s), "ppr repack");
+    CK(launch_ppr_repack_cols(a, K2, b.slot_map, nact, s), "ppr repack");
+    if (it & 1ull) {
+      a.contrib1 = idle;
+      a.contrib0 = cur;
+    } else {
+      a.contrib0 = idle;
+      a.contrib1 = cur;
+    }
+    a.K = (uint32_t)K2;
+    K = K2;
+    for (int j = 0; j < K; ++j) orig[j] = orig2[j];
+    narrowed_any = true;
+    PprState h = *b.h_st;
+    h.done = 0u;
+    h.narrowed = 0u;
+    h.narrow_at = K > 32 ? (unsigned int)(K / 2) : 0u;
+    *b.h_st = h;
+    CK(cudaMemcpyAsync(b.st, b.h_st, sizeof(PprState), cudaMemcpyHostToDevice, s), "copy ppr state");
+    const int grid = ppr_sweep_grid(K, g->sms);
+    for (;;) {  // a few sweeps per check: the narrowed phases are short
+      const uint64_t left = max_iters - b.h_st->iter, batch = left < 4 ? left : 4;
+      for (uint64_t i = 0; i < batch; ++i) CK(launch_ppr_sweep(a, K, grid, s), "ppr sweep");
+      CK(cudaMemcpyAsync(b.h_st, b.st, sizeof(PprState), cudaMemcpyDeviceToHost, s), "copy ppr state");
+      CK(cudaStreamSynchronize(s), "ppr sweep loop");
+      if (b.h_st->done || b.h_st->iter >= max_iters) break;
+    }
+  }
   CK(cudaEventRecord(g->ev1, s), "cudaEventRecord");
-  float* dst = opt.device_ptrs ? ranks_nxk : b.out;
-  CK(launch_ppr_output(b.rank, g->relabelled ? g->g.perm : nullptr, n, K, k, dst, g->sms, s), "ppr output");
+  if (narrowed_any) {
+    CK(cudaMemcpyAsync(b.slot_orig, orig, K * sizeof(uint32_t), cudaMemcpyHostToDevice, s), "copy slots");
+    CK(launch_ppr_output_slots(a.rank, perm, n, K, b.slot_orig, k, dst, g->sms, s), "ppr output");
+  } else {
+    CK(launch_ppr_output(a.rank, perm, n, K, k, dst, g->sms, s), "ppr output");
+  }
   if (!opt.device_ptrs)
     CK(cudaMemcpyAsync(ranks_nxk, dst, n * k * sizeof(float), cudaMemcpyDeviceToHost, s), "copy ranks");
-  uint32_t h_iters[128], h_conv[128];
-  double   h_err[128];
-  CK(cudaMemcpyAsync(h_iters, b.col_iters, K * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "copy col iters");
-  CK(cudaMemcpyAsync(h_conv, b.col_conv, K * sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "copy col flags");
-  CK(cudaMemcpyAsync(h_err, b.col_err, K * sizeof(double), cudaMemcpyDeviceToHost, s), "copy col err");
-  CK(cudaStreamSynchronize(s), "ppr output");
+  int rc = pull_stats(nullptr);  // synchronises the stream
+  if (rc) return rc;
   const PprState fin = *b.h_st;
   if (stats) {
     float ms = 0.f;

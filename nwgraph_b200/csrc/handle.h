@@ -90,6 +90,8 @@ struct PprBuffers {
   float           cg_damping = -1.f;
   bool            cg_weighted = false;
   float*          vbase = nullptr;  // weighted solves: n x K base terms (1 - d) t
+  uint32_t*       slot_map = nullptr;   // narrowing: old slot of each new slot
+  uint32_t*       slot_orig = nullptr;  // caller's column held by each slot (>= k: none)
   void            release(cudaStream_t s);  // returns the buffers to the pool on stream s
 };
 

@@ -16,6 +16,8 @@ struct PprState {
   unsigned int       ticket;
   unsigned int       done;
   unsigned int       aborted;
+  unsigned int       narrow_at;  // stop once at most this many columns still run (0: never), to narrow K
+  unsigned int       narrowed;   // the loop stopped for narrowing, not at the end of the solve
   unsigned int       pad_;
 };
 
@@ -71,6 +73,15 @@ cudaError_t launch_ppr_winit(const PprArgs& a, int K, const float* t_in, uint32_
 cudaError_t launch_ppr_output(const float* rank, const uint32_t* perm, uint64_t n, int K, uint32_t k, float* out,
                               int sms, cudaStream_t s);
 cudaError_t launch_ppr_sweep(const PprArgs& a, int K, int sweep_grid, cudaStream_t s);
+// Narrowing: dst (n x K_to) = the columns map[0, nact) of src (n x K_from), zeros after them.
+cudaError_t launch_ppr_repack(const float* src, float* dst, uint64_t n, int K_from, int K_to, const uint32_t* map,
+                              uint32_t nact, int sms, cudaStream_t s);
+// The per-column state (seeds, flags, sweep counts, errors) of slots map[0, nact) moved to slots [0, nact);
+// slots [nact, K_to) become stopped padding.
+cudaError_t launch_ppr_repack_cols(const PprArgs& a, int K_to, const uint32_t* map, uint32_t nact, cudaStream_t s);
+// out[i * k + slot_orig[j]] = rank[perm[i] * K + j] for the slots j < K whose column is < k.
+cudaError_t launch_ppr_output_slots(const float* rank, const uint32_t* perm, uint64_t n, int K, const uint32_t* slot_orig,
+                                    uint32_t k, float* out, int sms, cudaStream_t s);
 cudaError_t build_ppr_graph(cudaGraph_t g, const PprArgs& proto, int K, int sweep_grid, PprState* st,
                             cudaGraphExec_t* exec);
 

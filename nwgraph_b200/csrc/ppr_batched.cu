@@ -308,13 +308,18 @@ __global__ void __launch_bounds__(256) ppr_finish_kernel(const PprArgs a) {
   __syncthreads();
   if (!s_last || threadIdx.x != 0) return;
   __threadfence();
-  bool all_done = true;
-  for (int q = 0; q < K; ++q) all_done = all_done && *(volatile uint32_t*)&a.col_done[q] != 0u;
+  unsigned int running = 0u;
+  for (int q = 0; q < K; ++q) running += *(volatile uint32_t*)&a.col_done[q] == 0u ? 1u : 0u;
+  const bool               all_done = running == 0u;
   const unsigned long long done_iters = it + 1ull;
   st->iter = done_iters;
   const bool abort = a.abort_word && *a.abort_word;
-  const bool done = all_done || done_iters >= st->max_iters || abort;
+  const bool end = all_done || done_iters >= st->max_iters || abort;
+  // few enough columns still run to continue in a narrower layout: stop here for the host to repack
+  const bool narrow = !end && st->narrow_at != 0u && running <= st->narrow_at;
+  const bool done = end || narrow;
   st->aborted = (abort && !all_done) ? 1u : 0u;
+  st->narrowed = narrow ? 1u : 0u;
   st->done = done ? 1u : 0u;
   st->ticket = 0u;
   __threadfence();
@@ -368,6 +373,56 @@ __global__ void ppr_output_kernel(const float* __restrict__ rank, const uint32_t
   }
 }
 
+// Narrowing. The gather sums every column in the same order whatever K is (the
+// tiles, the rows within a tile and the crossing rows' partials do not depend
+// on it), so moving the running columns into a narrower matrix changes no
+// column's values.
+__global__ void ppr_repack_kernel(const float* __restrict__ src, float* __restrict__ dst, uint64_t n, uint32_t K_from,
+                                  uint32_t K_to, const uint32_t* __restrict__ map, uint32_t nact) {
+  const uint64_t total = n * K_to;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total; x += stride) {
+    const uint64_t i = x / K_to;
+    const uint32_t j = (uint32_t)(x % K_to);
+    dst[x] = j < nact ? src[i * K_from + map[j]] : 0.f;
+  }
+}
+
+// One CTA of 128 threads: every slot's state is read before any is written.
+__global__ void ppr_repack_cols_kernel(PprArgs a, uint32_t K_to, const uint32_t* __restrict__ map, uint32_t nact) {
+  __shared__ uint32_t s_seed[128], s_done[128], s_conv[128], s_iters[128];
+  __shared__ double   s_err[128];
+  const uint32_t      j = threadIdx.x;
+  if (j < nact) {
+    const uint32_t o = map[j];
+    s_seed[j] = a.seeds[o];
+    s_done[j] = a.col_done[o];
+    s_conv[j] = a.col_conv[o];
+    s_iters[j] = a.col_iters[o];
+    s_err[j] = a.col_err[o];
+  }
+  __syncthreads();
+  if (j >= K_to) return;
+  const bool live = j < nact;
+  const_cast<uint32_t*>(a.seeds)[j] = live ? s_seed[j] : 0xffffffffu;
+  a.col_done[j] = live ? s_done[j] : 1u;
+  a.col_conv[j] = live ? s_conv[j] : 0u;
+  a.col_iters[j] = live ? s_iters[j] : 0u;
+  a.col_err[j] = live ? s_err[j] : 0.0;
+}
+
+__global__ void ppr_output_slots_kernel(const float* __restrict__ rank, const uint32_t* __restrict__ perm, uint64_t n,
+                                        uint32_t K, const uint32_t* __restrict__ slot_orig, uint32_t k,
+                                        float* __restrict__ out) {
+  const uint64_t total = n * K;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total; x += stride) {
+    const uint64_t i = x / K;
+    const uint32_t j = (uint32_t)(x % K), c = slot_orig[j];
+    if (c < k) out[i * k + c] = rank[(perm ? (uint64_t)perm[i] : i) * K + j];
+  }
+}
+
 // Column set-up: internal seed ids, padding columns inactive from the start.
 __global__ void ppr_seed_kernel(const uint32_t* __restrict__ seeds_in, uint32_t k, int K,
                                 const uint32_t* __restrict__ perm, PprArgs a) {
@@ -396,6 +451,25 @@ cudaError_t launch_ppr_spans(const uint32_t* row_ptr, const uint32_t* tile_row, 
 cudaError_t launch_ppr_seeds(const uint32_t* seeds_in, uint32_t k, int K, const uint32_t* perm, const PprArgs& a,
                              cudaStream_t s) {
   ppr_seed_kernel<<<1, 128, 0, s>>>(seeds_in, k, K, perm, a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ppr_repack(const float* src, float* dst, uint64_t n, int K_from, int K_to, const uint32_t* map,
+                              uint32_t nact, int sms, cudaStream_t s) {
+  if (K_to <= 0 || K_to > K_from || nact > (uint32_t)K_to) return cudaErrorInvalidValue;
+  ppr_repack_kernel<<<sms * 8, 256, 0, s>>>(src, dst, n, (uint32_t)K_from, (uint32_t)K_to, map, nact);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ppr_repack_cols(const PprArgs& a, int K_to, const uint32_t* map, uint32_t nact, cudaStream_t s) {
+  if (K_to <= 0 || K_to > 128 || nact > (uint32_t)K_to) return cudaErrorInvalidValue;
+  ppr_repack_cols_kernel<<<1, 128, 0, s>>>(a, (uint32_t)K_to, map, nact);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ppr_output_slots(const float* rank, const uint32_t* perm, uint64_t n, int K, const uint32_t* slot_orig,
+                                    uint32_t k, float* out, int sms, cudaStream_t s) {
+  ppr_output_slots_kernel<<<sms * 8, 256, 0, s>>>(rank, perm, n, (uint32_t)K, slot_orig, k, out);
   return cudaGetLastError();
 }
 
