@@ -251,12 +251,17 @@ def ppr_batched_vs_looped(scale, k, stream, dist=None):
         for c in range(0, k, 8):
             h.ppr(dg, int(seeds[c]), out_1, DAMPING, 1e-6, 100, stream=stream)
             worst = max(worst, float((out_1 - out_b[:, c]).abs().max()))
-    t_batched, t_looped, worst = max_over_ranks([t_batched, t_looped, worst], dist, dev)
+    t_batched, t_looped, worst, b_sweeps, not_conv = max_over_ranks(
+        [t_batched, t_looped, worst, stb.iterations, 0.0 if stb.all_converged else 1.0], dist, dev)
+    if dist:  # whole-job sweep count of the looped solves
+        tot = torch.tensor([float(looped_sweeps)], dtype=torch.float64, device=dev)
+        dist.all_reduce(tot)
+        looped_sweeps = int(tot.item())
     return {"graph": f"rmat{scale}_ef16", "n": g.n, "nnz": g.nnz, "k": k_all, "threshold": 1e-6,
             "columns_per_rank": np.diff(cb).tolist(),
             "batched_ms": t_batched, "looped_ms": t_looped, "speedup": t_looped / t_batched,
-            "batched_sweeps": stb.iterations, "looped_sweeps_total": looped_sweeps,
-            "all_converged": stb.all_converged, "max_abs_batched_vs_looped": worst}
+            "batched_sweeps": int(b_sweeps), "looped_sweeps_total": looped_sweeps,
+            "all_converged": not_conv == 0.0, "max_abs_batched_vs_looped": worst}
 
 
 def ragged_sizes(num_graphs, max_n, seed=11):
