@@ -209,7 +209,7 @@ def cpu_reference_sample(g, deg, sweeps, nthreads):
             "sample": "1 sweep of the C restatement of page_rank_v10 on the full graph (includes init)"}
 
 
-def ppr_batched_vs_looped(scale, k, stream, dist=None):
+def ppr_batched_vs_looped(scale, k, stream, dist=None, launch="graph"):
     """Batched personalised PageRank (k one-hot seeds drawn among vertices with
     out-degree >= 1, per-column L1 < 1e-6, at most 100 sweeps) against k
     looped single-seed solves on the same engine, all resident in HBM. Over
@@ -230,19 +230,19 @@ def ppr_batched_vs_looped(scale, k, stream, dist=None):
     out_b = torch.empty((g.n, k), dtype=torch.float32, device=dev)
     out_1 = torch.empty(g.n, dtype=torch.float32, device=dev)
     with Graph(rp, cl) as h:
-        h.ppr_batched(dg, seeds, out_b, DAMPING, 1e-6, 100, stream=stream)  # warm-up
-        h.ppr(dg, int(seeds[0]), out_1, DAMPING, 1e-6, 100, stream=stream)
+        h.ppr_batched(dg, seeds, out_b, DAMPING, 1e-6, 100, stream=stream, launch=launch)  # warm-up
+        h.ppr(dg, int(seeds[0]), out_1, DAMPING, 1e-6, 100, stream=stream, launch=launch)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         e0.record(stream)
-        stb = h.ppr_batched(dg, seeds, out_b, DAMPING, 1e-6, 100, stream=stream)
+        stb = h.ppr_batched(dg, seeds, out_b, DAMPING, 1e-6, 100, stream=stream, launch=launch)
         e1.record(stream)
         torch.cuda.synchronize()
         t_batched = e0.elapsed_time(e1)
         looped_sweeps = 0
         e0.record(stream)
         for c in range(k):
-            st = h.ppr(dg, int(seeds[c]), out_1, DAMPING, 1e-6, 100, stream=stream)
+            st = h.ppr(dg, int(seeds[c]), out_1, DAMPING, 1e-6, 100, stream=stream, launch=launch)
             looped_sweeps += st.iterations
         e1.record(stream)
         torch.cuda.synchronize()
@@ -606,7 +606,8 @@ def run_ours(args):
     info = h.info()
     h.release()
     del rp_h, cl_h, deg_h, out_h
-    ppr = ppr_batched_vs_looped(args.ppr_scale, args.ppr_k, stream, dist) if args.ppr_scale > 0 else None
+    ppr = (ppr_batched_vs_looped(args.ppr_scale, args.ppr_k, stream, dist, launch=args.launch)
+           if args.ppr_scale > 0 else None)
     vjp = vjp_vs_forward(args.vjp_scale, stream) if args.vjp_scale > 0 else None
     wppr = wppr_batched_vs_looped(args.vjp_scale, 16, stream) if args.vjp_scale > 0 else None
     ragged = (ragged_vs_looped(args.ragged_graphs, args.ragged_max_n, stream, dist=dist)
