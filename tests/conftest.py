@@ -62,3 +62,22 @@ def gpu():
     import nwgraph_b200._native as N
     N.lib()
     return True
+
+
+@pytest.fixture
+def nccl_one_rank(gpu):
+    """A one-rank NCCL process group on cuda:0 (the torch.distributed code paths
+    of the sharded entry points, with nothing to wait for), destroyed after the test."""
+    import datetime
+    import socket
+
+    import torch
+    import torch.distributed as dist
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    store = dist.TCPStore("127.0.0.1", port, 1, True)
+    dist.init_process_group("nccl", store=store, rank=0, world_size=1, timeout=datetime.timedelta(seconds=60),
+                            device_id=torch.device("cuda", 0))
+    yield dist.group.WORLD
+    dist.destroy_process_group()

@@ -13,10 +13,6 @@ on one GPU.
 The emulated ranks solve one after another in this process: no kernel waits
 on another.
 """
-import datetime
-import os
-import socket
-
 import numpy as np
 import pytest
 import torch
@@ -86,26 +82,13 @@ def test_graph_shares_equal_the_whole_batch(gpu, world):
         assert np.array_equal(sq.graph_iterations, st.graph_iterations[lo:hi])
 
 
-@pytest.fixture
-def one_rank_group():
-    import torch.distributed as dist
-    with socket.socket() as s:
-        s.bind(("127.0.0.1", 0))
-        port = s.getsockname()[1]
-    store = dist.TCPStore("127.0.0.1", port, 1, True)
-    dist.init_process_group("nccl", store=store, rank=0, world_size=1, timeout=datetime.timedelta(seconds=60),
-                            device_id=torch.device("cuda", 0))
-    yield dist.group.WORLD
-    dist.destroy_process_group()
-
-
-def test_distributed_entry_points_on_one_rank(gpu, ppr_case, one_rank_group):
+def test_distributed_entry_points_on_one_rank(gpu, ppr_case, nccl_one_rank):
     g, deg, seeds = ppr_case
     whole, st = whole_ppr(g, deg, seeds)
     dev = torch.device("cuda", 0)
     deg_d = torch.from_numpy(deg.view(np.int32)).to(dev)
     with Graph(torch.from_numpy(g.row_ptr.view(np.int32)).to(dev), torch.from_numpy(g.col.view(np.int32)).to(dev)) as h:
-        scores, sst = S.ppr_batched(h, deg_d, seeds, D, 1e-6, 100, group=one_rank_group)
+        scores, sst = S.ppr_batched(h, deg_d, seeds, D, 1e-6, 100, group=nccl_one_rank)
     assert np.array_equal(scores.cpu().numpy().view(np.uint32), whole.view(np.uint32))
     assert sst.columns == (0, len(seeds)) and sst.iterations == st.iterations and sst.all_converged
     assert np.array_equal(sst.col_iterations, st.col_iterations)
@@ -115,7 +98,7 @@ def test_distributed_entry_points_on_one_rank(gpu, ppr_case, one_rank_group):
     with GraphBatch(vo, eo, rp, cl) as bt:
         bt.page_rank(dg, ref, D, 1e-6, 200)
     sb = S.ShardedBatch(vo, eo, torch.from_numpy(rp.view(np.int32)).to(dev), torch.from_numpy(cl.view(np.int32)).to(dev),
-                        group=one_rank_group)
+                        group=nccl_one_rank)
     try:
         v0, v1 = sb.vertex_range
         local = torch.empty(v1 - v0, dtype=torch.float32, device=dev)

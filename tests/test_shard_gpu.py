@@ -5,7 +5,9 @@ at a fixed sweep count the sharded ranks equal the single-GPU engine's
 (nwgpu_pr_run) bit for bit. Several shards run here in one process on one GPU
 (LocalExchange: their kernels never wait on one another; the slices are
 copied into the padded layout between sweeps); the exchange over
-torch.distributed is covered on CPU by tests/test_shard.py.
+torch.distributed is covered on CPU by tests/test_shard.py with two gloo ranks,
+and here by ShardedGraph over a one-rank NCCL group (all_gather_into_tensor and
+all_reduce on device buffers).
 """
 import numpy as np
 import pytest
@@ -85,3 +87,20 @@ def test_invalid_bounds(gpu):
     assert ei.value.status == N.ERR_INVALID_ARG
     with pytest.raises(NwgpuError):
         S.GpuShard(g.row_ptr, g.col, 2, 2, bounds, stride)
+
+
+def test_sharded_graph_over_nccl_one_rank(gpu, nccl_one_rank):
+    import torch
+    g = G.rmat(16, 16, 4)
+    deg = g.out_degree()
+    want, _ = single(g, deg, 0.0, 20)
+    dev = torch.device("cuda", 0)
+    sg = S.ShardedGraph(torch.from_numpy(g.row_ptr.view(np.int32)).to(dev),
+                        torch.from_numpy(g.col.view(np.int32)).to(dev), group=nccl_one_rank)
+    try:
+        out = torch.empty(g.n, dtype=torch.float32, device=dev)
+        st = sg.page_rank(torch.from_numpy(deg.view(np.int32)).to(dev), out, 0.85, 0.0, 20)
+    finally:
+        sg.release()
+    assert st.iterations == 20 and len(st.errors) == 20
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), want.view(np.uint32))
