@@ -190,6 +190,17 @@ int nwgpu_ppr_batched(nwgpu_graph* g, const uint32_t* out_degree, const uint32_t
 int nwgpu_wppr_batched(nwgpu_graph* g, const float* teleports, uint32_t k, float* ranks_nxk, float damping,
                        float threshold, uint64_t max_iters, const nwgpu_pr_options* options, nwgpu_ppr_stats* stats);
 
+/* The teleport-matrix form of nwgpu_ppr_batched, for unweighted graphs (no
+ * counterpart in the reference): column c solves
+ *   r_c = (1 - d) t_c + d A^T D^{-1} r_c,  r_c(0) = t_c,
+ * with teleports[n x k] (row-major, input order) and the caller's out-degrees
+ * (D, as in nwgpu_pr_run), and writes ranks_nxk (row-major, input order). A
+ * one-hot column t_c = e_s gives exactly nwgpu_ppr_batched's column for seed s.
+ * Stopping rule, k <= 128 and argument conventions as nwgpu_ppr_batched. */
+int nwgpu_ppr_batched_teleports(nwgpu_graph* g, const uint32_t* out_degree, const float* teleports, uint32_t k,
+                                float* ranks_nxk, float damping, float threshold, uint64_t max_iters,
+                                const nwgpu_pr_options* options, nwgpu_ppr_stats* stats);
+
 /* PageRank without any allocation. No counterpart in the reference.
  *
  * For callers that must not allocate:

@@ -106,6 +106,8 @@ SIGNATURES = {
                                     C.POINTER(PrOptions), C.POINTER(PprStats)]),
     "nwgpu_wppr_batched": (C.c_int, [_vp, _vp, C.c_uint32, _vp, C.c_float, C.c_float, C.c_uint64,
                                      C.POINTER(PrOptions), C.POINTER(PprStats)]),
+    "nwgpu_ppr_batched_teleports": (C.c_int, [_vp, _vp, _vp, C.c_uint32, _vp, C.c_float, C.c_float, C.c_uint64,
+                                              C.POINTER(PrOptions), C.POINTER(PprStats)]),
     "nwgpu_pr_run_noalloc": (C.c_int, [_vp, _vp, C.c_uint64, C.c_uint64, _vp, _vp, C.c_float, C.c_float,
                                        C.c_uint64, _vp, C.POINTER(PrStats)]),
     "nwgpu_abort": (C.c_int, [_vp]),

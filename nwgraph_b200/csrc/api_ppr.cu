@@ -175,7 +175,7 @@ int ppr_loop(nwgpu_graph* g, const PprArgs& a0, int K0, uint32_t k, float* ranks
              const nwgpu_pr_options& opt, nwgpu_ppr_stats* stats, cudaStream_t s) {
   PprBuffers&     b = g->ppr;
   const uint64_t  n = g->n;
-  const bool      weighted = a0.w != nullptr;
+  const int       mode = ppr_mode(a0);
   const uint32_t* perm = g->relabelled ? g->g.perm : nullptr;
   float*          dst = opt.device_ptrs ? ranks_nxk : b.out;
   PprArgs         a = a0;
@@ -205,14 +205,14 @@ int ppr_loop(nwgpu_graph* g, const PprArgs& a0, int K0, uint32_t k, float* ranks
   };
   CK(cudaEventRecord(g->ev0, s), "cudaEventRecord");
   if (opt.launch == NWGPU_LAUNCH_GRAPH) {
-    if (!b.cg_exec || b.cg_damping != damping || b.cg_weighted != weighted) {
+    if (!b.cg_exec || b.cg_damping != damping || b.cg_mode != mode) {
       if (b.cg_exec) cudaGraphExecDestroy(b.cg_exec);
       if (b.cg) cudaGraphDestroy(b.cg);
       b.cg_exec = nullptr;
       CK(cudaGraphCreate(&b.cg, 0), "cudaGraphCreate");
       CK(build_ppr_graph(b.cg, a, K, b.sweep_grid, b.st, &b.cg_exec), "ppr graph");
       b.cg_damping = damping;
-      b.cg_weighted = weighted;
+      b.cg_mode = mode;
     }
     const uint64_t max_launches = max_iters / kGraphChunk + 2;
     for (uint64_t l = 0;; ++l) {
@@ -253,6 +253,11 @@ int ppr_loop(nwgpu_graph* g, const PprArgs& a0, int K0, uint32_t k, float* ranks
     float*         idle = (it & 1ull) ? a.contrib0 : a.contrib1;
     CK(launch_ppr_repack(a.rank, idle, n, K, K2, b.slot_map, nact, g->sms, s), "ppr repack");
     CK(cudaMemcpyAsync(a.rank, idle, n * (uint64_t)K2 * sizeof(float), cudaMemcpyDeviceToDevice, s), "ppr repack");
+    if (a.vbase) {  // teleport vectors: their base terms move with their columns
+      CK(launch_ppr_repack(a.vbase, idle, n, K, K2, b.slot_map, nact, g->sms, s), "ppr repack");
+      CK(cudaMemcpyAsync(const_cast<float*>(a.vbase), idle, n * (uint64_t)K2 * sizeof(float), cudaMemcpyDeviceToDevice, s),
+         "ppr repack");
+    }
     CK(launch_ppr_repack(cur, idle, n, K, K2, b.slot_map, nact, g->sms, s), "ppr repack");
     CK(launch_ppr_repack_cols(a, K2, b.slot_map, nact, s), "ppr repack");
     if (it & 1ull) {
@@ -365,8 +370,64 @@ extern "C" int nwgpu_wppr_batched(nwgpu_graph* g, const float* teleports, uint32
   h.chunk_end = kGraphChunk;
   h.threshold = (double)threshold;
   h.done = (max_iters == 0) ? 1u : 0u;
+  h.narrow_at = K > 32 ? (unsigned int)(K / 2) : 0u;
   *b.h_st = h;
   CK(cudaMemcpyAsync(b.st, b.h_st, sizeof(PprState), cudaMemcpyHostToDevice, s), "copy ppr state");
   CK(launch_ppr_winit(a, K, t, k, g->g.inv, n, b.vbase, g->sms, s), "weighted ppr init");
+  return ppr_loop(g, a, K, k, ranks_nxk, damping, max_iters, opt, stats, s);
+}
+
+extern "C" int nwgpu_ppr_batched_teleports(nwgpu_graph* g, const uint32_t* out_degree, const float* teleports,
+                                           uint32_t k, float* ranks_nxk, float damping, float threshold,
+                                           uint64_t max_iters, const nwgpu_pr_options* options,
+                                           nwgpu_ppr_stats* stats) {
+  clear_error();
+  if (!g) return fail(NWGPU_ERR_INVALID_ARG, "graph is NULL");
+  if (k == 0 || k > 128) return fail(NWGPU_ERR_INVALID_ARG, "k = %u outside [1, 128]", k);
+  if (g->n && (!out_degree || !teleports || !ranks_nxk)) return fail(NWGPU_ERR_INVALID_ARG, "NULL array argument");
+  if (!(damping >= 0.0f && damping <= 1.0f)) return fail(NWGPU_ERR_INVALID_ARG, "damping %g outside [0, 1]", (double)damping);
+  nwgpu_pr_options opt = {};
+  if (options) memcpy(&opt, options, options->size && options->size < sizeof(opt) ? options->size : sizeof(opt));
+  if (opt.launch > NWGPU_LAUNCH_STREAM) return fail(NWGPU_ERR_INVALID_ARG, "launch %u unknown", opt.launch);
+  const int      K = ppr_padded_k(k);
+  const uint64_t n = g->n;
+  if (stats) {
+    uint32_t* ci = stats->col_iterations;
+    double*   ce = stats->col_errors;
+    int32_t*  cc = stats->col_converged;
+    memset(stats, 0, sizeof(*stats));
+    stats->col_iterations = ci;
+    stats->col_errors = ce;
+    stats->col_converged = cc;
+    stats->bytes_per_iter = 4.0 * (double)g->nnz + 4.0 * (double)(n + 1) + 4.0 * (double)n + 20.0 * k * (double)n;
+  }
+  if (n == 0) return NWGPU_OK;
+  int rc = ensure_solve_buffers(g);
+  if (rc) return rc;
+  if ((rc = ensure_ppr(g, K))) return rc;
+  PprBuffers& b = g->ppr;
+  if (!b.vbase) CK(dalloc(g, &b.vbase, n * (uint64_t)K), "cudaMalloc(ppr base terms)");
+  cudaStream_t s = opt.stream ? (cudaStream_t)opt.stream : g->stream;
+  *(volatile unsigned int*)g->h_abort = 0u;
+  if ((rc = load_degrees(g, out_degree, opt.device_ptrs != 0, s))) return rc;
+  // teleports on the device (the output staging holds n x K >= n x k floats)
+  const float* t = teleports;
+  if (!opt.device_ptrs) {
+    CK(cudaMemcpyAsync(b.out, teleports, n * k * sizeof(float), cudaMemcpyHostToDevice, s), "copy teleports");
+    t = b.out;
+  }
+  PprArgs a = make_ppr_args(g, damping);
+  a.vbase = b.vbase;  // base terms and out-degrees, no entry weights (kPprTeleports)
+  CK(cudaMemsetAsync(b.seeds_in, 0, k * sizeof(uint32_t), s), "ppr columns");
+  CK(launch_ppr_seeds(b.seeds_in, k, K, nullptr, a, s), "ppr columns");
+  PprState h = {};
+  h.max_iters = max_iters;
+  h.chunk_end = kGraphChunk;
+  h.threshold = (double)threshold;
+  h.done = (max_iters == 0) ? 1u : 0u;
+  h.narrow_at = K > 32 ? (unsigned int)(K / 2) : 0u;
+  *b.h_st = h;
+  CK(cudaMemcpyAsync(b.st, b.h_st, sizeof(PprState), cudaMemcpyHostToDevice, s), "copy ppr state");
+  CK(launch_ppr_winit(a, K, t, k, g->relabelled ? g->g.inv : nullptr, n, b.vbase, g->sms, s), "ppr teleports init");
   return ppr_loop(g, a, K, k, ranks_nxk, damping, max_iters, opt, stats, s);
 }

@@ -88,7 +88,7 @@ struct PprBuffers {
   cudaGraph_t     cg = nullptr;
   cudaGraphExec_t cg_exec = nullptr;
   float           cg_damping = -1.f;
-  bool            cg_weighted = false;
+  int             cg_mode = -1;  // ppr_mode of the solve baked into cg_exec
   float*          vbase = nullptr;  // weighted solves: n x K base terms (1 - d) t
   uint32_t*       slot_map = nullptr;   // narrowing: old slot of each new slot
   uint32_t*       slot_orig = nullptr;  // caller's column held by each slot (>= k: none)

@@ -7,6 +7,9 @@
 namespace nwgpu {
 
 constexpr int kPprTileItems = 512;  // merge items per warp tile
+// What a batched solve's columns are: one-hot teleports at seeds; teleport
+// vectors on a weighted graph; teleport vectors on an unweighted graph.
+constexpr int kPprSeeds = 0, kPprWeighted = 1, kPprTeleports = 2;
 
 struct PprState {
   unsigned long long iter;
@@ -51,14 +54,15 @@ struct PprArgs {
   int                          use_cond;
   float                        damping;
   float                        one_minus_d;
-  // Weighted solves (w != null): entry weights, base terms (1 - d) t (n x K)
-  // and out-weight sums (n), all in internal order.
+  // Teleport vectors: base terms (1 - d) t (n x K); weighted solves (w != null)
+  // also entry weights and out-weight sums (n), all in internal order.
   const float*                 w;
   const float*                 vbase;
   const float*                 vaux;
 };
 
 int         ppr_padded_k(uint32_t k);
+int         ppr_mode(const PprArgs& a);  // kPprSeeds, kPprWeighted or kPprTeleports
 // Rows crossing warp tiles (spans[count] = (row, first tile, last tile), any order).
 cudaError_t launch_ppr_spans(const uint32_t* row_ptr, const uint32_t* tile_row, const uint32_t* tile_nnz, uint32_t T,
                              uint32_t D, uint4* spans, unsigned int* count, int sms, cudaStream_t s);
@@ -66,8 +70,9 @@ int         ppr_sweep_grid(int K, int sms);
 cudaError_t launch_ppr_seeds(const uint32_t* seeds_in, uint32_t k, int K, const uint32_t* perm, const PprArgs& a,
                              cudaStream_t s);
 cudaError_t launch_ppr_init(const PprArgs& a, int K, uint64_t n, int sms, cudaStream_t s);
-// Weighted start from teleports t_in (n x k row-major, input order; inv:
-// internal -> input id): vbase = (1 - d) t, rank = t, contrib = t / s per column.
+// Start from teleports t_in (n x k row-major, input order; inv: internal ->
+// input id): vbase = (1 - d) t, rank = t, contrib = t / s per column, s the
+// out-weight sums a.vaux, or the out-degrees a.deg when a.vaux is null.
 cudaError_t launch_ppr_winit(const PprArgs& a, int K, const float* t_in, uint32_t k, const uint32_t* inv, uint64_t n,
                              float* vbase, int sms, cudaStream_t s);
 cudaError_t launch_ppr_output(const float* rank, const uint32_t* perm, uint64_t n, int K, uint32_t k, float* out,

@@ -217,11 +217,14 @@ __global__ void __launch_bounds__(256) ppr_fixup_kernel(const PprArgs a) {
 }
 
 // Epilogue, streaming over the n x K matrix, four columns per thread (16-byte
-// loads and stores): for each active column c, r' = (1 - d)[i == seed_c] + d z,
+// loads and stores): for each active column c, r' = (1 - d)[i == seed_c] + d z
+// (or (1 - d) t_ic + d z with teleport vectors),
 // FP64 |r' - r| into per-CTA column partials; converged columns keep their
 // ranks. contrib = r' / deg_i for every column. The grid stride is a multiple
 // of K / 4, so every thread stays on one group of four columns.
-template <int K, bool WEIGHTED>
+// EPI: kPprSeeds (one-hot teleports, out-degrees), kPprWeighted (base terms
+// (1 - d) t, out-weight sums), kPprTeleports (base terms, out-degrees).
+template <int K, int EPI>
 __global__ void __launch_bounds__(256) ppr_epilogue_kernel(const PprArgs a, uint64_t n) {
   constexpr int     C4 = K / 4;
   __shared__ double s_res[256][4];
@@ -249,15 +252,15 @@ __global__ void __launch_bounds__(256) ppr_epilogue_kernel(const PprArgs a, uint
       const float4   z = __ldcs(reinterpret_cast<const float4*>(cout) + x);
       const float4   old = __ldcs(reinterpret_cast<const float4*>(a.rank) + x);
       // weighted: divide by the out-weight sum; the base terms are (1 - d) t
-      const float    dg = WEIGHTED ? __ldg(a.vaux + i) : (float)__ldg(a.deg + i);
+      const float    dg = EPI == kPprWeighted ? __ldg(a.vaux + i) : (float)__ldg(a.deg + i);
       float4         tb = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (WEIGHTED) tb = __ldg(reinterpret_cast<const float4*>(a.vbase) + x);
+      if (EPI != kPprSeeds) tb = __ldg(reinterpret_cast<const float4*>(a.vbase) + x);
       const float    zv[4] = {z.x, z.y, z.z, z.w}, ov[4] = {old.x, old.y, old.z, old.w};
       const float    bv[4] = {tb.x, tb.y, tb.z, tb.w};
       float          nr[4], co[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const float tele = WEIGHTED ? bv[q] : ((seed[q] == i) ? a.one_minus_d : 0.f);
+        const float tele = EPI != kPprSeeds ? bv[q] : ((seed[q] == i) ? a.one_minus_d : 0.f);
         nr[q] = act[q] ? fmaf(a.damping, zv[q], tele) : ov[q];
         co[q] = nr[q] / dg;
         if (act[q]) res[q] += (double)fabsf(nr[q] - ov[q]);
@@ -340,9 +343,10 @@ __global__ void ppr_init_kernel(const PprArgs a, uint64_t n) {
   }
 }
 
-// Weighted start: per column c < k, t = t_in[inv[i] * k + c]; vbase = (1 - d) t,
-// rank = t, contrib = t / s_i (the single weighted solve's start, per column);
-// padding columns are 0.
+// Start from teleport vectors: per column c < k, t = t_in[inv[i] * k + c];
+// vbase = (1 - d) t, rank = t, contrib = t / s_i with s the out-weight sums
+// (weighted graphs: the single weighted solve's start, per column) or the
+// out-degrees (vaux null); padding columns are 0.
 template <int K>
 __global__ void ppr_winit_kernel(const PprArgs a, const float* __restrict__ t_in, uint32_t k,
                                  const uint32_t* __restrict__ inv, uint64_t n, float* __restrict__ vbase) {
@@ -355,7 +359,7 @@ __global__ void ppr_winit_kernel(const PprArgs a, const float* __restrict__ t_in
     const float    t = (c < k) ? t_in[src * k + c] : 0.f;
     vbase[x] = a.one_minus_d * t;
     a.rank[x] = t;
-    a.contrib0[x] = t / a.vaux[i];
+    a.contrib0[x] = t / (a.vaux ? a.vaux[i] : (float)a.deg[i]);
   }
 }
 
@@ -476,26 +480,35 @@ cudaError_t launch_ppr_output_slots(const float* rank, const uint32_t* perm, uin
 __global__ void ppr_arm_kernel(PprState* st) { st->chunk_end = st->iter + kGraphChunk; }
 
 // Rows per group: U * K = 512 floats, 2 KB of rows per group (16 floats per lane).
-template <int K, bool WEIGHTED>
+template <int K, int EPI>
 struct PprKernels {
   static constexpr int U = 512 / K;
   static void*         fn(int which) {
-    return which == 0   ? (void*)ppr_gather_kernel<K, kPprTileItems, U, WEIGHTED>
+    return which == 0   ? (void*)ppr_gather_kernel<K, kPprTileItems, U, EPI == kPprWeighted>
            : which == 1 ? (void*)ppr_fixup_kernel<K>
-           : which == 2 ? (void*)ppr_epilogue_kernel<K, WEIGHTED>
+           : which == 2 ? (void*)ppr_epilogue_kernel<K, EPI>
                         : (void*)ppr_finish_kernel<K>;
   }
 };
 
-// kernel 0 gather, 1 fix-up, 2 epilogue, 3 finish; weighted solves have their own gather and epilogue
-static void* ppr_fn(int K, int which, bool weighted = false) {
+template <int K>
+static void* ppr_fn_k(int which, int mode) {
+  return mode == kPprWeighted    ? PprKernels<K, kPprWeighted>::fn(which)
+         : mode == kPprTeleports ? PprKernels<K, kPprTeleports>::fn(which)
+                                 : PprKernels<K, kPprSeeds>::fn(which);
+}
+
+// kernel 0 gather, 1 fix-up, 2 epilogue, 3 finish, for the solve's mode
+static void* ppr_fn(int K, int which, int mode = kPprSeeds) {
   switch (K) {
-    case 32: return weighted ? PprKernels<32, true>::fn(which) : PprKernels<32, false>::fn(which);
-    case 64: return weighted ? PprKernels<64, true>::fn(which) : PprKernels<64, false>::fn(which);
-    case 128: return weighted ? PprKernels<128, true>::fn(which) : PprKernels<128, false>::fn(which);
+    case 32: return ppr_fn_k<32>(which, mode);
+    case 64: return ppr_fn_k<64>(which, mode);
+    case 128: return ppr_fn_k<128>(which, mode);
     default: return nullptr;
   }
 }
+
+int ppr_mode(const PprArgs& a) { return a.w ? kPprWeighted : (a.vbase ? kPprTeleports : kPprSeeds); }
 
 // Grid of each kernel: gather persistent at its occupancy, fix-up one warp
 // per row crossing tiles, epilogue epi_grid CTAs, finish one warp per column.
@@ -552,7 +565,7 @@ cudaError_t launch_ppr_sweep(const PprArgs& a, int K, int sweep_grid, cudaStream
   for (int w = 0; w < 4; ++w) {
     uint64_t    n = a.n;
     void*       eargs[] = {(void*)&a, (void*)&n};
-    cudaError_t e = cudaLaunchKernel(ppr_fn(K, w, a.w != nullptr), ppr_grid(a, w, sweep_grid), dim3(256),
+    cudaError_t e = cudaLaunchKernel(ppr_fn(K, w, ppr_mode(a)), ppr_grid(a, w, sweep_grid), dim3(256),
                                      w == 2 ? eargs : args, 0, s);
     if (e != cudaSuccess) return e;
   }
@@ -589,7 +602,7 @@ cudaError_t build_ppr_graph(cudaGraph_t g, const PprArgs& proto, int K, int swee
   cudaGraphNode_t      prev = nullptr;
   for (int w = 0; w < 4; ++w) {
     cudaKernelNodeParams kp2 = {};
-    kp2.func = ppr_fn(K, w, a.w != nullptr);
+    kp2.func = ppr_fn(K, w, ppr_mode(a));
     kp2.gridDim = ppr_grid(a, w, sweep_grid);
     kp2.blockDim = dim3(256);
     kp2.kernelParams = w == 2 ? eargs : args;

@@ -232,6 +232,33 @@ class Graph:
         return PprBatchStats(int(st.iterations), bool(st.all_converged), float(st.device_ms), float(st.ms_per_iter),
                              float(st.bytes_per_iter), ci, ce, cc.astype(bool))
 
+    def ppr_batched_teleports(self, degrees, teleports, out, damping_factor=0.85, threshold=1e-6, max_iters=100,
+                              launch="graph", stream=None) -> PprBatchStats:
+        """k personalised vectors with teleport vectors on an unweighted graph (nwgpu_ppr_batched_teleports);
+        ``teleports`` and ``out`` are n x k row-major float32, host arrays or CUDA tensors like ``degrees``."""
+        if len(teleports.shape) != 2 or tuple(out.shape) != tuple(teleports.shape):
+            raise ValueError("teleports and out must be n x k matrices")
+        if len(degrees) != self.n:
+            raise ValueError(f"degrees must have {self.n} entries")
+        k = int(teleports.shape[1])
+        (tp, op), dev, keep = self._f32_vectors([teleports.reshape(-1), out.reshape(-1)], [self.n * k, self.n * k])
+        dp, d_dev, keep_d = _ptr(degrees, np.uint32)
+        if self.n and d_dev != dev:
+            raise ValueError("degrees, teleports and out must all be host arrays or all device tensors")
+        opt = self._options(launch, dev, stream)
+        ci = np.zeros(k, np.uint32)
+        ce = np.zeros(k, np.float64)
+        cc = np.zeros(k, np.int32)
+        st = N.PprStats()
+        st.col_iterations = ci.ctypes.data_as(C.POINTER(C.c_uint32))
+        st.col_errors = ce.ctypes.data_as(C.POINTER(C.c_double))
+        st.col_converged = cc.ctypes.data_as(C.POINTER(C.c_int32))
+        N.check(N.lib().nwgpu_ppr_batched_teleports(self.handle, dp, tp, k, op, C.c_float(damping_factor),
+                                                    C.c_float(threshold), int(max_iters), C.byref(opt), C.byref(st)))
+        del keep, keep_d
+        return PprBatchStats(int(st.iterations), bool(st.all_converged), float(st.device_ms), float(st.ms_per_iter),
+                             float(st.bytes_per_iter), ci, ce, cc.astype(bool))
+
     def ppr_batched(self, degrees, seeds, out, damping_factor=0.85, threshold=1e-6, max_iters=100, launch="graph",
                     stream=None) -> PprBatchStats:
         """k personalised vectors at once (nwgpu_ppr_batched); ``out`` is n x k row-major float32."""
