@@ -43,3 +43,32 @@ def test_narrowed_batch_equals_32_column_batches(gpu, graph, k, iters):
             assert np.array_equal(sp.col_converged, st.col_converged[c0:c0 + 32])
         again, s2 = solve(h, deg, seeds, iters, launch="stream")
     assert np.array_equal(again.view(np.uint32), whole.view(np.uint32)) and s2.iterations == st.iterations
+
+
+def test_abort_in_a_narrowed_phase(gpu):
+    """39 seeds on isolated vertices stop exactly at their second sweep; the
+    40th, on a bipartite grid with d = 1, oscillates and never stops. The loop
+    narrows right away and then runs in its narrowed phase until aborted."""
+    import threading
+    import time
+
+    from nwgraph_b200 import NwgpuError
+    from nwgraph_b200 import _native as N
+    grid = G.grid(10000)
+    iso = 39
+    rp = np.concatenate([grid.row_ptr, np.full(iso, grid.row_ptr[-1], np.uint32)])
+    n = len(rp) - 1
+    deg = np.concatenate([grid.out_degree(), np.zeros(iso, np.uint32)])
+    seeds = np.concatenate([np.arange(grid.n, n), [grid.n // 2]]).astype(np.uint32)
+    out = np.empty((n, len(seeds)), np.float32)
+    with Graph(rp, grid.col) as h:
+        t = threading.Timer(0.5, h.abort)
+        t.start()
+        t0 = time.time()
+        with pytest.raises(NwgpuError) as ei:
+            h.ppr_batched(deg, seeds, out, 1.0, 1e-30, 2_000_000)
+        t.join()
+        assert ei.value.status == N.ERR_ABORTED
+        assert time.time() - t0 < 30
+        st = h.ppr_batched(deg, seeds[:4], np.empty((n, 4), np.float32), 0.85, 1e-6, 100)  # still usable
+        assert st.all_converged
