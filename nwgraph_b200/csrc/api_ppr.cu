@@ -318,16 +318,23 @@ int ppr_loop(nwgpu_graph* g, const PprArgs& a0, int K0, uint32_t k, float* ranks
 }
 }  // namespace nwgpu
 
-extern "C" int nwgpu_wppr_batched(nwgpu_graph* g, const float* teleports, uint32_t k, float* ranks_nxk, float damping,
-                                  float threshold, uint64_t max_iters, const nwgpu_pr_options* options,
-                                  nwgpu_ppr_stats* stats) {
-  clear_error();
+namespace nwgpu {
+// Both teleport-matrix forms of the batched solve. Weighted: entry weights in
+// the gather, out-weight sums as divisors. Unweighted: the caller's
+// out-degrees as divisors. Column c starts at t_c with base terms
+// (1 - d) t_c; the padding columns are stopped from the start.
+static int teleport_batched(nwgpu_graph* g, bool weighted, const uint32_t* out_degree, const float* teleports,
+                            uint32_t k, float* ranks_nxk, float damping, float threshold, uint64_t max_iters,
+                            const nwgpu_pr_options* options, nwgpu_ppr_stats* stats) {
   if (!g) return fail(NWGPU_ERR_INVALID_ARG, "graph is NULL");
   if (k == 0 || k > 128) return fail(NWGPU_ERR_INVALID_ARG, "k = %u outside [1, 128]", k);
-  if (g->n && (!teleports || !ranks_nxk)) return fail(NWGPU_ERR_INVALID_ARG, "NULL array argument");
+  if (g->n && (!teleports || !ranks_nxk || (!weighted && !out_degree)))
+    return fail(NWGPU_ERR_INVALID_ARG, "NULL array argument");
   if (!(damping >= 0.0f && damping <= 1.0f)) return fail(NWGPU_ERR_INVALID_ARG, "damping %g outside [0, 1]", (double)damping);
-  if (!g->g.w) return fail(NWGPU_ERR_UNSUPPORTED, "the graph has no edge weights (pass them to nwgpu_graph_create)");
-  if (!g->relabelled || !g->plan.ok) return fail(NWGPU_ERR_UNSUPPORTED, "weighted solves need a relabelled graph");
+  if (weighted && !g->g.w)
+    return fail(NWGPU_ERR_UNSUPPORTED, "the graph has no edge weights (pass them to nwgpu_graph_create)");
+  if (weighted && (!g->relabelled || !g->plan.ok))
+    return fail(NWGPU_ERR_UNSUPPORTED, "weighted solves need a relabelled graph");
   nwgpu_pr_options opt = {};
   if (options) memcpy(&opt, options, options->size && options->size < sizeof(opt) ? options->size : sizeof(opt));
   if (opt.launch > NWGPU_LAUNCH_STREAM) return fail(NWGPU_ERR_INVALID_ARG, "launch %u unknown", opt.launch);
@@ -341,17 +348,19 @@ extern "C" int nwgpu_wppr_batched(nwgpu_graph* g, const float* teleports, uint32
     stats->col_iterations = ci;
     stats->col_errors = ce;
     stats->col_converged = cc;
-    stats->bytes_per_iter = 8.0 * (double)g->nnz + 4.0 * (double)(n + 1) + 4.0 * (double)n + 20.0 * k * (double)n;
+    stats->bytes_per_iter =
+        (weighted ? 8.0 : 4.0) * (double)g->nnz + 4.0 * (double)(n + 1) + 4.0 * (double)n + 20.0 * k * (double)n;
   }
   if (n == 0) return NWGPU_OK;
   int rc = ensure_solve_buffers(g);
   if (rc) return rc;
-  if ((rc = ensure_wpr(g))) return rc;  // out-weight sums (internal order)
+  if (weighted && (rc = ensure_wpr(g))) return rc;  // out-weight sums (internal order)
   if ((rc = ensure_ppr(g, K))) return rc;
   PprBuffers& b = g->ppr;
   if (!b.vbase) CK(dalloc(g, &b.vbase, n * (uint64_t)K), "cudaMalloc(ppr base terms)");
   cudaStream_t s = opt.stream ? (cudaStream_t)opt.stream : g->stream;
   *(volatile unsigned int*)g->h_abort = 0u;
+  if (!weighted && (rc = load_degrees(g, out_degree, opt.device_ptrs != 0, s))) return rc;
   // teleports on the device (the output staging holds n x K >= n x k floats)
   const float* t = teleports;
   if (!opt.device_ptrs) {
@@ -359,65 +368,11 @@ extern "C" int nwgpu_wppr_batched(nwgpu_graph* g, const float* teleports, uint32
     t = b.out;
   }
   PprArgs a = make_ppr_args(g, damping);
-  a.w = g->g.w;
   a.vbase = b.vbase;
-  a.vaux = g->wpr.t.s;
-  // columns: the first k active, the padding ones stopped from the start
-  CK(cudaMemsetAsync(b.seeds_in, 0, k * sizeof(uint32_t), s), "ppr columns");
-  CK(launch_ppr_seeds(b.seeds_in, k, K, nullptr, a, s), "ppr columns");
-  PprState h = {};
-  h.max_iters = max_iters;
-  h.chunk_end = kGraphChunk;
-  h.threshold = (double)threshold;
-  h.done = (max_iters == 0) ? 1u : 0u;
-  h.narrow_at = K > 32 ? (unsigned int)(K / 2) : 0u;
-  *b.h_st = h;
-  CK(cudaMemcpyAsync(b.st, b.h_st, sizeof(PprState), cudaMemcpyHostToDevice, s), "copy ppr state");
-  CK(launch_ppr_winit(a, K, t, k, g->g.inv, n, b.vbase, g->sms, s), "weighted ppr init");
-  return ppr_loop(g, a, K, k, ranks_nxk, damping, max_iters, opt, stats, s);
-}
-
-extern "C" int nwgpu_ppr_batched_teleports(nwgpu_graph* g, const uint32_t* out_degree, const float* teleports,
-                                           uint32_t k, float* ranks_nxk, float damping, float threshold,
-                                           uint64_t max_iters, const nwgpu_pr_options* options,
-                                           nwgpu_ppr_stats* stats) {
-  clear_error();
-  if (!g) return fail(NWGPU_ERR_INVALID_ARG, "graph is NULL");
-  if (k == 0 || k > 128) return fail(NWGPU_ERR_INVALID_ARG, "k = %u outside [1, 128]", k);
-  if (g->n && (!out_degree || !teleports || !ranks_nxk)) return fail(NWGPU_ERR_INVALID_ARG, "NULL array argument");
-  if (!(damping >= 0.0f && damping <= 1.0f)) return fail(NWGPU_ERR_INVALID_ARG, "damping %g outside [0, 1]", (double)damping);
-  nwgpu_pr_options opt = {};
-  if (options) memcpy(&opt, options, options->size && options->size < sizeof(opt) ? options->size : sizeof(opt));
-  if (opt.launch > NWGPU_LAUNCH_STREAM) return fail(NWGPU_ERR_INVALID_ARG, "launch %u unknown", opt.launch);
-  const int      K = ppr_padded_k(k);
-  const uint64_t n = g->n;
-  if (stats) {
-    uint32_t* ci = stats->col_iterations;
-    double*   ce = stats->col_errors;
-    int32_t*  cc = stats->col_converged;
-    memset(stats, 0, sizeof(*stats));
-    stats->col_iterations = ci;
-    stats->col_errors = ce;
-    stats->col_converged = cc;
-    stats->bytes_per_iter = 4.0 * (double)g->nnz + 4.0 * (double)(n + 1) + 4.0 * (double)n + 20.0 * k * (double)n;
+  if (weighted) {
+    a.w = g->g.w;
+    a.vaux = g->wpr.t.s;
   }
-  if (n == 0) return NWGPU_OK;
-  int rc = ensure_solve_buffers(g);
-  if (rc) return rc;
-  if ((rc = ensure_ppr(g, K))) return rc;
-  PprBuffers& b = g->ppr;
-  if (!b.vbase) CK(dalloc(g, &b.vbase, n * (uint64_t)K), "cudaMalloc(ppr base terms)");
-  cudaStream_t s = opt.stream ? (cudaStream_t)opt.stream : g->stream;
-  *(volatile unsigned int*)g->h_abort = 0u;
-  if ((rc = load_degrees(g, out_degree, opt.device_ptrs != 0, s))) return rc;
-  // teleports on the device (the output staging holds n x K >= n x k floats)
-  const float* t = teleports;
-  if (!opt.device_ptrs) {
-    CK(cudaMemcpyAsync(b.out, teleports, n * k * sizeof(float), cudaMemcpyHostToDevice, s), "copy teleports");
-    t = b.out;
-  }
-  PprArgs a = make_ppr_args(g, damping);
-  a.vbase = b.vbase;  // base terms and out-degrees, no entry weights (kPprTeleports)
   CK(cudaMemsetAsync(b.seeds_in, 0, k * sizeof(uint32_t), s), "ppr columns");
   CK(launch_ppr_seeds(b.seeds_in, k, K, nullptr, a, s), "ppr columns");
   PprState h = {};
@@ -430,4 +385,20 @@ extern "C" int nwgpu_ppr_batched_teleports(nwgpu_graph* g, const uint32_t* out_d
   CK(cudaMemcpyAsync(b.st, b.h_st, sizeof(PprState), cudaMemcpyHostToDevice, s), "copy ppr state");
   CK(launch_ppr_winit(a, K, t, k, g->relabelled ? g->g.inv : nullptr, n, b.vbase, g->sms, s), "ppr teleports init");
   return ppr_loop(g, a, K, k, ranks_nxk, damping, max_iters, opt, stats, s);
+}
+}  // namespace nwgpu
+
+extern "C" int nwgpu_wppr_batched(nwgpu_graph* g, const float* teleports, uint32_t k, float* ranks_nxk, float damping,
+                                  float threshold, uint64_t max_iters, const nwgpu_pr_options* options,
+                                  nwgpu_ppr_stats* stats) {
+  clear_error();
+  return teleport_batched(g, true, nullptr, teleports, k, ranks_nxk, damping, threshold, max_iters, options, stats);
+}
+
+extern "C" int nwgpu_ppr_batched_teleports(nwgpu_graph* g, const uint32_t* out_degree, const float* teleports,
+                                           uint32_t k, float* ranks_nxk, float damping, float threshold,
+                                           uint64_t max_iters, const nwgpu_pr_options* options,
+                                           nwgpu_ppr_stats* stats) {
+  clear_error();
+  return teleport_batched(g, false, out_degree, teleports, k, ranks_nxk, damping, threshold, max_iters, options, stats);
 }
