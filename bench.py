@@ -110,6 +110,40 @@ def peaks():
         return FALLBACK_HBM_GBS, "fallback"
 
 
+def gather_ceiling(log2_len=24, iters=256, reps=5):
+    """The measured ceiling of random 4-byte L2 gathers on this GPU
+    (libnwprobe.so): the sweep's cold-gather load form, 8 in flight per thread,
+    one 1024-thread CTA per SM, uniform random indices into a 2^log2_len-float
+    (64 MB) L2-resident table. Returns loads per second."""
+    import ctypes as C
+    lib = C.CDLL(os.path.join(ROOT, "nwgraph_b200", "libnwprobe.so"))
+    rate, ms = C.c_double(), C.c_double()
+    rc = lib.nwprobe_gather_rate(C.c_uint32(log2_len), C.c_uint32(iters), C.c_uint32(reps), C.byref(rate),
+                                 C.byref(ms))
+    if rc:
+        raise RuntimeError(f"gather probe failed: cudaError {rc}")
+    return rate.value
+
+
+def hub_tier_counts(rp_d, cl_d, thresholds):
+    """Entries whose column, in the engine's internal ids (vertices by
+    descending row length, stably), is >= each threshold: the gathers that
+    leave the shared-memory hub table and the L1 tier in every sweep."""
+    import torch
+    ln = (rp_d[1:] - rp_d[:-1]).long()
+    order = torch.sort(-ln, stable=True).indices
+    newid = torch.empty(ln.numel(), dtype=torch.int32, device=ln.device)
+    newid[order] = torch.arange(ln.numel(), dtype=torch.int32, device=ln.device)
+    del ln, order
+    counts = [0] * len(thresholds)
+    step = 1 << 26
+    for s in range(0, cl_d.numel(), step):
+        ids = newid[cl_d[s:s + step].long()]
+        for j, t in enumerate(thresholds):
+            counts[j] += int((ids >= t).sum())
+    return counts
+
+
 def sweep_traffic_per_launch(args):
     """DRAM bytes per sweep launch from the committed ncu summary (RMAT-24, edge factor 16, relabelled)."""
     if args.scale != 24 or args.edge_factor != 16 or args.no_relabel:
@@ -552,7 +586,11 @@ def run_ours(args):
     deg_d = torch.from_numpy(deg.view(np.int32)).to(dev)
     out_d = torch.empty(n, dtype=torch.float32, device=dev)
     h = Graph(rp_d, cl_d, relabel=not args.no_relabel, autotune=not args.no_autotune)
+    info0 = h.info()
+    tiers = (hub_tier_counts(rp_d, cl_d, [info0["hub_smem_ids"], info0["hub_l1_ids"]])
+             if info0["binned"] and info0["hub_l1_ids"] else None)
     del rp_d, cl_d
+    torch.cuda.empty_cache()
     for _ in range(max(args.warmup, 3)):
         h.page_rank(deg_d, out_d, DAMPING, 0.0, SWEEPS, stream=stream, launch=args.launch)
     if dist:
@@ -616,6 +654,15 @@ def run_ours(args):
 
     peak, peak_kind = peaks()
     achieved = B / (t_sweep_ms * 1e-3) / 1e9
+    gather_roof = None
+    if tiers:
+        ceiling = gather_ceiling()
+        l2_rate = tiers[1] / (t_sweep_ms * 1e-3)
+        gather_roof = {"bound": "random 4-byte L2 gathers", "achieved": l2_rate / 1e9, "peak": ceiling / 1e9,
+                       "unit": "G loads/s", "frac": l2_rate / ceiling, "l2_loads_per_sweep": tiers[1],
+                       "loads_past_shared_memory_per_sweep": tiers[0],
+                       "peak_how": "libnwprobe.so on this GPU: the sweep's cold-gather load, 8 in flight per thread, "
+                                   "one 1024-thread CTA per SM, random indices into a 64 MB L2-resident table"}
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_reference_sample(g, deg, args.cpu_sample_sweeps, os.cpu_count() or 1)
@@ -638,6 +685,7 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": sweep_traffic_per_launch(args), "peak_kind": peak_kind,
                      "bytes_per_sweep": B, "sweep_ms": t_sweep_ms},
+        "gather_roofline": gather_roof,
         "gteps_per_sweep_kernel": nnz / (t_sweep_ms * 1e-3) / 1e9,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(4 * (n + 1) + 4 * nnz + 4 * n),
                 "d2h_bytes_per_step": int(4 * n), "ms_per_step": e2e_ms, "wall_ms_per_step": wall_e2e * 1e3,

@@ -68,6 +68,17 @@ def build_gen(force=False):
     return target
 
 
+def build_probe(force=False):
+    """libnwprobe.so: the random-gather ceiling probe the benchmark reports beside the HBM roofline."""
+    target = os.path.join(HERE, "libnwprobe.so")
+    deps = _deps(["probe_gather.cu"])
+    if not force and not _stale(target, deps):
+        return target
+    _run([NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-Xlinker",
+          "--exclude-libs,ALL", "-o", target, "probe_gather.cu"], cwd=CSRC)
+    return target
+
+
 def build_dropin_test(force=False):
     """tests/cpp/dropin_test: the C++20 header layer over libnwgpu.so."""
     src = os.path.join(ROOT, "tests", "cpp", "dropin_test.cpp")
@@ -84,6 +95,7 @@ def build_dropin_test(force=False):
 def build_all(force=False):
     build_gen(force)
     build_cuda(force)
+    build_probe(force)
     build_dropin_test(force)
 
 
