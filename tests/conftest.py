@@ -31,6 +31,23 @@ def small_graphs():
 
 
 @pytest.fixture(scope="session")
+def refdata():
+    """The reference's own test matrices (test/data/*.mtx) as its driver loads
+    them, with NWGraph's outputs: {name: {"row_ptr", "col", "deg", "v10_20", ...}}."""
+    z = np.load(os.path.join(GOLDEN, "refdata.npz"))
+    out = {}
+    for key in z.files:
+        if key == "names":
+            continue
+        name, field = key.split("/", 1)
+        out.setdefault(name, {})[field] = z[key]
+    return out
+
+
+REFDATA_NAMES = [str(x) for x in np.load(os.path.join(GOLDEN, "refdata.npz"))["names"]]
+
+
+@pytest.fixture(scope="session")
 def csr_golden():
     """Edge lists and the reference's CSRs for each clean-up flag set:
     {name: {"src", "dst", "n", flags: {"row_ptr", "col", "deg"}}}."""

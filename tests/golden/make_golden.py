@@ -26,6 +26,12 @@ the reference tree; the GPU host only reads the committed .npz files).
   by NWGraph's edge_list::serialize (edge_list.hpp:237-255) with its edges,
   and the karate adjacency<1> serialized as adjacency.hpp:180-184 writes it.
 
+* ``refdata.npz`` (``--only refdata``) -- the Matrix Market matrices of the
+  reference's own test data (test/data/*.mtx in coordinate format), each
+  loaded as the reference driver loads a graph (read_mm<directed>, then
+  adjacency<1>: io/mmio.hpp:86-103, 171-208; build.hpp:209-232), with its
+  build_degrees and NWGraph's FP32 outputs as for small_graphs.npz.
+
 All reference outputs come from oracle/_ref/libnwref.so, built from the
 reference headers by oracle/Makefile.
 """
@@ -159,13 +165,37 @@ def loader_fixtures(karate_i, karate_j):
     print("loaders:", sorted({k.split("/")[0] for k in out}), "+ general_ref.nw")
 
 
+def refdata_fixtures(ref_root):
+    data = os.path.join(ref_root, "test", "data")
+    out, names = {}, []
+    for fname in sorted(os.listdir(data)):
+        path = os.path.join(data, fname)
+        if not fname.endswith(".mtx") or "coordinate" not in open(path, errors="replace").readline():
+            continue
+        name = fname[:-4]
+        rp, cl = O.ref_load_mm(path)
+        if len(rp) < 3:
+            continue
+        deg = O.ref_build_degrees(rp, cl)
+        out[f"{name}/row_ptr"], out[f"{name}/col"], out[f"{name}/deg"] = rp, cl, deg
+        for key, val in ref_runs(rp, cl, deg).items():
+            out[f"{name}/{key}"] = val
+        names.append(name)
+        print(name, "n", len(rp) - 1, "nnz", len(cl), "v10 thr iters", int(out[f"{name}/v10_thr_iters"][0]))
+    out["names"] = np.array(names)
+    np.savez_compressed(os.path.join(HERE, "refdata.npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=os.environ.get("NWGRAPH_REF", "/root/reference"))
-    ap.add_argument("--only", choices=["csr", "loaders"], default=None,
-                    help="regenerate csr_build.npz, or files/ and loaders.npz, alone")
+    ap.add_argument("--only", choices=["csr", "loaders", "refdata"], default=None,
+                    help="regenerate csr_build.npz, files/ and loaders.npz, or refdata.npz alone")
     args = ap.parse_args()
     O.build(with_reference=True)
+    if args.only == "refdata":
+        refdata_fixtures(args.ref)
+        return
     if args.only:
         src = open(os.path.join(args.ref, "test", "page_rank_test.cpp")).read()
         ki, kj = np.array(parse_vector(src, "i"), np.uint32), np.array(parse_vector(src, "j"), np.uint32)
@@ -205,6 +235,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "small_graphs.npz"), **out)
     csr_fixtures(i, j)
     loader_fixtures(i, j)
+    refdata_fixtures(args.ref)
 
 
 if __name__ == "__main__":

@@ -14,6 +14,7 @@ import numpy as np
 import pytest
 
 import oracle as O
+from conftest import REFDATA_NAMES
 from nwgraph_b200 import graphs as G
 
 
@@ -43,6 +44,13 @@ def test_restatement_bitwise_vs_reference_fixtures(small_graphs, name):
     assert it == int(g["v10_thr_iters"][0])
     assert np.array_equal(r.view(np.uint32), g["v10_thr"].view(np.uint32))
     assert np.allclose(errs, g["v10_thr_errors"], rtol=0, atol=6e-11)  # trace prints 10 decimals
+
+
+@pytest.mark.parametrize("name", REFDATA_NAMES)
+def test_restatement_bitwise_on_the_reference_test_matrices(refdata, name):
+    """The same pins on the Matrix Market matrices of the reference's own test
+    data, loaded as its driver loads them (read_mm<directed>, adjacency<1>)."""
+    test_restatement_bitwise_vs_reference_fixtures({name: refdata[name]}, name)
 
 
 def test_karate_fp32_fixtures(karate):

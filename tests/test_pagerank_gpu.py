@@ -15,6 +15,7 @@ import numpy as np
 import pytest
 
 import oracle as O
+from conftest import REFDATA_NAMES
 from nwgraph_b200 import Graph, NwgpuError, graphs as G
 from nwgraph_b200 import _native as N
 
@@ -93,6 +94,20 @@ def test_small_fixtures(gpu, small_graphs, name, launch):
     if name not in HUB_GRAPHS:  # a hub's serial FP32 sum shifts the reference's error trace too
         assert np.allclose(st.errors, g["v10_thr_errors"], rtol=ERR_RTOL, atol=ERR_ATOL)
     close(r, g["v10_thr"], st.iterations)
+
+
+@pytest.mark.parametrize("name", REFDATA_NAMES)
+def test_reference_test_matrices(gpu, refdata, name):
+    """The Matrix Market matrices of the reference's own test data, loaded as its
+    driver loads them, against NWGraph's page_rank_v10 outputs on them."""
+    g = refdata[name]
+    r, st = solve(g["row_ptr"], g["col"], g["deg"], iters=20)
+    assert st.iterations == 20
+    assert_close(r, g["v10_20"])
+    r, st = solve(g["row_ptr"], g["col"], g["deg"], thr=1e-4, iters=100)
+    assert st.iterations == int(g["v10_thr_iters"][0])
+    assert np.allclose(st.errors, g["v10_thr_errors"], rtol=ERR_RTOL, atol=ERR_ATOL)
+    assert_close(r, g["v10_thr"])
 
 
 @pytest.mark.parametrize("name", ["rmat10", "directed", "isolated", "grid"])
