@@ -11,6 +11,15 @@
 // to one graph and the per-graph errors are sums of tile residuals in tile
 // order. Graphs that stopped keep their ranks: each sweep walks a list of the
 // running graphs' tiles, rebuilt after every sweep by the convergence kernel.
+//
+// Large graphs (at least 2^22 entries; NWGPU_RAGGED_SOLO_ENTRIES sets the
+// bound, 0 keeps every graph in the batch) are solved alone by the
+// single-graph engine (relabelled, degree-binned sweep), which sweeps them
+// about twice as fast as the merge-path batch sweep; launching them one by one
+// costs little next to their size. In the batch they are empty members (no
+// rows, no tiles); their handles read and write their slices of the batch's
+// degree and rank arrays. Whether a graph is solved alone depends only on its
+// own size, so a graph gets the same result in any batch.
 #include <cstdlib>
 #include <cstring>
 #include <new>
@@ -20,8 +29,17 @@
 
 namespace nwgpu {
 
+constexpr uint64_t kRaggedSoloEntries = 1ull << 22;
+
+struct RaggedSolo {
+  uint32_t     g = 0;  // the graph's index in the batch
+  uint64_t     v0 = 0, n = 0, nnz = 0;
+  nwgpu_graph* h = nullptr;
+};
+
 struct RaggedBatch {
   int          device = 0, sms = 0;
+  std::vector<RaggedSolo> solos;  // graphs solved alone (empty members of the batch)
   cudaStream_t stream = nullptr;
   uint32_t     num_graphs = 0;
   uint64_t     nv = 0, nnz = 0, nrp = 0;  // vertices, entries, row pointers of the batch
@@ -59,6 +77,7 @@ struct RaggedBatch {
     return e;
   }
   ~RaggedBatch() {
+    for (RaggedSolo& S : solos) delete S.h;  // not nwgpu_graph_destroy: that clears the caller's last error
     if (stream) cudaStreamSynchronize(stream);
     if (cg_exec) cudaGraphExecDestroy(cg_exec);
     if (cg) cudaGraphDestroy(cg);
@@ -162,8 +181,12 @@ int nwgpu_batch_create(uint64_t num_graphs, const uint64_t* vertex_offsets, cons
   if (vertex_offsets[0] != 0 || entry_offsets[0] != 0)
     return fail(NWGPU_ERR_INVALID_ARG, "vertex_offsets[0] and entry_offsets[0] must be 0");
   // Per-graph slices and tiles, checked on the host (the offsets are host arrays).
+  // Graphs solved alone are empty members: one zero row pointer, no entries.
+  const char*              solo_env = getenv("NWGPU_RAGGED_SOLO_ENTRIES");
+  const uint64_t           solo_min = solo_env && *solo_env ? strtoull(solo_env, nullptr, 10) : kRaggedSoloEntries;
   std::vector<RaggedGraph> hg(num_graphs);
-  uint64_t                 tiles = 0;
+  std::vector<RaggedSolo>  solos;
+  uint64_t                 tiles = 0, pc = 0, ec = 0;  // compacted row pointers and entries
   for (uint64_t g = 0; g < num_graphs; ++g) {
     if (vertex_offsets[g + 1] < vertex_offsets[g] || entry_offsets[g + 1] < entry_offsets[g])
       return fail(NWGPU_ERR_INVALID_ARG, "offsets decrease at graph %llu", (unsigned long long)g);
@@ -172,17 +195,28 @@ int nwgpu_batch_create(uint64_t num_graphs, const uint64_t* vertex_offsets, cons
       return fail(NWGPU_ERR_INVALID_ARG, "graph %llu: n = %llu, nnz = %llu do not fit uint32 local ids",
                   (unsigned long long)g, (unsigned long long)n, (unsigned long long)m);
     RaggedGraph& R = hg[g];
+    const bool   solo = solo_min && m >= solo_min;
     R.v0 = vertex_offsets[g];
-    R.e0 = entry_offsets[g];
-    R.p0 = vertex_offsets[g] + g;
-    R.n = (uint32_t)n;
-    R.nnz = (uint32_t)m;
+    R.e0 = ec;
+    R.p0 = pc;
+    R.n = solo ? 0u : (uint32_t)n;
+    R.nnz = solo ? 0u : (uint32_t)m;
     R.tile0 = (uint32_t)tiles;
-    R.tiles = (uint32_t)((n + m + kRaggedTileItems - 1) / kRaggedTileItems);
+    R.tiles = (uint32_t)((R.n + R.nnz + kRaggedTileItems - 1) / kRaggedTileItems);
     tiles += R.tiles;
+    pc += R.n + 1ull;
+    ec += R.nnz;
+    if (solo) {
+      RaggedSolo S;
+      S.g = (uint32_t)g;
+      S.v0 = vertex_offsets[g];
+      S.n = n;
+      S.nnz = m;
+      solos.push_back(S);
+    }
     if (tiles + num_graphs >= 0xFFFFFFF0ull) return fail(NWGPU_ERR_INVALID_ARG, "batch has too many tiles");
   }
-  const uint64_t nv = vertex_offsets[num_graphs], nnz = entry_offsets[num_graphs], nrp = nv + num_graphs;
+  const uint64_t nv = vertex_offsets[num_graphs], nnz = entry_offsets[num_graphs], nrp = pc;
   if (!row_ptr) return fail(NWGPU_ERR_INVALID_ARG, "row_ptr is NULL");
   if (nnz && !col) return fail(NWGPU_ERR_INVALID_ARG, "col is NULL with entries");
   int dev, sms;
@@ -203,6 +237,7 @@ int nwgpu_batch_create(uint64_t num_graphs, const uint64_t* vertex_offsets, cons
   b->nrp = nrp;
   b->num_tiles = (uint32_t)tiles;
   b->h_graphs = std::move(hg);
+  b->solos = std::move(solos);
   cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) return bail(cuda_fail(e, "cudaStreamCreate"));
   const cudaMemcpyKind kind = (flags & NWGPU_GRAPH_DEVICE_PTRS) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
@@ -214,17 +249,37 @@ int nwgpu_batch_create(uint64_t num_graphs, const uint64_t* vertex_offsets, cons
   } while (0)
   BK(b->alloc(&b->graphs, G), "cudaMalloc(graphs)");
   BK(b->alloc(&b->row_ptr, nrp), "cudaMalloc(row_ptr)");
-  BK(b->alloc(&b->col, nnz), "cudaMalloc(col)");
+  BK(b->alloc(&b->col, ec), "cudaMalloc(col)");
   BK(cudaMemcpyAsync(b->graphs, b->h_graphs.data(), G * sizeof(RaggedGraph), cudaMemcpyHostToDevice, b->stream),
      "upload graphs");
-  BK(cudaMemcpyAsync(b->row_ptr, row_ptr, nrp * sizeof(uint32_t), kind, b->stream), "upload row_ptr");
-  if (nnz) BK(cudaMemcpyAsync(b->col, col, nnz * sizeof(uint32_t), kind, b->stream), "upload col");
+  // Runs of graphs kept in the batch are contiguous in the input and in the
+  // compacted arrays: one copy of row pointers and one of entries per run.
+  // A solo graph's row pointer stays the zero the allocation wrote.
+  for (uint64_t g0 = 0; g0 < G;) {
+    if (b->h_graphs[g0].n == 0 && b->h_graphs[g0].nnz == 0) {
+      ++g0;
+      continue;
+    }
+    uint64_t g1 = g0 + 1;
+    while (g1 < G && !(b->h_graphs[g1].n == 0 && b->h_graphs[g1].nnz == 0 && solo_min &&
+                       entry_offsets[g1 + 1] - entry_offsets[g1] >= solo_min))
+      ++g1;
+    const uint64_t p_in = vertex_offsets[g0] + g0, p_end = vertex_offsets[g1] + g1;  // row pointers of [g0, g1)
+    BK(cudaMemcpyAsync(b->row_ptr + b->h_graphs[g0].p0, row_ptr + p_in, (p_end - p_in) * sizeof(uint32_t), kind,
+                       b->stream),
+       "upload row_ptr");
+    const uint64_t e_in = entry_offsets[g0], e_end = entry_offsets[g1];
+    if (e_end > e_in)
+      BK(cudaMemcpyAsync(b->col + b->h_graphs[g0].e0, col + e_in, (e_end - e_in) * sizeof(uint32_t), kind, b->stream),
+         "upload col");
+    g0 = g1;
+  }
   // Validate on the device before any kernel indexes with these arrays.
   unsigned int* d_err = nullptr;
   unsigned int  h_err = 0;
   BK(pool_alloc_n(&d_err, 1, b->stream), "cudaMalloc(err)");
   e = cudaMemsetAsync(d_err, 0, sizeof(unsigned int), b->stream);
-  if (e == cudaSuccess) e = validate_ragged(b->graphs, b->num_graphs, b->row_ptr, b->col, nrp, nnz, d_err, sms, b->stream);
+  if (e == cudaSuccess) e = validate_ragged(b->graphs, b->num_graphs, b->row_ptr, b->col, nrp, ec, d_err, sms, b->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(&h_err, d_err, sizeof(unsigned int), cudaMemcpyDeviceToHost, b->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
   pool_free(d_err, b->stream);
@@ -269,6 +324,16 @@ int nwgpu_batch_create(uint64_t num_graphs, const uint64_t* vertex_offsets, cons
   BK(cudaEventCreate(&b->ev1), "cudaEventCreate");
   BK(cudaStreamSynchronize(b->stream), "batch create");
 #undef BK
+  // The graphs solved alone: single-graph handles over the caller's slices.
+  for (RaggedSolo& S : b->solos) {
+    rc = nwgpu_graph_create(row_ptr + (vertex_offsets[S.g] + S.g), col + entry_offsets[S.g], nullptr, S.n, S.nnz,
+                            flags & NWGPU_GRAPH_DEVICE_PTRS, &S.h);
+    if (rc) {
+      char msg[400];
+      nwgpu_last_error(msg, sizeof(msg));
+      return bail(fail(rc, "graph %u: %s", S.g, msg));
+    }
+  }
   *out = b;
   return NWGPU_OK;
 }
@@ -336,9 +401,28 @@ int nwgpu_pr_ragged(nwgpu_batch* b, const uint32_t* out_degree, float* ranks, fl
       CK(cudaStreamSynchronize(s), "sweep loop");
     }
   }
-  CK(cudaEventRecord(b->ev1, s), "cudaEventRecord");
   const PrState fin = *b->h_st;
   if (fin.fault) return fail(NWGPU_ERR_CUDA, "a bounded device wait gave up (fault word %u)", fin.fault);
+  // The graphs solved alone, on the same stream, into their slices of the
+  // batch's rank array, from their slices of its degree array.
+  std::vector<nwgpu_pr_stats> solo_st(b->solos.size());
+  for (size_t i = 0; i < b->solos.size(); ++i) {
+    const RaggedSolo& S = b->solos[i];
+    nwgpu_pr_options  so = {};
+    so.size = sizeof(so);
+    so.mode = NWGPU_MODE_PARITY;
+    so.launch = opt.launch;
+    so.device_ptrs = 1;
+    so.stream = (void*)s;
+    solo_st[i] = nwgpu_pr_stats{};
+    int rc = nwgpu_pr_run(S.h, b->deg + S.v0, b->rank + S.v0, damping, threshold, max_iters, &so, &solo_st[i]);
+    if (rc) {
+      char msg[400];
+      nwgpu_last_error(msg, sizeof(msg));
+      return fail(rc, "graph %u: %s", S.g, msg);
+    }
+  }
+  CK(cudaEventRecord(b->ev1, s), "cudaEventRecord");
   if (nv)
     CK(cudaMemcpyAsync(ranks, b->rank, nv * sizeof(float), dptr ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s),
        "copy ranks");
@@ -353,14 +437,22 @@ int nwgpu_pr_ragged(nwgpu_batch* b, const uint32_t* out_degree, float* ranks, fl
     float ms = 0.f;
     cudaEventElapsedTime(&ms, b->ev0, b->ev1);
     double   swept = 0.0;
-    uint64_t nconv = 0;
+    uint64_t nconv = 0, sweeps = fin.iter;
+    for (size_t i = 0; i < b->solos.size(); ++i) {  // the solo graphs' own counts
+      const RaggedSolo& S = b->solos[i];
+      iters[S.g] = (uint32_t)solo_st[i].iterations;
+      conv[S.g] = solo_st[i].converged ? 1u : 0u;
+      swept += (double)S.nnz * (double)solo_st[i].iterations;
+      if (stats->graph_errors) stats->graph_errors[S.g] = solo_st[i].final_error;
+      if (solo_st[i].iterations > sweeps) sweeps = solo_st[i].iterations;
+    }
     for (uint64_t g = 0; g < G; ++g) {
-      swept += (double)b->h_graphs[g].nnz * (double)iters[g];
+      swept += (double)b->h_graphs[g].nnz * (double)iters[g];  // 0 entries for the solo graphs here
       nconv += conv[g] ? 1u : 0u;
       if (stats->graph_iterations) stats->graph_iterations[g] = iters[g];
       if (stats->graph_converged) stats->graph_converged[g] = conv[g] ? 1 : 0;
     }
-    stats->sweeps = fin.iter;
+    stats->sweeps = sweeps;
     stats->converged_graphs = nconv;
     stats->device_ms = ms;
     stats->entries_swept = swept;
