@@ -40,6 +40,8 @@ struct RaggedSolo {
 struct RaggedBatch {
   int          device = 0, sms = 0;
   std::vector<RaggedSolo> solos;  // graphs solved alone (empty members of the batch)
+  cudaStream_t solo_stream = nullptr;  // the solo graphs run here, beside the batch's sweep loop
+  cudaEvent_t  solo_done = nullptr;
   cudaStream_t stream = nullptr;
   uint32_t     num_graphs = 0;
   uint64_t     nv = 0, nnz = 0, nrp = 0;  // vertices, entries, row pointers of the batch
@@ -77,7 +79,10 @@ struct RaggedBatch {
     return e;
   }
   ~RaggedBatch() {
+    if (solo_stream) cudaStreamSynchronize(solo_stream);
     for (RaggedSolo& S : solos) delete S.h;  // not nwgpu_graph_destroy: that clears the caller's last error
+    if (solo_done) cudaEventDestroy(solo_done);
+    if (solo_stream) cudaStreamDestroy(solo_stream);
     if (stream) cudaStreamSynchronize(stream);
     if (cg_exec) cudaGraphExecDestroy(cg_exec);
     if (cg) cudaGraphDestroy(cg);
@@ -325,6 +330,11 @@ int nwgpu_batch_create(uint64_t num_graphs, const uint64_t* vertex_offsets, cons
   BK(cudaStreamSynchronize(b->stream), "batch create");
 #undef BK
   // The graphs solved alone: single-graph handles over the caller's slices.
+  if (!b->solos.empty()) {
+    if ((e = cudaStreamCreateWithFlags(&b->solo_stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&b->solo_done, cudaEventDisableTiming)) != cudaSuccess)
+      return bail(cuda_fail(e, "solo stream"));
+  }
   for (RaggedSolo& S : b->solos) {
     rc = nwgpu_graph_create(row_ptr + (vertex_offsets[S.g] + S.g), col + entry_offsets[S.g], nullptr, S.n, S.nnz,
                             flags & NWGPU_GRAPH_DEVICE_PTRS, &S.h);
@@ -377,6 +387,40 @@ int nwgpu_pr_ragged(nwgpu_batch* b, const uint32_t* out_degree, float* ranks, fl
   CK(launch_ragged_init(a, b->rs, b->num_graphs, nv, damping, h.done, b->sms, s), "ragged init");
   CK(launch_ragged_list(a, b->rs, b->sms, s), "ragged tile list");
   CK(cudaEventRecord(b->ev0, s), "cudaEventRecord");
+  // The graphs solved alone run on their own stream, after the degree copy,
+  // while the batch's sweep loop runs: each writes only its slice of the rank
+  // array, which no batch kernel touches. They start once the first round of
+  // the batch loop is queued.
+  std::vector<nwgpu_pr_stats> solo_st(b->solos.size());
+  bool                        solos_run = b->solos.empty();
+  auto                        run_solos = [&]() -> int {
+    solos_run = true;
+    CK(cudaStreamWaitEvent(b->solo_stream, b->ev0, 0), "solo stream");
+    for (size_t i = 0; i < b->solos.size(); ++i) {
+      const RaggedSolo& S = b->solos[i];
+      nwgpu_pr_options  so = {};
+      so.size = sizeof(so);
+      so.mode = NWGPU_MODE_PARITY;
+      so.launch = opt.launch;
+      so.device_ptrs = 1;
+      so.stream = (void*)b->solo_stream;
+      solo_st[i] = nwgpu_pr_stats{};
+      int rc = nwgpu_pr_run(S.h, b->deg + S.v0, b->rank + S.v0, damping, threshold, max_iters, &so, &solo_st[i]);
+      if (rc) {
+        char msg[400];
+        nwgpu_last_error(msg, sizeof(msg));
+        return fail(rc, "graph %u: %s", S.g, msg);
+      }
+    }
+    CK(cudaEventRecord(b->solo_done, b->solo_stream), "solo stream");
+    CK(cudaStreamWaitEvent(s, b->solo_done, 0), "solo stream");
+    return NWGPU_OK;
+  };
+  auto drained = [&](int rc) {  // nothing of this call left in flight on an error
+    cudaStreamSynchronize(s);
+    if (b->solo_stream) cudaStreamSynchronize(b->solo_stream);
+    return rc;
+  };
   if (opt.launch == NWGPU_LAUNCH_GRAPH) {
     if (!b->cg_exec || b->cg_damping != damping) {
       int rc = build_ragged_graph(b, a);
@@ -385,9 +429,14 @@ int nwgpu_pr_ragged(nwgpu_batch* b, const uint32_t* out_degree, float* ranks, fl
     const uint64_t max_launches = max_iters / kGraphChunk + 2;
     for (uint64_t launches = 0; !b->h_st->done; ++launches) {
       if (launches == max_launches)
-        return fail(NWGPU_ERR_CUDA, "sweep loop did not finish after %llu graph launches", (unsigned long long)launches);
+        return drained(
+            fail(NWGPU_ERR_CUDA, "sweep loop did not finish after %llu graph launches", (unsigned long long)launches));
       CK(cudaGraphLaunch(b->cg_exec, s), "cudaGraphLaunch");
       CK(cudaMemcpyAsync(b->h_st, b->st, sizeof(PrState), cudaMemcpyDeviceToHost, s), "copy state");
+      if (!solos_run) {
+        int rc = run_solos();
+        if (rc) return drained(rc);
+      }
       CK(cudaStreamSynchronize(s), "sweep loop");
     }
   } else {
@@ -398,31 +447,20 @@ int nwgpu_pr_ragged(nwgpu_batch* b, const uint32_t* out_degree, float* ranks, fl
         CK(launch_ragged_sweep(a, b->sweep_grid, b->finish_grid, b->num_graphs, b->rs, b->conv_grid, s), "ragged sweep");
       launched += batch;
       CK(cudaMemcpyAsync(b->h_st, b->st, sizeof(PrState), cudaMemcpyDeviceToHost, s), "copy state");
+      if (!solos_run) {
+        int rc = run_solos();
+        if (rc) return drained(rc);
+      }
       CK(cudaStreamSynchronize(s), "sweep loop");
     }
   }
-  const PrState fin = *b->h_st;
-  if (fin.fault) return fail(NWGPU_ERR_CUDA, "a bounded device wait gave up (fault word %u)", fin.fault);
-  // The graphs solved alone, on the same stream, into their slices of the
-  // batch's rank array, from their slices of its degree array.
-  std::vector<nwgpu_pr_stats> solo_st(b->solos.size());
-  for (size_t i = 0; i < b->solos.size(); ++i) {
-    const RaggedSolo& S = b->solos[i];
-    nwgpu_pr_options  so = {};
-    so.size = sizeof(so);
-    so.mode = NWGPU_MODE_PARITY;
-    so.launch = opt.launch;
-    so.device_ptrs = 1;
-    so.stream = (void*)s;
-    solo_st[i] = nwgpu_pr_stats{};
-    int rc = nwgpu_pr_run(S.h, b->deg + S.v0, b->rank + S.v0, damping, threshold, max_iters, &so, &solo_st[i]);
-    if (rc) {
-      char msg[400];
-      nwgpu_last_error(msg, sizeof(msg));
-      return fail(rc, "graph %u: %s", S.g, msg);
-    }
+  if (!solos_run) {  // the batch loop ran no round (max_iters 0)
+    int rc = run_solos();
+    if (rc) return drained(rc);
   }
-  CK(cudaEventRecord(b->ev1, s), "cudaEventRecord");
+  const PrState fin = *b->h_st;
+  if (fin.fault) return drained(fail(NWGPU_ERR_CUDA, "a bounded device wait gave up (fault word %u)", fin.fault));
+  CK(cudaEventRecord(b->ev1, s), "cudaEventRecord");  // after the solo graphs too (s waits for them)
   if (nv)
     CK(cudaMemcpyAsync(ranks, b->rank, nv * sizeof(float), dptr ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s),
        "copy ranks");
