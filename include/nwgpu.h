@@ -403,7 +403,14 @@ int nwgpu_shard_unpermute(nwgpu_shard* s, const float* ranks_all, float* ranks, 
  * entry_offsets[num_graphs]. vertex_offsets / entry_offsets are host arrays
  * of num_graphs + 1 non-decreasing values starting at 0; row_ptr / col are
  * host pointers unless flags has NWGPU_GRAPH_DEVICE_PTRS. Per graph n_g and
- * nnz_g must be below 2^32 - 16; the batch totals are 64-bit. */
+ * nnz_g must be below 2^32 - 16; the batch totals are 64-bit.
+ *
+ * Graphs with at least 2^22 entries (the environment variable
+ * NWGPU_RAGGED_SOLO_ENTRIES, read here, sets the bound; 0 keeps every graph in
+ * the batch) get a single-graph handle of their own (as nwgpu_graph_create)
+ * and are solved by it, beside the batch's sweep loop: for them that engine is
+ * faster. A graph's result therefore depends only on the graph, not on the
+ * batch it is in. */
 typedef struct nwgpu_batch nwgpu_batch;
 int nwgpu_batch_create(uint64_t num_graphs, const uint64_t* vertex_offsets, const uint64_t* entry_offsets,
                        const uint32_t* row_ptr, const uint32_t* col, uint32_t flags, nwgpu_batch** out);
