@@ -661,6 +661,8 @@ def run_ours(args):
         gather_roof = {"bound": "random 4-byte L2 gathers", "achieved": l2_rate / 1e9, "peak": ceiling / 1e9,
                        "unit": "G loads/s", "frac": l2_rate / ceiling, "l2_loads_per_sweep": tiers[1],
                        "loads_past_shared_memory_per_sweep": tiers[0],
+                       # counting the L1-tier loads as requests too (an upper bound on the request rate)
+                       "frac_past_shared_memory": tiers[0] / (t_sweep_ms * 1e-3) / ceiling,
                        "peak_how": "libnwprobe.so on this GPU: the sweep's cold-gather load, 8 in flight per thread, "
                                    "one 1024-thread CTA per SM, random indices into a 64 MB L2-resident table"}
     cpu = None
