@@ -64,3 +64,24 @@ def test_reference_arm_prints_once_under_torchrun():
     d = lines[0]
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["kind"] in ("reference", "port")
+
+
+def test_hub_tier_counts_follow_the_relabelling():
+    """bench.hub_tier_counts (the gather roofline's load count) against a
+    brute-force count over the engine's relabelling: vertices by descending
+    row length, stably."""
+    import numpy as np
+    import torch
+
+    import bench
+    from nwgraph_b200 import graphs as G
+    g = G.rmat(11, 16, 7)
+    lens = np.diff(g.row_ptr.astype(np.int64))
+    order = np.argsort(-lens, kind="stable")
+    newid = np.empty(g.n, np.int64)
+    newid[order] = np.arange(g.n)
+    ids = newid[g.col.astype(np.int64)]
+    thresholds = [0, 100, 512, 2000, g.n]
+    got = bench.hub_tier_counts(torch.from_numpy(g.row_ptr.view(np.int32)), torch.from_numpy(g.col.view(np.int32)),
+                                thresholds)
+    assert got == [int((ids >= t).sum()) for t in thresholds]
