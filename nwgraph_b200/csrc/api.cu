@@ -558,7 +558,59 @@ int solve_single(nwgpu_graph* g, const uint32_t* out_degree, float* ranks, float
   return NWGPU_OK;
 }
 
-}  // namespace
+}  // namespace nwgpu
+
+namespace nwgpu {
+int pr_solve_queue(nwgpu_graph* g, const uint32_t* d_degree, float* d_ranks, float damping, float threshold,
+                   uint64_t max_iters, cudaStream_t s, bool* queued) {
+  *queued = false;
+  if (!g || g->n == 0 || !g->relabelled || !g->plan.ok || max_iters == 0) return NWGPU_OK;
+  const uint64_t n = g->n;
+  const float    init = (float)(1.0 / (double)n);  // page_rank.hpp:92-94
+  const float    base = (float)((1.0 - (double)damping) / (double)n);
+  int            rc = ensure_solve_buffers(g);
+  if (rc) return rc;
+  *(volatile unsigned int*)g->h_abort = 0u;
+  if ((rc = load_degrees(g, d_degree, true, s))) return rc;
+  PrState h = {};
+  h.max_iters = max_iters;
+  h.chunk_end = kGraphChunk;
+  h.threshold = (double)threshold;
+  *g->h_st = h;
+  CK(cudaMemcpyAsync(g->st, g->h_st, sizeof(PrState), cudaMemcpyHostToDevice, s), "copy state");
+  const SweepArgs a = make_sweep_args(g, damping, base, kTeleportUniform, 0u);
+  CK(launch_pr_init(a, n, init, g->sms, s), "pr_init");
+  if (!g->cg_exec || !same_loop(g, a, &g->plan, kModePlain)) {
+    if ((rc = build_loop_graph(g, a, &g->plan, kModePlain))) return rc;
+  }
+  CK(cudaGraphLaunch(g->cg_exec, s), "cudaGraphLaunch");
+  CK(cudaMemcpyAsync(g->h_st, g->st, sizeof(PrState), cudaMemcpyDeviceToHost, s), "copy state");
+  CK(launch_gather_f32(g->rank, g->g.perm, d_ranks, n, g->sms, s), "permute ranks");
+  *queued = true;
+  return NWGPU_OK;
+}
+
+int pr_solve_finish(nwgpu_graph* g, float* d_ranks, float damping, float threshold, uint64_t max_iters, cudaStream_t s,
+                    nwgpu_pr_stats* stats) {
+  PrState fin = *g->h_st;
+  if (fin.fault) return fail(NWGPU_ERR_CUDA, "a bounded device wait gave up (fault word %u)", fin.fault);
+  if (!fin.done) {  // more sweeps than one graph launch runs: the loop goes on as nwgpu_pr_run's does
+    const SweepArgs a = make_sweep_args(g, damping, (float)((1.0 - (double)damping) / (double)g->n), kTeleportUniform, 0u);
+    int             rc = run_sweeps(g, a, NWGPU_LAUNCH_GRAPH, max_iters, s, &fin, &g->plan, kModePlain);
+    if (rc) return rc;
+    CK(launch_gather_f32(g->rank, g->g.perm, d_ranks, g->n, g->sms, s), "permute ranks");
+    CK(cudaStreamSynchronize(s), "permute ranks");
+  }
+  (void)threshold;
+  if (stats) {
+    stats->iterations = fin.iter;
+    stats->final_error = fin.last_error;
+    stats->converged = (int32_t)fin.converged;
+  }
+  if (fin.aborted) return fail(NWGPU_ERR_ABORTED, "solve aborted after %llu sweeps", (unsigned long long)fin.iter);
+  return NWGPU_OK;
+}
+}  // namespace nwgpu
 
 extern "C" {
 

@@ -396,7 +396,33 @@ int nwgpu_pr_ragged(nwgpu_batch* b, const uint32_t* out_degree, float* ranks, fl
   auto                        run_solos = [&]() -> int {
     solos_run = true;
     CK(cudaStreamWaitEvent(b->solo_stream, b->ev0, 0), "solo stream");
+    auto graph_fail = [&](int rc, uint32_t g) {
+      char msg[400];
+      nwgpu_last_error(msg, sizeof(msg));
+      return fail(rc, "graph %u: %s", g, msg);
+    };
+    // With the CUDA-graph loop, every solo solve is queued back to back and the
+    // stream is synchronized once; the rest (if any) take the full call.
+    std::vector<char> queued(b->solos.size(), 0);
+    if (opt.launch == NWGPU_LAUNCH_GRAPH) {
+      for (size_t i = 0; i < b->solos.size(); ++i) {
+        const RaggedSolo& S = b->solos[i];
+        bool              q = false;
+        int rc = pr_solve_queue(S.h, b->deg + S.v0, b->rank + S.v0, damping, threshold, max_iters, b->solo_stream, &q);
+        if (rc) return graph_fail(rc, S.g);
+        queued[i] = q ? 1 : 0;
+      }
+      CK(cudaStreamSynchronize(b->solo_stream), "solo graphs");
+      for (size_t i = 0; i < b->solos.size(); ++i) {
+        if (!queued[i]) continue;
+        const RaggedSolo& S = b->solos[i];
+        solo_st[i] = nwgpu_pr_stats{};
+        int rc = pr_solve_finish(S.h, b->rank + S.v0, damping, threshold, max_iters, b->solo_stream, &solo_st[i]);
+        if (rc) return graph_fail(rc, S.g);
+      }
+    }
     for (size_t i = 0; i < b->solos.size(); ++i) {
+      if (queued[i]) continue;
       const RaggedSolo& S = b->solos[i];
       nwgpu_pr_options  so = {};
       so.size = sizeof(so);
@@ -406,11 +432,7 @@ int nwgpu_pr_ragged(nwgpu_batch* b, const uint32_t* out_degree, float* ranks, fl
       so.stream = (void*)b->solo_stream;
       solo_st[i] = nwgpu_pr_stats{};
       int rc = nwgpu_pr_run(S.h, b->deg + S.v0, b->rank + S.v0, damping, threshold, max_iters, &so, &solo_st[i]);
-      if (rc) {
-        char msg[400];
-        nwgpu_last_error(msg, sizeof(msg));
-        return fail(rc, "graph %u: %s", S.g, msg);
-      }
+      if (rc) return graph_fail(rc, S.g);
     }
     CK(cudaEventRecord(b->solo_done, b->solo_stream), "solo stream");
     CK(cudaStreamWaitEvent(s, b->solo_done, 0), "solo stream");

@@ -193,4 +193,17 @@ int ensure_wpr(nwgpu_graph* g);
 int autotune_binned(nwgpu_graph* g);
 // degrees (input order, host or device) -> g->deg (internal order)
 int load_degrees(nwgpu_graph* g, const uint32_t* out_degree, bool device_ptrs, cudaStream_t s);
+// nwgpu_pr_run's solve in two halves, for callers that run many graphs back to
+// back on one stream (ragged batches). pr_solve_queue puts everything on s
+// without waiting: the degrees (device pointer), the start, the first launch
+// of the device-side sweep loop (a CUDA graph), the state copy and the ranks
+// permuted into d_ranks (device pointer, input order). *queued is false, with
+// nothing put on s, for the graphs that need the full call (no vertices, no
+// binned sweep); the caller uses nwgpu_pr_run for them. After s has been
+// synchronized, pr_solve_finish reads the state, runs the rest of a loop
+// longer than one graph launch, and fills stats.
+int pr_solve_queue(nwgpu_graph* g, const uint32_t* d_degree, float* d_ranks, float damping, float threshold,
+                   uint64_t max_iters, cudaStream_t s, bool* queued);
+int pr_solve_finish(nwgpu_graph* g, float* d_ranks, float damping, float threshold, uint64_t max_iters, cudaStream_t s,
+                    nwgpu_pr_stats* stats);
 }  // namespace nwgpu
