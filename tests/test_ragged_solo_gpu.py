@@ -125,3 +125,19 @@ def test_invalid_solo_graph_rejected(gpu, monkeypatch):
     with pytest.raises(NwgpuError) as ei:
         GraphBatch.from_graphs([(ok.row_ptr, ok.col), (bad.row_ptr, col)])
     assert ei.value.status == N.ERR_INVALID_GRAPH and "graph 1" in str(ei.value)
+
+
+def test_solo_solve_longer_than_one_graph_launch(gpu, monkeypatch):
+    """5000 fixed sweeps: the solo graphs' queued loop stops after one CUDA-graph
+    launch (4096 sweeps) and finishes on the full loop, with the same bits as a
+    single-graph handle."""
+    gs = [G.rmat(12, 16, 100), G.grid(900), G.rmat(12, 16, 103)]
+    parts, st = solve_batch(gs, monkeypatch, SOLO, thr=0.0, iters=5000)
+    assert st.sweeps == 5000
+    for i in (0, 2):
+        g = gs[i]
+        with Graph(g.row_ptr, g.col) as h:
+            r = np.empty(g.n, np.float32)
+            s1 = h.page_rank(g.out_degree(), r, D, 0.0, 5000)
+        assert s1.iterations == 5000 and int(st.graph_iterations[i]) == 5000
+        assert np.array_equal(parts[i].view(np.uint32), r.view(np.uint32)), i
