@@ -277,6 +277,15 @@ int nwgpu_spmv(nwgpu_graph* g, const float* x, float* y, const nwgpu_pr_options*
  * returns NWGPU_ERR_ABORTED. Safe to call from another host thread. */
 int nwgpu_abort(nwgpu_graph* g);
 
+/* Self-test of the engine's bounded device waits (no counterpart in the
+ * reference). The sweeps wait on shared-memory barriers for their bulk copies
+ * and give up after 2^20 polls, recording a fault that ends the solve with
+ * NWGPU_ERR_CUDA instead of hanging. This runs that same wait loop, with
+ * `polls` polls (1 .. 2^20), in one thread on a barrier that nothing ever
+ * completes: *gave_up is 1 when the wait gave up as it should, and *ms is how
+ * long that took. Nothing faults; the context stays usable. */
+int nwgpu_selftest_bounded_wait(uint32_t polls, uint32_t* gave_up, double* ms);
+
 /* ---- Graph construction on the device ------------------------------------
  * CSR from an edge list (src[e] -> dst[e], m edges over n vertices): the
  * reference's remove_self_loops (build.hpp:404-410), uniq (:394-402) and

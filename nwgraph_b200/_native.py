@@ -111,6 +111,7 @@ SIGNATURES = {
     "nwgpu_pr_run_noalloc": (C.c_int, [_vp, _vp, C.c_uint64, C.c_uint64, _vp, _vp, C.c_float, C.c_float,
                                        C.c_uint64, _vp, C.POINTER(PrStats)]),
     "nwgpu_abort": (C.c_int, [_vp]),
+    "nwgpu_selftest_bounded_wait": (C.c_int, [C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_double)]),
     "nwgpu_spmv": (C.c_int, [_vp, _vp, _vp, C.POINTER(PrOptions)]),
     "nwgpu_release_cached_memory": (C.c_int, []),
     "nwgpu_wpr_run": (C.c_int, [_vp, _vp, _vp, C.c_float, C.c_float, C.c_uint64, C.POINTER(PrOptions),

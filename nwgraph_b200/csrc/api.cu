@@ -616,6 +616,21 @@ extern "C" {
 
 int nwgpu_abi_version(void) { return NWGPU_ABI_VERSION; }
 
+int nwgpu_selftest_bounded_wait(uint32_t polls, uint32_t* gave_up, double* ms) {
+  clear_error();
+  if (!gave_up || !ms) return fail(NWGPU_ERR_INVALID_ARG, "NULL argument");
+  if (polls == 0 || polls > (1u << 20)) return fail(NWGPU_ERR_INVALID_ARG, "polls = %u outside [1, 2^20]", polls);
+  int dev, sms;
+  int rc = check_device(&dev, &sms);
+  if (rc) return rc;
+  unsigned int flag = 0;
+  float        t = 0.f;
+  CK(run_wait_selftest(polls, &flag, &t), "bounded-wait self-test");
+  *gave_up = flag;
+  *ms = t;
+  return NWGPU_OK;
+}
+
 int nwgpu_last_error(char* buf, size_t len) {
   const std::string& e = last_error_text();
   if (buf && len) {

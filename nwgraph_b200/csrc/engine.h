@@ -218,6 +218,9 @@ cudaError_t launch_op_state(PrState* st, cudaStream_t s);
 cudaError_t launch_gather_u32(const uint32_t* src, const uint32_t* idx, uint32_t* dst, uint64_t n, int sms,
                               cudaStream_t s);
 cudaError_t launch_gather_f32(const float* src, const uint32_t* idx, float* dst, uint64_t n, int sms, cudaStream_t s);
+// One thread waits, with the sweeps' bounded mbarrier wait and `polls` polls,
+// on a barrier that nothing completes; *gave_up = 1 when the wait gave up.
+cudaError_t run_wait_selftest(uint32_t polls, unsigned int* gave_up, float* ms);
 cudaError_t launch_pr_init(const SweepArgs& a, uint64_t n, float init, int sms, cudaStream_t s);
 // Residual push, first phase of the first iteration: rank = push ? r0 : 0,
 // delta = (push, deg > 0) ? r0 d / deg : 0, *pushed += vertices with both.

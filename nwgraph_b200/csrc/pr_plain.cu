@@ -59,13 +59,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait: gives up after ~2^20 suspended polls (well over a second).
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait: gives up after `polls` suspended polls; the sweeps allow 2^20.
+__device__ __forceinline__ bool mbar_wait_n(uint64_t* bar, uint32_t parity, uint32_t polls) {
 #pragma unroll 1
-  for (uint32_t it = 0; it < (1u << 20); ++it)
+  for (uint32_t it = 0; it < polls; ++it)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) { return mbar_wait_n(bar, parity, 1u << 20); }
 
 // ---------------------------------------------------------------------------
 // Shared-memory layout of the sweep kernel
@@ -1065,4 +1066,44 @@ cudaError_t launch_ragged_init(const SweepArgs& a, const RaggedState& rs, uint32
   return cudaGetLastError();
 }
 
+}  // namespace nwgpu
+
+// ---------------------------------------------------------------------------
+// Self-test of the bounded wait: one thread waits on an mbarrier that nothing
+// ever completes, with the sweeps' wait loop, and reports that it gave up.
+// ---------------------------------------------------------------------------
+namespace {
+__device__ unsigned int g_wait_selftest;
+
+__global__ void bounded_wait_selftest_kernel(uint32_t polls) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    nwgpu::mbar_init(&bar, 1);
+    nwgpu::fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) g_wait_selftest = nwgpu::mbar_wait_n(&bar, 0u, polls) ? 0u : 1u;
+}
+}  // namespace
+
+namespace nwgpu {
+cudaError_t run_wait_selftest(uint32_t polls, unsigned int* gave_up, float* ms) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  const unsigned int unset = 7u;  // neither answer, so a kernel that did not run shows
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_wait_selftest, &unset, sizeof(unset));
+  if (e == cudaSuccess) e = cudaEventRecord(e0);
+  if (e == cudaSuccess) {
+    bounded_wait_selftest_kernel<<<1, 32>>>(polls);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(e1);
+  if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+  if (e == cudaSuccess) e = cudaMemcpyFromSymbol(gave_up, g_wait_selftest, sizeof(unsigned int));
+  if (e == cudaSuccess) cudaEventElapsedTime(ms, e0, e1);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  return e;
+}
 }  // namespace nwgpu
