@@ -141,3 +141,17 @@ def test_solo_solve_longer_than_one_graph_launch(gpu, monkeypatch):
             s1 = h.page_rank(g.out_degree(), r, D, 0.0, 5000)
         assert s1.iterations == 5000 and int(st.graph_iterations[i]) == 5000
         assert np.array_equal(parts[i].view(np.uint32), r.view(np.uint32)), i
+
+
+@pytest.mark.parametrize("graphs", [[100, 103], [101]])
+def test_every_graph_solved_alone(gpu, monkeypatch, graphs):
+    """A batch whose graphs are all solved alone: the batch itself has no tiles
+    and no entries."""
+    gs = [G.rmat(12, 16, s) for s in graphs]
+    parts, st = solve_batch(gs, monkeypatch, SOLO)
+    assert st.converged_graphs == len(gs)
+    for i, g in enumerate(gs):
+        with Graph(g.row_ptr, g.col) as h:
+            r = np.empty(g.n, np.float32)
+            s1 = h.page_rank(g.out_degree(), r, D, 1e-6, 200)
+        assert np.array_equal(parts[i].view(np.uint32), r.view(np.uint32)) and int(st.graph_iterations[i]) == s1.iterations
