@@ -426,9 +426,9 @@ int nwgpu_batch_create(uint64_t num_graphs, const uint64_t* vertex_offsets, cons
 int nwgpu_batch_destroy(nwgpu_batch* b);
 
 typedef struct nwgpu_batch_stats {
-  uint64_t  sweeps;           /* batch sweeps run (the last graph to stop) */
+  uint64_t  sweeps;           /* sweeps of the last graph to stop (graphs solved alone included) */
   uint64_t  converged_graphs; /* graphs whose last L1 change was < threshold */
-  double    device_ms;        /* CUDA-event time of the sweep loop */
+  double    device_ms;        /* CUDA-event time of the sweep loop and the graphs solved alone */
   double    entries_swept;    /* sum over graphs of nnz_g x the graph's sweeps */
   double    gteps;            /* entries_swept / device time */
   uint32_t* graph_iterations; /* optional, caller-owned [num_graphs]: sweeps until graph g stopped */

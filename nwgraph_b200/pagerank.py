@@ -431,6 +431,8 @@ class GraphBatch:
     Per-vertex arrays (degrees, ranks) are concatenated in graph order, graph
     ``g``'s at ``vertex_offsets[g]``. No counterpart in the reference: each
     graph gets what ``page_rank`` (page_rank.hpp:92-147) gives for it alone.
+    Graphs of at least 2^22 entries (NWGPU_RAGGED_SOLO_ENTRIES, read when the
+    batch is created) are solved by single-graph handles beside the batch.
     """
 
     def __init__(self, vertex_offsets, entry_offsets, row_ptr, col):
