@@ -123,7 +123,8 @@ typedef struct nwgpu_pr_stats {
   double   ms_per_iter;
   double   bytes_per_iter; /* algorithmic bytes of one sweep: 4 nnz + 4 (n+1) + 20 n */
   double   gteps;          /* nnz * iterations / device time */
-  double*  errors;         /* optional, caller-owned: per-sweep L1 errors */
+  double*  errors;         /* optional, caller-owned: errors[i] = L1 change of sweep i, for the first
+                              min(iterations, errors_cap, 4096) sweeps (later sweeps are not recorded) */
   uint64_t errors_cap;     /* capacity of errors[] */
 } nwgpu_pr_stats;
 
@@ -226,8 +227,16 @@ int nwgpu_ppr_batched_teleports(nwgpu_graph* g, const uint32_t* out_degree, cons
  * `stream` is a cudaStream_t (NULL = the default stream). The call returns
  * when the solve has finished.
  *
+ * The arrays are read exactly within their lengths (row_ptr n + 1, col nnz,
+ * out_degree and ranks n elements): an array may end at the very end of its
+ * allocation.
+ *
  * The first call on a device looks up that device's copy of the array. Make
- * that first call before any stream capture on the device. The working array
+ * that first call before any stream capture on the device. Under CUDA's lazy
+ * module loading (the default), the library's kernels and this array are
+ * loaded on a device at its first use: a caller whose memory manager will
+ * take all of the device's memory should make one call (a warm-up solve on a
+ * tiny graph) before that, so the array is already resident. The working array
  * is shared by every call on a device: calls whose GPU work overlaps (from two
  * host threads, or on two streams at once) race, and both results are
  * undefined. Serialise them. */

@@ -104,7 +104,7 @@ struct SweepArgs {
   double*         res_part;    // residual partials: [0, sweep_grid) sweep kernel, then finishing kernel
   uint32_t        sweep_grid;
   PrState*        st;
-  double*         err_hist;    // per-sweep L1 errors (ring of err_cap)
+  double*         err_hist;    // L1 errors of the first err_cap sweeps (later sweeps are not recorded)
   uint32_t        err_cap;
   const volatile unsigned int* abort_word;  // host-mapped; nonzero -> stop
   cudaGraphConditionalHandle   cond;
@@ -118,6 +118,13 @@ struct SweepArgs {
   const float*                 vbase;      // per-row base term (weighted: (1-d) t; adjoint: c)
   const float*                 vaux;       // per-row factor (weighted: out-weight sum; adjoint: d / out-weight sum)
   float                        push_threshold;  // kModeResidual: residuals above this are pushed
+  // Nonzero: row_ptr, col, rank and deg are the caller's arrays of exactly
+  // n_rows + 1, n_entries, n_rows and n_rows elements, with no spare elements
+  // after them, so the merge-path sweep's tile copies read nothing past those
+  // lengths (the no-alloc solve). Zero: the arrays carry kPad spare elements.
+  int                          exact_ends;
+  uint32_t                     n_rows;
+  uint32_t                     n_entries;
   // Ragged batches only (the RAGGED sweep variant):
   const RaggedGraph*           graphs;
   const float*                 graph_base;  // per graph: (1 - d) / n

@@ -483,7 +483,7 @@ __global__ void __launch_bounds__(256) pr_binned_finish_kernel(const BinnedArgs 
     const unsigned long long done_iters = it + 1ull;
     st->iter = done_iters;
     st->last_error = e;
-    if (a.sw.err_hist) a.sw.err_hist[it % a.sw.err_cap] = e;
+    if (a.sw.err_hist && it < a.sw.err_cap) a.sw.err_hist[it] = e;  // the first err_cap sweeps
     const bool conv = e < st->threshold;
     const bool abort = a.sw.abort_word && *a.sw.abort_word;
     const bool done = conv || done_iters >= st->max_iters || abort;

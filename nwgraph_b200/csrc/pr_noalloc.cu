@@ -82,7 +82,9 @@ __global__ void noalloc_state_kernel(PrState* st, unsigned long long max_iters, 
 }
 
 // The pointer must be device (or managed) memory usable on device `dev`, and
-// 16-byte aligned: the sweep's bulk copies round each slice out to 16 bytes.
+// 16-byte aligned: the sweep's bulk copies start each slice at a 16-byte word
+// of the array (they round down at the start; at the end of an array they
+// stop before its last partial word, which is read with plain loads).
 int check_device_array(const void* p, int dev, const char* name) {
   if (reinterpret_cast<uintptr_t>(p) & 15u) return fail(NWGPU_ERR_INVALID_ARG, "%s is not 16-byte aligned", name);
   cudaPointerAttributes at = {};
@@ -206,6 +208,11 @@ extern "C" int nwgpu_pr_run_noalloc(const uint32_t* row_ptr, const uint32_t* col
   a.teleport = kTeleportUniform;
   a.seed = 0;
   a.hot_ids = hot_ids;
+  // The caller's arrays end exactly at n + 1, nnz, n and n elements: the
+  // tile copies load the last partial 16-byte word of each with plain loads.
+  a.exact_ends = 1;
+  a.n_rows = (uint32_t)n;
+  a.n_entries = (uint32_t)nnz;
   CK(launch_pr_init(a, n, (float)(1.0 / (double)n), sms, s), "pr_init");
   CK(cudaStreamSynchronize(s), "no-alloc set-up");
 

@@ -148,6 +148,22 @@ __device__ __forceinline__ void issue_ragged_tile(const SweepArgs& a, uint32_t i
   }
 }
 
+// Thread 0, arrays without spare elements: words [w0, w1) of src go to dst
+// (w0 and w1 multiples of 4), but src holds only `len` words and nothing at
+// or past len may be read. The words below min(w1, len & ~3) are left to the
+// bulk copy, whose word count is returned; the at most 3 words of
+// [len & ~3, len) inside the slice are loaded here with plain loads and
+// stored to shared memory before the stage's mbarrier arrival, which
+// releases them to the threads that wait on it. Stage words at or past len
+// stay unwritten; the sweep never reads them as values.
+__device__ __forceinline__ uint32_t stage_tail(uint32_t* dst, const uint32_t* src, uint32_t w0, uint32_t w1,
+                                               uint32_t len) {
+  if (w1 <= len) return w1 - w0;
+  const uint32_t b1 = max(w0, len & ~3u);
+  for (uint32_t w = b1; w < len; ++w) dst[w - w0] = __ldcg(src + w);
+  return b1 - w0;
+}
+
 // Thread 0: bring tile t's slices into stage `stg` and record where they landed.
 template <int NT, int IPT>
 __device__ __forceinline__ void issue_tile(const SweepArgs& a, uint32_t t, uint32_t* stg, TileMeta* m, uint64_t* bar,
@@ -167,12 +183,23 @@ __device__ __forceinline__ void issue_tile(const SweepArgs& a, uint32_t t, uint3
   m->rp_at = cw + (r0 - pa0);
   m->rk_at = stage_rows ? cw + pw + (r0 - va0) : ~0u;
   m->dg_at = cw + pw + vw + (r0 - va0);
-  mbar_arrive_expect_tx(bar, 4u * (cw + pw + 2u * vw));
-  if (cw) bulk_load(stg, a.col + ca0, 4u * cw, bar, pol);
-  bulk_load(stg + cw, a.row_ptr + pa0, 4u * pw, bar, pol);
-  if (vw) {
-    bulk_load(stg + cw + pw, a.rank + va0, 4u * vw, bar, pol);
-    bulk_load(stg + cw + pw + vw, a.deg + va0, 4u * vw, bar, pol);
+  // words of each slice that the bulk copies bring in: all of them, unless
+  // the slice runs past the end of an array without spare elements
+  uint32_t bc = cw, bp = pw, bv = vw;
+  if (a.exact_ends) {
+    if (cw) bc = stage_tail(stg, a.col, ca0, ca1, a.n_entries);
+    bp = stage_tail(stg + cw, a.row_ptr, pa0, pa1, a.n_rows + 1u);
+    if (vw) {
+      bv = stage_tail(stg + cw + pw, reinterpret_cast<const uint32_t*>(a.rank), va0, va1, a.n_rows);
+      stage_tail(stg + cw + pw + vw, a.deg, va0, va1, a.n_rows);
+    }
+  }
+  mbar_arrive_expect_tx(bar, 4u * (bc + bp + 2u * bv));
+  if (bc) bulk_load(stg, a.col + ca0, 4u * bc, bar, pol);
+  if (bp) bulk_load(stg + cw, a.row_ptr + pa0, 4u * bp, bar, pol);
+  if (bv) {
+    bulk_load(stg + cw + pw, a.rank + va0, 4u * bv, bar, pol);
+    bulk_load(stg + cw + pw + vw, a.deg + va0, 4u * bv, bar, pol);
   }
 }
 
@@ -573,7 +600,7 @@ __global__ void __launch_bounds__(256) pr_finish_kernel(const SweepArgs a) {
     const unsigned long long done_iters = it + 1ull;
     st->iter = done_iters;
     st->last_error = e;
-    if (a.err_hist) a.err_hist[it % a.err_cap] = e;
+    if (a.err_hist && it < a.err_cap) a.err_hist[it] = e;  // the first err_cap sweeps
     const bool conv = e < st->threshold;
     const bool abort = a.abort_word && *a.abort_word;
     const bool fault = *(volatile unsigned int*)&st->fault != 0u;
@@ -739,7 +766,7 @@ __global__ void __launch_bounds__(256) pr_ragged_converge_kernel(const SweepArgs
     const unsigned int       pending = *(volatile unsigned int*)&st->pending;
     st->iter = done_iters;
     st->last_error = e;
-    if (a.err_hist) a.err_hist[it % a.err_cap] = e;
+    if (a.err_hist && it < a.err_cap) a.err_hist[it] = e;  // the first err_cap sweeps
     const bool done = pending == 0u || done_iters >= st->max_iters || abort || fault;
     st->converged = 0u;
     st->aborted = (abort && pending) ? 1u : 0u;  // graphs were still running

@@ -139,3 +139,68 @@ def test_noalloc_rejects(gpu):
     # the engine is still usable afterwards
     rc, st, _ = noalloc(rp.data_ptr(), cl.data_ptr(), g.n, g.nnz, dg.data_ptr(), out.data_ptr(), *args)
     assert rc == N.OK and st.iterations == 5
+
+
+def _cudart():
+    import os
+    import nvidia.cuda_runtime as cr
+    lib = C.CDLL(os.path.join(list(cr.__path__)[0], "lib", "libcudart.so.12"))
+    lib.cudaMalloc.argtypes = [C.POINTER(C.c_void_p), C.c_size_t]
+    lib.cudaFree.argtypes = [C.c_void_p]
+    lib.cudaMemcpy.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]
+    return lib
+
+
+def _random_graph(n, m):
+    rng = np.random.default_rng(n + m)
+    return G.from_edges(rng.integers(0, n, m), rng.integers(0, n, m), n, symmetrize=False)
+
+
+# (n, sampled edges, expected nnz): n and nnz cover every residue mod 4, so row_ptr (n + 1 elements), col (nnz),
+# degrees and ranks (n) each end at every position inside their final 16-byte word in some case
+@pytest.mark.parametrize("n,m,nnz", [(3001, 20_011, 19_991), (3002, 15_003, 14_985), (3003, 30_003, 29_946),
+                                     (4096, 40_000, 39_963), (3001, 20_012, 19_984)])
+def test_noalloc_arrays_at_allocation_end(gpu, n, m, nnz):
+    """Every array is placed at the end of its own cudaMalloc of a 2 MiB multiple: it starts at the last
+    16-byte-aligned offset it fits at, so it ends inside the allocation's final 16 bytes (exactly at the end when
+    its byte length is a multiple of 16). The solve reads nothing past the arrays' lengths, and its ranks equal
+    the handle entry point's and the oracle's."""
+    import torch
+    g = _random_graph(n, m)
+    assert g.nnz == nnz
+    deg = g.out_degree()
+    ref, _, _ = O.jacobi_f32(g.row_ptr, g.col, deg, 0.85, 0.0, 12)
+    rt = _cudart()
+    two_mib = 2 << 20
+    allocs, ptrs = [], {}
+    try:
+        for key, arr in (("row_ptr", g.row_ptr), ("col", g.col), ("deg", deg), ("ranks", np.zeros(g.n, np.float32))):
+            nbytes = arr.nbytes
+            size = (nbytes + 16 + two_mib - 1) // two_mib * two_mib
+            base = C.c_void_p()
+            assert rt.cudaMalloc(C.byref(base), size) == 0
+            allocs.append(base.value)
+            off = (size - nbytes) & ~15
+            assert off + nbytes <= size and size - (off + nbytes) < 16
+            p = base.value + off
+            assert rt.cudaMemcpy(p, arr.ctypes.data, nbytes, 1) == 0
+            ptrs[key] = p
+        torch.cuda.synchronize()
+        outs = []
+        for _ in range(2):
+            rc, st, _ = noalloc(ptrs["row_ptr"], ptrs["col"], g.n, g.nnz, ptrs["deg"], ptrs["ranks"], 0.85, 0.0, 12)
+            assert rc == N.OK, last_error()
+            assert st.iterations == 12
+            got = np.empty(g.n, np.float32)
+            assert rt.cudaMemcpy(got.ctypes.data, ptrs["ranks"], got.nbytes, 2) == 0
+            close(got, ref)
+            outs.append(got)
+        assert np.array_equal(outs[0], outs[1])
+        handle_out = np.empty(g.n, np.float32)
+        with Graph(g.row_ptr, g.col) as h:
+            h.page_rank(deg, handle_out, 0.85, 0.0, 12)
+        close(outs[0], handle_out)
+    finally:
+        torch.cuda.synchronize()
+        for p in allocs:
+            rt.cudaFree(p)
