@@ -21,9 +21,15 @@
  *  - Errors throw std::runtime_error (the reference has no error path); there
  *    is no CPU fallback.
  *  - The CSR is uploaded on the first call for a graph and kept resident in
- *    HBM, keyed by the graph's address, its array addresses, n, nnz and a
- *    sampled hash of indices_. After mutating a graph in place, call
+ *    HBM, keyed by the graph's address, its array addresses, n, nnz, a hash
+ *    of all of indices_ and a hash of up to 65,536 evenly spaced column ids
+ *    (all of them in graphs of up to 65,536 entries). A graph rebuilt at the
+ *    same addresses with other row pointers, or with other column ids at the
+ *    sampled positions, is uploaded again. An in-place edit that touches only
+ *    unsampled column ids is not seen: after mutating a graph in place, call
  *    nw::graph::gpu::release(graph) (or release_all()) before the next solve.
+ *    At most cache_capacity() graphs (default 4) stay resident; the least
+ *    recently used one is released first.
  *  - No per-iteration trace is printed (page_rank.hpp:109,142); use
  *    resident_graph::run for per-sweep errors and timing.
  *
@@ -34,7 +40,7 @@
 
 #include <cstddef>
 #include <cstdint>
-#include <map>
+#include <list>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
@@ -122,70 +128,107 @@ struct cache_key {
   const void*   graph;
   const void*   indices;
   const void*   cols;
-  std::uint64_t n, nnz, sample_hash;
-  bool          operator<(const cache_key& o) const {
-    return std::tie(graph, indices, cols, n, nnz, sample_hash) <
-           std::tie(o.graph, o.indices, o.cols, o.n, o.nnz, o.sample_hash);
+  std::uint64_t n, nnz, row_hash, col_hash;
+  bool          operator==(const cache_key& o) const {
+    return std::tie(graph, indices, cols, n, nnz, row_hash, col_hash) ==
+           std::tie(o.graph, o.indices, o.cols, o.n, o.nnz, o.row_hash, o.col_hash);
   }
 };
 
-// FNV-1a over up to 4096 evenly spaced row pointers plus the last one.
-inline std::uint64_t sample_hash(const std::uint32_t* rp, std::uint64_t n) {
-  std::uint64_t       h = 1469598103934665603ull;
-  const std::uint64_t step = n / 4096 + 1;
-  auto                mix = [&](std::uint64_t v) {
-    h ^= v;
-    h *= 1099511628211ull;
-  };
-  for (std::uint64_t i = 0; i <= n; i += step) mix(rp[i]);
-  mix(rp[n]);
+// 64-bit multiply-xor mix of one word into the running hash.
+inline std::uint64_t mix64(std::uint64_t h, std::uint64_t v) {
+  h = (h ^ v) * 0x9E3779B97F4A7C15ull;
+  return h ^ (h >> 29);
+}
+
+// All n + 1 row pointers, two per step (about 67 MB at n = 2^24, read once per call).
+inline std::uint64_t row_hash(const std::uint32_t* rp, std::uint64_t n) {
+  std::uint64_t       h = 0x243F6A8885A308D3ull ^ n;
+  const std::uint64_t m = n + 1;
+  std::uint64_t       i = 0;
+  for (; i + 1 < m; i += 2) h = mix64(h, (std::uint64_t)rp[i] | ((std::uint64_t)rp[i + 1] << 32));
+  if (i < m) h = mix64(h, rp[i]);
   return h;
 }
 
-inline std::mutex& cache_mutex() {
-  static std::mutex m;
-  return m;
+// Up to 65,536 evenly spaced column ids plus the last one (every id when nnz <= 65,536).
+inline std::uint64_t col_hash(const std::uint32_t* col, std::uint64_t nnz) {
+  std::uint64_t h = 0x13198A2E03707344ull ^ nnz;
+  if (!nnz) return h;
+  const std::uint64_t step = (nnz + 65535) / 65536;
+  for (std::uint64_t k = 0; k < nnz; k += step) h = mix64(h, ((std::uint64_t)k << 32) | col[k]);
+  return mix64(h, col[nnz - 1]);
 }
-inline std::map<cache_key, std::shared_ptr<resident_graph>>& cache() {
-  static std::map<cache_key, std::shared_ptr<resident_graph>> c;
+
+struct cache_state {
+  std::mutex mu;
+  std::size_t capacity = 4;
+  // most recently used first
+  std::list<std::pair<cache_key, std::shared_ptr<resident_graph>>> entries;
+};
+
+inline cache_state& cache() {
+  static cache_state c;
   return c;
 }
 
 template <gpu_csr_graph Graph>
 cache_key key_of(const Graph& g) {
-  const std::uint64_t n = g.indices_.size() - 1;
-  return {&g, g.indices_.data(), std::get<0>(g.to_be_indexed_).data(), n, std::get<0>(g.to_be_indexed_).size(),
-          sample_hash(g.indices_.data(), n)};
+  const std::uint64_t  n = g.indices_.size() - 1;
+  const auto&          cols = std::get<0>(g.to_be_indexed_);
+  return {&g, g.indices_.data(), cols.data(), n, cols.size(), row_hash(g.indices_.data(), n),
+          col_hash(cols.data(), cols.size())};
 }
 }  // namespace detail
+
+/// Number of graphs kept resident by the drop-in calls.
+inline std::size_t cache_capacity() {
+  std::lock_guard<std::mutex> lock(detail::cache().mu);
+  return detail::cache().capacity;
+}
+
+/// Keep at most `capacity` graphs (>= 1) resident; releases the least recently used ones beyond it.
+inline void set_cache_capacity(std::size_t capacity) {
+  auto&                       c = detail::cache();
+  std::lock_guard<std::mutex> lock(c.mu);
+  c.capacity = capacity ? capacity : 1;
+  while (c.entries.size() > c.capacity) c.entries.pop_back();
+}
 
 /// The resident copy of graph, uploading it on first use.
 template <gpu_csr_graph Graph>
 std::shared_ptr<resident_graph> resident(const Graph& graph) {
   if (graph.indices_.empty()) throw gpu_error(NWGPU_ERR_INVALID_ARG, "graph has no indices_ (not even indices_[0])");
-  auto                        key = detail::key_of(graph);
-  std::lock_guard<std::mutex> lock(detail::cache_mutex());
+  const auto                  key = detail::key_of(graph);
   auto&                       c = detail::cache();
-  auto                        it = c.find(key);
-  if (it != c.end()) return it->second;
-  // drop stale entries of the same graph object (mutated in place)
-  for (auto i = c.begin(); i != c.end();) i = (i->first.graph == key.graph) ? c.erase(i) : std::next(i);
+  std::lock_guard<std::mutex> lock(c.mu);
+  for (auto it = c.entries.begin(); it != c.entries.end(); ++it)
+    if (it->first == key) {
+      c.entries.splice(c.entries.begin(), c.entries, it);  // most recently used
+      return c.entries.front().second;
+    }
+  // an entry for the same graph object or the same arrays is stale (mutated or rebuilt in place)
+  c.entries.remove_if([&](const auto& e) {
+    return e.first.graph == key.graph || e.first.indices == key.indices || e.first.cols == key.cols;
+  });
   auto r = std::make_shared<resident_graph>(graph);
-  c.emplace(key, r);
+  c.entries.emplace_front(key, r);
+  while (c.entries.size() > c.capacity) c.entries.pop_back();
   return r;
 }
 
 /// Free the resident copy of graph (after mutating it, or to return HBM).
 template <class Graph>
 void release(const Graph& graph) {
-  std::lock_guard<std::mutex> lock(detail::cache_mutex());
   auto&                       c = detail::cache();
-  for (auto i = c.begin(); i != c.end();) i = (i->first.graph == (const void*)&graph) ? c.erase(i) : std::next(i);
+  std::lock_guard<std::mutex> lock(c.mu);
+  c.entries.remove_if([&](const auto& e) { return e.first.graph == (const void*)&graph; });
 }
 
 inline void release_all() {
-  std::lock_guard<std::mutex> lock(detail::cache_mutex());
-  detail::cache().clear();
+  auto&                       c = detail::cache();
+  std::lock_guard<std::mutex> lock(c.mu);
+  c.entries.clear();
 }
 
 /**
