@@ -38,11 +38,17 @@ def _p(a, t):
     return a.ctypes.data_as(t) if a is not None else None
 
 
+def default_reference_root() -> str:
+    """Where the reference tree is looked for when NWGRAPH_REF is unset: a
+    directory named ``reference`` beside this repository."""
+    return os.path.normpath(os.path.join(_HERE, "..", "..", "reference"))
+
+
 def build(with_reference: bool | None = None) -> None:
     """Compile the restatement (always) and the reference driver (when the
     reference tree is present, or when asked)."""
     subprocess.run(["make", "-s", "-C", _HERE, "liboracle.so"], check=True)
-    ref_root = os.environ.get("NWGRAPH_REF", "/root/reference")
+    ref_root = os.environ.get("NWGRAPH_REF") or default_reference_root()
     if with_reference is None:
         with_reference = os.path.isdir(os.path.join(ref_root, "include", "nwgraph"))
     if with_reference:

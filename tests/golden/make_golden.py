@@ -1,7 +1,7 @@
 """Regenerate the golden fixtures in tests/golden/ (run in a container that has
 the reference tree; the GPU host only reads the committed .npz files).
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref <reference tree>]
 
 * ``karate.npz`` -- the karate edge list and the 34 expected values of
   test/page_rank_test.cpp:41-75 (parsed from the test source as text), the
@@ -13,7 +13,8 @@ the reference tree; the GPU host only reads the committed .npz files).
   grid, a star, a path, a directed graph with sinks and sources, isolated
   vertices) with NWGraph's FP32 page_rank_v10 (20 sweeps, threshold 0, and
   threshold 1e-4 with its sweep count and per-sweep errors) and page_rank v11
-  on one thread.
+  on one thread (20 sweeps, 100 sweeps, and threshold 1e-4 with its sweep
+  count and per-sweep errors).
 * ``csr_build.npz`` -- edge lists with repeated edges, reversed pairs and
   self-loops (and the karate list), and the CSR the reference builds from
   each with every combination of remove_self_loops, lexical sort + uniq, and
@@ -26,6 +27,10 @@ the reference tree; the GPU host only reads the committed .npz files).
   by NWGraph's edge_list::serialize (edge_list.hpp:237-255) with its edges,
   and the karate adjacency<1> serialized as adjacency.hpp:180-184 writes it.
 
+* ``c1_rmat16.npz`` (``--only c1``) -- configuration 1 (RMAT scale 16, the
+  rows read_mm<directed> builds, sorted): the CSR's SHA-256 and NWGraph's
+  page_rank (v11) converged, at threshold 1e-4, and at the configuration's own
+  threshold 1e-4 with max_iters 20, with sweep counts.
 * ``refdata.npz`` (``--only refdata``) -- the Matrix Market matrices of the
   reference's own test data (test/data/*.mtx in coordinate format), each
   loaded as the reference driver loads a graph (read_mm<directed>, then
@@ -60,16 +65,59 @@ def parse_vector(src: str, name: str):
 
 
 def ref_runs(rp, cl, deg):
+    """NWGraph's FP32 outputs on one graph: page_rank_v10 and page_rank (v11, one thread) at 20 sweeps, v11
+    converged (100 sweeps), and the threshold-1e-4 runs of both with their sweep counts and per-sweep errors."""
     out = {}
     r10, it10, _, _ = O.ref_page_rank(10, rp, cl, deg, 0.85, 0.0, 20, 1)
     r11, it11, _, _ = O.ref_page_rank(11, rp, cl, deg, 0.85, 0.0, 20, 1)
     r10t, it10t, e10t, _ = O.ref_page_rank(10, rp, cl, deg, 0.85, 1e-4, 100, 1)
+    r11c, _, _, _ = O.ref_page_rank(11, rp, cl, deg, 0.85, 0.0, 100, 1)
+    r11t, it11t, e11t, _ = O.ref_page_rank(11, rp, cl, deg, 0.85, 1e-4, 1000, 1)
     out["v10_20"] = r10
     out["v11_20_t1"] = r11
     out["v10_thr"] = r10t
     out["v10_thr_iters"] = np.array([it10t], np.int64)
     out["v10_thr_errors"] = e10t
+    out["v11_100_t1"] = r11c
+    out["v11_thr"] = r11t
+    out["v11_thr_iters"] = np.array([it11t], np.int64)
+    out["v11_thr_errors"] = e11t
     return out
+
+
+def c1_fixture(tmpdir):
+    """Configuration 1: RMAT scale 16 (edge factor 16, seed 42), damping 0.85. The reference reads it from
+    Matrix Market with read_mm<directed> into adjacency<1>; its fill sorts with an unstable sort, so it builds
+    the builder's rows with the entries of each row in another order. The fixture runs NWGraph on the builder's
+    CSR (rows sorted, as sort_adjacency leaves them) after checking that the two CSRs hold the same rows; the
+    CSR itself is not stored (the builder regenerates it, checked against the SHA-256 kept here). Stored:
+    page_rank (v11, one thread) converged at 100 sweeps, its threshold-1e-4 run, the configuration's own run
+    (threshold 1e-4, at most 20 sweeps) with sweep counts and per-sweep errors, and page_rank_v10's
+    threshold-1e-4 sweep count."""
+    import hashlib
+    g = G.rmat(16, 16, 42)
+    path = os.path.join(tmpdir, "rmat16.mtx")
+    rows = np.repeat(np.arange(g.n, dtype=np.int64), np.diff(g.row_ptr))
+    with open(path, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate pattern general\n")
+        f.write(f"{g.n} {g.n} {g.nnz}\n")
+        np.savetxt(f, np.stack([g.col.astype(np.int64) + 1, rows + 1], axis=1), fmt="%d")
+    rp, cl = O.ref_load_mm(path)
+    assert np.array_equal(rp, g.row_ptr)
+    for i in range(g.n):
+        assert np.array_equal(np.sort(cl[rp[i]:rp[i + 1]]), g.col[g.row_ptr[i]:g.row_ptr[i + 1]]), i
+    rp, cl = g.row_ptr, g.col
+    deg = O.ref_build_degrees(rp, cl)
+    r11c, _, _, _ = O.ref_page_rank(11, rp, cl, deg, 0.85, 0.0, 100, 1)
+    _, it11t, e11t, _ = O.ref_page_rank(11, rp, cl, deg, 0.85, 1e-4, 1000, 1)
+    r11, it11, e11, _ = O.ref_page_rank(11, rp, cl, deg, 0.85, 1e-4, 20, 1)
+    _, it10t, _, _ = O.ref_page_rank(10, rp, cl, deg, 0.85, 1e-4, 1000, 1)
+    out = {"csr_sha256": np.array(hashlib.sha256(rp.tobytes() + cl.tobytes()).hexdigest()),
+           "v11_100_t1": r11c, "v11_thr_iters": np.array([it11t], np.int64), "v11_thr_errors": e11t,
+           "v11_c1": r11, "v11_c1_iters": np.array([it11], np.int64), "v11_c1_errors": e11,
+           "v10_thr_iters": np.array([it10t], np.int64)}
+    np.savez_compressed(os.path.join(HERE, "c1_rmat16.npz"), **out)
+    print("c1: n", g.n, "nnz", g.nnz, "v10 thr iters", it10t, "v11 thr iters", it11t, "v11 (1e-4, 20) iters", it11)
 
 
 def directed_with_sinks(n=300, m=1500, seed=3):
@@ -188,13 +236,23 @@ def refdata_fixtures(ref_root):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default=os.environ.get("NWGRAPH_REF", "/root/reference"))
-    ap.add_argument("--only", choices=["csr", "loaders", "refdata"], default=None,
-                    help="regenerate csr_build.npz, files/ and loaders.npz, or refdata.npz alone")
+    ap.add_argument("--ref", default=os.environ.get("NWGRAPH_REF") or O.default_reference_root(),
+                    help="the reference tree (default: $NWGRAPH_REF, else a directory named reference beside "
+                         "this repository)")
+    ap.add_argument("--only", choices=["csr", "loaders", "refdata", "c1"], default=None,
+                    help="regenerate csr_build.npz, files/ and loaders.npz, refdata.npz or c1_rmat16.npz alone")
     args = ap.parse_args()
+    if not os.path.isdir(os.path.join(args.ref, "include", "nwgraph")):
+        ap.error(f"no reference tree at {args.ref} (set --ref or NWGRAPH_REF)")
+    os.environ["NWGRAPH_REF"] = args.ref
     O.build(with_reference=True)
     if args.only == "refdata":
         refdata_fixtures(args.ref)
+        return
+    if args.only == "c1":
+        import tempfile
+        with tempfile.TemporaryDirectory() as d:
+            c1_fixture(d)
         return
     if args.only:
         src = open(os.path.join(args.ref, "test", "page_rank_test.cpp")).read()
@@ -236,6 +294,9 @@ def main():
     csr_fixtures(i, j)
     loader_fixtures(i, j)
     refdata_fixtures(args.ref)
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        c1_fixture(d)
 
 
 if __name__ == "__main__":

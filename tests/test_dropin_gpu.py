@@ -53,10 +53,16 @@ def test_cpp_dropin_standin_graph(gpu, tmp_path):
 @pytest.mark.skipif(not os.path.exists(DROPIN_REF), reason="oracle/_ref/dropin_ref not built")
 @pytest.mark.parametrize("scale", [10, 16])
 def test_cpp_dropin_on_reference_adjacency(gpu, tmp_path, scale):
-    """Config 1's path: RMAT written as .mtx, read by read_mm into adjacency<1>."""
+    """Config 1's path: RMAT written as .mtx, read by read_mm into adjacency<1>; the drop-in against
+    page_rank_v10 at 20 sweeps, and against page_rank (v11) converged, on top-100 order and on the
+    threshold-1e-4 sweep counts (oracle/dropin_ref.cpp, mode o2)."""
     g = G.rmat(scale, 16, 42)
     path = tmp_path / f"rmat{scale}.mtx"
     write_mtx(path, g)
-    res = subprocess.run([DROPIN_REF, str(path), "20"], capture_output=True, text=True, timeout=600)
-    assert res.returncode == 0, res.stdout + res.stderr
+    res = subprocess.run([DROPIN_REF, str(path), "20", "o2"], capture_output=True, text=True, timeout=600)
+    assert res.returncode == 0, res.stdout[-2000:] + res.stderr
     assert "dropin_ref" in res.stdout
+    # oracle O2 on the reference's own adjacency<1>: the production solver nw::graph::page_rank (v11)
+    o2 = dict(kv.split("=") for kv in res.stdout.strip().splitlines()[-1].split()[1:])
+    assert float(o2["converged_max_abs"]) <= 1e-9 and int(o2["top100_order_breaks"]) == 0
+    assert int(o2["thr_sweeps_engine"]) == int(o2["thr_sweeps_v10"]) and int(o2["thr_sweeps_v11"]) >= 1
