@@ -19,9 +19,71 @@
  * deg[j] is the out-degree of j (bench/gapbs/common.hpp:110-121).
  */
 #include <math.h>
+#include <pthread.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
+
+/*
+ * Host threads for the FP64 oracles (orc_pr_f64, orc_pr_vjp_f64): every row
+ * is still summed by one thread in CSR order, so their vectors do not depend
+ * on the thread count; only the L1 change of a sweep is summed per thread and
+ * then in thread order. ORACLE_THREADS overrides the online core count.
+ */
+static int orc_threads(void) {
+  const char* e = getenv("ORACLE_THREADS");
+  long        t = e ? atol(e) : sysconf(_SC_NPROCESSORS_ONLN);
+  if (t < 1) t = 1;
+  if (t > 64) t = 64;
+  return (int)t;
+}
+
+typedef void (*orc_rows_fn)(void* ctx, uint64_t lo, uint64_t hi, int part);
+
+typedef struct {
+  orc_rows_fn fn;
+  void*       ctx;
+  uint64_t    lo, hi;
+  int         part;
+} orc_task;
+
+static void* orc_task_run(void* a) {
+  orc_task* t = (orc_task*)a;
+  t->fn(t->ctx, t->lo, t->hi, t->part);
+  return NULL;
+}
+
+/* Runs fn over rows [0, n) in `parts` ranges of about equal rows + entries
+ * (row_ptr, may be NULL for rows alone), one thread each; part p gets the
+ * p-th range. */
+static void orc_parallel_rows(const uint32_t* row_ptr, uint64_t n, int parts, orc_rows_fn fn, void* ctx) {
+  orc_task  task[64];
+  pthread_t th[64];
+  int       started[64] = {0};
+  uint64_t  total = n + (row_ptr ? row_ptr[n] : 0), lo = 0;
+  for (int p = 0; p < parts; ++p) {
+    uint64_t want = total * (uint64_t)(p + 1) / (uint64_t)parts, hi = lo;
+    if (p == parts - 1) {
+      hi = n;
+    } else {
+      uint64_t a = lo, b = n; /* smallest hi with hi + row_ptr[hi] >= want */
+      while (a < b) {
+        uint64_t m = (a + b) / 2;
+        if (m + (row_ptr ? row_ptr[m] : 0) < want) a = m + 1; else b = m;
+      }
+      hi = a;
+    }
+    task[p] = (orc_task){fn, ctx, lo, hi, p};
+    lo = hi;
+  }
+  for (int p = 1; p < parts; ++p) started[p] = pthread_create(&th[p], NULL, orc_task_run, &task[p]) == 0;
+  orc_task_run(&task[0]);
+  for (int p = 1; p < parts; ++p) {
+    if (started[p]) pthread_join(th[p], NULL);
+    else orc_task_run(&task[p]);
+  }
+}
 
 /* Constants exactly as page_rank.hpp:92-94: computed in double, stored as float. */
 static void pr_constants_f32(uint64_t n, float damping, float* init, float* base) {
@@ -188,6 +250,28 @@ void orc_out_weight(const uint32_t* row_ptr, const uint32_t* col, uint64_t n, co
  * sweep is < tol or max_iters sweeps. Returns sweeps run; *final_err = last L1.
  * This is the FP64 oracle O3 (plain) and O4 (PPR / weighted).
  */
+typedef struct {
+  const uint32_t *row_ptr, *col;
+  const float*    w;
+  const double *  teleport, *c, *r;
+  double*         nr;
+  double          damping, inv_n;
+  double          err[64];
+} orc_pr_sweep;
+
+static void orc_pr_rows(void* p, uint64_t lo, uint64_t hi, int part) {
+  orc_pr_sweep* a = (orc_pr_sweep*)p;
+  double        err = 0.0;
+  for (uint64_t i = lo; i < hi; ++i) {
+    double z = 0.0;
+    for (uint32_t k = a->row_ptr[i]; k < a->row_ptr[i + 1]; ++k) z += (a->w ? (double)a->w[k] : 1.0) * a->c[a->col[k]];
+    double t = a->teleport ? a->teleport[i] : a->inv_n;
+    a->nr[i] = (1.0 - a->damping) * t + a->damping * z;
+    err += fabs(a->nr[i] - a->r[i]);
+  }
+  a->err[part] = err;
+}
+
 int64_t orc_pr_f64(const uint32_t* row_ptr, const uint32_t* col, uint64_t n, const float* w, const double* teleport,
                    const double* r0, double damping, double tol, uint64_t max_iters, double* r, double* final_err) {
   double* s = (double*)malloc((n ? n : 1) * sizeof(double));
@@ -198,16 +282,13 @@ int64_t orc_pr_f64(const uint32_t* row_ptr, const uint32_t* col, uint64_t n, con
   for (uint64_t i = 0; i < n; ++i) r[i] = r0 ? r0[i] : (teleport ? teleport[i] : 1.0 / (double)n);
   uint64_t it = 0;
   double   err = INFINITY;
+  const int    parts = n >= 65536 ? orc_threads() : 1;
+  orc_pr_sweep sw = {row_ptr, col, w, teleport, c, r, nr, damping, 1.0 / (double)n, {0}};
   for (; it < max_iters; ++it) {
     for (uint64_t j = 0; j < n; ++j) c[j] = r[j] / s[j];
+    orc_parallel_rows(row_ptr, n, parts, orc_pr_rows, &sw);
     err = 0.0;
-    for (uint64_t i = 0; i < n; ++i) {
-      double z = 0.0;
-      for (uint32_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k) z += (w ? (double)w[k] : 1.0) * c[col[k]];
-      double t = teleport ? teleport[i] : 1.0 / (double)n;
-      nr[i] = (1.0 - damping) * t + damping * z;
-      err += fabs(nr[i] - r[i]);
-    }
+    for (int p = 0; p < parts; ++p) err += sw.err[p];
     memcpy(r, nr, n * sizeof(double));
     if (err < tol) {
       ++it;
@@ -232,30 +313,72 @@ int64_t orc_pr_f64(const uint32_t* row_ptr, const uint32_t* col, uint64_t n, con
  * CSR. Iterates lambda to L1 change < tol. Writes lambda, dL/dt (n) and
  * dL/dw (nnz, may be NULL). Returns sweeps run.
  */
+typedef struct {
+  const uint64_t* tptr;  /* n + 1: out-row j's entries are [tptr[j], tptr[j+1]) */
+  const uint32_t* trow;  /* the in-row (destination) i of each entry, ascending k within j */
+  const double*   twn;   /* its normalised weight wn(j->i) */
+  const double *  lambda, *cvec;
+  double*         out;   /* per j: cvec_j + d * sum (step), or the plain sum (damping < 0) */
+  double          damping;
+  double          err[64];
+} orc_adj_sweep;
+
+static void orc_adj_rows(void* p, uint64_t lo, uint64_t hi, int part) {
+  orc_adj_sweep* a = (orc_adj_sweep*)p;
+  double         err = 0.0;
+  for (uint64_t j = lo; j < hi; ++j) {
+    double z = 0.0;
+    for (uint64_t e = a->tptr[j]; e < a->tptr[j + 1]; ++e) z += a->twn[e] * a->lambda[a->trow[e]];
+    if (a->damping < 0.0) {
+      a->out[j] = z;
+    } else {
+      double v = a->cvec[j] + a->damping * z;
+      err += fabs(v - a->lambda[j]);
+      a->out[j] = v;
+    }
+  }
+  a->err[part] = err;
+}
+
 int64_t orc_pr_vjp_f64(const uint32_t* row_ptr, const uint32_t* col, uint64_t n, const float* w, const double* r,
                        const double* cvec, double damping, double tol, uint64_t max_iters, double* lambda, double* d_t,
                        double* d_w) {
-  uint64_t nnz = row_ptr[n];
-  double*  s = (double*)malloc((n ? n : 1) * sizeof(double));
-  double*  nl = (double*)malloc((n ? n : 1) * sizeof(double));
-  double*  q = (double*)malloc((n ? n : 1) * sizeof(double));
-  if (!s || !nl || !q) return -1;
+  uint64_t  nnz = row_ptr[n];
+  double*   s = (double*)malloc((n ? n : 1) * sizeof(double));
+  double*   nl = (double*)malloc((n ? n : 1) * sizeof(double));
+  double*   q = (double*)malloc((n ? n : 1) * sizeof(double));
+  uint64_t* tptr = (uint64_t*)calloc(n + 1, sizeof(uint64_t));
+  uint32_t* trow = (uint32_t*)malloc((nnz ? nnz : 1) * sizeof(uint32_t));
+  double*   twn = (double*)malloc((nnz ? nnz : 1) * sizeof(double));
+  if (!s || !nl || !q || !tptr || !trow || !twn) return -1;
   orc_out_weight(row_ptr, col, n, w, s);
-  for (uint64_t j = 0; j < n; ++j) lambda[j] = cvec[j];
-  uint64_t it = 0;
-  for (; it < max_iters; ++it) {
-    for (uint64_t j = 0; j < n; ++j) nl[j] = 0.0;
+  /* The out-row CSR, each out-row's entries in ascending in-row order: the
+   * order in which a serial scatter over the in-row CSR adds them, so the
+   * gathered sums equal that scatter's bit for bit. */
+  for (uint64_t k = 0; k < nnz; ++k) ++tptr[col[k] + 1];
+  for (uint64_t j = 0; j < n; ++j) tptr[j + 1] += tptr[j];
+  {
+    uint64_t* fill = (uint64_t*)malloc((n ? n : 1) * sizeof(uint64_t));
+    if (!fill) return -1;
+    memcpy(fill, tptr, n * sizeof(uint64_t));
     for (uint64_t i = 0; i < n; ++i)
       for (uint32_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k) {
         uint32_t j = col[k];
-        nl[j] += (w ? (double)w[k] : 1.0) / s[j] * lambda[i];
+        uint64_t e = fill[j]++;
+        trow[e] = (uint32_t)i;
+        twn[e] = (w ? (double)w[k] : 1.0) / s[j];
       }
+    free(fill);
+  }
+  for (uint64_t j = 0; j < n; ++j) lambda[j] = cvec[j];
+  const int     parts = n >= 65536 ? orc_threads() : 1;
+  orc_adj_sweep sw = {tptr, trow, twn, lambda, cvec, nl, damping, {0}};
+  uint64_t      it = 0;
+  for (; it < max_iters; ++it) {
+    orc_parallel_rows(NULL, n, parts, orc_adj_rows, &sw);
     double err = 0.0;
-    for (uint64_t j = 0; j < n; ++j) {
-      double v = cvec[j] + damping * nl[j];
-      err += fabs(v - lambda[j]);
-      lambda[j] = v;
-    }
+    for (int p = 0; p < parts; ++p) err += sw.err[p];
+    memcpy(lambda, nl, n * sizeof(double));
     if (err < tol) {
       ++it;
       break;
@@ -264,22 +387,20 @@ int64_t orc_pr_vjp_f64(const uint32_t* row_ptr, const uint32_t* col, uint64_t n,
   for (uint64_t j = 0; j < n; ++j) d_t[j] = (1.0 - damping) * lambda[j];
   if (d_w) {
     /* q_j = sum_{i: j->i} wn(j->i) lambda_i */
-    for (uint64_t j = 0; j < n; ++j) q[j] = 0.0;
-    for (uint64_t i = 0; i < n; ++i)
-      for (uint32_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k) {
-        uint32_t j = col[k];
-        q[j] += (w ? (double)w[k] : 1.0) / s[j] * lambda[i];
-      }
+    orc_adj_sweep qs = {tptr, trow, twn, lambda, cvec, q, -1.0, {0}};
+    orc_parallel_rows(NULL, n, parts, orc_adj_rows, &qs);
     for (uint64_t i = 0; i < n; ++i)
       for (uint32_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k) {
         uint32_t j = col[k];
         d_w[k] = damping * r[j] / s[j] * (lambda[i] - q[j]);
       }
   }
-  (void)nnz;
   free(s);
   free(nl);
   free(q);
+  free(tptr);
+  free(trow);
+  free(twn);
   return (int64_t)it;
 }
 
