@@ -301,38 +301,6 @@ def ppr_batched_vs_looped(scale, k, stream, dist=None, launch="graph"):
             "all_converged": not_conv == 0.0, "max_abs_batched_vs_looped": worst}
 
 
-def ragged_sizes(num_graphs, max_n, seed=11):
-    """Vertex counts (log-uniform in [1e3, max_n]) and RMAT edge factors
-    (U{8..32}) of the ragged configuration's graphs."""
-    rng = np.random.default_rng(seed)
-    ns = np.exp(rng.uniform(np.log(1e3), np.log(max_n), num_graphs)).astype(np.int64)
-    return ns, rng.integers(8, 33, num_graphs)
-
-
-def ragged_batch(num_graphs, max_n, seed=11, graphs=None):
-    """The ragged configuration, built on the GPU: n_g log-uniform in
-    [1e3, max_n] (seed 11); even graph ids symmetrised RMAT (edge factor
-    U{8..32}, scale ceil(log2 n_g), ids taken modulo n_g, self-loops and
-    repeats dropped), odd ids floor(sqrt(n_g))^2 4-neighbour grids. Returns the
-    device CSRs and degrees of the graphs ``graphs`` (a range of ids; all of
-    them by default)."""
-    import math
-    from nwgraph_b200 import construct as K
-    ns, efs = ragged_sizes(num_graphs, max_n, seed)
-    parts, degs = [], []
-    for g in (range(num_graphs) if graphs is None else graphs):
-        n = int(ns[g])
-        if g % 2 == 0:
-            src, dst = K.rmat_edges(max(1, math.ceil(math.log2(n))), int(efs[g]) * n, seed=seed + g, n=n)
-            rp, cl, dg = K.csr_from_edges(src, dst, n, K.SIMPLE_UNDIRECTED)
-            del src, dst
-        else:
-            rp, cl, dg = K.grid(n, device_out=True)
-        parts.append((rp, cl))
-        degs.append(dg)
-    return parts, degs
-
-
 def ragged_vs_looped(num_graphs, max_n, stream, sample_mod=16, dist=None):
     """One ragged-batch solve of every graph (per-graph L1 < 1e-6, at most 200
     sweeps) against looped single-graph solves on the same engine, timed on a
@@ -343,12 +311,12 @@ def ragged_vs_looped(num_graphs, max_n, stream, sample_mod=16, dist=None):
     import torch
     from nwgraph_b200 import Graph, construct as K, shard as S
     world, rank = (dist.get_world_size(), dist.get_rank()) if dist else (1, 0)
-    ns, efs = ragged_sizes(num_graphs, max_n)
+    ns, efs = K.ragged_sizes(num_graphs, max_n)
     ids = np.arange(num_graphs)
     gb = S.weighted_bounds(np.where(ids % 2 == 0, ns * (1 + 2 * efs), 5 * ns), world)
     mine = range(int(gb[rank]), int(gb[rank + 1]))
     t0 = time.time()
-    parts, degs = ragged_batch(num_graphs, max_n, graphs=mine)
+    parts, degs = K.ragged_graphs(num_graphs, max_n, graphs=mine)
     torch.cuda.synchronize()
     build_s = time.time() - t0
     nv = sum(int(p[0].numel()) - 1 for p in parts)
@@ -516,14 +484,25 @@ def wppr_batched_vs_looped(scale, k, stream):
             "max_abs_batched_vs_looped_last_column": worst}
 
 
+class _HostCsr:
+    def __init__(self, row_ptr, col):
+        self.row_ptr, self.col = row_ptr, col
+        self.n, self.nnz = len(row_ptr) - 1, int(row_ptr[-1])
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    g, deg, _ = make_graph(args)
     nthreads = os.cpu_count() or 1
     import oracle as O
     kind = "reference" if O.ref_available(fast=True) else "port"
+    if kind == "reference":
+        # the input from the builder copy inside the reference library: this arm maps none of the engine's
+        g = _HostCsr(*O.ref_rmat(args.scale, args.edge_factor, args.seed))
+        deg = np.bincount(g.col, minlength=g.n).astype(np.uint32)
+    else:
+        g, deg, _ = make_graph(args)
     if kind == "reference":
         rg = O.RefGraph(g.row_ptr, g.col, deg, fast=True)
         run = lambda: rg.page_rank(11, DAMPING, 0.0, args.cpu_sample_sweeps, nthreads)[3]  # noqa: E731

@@ -112,6 +112,37 @@ def grid(n_target: int, device_out: bool = False):
     return CSR(rp.cpu().numpy().view(np.uint32), cl.cpu().numpy().view(np.uint32))
 
 
+def ragged_sizes(num_graphs: int, max_n: float = 1e6, seed: int = 11):
+    """Vertex counts (log-uniform in [1e3, max_n]) and RMAT edge factors
+    (U{8..32}) of the ragged configuration's graphs."""
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(np.log(1e3), np.log(max_n), num_graphs)).astype(np.int64)
+    return ns, rng.integers(8, 33, num_graphs)
+
+
+def ragged_graphs(num_graphs: int, max_n: float = 1e6, seed: int = 11, graphs=None):
+    """The ragged configuration, built on the GPU: n_g log-uniform in
+    [1e3, max_n] (seed 11); even graph ids symmetrised RMAT (edge factor
+    U{8..32}, scale ceil(log2 n_g), ids taken modulo n_g, self-loops and
+    repeats dropped), odd ids floor(sqrt(n_g))^2 4-neighbour grids. Returns the
+    device CSRs [(row_ptr, col)] and degrees of the graphs ``graphs`` (an
+    iterable of ids; all of them by default)."""
+    import math
+    ns, efs = ragged_sizes(num_graphs, max_n, seed)
+    parts, degs = [], []
+    for g in (range(num_graphs) if graphs is None else graphs):
+        n = int(ns[g])
+        if g % 2 == 0:
+            src, dst = rmat_edges(max(1, math.ceil(math.log2(n))), int(efs[g]) * n, seed=seed + g, n=n)
+            rp, cl, dg = csr_from_edges(src, dst, n, SIMPLE_UNDIRECTED)
+            del src, dst
+        else:
+            rp, cl, dg = grid(n, device_out=True)
+        parts.append((rp, cl))
+        degs.append(dg)
+    return parts, degs
+
+
 def batch_from_device_csrs(parts, degrees=None):
     """A :class:`GraphBatch` from device-built graphs ``[(row_ptr, col), ...]``
     (int32 CUDA tensors, local ids), concatenated on the device in order.

@@ -273,6 +273,37 @@ class RefGraph:
     __del__ = close
 
 
+class _NwgenCsr(C.Structure):
+    _fields_ = [("n", C.c_uint64), ("nnz", C.c_uint64), ("row_ptr", _u32p), ("col", _u32p)]
+
+
+def ref_rmat(scale, edge_factor=16, seed=42, abc=(0.57, 0.19, 0.19), nthreads=0):
+    """The benchmark's seeded RMAT CSR (symmetrised, deduplicated, rows
+    sorted), built by the copy of the input builder that
+    oracle/_ref/libnwref_fast.so carries, so that a process timing NWGraph
+    maps no library of the engine. The same graph bit for bit as
+    nwgraph_b200.graphs.rmat. Returns (row_ptr, col)."""
+    L = ref(fast=True)
+    if not getattr(L, "_nwgen_bound", False):
+        L.nwgen_rmat.restype = C.c_int
+        L.nwgen_rmat.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64, C.c_int,
+                                 C.POINTER(_NwgenCsr)]
+        L.nwgen_free.restype = None
+        L.nwgen_free.argtypes = [C.POINTER(_NwgenCsr)]
+        L._nwgen_bound = True
+    g = _NwgenCsr()
+    rc = L.nwgen_rmat(int(scale), float(edge_factor), abc[0], abc[1], abc[2], int(seed), int(nthreads), C.byref(g))
+    if rc != 0:
+        raise RuntimeError(f"nwgen_rmat failed with status {rc}")
+    try:
+        n, nnz = int(g.n), int(g.nnz)
+        rp = np.ctypeslib.as_array(g.row_ptr, shape=(n + 1,)).copy()
+        cl = np.ctypeslib.as_array(g.col, shape=(max(nnz, 1),))[:nnz].copy()
+    finally:
+        L.nwgen_free(C.byref(g))
+    return rp, cl
+
+
 def ref_page_rank_v1_f64(row_ptr, col, deg, damping=0.85, threshold=1e-7, max_iters=100):
     n = len(row_ptr) - 1
     r = np.empty(n, np.float64)

@@ -171,3 +171,13 @@ def test_residual_restatement_matches_reference_v13():
             r, it, _ = O.residual_f32(g.row_ptr, g.col, deg, 0.85, thr, iters)
             rr, rit, _, _ = O.ref_page_rank(13, g.row_ptr, g.col, deg, 0.85, thr, iters, 1)
             assert it == rit and np.array_equal(r.view(np.uint32), rr.view(np.uint32)), (g.n, thr)
+
+
+@pytest.mark.skipif(not O.ref_available(fast=True), reason="oracle/_ref not built")
+def test_reference_library_input_builder_matches():
+    """The benchmark's reference arm builds its RMAT input with the builder copy in the reference library: the
+    same CSR as the engine's builder."""
+    from nwgraph_b200 import graphs as G
+    rp, cl = O.ref_rmat(12, 16, 42)
+    g = G.rmat(12, 16, 42)
+    assert np.array_equal(rp, g.row_ptr) and np.array_equal(cl, g.col)
