@@ -21,7 +21,10 @@ Our arm prints one JSON line with
   cpu_baseline  NWGraph's page_rank (v11) compiled from its headers at its
             release flags, timed on this host's cores on a 2-sweep sample.
 With --gpus N (torchrun) every rank solves its own resident replica
-(weak scaling, no data-path collective).
+(weak scaling, no data-path collective: the headline), and the row-sharded
+solve of the one graph across the ranks is timed beside it (strong scaling,
+key row_sharded: an all-gather of contributions and an all-reduce of the L1
+change per sweep over NCCL, the stopping decision taken on the device).
 
 --impl reference runs NWGraph's own page_rank on this host's CPU cores
 (rank 0 only), each step a 2-sweep sample of the same workload.
@@ -31,7 +34,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import re
 import statistics
 import subprocess
 import sys
@@ -63,9 +65,9 @@ def parse():
     ap.add_argument("--cpu-sample-sweeps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-relabel", action="store_true", help="keep the input vertex order on the device")
-    ap.add_argument("--shard", action="store_true",
-                    help="with N > 1 GPUs also time the row-sharded solve of the one graph across the ranks "
-                         "(all-gather over NCCL each sweep); at N = 1 a one-shard solve is always timed")
+    ap.add_argument("--no-shard", action="store_true",
+                    help="skip the row-sharded solve of the one graph across the ranks (all-gather over NCCL each "
+                         "sweep, stopping decided on the device), timed by default next to the replica headline")
     ap.add_argument("--no-autotune", action="store_true",
                     help="default launch settings instead of the tuned ones (tuning runs at graph creation)")
     ap.add_argument("--ppr-scale", type=int, default=22, help="graph scale of the batched-PPR comparison (0: skip)")
@@ -145,15 +147,18 @@ def hub_tier_counts(rp_d, cl_d, thresholds):
 
 
 def sweep_traffic_per_launch(args):
-    """DRAM bytes per sweep launch from the committed ncu summary (RMAT-24, edge factor 16, relabelled)."""
-    if args.scale != 24 or args.edge_factor != 16 or args.no_relabel:
-        return None
-    path = os.path.join(ROOT, "profiles", "pr_binned_sweep_rmat24_traffic.md")
+    """DRAM bytes per sweep launch of this workload from roofline_traffic.json
+    (one ncu capture of the benchmark command), or None without a capture."""
+    workload = f"rmat{args.scale}_ef{int(args.edge_factor)}_pagerank_f32"
     try:
-        m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
-        return float(m.group(1)) if m else None
-    except OSError:
+        with open(os.path.join(ROOT, "roofline_traffic.json")) as f:
+            entries = json.load(f)["entries"]
+    except (OSError, ValueError, KeyError):
         return None
+    for e in entries:
+        if e.get("workload") == workload and bool(e.get("relabel")) == (not args.no_relabel):
+            return float(e["traffic_bytes_per_launch"])
+    return None
 
 
 class ClockSampler:
@@ -234,11 +239,16 @@ def cpu_reference_sample(g, deg, sweeps, nthreads):
     if O.ref_available(fast=True):
         rg = O.RefGraph(g.row_ptr, g.col, deg, fast=True)
         _, it, _, secs = rg.page_rank(11, DAMPING, 0.0, sweeps, nthreads)
+        # the configuration's threshold-1e-4 run on the reference: both solvers' sweep counts
+        _, it11, e11, _ = rg.page_rank(11, DAMPING, 1e-4, 1000, nthreads)
+        _, it10, _, _ = rg.page_rank(10, DAMPING, 1e-4, 1000, nthreads)
         rg.close()
         t = float(np.mean(secs))
         return {"value": g.nnz / t / 1e9, "unit": UNIT, "cores": nthreads, "kind": "reference",
                 "sample": f"{it} sweeps of nw::graph::page_rank (v11, -Ofast, TBB-API shim) on the full graph; "
-                          f"mean sweep {t * 1e3:.1f} ms from the reference's own trace"}
+                          f"mean sweep {t * 1e3:.1f} ms from the reference's own trace",
+                "threshold_1e-4_sweeps": {"page_rank_v11": it11, "page_rank_v10": it10, "threads": nthreads,
+                                          "v11_last_error": float(e11[-1]) if len(e11) else None}}
     t0 = time.perf_counter()
     O.jacobi_f32(g.row_ptr, g.col, deg, DAMPING, 0.0, 1)
     t = time.perf_counter() - t0
@@ -632,7 +642,7 @@ def run_ours(args):
     wppr = wppr_batched_vs_looped(args.vjp_scale, 16, stream) if args.vjp_scale > 0 else None
     ragged = (ragged_vs_looped(args.ragged_graphs, args.ragged_max_n, stream, dist=dist)
               if args.ragged_graphs > 0 else None)
-    sharded = row_sharded(g, deg, dev, dist, args.steps) if (world == 1 or args.shard) else None
+    sharded = row_sharded(g, deg, dev, dist, args.steps) if not args.no_shard else None
 
     peak, peak_kind = peaks()
     achieved = B / (t_sweep_ms * 1e-3) / 1e9
@@ -691,6 +701,9 @@ def run_ours(args):
     if sharded:
         line["row_sharded"] = sharded
     if cpu:
+        ref_counts = cpu.pop("threshold_1e-4_sweeps", None)
+        if ref_counts:
+            line["threshold_run"]["reference"] = ref_counts
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
     return 0

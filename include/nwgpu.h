@@ -381,7 +381,8 @@ int nwgpu_grid_edges(uint64_t side, uint32_t* src, uint32_t* dst, void* stream);
  * one equal-count all-gather of the ranks' slices (stride floats each)
  * rebuilds the whole vector between sweeps. The caller runs that exchange and
  * the sum of the ranks' FP64 L1 changes (nwgraph_b200/shard.py does it over
- * NCCL through torch.distributed) and decides when to stop. bounds[world+1]
+ * NCCL through torch.distributed); nwgpu_shard_decide takes the stopping
+ * decision from that sum on the device. bounds[world+1]
  * (host) must run from 0 to n, stride be a multiple of 4 and at least every
  * rank's row count; every rank passes the same bounds and stride.
  * All vectors below are device pointers; stream is a cudaStream_t, NULL
@@ -400,6 +401,18 @@ int nwgpu_shard_start(nwgpu_shard* s, const uint32_t* out_degree, int device_ptr
  * device; NaN if a bounded device wait gave up). */
 int nwgpu_shard_sweep(nwgpu_shard* s, const float* contrib_all, float* contrib_slice, float damping, double* l1,
                       void* stream);
+/* The stopping decision of the sweep just run, taken on the device from
+ * *l1_total (the ranks' summed L1 changes, device; every rank passes the same
+ * value) so the host need not read it back each sweep: stop after the first
+ * sweep whose total is < threshold (page_rank.hpp:144), after max_iters
+ * sweeps, or on a NaN total. Once stopped, the shard's later sweeps return
+ * at once and change nothing (their *l1 repeats the last change), so a caller
+ * may queue several sweeps, each with its exchange and decision, and read
+ * state back once per batch. state[4] (device, zeroed by the caller before
+ * the first sweep) = {sweeps decided, stopped, converged, failed};
+ * errors[k] (device, may be NULL) receives the total of sweep k < errors_cap. */
+int nwgpu_shard_decide(nwgpu_shard* s, const double* l1_total, double threshold, uint64_t max_iters, uint64_t* state,
+                       double* errors, uint64_t errors_cap, void* stream);
 /* This rank's ranks into rank_slice[stride]; after the caller gathers every
  * slice into ranks_all[world * stride], nwgpu_shard_unpermute writes the
  * ranks in input order into ranks[n]. */

@@ -133,6 +133,7 @@ SIGNATURES = {
     "nwgpu_shard_destroy": (C.c_int, [_vp]),
     "nwgpu_shard_start": (C.c_int, [_vp, _vp, C.c_int, _vp, _vp]),
     "nwgpu_shard_sweep": (C.c_int, [_vp, _vp, _vp, C.c_float, _vp, _vp]),
+    "nwgpu_shard_decide": (C.c_int, [_vp, _vp, C.c_double, C.c_uint64, _vp, _vp, C.c_uint64, _vp]),
     "nwgpu_shard_rank_slice": (C.c_int, [_vp, _vp, _vp]),
     "nwgpu_shard_unpermute": (C.c_int, [_vp, _vp, _vp, _vp]),
     "nwgpu_batch_create": (C.c_int, [C.c_uint64, _vp, _vp, _vp, _vp, C.c_uint32, C.POINTER(_vp)]),

@@ -66,6 +66,30 @@ __global__ void shard_err_kernel(const PrState* __restrict__ st, double* __restr
   *out = st->fault ? __longlong_as_double(0x7ff8000000000000ll) : st->last_error;
 }
 
+// The stopping decision of one sweep, on the device, from the ranks' summed
+// L1 change `total` (page_rank.hpp:144): after the first sweep whose total is
+// below the threshold, or max_iters sweeps, or a NaN total (a rank's bounded
+// wait gave up), the shard's state is marked done, so its later sweep
+// launches return at once and leave ranks and contributions as they are.
+// state[4] = {sweeps decided, done, converged, failed}; hist[k] = total of sweep k (k < hist_cap).
+__global__ void shard_decide_kernel(PrState* __restrict__ st, const double* __restrict__ total, double threshold,
+                                    unsigned long long max_iters, unsigned long long* __restrict__ state,
+                                    double* __restrict__ hist, unsigned long long hist_cap) {
+  if (state[1]) return;
+  const double             e = *total;
+  const unsigned long long k = state[0];
+  if (hist && k < hist_cap) hist[k] = e;
+  const bool failed = !(e == e);
+  const bool conv = !failed && e < threshold;
+  state[0] = k + 1;
+  if (conv || failed || k + 1 >= max_iters) {
+    state[1] = 1ull;
+    state[2] = conv ? 1ull : 0ull;
+    state[3] = failed ? 1ull : 0ull;
+    st->done = 1u;
+  }
+}
+
 }  // namespace
 }  // namespace nwgpu
 
@@ -274,6 +298,19 @@ int nwgpu_shard_sweep(nwgpu_shard* sh, const float* contrib_all, float* contrib_
   }
   CK(cudaGetLastError(), "shard sweep");
   ++sh->sweeps;
+  return NWGPU_OK;
+}
+
+int nwgpu_shard_decide(nwgpu_shard* sh, const double* l1_total, double threshold, uint64_t max_iters,
+                       uint64_t* state, double* errors, uint64_t errors_cap, void* stream) {
+  clear_error();
+  if (!sh || !l1_total || !state) return fail(NWGPU_ERR_INVALID_ARG, "NULL argument");
+  nwgpu_graph* g = sh->inner;
+  cudaStream_t s = (cudaStream_t)stream;  // NULL: the CUDA default stream
+  shard_decide_kernel<<<1, 1, 0, s>>>(g->st, l1_total, threshold, (unsigned long long)max_iters,
+                                      reinterpret_cast<unsigned long long*>(state), errors,
+                                      (unsigned long long)errors_cap);
+  CK(cudaGetLastError(), "shard decide");
   return NWGPU_OK;
 }
 

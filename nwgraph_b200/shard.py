@@ -22,7 +22,6 @@ or plain copies when one process holds every shard (:class:`LocalExchange`).
 from __future__ import annotations
 
 import ctypes as C
-import math
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -77,6 +76,11 @@ class GpuShard:
         N.check(N.lib().nwgpu_shard_sweep(self._h, contrib_all.data_ptr(), contrib_slice.data_ptr(),
                                           C.c_float(damping), l1.data_ptr(), stream))
 
+    def decide(self, total, threshold, max_iters, state, errors, errors_cap, stream):
+        N.check(N.lib().nwgpu_shard_decide(self._h, total.data_ptr(), float(threshold), int(max_iters),
+                                           state.data_ptr(), errors.data_ptr() if errors is not None else None,
+                                           int(errors_cap), stream))
+
     def rank_slice(self, out, stream):
         N.check(N.lib().nwgpu_shard_rank_slice(self._h, out.data_ptr(), stream))
 
@@ -113,8 +117,9 @@ class DistExchange:
             self.dist.all_gather_into_tensor(full, s, group=self.group)
 
     def total(self, l1):
+        """The ranks' summed L1 change, left on the device (l1 holds this rank's one shard's change)."""
         self.dist.all_reduce(l1, op=self.dist.ReduceOp.SUM, group=self.group)
-        return float(l1.sum().item())
+        return l1
 
 
 class LocalExchange:
@@ -127,7 +132,11 @@ class LocalExchange:
             full[q * stride:(q + 1) * stride].copy_(s)
 
     def total(self, l1):
-        return math.fsum(l1.cpu().tolist()) if l1.numel() > 1 else float(l1.item())
+        """The shards' L1 changes summed in rank order, left on the device."""
+        t = l1[0:1].clone()
+        for j in range(1, l1.numel()):
+            t += l1[j:j + 1]
+        return t
 
 
 @dataclass
@@ -139,13 +148,18 @@ class ShardedStats:
     errors: list = field(default_factory=list)
 
 
-def run(shards, exchange, degrees, ranks_out, damping=0.85, threshold=1e-4, max_iters=20, device=None):
-    """The sharded solve: start, then per sweep (every local shard sweeps,
-    the slices are gathered, the L1 changes summed), stop at the first sweep
-    whose summed change is < threshold or after max_iters; the ranks are
-    gathered and written to ``ranks_out`` (n floats, input order) on every
-    rank. ``shards`` are this process's shards in rank order; ``device`` is the
-    torch device of the buffers."""
+def run(shards, exchange, degrees, ranks_out, damping=0.85, threshold=1e-4, max_iters=20, device=None, chunk=8):
+    """The sharded solve: start, then per sweep every local shard sweeps, the
+    slices are gathered, the L1 changes summed over the ranks, and every shard
+    takes the stopping decision from that sum on the device (the first sweep
+    whose summed change is < threshold, or max_iters; page_rank.hpp:144). The
+    host does not read the change back each sweep: it queues ``chunk`` sweeps
+    (each with its exchange and decision) and reads the decision state once
+    per chunk. A shard that has stopped skips its later sweeps, whose
+    exchanges then move unchanged slices, so every rank takes the same
+    collective steps. The ranks are gathered and written to ``ranks_out`` (n
+    floats, input order) on every rank. ``shards`` are this process's shards
+    in rank order; ``device`` is the torch device of the buffers."""
     import torch
     dev = torch.device(device) if device is not None else (ranks_out.device if hasattr(ranks_out, "device") else None)
     stride, world = shards[0].stride, shards[0].world
@@ -154,37 +168,44 @@ def run(shards, exchange, degrees, ranks_out, damping=0.85, threshold=1e-4, max_
     full = torch.zeros(world * stride, dtype=torch.float32, device=dev)
     slices = [torch.zeros(stride, dtype=torch.float32, device=dev) for _ in shards]
     l1 = torch.zeros(len(shards), dtype=torch.float64, device=dev)
+    state = torch.zeros((len(shards), 4), dtype=torch.int64, device=dev)  # sweeps, stopped, converged, failed
+    cap = int(min(max(int(max_iters), 1), 1 << 16))
+    hist = torch.zeros(cap, dtype=torch.float64, device=dev)
     for sh, s in zip(shards, slices):
         sh.start(degrees, s, stream)
     exchange.gather(full, slices)
     if on_gpu:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-    errors = []
-    converged = False
-    for _ in range(int(max_iters)):
-        for j, (sh, s) in enumerate(zip(shards, slices)):
-            sh.sweep(full, s, damping, l1[j:j + 1], stream)
-        exchange.gather(full, slices)
-        e = exchange.total(l1)
-        errors.append(e)
-        if not math.isfinite(e):
-            raise NwgpuError(N.ERR_CUDA, "a bounded device wait gave up on some rank")
-        if e < float(threshold):
-            converged = True
+    launched, host_state = 0, [0, 0, 0, 0]
+    while launched < int(max_iters):
+        for _ in range(min(int(chunk), int(max_iters) - launched)):
+            for j, (sh, s) in enumerate(zip(shards, slices)):
+                sh.sweep(full, s, damping, l1[j:j + 1], stream)
+            exchange.gather(full, slices)
+            total = exchange.total(l1)
+            for j, sh in enumerate(shards):
+                sh.decide(total, threshold, max_iters, state[j], hist if j == 0 else None, cap, stream)
+            launched += 1
+        host_state = [int(x) for x in state[0].cpu()]  # one read-back per chunk
+        if host_state[1]:
             break
     ms = 0.0
     if on_gpu:
         e1.record()
         torch.cuda.synchronize(dev)
         ms = e0.elapsed_time(e1)
+    if host_state[3]:
+        raise NwgpuError(N.ERR_CUDA, "a bounded device wait gave up on some rank")
+    sweeps = host_state[0]
+    errors = hist[:min(sweeps, cap)].cpu().tolist()
     for sh, s in zip(shards, slices):
         sh.rank_slice(s, stream)
     exchange.gather(full, slices)
     shards[0].unpermute(full, ranks_out, stream)
     if on_gpu:
         torch.cuda.synchronize(dev)
-    return ShardedStats(len(errors), errors[-1] if errors else 0.0, converged, ms, errors)
+    return ShardedStats(sweeps, errors[-1] if errors else 0.0, bool(host_state[2]), ms, errors)
 
 
 class ShardedGraph:
