@@ -146,9 +146,10 @@ def hub_tier_counts(rp_d, cl_d, thresholds):
     return counts
 
 
-def sweep_traffic_per_launch(args):
-    """DRAM bytes per sweep launch of this workload from roofline_traffic.json
-    (one ncu capture of the benchmark command), or None without a capture."""
+def sweep_traffic_per_launch(args, sweep):
+    """DRAM bytes per launch of this workload's sweep kernel (``sweep``:
+    "blocked" or "binned") from roofline_traffic.json (one ncu capture of the
+    benchmark command), or None without a capture."""
     workload = f"rmat{args.scale}_ef{int(args.edge_factor)}_pagerank_f32"
     try:
         with open(os.path.join(ROOT, "roofline_traffic.json")) as f:
@@ -156,7 +157,8 @@ def sweep_traffic_per_launch(args):
     except (OSError, ValueError, KeyError):
         return None
     for e in entries:
-        if e.get("workload") == workload and bool(e.get("relabel")) == (not args.no_relabel):
+        if (e.get("workload") == workload and bool(e.get("relabel")) == (not args.no_relabel)
+                and e.get("sweep") == sweep):
             return float(e["traffic_bytes_per_launch"])
     return None
 
@@ -579,8 +581,10 @@ def run_ours(args):
     out_d = torch.empty(n, dtype=torch.float32, device=dev)
     h = Graph(rp_d, cl_d, relabel=not args.no_relabel, autotune=not args.no_autotune)
     info0 = h.info()
+    # the random-gather ceiling bounds the binned sweep (row order); the blocked sweep reads its gathers in
+    # source order and is bounded by the DRAM stream of its entries instead
     tiers = (hub_tier_counts(rp_d, cl_d, [info0["hub_smem_ids"], info0["hub_l1_ids"]])
-             if info0["binned"] and info0["hub_l1_ids"] else None)
+             if info0["binned"] and info0["hub_l1_ids"] and not info0["blocked"] else None)
     del rp_d, cl_d
     torch.cuda.empty_cache()
     for _ in range(max(args.warmup, 3)):
@@ -674,10 +678,13 @@ def run_ours(args):
                    "l2": "inputs larger than L2 (col 4*nnz bytes), no flush", "parallelism": f"replicas{world}",
                    "tile_items": info["tile_items"], "grid": info["grid"], "num_tiles": info["num_tiles"],
                    "launch": args.launch, "relabel": not args.no_relabel,
-                   "sweep": {k: info[k] for k in ("binned", "sweep_threads", "sweep_grid", "hub_smem_ids",
+                   "sweep": {k: info[k] for k in ("blocked", "block_count", "block_items", "block_loads",
+                                                  "block_piece_entries", "binned",
+                                                  "sweep_threads", "sweep_grid", "hub_smem_ids",
                                                   "hub_l1_ids", "tuned", "tuned_us_per_sweep")}},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": sweep_traffic_per_launch(args), "peak_kind": peak_kind,
+                     "traffic": sweep_traffic_per_launch(args, "blocked" if info["blocked"] else "binned"),
+                     "peak_kind": peak_kind,
                      "bytes_per_sweep": B, "sweep_ms": t_sweep_ms},
         "gather_roofline": gather_roof,
         "gteps_per_sweep_kernel": nnz / (t_sweep_ms * 1e-3) / 1e9,

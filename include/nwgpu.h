@@ -44,7 +44,7 @@
 extern "C" {
 #endif
 
-#define NWGPU_ABI_VERSION 1
+#define NWGPU_ABI_VERSION 2
 
 enum nwgpu_status {
   NWGPU_OK = 0,
@@ -96,6 +96,11 @@ typedef struct nwgpu_graph_info {
   uint32_t hub_l1_ids;     /* binned: ids [hub_smem_ids, hub_l1_ids) gathered through L1 */
   int32_t  tuned;          /* 0 defaults, 1 timed at creation, 2 taken from the tuning cache */
   float    tuned_us_per_sweep;
+  int32_t  blocked;        /* 1: plain solves run the destination-blocked sweep (exact fixed-point row sums) */
+  uint32_t block_count;    /* blocked: destination blocks of 28,672 rows */
+  uint32_t block_items;    /* blocked: work items per sweep (blocks, the large ones cut into pieces) */
+  uint32_t block_loads;    /* blocked: entries in flight per thread */
+  uint64_t block_piece_entries; /* blocked: the largest work item */
 } nwgpu_graph_info;
 int nwgpu_graph_get_info(const nwgpu_graph* g, nwgpu_graph_info* info);
 

@@ -50,7 +50,9 @@ class GraphInfo(C.Structure):
                 ("grid", C.c_uint32), ("device_bytes", C.c_uint64), ("device", C.c_int32),
                 ("has_weights", C.c_int32), ("has_transpose", C.c_int32), ("binned", C.c_int32),
                 ("sweep_threads", C.c_uint32), ("sweep_grid", C.c_uint32), ("hub_smem_ids", C.c_uint32),
-                ("hub_l1_ids", C.c_uint32), ("tuned", C.c_int32), ("tuned_us_per_sweep", C.c_float)]
+                ("hub_l1_ids", C.c_uint32), ("tuned", C.c_int32), ("tuned_us_per_sweep", C.c_float),
+                ("blocked", C.c_int32), ("block_count", C.c_uint32), ("block_items", C.c_uint32),
+                ("block_loads", C.c_uint32), ("block_piece_entries", C.c_uint64)]
 
 
 class PrOptions(C.Structure):

@@ -188,6 +188,7 @@ int check_device(int* dev_out, int* sms_out) {
   std::call_once(g_config_once, [] {
     g_config_err = configure_sweep_kernels();
     if (g_config_err == cudaSuccess) g_config_err = configure_binned_kernels();
+    if (g_config_err == cudaSuccess) g_config_err = configure_blocked_kernels();
   });
   if (g_config_err != cudaSuccess) return cuda_fail(g_config_err, "configure kernels");
   *dev_out = dev;
@@ -370,6 +371,10 @@ SweepArgs make_sweep_args(nwgpu_graph* g, float damping, float base, int telepor
   return a;
 }
 
+bool use_blocked(const nwgpu_graph* g, const BinPlan* plan, int mode) {
+  return g->bplan.ok && mode == kModePlain && (plan == nullptr || plan == &g->plan);
+}
+
 int build_loop_graph(nwgpu_graph* g, const SweepArgs& proto, const BinPlan* plan, int mode) {
   if (g->cg_exec) {
     cudaGraphExecDestroy(g->cg_exec);
@@ -395,7 +400,10 @@ int build_loop_graph(nwgpu_graph* g, const SweepArgs& proto, const BinPlan* plan
   SweepArgs   a = proto;
   a.cond = cond;
   a.use_cond = 1;
-  if (plan)
+  if (use_blocked(g, plan, mode))
+    CK(add_blocked_nodes(body, make_blocked_args(g->bplan, a, g->n), g->bplan.sweep_grid, g->bplan.loads),
+       "cudaGraphAddKernelNode(blocked)");
+  else if (plan)
     CK(add_binned_nodes(body, make_binned_args(g, *plan, a, mode), plan->hot, mode, binned_grid(g, *plan, mode),
                         plan->finish_grid),
        "cudaGraphAddKernelNode(binned)");
@@ -437,9 +445,13 @@ int run_sweeps(nwgpu_graph* g, const SweepArgs& a, uint32_t launch, uint64_t max
     uint64_t launched = 0;
     for (;;) {
       const uint64_t batch = (max_iters - launched) < kGraphChunk ? (max_iters - launched) : kGraphChunk;
-      const BinnedArgs ba = plan ? make_binned_args(g, *plan, a, mode) : BinnedArgs{};
+      const bool       blk = use_blocked(g, plan, mode);
+      const BinnedArgs ba = (plan && !blk) ? make_binned_args(g, *plan, a, mode) : BinnedArgs{};
+      const BlockedArgs bk = blk ? make_blocked_args(g->bplan, a, g->n) : BlockedArgs{};
       for (uint64_t b = 0; b < batch; ++b) {
-        if (plan) {
+        if (blk) {
+          CK(launch_blocked_sweep(bk, g->bplan.sweep_grid, g->bplan.loads, s), "pr_blocked_sweep");
+        } else if (plan) {
           CK(launch_binned_sweep(ba, plan->hot, mode, binned_grid(g, *plan, mode), plan->finish_grid, s), "pr_binned_sweep");
         } else {
           CK(launch_pr_sweep(a, g->variant, g->grid, s), "pr_sweep");
@@ -808,11 +820,29 @@ int finish_create(nwgpu_graph* g, const float* weights, uint32_t flags, nwgpu_gr
     if (rc) return bail(rc);
   }
   trace.mark("bins");
+  // The destination-blocked sweep of plain solves: relabelled unweighted graphs, unless NWGPU_SWEEP names
+  // another sweep (NWGPU_BLOCK_PIECE_ENTRIES sets the largest work item).
+  if (g->relabelled && !weights && !(flags & kGraphNoBlockedPlan) && (!which || !strcmp(which, "blocked"))) {
+    const long piece = env_int("NWGPU_BLOCK_PIECE_ENTRIES", 0);
+    const char* fmt = getenv("NWGPU_BLOCK_FORMAT");  // "wide": 6-byte entries instead of the packed 4-byte words
+    if ((e = build_block_plan(g->g.row_ptr, g->g.col, n, nnz, n, sms, piece > 0 ? (uint64_t)piece : 0,
+                              !(fmt && !strcmp(fmt, "wide")), &g->bplan, g->stream)) != cudaSuccess)
+      return bail(cuda_fail(e, "blocked entry order"));
+    g->device_bytes += g->bplan.bytes;
+    const int loads = env_int("NWGPU_BLOCK_LOADS", 8);  // entries in flight per thread: 4, 8 or 16
+    g->bplan.loads = loads <= 4 ? 4 : (loads >= 16 ? 16 : 8);
+    trace.mark("blocked");
+  }
   {
     // explicit launch settings in the environment take precedence over tuning
     const char* tune = getenv("NWGPU_AUTOTUNE");
     const bool  want_tune = (flags & NWGPU_GRAPH_AUTOTUNE) || (tune && !strcmp(tune, "1"));
-    if (want_tune && g->plan.ok && !which && !getenv("NWGPU_HOT_IDS") && !getenv("NWGPU_HOT_L1_IDS")) {
+    if (want_tune && g->bplan.ok && !getenv("NWGPU_BLOCK_LOADS") && !getenv("NWGPU_BLOCK_PIECE_ENTRIES")) {
+      rc = autotune_blocked(g);  // plain solves run the blocked sweep
+      if (rc) return bail(rc);
+      trace.mark("autotune");
+    } else if (want_tune && g->plan.ok && !g->bplan.ok && !which && !getenv("NWGPU_HOT_IDS") &&
+               !getenv("NWGPU_HOT_L1_IDS")) {
       rc = autotune_binned(g);
       if (rc) return bail(rc);
       trace.mark("autotune");
@@ -862,6 +892,11 @@ int nwgpu_graph_get_info(const nwgpu_graph* g, nwgpu_graph_info* info) {
   }
   info->tuned = g->tuned;
   info->tuned_us_per_sweep = g->tune_us;
+  info->blocked = g->bplan.ok ? 1 : 0;
+  info->block_count = g->bplan.num_blocks;
+  info->block_items = g->bplan.num_items;
+  info->block_loads = g->bplan.ok ? (uint32_t)g->bplan.loads : 0u;
+  info->block_piece_entries = g->bplan.ok ? g->bplan.piece_entries : 0ull;
   return NWGPU_OK;
 }
 

@@ -16,6 +16,8 @@
 // slice, the final unpermute); the exchange between sweeps (the all-gather of
 // the slices and the sum of the ranks' FP64 L1 changes) belongs to the caller,
 // which runs it over NCCL through torch.distributed (nwgraph_b200/shard.py).
+#include <cstdlib>
+#include <cstring>
 #include <new>
 #include <vector>
 
@@ -145,7 +147,8 @@ int nwgpu_shard_create(const uint32_t* row_ptr, const uint32_t* col, uint64_t n,
   if (flags & ~NWGPU_GRAPH_DEVICE_PTRS) return fail(NWGPU_ERR_UNSUPPORTED, "flags 0x%x", flags);
   // The whole graph, validated and relabelled exactly as nwgpu_graph_create does.
   nwgpu_graph* whole = nullptr;
-  int          rc = nwgpu_graph_create(row_ptr, col, nullptr, n, nnz, flags & NWGPU_GRAPH_DEVICE_PTRS, &whole);
+  int          rc = nwgpu_graph_create(row_ptr, col, nullptr, n, nnz,
+                                       (flags & NWGPU_GRAPH_DEVICE_PTRS) | kGraphNoBlockedPlan, &whole);
   if (rc) return rc;
   if (!whole->relabelled) {
     nwgpu_graph_destroy(whole);
@@ -234,6 +237,19 @@ int nwgpu_shard_create(const uint32_t* row_ptr, const uint32_t* col, uint64_t n,
     g->plan.bin.l1_ids = (uint32_t)(hub + 16384);
   }
   g->finish_grid = 1;
+  // The blocked sweep of the local rows, as the single-GPU engine runs it: row
+  // sums are exact fixed-point sums, so each row's value does not depend on
+  // how the rows are cut into blocks or shards, and the sharded ranks equal
+  // the single-GPU engine's bit for bit.
+  const char* which = getenv("NWGPU_SWEEP");
+  if (sh->rows && (!which || !strcmp(which, "blocked"))) {
+    const char* fmt = getenv("NWGPU_BLOCK_FORMAT");
+    if ((e = build_block_plan(g->g.row_ptr, g->g.col, sh->rows, m, (uint64_t)world * stride, g->sms, 0,
+                              !(fmt && !strcmp(fmt, "wide")), &g->bplan, s)) != cudaSuccess) {
+      delete sh;
+      return cuda_fail(e, "shard blocked entry order");
+    }
+  }
   rc = ensure_solve_buffers(g);
   if (rc) {
     delete sh;
@@ -290,8 +306,12 @@ int nwgpu_shard_sweep(nwgpu_shard* sh, const float* contrib_all, float* contrib_
     float* all = const_cast<float*>(contrib_all);
     a.contrib0 = (sh->sweeps & 1) ? contrib_slice : all;
     a.contrib1 = (sh->sweeps & 1) ? all : contrib_slice;
-    const BinnedArgs ba = make_binned_args(g, g->plan, a, kModePlain);
-    CK(launch_binned_sweep(ba, g->plan.hot, kModePlain, g->plan.sweep_grid, g->plan.finish_grid, s), "shard sweep");
+    if (g->bplan.ok) {
+      CK(launch_blocked_sweep(make_blocked_args(g->bplan, a, sh->rows), g->bplan.sweep_grid, g->bplan.loads, s), "shard sweep");
+    } else {
+      const BinnedArgs ba = make_binned_args(g, g->plan, a, kModePlain);
+      CK(launch_binned_sweep(ba, g->plan.hot, kModePlain, g->plan.sweep_grid, g->plan.finish_grid, s), "shard sweep");
+    }
     shard_err_kernel<<<1, 1, 0, s>>>(g->st, l1);
   } else {
     CK(cudaMemsetAsync(l1, 0, sizeof(double), s), "shard sweep");

@@ -1,4 +1,5 @@
-// Autotuner of the degree-binned sweep's launch parameters.
+// Autotuners of the sweeps' launch parameters: the destination-blocked sweep
+// (autotune_blocked, below) and the degree-binned sweep.
 //
 // No counterpart in the reference (its page_rank has no tunables beyond the
 // TBB grain). The binned sweep's runtime knobs are the launch shape (one
@@ -17,6 +18,7 @@
 // so a graph like one already tuned reuses its choice without timing.
 #include <cmath>
 #include <cstdio>
+#include <algorithm>
 #include <cstdlib>
 #include <map>
 #include <mutex>
@@ -118,7 +120,98 @@ int time_plan(nwgpu_graph* g, const SweepArgs& a, int sweeps, float* us) {
   return NWGPU_OK;
 }
 
+// Microseconds per sweep of the blocked plan's current settings (after one warm sweep).
+int time_blocked(nwgpu_graph* g, const SweepArgs& a, int sweeps, float* us) {
+  const BlockPlan&  p = g->bplan;
+  const BlockedArgs ba = make_blocked_args(p, a, g->n);
+  CK(launch_blocked_sweep(ba, p.sweep_grid, p.loads, g->stream), "tune sweep");
+  CK(cudaEventRecord(g->ev0, g->stream), "cudaEventRecord");
+  for (int i = 0; i < sweeps; ++i) CK(launch_blocked_sweep(ba, p.sweep_grid, p.loads, g->stream), "tune sweep");
+  CK(cudaEventRecord(g->ev1, g->stream), "cudaEventRecord");
+  CK(cudaEventSynchronize(g->ev1), "tune sweep");
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, g->ev0, g->ev1), "cudaEventElapsedTime");
+  *us = 1e3f * ms / (float)sweeps;
+  return NWGPU_OK;
+}
+
+// Timing state of a plain solve: unit degrees, uniform start, a sweep limit
+// never reached, threshold 0 (never converged).
+int start_timing(nwgpu_graph* g, SweepArgs* a) {
+  int rc = ensure_solve_buffers(g);
+  if (rc) return rc;
+  fill_u32_kernel<<<g->sms * 4, 256, 0, g->stream>>>(g->deg, g->n, 1u);
+  CK(cudaGetLastError(), "tune degrees");
+  PrState h = {};
+  h.max_iters = ~0ull;
+  h.chunk_end = ~0ull;
+  h.threshold = 0.0;
+  *g->h_st = h;
+  CK(cudaMemcpyAsync(g->st, g->h_st, sizeof(PrState), cudaMemcpyHostToDevice, g->stream), "tune state");
+  const float base = (float)(0.15 / (double)g->n);
+  *a = make_sweep_args(g, 0.85f, base, kTeleportUniform, 0u);
+  CK(launch_pr_init(*a, g->n, (float)(1.0 / (double)g->n), g->sms, g->stream), "tune init");
+  return NWGPU_OK;
+}
+
 }  // namespace
+
+// The blocked sweep's knobs: entries in flight per thread (4, 8, 16) and the
+// largest work item (nnz / (f * SMs) entries for f = 1, 2, 4). The row sums
+// are exact, so every choice gives bitwise-equal ranks; the tuner only times.
+// Cached like the binned choices, under a "blocked" signature (SM count,
+// log2 n in half steps, average degree, share of entries in the first
+// block); the cache line's fields hold the loads and f.
+int autotune_blocked(nwgpu_graph* g) {
+  BlockPlan& p = g->bplan;
+  if (!p.ok || g->n == 0 || g->nnz == 0) return NWGPU_OK;
+  const double nnz = (double)g->nnz, n = (double)g->n;
+  char         buf[160];
+  snprintf(buf, sizeof buf, "blocked sms=%d log2n=%.1f deg=%ld first=%d%%", g->sms, std::round(2.0 * std::log2(n)) / 2.0,
+           std::lround(nnz / n), (int)(std::lround(20.0 * (double)(p.block_ptr[1] - p.block_ptr[0]) / nnz) * 5));
+  const std::string sig = buf;
+  auto piece_of = [&](int f) { return std::max<uint64_t>(1ull << 16, g->nnz / ((uint64_t)g->sms * (uint64_t)f)); };
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    load_locked();
+    auto it = g_cache.find(sig);
+    if (it != g_cache.end()) {
+      const Choice c = it->second;
+      p.loads = c.hot;
+      CK(set_block_items(&p, g->sms, piece_of((int)c.smem_ids), g->stream), "blocked work list");
+      g->tuned = 2;
+      g->tune_us = c.us;
+      return NWGPU_OK;
+    }
+  }
+  SweepArgs a;
+  int       rc = start_timing(g, &a);
+  if (rc) return rc;
+  const int sweeps = g->nnz > (1u << 26) ? 3 : 8;
+  Choice    best;
+  best.us = 3.4e38f;
+  for (int f : {1, 2, 4}) {
+    CK(set_block_items(&p, g->sms, piece_of(f), g->stream), "blocked work list");
+    for (int loads : {4, 8, 16}) {
+      p.loads = loads;
+      float us = 0.f;
+      if ((rc = time_blocked(g, a, sweeps, &us))) return rc;
+      if (us < best.us) {
+        best.hot = loads;
+        best.smem_ids = (uint32_t)f;
+        best.l1_ids = 0;
+        best.us = us;
+      }
+    }
+  }
+  p.loads = best.hot;
+  CK(set_block_items(&p, g->sms, piece_of((int)best.smem_ids), g->stream), "blocked work list");
+  g->tuned = 1;
+  g->tune_us = best.us;
+  std::lock_guard<std::mutex> lk(g_mu);
+  store_locked(sig, best);
+  return NWGPU_OK;
+}
 
 int autotune_binned(nwgpu_graph* g) {
   if (!g->plan.ok || g->n == 0) return NWGPU_OK;
@@ -165,21 +258,8 @@ int autotune_binned(nwgpu_graph* g) {
     c.l1_ids = l1;
     cands.push_back(c);
   }
-  // Timing state: unit degrees, uniform start, a sweep limit never reached,
-  // threshold 0 (never converged).
-  rc = ensure_solve_buffers(g);
-  if (rc) return rc;
-  fill_u32_kernel<<<g->sms * 4, 256, 0, g->stream>>>(g->deg, g->n, 1u);
-  CK(cudaGetLastError(), "tune degrees");
-  PrState h = {};
-  h.max_iters = ~0ull;
-  h.chunk_end = ~0ull;
-  h.threshold = 0.0;
-  *g->h_st = h;
-  CK(cudaMemcpyAsync(g->st, g->h_st, sizeof(PrState), cudaMemcpyHostToDevice, g->stream), "tune state");
-  const float     base = (float)(0.15 / (double)g->n);
-  const SweepArgs a = make_sweep_args(g, 0.85f, base, kTeleportUniform, 0u);
-  CK(launch_pr_init(a, g->n, (float)(1.0 / (double)g->n), g->sms, g->stream), "tune init");
+  SweepArgs a;
+  if ((rc = start_timing(g, &a))) return rc;
   const int sweeps = g->nnz > (1u << 26) ? 3 : 8;
   Choice    best;
   best.us = 3.4e38f;

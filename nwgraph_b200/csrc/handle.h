@@ -10,6 +10,7 @@
 #include "engine.h"
 #include "ppr.h"
 #include "binned.h"
+#include "blocked.h"
 
 namespace nwgpu {
 
@@ -112,6 +113,8 @@ struct nwgpu_graph {
   float        tune_us = 0.f;    // the chosen parameters' time per sweep when tuned
   // Degree-binned sweep (relabelled graphs with non-increasing row lengths).
   nwgpu::BinPlan plan;
+  // Destination-blocked sweep (plain and single-seed solves), built at creation unless NWGPU_SWEEP names another.
+  nwgpu::BlockPlan bplan;
   int          finish_grid = 1;  // finishing-kernel CTAs
   uint64_t     device_bytes = 0;
 
@@ -148,6 +151,7 @@ struct nwgpu_graph {
     ppr.release(stream);
     wpr.release(stream);
     plan.release(stream);
+    bplan.release(stream);
     if (cg_exec) cudaGraphExecDestroy(cg_exec);
     if (cg) cudaGraphDestroy(cg);
     void* dev_ptrs[] = {g.row_ptr, g.col, g.w, g.perm, g.inv, g.emap, tiling.tile_row, tiling.tile_nnz, rank, contrib[0],
@@ -186,11 +190,18 @@ SweepArgs make_sweep_args(nwgpu_graph* g, float damping, float base, int telepor
 int run_sweeps(nwgpu_graph* g, const SweepArgs& a, uint32_t launch, uint64_t max_iters, cudaStream_t s, PrState* fin,
                const BinPlan* plan, int mode);
 nwgpu_pr_options read_options(const nwgpu_pr_options* options);
+// Graph-creation flag for internal callers: no blocked plan (a whole graph that
+// is only relabelled and then cut into shards).
+constexpr uint32_t kGraphNoBlockedPlan = 0x80000000u;
+// Whether a solve in `mode` over `plan` (the handle's forward plan or none) runs the blocked sweep.
+bool use_blocked(const nwgpu_graph* g, const BinPlan* plan, int mode);
 // Out-row CSR, its bins and the buffers of the weighted solve and its adjoint.
 int ensure_wpr(nwgpu_graph* g);
 // api_tune.cu: picks the binned sweep's launch shape and hub tiers for g
 // (timed, or from the per-signature cache) and sets g->plan accordingly.
 int autotune_binned(nwgpu_graph* g);
+// api_tune.cu: picks the blocked sweep's entries in flight and piece size (timed, or cached per signature).
+int autotune_blocked(nwgpu_graph* g);
 // degrees (input order, host or device) -> g->deg (internal order)
 int load_degrees(nwgpu_graph* g, const uint32_t* out_degree, bool device_ptrs, cudaStream_t s);
 // nwgpu_pr_run's solve in two halves, for callers that run many graphs back to

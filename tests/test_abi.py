@@ -35,7 +35,7 @@ def test_python_binding_covers_header():
 
 def test_abi_version():
     from nwgraph_b200 import _native as N
-    assert N.lib().nwgpu_abi_version() == 1
+    assert N.lib().nwgpu_abi_version() == 2
 
 
 @pytest.mark.skipif(has_gpu(), reason="checks the no-device error path")

@@ -1,7 +1,9 @@
-"""Autotuner of the binned sweep (NWGPU_GRAPH_AUTOTUNE): every candidate gives
-bitwise-equal ranks, so a tuned graph must reproduce the default graph's
-ranks bit for bit; choices are cached per graph signature in the process and,
-with NWGPU_TUNE_CACHE, in a file that a later process reuses."""
+"""Autotuner (NWGPU_GRAPH_AUTOTUNE) of the blocked sweep (entries in flight,
+piece size) and, with NWGPU_SWEEP=binned*, of the binned sweep (launch shape,
+hub tiers): every candidate gives bitwise-equal ranks, so a tuned graph must
+reproduce the default graph's ranks bit for bit; choices are cached per graph
+signature in the process and, with NWGPU_TUNE_CACHE, in a file that a later
+process reuses."""
 import json
 import os
 import subprocess
@@ -35,7 +37,7 @@ def test_tuned_ranks_are_bitwise_equal_and_cached(gpu, monkeypatch):
     assert i0["tuned"] == 0 and i0["binned"] == 1
     assert i1["tuned"] in (1, 2) and i1["tuned_us_per_sweep"] > 0
     assert i2["tuned"] == 2  # same signature: taken from the cache
-    for k in ("sweep_threads", "hub_smem_ids", "hub_l1_ids"):
+    for k in ("sweep_threads", "hub_smem_ids", "hub_l1_ids", "block_loads", "block_piece_entries"):
         assert i1[k] == i2[k]
     assert np.array_equal(r0.view(np.uint32), r1.view(np.uint32))
     assert np.array_equal(r0.view(np.uint32), r2.view(np.uint32))
@@ -72,9 +74,10 @@ def test_cache_file_is_reused_by_another_process(gpu, tmp_path):
                                   text=True).stdout.strip().splitlines()[-1])
     assert a["tuned"] == 1 and path.exists()
     lines = path.read_text().strip().splitlines()
-    assert len(lines) == 1 and lines[0].startswith("binned sms=")
+    assert len(lines) == 1 and lines[0].startswith("blocked sms=")
     b = json.loads(subprocess.run([sys.executable, "-c", code], env=env, check=True, capture_output=True,
                                   text=True).stdout.strip().splitlines()[-1])
     assert b["tuned"] == 2
-    for k in ("sweep_threads", "hub_smem_ids", "hub_l1_ids"):
+    for k in ("sweep_threads", "hub_smem_ids", "hub_l1_ids", "block_loads", "block_piece_entries"):
         assert a[k] == b[k]
+

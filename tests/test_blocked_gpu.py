@@ -1,0 +1,187 @@
+"""The destination-blocked sweep (pr_blocked.cu), the default for plain solves on relabelled graphs.
+
+Its row sums are exact 64-bit fixed-point sums rounded once to FP32, so:
+
+* parity: within 1e-6 max-abs and 1e-5 L1 of page_rank_v10 restated after a
+  fixed sweep count, with the same stopping sweep for threshold runs, on
+  graphs of one and many blocks (28,672 rows each), with empty rows, dangling
+  vertices and hubs, and on the reference's own test matrices; where hub rows
+  of 10^5 entries make the reference's serial FP32 sums drift beyond 1e-6,
+  at least as close as the reference to FP64 arithmetic;
+* the ranks do not depend on how the work is cut or stored: bitwise equal for
+  every piece size (NWGPU_BLOCK_PIECE_ENTRIES, which splits the large blocks
+  into pieces that meet in a global accumulator), every number of entries in
+  flight (NWGPU_BLOCK_LOADS), the packed 4-byte entries (with wide groups) and
+  the 6-byte ones (NWGPU_BLOCK_FORMAT=wide), in CUDA-graph and stream launch,
+  run after run, and for a row-sharded solve of any shard count;
+* accuracy: at least as close to the FP64 fixed point as the binned sweep's
+  FP32 tree sums (NWGPU_SWEEP=binned_hot).
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import REFDATA_NAMES
+from nwgraph_b200 import Graph, graphs as G, shard as S
+
+pytestmark = pytest.mark.gpu
+
+D = 0.85
+
+
+def solve(g, deg, thr=0.0, iters=20, launch="graph"):
+    with Graph(g.row_ptr, g.col) as h:
+        out = np.empty(g.n, np.float32)
+        st = h.page_rank(deg, out, D, thr, iters, launch=launch, record_errors=True)
+        info = h.info()
+    return out, st, info
+
+
+def close(a, b, max_abs=1e-6, l1=1e-5):
+    d = np.abs(np.asarray(a, np.float64) - np.asarray(b, np.float64))
+    assert d.max() <= max_abs and d.sum() <= l1, (d.max(), d.sum())
+
+
+def parity_or_more_accurate(r, ref, g, sweeps):
+    """Within 1e-6 / 1e-5 of the reference, or -- on graphs whose hub rows make the reference's serial FP32 row
+    sums themselves drift beyond that -- at least as close as the reference to FP64 arithmetic with the same
+    sweep count."""
+    d = np.abs(r.astype(np.float64) - ref)
+    if d.max() <= 1e-6 and d.sum() <= 1e-5:
+        return
+    exact, _, _ = O.pr_f64(g.row_ptr, g.col, damping=D, tol=0.0, max_iters=sweeps)
+    e_ref, e_eng = np.abs(ref - exact), np.abs(r - exact)
+    assert e_ref.max() > 1e-6, "the reference is accurate here, so the engine must match it"
+    assert e_eng.max() <= e_ref.max() and e_eng.sum() <= e_ref.sum(), (e_eng.max(), e_ref.max())
+
+
+def graphs():
+    rng = np.random.default_rng(12)
+    n = 100_003  # four blocks, the last one partial
+    src = rng.integers(0, n, 400_000).astype(np.uint32)
+    dst = (rng.pareto(1.2, 400_000) * 40).astype(np.uint32) % n  # skewed: hubs, dangling vertices, empty rows
+    star_n = 70_001
+    return {
+        "rmat15": G.rmat(15, 16, 4),
+        "rmat18": G.rmat(18, 16, 8),
+        "directed": G.from_edges(src, dst, n),
+        "star": G.from_edges(np.zeros(star_n - 1, np.uint32), np.arange(1, star_n, dtype=np.uint32), star_n,
+                             symmetrize=True),
+        "grid": G.grid(200_000),
+        "wide": wide_group_graph(),
+    }
+
+
+def wide_group_graph():
+    """Rows of 14 entries on average fill the first block; 20 more rows of one entry each, whose sources lie far
+    apart, make a 32-entry group of the next block span more than 2^17 ids: a wide group in the packed format."""
+    rng = np.random.default_rng(5)
+    n = 300_000
+    src = np.concatenate([rng.integers(0, n, 400_000), np.arange(20) * 15_000 + 7]).astype(np.uint32)
+    dst = np.concatenate([rng.integers(0, 28_672, 400_000), 200_000 + np.arange(20)]).astype(np.uint32)
+    return G.from_edges(src, dst, n)
+
+
+@pytest.fixture(scope="module")
+def cases():
+    return graphs()
+
+
+@pytest.mark.parametrize("name", ["rmat15", "rmat18", "directed", "grid", "wide"])
+def test_parity_with_page_rank_v10(gpu, cases, name):
+    g = cases[name]
+    deg = g.out_degree()
+    r, st, info = solve(g, deg)
+    assert info["blocked"] == 1
+    ref, _, errs = O.jacobi_f32(g.row_ptr, g.col, deg, D, 0.0, 20)
+    parity_or_more_accurate(r, ref, g, 20)
+    assert np.allclose(st.errors, errs, rtol=1e-4, atol=1e-5)
+    r, st, _ = solve(g, deg, thr=1e-4, iters=100)
+    ref, it, _ = O.jacobi_f32(g.row_ptr, g.col, deg, D, 1e-4, 100)
+    assert st.converged and st.iterations == it
+    parity_or_more_accurate(r, ref, g, it)
+
+
+def test_hub_row_more_accurate_than_serial_fp32(gpu, cases):
+    """A 70,000-leaf star: the reference's serial FP32 sum over the hub's row is off by more than 1e-6; the
+    exact fixed-point row sum is closer to FP64 arithmetic than it."""
+    g = cases["star"]
+    deg = g.out_degree()
+    r, _, _ = solve(g, deg, iters=10)
+    ref, _, _ = O.jacobi_f32(g.row_ptr, g.col, deg, D, 0.0, 10)
+    exact, _, _ = O.pr_f64(g.row_ptr, g.col, damping=D, tol=0.0, max_iters=10)
+    e_ref = np.abs(ref - exact).max()
+    e_eng = np.abs(r - exact).max()
+    assert e_ref > 1e-6 and e_eng <= e_ref and e_eng < 1e-7, (e_eng, e_ref)
+
+
+@pytest.mark.parametrize("name", REFDATA_NAMES)
+def test_reference_test_matrices(gpu, refdata, name):
+    g = refdata[name]
+    rp, cl, deg = g["row_ptr"], g["col"], g["deg"]
+    with Graph(rp, cl) as h:
+        out = np.empty(len(rp) - 1, np.float32)
+        h.page_rank(deg, out, D, 0.0, 20)
+        close(out, g["v10_20"])
+        st = h.page_rank(deg, out, D, 1e-4, 100)
+        assert st.iterations == int(g["v10_thr_iters"][0])
+        close(out, g["v10_thr"])
+
+
+@pytest.mark.parametrize("name", ["rmat18", "directed", "wide"])
+def test_bitwise_equal_for_any_piece_size_launch_and_format(gpu, cases, name, monkeypatch):
+    g = cases[name]
+    deg = g.out_degree()
+    a, sa, _ = solve(g, deg)
+    b, _, _ = solve(g, deg, launch="stream")
+    outs = []
+    for piece in ("1000", "65536", "5000000"):
+        monkeypatch.setenv("NWGPU_BLOCK_PIECE_ENTRIES", piece)
+        outs.append(solve(g, deg)[0])
+    monkeypatch.delenv("NWGPU_BLOCK_PIECE_ENTRIES")
+    for loads in ("4", "16"):
+        monkeypatch.setenv("NWGPU_BLOCK_LOADS", loads)
+        outs.append(solve(g, deg)[0])
+    monkeypatch.delenv("NWGPU_BLOCK_LOADS")
+    monkeypatch.setenv("NWGPU_BLOCK_FORMAT", "wide")  # 6-byte entries instead of packed words
+    outs.append(solve(g, deg)[0])
+    monkeypatch.setenv("NWGPU_BLOCK_PIECE_ENTRIES", "3000")
+    outs.append(solve(g, deg)[0])
+    monkeypatch.delenv("NWGPU_BLOCK_PIECE_ENTRIES")
+    monkeypatch.delenv("NWGPU_BLOCK_FORMAT")
+    for x in [b] + outs:
+        assert np.array_equal(a.view(np.uint32), x.view(np.uint32))
+    again, sb, _ = solve(g, deg)
+    assert np.array_equal(a.view(np.uint32), again.view(np.uint32))
+    assert np.array_equal(sa.errors, sb.errors)
+
+
+def test_at_least_as_accurate_as_binned(gpu, cases, monkeypatch):
+    g = cases["rmat18"]
+    deg = g.out_degree()
+    a, _, _ = solve(g, deg, iters=30)
+    monkeypatch.setenv("NWGPU_SWEEP", "binned_hot")
+    b, _, info = solve(g, deg, iters=30)
+    assert info["blocked"] == 0
+    exact, _, _ = O.pr_f64(g.row_ptr, g.col, damping=D, tol=0.0, max_iters=30)
+    assert np.abs(a - exact).max() <= np.abs(b - exact).max() * 1.05 + 1e-12
+    close(a, b)
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_shards_equal_single_gpu_bitwise(gpu, cases, world):
+    """Exact row sums do not depend on the partition: a row-sharded solve (blocked sweep per shard) gives the
+    single-GPU ranks bit for bit."""
+    import torch
+    g = cases["rmat18"]
+    deg = g.out_degree()
+    ref, _, _ = solve(g, deg)
+    dev = torch.device("cuda")
+    bounds, stride = S.shard_bounds(g.row_ptr, world)
+    shards = [S.GpuShard(g.row_ptr, g.col, world, q, bounds, stride) for q in range(world)]
+    out = torch.empty(g.n, dtype=torch.float32, device=dev)
+    st = S.run(shards, S.LocalExchange(), deg, out, D, 0.0, 20, device=dev)
+    for s in shards:
+        s.release()
+    assert st.iterations == 20
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), ref.view(np.uint32))

@@ -274,7 +274,7 @@ def test_scale20_properties(gpu):
     assert abs(float(r.astype(np.float64).sum()) - float(ref.astype(np.float64).sum())) < 1e-5
 
 
-@pytest.mark.parametrize("sweep", ["binned", "binned_hot", "base", "hot", "hot512"])
+@pytest.mark.parametrize("sweep", ["blocked", "binned", "binned_hot", "base", "hot", "hot512"])
 def test_sweep_variants_agree(gpu, sweep, monkeypatch):
     """Every sweep kernel variant (degree-binned, merge-path with L1 hot ids,
     merge-path with the hot ids in shared memory) meets the same bar."""
