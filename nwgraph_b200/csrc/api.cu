@@ -372,7 +372,7 @@ SweepArgs make_sweep_args(nwgpu_graph* g, float damping, float base, int telepor
 }
 
 bool use_blocked(const nwgpu_graph* g, const BinPlan* plan, int mode) {
-  return g->bplan.ok && mode == kModePlain && (plan == nullptr || plan == &g->plan);
+  return g->bplan.ok && !g->blocked_off && mode == kModePlain && (plan == nullptr || plan == &g->plan);
 }
 
 int build_loop_graph(nwgpu_graph* g, const SweepArgs& proto, const BinPlan* plan, int mode) {
@@ -413,13 +413,15 @@ int build_loop_graph(nwgpu_graph* g, const SweepArgs& proto, const BinPlan* plan
   g->cg_args = proto;
   g->cg_plan = plan;
   g->cg_mode = mode;
+  g->cg_blocked = use_blocked(g, plan, mode);
   return NWGPU_OK;
 }
 
 // The arguments a cached loop graph baked in.
 bool same_loop(const nwgpu_graph* g, const SweepArgs& y, const BinPlan* plan, int mode) {
   const SweepArgs& x = g->cg_args;
-  return g->cg_plan == plan && g->cg_mode == mode && x.damping == y.damping && x.base == y.base &&
+  return g->cg_plan == plan && g->cg_mode == mode && g->cg_blocked == use_blocked(g, plan, mode) &&
+         x.damping == y.damping && x.base == y.base &&
          x.teleport == y.teleport && x.seed == y.seed && x.row_ptr == y.row_ptr && x.col == y.col && x.w == y.w &&
          x.vbase == y.vbase && x.vaux == y.vaux && x.push_threshold == y.push_threshold;
 }
@@ -465,6 +467,7 @@ int run_sweeps(nwgpu_graph* g, const SweepArgs& a, uint32_t launch, uint64_t max
     }
   }
   *fin = *g->h_st;
+  if (fin->fault == kFaultDegrees && use_blocked(g, plan, mode)) return kRetryBinned;
   if (fin->fault) return fail(NWGPU_ERR_CUDA, "a bounded device wait gave up (fault word %u)", fin->fault);
   return NWGPU_OK;
 }
@@ -527,13 +530,25 @@ int solve_single(nwgpu_graph* g, const uint32_t* out_degree, float* ranks, float
   h.done = (max_iters == 0) ? 1u : 0u;
   *g->h_st = h;
   CK(cudaMemcpyAsync(g->st, g->h_st, sizeof(PrState), cudaMemcpyHostToDevice, s), "copy state");
+  const BinPlan* plan = g->plan.ok ? &g->plan : nullptr;
+  if (use_blocked(g, plan, kModePlain)) CK(launch_check_degrees(g->bplan, g->deg, g->st, g->sms, s), "check degrees");
   SweepArgs a = make_sweep_args(g, damping, base, teleport, seed);
   CK(launch_pr_init(a, n, init, g->sms, s), "pr_init");
 
   trace.mark("degrees + init");
   CK(cudaEventRecord(g->ev0, s), "cudaEventRecord");
   PrState fin{};
-  rc = run_sweeps(g, a, opt.launch, max_iters, s, &fin, g->plan.ok ? &g->plan : nullptr, kModePlain);
+  rc = run_sweeps(g, a, opt.launch, max_iters, s, &fin, plan, kModePlain);
+  if (rc == kRetryBinned) {
+    // out-degrees below the entry counts: the binned sweep, whose FP32 sums follow the reference for any degrees
+    g->blocked_off = true;
+    *g->h_st = h;
+    CK(cudaMemcpyAsync(g->st, g->h_st, sizeof(PrState), cudaMemcpyHostToDevice, s), "copy state");
+    CK(launch_pr_init(a, n, init, g->sms, s), "pr_init");
+    CK(cudaEventRecord(g->ev0, s), "cudaEventRecord");
+    rc = run_sweeps(g, a, opt.launch, max_iters, s, &fin, plan, kModePlain);
+    g->blocked_off = false;
+  }
   if (rc) return rc;
   CK(cudaEventRecord(g->ev1, s), "cudaEventRecord");
   trace.mark("sweeps");
@@ -590,6 +605,7 @@ int pr_solve_queue(nwgpu_graph* g, const uint32_t* d_degree, float* d_ranks, flo
   h.threshold = (double)threshold;
   *g->h_st = h;
   CK(cudaMemcpyAsync(g->st, g->h_st, sizeof(PrState), cudaMemcpyHostToDevice, s), "copy state");
+  if (use_blocked(g, &g->plan, kModePlain)) CK(launch_check_degrees(g->bplan, g->deg, g->st, g->sms, s), "check degrees");
   const SweepArgs a = make_sweep_args(g, damping, base, kTeleportUniform, 0u);
   CK(launch_pr_init(a, n, init, g->sms, s), "pr_init");
   if (!g->cg_exec || !same_loop(g, a, &g->plan, kModePlain)) {
@@ -605,6 +621,24 @@ int pr_solve_queue(nwgpu_graph* g, const uint32_t* d_degree, float* d_ranks, flo
 int pr_solve_finish(nwgpu_graph* g, float* d_ranks, float damping, float threshold, uint64_t max_iters, cudaStream_t s,
                     nwgpu_pr_stats* stats) {
   PrState fin = *g->h_st;
+  if (fin.fault == kFaultDegrees && use_blocked(g, &g->plan, kModePlain)) {
+    // out-degrees below the entry counts: solve again with the binned sweep
+    const float init = (float)(1.0 / (double)g->n);
+    PrState     h = {};
+    h.max_iters = max_iters;
+    h.chunk_end = kGraphChunk;
+    h.threshold = (double)threshold;
+    g->blocked_off = true;
+    *g->h_st = h;
+    CK(cudaMemcpyAsync(g->st, g->h_st, sizeof(PrState), cudaMemcpyHostToDevice, s), "copy state");
+    const SweepArgs a = make_sweep_args(g, damping, (float)((1.0 - (double)damping) / (double)g->n), kTeleportUniform, 0u);
+    CK(launch_pr_init(a, g->n, init, g->sms, s), "pr_init");
+    int rc = run_sweeps(g, a, NWGPU_LAUNCH_GRAPH, max_iters, s, &fin, &g->plan, kModePlain);
+    g->blocked_off = false;
+    if (rc) return rc;
+    CK(launch_gather_f32(g->rank, g->g.perm, d_ranks, g->n, g->sms, s), "permute ranks");
+    CK(cudaStreamSynchronize(s), "permute ranks");
+  }
   if (fin.fault) return fail(NWGPU_ERR_CUDA, "a bounded device wait gave up (fault word %u)", fin.fault);
   if (!fin.done) {  // more sweeps than one graph launch runs: the loop goes on as nwgpu_pr_run's does
     const SweepArgs a = make_sweep_args(g, damping, (float)((1.0 - (double)damping) / (double)g->n), kTeleportUniform, 0u);

@@ -12,6 +12,10 @@ namespace nwgpu {
 // per SM).
 constexpr uint32_t kBlockRows = 28672;
 constexpr int      kBlockedThreads = 1024;
+// PrState::fault bit set before a solve when some out_degree[j] is below the
+// number of entries whose column is j: then row sums are no longer bounded by
+// 1 and could overflow the fixed-point sums, so the solve runs the binned sweep.
+constexpr unsigned int kFaultDegrees = 0x40000000u;
 
 // One unit of work of a sweep: entries [e0, e1) of block `block` in the
 // blocked entry order. A block of more than the piece size is cut into
@@ -63,6 +67,7 @@ struct BlockPlan {
   uint32_t*           blk_e0 = nullptr;
   uint32_t*           blk_g0 = nullptr;
   uint64_t            wide_groups = 0;
+  uint32_t*           outcount = nullptr;  // n: entries whose column is j (the true out-degrees)
   BlockItem*          items = nullptr;
   uint32_t            num_items = 0;
   uint32_t*           zoff = nullptr;
@@ -88,6 +93,8 @@ cudaError_t build_block_plan(const uint32_t* row_ptr, const uint32_t* col, uint6
 // Rebuilds p's work list for another piece size (the entry order stays).
 cudaError_t set_block_items(BlockPlan* p, int sms, uint64_t piece_entries, cudaStream_t s);
 BlockedArgs make_blocked_args(const BlockPlan& p, const SweepArgs& sw, uint64_t n);
+// Sets kFaultDegrees in st->fault when some deg[j] (internal order) < outcount[j].
+cudaError_t launch_check_degrees(const BlockPlan& p, const uint32_t* deg, PrState* st, int sms, cudaStream_t s);
 cudaError_t configure_blocked_kernels();
 cudaError_t launch_blocked_sweep(const BlockedArgs& a, int sweep_grid, int loads, cudaStream_t s);
 cudaError_t add_blocked_nodes(cudaGraph_t body, const BlockedArgs& a, int sweep_grid, int loads);

@@ -61,7 +61,7 @@ struct WprBuffers {
   double*    part = nullptr;
   double*    dout = nullptr;
   float*     f = nullptr;        // n: dL/dw factors d r_j / s_j
-  float*     q = nullptr;        // n: dL/dw offsets q_j
+  double*    q = nullptr;        // n: dL/dw offsets q_j (FP64)
   void       release(cudaStream_t s);
 };
 
@@ -115,6 +115,8 @@ struct nwgpu_graph {
   nwgpu::BinPlan plan;
   // Destination-blocked sweep (plain and single-seed solves), built at creation unless NWGPU_SWEEP names another.
   nwgpu::BlockPlan bplan;
+  bool             blocked_off = false;  // this solve's degrees failed the blocked sweep's check: binned sweep
+  bool             cg_blocked = false;   // the cached loop graph runs the blocked sweep
   int          finish_grid = 1;  // finishing-kernel CTAs
   uint64_t     device_bytes = 0;
 
@@ -195,6 +197,8 @@ nwgpu_pr_options read_options(const nwgpu_pr_options* options);
 constexpr uint32_t kGraphNoBlockedPlan = 0x80000000u;
 // Whether a solve in `mode` over `plan` (the handle's forward plan or none) runs the blocked sweep.
 bool use_blocked(const nwgpu_graph* g, const BinPlan* plan, int mode);
+// run_sweeps' result when the degree check stopped a blocked solve before its first sweep (internal).
+constexpr int kRetryBinned = 1000;
 // Out-row CSR, its bins and the buffers of the weighted solve and its adjoint.
 int ensure_wpr(nwgpu_graph* g);
 // api_tune.cu: picks the binned sweep's launch shape and hub tiers for g

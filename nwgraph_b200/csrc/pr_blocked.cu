@@ -164,6 +164,7 @@ __global__ void __launch_bounds__(kBlockedThreads, 1) pr_blocked_sweep_kernel(co
   PrState*            st = a.sw.st;
   if (a.sw.use_cond && blockIdx.x == 0 && tid == 0) cudaGraphSetConditional(a.sw.cond, 0u);
   if (*(volatile unsigned int*)&st->done) return;
+  if (*(volatile unsigned int*)&st->fault) return;  // degrees below the entry counts: the finishing kernel stops
   const unsigned long long it = *(volatile unsigned long long*)&st->iter;
   const float* __restrict__ cin = (it & 1ull) ? a.sw.contrib1 : a.sw.contrib0;
   float* __restrict__ cout = (it & 1ull) ? a.sw.contrib0 : a.sw.contrib1;
@@ -233,9 +234,10 @@ __global__ void __launch_bounds__(1024) pr_blocked_finish_kernel(const BlockedAr
     st->iter = done_iters;
     st->last_error = e;
     if (a.sw.err_hist && it < a.sw.err_cap) a.sw.err_hist[it] = e;  // the first err_cap sweeps
-    const bool conv = e < st->threshold;
+    const bool fault = *(volatile unsigned int*)&st->fault != 0u;
+    const bool conv = !fault && e < st->threshold;
     const bool abort = a.sw.abort_word && *a.sw.abort_word;
-    const bool done = conv || done_iters >= st->max_iters || abort;
+    const bool done = conv || done_iters >= st->max_iters || abort || fault;
     st->converged = conv ? 1u : 0u;
     st->aborted = (abort && !conv) ? 1u : 0u;
     st->done = done ? 1u : 0u;
@@ -347,6 +349,29 @@ __global__ void __launch_bounds__(256) pack_groups_kernel(const unsigned long lo
   }
 }
 
+// outcount[source] += entries, one atomic per run of equal sources in a warp's
+// 32 consecutive sorted entries.
+__global__ void count_sources_kernel(const unsigned long long* __restrict__ keys, uint64_t nnz, int id_bits,
+                                     uint32_t* __restrict__ outcount) {
+  const unsigned long long mask = (1ull << id_bits) - 1ull;
+  const uint64_t           stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < nnz; base += stride) {
+    const uint64_t k = base + threadIdx.x;
+    const bool     ok = k < nnz;
+    const uint32_t src = ok ? (uint32_t)(keys[k] & mask) : 0xffffffffu;
+    const unsigned same = __match_any_sync(kFullMask, src);
+    if (ok && (threadIdx.x & 31u) == (unsigned)(__ffs(same) - 1)) atomicAdd(outcount + src, (uint32_t)__popc(same));
+  }
+}
+
+__global__ void check_degrees_kernel(const uint32_t* __restrict__ deg, const uint32_t* __restrict__ outcount,
+                                     uint64_t n, PrState* st) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  bool           bad = false;
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) bad |= deg[j] < outcount[j];
+  if (__any_sync(kFullMask, bad) && (threadIdx.x & 31u) == 0u) atomicOr(&st->fault, kFaultDegrees);
+}
+
 template <class T>
 void free_ptr(T*& p, cudaStream_t s) {
   pool_free(p, s);
@@ -362,6 +387,7 @@ void BlockPlan::release(cudaStream_t s) {
   free_ptr(wide, s);
   free_ptr(blk_e0, s);
   free_ptr(blk_g0, s);
+  free_ptr(outcount, s);
   packed = false;
   wide_groups = 0;
   free_ptr(items, s);
@@ -426,6 +452,10 @@ cudaError_t build_block_plan(const uint32_t* row_ptr, const uint32_t* col, uint6
       p->dst = vb.Current();
       vals1 = t;
     }
+    BK(pool_alloc_n(&p->outcount, id_bound + kPad, s));
+    BK(cudaMemsetAsync(p->outcount, 0, (id_bound + kPad) * sizeof(uint32_t), s));
+    count_sources_kernel<<<sms * 8, 256, 0, s>>>(kb.Current(), nnz, id_bits, p->outcount);
+    BK(cudaGetLastError());
     BK(pool_alloc_n(&p->src, nnz + kPad, s));
     if (packed && id_bound <= (uint64_t)kWideGroup) {
       // block and group offsets, then one word per entry and one base per group
@@ -534,6 +564,12 @@ cudaError_t set_block_items(BlockPlan* p, int sms, uint64_t piece_entries, cudaS
   p->bytes = (nnz + kPad) * (p->packed ? 4 : 6) + (p->packed ? (nnz / 32 + nb) * 4 + p->wide_groups * 128 : 0) +
              items.size() * sizeof(BlockItem) + (uint64_t)nb * 16 + zrows * 8;
   return cudaSuccess;
+}
+
+cudaError_t launch_check_degrees(const BlockPlan& p, const uint32_t* deg, PrState* st, int sms, cudaStream_t s) {
+  if (!p.outcount || !p.n) return cudaSuccess;
+  check_degrees_kernel<<<sms * 4, 256, 0, s>>>(deg, p.outcount, p.n, st);
+  return cudaGetLastError();
 }
 
 BlockedArgs make_blocked_args(const BlockPlan& p, const SweepArgs& sw, uint64_t n) {

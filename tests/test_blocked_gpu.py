@@ -185,3 +185,19 @@ def test_shards_equal_single_gpu_bitwise(gpu, cases, world):
         s.release()
     assert st.iterations == 20
     assert np.array_equal(out.cpu().numpy().view(np.uint32), ref.view(np.uint32))
+
+
+def test_degrees_below_entry_counts_take_the_binned_sweep(gpu, cases, monkeypatch):
+    """Fixed-point row sums are bounded by 1 only when every out_degree[j] is at least the number of entries
+    whose column is j (build_degrees gives exactly that). With smaller degrees the solve checks, stops before
+    its first sweep, and runs the binned sweep, whose FP32 sums follow the reference for any degrees: the same
+    ranks as a binned solve, bit for bit, and within parity of the restated page_rank_v10."""
+    g = cases["rmat15"]
+    deg = np.maximum(g.out_degree() // 2, 1).astype(np.uint32)
+    a, sa, _ = solve(g, deg, iters=10)
+    monkeypatch.setenv("NWGPU_SWEEP", "binned_hot")
+    b, sb, _ = solve(g, deg, iters=10)
+    assert sa.iterations == sb.iterations == 10
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    ref, _, _ = O.jacobi_f32(g.row_ptr, g.col, deg, D, 0.0, 10)
+    assert np.allclose(a, ref, rtol=1e-5, atol=1e-6)
