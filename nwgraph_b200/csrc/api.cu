@@ -854,9 +854,9 @@ int finish_create(nwgpu_graph* g, const float* weights, uint32_t flags, nwgpu_gr
     if (rc) return bail(rc);
   }
   trace.mark("bins");
-  // The destination-blocked sweep of plain solves: relabelled unweighted graphs, unless NWGPU_SWEEP names
-  // another sweep (NWGPU_BLOCK_PIECE_ENTRIES sets the largest work item).
-  if (g->relabelled && !weights && !(flags & kGraphNoBlockedPlan) && (!which || !strcmp(which, "blocked"))) {
+  // The destination-blocked sweep of plain solves (NWGPU_SWEEP=blocked): relabelled unweighted graphs
+  // (NWGPU_BLOCK_PIECE_ENTRIES sets the largest work item).
+  if (g->relabelled && !weights && !(flags & kGraphNoBlockedPlan) && which && !strcmp(which, "blocked")) {
     const long piece = env_int("NWGPU_BLOCK_PIECE_ENTRIES", 0);
     const char* fmt = getenv("NWGPU_BLOCK_FORMAT");  // "wide": 6-byte entries instead of the packed 4-byte words
     if ((e = build_block_plan(g->g.row_ptr, g->g.col, n, nnz, n, sms, piece > 0 ? (uint64_t)piece : 0,

@@ -237,12 +237,12 @@ int nwgpu_shard_create(const uint32_t* row_ptr, const uint32_t* col, uint64_t n,
     g->plan.bin.l1_ids = (uint32_t)(hub + 16384);
   }
   g->finish_grid = 1;
-  // The blocked sweep of the local rows, as the single-GPU engine runs it: row
-  // sums are exact fixed-point sums, so each row's value does not depend on
-  // how the rows are cut into blocks or shards, and the sharded ranks equal
-  // the single-GPU engine's bit for bit.
+  // With NWGPU_SWEEP=blocked, the blocked sweep of the local rows, as the
+  // single-GPU engine then runs it: row sums are exact fixed-point sums, so
+  // each row's value does not depend on how the rows are cut into blocks or
+  // shards, and the sharded ranks equal the single-GPU engine's bit for bit.
   const char* which = getenv("NWGPU_SWEEP");
-  if (sh->rows && (!which || !strcmp(which, "blocked"))) {
+  if (sh->rows && which && !strcmp(which, "blocked")) {
     const char* fmt = getenv("NWGPU_BLOCK_FORMAT");
     if ((e = build_block_plan(g->g.row_ptr, g->g.col, sh->rows, m, (uint64_t)world * stride, g->sms, 0,
                               !(fmt && !strcmp(fmt, "wide")), &g->bplan, s)) != cudaSuccess) {

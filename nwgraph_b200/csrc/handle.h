@@ -113,7 +113,7 @@ struct nwgpu_graph {
   float        tune_us = 0.f;    // the chosen parameters' time per sweep when tuned
   // Degree-binned sweep (relabelled graphs with non-increasing row lengths).
   nwgpu::BinPlan plan;
-  // Destination-blocked sweep (plain and single-seed solves), built at creation unless NWGPU_SWEEP names another.
+  // Destination-blocked sweep (plain and single-seed solves), built at creation with NWGPU_SWEEP=blocked.
   nwgpu::BlockPlan bplan;
   bool             blocked_off = false;  // this solve's degrees failed the blocked sweep's check: binned sweep
   bool             cg_blocked = false;   // the cached loop graph runs the blocked sweep

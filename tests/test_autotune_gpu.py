@@ -1,9 +1,9 @@
-"""Autotuner (NWGPU_GRAPH_AUTOTUNE) of the blocked sweep (entries in flight,
-piece size) and, with NWGPU_SWEEP=binned*, of the binned sweep (launch shape,
-hub tiers): every candidate gives bitwise-equal ranks, so a tuned graph must
-reproduce the default graph's ranks bit for bit; choices are cached per graph
-signature in the process and, with NWGPU_TUNE_CACHE, in a file that a later
-process reuses."""
+"""Autotuner (NWGPU_GRAPH_AUTOTUNE) of the binned sweep (launch shape, hub
+tiers) and, with NWGPU_SWEEP=blocked, of the blocked sweep (entries in
+flight, piece size): every candidate gives bitwise-equal ranks, so a tuned
+graph must reproduce the default graph's ranks bit for bit; choices are
+cached per graph signature in the process and, with NWGPU_TUNE_CACHE, in a
+file that a later process reuses."""
 import json
 import os
 import subprocess
@@ -74,10 +74,25 @@ def test_cache_file_is_reused_by_another_process(gpu, tmp_path):
                                   text=True).stdout.strip().splitlines()[-1])
     assert a["tuned"] == 1 and path.exists()
     lines = path.read_text().strip().splitlines()
-    assert len(lines) == 1 and lines[0].startswith("blocked sms=")
+    assert len(lines) == 1 and lines[0].startswith("binned sms=")
     b = json.loads(subprocess.run([sys.executable, "-c", code], env=env, check=True, capture_output=True,
                                   text=True).stdout.strip().splitlines()[-1])
     assert b["tuned"] == 2
     for k in ("sweep_threads", "hub_smem_ids", "hub_l1_ids", "block_loads", "block_piece_entries"):
         assert a[k] == b[k]
 
+
+
+def test_blocked_tuning_bitwise_equal_and_cached(gpu, monkeypatch):
+    monkeypatch.delenv("NWGPU_TUNE_CACHE", raising=False)
+    monkeypatch.setenv("NWGPU_SWEEP", "blocked")
+    g = G.rmat(17, 16, 6)
+    deg = g.out_degree()
+    r0, i0 = solve(g, deg)
+    r1, i1 = solve(g, deg, autotune=True)
+    r2, i2 = solve(g, deg, autotune=True)
+    assert i0["blocked"] == 1 and i0["tuned"] == 0
+    assert i1["tuned"] in (1, 2) and i2["tuned"] == 2
+    assert (i1["block_loads"], i1["block_piece_entries"]) == (i2["block_loads"], i2["block_piece_entries"])
+    assert np.array_equal(r0.view(np.uint32), r1.view(np.uint32))
+    assert np.array_equal(r0.view(np.uint32), r2.view(np.uint32))

@@ -182,7 +182,10 @@ def test_c5_weighted_adjoint_rmat20(gpu):
     dw = np.empty(g.nnz, np.float32)
     dt = np.empty(g.n, np.float32)
     with Graph(g.row_ptr, g.col, weights=w) as h:
-        h.weighted_page_rank(None, r, D, 1e-7, 1000)
+        # forward to an L1 change of 1e-9 (50 sweeps): dL/dw is proportional to r_j, and at 1e-7 (25 sweeps) the
+        # ranks of the least-ranked vertices still carry 0.5% relative error, which moves their gradients by
+        # 1.2e-3 of the largest one
+        h.weighted_page_rank(None, r, D, 1e-9, 1000)
         sb = h.page_rank_vjp(r, cvec, dw, dt, D, 1e-7 * float(np.abs(cvec).sum()), 3000)
     assert sb.converged
     r64, _, _ = O.pr_f64(g.row_ptr, g.col, weights=w, damping=D, tol=1e-15)
