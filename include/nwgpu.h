@@ -269,8 +269,7 @@ int nwgpu_wpr_run(nwgpu_graph* g, const float* teleport, float* ranks, float dam
  * by implicit differentiation, with the same sweep over the out-row CSR (no
  * forward iterates are stored), to an FP64 L1 change < threshold, then writes
  *   dL_dt[v] = (1 - d) l_v                                (n, may be NULL)
- *   dL_dw[k] = d r_j / s_j (l_i - q_j),  q_j = sum_{k': col[k'] = j} (w_k' / s_j) l_{row(k')}
- * (q_j summed in FP64, the gradient formed in FP64 and rounded once)
+ *   dL_dw[k] = d r_j / s_j (l_i - q_j),  q_j = (l_j - dL_dr_j) / d
  * for entry k of row i with col[k] = j, in the input entry order (nnz, may be
  * NULL). stats describe the adjoint solve. The out-rows must be in the
  * relabelled length order, which holds for symmetric graphs; otherwise

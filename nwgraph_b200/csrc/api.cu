@@ -847,7 +847,8 @@ int finish_create(nwgpu_graph* g, const float* weights, uint32_t flags, nwgpu_gr
   g->finish_grid = finish_grid_for(g->tiling.num_tiles);
   if ((e = cudaStreamSynchronize(g->stream)) != cudaSuccess) return bail(cuda_fail(e, "graph create"));
   trace.mark("tiling");
-  const bool want_binned = which ? (!strcmp(which, "binned") || !strcmp(which, "binned_hot")) : true;
+  const bool want_binned =
+      which ? (!strcmp(which, "binned") || !strcmp(which, "binned_hot") || !strcmp(which, "blocked")) : true;
   if (g->relabelled && want_binned) {
     // NWGPU_SWEEP=binned keeps the hubs in L1 only (256-thread CTAs)
     rc = build_bin_plan(g, g->g.row_ptr, n, !which || strcmp(which, "binned") != 0, &g->plan);

@@ -16,7 +16,9 @@
 // bound, 0 keeps every graph in the batch) are solved alone by the
 // single-graph engine (relabelled, degree-binned sweep), which sweeps them
 // about twice as fast as the merge-path batch sweep; launching them one by one
-// costs little next to their size. In the batch they are empty members (no
+// costs little next to their size, and they are spread round robin over a
+// few streams (NWGPU_RAGGED_SOLO_STREAMS, default 4) so the short sweeps of
+// the smaller ones overlap. In the batch they are empty members (no
 // rows, no tiles); their handles read and write their slices of the batch's
 // degree and rank arrays. Whether a graph is solved alone depends only on its
 // own size, so a graph gets the same result in any batch.
@@ -30,6 +32,7 @@
 namespace nwgpu {
 
 constexpr uint64_t kRaggedSoloEntries = 1ull << 22;
+constexpr long     kRaggedSoloStreams = 4;  // NWGPU_RAGGED_SOLO_STREAMS
 
 struct RaggedSolo {
   uint32_t     g = 0;  // the graph's index in the batch
@@ -40,8 +43,11 @@ struct RaggedSolo {
 struct RaggedBatch {
   int          device = 0, sms = 0;
   std::vector<RaggedSolo> solos;  // graphs solved alone (empty members of the batch)
-  cudaStream_t solo_stream = nullptr;  // the solo graphs run here, beside the batch's sweep loop
-  cudaEvent_t  solo_done = nullptr;
+  // The solo graphs run on these streams, round robin, beside the batch's
+  // sweep loop: the short sweeps of mid-size graphs overlap one another's
+  // launch gaps and finishing kernels.
+  std::vector<cudaStream_t> solo_streams;
+  std::vector<cudaEvent_t>  solo_done;
   cudaStream_t stream = nullptr;
   uint32_t     num_graphs = 0;
   uint64_t     nv = 0, nnz = 0, nrp = 0;  // vertices, entries, row pointers of the batch
@@ -79,10 +85,10 @@ struct RaggedBatch {
     return e;
   }
   ~RaggedBatch() {
-    if (solo_stream) cudaStreamSynchronize(solo_stream);
+    for (cudaStream_t t : solo_streams) cudaStreamSynchronize(t);
     for (RaggedSolo& S : solos) delete S.h;  // not nwgpu_graph_destroy: that clears the caller's last error
-    if (solo_done) cudaEventDestroy(solo_done);
-    if (solo_stream) cudaStreamDestroy(solo_stream);
+    for (cudaEvent_t ev : solo_done) cudaEventDestroy(ev);
+    for (cudaStream_t t : solo_streams) cudaStreamDestroy(t);
     if (stream) cudaStreamSynchronize(stream);
     if (cg_exec) cudaGraphExecDestroy(cg_exec);
     if (cg) cudaGraphDestroy(cg);
@@ -331,9 +337,18 @@ int nwgpu_batch_create(uint64_t num_graphs, const uint64_t* vertex_offsets, cons
 #undef BK
   // The graphs solved alone: single-graph handles over the caller's slices.
   if (!b->solos.empty()) {
-    if ((e = cudaStreamCreateWithFlags(&b->solo_stream, cudaStreamNonBlocking)) != cudaSuccess ||
-        (e = cudaEventCreateWithFlags(&b->solo_done, cudaEventDisableTiming)) != cudaSuccess)
-      return bail(cuda_fail(e, "solo stream"));
+    const char* ns_env = getenv("NWGPU_RAGGED_SOLO_STREAMS");
+    long        ns = ns_env && *ns_env ? strtol(ns_env, nullptr, 10) : kRaggedSoloStreams;
+    if (ns < 1) ns = 1;
+    if ((size_t)ns > b->solos.size()) ns = (long)b->solos.size();
+    for (long i = 0; i < ns; ++i) {
+      cudaStream_t t = nullptr;
+      cudaEvent_t  ev = nullptr;
+      if ((e = cudaStreamCreateWithFlags(&t, cudaStreamNonBlocking)) != cudaSuccess) return bail(cuda_fail(e, "solo stream"));
+      b->solo_streams.push_back(t);
+      if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return bail(cuda_fail(e, "solo stream"));
+      b->solo_done.push_back(ev);
+    }
   }
   for (RaggedSolo& S : b->solos) {
     rc = nwgpu_graph_create(row_ptr + (vertex_offsets[S.g] + S.g), col + entry_offsets[S.g], nullptr, S.n, S.nnz,
@@ -395,7 +410,9 @@ int nwgpu_pr_ragged(nwgpu_batch* b, const uint32_t* out_degree, float* ranks, fl
   bool                        solos_run = b->solos.empty();
   auto                        run_solos = [&]() -> int {
     solos_run = true;
-    CK(cudaStreamWaitEvent(b->solo_stream, b->ev0, 0), "solo stream");
+    const size_t nstreams = b->solo_streams.size();
+    auto         stream_of = [&](size_t i) { return b->solo_streams[i % nstreams]; };
+    for (cudaStream_t t : b->solo_streams) CK(cudaStreamWaitEvent(t, b->ev0, 0), "solo stream");
     auto graph_fail = [&](int rc, uint32_t g) {
       char msg[400];
       nwgpu_last_error(msg, sizeof(msg));
@@ -408,16 +425,16 @@ int nwgpu_pr_ragged(nwgpu_batch* b, const uint32_t* out_degree, float* ranks, fl
       for (size_t i = 0; i < b->solos.size(); ++i) {
         const RaggedSolo& S = b->solos[i];
         bool              q = false;
-        int rc = pr_solve_queue(S.h, b->deg + S.v0, b->rank + S.v0, damping, threshold, max_iters, b->solo_stream, &q);
+        int rc = pr_solve_queue(S.h, b->deg + S.v0, b->rank + S.v0, damping, threshold, max_iters, stream_of(i), &q);
         if (rc) return graph_fail(rc, S.g);
         queued[i] = q ? 1 : 0;
       }
-      CK(cudaStreamSynchronize(b->solo_stream), "solo graphs");
+      for (cudaStream_t t : b->solo_streams) CK(cudaStreamSynchronize(t), "solo graphs");
       for (size_t i = 0; i < b->solos.size(); ++i) {
         if (!queued[i]) continue;
         const RaggedSolo& S = b->solos[i];
         solo_st[i] = nwgpu_pr_stats{};
-        int rc = pr_solve_finish(S.h, b->rank + S.v0, damping, threshold, max_iters, b->solo_stream, &solo_st[i]);
+        int rc = pr_solve_finish(S.h, b->rank + S.v0, damping, threshold, max_iters, stream_of(i), &solo_st[i]);
         if (rc) return graph_fail(rc, S.g);
       }
     }
@@ -429,18 +446,20 @@ int nwgpu_pr_ragged(nwgpu_batch* b, const uint32_t* out_degree, float* ranks, fl
       so.mode = NWGPU_MODE_PARITY;
       so.launch = opt.launch;
       so.device_ptrs = 1;
-      so.stream = (void*)b->solo_stream;
+      so.stream = (void*)stream_of(i);
       solo_st[i] = nwgpu_pr_stats{};
       int rc = nwgpu_pr_run(S.h, b->deg + S.v0, b->rank + S.v0, damping, threshold, max_iters, &so, &solo_st[i]);
       if (rc) return graph_fail(rc, S.g);
     }
-    CK(cudaEventRecord(b->solo_done, b->solo_stream), "solo stream");
-    CK(cudaStreamWaitEvent(s, b->solo_done, 0), "solo stream");
+    for (size_t i = 0; i < nstreams; ++i) {
+      CK(cudaEventRecord(b->solo_done[i], b->solo_streams[i]), "solo stream");
+      CK(cudaStreamWaitEvent(s, b->solo_done[i], 0), "solo stream");
+    }
     return NWGPU_OK;
   };
   auto drained = [&](int rc) {  // nothing of this call left in flight on an error
     cudaStreamSynchronize(s);
-    if (b->solo_stream) cudaStreamSynchronize(b->solo_stream);
+    for (cudaStream_t t : b->solo_streams) cudaStreamSynchronize(t);
     return rc;
   };
   if (opt.launch == NWGPU_LAUNCH_GRAPH) {

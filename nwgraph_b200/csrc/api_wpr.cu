@@ -348,7 +348,7 @@ extern "C" int nwgpu_pr_vjp(nwgpu_graph* g, const float* ranks, const float* dL_
   if (dL_dw) {
     if (!opt.device_ptrs && !b.gw) CK(dalloc(g, &b.gw, nnz), "cudaMalloc(dL/dw staging)");
     float* dst = opt.device_ptrs ? dL_dw : b.gw;
-    CK(launch_vjp_grad_w(b.t, g->g.col, g->g.emap, b.r_int, g->rank, n, nnz, damping, b.f, b.q, dst, g->sms, s),
+    CK(launch_vjp_grad_w(b.t, g->g.col, g->g.emap, b.r_int, g->rank, b.vbase, n, nnz, damping, b.f, b.q, dst, g->sms, s),
        "dL/dw");
     if (!opt.device_ptrs) CK(cudaMemcpyAsync(dL_dw, dst, nnz * sizeof(float), cudaMemcpyDeviceToHost, s), "copy dL/dw");
   }

@@ -192,10 +192,10 @@ cudaError_t launch_wpr_prepare(const float* t, const uint32_t* inv, const float*
 cudaError_t launch_vjp_prepare(const float* r, const float* c, const uint32_t* inv, const float* s, uint64_t n,
                                float damping, float* r_int, float* vbase, float* vaux, float* lam, float* contrib, int sms,
                                cudaStream_t st);
-// dL/dw over the forward entries (col: the forward CSR's columns); f: n floats, q: n doubles of scratch
+// dL/dw over the forward entries (col: the forward CSR's columns); f, q: n-float scratch
 cudaError_t launch_vjp_grad_w(const Transposed& t, const uint32_t* col, const uint32_t* emap, const float* r_int,
-                              const float* lam, uint64_t n, uint64_t nnz, float damping, float* f, double* q,
-                              float* d_w, int sms, cudaStream_t st);
+                              const float* lam, const float* c_int, uint64_t n, uint64_t nnz, float damping, float* f,
+                              float* q, float* d_w, int sms, cudaStream_t st);
 cudaError_t launch_vjp_grad_t(const float* lam, const uint32_t* perm, uint64_t n, float damping, float* d_t, int sms,
                               cudaStream_t st);
 

@@ -61,7 +61,7 @@ struct WprBuffers {
   double*    part = nullptr;
   double*    dout = nullptr;
   float*     f = nullptr;        // n: dL/dw factors d r_j / s_j
-  double*    q = nullptr;        // n: dL/dw offsets q_j (FP64)
+  float*     q = nullptr;        // n: dL/dw offsets q_j
   void       release(cudaStream_t s);
 };
 

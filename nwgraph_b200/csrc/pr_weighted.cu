@@ -52,47 +52,28 @@ __global__ void vjp_prepare_kernel(const float* __restrict__ r, const float* __r
 
 // Per-vertex factors of dL/dw: f_j = d r_j / s_j, q_j = (l_j - c_j) / d
 // (= sum over j's out-entries of (w / s_j) l_dest at the adjoint's fixed point).
-// f_j = d r_j / s_j for every source j.
-__global__ void vjp_f_kernel(const float* __restrict__ r_int, const float* __restrict__ s, uint64_t n, float damping,
-                             float* __restrict__ f) {
+__global__ void vjp_fq_kernel(const float* __restrict__ r_int, const float* __restrict__ s, const float* __restrict__ lam,
+                              const float* __restrict__ c_int, uint64_t n, float damping, float* __restrict__ f,
+                              float* __restrict__ q) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
     const bool live = damping > 0.f && s[j] > 0.f;
     f[j] = live ? damping * r_int[j] / s[j] : 0.f;
+    q[j] = live ? (lam[j] - c_int[j]) / damping : 0.f;
   }
 }
 
-// q_j = sum over j's out-row of (w / s_j) l_i, summed in FP64 from the FP32
-// adjoint: one warp per out-row, lane-strided partial sums and a fixed tree.
-// Summed directly rather than taken from the fixed-point identity
-// q_j = (l_j - c_j) / d, which carries the adjoint solve's residual at j and
-// cancels against l_i on rows of few entries (an out-row of one entry has
-// q_j = l_i exactly, so its gradient is exactly 0).
-__global__ void vjp_q_kernel(const uint32_t* __restrict__ trp, const uint32_t* __restrict__ tcol,
-                             const float* __restrict__ tw, const float* __restrict__ s, const float* __restrict__ lam,
-                             uint64_t n, double* __restrict__ q) {
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-  for (uint64_t j = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); j < n; j += warps) {
-    const uint32_t k0 = trp[j], k1 = trp[j + 1];
-    double         acc = 0.0;
-    for (uint32_t k = k0 + lane; k < k1; k += 32u) acc += (double)tw[k] * (double)lam[tcol[k]];
-    acc = warp_sum_lane0(acc);
-    if (lane == 0) q[j] = (s[j] > 0.f) ? acc / (double)s[j] : 0.0;
-  }
-}
-
-// dL/dw_k = f_j (l_i - q_j) for forward entry k of row i, col[k] = j, in
-// FP64, written to the input entry emap[k].
+// dL/dw_k = f_j (l_i - q_j) for forward entry k of row i, col[k] = j; written
+// to the input entry emap[k].
 __global__ void vjp_grad_w_kernel(const uint32_t* __restrict__ erow, const uint32_t* __restrict__ col,
                                   const uint32_t* __restrict__ emap, const float* __restrict__ f,
-                                  const double* __restrict__ q, const float* __restrict__ lam, uint64_t nnz,
+                                  const float* __restrict__ q, const float* __restrict__ lam, uint64_t nnz,
                                   float* __restrict__ d_w) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += stride) {
     const uint32_t j = __ldcs(col + k);
-    const double   g = (double)f[j] * ((double)lam[__ldcs(erow + k)] - q[j]);
-    d_w[emap ? __ldcs(emap + k) : k] = (float)g;
+    const float    g = f[j] * (lam[__ldcs(erow + k)] - q[j]);
+    d_w[emap ? __ldcs(emap + k) : k] = g;
   }
 }
 
@@ -120,11 +101,10 @@ cudaError_t launch_vjp_prepare(const float* r, const float* c, const uint32_t* i
 }
 
 cudaError_t launch_vjp_grad_w(const Transposed& t, const uint32_t* col, const uint32_t* emap, const float* r_int,
-                              const float* lam, uint64_t n, uint64_t nnz, float damping, float* f, double* q,
-                              float* d_w, int sms, cudaStream_t st) {
+                              const float* lam, const float* c_int, uint64_t n, uint64_t nnz, float damping, float* f,
+                              float* q, float* d_w, int sms, cudaStream_t st) {
   if (n) {
-    vjp_f_kernel<<<sms * 8, 256, 0, st>>>(r_int, t.s, n, damping, f);
-    vjp_q_kernel<<<sms * 8, 256, 0, st>>>(t.row_ptr, t.col, t.w, t.s, lam, n, q);
+    vjp_fq_kernel<<<sms * 8, 256, 0, st>>>(r_int, t.s, lam, c_int, n, damping, f, q);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
