@@ -101,6 +101,8 @@ typedef struct nwgpu_graph_info {
   uint32_t block_items;    /* blocked: work items per sweep (blocks, the large ones cut into pieces) */
   uint32_t block_loads;    /* blocked: entries in flight per thread */
   uint64_t block_piece_entries; /* blocked: the largest work item */
+  uint32_t long_row_entries;    /* binned: rows longer than this are cut into chunks */
+  uint32_t chunk_entries;       /* binned: entries per long-row chunk */
 } nwgpu_graph_info;
 int nwgpu_graph_get_info(const nwgpu_graph* g, nwgpu_graph_info* info);
 

@@ -242,8 +242,13 @@ int load_degrees(nwgpu_graph* g, const uint32_t* out_degree, bool device_ptrs, c
 // Bin tables of the CSR (row_ptr, n rows) for the degree-binned sweep. Rows
 // must be in non-increasing length order (relabelled graphs); otherwise
 // p->ok stays false and the caller uses another sweep. hot: the launch shape
-// with the hub contributions staged in shared memory.
-int build_bin_plan(nwgpu_graph* g, const uint32_t* row_ptr, uint64_t n64, bool hot, BinPlan* p) {
+// with the hub contributions staged in shared memory. Rows of more than
+// long_row entries are cut into chunks of `chunk` entries.
+int build_bin_plan(nwgpu_graph* g, const uint32_t* row_ptr, uint64_t n64, bool hot, BinPlan* p, uint32_t long_row,
+                   uint32_t chunk) {
+  if (long_row < 256u || chunk < 256u || chunk % 256u)
+    return fail(NWGPU_ERR_INVALID_ARG, "long-row cut-off %u / chunk %u: both >= 256, the chunk a multiple of 256",
+                long_row, chunk);
   const uint32_t n = (uint32_t)n64;
   uint32_t*      d_out = nullptr;
   unsigned int*  d_bad = nullptr;
@@ -252,7 +257,7 @@ int build_bin_plan(nwgpu_graph* g, const uint32_t* row_ptr, uint64_t n64, bool h
   uint32_t     h_out[kNumBins + 2];
   unsigned int h_bad = 0;
   cudaError_t  e = cudaMemsetAsync(d_bad, 0, sizeof(unsigned int), g->stream);
-  if (e == cudaSuccess) e = launch_bin_bounds(row_ptr, n, d_out, d_bad, g->sms, g->stream);
+  if (e == cudaSuccess) e = launch_bin_bounds(row_ptr, n, long_row, chunk, d_out, d_bad, g->sms, g->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(h_out, d_out, sizeof(h_out), cudaMemcpyDeviceToHost, g->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(&h_bad, d_bad, sizeof(h_bad), cudaMemcpyDeviceToHost, g->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
@@ -261,6 +266,8 @@ int build_bin_plan(nwgpu_graph* g, const uint32_t* row_ptr, uint64_t n64, bool h
   if (h_bad) return NWGPU_OK;  // lengths not sorted
   BinnedArgs&    b = p->bin;
   const uint32_t nlong = h_out[0];
+  b.long_row = long_row;
+  b.chunk = chunk;
   b.num_long_rows = nlong;
   b.num_big_rows = h_out[kNumBins + 1] < nlong ? h_out[kNumBins + 1] : nlong;
   // rows one warp handles in each bin (pr_binned.cu: range_bin, group_bin<G>, empty_rows)
@@ -282,7 +289,7 @@ int build_bin_plan(nwgpu_graph* g, const uint32_t* row_ptr, uint64_t n64, bool h
     size_t    tmp_bytes = 0;
     CK(pool_alloc_n(&cnt, (uint64_t)nlong + 1, g->stream), "cudaMalloc(chunk counts)");
     e = cudaMemsetAsync(cnt + nlong, 0, sizeof(uint32_t), g->stream);
-    if (e == cudaSuccess) e = launch_chunk_count(row_ptr, nlong, cnt, g->sms, g->stream);
+    if (e == cudaSuccess) e = launch_chunk_count(row_ptr, nlong, chunk, cnt, g->sms, g->stream);
     if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, cnt, p->first, (int64_t)nlong + 1, g->stream);
     if (e == cudaSuccess) e = pool_alloc(&tmp, tmp_bytes, g->stream);
     if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, cnt, p->first, (int64_t)nlong + 1, g->stream);
@@ -318,7 +325,25 @@ int build_bin_plan(nwgpu_graph* g, const uint32_t* row_ptr, uint64_t n64, bool h
   }
   p->sweep_grid = binned_sweep_grid(g->sms, hot);
   p->finish_grid = binned_finish_grid(b);
+  p->bytes = ((uint64_t)nlong + 1 + kPad + 2 * ((uint64_t)num_chunks + kPad)) * sizeof(uint32_t);
   p->ok = true;
+  return NWGPU_OK;
+}
+
+int rebuild_bin_plan(nwgpu_graph* g, uint32_t long_row, uint32_t chunk) {
+  BinPlan&       p = g->plan;
+  if (!p.ok) return NWGPU_OK;
+  if (p.bin.long_row == long_row && p.bin.chunk == chunk) return NWGPU_OK;
+  const bool     hot = p.hot;
+  const uint32_t smem = p.bin.smem_ids, l1 = p.bin.l1_ids;
+  CK(cudaStreamSynchronize(g->stream), "bin plan");
+  g->device_bytes -= p.bytes;
+  p.release(g->stream);
+  const int rc = build_bin_plan(g, g->g.row_ptr, g->n, hot, &p, long_row, chunk);
+  if (rc) return rc;
+  p.bin.smem_ids = smem;
+  p.bin.l1_ids = l1;
+  g->cg_plan = nullptr;  // a cached loop graph holds the old tables
   return NWGPU_OK;
 }
 
@@ -850,8 +875,11 @@ int finish_create(nwgpu_graph* g, const float* weights, uint32_t flags, nwgpu_gr
   const bool want_binned =
       which ? (!strcmp(which, "binned") || !strcmp(which, "binned_hot") || !strcmp(which, "blocked")) : true;
   if (g->relabelled && want_binned) {
-    // NWGPU_SWEEP=binned keeps the hubs in L1 only (256-thread CTAs)
-    rc = build_bin_plan(g, g->g.row_ptr, n, !which || strcmp(which, "binned") != 0, &g->plan);
+    // NWGPU_SWEEP=binned keeps the hubs in L1 only (256-thread CTAs); NWGPU_LONG_ROW and
+    // NWGPU_CHUNK_ENTRIES set the long-row cut-offs (the tuner's choice otherwise)
+    rc = build_bin_plan(g, g->g.row_ptr, n, !which || strcmp(which, "binned") != 0, &g->plan,
+                        (uint32_t)env_int("NWGPU_LONG_ROW", (int)kLongRow),
+                        (uint32_t)env_int("NWGPU_CHUNK_ENTRIES", (int)kChunk));
     if (rc) return bail(rc);
   }
   trace.mark("bins");
@@ -877,7 +905,7 @@ int finish_create(nwgpu_graph* g, const float* weights, uint32_t flags, nwgpu_gr
       if (rc) return bail(rc);
       trace.mark("autotune");
     } else if (want_tune && g->plan.ok && !g->bplan.ok && !which && !getenv("NWGPU_HOT_IDS") &&
-               !getenv("NWGPU_HOT_L1_IDS")) {
+               !getenv("NWGPU_HOT_L1_IDS") && !getenv("NWGPU_LONG_ROW") && !getenv("NWGPU_CHUNK_ENTRIES")) {
       rc = autotune_binned(g);
       if (rc) return bail(rc);
       trace.mark("autotune");
@@ -921,6 +949,8 @@ int nwgpu_graph_get_info(const nwgpu_graph* g, nwgpu_graph_info* info) {
     info->sweep_grid = (uint32_t)g->plan.sweep_grid;
     info->hub_smem_ids = g->plan.bin.smem_ids;
     info->hub_l1_ids = g->plan.bin.l1_ids;
+    info->long_row_entries = g->plan.bin.long_row;
+    info->chunk_entries = g->plan.bin.chunk;
   } else {
     info->sweep_threads = (uint32_t)g->variant.threads;
     info->sweep_grid = (uint32_t)g->grid;

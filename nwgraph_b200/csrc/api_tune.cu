@@ -5,11 +5,17 @@
 // TBB grain). The binned sweep's runtime knobs are the launch shape (one
 // 1024-thread CTA per SM with the hub contributions staged in shared memory,
 // or four 256-thread CTAs per SM with the hubs in L1), how many hub
-// contributions the hot shape stages, and how many more ids go through L1
-// with an evict-last policy. Every choice gives bitwise-equal ranks (the
-// summation order does not depend on where a contribution is read from), so
-// the tuner only times: a few sweeps of each candidate on the resident graph
-// with unit degrees, and keeps the fastest.
+// contributions the hot shape stages, how many more ids go through L1 with
+// an evict-last policy, and the long-row cut-offs: the row length above which
+// rows are cut into chunks (one warp each) and the chunk length. The tuner
+// times a few sweeps of each candidate on the resident graph with unit
+// degrees and keeps the fastest: first the cut-offs at the default launch
+// shape, then the launch shapes and hub tiers at the chosen cut-offs.
+// Launch shape and hub tiers do not change the summation order (ranks are
+// bitwise equal whichever is chosen); the cut-offs do (a chunked row is
+// summed per chunk, then over the chunks), so a tuned graph gives the ranks
+// of an untuned one created with the same NWGPU_LONG_ROW and
+// NWGPU_CHUNK_ENTRIES, bit for bit, and the graph info reports both.
 //
 // Choices are cached per graph signature -- the SM count, log2 of the vertex
 // count in half steps, the average degree, and the share of entries in
@@ -34,6 +40,7 @@ struct Choice {
   int      hot = 1;
   uint32_t smem_ids = 0, l1_ids = 0;
   float    us = 0.f;  // measured time per sweep
+  uint32_t long_row = kLongRow, chunk = kChunk;
 };
 
 std::mutex                    g_mu;
@@ -58,7 +65,9 @@ void load_locked() {
     Choice c;
     if (!tab) continue;
     *tab = 0;
-    if (sscanf(tab + 1, "%d %u %u %f", &c.hot, &c.smem_ids, &c.l1_ids, &c.us) == 4) g_cache[line] = c;
+    // hot smem_ids l1_ids us [long_row chunk]
+    if (sscanf(tab + 1, "%d %u %u %f %u %u", &c.hot, &c.smem_ids, &c.l1_ids, &c.us, &c.long_row, &c.chunk) >= 4)
+      g_cache[line] = c;
   }
   fclose(f);
 }
@@ -69,7 +78,7 @@ void store_locked(const std::string& sig, const Choice& c) {
   if (!path) return;
   FILE* f = fopen(path, "a");
   if (!f) return;
-  fprintf(f, "%s\t%d %u %u %.2f\n", sig.c_str(), c.hot, c.smem_ids, c.l1_ids, c.us);
+  fprintf(f, "%s\t%d %u %u %.2f %u %u\n", sig.c_str(), c.hot, c.smem_ids, c.l1_ids, c.us, c.long_row, c.chunk);
   fclose(f);
 }
 
@@ -96,12 +105,15 @@ int signature(nwgpu_graph* g, std::string* out) {
   return NWGPU_OK;
 }
 
-void apply(nwgpu_graph* g, const Choice& c) {
+int apply(nwgpu_graph* g, const Choice& c) {
+  int rc = rebuild_bin_plan(g, c.long_row, c.chunk);
+  if (rc) return rc;
   BinPlan& p = g->plan;
   p.hot = c.hot != 0;
   p.bin.smem_ids = c.smem_ids;
   p.bin.l1_ids = c.l1_ids;
   p.sweep_grid = binned_sweep_grid(g->sms, p.hot);
+  return NWGPU_OK;
 }
 
 // Microseconds per sweep of the plan's current settings (after one warm sweep).
@@ -229,15 +241,41 @@ int autotune_binned(nwgpu_graph* g) {
       if (c.smem_ids > lim) c.smem_ids = lim;
       if (c.smem_ids > n) c.smem_ids = n & ~3u;
       if (c.l1_ids < c.smem_ids) c.l1_ids = c.smem_ids;
-      apply(g, c);
+      if ((rc = apply(g, c))) return rc;
       g->tuned = 2;
       g->tune_us = c.us;
       return NWGPU_OK;
     }
   }
-  // Candidates: the hot shape with 16K / 32K / 48K staged ids (as the shared
-  // memory allows) and an L1 tier of 0 / 16K / 32K more; the 256-thread shape
-  // with 16K / 32K / 64K ids through L1.
+  SweepArgs a;
+  if ((rc = start_timing(g, &a))) return rc;
+  const int sweeps = g->nnz > (1u << 26) ? 3 : 8;
+  // Long-row cut-offs (row length above which rows are chunked, chunk length)
+  // at the plan's launch shape and hub tiers; the default pair first, so a
+  // tie keeps it.
+  Choice best;
+  best.us = 3.4e38f;
+  {
+    static const uint32_t cuts[][2] = {{kLongRow, kChunk}, {1024, 512}, {1024, 1024}, {4096, 1024},
+                                       {4096, 2048}, {8192, 2048}, {512, 512}};
+    Choice c;
+    c.hot = g->plan.hot ? 1 : 0;
+    c.smem_ids = g->plan.bin.smem_ids;
+    c.l1_ids = g->plan.bin.l1_ids;
+    for (const auto& cut : cuts) {
+      c.long_row = cut[0];
+      c.chunk = cut[1];
+      if ((rc = apply(g, c))) return rc;
+      float us = 0.f;
+      if ((rc = time_plan(g, a, sweeps, &us))) return rc;
+      c.us = us;
+      if (us < best.us) best = c;
+    }
+  }
+  // Candidates at those cut-offs: the hot shape with 16K / 32K / 48K staged
+  // ids (as the shared memory allows) and an L1 tier of 0 / 16K / 32K more;
+  // the 256-thread shape with 16K / 32K / 64K ids through L1.
+  const uint32_t long_row = best.long_row, chunk = best.chunk;
   std::vector<Choice> cands;
   for (uint32_t s : {16384u, 32768u, 49152u}) {
     uint32_t st = s < lim ? s : lim;
@@ -247,6 +285,8 @@ int autotune_binned(nwgpu_graph* g) {
       c.hot = 1;
       c.smem_ids = st;
       c.l1_ids = st + l1;
+      c.long_row = long_row;
+      c.chunk = chunk;
       bool dup = false;
       for (const Choice& d : cands) dup |= d.hot == 1 && d.smem_ids == c.smem_ids && d.l1_ids == c.l1_ids;
       if (!dup) cands.push_back(c);
@@ -256,21 +296,18 @@ int autotune_binned(nwgpu_graph* g) {
     Choice c;
     c.hot = 0;
     c.l1_ids = l1;
+    c.long_row = long_row;
+    c.chunk = chunk;
     cands.push_back(c);
   }
-  SweepArgs a;
-  if ((rc = start_timing(g, &a))) return rc;
-  const int sweeps = g->nnz > (1u << 26) ? 3 : 8;
-  Choice    best;
-  best.us = 3.4e38f;
   for (Choice c : cands) {
-    apply(g, c);
+    if ((rc = apply(g, c))) return rc;
     float us = 0.f;
     if ((rc = time_plan(g, a, sweeps, &us))) return rc;
     c.us = us;
     if (us < best.us) best = c;
   }
-  apply(g, best);
+  if ((rc = apply(g, best))) return rc;
   g->tuned = 1;
   g->tune_us = best.us;
   std::lock_guard<std::mutex> lk(g_mu);

@@ -5,12 +5,15 @@
 
 namespace nwgpu {
 
+// Defaults of the plan's two runtime cut-offs (the tuner searches both):
 constexpr uint32_t kLongRow = 2048;  // rows longer than this are split into chunks
 constexpr uint32_t kChunk = 1024;    // entries per long-row chunk (one warp)
 constexpr int      kNumBins = 8;     // warp per row, then G = 32, 16, 8, 4, 2, 1, empty
 
 struct BinnedArgs {
   SweepArgs       sw;                     // row_ptr / col / vectors / state / loop control
+  uint32_t        long_row;               // rows longer than this are chunked (> 128)
+  uint32_t        chunk;                  // entries per long-row chunk (a multiple of 256)
   uint32_t        num_long_rows;          // rows [0, num_long_rows) are chunked
   uint32_t        num_big_rows;           // rows [0, num_big_rows) have more than 32 chunks
   uint32_t        num_chunks;
@@ -20,7 +23,7 @@ struct BinnedArgs {
   uint32_t        bin_row_begin[kNumBins];
   uint32_t        bin_row_end[kNumBins];
   uint32_t        bin_warp_end[kNumBins]; // cumulative warps over the bins
-  // bin 0: 129..kLongRow entries, one warp per row; bins 1-6: G = 32..1 lanes
+  // bin 0: 129..long_row entries, one warp per row; bins 1-6: G = 32..1 lanes
   // per row, two rows per lane group, rows of (2G, 4G] entries (G = 1: 1..4);
   // bin 7: empty rows
   uint32_t        smem_ids;               // hot variant: contrib[0, smem_ids) is staged in shared memory
@@ -33,9 +36,10 @@ struct BinnedArgs {
 constexpr int kBinnedThreads = 256;
 constexpr int kBinnedHotThreads = 1024;
 
-cudaError_t launch_bin_bounds(const uint32_t* row_ptr, uint32_t n, uint32_t* d_out, unsigned int* d_unsorted, int sms,
-                              cudaStream_t s);
-cudaError_t launch_chunk_count(const uint32_t* row_ptr, uint32_t nlong, uint32_t* cnt, int sms, cudaStream_t s);
+cudaError_t launch_bin_bounds(const uint32_t* row_ptr, uint32_t n, uint32_t long_row, uint32_t chunk, uint32_t* d_out,
+                              unsigned int* d_unsorted, int sms, cudaStream_t s);
+cudaError_t launch_chunk_count(const uint32_t* row_ptr, uint32_t nlong, uint32_t chunk, uint32_t* cnt, int sms,
+                               cudaStream_t s);
 cudaError_t launch_chunk_fill(const uint32_t* first, uint32_t nlong, uint32_t* chunk_row, int sms, cudaStream_t s);
 int         binned_sweep_grid(int sms, bool hot);
 uint32_t    binned_hot_capacity();  // ids the hot variant can stage (a multiple of 4)

@@ -37,6 +37,7 @@ struct BinPlan {
   uint32_t*  chunk_row = nullptr;
   float*     chunk_part = nullptr;
   int        sweep_grid = 0, finish_grid = 1;
+  uint64_t   bytes = 0;                 // device memory of the chunk tables
   void       release(cudaStream_t s);
 };
 
@@ -180,7 +181,10 @@ cudaError_t dalloc(nwgpu_graph* g, T** p, uint64_t count) {
   return e;
 }
 int ensure_solve_buffers(nwgpu_graph* g);
-int build_bin_plan(nwgpu_graph* g, const uint32_t* row_ptr, uint64_t n, bool hot, BinPlan* p);
+int build_bin_plan(nwgpu_graph* g, const uint32_t* row_ptr, uint64_t n, bool hot, BinPlan* p,
+                   uint32_t long_row = kLongRow, uint32_t chunk = kChunk);
+// g->plan rebuilt with other long-row cut-offs, keeping its launch shape and hub tiers.
+int rebuild_bin_plan(nwgpu_graph* g, uint32_t long_row, uint32_t chunk);
 // Sweep grid of a binned solve (the weighted and adjoint sweeps always use the
 // hot launch shape) and the kernel arguments of one.
 int        binned_grid(nwgpu_graph* g, const BinPlan& p, int mode);

@@ -3,10 +3,11 @@
 //
 // After relabelling, rows of similar length are contiguous, so the sweep is
 // split into bins without any per-row indirection:
-//   long   len > kLongRow     : chunks of kChunk entries, one warp per chunk;
+//   long   len > long_row     : chunks of `chunk` entries, one warp per chunk;
 //                               pr_binned_finish_kernel sums each row's chunk
 //                               partials in chunk order
-//   bin 0  128 < len <= kLongRow: one warp per row, lanes stride the row
+//   bin 0  128 < len <= long_row: one warp per row, lanes stride the row
+// (long_row and chunk are the plan's, 2048 and 1024 unless tuned or set)
 //   G = 32, 16, 8, 4, 2, 1      : rows of (G*2, G*4] entries (G = 1: 1..4),
 //                               G lanes per row, two rows per lane group,
 //                               <= 4 entries of each per lane
@@ -186,8 +187,8 @@ __device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src,
     if (CHUNK) {
       row = a.chunk_row[unit];
       const uint32_t rs = a.sw.row_ptr[row], re = a.sw.row_ptr[row + 1];
-      k0 = rs + (unit - a.row_first_chunk[row]) * kChunk;
-      k1 = min(re, k0 + kChunk);
+      k0 = rs + (unit - a.row_first_chunk[row]) * a.chunk;
+      k1 = min(re, k0 + a.chunk);
     } else {
       row = rb + unit;
       k0 = ld_stream(a.sw.row_ptr + rb + unit);
@@ -516,13 +517,13 @@ __device__ uint32_t first_row_at_most(const uint32_t* row_ptr, uint32_t n, uint3
 // out[0] = end of long rows, out[1..kNumBins] = ends of bins 0..kNumBins-1,
 // out[kNumBins + 1] = end of the rows of more than 32 chunks; flag = 1 if the
 // lengths are not non-increasing (then the binned sweep cannot be used).
-__global__ void bin_bounds_kernel(const uint32_t* __restrict__ row_ptr, uint32_t n, uint32_t* out,
-                                  unsigned int* unsorted) {
+__global__ void bin_bounds_kernel(const uint32_t* __restrict__ row_ptr, uint32_t n, uint32_t long_row, uint32_t chunk,
+                                  uint32_t* out, unsigned int* unsorted) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    const uint32_t limits[kNumBins] = {kLongRow, 128, 64, 32, 16, 8, 4, 0};
+    const uint32_t limits[kNumBins] = {long_row, 128, 64, 32, 16, 8, 4, 0};
     for (int b = 0; b < kNumBins; ++b) out[b] = first_row_at_most(row_ptr, n, limits[b]);
     out[kNumBins] = n;
-    out[kNumBins + 1] = first_row_at_most(row_ptr, n, 32u * kChunk);  // rows of more than 32 chunks
+    out[kNumBins + 1] = first_row_at_most(row_ptr, n, 32u * chunk);  // rows of more than 32 chunks
   }
   unsigned int bad = 0;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i + 1 < n; i += gridDim.x * blockDim.x)
@@ -530,9 +531,10 @@ __global__ void bin_bounds_kernel(const uint32_t* __restrict__ row_ptr, uint32_t
   if (bad) atomicOr(unsorted, 1u);
 }
 
-__global__ void chunk_count_kernel(const uint32_t* __restrict__ row_ptr, uint32_t nlong, uint32_t* __restrict__ cnt) {
+__global__ void chunk_count_kernel(const uint32_t* __restrict__ row_ptr, uint32_t nlong, uint32_t chunk,
+                                   uint32_t* __restrict__ cnt) {
   for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < nlong; r += gridDim.x * blockDim.x)
-    cnt[r] = (row_ptr[r + 1] - row_ptr[r] + kChunk - 1) / kChunk;
+    cnt[r] = (row_ptr[r + 1] - row_ptr[r] + chunk - 1) / chunk;
 }
 
 __global__ void chunk_fill_kernel(const uint32_t* __restrict__ first, uint32_t nlong, uint32_t* __restrict__ chunk_row) {
@@ -540,14 +542,15 @@ __global__ void chunk_fill_kernel(const uint32_t* __restrict__ first, uint32_t n
     for (uint32_t c = first[r]; c < first[r + 1]; ++c) chunk_row[c] = r;
 }
 
-cudaError_t launch_bin_bounds(const uint32_t* row_ptr, uint32_t n, uint32_t* d_out, unsigned int* d_unsorted, int sms,
-                              cudaStream_t s) {
-  bin_bounds_kernel<<<sms * 4, 256, 0, s>>>(row_ptr, n, d_out, d_unsorted);
+cudaError_t launch_bin_bounds(const uint32_t* row_ptr, uint32_t n, uint32_t long_row, uint32_t chunk, uint32_t* d_out,
+                              unsigned int* d_unsorted, int sms, cudaStream_t s) {
+  bin_bounds_kernel<<<sms * 4, 256, 0, s>>>(row_ptr, n, long_row, chunk, d_out, d_unsorted);
   return cudaGetLastError();
 }
-cudaError_t launch_chunk_count(const uint32_t* row_ptr, uint32_t nlong, uint32_t* cnt, int sms, cudaStream_t s) {
+cudaError_t launch_chunk_count(const uint32_t* row_ptr, uint32_t nlong, uint32_t chunk, uint32_t* cnt, int sms,
+                               cudaStream_t s) {
   if (!nlong) return cudaSuccess;
-  chunk_count_kernel<<<sms, 256, 0, s>>>(row_ptr, nlong, cnt);
+  chunk_count_kernel<<<sms, 256, 0, s>>>(row_ptr, nlong, chunk, cnt);
   return cudaGetLastError();
 }
 cudaError_t launch_chunk_fill(const uint32_t* first, uint32_t nlong, uint32_t* chunk_row, int sms, cudaStream_t s) {

@@ -1,9 +1,12 @@
-"""Autotuner (NWGPU_GRAPH_AUTOTUNE) of the binned sweep (launch shape, hub
-tiers) and, with NWGPU_SWEEP=blocked, of the blocked sweep (entries in
-flight, piece size): every candidate gives bitwise-equal ranks, so a tuned
-graph must reproduce the default graph's ranks bit for bit; choices are
-cached per graph signature in the process and, with NWGPU_TUNE_CACHE, in a
-file that a later process reuses."""
+"""Autotuner (NWGPU_GRAPH_AUTOTUNE) of the binned sweep (long-row cut-offs,
+launch shape, hub tiers) and, with NWGPU_SWEEP=blocked, of the blocked sweep
+(entries in flight, piece size). Launch shape, hub tiers and the blocked
+knobs do not change the summation order; the long-row cut-offs do, so a tuned
+graph must give, bit for bit, the ranks of an untuned graph created with the
+tuner's cut-offs (NWGPU_LONG_ROW, NWGPU_CHUNK_ENTRIES), and every cut-off pair
+must keep parity with page_rank_v10 restated. Choices are cached per graph
+signature in the process and, with NWGPU_TUNE_CACHE, in a file that a later
+process reuses."""
 import json
 import os
 import subprocess
@@ -27,6 +30,10 @@ def solve(g, deg, **kw):
         return out, h.info()
 
 
+KEYS = ("sweep_threads", "hub_smem_ids", "hub_l1_ids", "long_row_entries", "chunk_entries", "block_loads",
+        "block_piece_entries")
+
+
 def test_tuned_ranks_are_bitwise_equal_and_cached(gpu, monkeypatch):
     monkeypatch.delenv("NWGPU_TUNE_CACHE", raising=False)
     g = G.rmat(17, 16, 5)
@@ -35,14 +42,54 @@ def test_tuned_ranks_are_bitwise_equal_and_cached(gpu, monkeypatch):
     r1, i1 = solve(g, deg, autotune=True)
     r2, i2 = solve(g, deg, autotune=True)
     assert i0["tuned"] == 0 and i0["binned"] == 1
+    assert (i0["long_row_entries"], i0["chunk_entries"]) == (2048, 1024)
     assert i1["tuned"] in (1, 2) and i1["tuned_us_per_sweep"] > 0
     assert i2["tuned"] == 2  # same signature: taken from the cache
-    for k in ("sweep_threads", "hub_smem_ids", "hub_l1_ids", "block_loads", "block_piece_entries"):
+    for k in KEYS:
         assert i1[k] == i2[k]
-    assert np.array_equal(r0.view(np.uint32), r1.view(np.uint32))
-    assert np.array_equal(r0.view(np.uint32), r2.view(np.uint32))
+    assert np.array_equal(r1.view(np.uint32), r2.view(np.uint32))
+    # an untuned graph with the tuner's cut-offs sums in the same order
+    monkeypatch.setenv("NWGPU_LONG_ROW", str(i1["long_row_entries"]))
+    monkeypatch.setenv("NWGPU_CHUNK_ENTRIES", str(i1["chunk_entries"]))
+    r3, i3 = solve(g, deg)
+    assert i3["tuned"] == 0
+    assert np.array_equal(r1.view(np.uint32), r3.view(np.uint32))
     ref, _, _ = O.jacobi_f32(g.row_ptr, g.col, deg, 0.85, 0.0, 20)
-    assert np.abs(r1.astype(np.float64) - ref).max() <= 1e-6
+    for r in (r0, r1):
+        assert np.abs(r.astype(np.float64) - ref).max() <= 1e-6
+
+
+@pytest.mark.parametrize("long_row,chunk", [(256, 256), (1024, 512), (4096, 2048), (8192, 2048)])
+def test_long_row_cutoffs_keep_parity(gpu, monkeypatch, long_row, chunk):
+    """Rows of more than long_row entries are cut into chunks of `chunk` entries; at RMAT scale 17 the cut-offs
+    move rows of 257 to 8192 entries between the warp-per-row bin and the chunks (rows of more than 32 chunks
+    get a warp in the finishing kernel at 256-entry chunks)."""
+    monkeypatch.setenv("NWGPU_LONG_ROW", str(long_row))
+    monkeypatch.setenv("NWGPU_CHUNK_ENTRIES", str(chunk))
+    g = G.rmat(17, 16, 5)
+    deg = g.out_degree()
+    with Graph(g.row_ptr, g.col) as h:
+        out = np.empty(g.n, np.float32)
+        h.page_rank(deg, out, 0.85, 0.0, 20)
+        info = h.info()
+        assert (info["long_row_entries"], info["chunk_entries"]) == (long_row, chunk)
+        ref, _, _ = O.jacobi_f32(g.row_ptr, g.col, deg, 0.85, 0.0, 20)
+        d = np.abs(out.astype(np.float64) - ref)
+        assert d.max() <= 1e-6 and d.sum() <= 1e-5
+        st = h.page_rank(deg, out, 0.85, 1e-4, 100)
+        ref, it, _ = O.jacobi_f32(g.row_ptr, g.col, deg, 0.85, 1e-4, 100)
+        assert st.iterations == it
+        d = np.abs(out.astype(np.float64) - ref)
+        assert d.max() <= 1e-6 and d.sum() <= 1e-5
+
+
+@pytest.mark.parametrize("long_row,chunk", [(255, 1024), (2048, 100), (2048, 1000)])
+def test_bad_cutoffs_are_refused(gpu, monkeypatch, long_row, chunk):
+    monkeypatch.setenv("NWGPU_LONG_ROW", str(long_row))
+    monkeypatch.setenv("NWGPU_CHUNK_ENTRIES", str(chunk))
+    g = G.rmat(12, 16, 5)
+    with pytest.raises(Exception, match="long-row cut-off"):
+        Graph(g.row_ptr, g.col)
 
 
 def test_environment_settings_take_precedence(gpu, monkeypatch):
@@ -78,7 +125,7 @@ def test_cache_file_is_reused_by_another_process(gpu, tmp_path):
     b = json.loads(subprocess.run([sys.executable, "-c", code], env=env, check=True, capture_output=True,
                                   text=True).stdout.strip().splitlines()[-1])
     assert b["tuned"] == 2
-    for k in ("sweep_threads", "hub_smem_ids", "hub_l1_ids", "block_loads", "block_piece_entries"):
+    for k in KEYS:
         assert a[k] == b[k]
 
 
