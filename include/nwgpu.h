@@ -63,10 +63,12 @@ typedef struct nwgpu_graph nwgpu_graph;
 #define NWGPU_GRAPH_DEVICE_PTRS 0x1u /* row_ptr / col / weights are device pointers (copied device-to-device) */
 #define NWGPU_GRAPH_TRANSPOSE 0x2u   /* build the out-row CSR (adjacency<0>) of nwgpu_pr_vjp at creation, not on first use */
 #define NWGPU_GRAPH_NO_RELABEL 0x4u  /* keep the input vertex order on the device (default: hubs first) */
-#define NWGPU_GRAPH_AUTOTUNE 0x8u    /* pick the sweep's launch shape and hub tiers by timing a few sweeps of
-                                        each candidate (or reuse the choice cached for graphs of the same
-                                        signature; NWGPU_TUNE_CACHE=<file> keeps the cache across processes).
-                                        Every choice gives bitwise-equal ranks. Also set by NWGPU_AUTOTUNE=1 */
+#define NWGPU_GRAPH_AUTOTUNE 0x8u    /* pick the sweep's long-row cut-offs, launch shape and hub tiers by
+                                        timing a few sweeps of each candidate (or reuse the choice cached for
+                                        graphs of the same signature; NWGPU_TUNE_CACHE=<file> keeps the cache
+                                        across processes). Launch shape and hub tiers give bitwise-equal ranks;
+                                        the cut-offs (reported by nwgpu_graph_get_info) set which rows are
+                                        summed in chunks. Also set by NWGPU_AUTOTUNE=1 */
 
 /* Upload a CSR once (replaces the per-call use of graph.indices_ /
  * to_be_indexed_ at page_rank.hpp:129). Validates it on the device
