@@ -196,6 +196,16 @@ int check_device(int* dev_out, int* sms_out) {
   return NWGPU_OK;
 }
 
+uint64_t residual_parts(const nwgpu_graph* g) {
+  uint64_t parts = (uint64_t)g->grid + (uint64_t)g->finish_grid;
+  if (g->plan.ok) {
+    const int      a = binned_sweep_grid(g->sms, false), b = binned_sweep_grid(g->sms, true);
+    const uint64_t bp = (uint64_t)(a > b ? a : b) + (uint64_t)g->plan.finish_grid;
+    if (bp > parts) parts = bp;
+  }
+  return parts;
+}
+
 int ensure_solve_buffers(nwgpu_graph* g) {
   if (g->solve_ready) return NWGPU_OK;
   const uint64_t n = g->n, T = g->tiling.num_tiles;
@@ -206,9 +216,8 @@ int ensure_solve_buffers(nwgpu_graph* g) {
   CK(dalloc(g, &g->stage_u32, n), "cudaMalloc(staging)");
   CK(dalloc(g, &g->cpart, T + 1), "cudaMalloc(cpart)");
   CK(dalloc(g, &g->epart, T + 1), "cudaMalloc(epart)");
-  const uint64_t parts = (uint64_t)g->grid + (uint64_t)g->finish_grid;
-  const uint64_t bparts = (uint64_t)g->plan.sweep_grid + (uint64_t)g->plan.finish_grid;
-  CK(dalloc(g, &g->res_part, parts > bparts ? parts : bparts), "cudaMalloc(res_part)");
+  g->res_parts = residual_parts(g);
+  CK(dalloc(g, &g->res_part, g->res_parts), "cudaMalloc(res_part)");
   CK(dalloc(g, &g->st, 1), "cudaMalloc(state)");
   CK(dalloc(g, &g->err_hist, g->err_cap), "cudaMalloc(err_hist)");
   static_assert(sizeof(PrState) <= kHostBlock, "state mirror fits a host block");
@@ -344,6 +353,16 @@ int rebuild_bin_plan(nwgpu_graph* g, uint32_t long_row, uint32_t chunk) {
   p.bin.smem_ids = smem;
   p.bin.l1_ids = l1;
   g->cg_plan = nullptr;  // a cached loop graph holds the old tables
+  // more long rows can mean more finishing CTAs, each writing a residual partial
+  if (g->solve_ready && residual_parts(g) > g->res_parts) {
+    CK(cudaStreamSynchronize(g->stream), "residual partials");
+    pool_free(g->res_part, g->stream);
+    g->device_bytes -= (g->res_parts + kPad) * sizeof(double);
+    g->res_part = nullptr;
+    g->res_parts = residual_parts(g);
+    CK(dalloc(g, &g->res_part, g->res_parts), "cudaMalloc(res_part)");
+    CK(cudaStreamSynchronize(g->stream), "residual partials");
+  }
   return NWGPU_OK;
 }
 
@@ -899,14 +918,15 @@ int finish_create(nwgpu_graph* g, const float* weights, uint32_t flags, nwgpu_gr
   {
     // explicit launch settings in the environment take precedence over tuning
     const char* tune = getenv("NWGPU_AUTOTUNE");
-    const bool  want_tune = (flags & NWGPU_GRAPH_AUTOTUNE) || (tune && !strcmp(tune, "1"));
+    const bool  shapes_only = (flags & kGraphTuneShapes) && !(flags & NWGPU_GRAPH_AUTOTUNE);
+    const bool  want_tune = (flags & (NWGPU_GRAPH_AUTOTUNE | kGraphTuneShapes)) || (tune && !strcmp(tune, "1"));
     if (want_tune && g->bplan.ok && !getenv("NWGPU_BLOCK_LOADS") && !getenv("NWGPU_BLOCK_PIECE_ENTRIES")) {
       rc = autotune_blocked(g);  // plain solves run the blocked sweep
       if (rc) return bail(rc);
       trace.mark("autotune");
     } else if (want_tune && g->plan.ok && !g->bplan.ok && !which && !getenv("NWGPU_HOT_IDS") &&
                !getenv("NWGPU_HOT_L1_IDS") && !getenv("NWGPU_LONG_ROW") && !getenv("NWGPU_CHUNK_ENTRIES")) {
-      rc = autotune_binned(g);
+      rc = autotune_binned(g, shapes_only);
       if (rc) return bail(rc);
       trace.mark("autotune");
     }

@@ -350,9 +350,15 @@ int nwgpu_batch_create(uint64_t num_graphs, const uint64_t* vertex_offsets, cons
       b->solo_done.push_back(ev);
     }
   }
+  // A solo graph's launch shape and hub tiers are tuned (cached per graph
+  // signature, so graphs alike are timed once): bitwise-neutral, and a small
+  // graph can stage fewer hub contributions per sweep than a large one.
+  // NWGPU_RAGGED_SOLO_TUNE=0 keeps the defaults.
+  const char*    solo_tune_env = getenv("NWGPU_RAGGED_SOLO_TUNE");
+  const uint32_t solo_tune = (solo_tune_env && !strcmp(solo_tune_env, "0")) ? 0u : kGraphTuneShapes;
   for (RaggedSolo& S : b->solos) {
     rc = nwgpu_graph_create(row_ptr + (vertex_offsets[S.g] + S.g), col + entry_offsets[S.g], nullptr, S.n, S.nnz,
-                            flags & NWGPU_GRAPH_DEVICE_PTRS, &S.h);
+                            (flags & NWGPU_GRAPH_DEVICE_PTRS) | solo_tune, &S.h);
     if (rc) {
       char msg[400];
       nwgpu_last_error(msg, sizeof(msg));

@@ -87,7 +87,7 @@ __global__ void fill_u32_kernel(uint32_t* __restrict__ p, uint64_t n, uint32_t v
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) p[i] = v;
 }
 
-int signature(nwgpu_graph* g, std::string* out) {
+int signature(nwgpu_graph* g, bool shapes_only, std::string* out) {
   const BinnedArgs& b = g->plan.bin;
   uint32_t          at[2] = {0, 0};  // row_ptr at the end of the long rows and of bin 0
   CK(cudaMemcpyAsync(&at[0], g->g.row_ptr + b.num_long_rows, sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream),
@@ -99,8 +99,9 @@ int signature(nwgpu_graph* g, std::string* out) {
   const double n = g->n ? (double)g->n : 1.0;
   auto         pct5 = [&](double x) { return (int)(std::lround(20.0 * x / nnz) * 5); };
   char         buf[160];
-  snprintf(buf, sizeof buf, "binned sms=%d log2n=%.1f deg=%ld long=%d%% warp=%d%%", g->sms,
-           std::round(2.0 * std::log2(n)) / 2.0, std::lround(nnz / n), pct5(at[0]), pct5((double)at[1] - at[0]));
+  snprintf(buf, sizeof buf, "%s sms=%d log2n=%.1f deg=%ld long=%d%% warp=%d%%",
+           shapes_only ? "binned-shapes" : "binned", g->sms, std::round(2.0 * std::log2(n)) / 2.0,
+           std::lround(nnz / n), pct5(at[0]), pct5((double)at[1] - at[0]));
   *out = buf;
   return NWGPU_OK;
 }
@@ -225,10 +226,10 @@ int autotune_blocked(nwgpu_graph* g) {
   return NWGPU_OK;
 }
 
-int autotune_binned(nwgpu_graph* g) {
+int autotune_binned(nwgpu_graph* g, bool shapes_only) {
   if (!g->plan.ok || g->n == 0) return NWGPU_OK;
   std::string sig;
-  int         rc = signature(g, &sig);
+  int         rc = signature(g, shapes_only, &sig);
   if (rc) return rc;
   const uint32_t lim = binned_hot_capacity();
   const uint32_t n = (uint32_t)g->n;
@@ -252,10 +253,13 @@ int autotune_binned(nwgpu_graph* g) {
   const int sweeps = g->nnz > (1u << 26) ? 3 : 8;
   // Long-row cut-offs (row length above which rows are chunked, chunk length)
   // at the plan's launch shape and hub tiers; the default pair first, so a
-  // tie keeps it.
+  // tie keeps it. shapes_only: the plan's own cut-offs (cached under their
+  // own signature, so the two kinds of choice never mix).
   Choice best;
   best.us = 3.4e38f;
-  {
+  best.long_row = g->plan.bin.long_row;
+  best.chunk = g->plan.bin.chunk;
+  if (!shapes_only) {
     static const uint32_t cuts[][2] = {{kLongRow, kChunk}, {1024, 512}, {1024, 1024}, {4096, 1024},
                                        {4096, 2048}, {8192, 2048}, {512, 512}};
     Choice c;

@@ -130,6 +130,7 @@ struct nwgpu_graph {
   float*        cpart = nullptr;
   float*        epart = nullptr;
   double*       res_part = nullptr;
+  uint64_t      res_parts = 0;          // entries of res_part
   nwgpu::PrState* st = nullptr;
   double*       err_hist = nullptr;
   uint32_t      err_cap = 4096;
@@ -185,6 +186,9 @@ int build_bin_plan(nwgpu_graph* g, const uint32_t* row_ptr, uint64_t n, bool hot
                    uint32_t long_row = kLongRow, uint32_t chunk = kChunk);
 // g->plan rebuilt with other long-row cut-offs, keeping its launch shape and hub tiers.
 int rebuild_bin_plan(nwgpu_graph* g, uint32_t long_row, uint32_t chunk);
+// Residual partials the handle's sweeps write: the merge-path sweep's, or the
+// binned plan's in its larger launch shape (the tuner may switch shapes).
+uint64_t residual_parts(const nwgpu_graph* g);
 // Sweep grid of a binned solve (the weighted and adjoint sweeps always use the
 // hot launch shape) and the kernel arguments of one.
 int        binned_grid(nwgpu_graph* g, const BinPlan& p, int mode);
@@ -199,15 +203,21 @@ nwgpu_pr_options read_options(const nwgpu_pr_options* options);
 // Graph-creation flag for internal callers: no blocked plan (a whole graph that
 // is only relabelled and then cut into shards).
 constexpr uint32_t kGraphNoBlockedPlan = 0x80000000u;
+// Graph-creation flag for internal callers: tune the binned sweep's launch
+// shape and hub tiers only, keeping the default long-row cut-offs, so the
+// ranks equal an untuned handle's bit for bit (the graphs a ragged batch
+// solves alone).
+constexpr uint32_t kGraphTuneShapes = 0x40000000u;
 // Whether a solve in `mode` over `plan` (the handle's forward plan or none) runs the blocked sweep.
 bool use_blocked(const nwgpu_graph* g, const BinPlan* plan, int mode);
 // run_sweeps' result when the degree check stopped a blocked solve before its first sweep (internal).
 constexpr int kRetryBinned = 1000;
 // Out-row CSR, its bins and the buffers of the weighted solve and its adjoint.
 int ensure_wpr(nwgpu_graph* g);
-// api_tune.cu: picks the binned sweep's launch shape and hub tiers for g
-// (timed, or from the per-signature cache) and sets g->plan accordingly.
-int autotune_binned(nwgpu_graph* g);
+// api_tune.cu: picks the binned sweep's long-row cut-offs (unless
+// shapes_only), launch shape and hub tiers for g (timed, or from the
+// per-signature cache) and sets g->plan accordingly.
+int autotune_binned(nwgpu_graph* g, bool shapes_only = false);
 // api_tune.cu: picks the blocked sweep's entries in flight and piece size (timed, or cached per signature).
 int autotune_blocked(nwgpu_graph* g);
 // degrees (input order, host or device) -> g->deg (internal order)

@@ -143,3 +143,32 @@ def test_blocked_tuning_bitwise_equal_and_cached(gpu, monkeypatch):
     assert (i1["block_loads"], i1["block_piece_entries"]) == (i2["block_loads"], i2["block_piece_entries"])
     assert np.array_equal(r0.view(np.uint32), r1.view(np.uint32))
     assert np.array_equal(r0.view(np.uint32), r2.view(np.uint32))
+
+
+@pytest.mark.parametrize("scale", [10, 12, 14])
+def test_small_tuned_graphs_stop_where_untuned_ones_do(gpu, monkeypatch, scale):
+    """A small graph has few merge-path tiles, so its merge-path sweep writes fewer residual partials than the
+    binned sweep's 256-thread shape (four CTAs per SM), which the tuner times and may keep; the handle's partials
+    are sized for the larger of its sweeps. The tuned solve must stop at the sweep of an untuned solve with the
+    tuner's cut-offs, with the same ranks and stopping error, and keep parity with the restated page_rank_v10."""
+    monkeypatch.delenv("NWGPU_TUNE_CACHE", raising=False)
+    g = G.rmat(scale, 16, 21)
+    deg = g.out_degree()
+
+    def run(tune):
+        with Graph(g.row_ptr, g.col, autotune=tune) as h:
+            out = np.empty(g.n, np.float32)
+            st = h.page_rank(deg, out, 0.85, 1e-6, 200)
+            return out, st, h.info()
+
+    r1, s1, i1 = run(True)
+    assert i1["tuned"] in (1, 2)
+    monkeypatch.setenv("NWGPU_LONG_ROW", str(i1["long_row_entries"]))
+    monkeypatch.setenv("NWGPU_CHUNK_ENTRIES", str(i1["chunk_entries"]))
+    r0, s0, _ = run(False)
+    assert s0.converged and s1.converged and s0.iterations == s1.iterations
+    assert s0.final_error == s1.final_error
+    assert np.array_equal(r0.view(np.uint32), r1.view(np.uint32))
+    ref, it, _ = O.jacobi_f32(g.row_ptr, g.col, deg, 0.85, 1e-6, 200)
+    assert s1.iterations == it
+    assert np.abs(r1.astype(np.float64) - ref).max() <= 1e-6
