@@ -893,12 +893,18 @@ int finish_create(nwgpu_graph* g, const float* weights, uint32_t flags, nwgpu_gr
   trace.mark("tiling");
   const bool want_binned =
       which ? (!strcmp(which, "binned") || !strcmp(which, "binned_hot") || !strcmp(which, "blocked")) : true;
+  const char* tune_env = getenv("NWGPU_AUTOTUNE");
+  const bool  tune_all = ((flags & NWGPU_GRAPH_AUTOTUNE) || (tune_env && !strcmp(tune_env, "1"))) && !which &&
+                        !getenv("NWGPU_HOT_IDS") && !getenv("NWGPU_HOT_L1_IDS") && !getenv("NWGPU_LONG_ROW") &&
+                        !getenv("NWGPU_CHUNK_ENTRIES");
   if (g->relabelled && want_binned) {
     // NWGPU_SWEEP=binned keeps the hubs in L1 only (256-thread CTAs); NWGPU_LONG_ROW and
-    // NWGPU_CHUNK_ENTRIES set the long-row cut-offs (the tuner's choice otherwise)
-    rc = build_bin_plan(g, g->g.row_ptr, n, !which || strcmp(which, "binned") != 0, &g->plan,
-                        (uint32_t)env_int("NWGPU_LONG_ROW", (int)kLongRow),
-                        (uint32_t)env_int("NWGPU_CHUNK_ENTRIES", (int)kChunk));
+    // NWGPU_CHUNK_ENTRIES set the long-row cut-offs (the tuner's choice otherwise: the cached
+    // one for this graph's signature, if any, so the plan is built once)
+    uint32_t long_row = (uint32_t)env_int("NWGPU_LONG_ROW", (int)kLongRow);
+    uint32_t chunk = (uint32_t)env_int("NWGPU_CHUNK_ENTRIES", (int)kChunk);
+    if (tune_all && (rc = cached_cutoffs(g, &long_row, &chunk))) return bail(rc);
+    rc = build_bin_plan(g, g->g.row_ptr, n, !which || strcmp(which, "binned") != 0, &g->plan, long_row, chunk);
     if (rc) return bail(rc);
   }
   trace.mark("bins");

@@ -87,13 +87,22 @@ __global__ void fill_u32_kernel(uint32_t* __restrict__ p, uint64_t n, uint32_t v
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) p[i] = v;
 }
 
+// The graph's signature, from the bins at the default cut-offs whatever the
+// plan's own are (so a plan built with cached cut-offs finds its entry).
 int signature(nwgpu_graph* g, bool shapes_only, std::string* out) {
-  const BinnedArgs& b = g->plan.bin;
-  uint32_t          at[2] = {0, 0};  // row_ptr at the end of the long rows and of bin 0
-  CK(cudaMemcpyAsync(&at[0], g->g.row_ptr + b.num_long_rows, sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream),
-     "signature");
-  CK(cudaMemcpyAsync(&at[1], g->g.row_ptr + b.bin_row_end[0], sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream),
-     "signature");
+  uint32_t*     d_out = nullptr;
+  uint32_t      h_out[kNumBins + 2];
+  uint32_t      at[2] = {0, 0};  // row_ptr at the end of the long rows and of bin 0
+  CK(pool_alloc((void**)&d_out, (kNumBins + 3) * sizeof(uint32_t), g->stream), "signature");
+  unsigned int* d_bad = reinterpret_cast<unsigned int*>(d_out + kNumBins + 2);
+  cudaError_t   e = cudaMemsetAsync(d_bad, 0, sizeof(unsigned int), g->stream);
+  if (e == cudaSuccess) e = launch_bin_bounds(g->g.row_ptr, (uint32_t)g->n, kLongRow, kChunk, d_out, d_bad, g->sms, g->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h_out, d_out, sizeof(h_out), cudaMemcpyDeviceToHost, g->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  pool_free(d_out, g->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "signature");
+  CK(cudaMemcpyAsync(&at[0], g->g.row_ptr + h_out[0], sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream), "signature");
+  CK(cudaMemcpyAsync(&at[1], g->g.row_ptr + h_out[1], sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream), "signature");
   CK(cudaStreamSynchronize(g->stream), "signature");
   const double nnz = g->nnz ? (double)g->nnz : 1.0;
   const double n = g->n ? (double)g->n : 1.0;
@@ -223,6 +232,21 @@ int autotune_blocked(nwgpu_graph* g) {
   g->tune_us = best.us;
   std::lock_guard<std::mutex> lk(g_mu);
   store_locked(sig, best);
+  return NWGPU_OK;
+}
+
+int cached_cutoffs(nwgpu_graph* g, uint32_t* long_row, uint32_t* chunk) {
+  if (g->n == 0) return NWGPU_OK;
+  std::string sig;
+  int         rc = signature(g, false, &sig);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(g_mu);
+  load_locked();
+  auto it = g_cache.find(sig);
+  if (it != g_cache.end()) {
+    *long_row = it->second.long_row;
+    *chunk = it->second.chunk;
+  }
   return NWGPU_OK;
 }
 

@@ -218,6 +218,10 @@ int ensure_wpr(nwgpu_graph* g);
 // shapes_only), launch shape and hub tiers for g (timed, or from the
 // per-signature cache) and sets g->plan accordingly.
 int autotune_binned(nwgpu_graph* g, bool shapes_only = false);
+// api_tune.cu: the long-row cut-offs cached for g's signature, if any (else
+// the arguments are left as they are), so a tuned graph like one already
+// tuned builds its bin plan once.
+int cached_cutoffs(nwgpu_graph* g, uint32_t* long_row, uint32_t* chunk);
 // api_tune.cu: picks the blocked sweep's entries in flight and piece size (timed, or cached per signature).
 int autotune_blocked(nwgpu_graph* g);
 // degrees (input order, host or device) -> g->deg (internal order)

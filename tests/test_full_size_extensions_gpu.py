@@ -1,4 +1,4 @@
-"""The north-star extensions at their configurations' full sizes, against the oracle.
+"""The extensions (batched PPR, ragged batches, weighted PR with its adjoint) at full size, against the oracle.
 
 * C3 -- batched personalised PageRank: RMAT scale 22 (n = 4,194,304), k = 64
   one-hot seeds drawn among vertices with out-degree >= 1 (graphs.random_sources,
