@@ -279,8 +279,8 @@ int build_bin_plan(nwgpu_graph* g, const uint32_t* row_ptr, uint64_t n64, bool h
   b.chunk = chunk;
   b.num_long_rows = nlong;
   b.num_big_rows = h_out[kNumBins + 1] < nlong ? h_out[kNumBins + 1] : nlong;
-  // rows one warp handles in each bin (pr_binned.cu: range_bin, group_bin<G>, empty_rows)
-  static const uint32_t rows_per_warp[kNumBins] = {1, 2, 4, 8, 16, 32, 64, 128};
+  // rows one warp handles in each bin (pr_binned.cu: pair_bin, group_bin<G>, empty_rows)
+  static const uint32_t rows_per_warp[kNumBins] = {2, 2, 4, 8, 16, 32, 64, 128};
   uint32_t              warps = 0;
   for (int i = 0; i < kNumBins; ++i) {
     b.bin_row_begin[i] = h_out[i];

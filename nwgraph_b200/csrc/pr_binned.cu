@@ -6,7 +6,8 @@
 //   long   len > long_row     : chunks of `chunk` entries, one warp per chunk;
 //                               pr_binned_finish_kernel sums each row's chunk
 //                               partials in chunk order
-//   bin 0  128 < len <= long_row: one warp per row, lanes stride the row
+//   bin 0  128 < len <= long_row: half a warp per row (two rows per warp),
+//                               16 lanes stride the row
 // (long_row and chunk are the plan's, 2048 and 1024 unless tuned or set)
 //   G = 32, 16, 8, 4, 2, 1      : rows of (G*2, G*4] entries (G = 1: 1..4),
 //                               G lanes per row, two rows per lane group,
@@ -175,8 +176,8 @@ __device__ __forceinline__ uint32_t first_unit(uint32_t gwarp, uint32_t nwarps, 
 }
 
 // Units that are entry ranges, one warp each, walked in steps of 8 x 32
-// entries. CHUNK: unit c = chunk c of a long row, partial sum to chunk_part[c].
-// Otherwise: unit w = row rb + w (bin 0), epilogue.
+// entries. CHUNK: unit c = chunk c of a long row, partial sum to chunk_part[c]
+// (the long rows). Otherwise: unit w = row rb + w, epilogue.
 template <bool HOT, bool CHUNK, int MODE>
 __device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src, float* __restrict__ cout, uint32_t rb,
                                             uint32_t nunits, uint32_t w, uint32_t nwarps, int lane) {
@@ -259,6 +260,97 @@ __device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src,
       row = nrow;
       if (w + nwarps < nunits) bounds(w + nwarps, nk0, nk1, nrow);
       if (!CHUNK && lane == 0) in = load_row_in<MODE>(a, row);
+    }
+    base = nbase;
+  }
+  if (pending) finish();
+  return res;
+}
+
+// Bin 0 (rows of 129 entries to the long-row cut-off): a unit is two
+// consecutive rows, one per half-warp, 16 lanes striding each row in steps
+// of 8 x 16 entries. Half-warps waste fewer lanes on a row's last, partial
+// step than a whole warp's 256-entry steps (adjacent rows have about the same
+// length: the rows are in length order). The walk is range_bin's: the next
+// step's column ids and the next unit's row bounds load while the gathers are
+// in flight, and a unit's reduction (a 16-lane xor tree per half) and
+// epilogue wait until the next unit's gathers are issued.
+template <bool HOT, int MODE>
+__device__ __forceinline__ double pair_bin(const BinnedArgs& a, const Src& src, float* __restrict__ cout, uint32_t rb,
+                                           uint32_t re_bin, uint32_t nunits, uint32_t w, uint32_t nwarps, int lane) {
+  constexpr int      U = 8;
+  constexpr uint32_t STEP = U * 16;
+  if (w >= nunits) return 0.0;
+  const uint32_t h = (uint32_t)lane >> 4, sub = (uint32_t)lane & 15u;
+  auto bounds = [&](uint32_t unit, uint32_t& k0, uint32_t& k1, uint32_t& row) {
+    row = rb + 2u * unit + h;
+    if (row < re_bin) {
+      k0 = ld_stream(a.sw.row_ptr + row);
+      k1 = ld_stream(a.sw.row_ptr + row + 1);
+    } else {  // the bin's odd last row: this half has nothing
+      k0 = k1 = 0u;
+    }
+  };
+  auto load_ids = [&](uint32_t base, uint32_t end, uint32_t(&dst)[U]) {
+#pragma unroll
+    for (int q = 0; q < U; ++q) {
+      const uint32_t k = base + sub + (uint32_t)q * 16u;
+      dst[q] = (k < end) ? ld_stream(a.sw.col + k) : 0u;
+    }
+  };
+  uint32_t k0, k1, row, nk0 = 0, nk1 = 0, nrow = 0;
+  bounds(w, k0, k1, row);
+  if (w + nwarps < nunits) bounds(w + nwarps, nk0, nk1, nrow);
+  uint32_t id[U];
+  uint32_t base = k0;
+  load_ids(base, k1, id);
+  RowIn in = no_row_in();
+  if (sub == 0 && row < re_bin) in = load_row_in<MODE>(a, row);
+  float    acc = 0.f;
+  double   res = 0.0;
+  bool     pending = false;
+  float    acc_done = 0.f;
+  uint32_t row_done = 0u;
+  RowIn    in_done = no_row_in();
+  auto     finish = [&]() {
+    float z = acc_done;
+#pragma unroll
+    for (int off = 8; off > 0; off >>= 1) z += __shfl_xor_sync(kFullMask, z, off);
+    if (sub == 0 && row_done < re_bin) res += binned_update<MODE>(a, cout, row_done, z, in_done, src.pol);
+  };
+#pragma unroll 1
+  for (;;) {
+    float v[U];
+#pragma unroll
+    for (int q = 0; q < U; ++q) {
+      const uint32_t k = base + sub + (uint32_t)q * 16u;
+      v[q] = (k < k1) ? term<HOT, MODE>(a, src, id[q], k) : 0.f;
+    }
+    if (pending) {
+      finish();
+      pending = false;
+    }
+    // the next step: the rest of this unit (either half still has entries), or the next unit's first
+    const bool     mine = base + STEP < k1;
+    const bool     more = __any_sync(kFullMask, mine);  // warp-uniform
+    const bool     has_next = w + nwarps < nunits;
+    const uint32_t nbase = more ? base + STEP : nk0;
+    const uint32_t nend = more ? k1 : (has_next ? nk1 : 0u);
+    load_ids(nbase, nend, id);
+#pragma unroll
+    for (int q = 0; q < U; ++q) acc += v[q];
+    if (!more) {
+      pending = true;
+      acc_done = acc;
+      row_done = row;
+      in_done = in;
+      acc = 0.f;
+      w += nwarps;
+      if (w >= nunits) break;
+      k1 = nk1;
+      row = nrow;
+      if (w + nwarps < nunits) bounds(w + nwarps, nk0, nk1, nrow);
+      if (sub == 0 && row < re_bin) in = load_row_in<MODE>(a, row);
     }
     base = nbase;
   }
@@ -404,7 +496,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) pr_binned_sweep_kernel(const Bi
     const uint32_t w0 = first_unit(gwarp, nwarps, begin);
     const uint32_t rb = a.bin_row_begin[b], re = a.bin_row_end[b];
     switch (b) {
-      case 0: res += range_bin<HOT, false, MODE>(a, src, cout, rb, nu, w0, nwarps, lane); break;
+      case 0: res += pair_bin<HOT, MODE>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
       case 1: res += group_bin<HOT, 32, MODE>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
       case 2: res += group_bin<HOT, 16, MODE>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
       case 3: res += group_bin<HOT, 8, MODE>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
