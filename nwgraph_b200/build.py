@@ -24,7 +24,7 @@ INCLUDE = os.path.join(ROOT, "include")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CXX = os.environ.get("CXX", "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CUDA_SOURCES = ["api.cu", "api_ppr.cu", "pr_plain.cu", "pr_binned.cu", "graph_build.cu", "ppr_batched.cu", "pr_noalloc.cu", "devmem.cu", "pr_weighted.cu", "api_wpr.cu", "api_ragged.cu", "csr_build.cu", "api_tune.cu", "api_shard.cu", "pr_blocked.cu", "loaders.cpp"]
+CUDA_SOURCES = ["api.cu", "api_ppr.cu", "pr_plain.cu", "pr_binned.cu", "graph_build.cu", "ppr_batched.cu", "pr_noalloc.cu", "devmem.cu", "pr_weighted.cu", "api_wpr.cu", "api_ragged.cu", "csr_build.cu", "api_tune.cu", "api_shard.cu", "pr_blocked.cu", "ragged_union.cu", "loaders.cpp"]
 
 
 def _run(cmd, cwd=None):

@@ -22,12 +22,21 @@
 // rows, no tiles); their handles read and write their slices of the batch's
 // degree and rank arrays. Whether a graph is solved alone depends only on its
 // own size, so a graph gets the same result in any batch.
+//
+// The graphs kept in the batch are solved together as one union graph by
+// default (ragged_union.cu): their CSRs become diagonal blocks of one CSR,
+// relabelled and swept by the degree-binned kernel in kModeRagged, each graph
+// stopping at its own first sweep below the threshold and its rows then left
+// alone. Every graph gets, sweep for sweep, a single-graph handle's ranks bit
+// for bit. NWGPU_RAGGED_UNION=0 keeps the merge-path batch sweep; it is also
+// used when the union's vertex or entry count does not fit 32-bit ids.
 #include <cstdlib>
 #include <cstring>
 #include <new>
 #include <vector>
 
 #include "handle.h"
+#include "ragged_union.h"
 
 namespace nwgpu {
 
@@ -38,6 +47,24 @@ struct RaggedSolo {
   uint32_t     g = 0;  // the graph's index in the batch
   uint64_t     v0 = 0, n = 0, nnz = 0;
   nwgpu_graph* h = nullptr;
+};
+
+// A group of the graphs kept in a batch solved as one union graph: the
+// union's handle and its per-row and per-part tables, and its solve loop.
+struct RaggedUnion {
+  nwgpu_graph*    h = nullptr;
+  UnionParts      parts{};
+  uint32_t*       ids = nullptr;
+  uint64_t *      voff = nullptr, *eoff = nullptr;
+  uint32_t*       coff = nullptr;       // per part: its first vertex chunk
+  double*         chunk_part = nullptr;
+  uint32_t*       row_graph = nullptr;  // per internal row: its batch graph
+  double*         row_res = nullptr;    // per internal row: |dr| of the last sweep
+  cudaGraph_t     cg = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  float           damping = -1.f;       // the damping and threshold exec was built for
+  double          threshold = -1.0;
+  BinnedArgs      args{};               // this solve's sweep arguments
 };
 
 struct RaggedBatch {
@@ -73,6 +100,9 @@ struct RaggedBatch {
   cudaGraph_t  cg = nullptr;
   cudaGraphExec_t cg_exec = nullptr;
   float        cg_damping = -1.f;
+  // The graphs kept in the batch, solved as unions by the degree-binned
+  // sweep (none: the merge-path batch sweep instead).
+  std::vector<RaggedUnion> unions;
 
   template <class T>
   cudaError_t alloc(T** p, uint64_t count) {
@@ -87,6 +117,13 @@ struct RaggedBatch {
   ~RaggedBatch() {
     for (cudaStream_t t : solo_streams) cudaStreamSynchronize(t);
     for (RaggedSolo& S : solos) delete S.h;  // not nwgpu_graph_destroy: that clears the caller's last error
+    for (RaggedUnion& U : unions) {
+      if (U.exec) cudaGraphExecDestroy(U.exec);
+      if (U.cg) cudaGraphDestroy(U.cg);
+      delete U.h;
+      void* up[] = {U.ids, U.voff, U.eoff, U.coff, U.chunk_part, U.row_graph, U.row_res};
+      for (void* p : up) pool_free(p, stream);
+    }
     for (cudaEvent_t ev : solo_done) cudaEventDestroy(ev);
     for (cudaStream_t t : solo_streams) cudaStreamDestroy(t);
     if (stream) cudaStreamSynchronize(stream);
@@ -169,6 +206,109 @@ int build_ragged_graph(RaggedBatch* b, const SweepArgs& proto) {
      "cudaGraphAddKernelNode(ragged)");
   CK(cudaGraphInstantiate(&b->cg_exec, b->cg, 0), "cudaGraphInstantiate");
   b->cg_damping = proto.damping;
+  return NWGPU_OK;
+}
+
+// The graphs kept in the batch (all but the solo graphs), in batch order, cut
+// into unions of at most NWGPU_RAGGED_UNION_VERTICES vertices (default 2^22:
+// a union's contributions, 16 MB, stay in L2 while its sweep gathers them):
+// each one relabelled CSR over its graphs' vertices, graph after graph, swept
+// by the degree-binned kernel in kModeRagged. Built unless
+// NWGPU_RAGGED_UNION=0; a union whose binned plan cannot be built (an
+// NWGPU_SWEEP naming a merge-path sweep) sends the batch back to its
+// merge-path sweep.
+int build_union(RaggedBatch* b, const std::vector<uint32_t>& ids, const std::vector<uint64_t>& voff,
+                const std::vector<uint64_t>& eoff, int sms, RaggedUnion* U) {
+  const uint64_t m = ids.size(), n = voff.back(), nnz = eoff.back();
+  cudaStream_t   s = b->stream;
+  CK(b->alloc(&U->ids, m), "cudaMalloc(union)");
+  CK(b->alloc(&U->voff, m + 1), "cudaMalloc(union)");
+  CK(b->alloc(&U->eoff, m + 1), "cudaMalloc(union)");
+  CK(cudaMemcpyAsync(U->ids, ids.data(), m * sizeof(uint32_t), cudaMemcpyHostToDevice, s), "upload union");
+  CK(cudaMemcpyAsync(U->voff, voff.data(), (m + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s), "upload union");
+  CK(cudaMemcpyAsync(U->eoff, eoff.data(), (m + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s), "upload union");
+  std::vector<uint32_t> coff(m + 1, 0u);
+  for (uint64_t j = 0; j < m; ++j)
+    coff[j + 1] = coff[j] + (uint32_t)((voff[j + 1] - voff[j] + kUnionChunk - 1) / kUnionChunk);
+  CK(b->alloc(&U->coff, m + 1), "cudaMalloc(union)");
+  CK(b->alloc(&U->chunk_part, (uint64_t)coff[m] + 1), "cudaMalloc(union)");
+  CK(cudaMemcpyAsync(U->coff, coff.data(), (m + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, s), "upload union");
+  const UnionParts p{U->ids, U->voff, U->eoff, U->coff, U->chunk_part, (uint32_t)m, coff[m], n, nnz};
+  uint32_t *       rp = nullptr, *col = nullptr;
+  CK(pool_alloc_n(&rp, n + 1 + kPad, s), "cudaMalloc(union CSR)");
+  CK(pool_alloc_n(&col, nnz + kPad, s), "cudaMalloc(union CSR)");
+  cudaError_t e = launch_union_build(b->graphs, b->row_ptr, b->col, p, rp, col, sms, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  int rc = e == cudaSuccess ? nwgpu_graph_create(rp, col, nullptr, n, nnz, NWGPU_GRAPH_DEVICE_PTRS | kGraphNoBlockedPlan,
+                                                 &U->h)
+                            : cuda_fail(e, "union CSR");
+  pool_free(rp, s);
+  pool_free(col, s);
+  if (rc) return rc;
+  if (!U->h->relabelled || !U->h->plan.ok) return NWGPU_OK;  // the caller drops the unions
+  CK(b->alloc(&U->row_graph, n), "cudaMalloc(union rows)");
+  CK(b->alloc(&U->row_res, n), "cudaMalloc(union rows)");
+  CK(launch_union_row_graph(U->h->g.inv, p, U->row_graph, sms, s), "union rows");
+  CK(cudaStreamSynchronize(s), "union");
+  U->parts = p;
+  return NWGPU_OK;
+}
+
+int build_unions(RaggedBatch* b, int sms) {
+  const char* env = getenv("NWGPU_RAGGED_UNION");
+  if (env && !strcmp(env, "0")) return NWGPU_OK;
+  const char*    vmax_env = getenv("NWGPU_RAGGED_UNION_VERTICES");
+  const long long vm = vmax_env && *vmax_env ? strtoll(vmax_env, nullptr, 10) : (1ll << 22);
+  const uint64_t vmax = vm > 1 ? (uint64_t)vm : 2u;
+  std::vector<char> solo(b->num_graphs, 0);
+  for (const RaggedSolo& S : b->solos) solo[S.g] = 1;
+  // groups of consecutive graphs kept in the batch; a last group of fewer than two vertices joins the one before
+  std::vector<std::vector<uint32_t>> groups;
+  uint64_t                           gv = 0, ge = 0;
+  for (uint32_t g = 0; g < b->num_graphs; ++g) {
+    if (solo[g]) continue;
+    const RaggedGraph& R = b->h_graphs[g];
+    if (groups.empty() || gv + R.n > vmax || ge + R.nnz >= 0xFFFFFFF0ull) {
+      groups.emplace_back();
+      gv = ge = 0;
+    }
+    groups.back().push_back(g);
+    gv += R.n;
+    ge += R.nnz;
+  }
+  if (groups.size() >= 2 && gv < 2) {
+    std::vector<uint32_t> last = std::move(groups.back());
+    groups.pop_back();
+    groups.back().insert(groups.back().end(), last.begin(), last.end());
+  }
+  bool ok = !groups.empty();
+  for (const std::vector<uint32_t>& gr : groups) {
+    std::vector<uint64_t> voff(1, 0), eoff(1, 0);
+    for (uint32_t g : gr) {
+      voff.push_back(voff.back() + b->h_graphs[g].n);
+      eoff.push_back(eoff.back() + b->h_graphs[g].nnz);
+    }
+    if (voff.back() < 2 || voff.back() >= 0xFFFFFFF0ull || eoff.back() >= 0xFFFFFFF0ull) {
+      ok = false;  // a graph too large, or too few vertices: the merge-path sweep
+      break;
+    }
+    b->unions.emplace_back();
+    const int rc = build_union(b, gr, voff, eoff, sms, &b->unions.back());
+    if (rc) return rc;
+    if (!b->unions.back().h->plan.ok) {
+      ok = false;
+      break;
+    }
+  }
+  if (!ok) {  // the merge-path sweep for every graph kept in the batch
+    for (RaggedUnion& U : b->unions) {
+      delete U.h;
+      void* up[] = {U.ids, U.voff, U.eoff, U.coff, U.chunk_part, U.row_graph, U.row_res};
+      for (void* p : up) pool_free(p, b->stream);
+    }
+    b->unions.clear();
+    CK(cudaStreamSynchronize(b->stream), "union");
+  }
   return NWGPU_OK;
 }
 
@@ -335,12 +475,16 @@ int nwgpu_batch_create(uint64_t num_graphs, const uint64_t* vertex_offsets, cons
   BK(cudaEventCreate(&b->ev1), "cudaEventCreate");
   BK(cudaStreamSynchronize(b->stream), "batch create");
 #undef BK
+  // The unions of the graphs kept in the batch (no merge-path sweep then).
+  if ((rc = build_unions(b, sms))) return bail(rc);
   // The graphs solved alone: single-graph handles over the caller's slices.
-  if (!b->solos.empty()) {
-    const char* ns_env = getenv("NWGPU_RAGGED_SOLO_STREAMS");
-    long        ns = ns_env && *ns_env ? strtol(ns_env, nullptr, 10) : kRaggedSoloStreams;
+  // Solo graphs and unions run on a few streams beside each other.
+  if (!b->solos.empty() || !b->unions.empty()) {
+    const char*  ns_env = getenv("NWGPU_RAGGED_SOLO_STREAMS");
+    long         ns = ns_env && *ns_env ? strtol(ns_env, nullptr, 10) : kRaggedSoloStreams;
+    const size_t jobs = b->solos.size() + b->unions.size();
     if (ns < 1) ns = 1;
-    if ((size_t)ns > b->solos.size()) ns = (long)b->solos.size();
+    if ((size_t)ns > jobs) ns = (long)jobs;
     for (long i = 0; i < ns; ++i) {
       cudaStream_t t = nullptr;
       cudaEvent_t  ev = nullptr;
@@ -397,16 +541,19 @@ int nwgpu_pr_ragged(nwgpu_batch* b, const uint32_t* out_degree, float* ranks, fl
   h.chunk_end = kGraphChunk;
   h.threshold = (double)threshold;
   h.done = (max_iters == 0) ? 1u : 0u;
-  *b->h_st = h;
-  CK(cudaMemcpyAsync(b->st, b->h_st, sizeof(PrState), cudaMemcpyHostToDevice, s), "copy state");
-  // every graph starts running: the tile list is all tiles
-  b->h_act.resize(G + 1);
-  for (uint64_t g = 0; g <= G; ++g) b->h_act[g] = g < G ? b->h_graphs[g].tile0 : b->num_tiles;
-  CK(cudaMemcpyAsync(b->rs.act_off, b->h_act.data(), (G + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, s),
-     "copy tile list");
+  const bool      use_unions = !b->unions.empty();
   const SweepArgs a = ragged_args(b, damping);
-  CK(launch_ragged_init(a, b->rs, b->num_graphs, nv, damping, h.done, b->sms, s), "ragged init");
-  CK(launch_ragged_list(a, b->rs, b->sms, s), "ragged tile list");
+  if (!use_unions) {
+    *b->h_st = h;
+    CK(cudaMemcpyAsync(b->st, b->h_st, sizeof(PrState), cudaMemcpyHostToDevice, s), "copy state");
+    // every graph starts running: the tile list is all tiles
+    b->h_act.resize(G + 1);
+    for (uint64_t g = 0; g <= G; ++g) b->h_act[g] = g < G ? b->h_graphs[g].tile0 : b->num_tiles;
+    CK(cudaMemcpyAsync(b->rs.act_off, b->h_act.data(), (G + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, s),
+       "copy tile list");
+    CK(launch_ragged_init(a, b->rs, b->num_graphs, nv, damping, h.done, b->sms, s), "ragged init");
+    CK(launch_ragged_list(a, b->rs, b->sms, s), "ragged tile list");
+  }
   CK(cudaEventRecord(b->ev0, s), "cudaEventRecord");
   // The graphs solved alone run on their own stream, after the degree copy,
   // while the batch's sweep loop runs: each writes only its slice of the rank
@@ -468,44 +615,138 @@ int nwgpu_pr_ragged(nwgpu_batch* b, const uint32_t* out_degree, float* ranks, fl
     for (cudaStream_t t : b->solo_streams) cudaStreamSynchronize(t);
     return rc;
   };
-  if (opt.launch == NWGPU_LAUNCH_GRAPH) {
-    if (!b->cg_exec || b->cg_damping != damping) {
-      int rc = build_ragged_graph(b, a);
-      if (rc) return rc;
-    }
-    const uint64_t max_launches = max_iters / kGraphChunk + 2;
-    for (uint64_t launches = 0; !b->h_st->done; ++launches) {
-      if (launches == max_launches)
-        return drained(
-            fail(NWGPU_ERR_CUDA, "sweep loop did not finish after %llu graph launches", (unsigned long long)launches));
-      CK(cudaGraphLaunch(b->cg_exec, s), "cudaGraphLaunch");
-      CK(cudaMemcpyAsync(b->h_st, b->st, sizeof(PrState), cudaMemcpyDeviceToHost, s), "copy state");
-      if (!solos_run) {
-        int rc = run_solos();
-        if (rc) return drained(rc);
+  PrState fin{};
+  if (use_unions) {
+    // Each union's whole solve goes on a stream of its own (round robin with the solo graphs'): the per-graph
+    // tables start, then the CUDA-graph loop (or, in stream mode, a few sweeps at a time until it stops).
+    const size_t ns = b->solo_streams.size();
+    auto         ustream = [&](size_t j) { return b->solo_streams[(b->solos.size() + j) % ns]; };
+    for (cudaStream_t t : b->solo_streams) CK(cudaStreamWaitEvent(t, b->ev0, 0), "union stream");
+    for (size_t j = 0; j < b->unions.size(); ++j) {
+      RaggedUnion& U = b->unions[j];
+      nwgpu_graph* uh = U.h;
+      cudaStream_t t = ustream(j);
+      int          rc = ensure_solve_buffers(uh);
+      if (rc) return drained(rc);
+      *uh->h_st = h;
+      CK(cudaMemcpyAsync(uh->st, uh->h_st, sizeof(PrState), cudaMemcpyHostToDevice, t), "copy state");
+      CK(launch_union_start(b->graphs, U.parts, uh->g.inv, U.row_graph, b->deg, damping, h.done, b->base, b->rs,
+                            uh->deg, uh->rank, uh->contrib[0], b->sms, t),
+         "union start");
+      SweepArgs sw = make_sweep_args(uh, damping, 0.f, kTeleportUniform, 0u);
+      sw.abort_word = b->d_abort;
+      sw.graph_base = b->base;
+      sw.row_graph = U.row_graph;
+      sw.graph_done = b->rs.done;
+      sw.row_res = U.row_res;
+      U.args = make_binned_args(uh, uh->plan, sw, kModeRagged);
+      if (opt.launch == NWGPU_LAUNCH_GRAPH &&
+          (!U.exec || U.damping != damping || U.threshold != (double)threshold)) {
+        if (U.exec) cudaGraphExecDestroy(U.exec);
+        if (U.cg) cudaGraphDestroy(U.cg);
+        U.exec = nullptr;
+        U.cg = nullptr;
+        CK(cudaGraphCreate(&U.cg, 0), "cudaGraphCreate");
+        CK(build_union_graph(U.cg, U.args, binned_grid(uh, uh->plan, kModeRagged), uh->plan.finish_grid, U.parts,
+                             uh->g.perm, U.row_res, b->rs, uh->st, (double)threshold, b->d_abort, b->sms, &U.exec),
+           "union graph");
+        U.damping = damping;
+        U.threshold = (double)threshold;
       }
-      CK(cudaStreamSynchronize(s), "sweep loop");
+    }
+    // Queue every running union's next round, then read their states back: one CUDA-graph launch (up to
+    // kGraphChunk sweeps) or, in stream mode, up to 8 sweeps.
+    auto queue_round = [&]() -> int {
+      for (size_t j = 0; j < b->unions.size(); ++j) {
+        RaggedUnion& U = b->unions[j];
+        nwgpu_graph* uh = U.h;
+        cudaStream_t t = ustream(j);
+        if (uh->h_st->done) continue;
+        if (opt.launch == NWGPU_LAUNCH_GRAPH) {
+          CK(cudaGraphLaunch(U.exec, t), "cudaGraphLaunch");
+        } else {
+          const uint64_t left = max_iters - uh->h_st->iter, k = left < 8 ? left : 8;
+          for (uint64_t i = 0; i < k; ++i) {
+            CK(launch_binned_sweep(U.args, true, kModeRagged, binned_grid(uh, uh->plan, kModeRagged),
+                                   uh->plan.finish_grid, t),
+               "union sweep");
+            CK(launch_union_converge(U.parts, uh->g.perm, U.row_res, b->rs, uh->st, (double)threshold, b->d_abort,
+                                     b->sms, t),
+               "union convergence");
+          }
+        }
+        CK(cudaMemcpyAsync(uh->h_st, uh->st, sizeof(PrState), cudaMemcpyDeviceToHost, t), "copy state");
+      }
+      return NWGPU_OK;
+    };
+    const uint64_t max_rounds = (opt.launch == NWGPU_LAUNCH_GRAPH ? max_iters / kGraphChunk : max_iters / 8) + 2;
+    for (uint64_t round = 0;; ++round) {
+      if (round == max_rounds)
+        return drained(fail(NWGPU_ERR_CUDA, "union sweep loop did not finish after %llu rounds", (unsigned long long)round));
+      int rc = queue_round();
+      if (rc) return drained(rc);
+      if (!solos_run) {
+        if ((rc = run_solos())) return drained(rc);
+      }
+      for (cudaStream_t t : b->solo_streams) CK(cudaStreamSynchronize(t), "union sweep loop");
+      bool all = true;
+      for (RaggedUnion& U : b->unions) all = all && (U.h->h_st->done || U.h->h_st->iter >= max_iters);
+      if (all) break;
+    }
+    for (size_t j = 0; j < b->unions.size(); ++j) {
+      RaggedUnion&   U = b->unions[j];
+      const PrState& f = *U.h->h_st;
+      fin.iter = f.iter > fin.iter ? f.iter : fin.iter;
+      fin.fault |= f.fault;
+      fin.aborted |= f.aborted;
+      CK(launch_union_output(b->graphs, U.parts, U.h->g.perm, U.h->rank, b->rank, b->sms, ustream(j)), "union ranks");
+    }
+    for (size_t i = 0; i < b->solo_streams.size(); ++i) {
+      CK(cudaEventRecord(b->solo_done[i], b->solo_streams[i]), "union stream");
+      CK(cudaStreamWaitEvent(s, b->solo_done[i], 0), "union stream");
     }
   } else {
-    uint64_t launched = 0;
-    while (!b->h_st->done && launched < max_iters) {
-      const uint64_t batch = (max_iters - launched) < kGraphChunk ? (max_iters - launched) : kGraphChunk;
-      for (uint64_t k = 0; k < batch; ++k)
-        CK(launch_ragged_sweep(a, b->sweep_grid, b->finish_grid, b->num_graphs, b->rs, b->conv_grid, s), "ragged sweep");
-      launched += batch;
-      CK(cudaMemcpyAsync(b->h_st, b->st, sizeof(PrState), cudaMemcpyDeviceToHost, s), "copy state");
-      if (!solos_run) {
-        int rc = run_solos();
-        if (rc) return drained(rc);
+    if (opt.launch == NWGPU_LAUNCH_GRAPH) {
+      if (!b->cg_exec || b->cg_damping != damping) {
+        int rc = build_ragged_graph(b, a);
+        if (rc) return rc;
       }
-      CK(cudaStreamSynchronize(s), "sweep loop");
+      cudaGraphExec_t exec = b->cg_exec;
+      const uint64_t max_launches = max_iters / kGraphChunk + 2;
+      for (uint64_t launches = 0; !b->h_st->done; ++launches) {
+        if (launches == max_launches)
+          return drained(
+              fail(NWGPU_ERR_CUDA, "sweep loop did not finish after %llu graph launches", (unsigned long long)launches));
+        CK(cudaGraphLaunch(exec, s), "cudaGraphLaunch");
+        CK(cudaMemcpyAsync(b->h_st, b->st, sizeof(PrState), cudaMemcpyDeviceToHost, s), "copy state");
+        if (!solos_run) {
+          int rc = run_solos();
+          if (rc) return drained(rc);
+        }
+        CK(cudaStreamSynchronize(s), "sweep loop");
+      }
+    } else {
+      uint64_t launched = 0;
+      while (!b->h_st->done && launched < max_iters) {
+        const uint64_t batch = (max_iters - launched) < kGraphChunk ? (max_iters - launched) : kGraphChunk;
+        for (uint64_t k = 0; k < batch; ++k)
+          CK(launch_ragged_sweep(a, b->sweep_grid, b->finish_grid, b->num_graphs, b->rs, b->conv_grid, s), "ragged sweep");
+        launched += batch;
+        CK(cudaMemcpyAsync(b->h_st, b->st, sizeof(PrState), cudaMemcpyDeviceToHost, s), "copy state");
+        if (!solos_run) {
+          int rc = run_solos();
+          if (rc) return drained(rc);
+        }
+        CK(cudaStreamSynchronize(s), "sweep loop");
+      }
     }
+    if (!solos_run) {  // the batch loop ran no round (max_iters 0)
+      int rc = run_solos();
+      if (rc) return drained(rc);
+    }
+    fin = *b->h_st;
   }
-  if (!solos_run) {  // the batch loop ran no round (max_iters 0)
-    int rc = run_solos();
-    if (rc) return drained(rc);
-  }
-  const PrState fin = *b->h_st;
+
   if (fin.fault) return drained(fail(NWGPU_ERR_CUDA, "a bounded device wait gave up (fault word %u)", fin.fault));
   CK(cudaEventRecord(b->ev1, s), "cudaEventRecord");  // after the solo graphs too (s waits for them)
   if (nv)

@@ -48,6 +48,8 @@ int         binned_finish_grid(const BinnedArgs& a);
 // mode: SweepMode. The weighted and adjoint sweeps always use the hot shape
 // (sweep_grid = binned_sweep_grid(sms, true)).
 cudaError_t launch_binned_sweep(const BinnedArgs& a, bool hot, int mode, int sweep_grid, int finish_grid, cudaStream_t s);
-cudaError_t add_binned_nodes(cudaGraph_t body, const BinnedArgs& a, bool hot, int mode, int sweep_grid, int finish_grid);
+// finish_node (optional): the finishing kernel's node, the body's last.
+cudaError_t add_binned_nodes(cudaGraph_t body, const BinnedArgs& a, bool hot, int mode, int sweep_grid, int finish_grid,
+                             cudaGraphNode_t* finish_node = nullptr);
 
 }  // namespace nwgpu

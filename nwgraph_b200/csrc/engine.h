@@ -86,6 +86,9 @@ enum SweepMode : int {
   kModeAdjoint = 2,   // z = sum w * lambda;   l = vbase + vaux * z;    contrib' = l         (vaux = d / out-weight sum)
   kModeResidual = 3,  // residual push (page_rank_v13): z = sum delta; if z > push_threshold: r += z and
                       // delta' = z d / deg (deg > 0), else delta' = 0; the sweep "error" counts pushes
+  kModeRagged = 4,    // the union of a ragged batch's graphs: as kModePlain with the row's graph's base term
+                      // graph_base[row_graph[r]]; rows of stopped graphs (graph_done) are neither gathered nor
+                      // updated; each updated row's FP64 |dr| goes to row_res[r] for the per-graph sums
 };
 
 struct SweepArgs {
@@ -136,6 +139,11 @@ struct SweepArgs {
   const uint32_t*              act_off;
   const uint2*                 act_list;
   uint32_t                     num_graphs;
+  // kModeRagged (a union of graphs in one relabelled CSR): per internal row its graph, per graph whether it
+  // stopped, per internal row the FP64 L1 change of the last sweep.
+  const uint32_t*              row_graph;
+  const uint32_t*              graph_done;
+  double*                      row_res;
 };
 
 // Per-graph results of a ragged solve, written by the convergence kernel.

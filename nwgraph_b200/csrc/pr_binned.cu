@@ -78,11 +78,22 @@ struct RowIn {
   float    base;  // kModeWeighted: (1-d) t; kModeAdjoint: c
 };
 
+// kModeRagged: whether row r's graph has stopped (its rows are neither
+// gathered nor updated).
+__device__ __forceinline__ bool ragged_frozen(const BinnedArgs& a, uint32_t r) {
+  return __ldg(a.sw.graph_done + __ldg(a.sw.row_graph + r)) != 0u;
+}
+
 template <int MODE>
 __device__ __forceinline__ RowIn load_row_in(const BinnedArgs& a, uint32_t r) {
   RowIn x;
   x.old = ld_stream(a.sw.rank + r);
-  if constexpr (MODE == kModePlain || MODE == kModeResidual) {
+  if constexpr (MODE == kModeRagged) {  // base: the row's graph's (1 - d) / n_g; aux: 1 if that graph stopped
+    const uint32_t g = __ldg(a.sw.row_graph + r);
+    x.dg = ld_stream(a.sw.deg + r);
+    x.base = __ldg(a.sw.graph_base + g);
+    x.aux = __ldg(a.sw.graph_done + g) != 0u ? 1.f : 0.f;
+  } else if constexpr (MODE == kModePlain || MODE == kModeResidual) {
     x.dg = ld_stream(a.sw.deg + r);
     x.aux = 1.f;
     x.base = 0.f;
@@ -99,6 +110,15 @@ __device__ __forceinline__ RowIn no_row_in() { return RowIn{0.f, 1u, 1.f, 0.f}; 
 template <int MODE>
 __device__ __forceinline__ double binned_update(const BinnedArgs& a, float* __restrict__ cout, uint32_t r, float z,
                                                 const RowIn& in, uint64_t pol) {
+  if constexpr (MODE == kModeRagged) {
+    if (in.aux != 0.f) return 0.0;  // the row's graph has stopped: its rank and contribution stay
+    const float  nr = fmaf(a.sw.damping, z, in.base);
+    const double e = (double)fabsf(nr - in.old);
+    st_stream(a.sw.rank + r, nr);
+    st_keep(cout + r, nr / (float)in.dg, pol);
+    a.sw.row_res[r] = e;
+    return e;
+  }
   float nr, c;
   if constexpr (MODE == kModePlain) {
     nr = fmaf(a.sw.damping, z, binned_base(a, r));
@@ -138,7 +158,7 @@ __device__ __forceinline__ double binned_epilogue(const BinnedArgs& a, float* __
 template <bool HOT, int MODE>
 __device__ __forceinline__ float term(const BinnedArgs& a, const Src& src, uint32_t id, uint32_t k) {
   const float c = gather_one<HOT>(src, id);
-  if constexpr (MODE == kModePlain || MODE == kModeResidual) return c;
+  if constexpr (MODE == kModePlain || MODE == kModeResidual || MODE == kModeRagged) return c;
   else return ld_stream(a.sw.w + k) * c;
 }
 
@@ -190,6 +210,7 @@ __device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src,
       const uint32_t rs = a.sw.row_ptr[row], re = a.sw.row_ptr[row + 1];
       k0 = rs + (unit - a.row_first_chunk[row]) * a.chunk;
       k1 = min(re, k0 + a.chunk);
+      if (MODE == kModeRagged && ragged_frozen(a, row)) k1 = k0;  // a stopped graph's row: nothing to gather
     } else {
       row = rb + unit;
       k0 = ld_stream(a.sw.row_ptr + rb + unit);
@@ -287,6 +308,7 @@ __device__ __forceinline__ double pair_bin(const BinnedArgs& a, const Src& src, 
     if (row < re_bin) {
       k0 = ld_stream(a.sw.row_ptr + row);
       k1 = ld_stream(a.sw.row_ptr + row + 1);
+      if (MODE == kModeRagged && ragged_frozen(a, row)) k1 = k0;  // a stopped graph's row: nothing to gather
     } else {  // the bin's odd last row: this half has nothing
       k0 = k1 = 0u;
     }
@@ -359,7 +381,7 @@ __device__ __forceinline__ double pair_bin(const BinnedArgs& a, const Src& src, 
 }
 
 // Row bounds of the two rows a lane owns in unit w of a G-bin (len 0: no row).
-template <int G>
+template <int G, int MODE>
 __device__ __forceinline__ void group_bounds(const BinnedArgs& a, uint32_t rb, uint32_t re_bin, uint32_t w,
                                              uint32_t nunits, int lane, uint32_t (&rs)[2], uint32_t (&len)[2]) {
   constexpr uint32_t PER = 32 / G;
@@ -373,6 +395,7 @@ __device__ __forceinline__ void group_bounds(const BinnedArgs& a, uint32_t rb, u
         const uint32_t s0 = ld_stream(a.sw.row_ptr + row);
         rs[h] = s0;
         len[h] = ld_stream(a.sw.row_ptr + row + 1) - s0;
+        if (MODE == kModeRagged && ragged_frozen(a, row)) len[h] = 0u;  // a stopped graph's row
       }
     }
   }
@@ -399,9 +422,9 @@ __device__ __forceinline__ double group_bin(const BinnedArgs& a, const Src& src,
   if (w >= nunits) return 0.0;
   const int sub = lane & (G - 1);
   uint32_t  rs[2], len[2], nrs[2], nlen[2], id[2][4];
-  group_bounds<G>(a, rb, re_bin, w, nunits, lane, rs, len);
+  group_bounds<G, MODE>(a, rb, re_bin, w, nunits, lane, rs, len);
   group_ids<G>(a, rs, len, sub, id);
-  group_bounds<G>(a, rb, re_bin, w + nwarps, nunits, lane, nrs, nlen);
+  group_bounds<G, MODE>(a, rb, re_bin, w + nwarps, nunits, lane, nrs, nlen);
   double res = 0.0;
   // As in range_bin, a unit's shuffle tree and epilogue wait until the next
   // unit's gathers are in flight; not in the weighted mode, whose wider
@@ -445,7 +468,7 @@ __device__ __forceinline__ double group_bin(const BinnedArgs& a, const Src& src,
       rs[h] = nrs[h];
       len[h] = nlen[h];
     }
-    group_bounds<G>(a, rb, re_bin, w + 2u * nwarps, nunits, lane, nrs, nlen);
+    group_bounds<G, MODE>(a, rb, re_bin, w + 2u * nwarps, nunits, lane, nrs, nlen);
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       float acc = 0.f;
@@ -576,6 +599,12 @@ __global__ void __launch_bounds__(256) pr_binned_finish_kernel(const BinnedArgs 
     const unsigned long long done_iters = it + 1ull;
     st->iter = done_iters;
     st->last_error = e;
+    if constexpr (MODE == kModeRagged) {
+      // each graph's stopping test and the loop's continuation are the per-graph convergence kernel's
+      st->ticket = 0u;
+      __threadfence();
+      return;
+    }
     if (a.sw.err_hist && it < a.sw.err_cap) a.sw.err_hist[it] = e;  // the first err_cap sweeps
     const bool conv = e < st->threshold;
     const bool abort = a.sw.abort_word && *a.sw.abort_word;
@@ -667,7 +696,8 @@ cudaError_t configure_binned_kernels() {
   void* const hot[] = {(void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModePlain>,
                        (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModeWeighted>,
                        (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModeAdjoint>,
-                       (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModeResidual>};
+                       (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModeResidual>,
+                       (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModeRagged>};
   for (void* fn : hot) {
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, binned_hot_smem_bytes());
     if (e != cudaSuccess) return e;
@@ -692,6 +722,7 @@ static void* binned_fn(bool hot, int mode) {
   if (mode == kModeWeighted) return (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModeWeighted>;
   if (mode == kModeAdjoint) return (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModeAdjoint>;
   if (mode == kModeResidual) return (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModeResidual>;
+  if (mode == kModeRagged) return (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModeRagged>;
   return hot ? (void*)pr_binned_sweep_kernel<kBinnedHotThreads, true, kModePlain>
              : (void*)pr_binned_sweep_kernel<kBinnedThreads, false, kModePlain>;
 }
@@ -699,6 +730,7 @@ static void* binned_finish_fn(int mode) {
   if (mode == kModeWeighted) return (void*)pr_binned_finish_kernel<kModeWeighted>;
   if (mode == kModeAdjoint) return (void*)pr_binned_finish_kernel<kModeAdjoint>;
   if (mode == kModeResidual) return (void*)pr_binned_finish_kernel<kModeResidual>;
+  if (mode == kModeRagged) return (void*)pr_binned_finish_kernel<kModeRagged>;
   return (void*)pr_binned_finish_kernel<kModePlain>;
 }
 static bool binned_shape_hot(bool hot, int mode) { return hot || mode != kModePlain; }
@@ -718,7 +750,8 @@ cudaError_t launch_binned_sweep(const BinnedArgs& a, bool hot, int mode, int swe
   return cudaLaunchKernel(binned_finish_fn(mode), dim3((unsigned)finish_grid), dim3(256), args, 0, s);
 }
 
-cudaError_t add_binned_nodes(cudaGraph_t body, const BinnedArgs& a, bool hot, int mode, int sweep_grid, int finish_grid) {
+cudaError_t add_binned_nodes(cudaGraph_t body, const BinnedArgs& a, bool hot, int mode, int sweep_grid, int finish_grid,
+                             cudaGraphNode_t* finish_node) {
   void*                args[] = {(void*)&a};
   const bool           h = binned_shape_hot(hot, mode);
   cudaKernelNodeParams kp = {};
@@ -735,7 +768,9 @@ cudaError_t add_binned_nodes(cudaGraph_t body, const BinnedArgs& a, bool hot, in
   fp.gridDim = dim3((unsigned)finish_grid);
   fp.blockDim = dim3(256);
   fp.kernelParams = args;
-  return cudaGraphAddKernelNode(&fn, body, &sn, 1, &fp);
+  e = cudaGraphAddKernelNode(&fn, body, &sn, 1, &fp);
+  if (e == cudaSuccess && finish_node) *finish_node = fn;
+  return e;
 }
 
 }  // namespace nwgpu
