@@ -210,8 +210,8 @@ int build_ragged_graph(RaggedBatch* b, const SweepArgs& proto) {
 }
 
 // The graphs kept in the batch (all but the solo graphs), in batch order, cut
-// into unions of at most NWGPU_RAGGED_UNION_VERTICES vertices (default 2^22:
-// a union's contributions, 16 MB, stay in L2 while its sweep gathers them):
+// into unions of at most NWGPU_RAGGED_UNION_VERTICES vertices (default 2^23:
+// a union's contributions, 32 MB, stay in L2 while its sweep gathers them):
 // each one relabelled CSR over its graphs' vertices, graph after graph, swept
 // by the degree-binned kernel in kModeRagged. Built unless
 // NWGPU_RAGGED_UNION=0; a union whose binned plan cannot be built (an
@@ -258,7 +258,7 @@ int build_unions(RaggedBatch* b, int sms) {
   const char* env = getenv("NWGPU_RAGGED_UNION");
   if (env && !strcmp(env, "0")) return NWGPU_OK;
   const char*    vmax_env = getenv("NWGPU_RAGGED_UNION_VERTICES");
-  const long long vm = vmax_env && *vmax_env ? strtoll(vmax_env, nullptr, 10) : (1ll << 22);
+  const long long vm = vmax_env && *vmax_env ? strtoll(vmax_env, nullptr, 10) : (1ll << 23);
   const uint64_t vmax = vm > 1 ? (uint64_t)vm : 2u;
   std::vector<char> solo(b->num_graphs, 0);
   for (const RaggedSolo& S : b->solos) solo[S.g] = 1;
