@@ -237,10 +237,14 @@ int build_union(RaggedBatch* b, const std::vector<uint32_t>& ids, const std::vec
   uint32_t *       rp = nullptr, *col = nullptr;
   CK(pool_alloc_n(&rp, n + 1 + kPad, s), "cudaMalloc(union CSR)");
   CK(pool_alloc_n(&col, nnz + kPad, s), "cudaMalloc(union CSR)");
-  cudaError_t e = launch_union_build(b->graphs, b->row_ptr, b->col, p, rp, col, sms, s);
+  // The union's launch shape and hub tiers are tuned like a solo graph's
+  // (bitwise-neutral); NWGPU_RAGGED_UNION_TUNE=0 keeps the defaults.
+  const char*    tune_env = getenv("NWGPU_RAGGED_UNION_TUNE");
+  const uint32_t tune = (tune_env && !strcmp(tune_env, "0")) ? 0u : kGraphTuneShapes;
+  cudaError_t    e = launch_union_build(b->graphs, b->row_ptr, b->col, p, rp, col, sms, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  int rc = e == cudaSuccess ? nwgpu_graph_create(rp, col, nullptr, n, nnz, NWGPU_GRAPH_DEVICE_PTRS | kGraphNoBlockedPlan,
-                                                 &U->h)
+  int rc = e == cudaSuccess ? nwgpu_graph_create(rp, col, nullptr, n, nnz,
+                                                 NWGPU_GRAPH_DEVICE_PTRS | kGraphNoBlockedPlan | tune, &U->h)
                             : cuda_fail(e, "union CSR");
   pool_free(rp, s);
   pool_free(col, s);
