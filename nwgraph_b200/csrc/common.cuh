@@ -11,6 +11,7 @@ constexpr unsigned kFullMask = 0xffffffffu;
 // Streaming loads/stores for arrays touched once per sweep (col, row_ptr,
 // rank, degree): evict-first so the gathered contribution vector keeps L2.
 __device__ __forceinline__ uint32_t ld_stream(const uint32_t* p) { return __ldcs(p); }
+__device__ __forceinline__ uint4 ld_stream4(const uint4* p) { return __ldcs(p); }
 __device__ __forceinline__ float ld_stream(const float* p) { return __ldcs(p); }
 __device__ __forceinline__ void st_stream(float* p, float v) { __stcs(p, v); }
 

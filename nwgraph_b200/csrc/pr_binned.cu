@@ -15,10 +15,11 @@
 //   empty  len = 0             : epilogue only
 // Every lane's entries are summed in a fixed order and combined by a fixed
 // xor-shuffle tree, so ranks are bit-reproducible. Column ids stream through
-// (coalesced, evict-first); contributions are gathered with 8 loads in flight
-// per lane. Each warp walks its units software-pipelined: while the gathers of
-// one step are in flight, the column ids of the next step and the row bounds
-// of the unit after it are already loading.
+// (coalesced, evict-first; 128-bit loads in the long-row chunks and bin 0);
+// contributions are gathered with 8 loads in flight per lane. Each warp walks
+// its units software-pipelined: while the gathers of one step are in flight,
+// the column ids of the next step and the row bounds of the unit after it are
+// already loading.
 //
 // pr_binned_finish_kernel, launched right after, finishes the long rows; its
 // last CTA to finish (a ticket) reduces all FP64 residual partials in a fixed
@@ -88,12 +89,7 @@ template <int MODE>
 __device__ __forceinline__ RowIn load_row_in(const BinnedArgs& a, uint32_t r) {
   RowIn x;
   x.old = ld_stream(a.sw.rank + r);
-  if constexpr (MODE == kModeRagged) {  // base: the row's graph's (1 - d) / n_g; aux: 1 if that graph stopped
-    const uint32_t g = __ldg(a.sw.row_graph + r);
-    x.dg = ld_stream(a.sw.deg + r);
-    x.base = __ldg(a.sw.graph_base + g);
-    x.aux = __ldg(a.sw.graph_done + g) != 0u ? 1.f : 0.f;
-  } else if constexpr (MODE == kModePlain || MODE == kModeResidual) {
+  if constexpr (MODE == kModePlain || MODE == kModeResidual || MODE == kModeRagged) {
     x.dg = ld_stream(a.sw.deg + r);
     x.aux = 1.f;
     x.base = 0.f;
@@ -111,8 +107,11 @@ template <int MODE>
 __device__ __forceinline__ double binned_update(const BinnedArgs& a, float* __restrict__ cout, uint32_t r, float z,
                                                 const RowIn& in, uint64_t pol) {
   if constexpr (MODE == kModeRagged) {
-    if (in.aux != 0.f) return 0.0;  // the row's graph has stopped: its rank and contribution stay
-    const float  nr = fmaf(a.sw.damping, z, in.base);
+    // the row's graph: stopped (its rank and contribution stay), else its base term (1 - d) / n_g; read here
+    // rather than with the row's other inputs, which keeps them out of the registers held across a step
+    const uint32_t g = __ldg(a.sw.row_graph + r);
+    if (__ldg(a.sw.graph_done + g) != 0u) return 0.0;
+    const float  nr = fmaf(a.sw.damping, z, __ldg(a.sw.graph_base + g));
     const double e = (double)fabsf(nr - in.old);
     st_stream(a.sw.rank + r, nr);
     st_keep(cout + r, nr / (float)in.dg, pol);
@@ -195,9 +194,45 @@ __device__ __forceinline__ uint32_t first_unit(uint32_t gwarp, uint32_t nwarps, 
   return gwarp >= r ? gwarp - r : gwarp + nwarps - r;
 }
 
-// Units that are entry ranges, one warp each, walked in steps of 8 x 32
-// entries. CHUNK: unit c = chunk c of a long row, partial sum to chunk_part[c]
-// (the long rows). Otherwise: unit w = row rb + w, epilogue.
+// Column ids in 128-bit loads. A step of a unit covers a window of L
+// consecutive entries starting at `start` (the unit's first entry plus a
+// multiple of L), walked by L/8 lanes (a warp for L = 256, a half-warp for
+// L = 128): each lane takes 4 consecutive entries of each half of it, so slot
+// q of lane i holds the entry
+//   start + (L/2) * (q / 4) + 4 * i + q % 4.
+// The mapping is relative to the row (or chunk) start, so a row is summed in
+// the same order wherever it lies in the CSR: in a graph alone, in a union
+// of graphs, in any shard. The ids arrive in 16-byte-aligned uint4 words:
+// with p = start % 4, lane i's 4 entries of a half lie in the aligned word at
+// start - p + (L/2) * half + 4 i and, for p > 0, partly in the next word,
+// which the lane loads too; the words are then shifted by p. A word is loaded
+// only when one of the lane's entries in it lies before `end`, so the loads
+// reach at most 3 entries past the array's last one (inside the padding every
+// column array of a handle carries) and never a word before the array's start.
+template <uint32_t L>
+__device__ __forceinline__ uint32_t window_entry(uint32_t start, uint32_t lanei, int q) {
+  return start + (L / 2u) * (uint32_t)(q >> 2) + 4u * lanei + (uint32_t)(q & 3);
+}
+template <uint32_t L>
+__device__ __forceinline__ void load_window(const uint32_t* __restrict__ col, uint32_t start, uint32_t end,
+                                            uint32_t lanei, uint32_t (&dst)[8]) {
+  const uint32_t p = start & 3u;
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const uint32_t w0 = (start & ~3u) + (L / 2u) * (uint32_t)j + 4u * lanei;  // aligned word of the first entry
+    uint4          x = make_uint4(0u, 0u, 0u, 0u), y = x;
+    if (w0 + p < end) x = ld_stream4(reinterpret_cast<const uint4*>(col + w0));
+    if (p != 0u && w0 + 4u < end) y = ld_stream4(reinterpret_cast<const uint4*>(col + w0 + 4u));
+    dst[4 * j] = p == 0u ? x.x : p == 1u ? x.y : p == 2u ? x.z : x.w;
+    dst[4 * j + 1] = p == 0u ? x.y : p == 1u ? x.z : p == 2u ? x.w : y.x;
+    dst[4 * j + 2] = p == 0u ? x.z : p == 1u ? x.w : p == 2u ? y.x : y.y;
+    dst[4 * j + 3] = p == 0u ? x.w : p == 1u ? y.x : p == 2u ? y.y : y.z;
+  }
+}
+
+// Units that are entry ranges, one warp each, walked in 256-entry windows
+// (load_window). CHUNK: unit c = chunk c of a long row, partial sum to
+// chunk_part[c] (the long rows). Otherwise: unit w = row rb + w, epilogue.
 template <bool HOT, bool CHUNK, int MODE>
 __device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src, float* __restrict__ cout, uint32_t rb,
                                             uint32_t nunits, uint32_t w, uint32_t nwarps, int lane) {
@@ -217,19 +252,12 @@ __device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src,
       k1 = ld_stream(a.sw.row_ptr + rb + unit + 1);
     }
   };
-  auto load_ids = [&](uint32_t base, uint32_t end, uint32_t(&dst)[U]) {
-#pragma unroll
-    for (int q = 0; q < U; ++q) {
-      const uint32_t k = base + (uint32_t)lane + (uint32_t)q * 32u;
-      dst[q] = (k < end) ? ld_stream(a.sw.col + k) : 0u;
-    }
-  };
   uint32_t k0, k1, row, nk0 = 0, nk1 = 0, nrow = 0;
   bounds(w, k0, k1, row);
   if (w + nwarps < nunits) bounds(w + nwarps, nk0, nk1, nrow);
   uint32_t id[U];
-  uint32_t base = k0;
-  load_ids(base, k1, id);
+  uint32_t base = k0;  // the window's first entry
+  load_window<STEP>(a.sw.col, base, k1, (uint32_t)lane, id);
   RowIn in = no_row_in();
   if (!CHUNK && lane == 0) in = load_row_in<MODE>(a, row);
   float  acc = 0.f;
@@ -254,7 +282,7 @@ __device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src,
     float v[U];
 #pragma unroll
     for (int q = 0; q < U; ++q) {
-      const uint32_t k = base + (uint32_t)lane + (uint32_t)q * 32u;
+      const uint32_t k = window_entry<STEP>(base, (uint32_t)lane, q);
       v[q] = (k < k1) ? term<HOT, MODE>(a, src, id[q], k) : 0.f;
     }
     if (pending) {
@@ -266,7 +294,7 @@ __device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src,
     const bool     has_next = w + nwarps < nunits;
     const uint32_t nbase = more ? base + STEP : nk0;
     const uint32_t nend = more ? k1 : (has_next ? nk1 : 0u);
-    load_ids(nbase, nend, id);
+    load_window<STEP>(a.sw.col, nbase, nend, (uint32_t)lane, id);
 #pragma unroll
     for (int q = 0; q < U; ++q) acc += v[q];
     if (!more) {
@@ -289,8 +317,8 @@ __device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src,
 }
 
 // Bin 0 (rows of 129 entries to the long-row cut-off): a unit is two
-// consecutive rows, one per half-warp, 16 lanes striding each row in steps
-// of 8 x 16 entries. Half-warps waste fewer lanes on a row's last, partial
+// consecutive rows, one per half-warp, 16 lanes walking each row in 128-entry
+// windows (load_window). Half-warps waste fewer lanes on a row's last, partial
 // step than a whole warp's 256-entry steps (adjacent rows have about the same
 // length: the rows are in length order). The walk is range_bin's: the next
 // step's column ids and the next unit's row bounds load while the gathers are
@@ -313,19 +341,12 @@ __device__ __forceinline__ double pair_bin(const BinnedArgs& a, const Src& src, 
       k0 = k1 = 0u;
     }
   };
-  auto load_ids = [&](uint32_t base, uint32_t end, uint32_t(&dst)[U]) {
-#pragma unroll
-    for (int q = 0; q < U; ++q) {
-      const uint32_t k = base + sub + (uint32_t)q * 16u;
-      dst[q] = (k < end) ? ld_stream(a.sw.col + k) : 0u;
-    }
-  };
   uint32_t k0, k1, row, nk0 = 0, nk1 = 0, nrow = 0;
   bounds(w, k0, k1, row);
   if (w + nwarps < nunits) bounds(w + nwarps, nk0, nk1, nrow);
   uint32_t id[U];
-  uint32_t base = k0;
-  load_ids(base, k1, id);
+  uint32_t base = k0;  // this half's window's first entry
+  load_window<STEP>(a.sw.col, base, k1, sub, id);
   RowIn in = no_row_in();
   if (sub == 0 && row < re_bin) in = load_row_in<MODE>(a, row);
   float    acc = 0.f;
@@ -345,7 +366,7 @@ __device__ __forceinline__ double pair_bin(const BinnedArgs& a, const Src& src, 
     float v[U];
 #pragma unroll
     for (int q = 0; q < U; ++q) {
-      const uint32_t k = base + sub + (uint32_t)q * 16u;
+      const uint32_t k = window_entry<STEP>(base, sub, q);
       v[q] = (k < k1) ? term<HOT, MODE>(a, src, id[q], k) : 0.f;
     }
     if (pending) {
@@ -358,7 +379,7 @@ __device__ __forceinline__ double pair_bin(const BinnedArgs& a, const Src& src, 
     const bool     has_next = w + nwarps < nunits;
     const uint32_t nbase = more ? base + STEP : nk0;
     const uint32_t nend = more ? k1 : (has_next ? nk1 : 0u);
-    load_ids(nbase, nend, id);
+    load_window<STEP>(a.sw.col, nbase, nend, sub, id);
 #pragma unroll
     for (int q = 0; q < U; ++q) acc += v[q];
     if (!more) {
