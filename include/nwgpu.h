@@ -78,7 +78,9 @@ typedef struct nwgpu_graph nwgpu_graph;
  * the same order; results are returned in input order) and partitions it into
  * equal-work merge-path tiles. weights may be NULL
  * (unweighted); with weights the graph can also run weighted PageRank and its
- * adjoint. Uses the current CUDA device. */
+ * adjoint. Uses the current CUDA device. n must be below 2^32 - 16 and nnz at
+ * most 2^32 - 512 (the reference's uint32 row pointers allow 2^32 - 1; the
+ * sweep forms entry indices up to 255 past a row's end in 32 bits). */
 int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float* weights, uint64_t n, uint64_t nnz,
                        uint32_t flags, nwgpu_graph** out);
 int nwgpu_graph_destroy(nwgpu_graph* g);
@@ -443,7 +445,8 @@ int nwgpu_shard_unpermute(nwgpu_shard* s, const float* ranks_all, float* ranks, 
  * entry_offsets[num_graphs]. vertex_offsets / entry_offsets are host arrays
  * of num_graphs + 1 non-decreasing values starting at 0; row_ptr / col are
  * host pointers unless flags has NWGPU_GRAPH_DEVICE_PTRS. Per graph n_g and
- * nnz_g must be below 2^32 - 16; the batch totals are 64-bit.
+ * nnz_g must be below 2^32 - 16, and a graph solved alone (below) at most
+ * 2^32 - 512 entries, as for nwgpu_graph_create; the batch totals are 64-bit.
  *
  * Graphs with at least 2^22 entries (the environment variable
  * NWGPU_RAGGED_SOLO_ENTRIES, read here, sets the bound; 0 keeps every graph in

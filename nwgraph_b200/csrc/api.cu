@@ -745,8 +745,9 @@ int nwgpu_graph_create(const uint32_t* row_ptr, const uint32_t* col, const float
   if (!row_ptr) return fail(NWGPU_ERR_INVALID_ARG, "row_ptr is NULL");
   if (nnz && !col) return fail(NWGPU_ERR_INVALID_ARG, "col is NULL with nnz > 0");
   if (n >= 0xFFFFFFF0ull) return fail(NWGPU_ERR_INVALID_ARG, "n = %llu does not fit uint32 vertex ids", (unsigned long long)n);
-  if (nnz > 0xFFFFFFF0ull)
-    return fail(NWGPU_ERR_INVALID_ARG, "nnz = %llu does not fit uint32 row pointers", (unsigned long long)nnz);
+  if (nnz > kMaxEntries)
+    return fail(NWGPU_ERR_INVALID_ARG, "nnz = %llu is above the limit of %llu entries (uint32 row pointers and entry indices)",
+                (unsigned long long)nnz, (unsigned long long)kMaxEntries);
   int dev, sms;
   int rc = check_device(&dev, &sms);
   if (rc) return rc;

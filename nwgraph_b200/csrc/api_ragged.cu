@@ -272,7 +272,7 @@ int build_unions(RaggedBatch* b, int sms) {
   for (uint32_t g = 0; g < b->num_graphs; ++g) {
     if (solo[g]) continue;
     const RaggedGraph& R = b->h_graphs[g];
-    if (groups.empty() || gv + R.n > vmax || ge + R.nnz >= 0xFFFFFFF0ull) {
+    if (groups.empty() || gv + R.n > vmax || ge + R.nnz > kMaxEntries) {
       groups.emplace_back();
       gv = ge = 0;
     }
@@ -292,7 +292,7 @@ int build_unions(RaggedBatch* b, int sms) {
       voff.push_back(voff.back() + b->h_graphs[g].n);
       eoff.push_back(eoff.back() + b->h_graphs[g].nnz);
     }
-    if (voff.back() < 2 || voff.back() >= 0xFFFFFFF0ull || eoff.back() >= 0xFFFFFFF0ull) {
+    if (voff.back() < 2 || voff.back() >= 0xFFFFFFF0ull || eoff.back() > kMaxEntries) {
       ok = false;  // a graph too large, or too few vertices: the merge-path sweep
       break;
     }

@@ -9,6 +9,10 @@ namespace nwgpu {
 // Every device array is allocated with kPad spare elements so that 16-byte
 // aligned bulk copies that round a slice outward stay inside the allocation.
 constexpr uint64_t kPad = 16;
+// Largest entry count of a graph (and of a ragged union). Row pointers and
+// entry indices are uint32, and a sweep step forms indices up to 255 past a
+// row's last entry (a 256-entry window), so those must stay below 2^32.
+constexpr uint64_t kMaxEntries = 0xFFFFFE00ull;
 constexpr int      kSweepThreads = 256;
 constexpr unsigned long long kGraphChunk = 4096;  // sweeps per graph launch, at most
 

@@ -57,3 +57,17 @@ def test_null_arguments_rejected_before_device_use():
     assert N.lib().nwgpu_graph_create(None, None, None, 3, 0, 0, None) == N.ERR_INVALID_ARG
     assert N.lib().nwgpu_pr_run(None, None, None, 0.85, 1e-4, 20, None, None) == N.ERR_INVALID_ARG
     assert N.lib().nwgpu_graph_destroy(None) == N.OK
+
+
+def test_entry_count_limit_rejected_before_device_use():
+    """nnz above 2^32 - 512 is refused before any copy: the sweep forms entry indices up to 255 past a row's
+    end in 32-bit arithmetic (the reference's own row pointers are uint32, page_rank.hpp:129)."""
+    import numpy as np
+    from nwgraph_b200 import _native as N
+    rp = np.zeros(4, np.uint32)
+    cl = np.zeros(4, np.uint32)
+    h = C.c_void_p()
+    for nnz in (2**32 - 511, 2**32 - 16, 2**32):
+        rc = N.lib().nwgpu_graph_create(rp.ctypes.data, cl.ctypes.data, None, 3, nnz, 0, C.byref(h))
+        assert rc == N.ERR_INVALID_ARG, nnz
+        assert "limit" in N.last_error()
