@@ -681,7 +681,7 @@ def run_ours(args):
                    "sweep": {k: info[k] for k in ("blocked", "block_count", "block_items", "block_loads",
                                                   "block_piece_entries", "binned",
                                                   "sweep_threads", "sweep_grid", "hub_smem_ids",
-                                                  "hub_l1_ids", "long_row_entries", "chunk_entries", "tuned",
+                                                  "hub_l1_ids", "long_row_entries", "chunk_entries", "bin0_rows_per_warp", "tuned",
                                                   "tuned_us_per_sweep")}},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": sweep_traffic_per_launch(args, "blocked" if info["blocked"] else "binned"),

@@ -67,8 +67,8 @@ typedef struct nwgpu_graph nwgpu_graph;
                                         timing a few sweeps of each candidate (or reuse the choice cached for
                                         graphs of the same signature; NWGPU_TUNE_CACHE=<file> keeps the cache
                                         across processes). Launch shape and hub tiers give bitwise-equal ranks;
-                                        the cut-offs (reported by nwgpu_graph_get_info) set which rows are
-                                        summed in chunks. Also set by NWGPU_AUTOTUNE=1 */
+                                        the cut-offs and bin-0 rows per warp (reported by nwgpu_graph_get_info)
+                                        set how rows are summed. Also set by NWGPU_AUTOTUNE=1 */
 
 /* Upload a CSR once (replaces the per-call use of graph.indices_ /
  * to_be_indexed_ at page_rank.hpp:129). Validates it on the device
@@ -107,6 +107,8 @@ typedef struct nwgpu_graph_info {
   uint64_t block_piece_entries; /* blocked: the largest work item */
   uint32_t long_row_entries;    /* binned: rows longer than this are cut into chunks */
   uint32_t chunk_entries;       /* binned: entries per long-row chunk */
+  uint32_t bin0_rows_per_warp;  /* binned: rows of 129 entries to the long-row cut-off per warp: 2 (half a warp
+                                   each) or 1 (a whole warp); like the cut-offs it sets the rows' summation order */
 } nwgpu_graph_info;
 int nwgpu_graph_get_info(const nwgpu_graph* g, nwgpu_graph_info* info);
 

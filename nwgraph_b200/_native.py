@@ -53,7 +53,8 @@ class GraphInfo(C.Structure):
                 ("hub_l1_ids", C.c_uint32), ("tuned", C.c_int32), ("tuned_us_per_sweep", C.c_float),
                 ("blocked", C.c_int32), ("block_count", C.c_uint32), ("block_items", C.c_uint32),
                 ("block_loads", C.c_uint32), ("block_piece_entries", C.c_uint64),
-                ("long_row_entries", C.c_uint32), ("chunk_entries", C.c_uint32)]
+                ("long_row_entries", C.c_uint32), ("chunk_entries", C.c_uint32),
+                ("bin0_rows_per_warp", C.c_uint32)]
 
 
 class PrOptions(C.Structure):

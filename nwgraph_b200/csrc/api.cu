@@ -252,12 +252,15 @@ int load_degrees(nwgpu_graph* g, const uint32_t* out_degree, bool device_ptrs, c
 // must be in non-increasing length order (relabelled graphs); otherwise
 // p->ok stays false and the caller uses another sweep. hot: the launch shape
 // with the hub contributions staged in shared memory. Rows of more than
-// long_row entries are cut into chunks of `chunk` entries.
+// long_row entries are cut into chunks of `chunk` entries. bin0_rows: rows of
+// bin 0 per warp, 2 (half a warp each) or 1 (a whole warp).
 int build_bin_plan(nwgpu_graph* g, const uint32_t* row_ptr, uint64_t n64, bool hot, BinPlan* p, uint32_t long_row,
-                   uint32_t chunk) {
+                   uint32_t chunk, uint32_t bin0_rows) {
   if (long_row < 256u || chunk < 256u || chunk % 256u)
     return fail(NWGPU_ERR_INVALID_ARG, "long-row cut-off %u / chunk %u: both >= 256, the chunk a multiple of 256",
                 long_row, chunk);
+  if (bin0_rows != 1u && bin0_rows != 2u)
+    return fail(NWGPU_ERR_INVALID_ARG, "bin-0 rows per warp %u: 1 or 2", bin0_rows);
   const uint32_t n = (uint32_t)n64;
   uint32_t*      d_out = nullptr;
   unsigned int*  d_bad = nullptr;
@@ -277,10 +280,11 @@ int build_bin_plan(nwgpu_graph* g, const uint32_t* row_ptr, uint64_t n64, bool h
   const uint32_t nlong = h_out[0];
   b.long_row = long_row;
   b.chunk = chunk;
+  b.bin0_rows = bin0_rows;
   b.num_long_rows = nlong;
   b.num_big_rows = h_out[kNumBins + 1] < nlong ? h_out[kNumBins + 1] : nlong;
-  // rows one warp handles in each bin (pr_binned.cu: pair_bin, group_bin<G>, empty_rows)
-  static const uint32_t rows_per_warp[kNumBins] = {2, 2, 4, 8, 16, 32, 64, 128};
+  // rows one warp handles in each bin (pr_binned.cu: pair_bin or range_bin, group_bin<G>, empty_rows)
+  const uint32_t rows_per_warp[kNumBins] = {bin0_rows, 2, 4, 8, 16, 32, 64, 128};
   uint32_t              warps = 0;
   for (int i = 0; i < kNumBins; ++i) {
     b.bin_row_begin[i] = h_out[i];
@@ -339,16 +343,16 @@ int build_bin_plan(nwgpu_graph* g, const uint32_t* row_ptr, uint64_t n64, bool h
   return NWGPU_OK;
 }
 
-int rebuild_bin_plan(nwgpu_graph* g, uint32_t long_row, uint32_t chunk) {
+int rebuild_bin_plan(nwgpu_graph* g, uint32_t long_row, uint32_t chunk, uint32_t bin0_rows) {
   BinPlan&       p = g->plan;
   if (!p.ok) return NWGPU_OK;
-  if (p.bin.long_row == long_row && p.bin.chunk == chunk) return NWGPU_OK;
+  if (p.bin.long_row == long_row && p.bin.chunk == chunk && p.bin.bin0_rows == bin0_rows) return NWGPU_OK;
   const bool     hot = p.hot;
   const uint32_t smem = p.bin.smem_ids, l1 = p.bin.l1_ids;
   CK(cudaStreamSynchronize(g->stream), "bin plan");
   g->device_bytes -= p.bytes;
   p.release(g->stream);
-  const int rc = build_bin_plan(g, g->g.row_ptr, g->n, hot, &p, long_row, chunk);
+  const int rc = build_bin_plan(g, g->g.row_ptr, g->n, hot, &p, long_row, chunk, bin0_rows);
   if (rc) return rc;
   p.bin.smem_ids = smem;
   p.bin.l1_ids = l1;
@@ -897,15 +901,18 @@ int finish_create(nwgpu_graph* g, const float* weights, uint32_t flags, nwgpu_gr
   const char* tune_env = getenv("NWGPU_AUTOTUNE");
   const bool  tune_all = ((flags & NWGPU_GRAPH_AUTOTUNE) || (tune_env && !strcmp(tune_env, "1"))) && !which &&
                         !getenv("NWGPU_HOT_IDS") && !getenv("NWGPU_HOT_L1_IDS") && !getenv("NWGPU_LONG_ROW") &&
-                        !getenv("NWGPU_CHUNK_ENTRIES");
+                        !getenv("NWGPU_CHUNK_ENTRIES") && !getenv("NWGPU_BIN0_ROWS");
   if (g->relabelled && want_binned) {
     // NWGPU_SWEEP=binned keeps the hubs in L1 only (256-thread CTAs); NWGPU_LONG_ROW and
-    // NWGPU_CHUNK_ENTRIES set the long-row cut-offs (the tuner's choice otherwise: the cached
-    // one for this graph's signature, if any, so the plan is built once)
+    // NWGPU_CHUNK_ENTRIES set the long-row cut-offs, NWGPU_BIN0_ROWS the bin-0 rows per warp
+    // (the tuner's choice otherwise: the cached one for this graph's signature, if any, so the
+    // plan is built once)
     uint32_t long_row = (uint32_t)env_int("NWGPU_LONG_ROW", (int)kLongRow);
     uint32_t chunk = (uint32_t)env_int("NWGPU_CHUNK_ENTRIES", (int)kChunk);
-    if (tune_all && (rc = cached_cutoffs(g, &long_row, &chunk))) return bail(rc);
-    rc = build_bin_plan(g, g->g.row_ptr, n, !which || strcmp(which, "binned") != 0, &g->plan, long_row, chunk);
+    uint32_t bin0_rows = (uint32_t)env_int("NWGPU_BIN0_ROWS", (int)kBin0Rows);
+    if (tune_all && (rc = cached_cutoffs(g, &long_row, &chunk, &bin0_rows))) return bail(rc);
+    rc = build_bin_plan(g, g->g.row_ptr, n, !which || strcmp(which, "binned") != 0, &g->plan, long_row, chunk,
+                        bin0_rows);
     if (rc) return bail(rc);
   }
   trace.mark("bins");
@@ -932,7 +939,8 @@ int finish_create(nwgpu_graph* g, const float* weights, uint32_t flags, nwgpu_gr
       if (rc) return bail(rc);
       trace.mark("autotune");
     } else if (want_tune && g->plan.ok && !g->bplan.ok && !which && !getenv("NWGPU_HOT_IDS") &&
-               !getenv("NWGPU_HOT_L1_IDS") && !getenv("NWGPU_LONG_ROW") && !getenv("NWGPU_CHUNK_ENTRIES")) {
+               !getenv("NWGPU_HOT_L1_IDS") && !getenv("NWGPU_LONG_ROW") && !getenv("NWGPU_CHUNK_ENTRIES") &&
+               !getenv("NWGPU_BIN0_ROWS")) {
       rc = autotune_binned(g, shapes_only);
       if (rc) return bail(rc);
       trace.mark("autotune");
@@ -978,6 +986,7 @@ int nwgpu_graph_get_info(const nwgpu_graph* g, nwgpu_graph_info* info) {
     info->hub_l1_ids = g->plan.bin.l1_ids;
     info->long_row_entries = g->plan.bin.long_row;
     info->chunk_entries = g->plan.bin.chunk;
+    info->bin0_rows_per_warp = g->plan.bin.bin0_rows;
   } else {
     info->sweep_threads = (uint32_t)g->variant.threads;
     info->sweep_grid = (uint32_t)g->grid;

@@ -6,16 +6,18 @@
 // 1024-thread CTA per SM with the hub contributions staged in shared memory,
 // or four 256-thread CTAs per SM with the hubs in L1), how many hub
 // contributions the hot shape stages, how many more ids go through L1 with
-// an evict-last policy, and the long-row cut-offs: the row length above which
-// rows are cut into chunks (one warp each) and the chunk length. The tuner
-// times a few sweeps of each candidate on the resident graph with unit
-// degrees and keeps the fastest: first the cut-offs at the default launch
-// shape, then the launch shapes and hub tiers at the chosen cut-offs.
+// an evict-last policy, the long-row cut-offs (the row length above which
+// rows are cut into chunks, one warp each, and the chunk length) and the rows
+// per warp of bin 0 (two, half a warp each, or one). The tuner times a few
+// sweeps of each candidate on the resident graph with unit degrees and keeps
+// the fastest: first the cut-offs at the default launch shape, then bin 0's
+// rows per warp, then the launch shapes and hub tiers.
 // Launch shape and hub tiers do not change the summation order (ranks are
-// bitwise equal whichever is chosen); the cut-offs do (a chunked row is
-// summed per chunk, then over the chunks), so a tuned graph gives the ranks
-// of an untuned one created with the same NWGPU_LONG_ROW and
-// NWGPU_CHUNK_ENTRIES, bit for bit, and the graph info reports both.
+// bitwise equal whichever is chosen); the cut-offs and bin 0's rows per warp
+// do (a chunked row is summed per chunk, then over the chunks; a bin-0 row
+// over 16 or 32 lanes), so a tuned graph gives the ranks of an untuned one
+// created with the same NWGPU_LONG_ROW, NWGPU_CHUNK_ENTRIES and
+// NWGPU_BIN0_ROWS, bit for bit, and the graph info reports all three.
 //
 // Choices are cached per graph signature -- the SM count, log2 of the vertex
 // count in half steps, the average degree, and the share of entries in
@@ -40,7 +42,7 @@ struct Choice {
   int      hot = 1;
   uint32_t smem_ids = 0, l1_ids = 0;
   float    us = 0.f;  // measured time per sweep
-  uint32_t long_row = kLongRow, chunk = kChunk;
+  uint32_t long_row = kLongRow, chunk = kChunk, bin0_rows = kBin0Rows;
 };
 
 std::mutex                    g_mu;
@@ -65,9 +67,12 @@ void load_locked() {
     Choice c;
     if (!tab) continue;
     *tab = 0;
-    // hot smem_ids l1_ids us [long_row chunk]
-    if (sscanf(tab + 1, "%d %u %u %f %u %u", &c.hot, &c.smem_ids, &c.l1_ids, &c.us, &c.long_row, &c.chunk) >= 4)
+    // hot smem_ids l1_ids us [long_row chunk [bin0_rows]]
+    if (sscanf(tab + 1, "%d %u %u %f %u %u %u", &c.hot, &c.smem_ids, &c.l1_ids, &c.us, &c.long_row, &c.chunk,
+               &c.bin0_rows) >= 4) {
+      if (c.bin0_rows != 1u && c.bin0_rows != 2u) c.bin0_rows = kBin0Rows;
       g_cache[line] = c;
+    }
   }
   fclose(f);
 }
@@ -78,7 +83,8 @@ void store_locked(const std::string& sig, const Choice& c) {
   if (!path) return;
   FILE* f = fopen(path, "a");
   if (!f) return;
-  fprintf(f, "%s\t%d %u %u %.2f %u %u\n", sig.c_str(), c.hot, c.smem_ids, c.l1_ids, c.us, c.long_row, c.chunk);
+  fprintf(f, "%s\t%d %u %u %.2f %u %u %u\n", sig.c_str(), c.hot, c.smem_ids, c.l1_ids, c.us, c.long_row, c.chunk,
+          c.bin0_rows);
   fclose(f);
 }
 
@@ -116,7 +122,7 @@ int signature(nwgpu_graph* g, bool shapes_only, std::string* out) {
 }
 
 int apply(nwgpu_graph* g, const Choice& c) {
-  int rc = rebuild_bin_plan(g, c.long_row, c.chunk);
+  int rc = rebuild_bin_plan(g, c.long_row, c.chunk, c.bin0_rows);
   if (rc) return rc;
   BinPlan& p = g->plan;
   p.hot = c.hot != 0;
@@ -235,7 +241,7 @@ int autotune_blocked(nwgpu_graph* g) {
   return NWGPU_OK;
 }
 
-int cached_cutoffs(nwgpu_graph* g, uint32_t* long_row, uint32_t* chunk) {
+int cached_cutoffs(nwgpu_graph* g, uint32_t* long_row, uint32_t* chunk, uint32_t* bin0_rows) {
   if (g->n == 0) return NWGPU_OK;
   std::string sig;
   int         rc = signature(g, false, &sig);
@@ -246,6 +252,7 @@ int cached_cutoffs(nwgpu_graph* g, uint32_t* long_row, uint32_t* chunk) {
   if (it != g_cache.end()) {
     *long_row = it->second.long_row;
     *chunk = it->second.chunk;
+    *bin0_rows = it->second.bin0_rows;
   }
   return NWGPU_OK;
 }
@@ -283,6 +290,7 @@ int autotune_binned(nwgpu_graph* g, bool shapes_only) {
   best.us = 3.4e38f;
   best.long_row = g->plan.bin.long_row;
   best.chunk = g->plan.bin.chunk;
+  best.bin0_rows = g->plan.bin.bin0_rows;
   if (!shapes_only) {
     static const uint32_t cuts[][2] = {{kLongRow, kChunk}, {1024, 512}, {1024, 1024}, {4096, 1024},
                                        {4096, 2048}, {8192, 2048}, {512, 512}};
@@ -290,6 +298,7 @@ int autotune_binned(nwgpu_graph* g, bool shapes_only) {
     c.hot = g->plan.hot ? 1 : 0;
     c.smem_ids = g->plan.bin.smem_ids;
     c.l1_ids = g->plan.bin.l1_ids;
+    c.bin0_rows = kBin0Rows;
     for (const auto& cut : cuts) {
       c.long_row = cut[0];
       c.chunk = cut[1];
@@ -299,11 +308,22 @@ int autotune_binned(nwgpu_graph* g, bool shapes_only) {
       c.us = us;
       if (us < best.us) best = c;
     }
+    // bin 0 at the chosen cut-offs: a warp per row instead of half a warp
+    // (only when the bin has rows; the two differ in nothing else)
+    c = best;
+    c.bin0_rows = 1u;
+    if ((rc = apply(g, c))) return rc;
+    if (g->plan.bin.bin_row_end[0] > g->plan.bin.bin_row_begin[0]) {
+      float us = 0.f;
+      if ((rc = time_plan(g, a, sweeps, &us))) return rc;
+      c.us = us;
+      if (us < best.us) best = c;
+    }
   }
   // Candidates at those cut-offs: the hot shape with 16K / 32K / 48K staged
   // ids (as the shared memory allows) and an L1 tier of 0 / 16K / 32K more;
   // the 256-thread shape with 16K / 32K / 64K ids through L1.
-  const uint32_t long_row = best.long_row, chunk = best.chunk;
+  const uint32_t long_row = best.long_row, chunk = best.chunk, bin0_rows = best.bin0_rows;
   std::vector<Choice> cands;
   for (uint32_t s : {16384u, 32768u, 49152u}) {
     uint32_t st = s < lim ? s : lim;
@@ -315,6 +335,7 @@ int autotune_binned(nwgpu_graph* g, bool shapes_only) {
       c.l1_ids = st + l1;
       c.long_row = long_row;
       c.chunk = chunk;
+      c.bin0_rows = bin0_rows;
       bool dup = false;
       for (const Choice& d : cands) dup |= d.hot == 1 && d.smem_ids == c.smem_ids && d.l1_ids == c.l1_ids;
       if (!dup) cands.push_back(c);
@@ -326,6 +347,7 @@ int autotune_binned(nwgpu_graph* g, bool shapes_only) {
     c.l1_ids = l1;
     c.long_row = long_row;
     c.chunk = chunk;
+    c.bin0_rows = bin0_rows;
     cands.push_back(c);
   }
   for (Choice c : cands) {

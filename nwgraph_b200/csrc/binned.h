@@ -8,12 +8,14 @@ namespace nwgpu {
 // Defaults of the plan's two runtime cut-offs (the tuner searches both):
 constexpr uint32_t kLongRow = 2048;  // rows longer than this are split into chunks
 constexpr uint32_t kChunk = 1024;    // entries per long-row chunk (one warp)
+constexpr uint32_t kBin0Rows = 2;    // bin-0 rows per warp: 2 (half a warp each) or 1 (a whole warp)
 constexpr int      kNumBins = 8;     // warp per row, then G = 32, 16, 8, 4, 2, 1, empty
 
 struct BinnedArgs {
   SweepArgs       sw;                     // row_ptr / col / vectors / state / loop control
   uint32_t        long_row;               // rows longer than this are chunked (> 128)
   uint32_t        chunk;                  // entries per long-row chunk (a multiple of 256)
+  uint32_t        bin0_rows;              // bin-0 rows per warp (kBin0Rows unless tuned or set): 2 or 1
   uint32_t        num_long_rows;          // rows [0, num_long_rows) are chunked
   uint32_t        num_big_rows;           // rows [0, num_big_rows) have more than 32 chunks
   uint32_t        num_chunks;
@@ -23,7 +25,7 @@ struct BinnedArgs {
   uint32_t        bin_row_begin[kNumBins];
   uint32_t        bin_row_end[kNumBins];
   uint32_t        bin_warp_end[kNumBins]; // cumulative warps over the bins
-  // bin 0: 129..long_row entries, one warp per row; bins 1-6: G = 32..1 lanes
+  // bin 0: 129..long_row entries, half a warp or a warp per row; bins 1-6: G = 32..1 lanes
   // per row, two rows per lane group, rows of (2G, 4G] entries (G = 1: 1..4);
   // bin 7: empty rows
   uint32_t        smem_ids;               // hot variant: contrib[0, smem_ids) is staged in shared memory

@@ -183,9 +183,10 @@ cudaError_t dalloc(nwgpu_graph* g, T** p, uint64_t count) {
 }
 int ensure_solve_buffers(nwgpu_graph* g);
 int build_bin_plan(nwgpu_graph* g, const uint32_t* row_ptr, uint64_t n, bool hot, BinPlan* p,
-                   uint32_t long_row = kLongRow, uint32_t chunk = kChunk);
-// g->plan rebuilt with other long-row cut-offs, keeping its launch shape and hub tiers.
-int rebuild_bin_plan(nwgpu_graph* g, uint32_t long_row, uint32_t chunk);
+                   uint32_t long_row = kLongRow, uint32_t chunk = kChunk, uint32_t bin0_rows = kBin0Rows);
+// g->plan rebuilt with other long-row cut-offs or bin-0 rows per warp, keeping
+// its launch shape and hub tiers.
+int rebuild_bin_plan(nwgpu_graph* g, uint32_t long_row, uint32_t chunk, uint32_t bin0_rows);
 // Residual partials the handle's sweeps write: the merge-path sweep's, or the
 // binned plan's in its larger launch shape (the tuner may switch shapes).
 uint64_t residual_parts(const nwgpu_graph* g);
@@ -218,10 +219,10 @@ int ensure_wpr(nwgpu_graph* g);
 // shapes_only), launch shape and hub tiers for g (timed, or from the
 // per-signature cache) and sets g->plan accordingly.
 int autotune_binned(nwgpu_graph* g, bool shapes_only = false);
-// api_tune.cu: the long-row cut-offs cached for g's signature, if any (else
-// the arguments are left as they are), so a tuned graph like one already
-// tuned builds its bin plan once.
-int cached_cutoffs(nwgpu_graph* g, uint32_t* long_row, uint32_t* chunk);
+// api_tune.cu: the long-row cut-offs and bin-0 rows per warp cached for g's
+// signature, if any (else the arguments are left as they are), so a tuned
+// graph like one already tuned builds its bin plan once.
+int cached_cutoffs(nwgpu_graph* g, uint32_t* long_row, uint32_t* chunk, uint32_t* bin0_rows);
 // api_tune.cu: picks the blocked sweep's entries in flight and piece size (timed, or cached per signature).
 int autotune_blocked(nwgpu_graph* g);
 // degrees (input order, host or device) -> g->deg (internal order)

@@ -7,7 +7,8 @@
 //                               pr_binned_finish_kernel sums each row's chunk
 //                               partials in chunk order
 //   bin 0  128 < len <= long_row: half a warp per row (two rows per warp),
-//                               16 lanes stride the row
+//                               16 lanes walk the row; or, as the plan
+//                               sets (bin0_rows), a warp per row
 // (long_row and chunk are the plan's, 2048 and 1024 unless tuned or set)
 //   G = 32, 16, 8, 4, 2, 1      : rows of (G*2, G*4] entries (G = 1: 1..4),
 //                               G lanes per row, two rows per lane group,
@@ -232,7 +233,8 @@ __device__ __forceinline__ void load_window(const uint32_t* __restrict__ col, ui
 
 // Units that are entry ranges, one warp each, walked in 256-entry windows
 // (load_window). CHUNK: unit c = chunk c of a long row, partial sum to
-// chunk_part[c] (the long rows). Otherwise: unit w = row rb + w, epilogue.
+// chunk_part[c] (the long rows). Otherwise: unit w = row rb + w, epilogue
+// (bin 0 when the plan gives it a warp per row).
 template <bool HOT, bool CHUNK, int MODE>
 __device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src, float* __restrict__ cout, uint32_t rb,
                                             uint32_t nunits, uint32_t w, uint32_t nwarps, int lane) {
@@ -244,12 +246,13 @@ __device__ __forceinline__ double range_bin(const BinnedArgs& a, const Src& src,
       row = a.chunk_row[unit];
       const uint32_t rs = a.sw.row_ptr[row], re = a.sw.row_ptr[row + 1];
       k0 = rs + (unit - a.row_first_chunk[row]) * a.chunk;
-      k1 = min(re, k0 + a.chunk);
+      k1 = k0 + min(re - k0, a.chunk);  // no 32-bit wrap near the entry limit
       if (MODE == kModeRagged && ragged_frozen(a, row)) k1 = k0;  // a stopped graph's row: nothing to gather
     } else {
       row = rb + unit;
       k0 = ld_stream(a.sw.row_ptr + rb + unit);
       k1 = ld_stream(a.sw.row_ptr + rb + unit + 1);
+      if (MODE == kModeRagged && ragged_frozen(a, row)) k1 = k0;  // a stopped graph's row: nothing to gather
     }
   };
   uint32_t k0, k1, row, nk0 = 0, nk1 = 0, nrow = 0;
@@ -540,7 +543,10 @@ __global__ void __launch_bounds__(NT, 1024 / NT) pr_binned_sweep_kernel(const Bi
     const uint32_t w0 = first_unit(gwarp, nwarps, begin);
     const uint32_t rb = a.bin_row_begin[b], re = a.bin_row_end[b];
     switch (b) {
-      case 0: res += pair_bin<HOT, MODE>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
+      case 0:
+        res += a.bin0_rows == 1u ? range_bin<HOT, false, MODE>(a, src, cout, rb, nu, w0, nwarps, lane)
+                                 : pair_bin<HOT, MODE>(a, src, cout, rb, re, nu, w0, nwarps, lane);
+        break;
       case 1: res += group_bin<HOT, 32, MODE>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
       case 2: res += group_bin<HOT, 16, MODE>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
       case 3: res += group_bin<HOT, 8, MODE>(a, src, cout, rb, re, nu, w0, nwarps, lane); break;
@@ -675,8 +681,10 @@ __global__ void bin_bounds_kernel(const uint32_t* __restrict__ row_ptr, uint32_t
 
 __global__ void chunk_count_kernel(const uint32_t* __restrict__ row_ptr, uint32_t nlong, uint32_t chunk,
                                    uint32_t* __restrict__ cnt) {
-  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < nlong; r += gridDim.x * blockDim.x)
-    cnt[r] = (row_ptr[r + 1] - row_ptr[r] + chunk - 1) / chunk;
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < nlong; r += gridDim.x * blockDim.x) {
+    const uint32_t len = row_ptr[r + 1] - row_ptr[r];
+    cnt[r] = len / chunk + (len % chunk != 0u ? 1u : 0u);
+  }
 }
 
 __global__ void chunk_fill_kernel(const uint32_t* __restrict__ first, uint32_t nlong, uint32_t* __restrict__ chunk_row) {
