@@ -344,3 +344,41 @@ def test_binned_launch_shapes_and_modes_agree(gpu, graph, monkeypatch):
     for _ in range(2):
         d, _ = solve(g.row_ptr, g.col, deg)
         assert np.array_equal(d.view(np.uint32), b.view(np.uint32))
+
+
+def boundary_graph(seed=17):
+    """A directed graph whose row lengths sit on and beside every bin and window boundary of the binned sweep
+    (4-entry lanes, the G-bins' 2G/4G edges, bin 0's 128/129, 256-entry windows, the long-row cut-off 2048 and
+    1024-entry chunks), several rows of each, so that after relabelling the rows start at every offset mod 4."""
+    rng = np.random.default_rng(seed)
+    lengths = [1, 2, 3, 4, 5, 7, 8, 9, 15, 16, 17, 31, 32, 33, 63, 64, 65, 127, 128, 129, 130, 131, 255, 256, 257,
+               511, 512, 513, 1023, 1024, 1025, 2047, 2048, 2049, 2050, 3071, 3072, 3073, 4096, 4097, 9000]
+    lens = np.array([L for L in lengths for _ in range(5)] + [0] * 40, np.int64)
+    rng.shuffle(lens)
+    n = 6000
+    lens = np.concatenate([lens, rng.integers(0, 12, n - len(lens))])
+    rp = np.zeros(n + 1, np.uint32)
+    rp[1:] = np.cumsum(lens)
+    cl = rng.integers(0, n - 50, int(rp[-1])).astype(np.uint32)  # the last 50 vertices have no out-edges
+    deg = np.bincount(cl, minlength=n).astype(np.uint32)
+    return rp, cl, deg
+
+
+@pytest.mark.parametrize("env", [{}, {"NWGPU_BIN0_ROWS": "1"}, {"NWGPU_LONG_ROW": "256", "NWGPU_CHUNK_ENTRIES": "256"},
+                                 {"NWGPU_SWEEP": "binned"}])
+def test_rows_at_bin_and_window_boundaries(gpu, monkeypatch, env):
+    """Rows of every boundary length at every start alignment: the 128-bit id windows (long-row chunks, bin 0),
+    the G-bins and the empty rows against page_rank_v10 restated, at a fixed sweep count and at threshold 1e-5
+    with the same stopping sweep; the graph launch and the stream launch give the same bits."""
+    for k, v in env.items():
+        monkeypatch.setenv(k, v)
+    rp, cl, deg = boundary_graph()
+    a, _ = solve(rp, cl, deg, 0.0, 20)
+    b, _ = solve(rp, cl, deg, 0.0, 20, launch="stream")
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    ref, _, _ = O.jacobi_f32(rp, cl, deg, 0.85, 0.0, 20)
+    assert_close(a, ref)
+    r, st = solve(rp, cl, deg, 1e-5, 200)
+    ref, it, _ = O.jacobi_f32(rp, cl, deg, 0.85, 1e-5, 200)
+    assert st.iterations == it
+    assert_close(r, ref)
