@@ -32,7 +32,7 @@
 namespace nwgpu {
 
 // ---------------------------------------------------------------------------
-// TMA bulk copy + mbarrier helpers (no multicast anywhere)
+// TMA bulk copy + mbarrier helpers (each copy lands in the issuing CTA's own shared memory)
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
