@@ -130,8 +130,8 @@ int nwgpu_shard_create(const uint32_t* row_ptr, const uint32_t* col, uint64_t n,
   *out = nullptr;
   if (!row_ptr || (nnz && !col) || !bounds) return fail(NWGPU_ERR_INVALID_ARG, "row_ptr / col / bounds is NULL");
   if (world == 0 || rank >= world) return fail(NWGPU_ERR_INVALID_ARG, "rank %u of world %u", rank, world);
-  if (n < 2 || n >= 0xFFFFFFF0ull || nnz > 0xFFFFFFF0ull)
-    return fail(NWGPU_ERR_INVALID_ARG, "n = %llu, nnz = %llu: a shard needs 2 <= n < 2^32 - 16 and nnz < 2^32 - 16",
+  if (n < 2 || n >= 0xFFFFFFF0ull || nnz > kMaxEntries)
+    return fail(NWGPU_ERR_INVALID_ARG, "n = %llu, nnz = %llu: a shard needs 2 <= n < 2^32 - 16 and nnz <= 2^32 - 512",
                 (unsigned long long)n, (unsigned long long)nnz);
   if (bounds[0] != 0 || bounds[world] != n)
     return fail(NWGPU_ERR_INVALID_ARG, "bounds must run from 0 to n = %llu", (unsigned long long)n);
