@@ -369,7 +369,8 @@ def boundary_graph(seed=17):
 def test_rows_at_bin_and_window_boundaries(gpu, monkeypatch, env):
     """Rows of every boundary length at every start alignment: the 128-bit id windows (long-row chunks, bin 0),
     the G-bins and the empty rows against page_rank_v10 restated, at a fixed sweep count and at threshold 1e-5
-    with the same stopping sweep; the graph launch and the stream launch give the same bits."""
+    with the same stopping sweep; the graph launch and the stream launch give the same bits; the weighted mode's
+    SpMV against FP64 row sums."""
     for k, v in env.items():
         monkeypatch.setenv(k, v)
     rp, cl, deg = boundary_graph()
@@ -382,3 +383,14 @@ def test_rows_at_bin_and_window_boundaries(gpu, monkeypatch, env):
     ref, it, _ = O.jacobi_f32(rp, cl, deg, 0.85, 1e-5, 200)
     assert st.iterations == it
     assert_close(r, ref)
+    # the weighted mode of the same walk: SpMV against FP64 row sums
+    w = G.edge_weights(len(cl), seed=3)
+    x = np.random.default_rng(5).standard_normal(len(rp) - 1).astype(np.float32)
+    with Graph(rp, cl, weights=w) as h:
+        y = np.empty(len(rp) - 1, np.float32)
+        h.spmv(x, y)
+    rows = np.repeat(np.arange(len(rp) - 1), np.diff(rp.astype(np.int64)))
+    t = w.astype(np.float64) * x.astype(np.float64)[cl]
+    exact = np.bincount(rows, weights=t, minlength=len(rp) - 1)
+    mag = np.bincount(rows, weights=np.abs(t), minlength=len(rp) - 1)
+    assert np.all(np.abs(y - exact) <= 1e-6 * mag + 1e-30)
